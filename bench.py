@@ -1,0 +1,364 @@
+#!/usr/bin/env python
+"""Benchmark: ms per MAS-PCG solve to relative residual 1e-8 at 1.6 M DOF.
+
+Workload: the 80^3 tetrahedral elasticity system (531,441 vertices, 1,594,323 DOF, Kuhn 6-tet
+split, vertices jittered +-0.2h, E lognormal(ln 1e5, 1.0) per element, K + M/h^2 with h = 1e-2,
+Dirichlet on x = 0), BSR 3x3, 32-vertex Morton subdomains, b ~ N(0, 1). Synthetic, seeded.
+
+A step is one solve from x0 = 0 to ||b - A x|| <= 1e-8 ||b||.
+  * value:  the chosen configuration (FP32 MAS, true residual every 50, device-side convergence test
+            every iteration), inputs resident in HBM, solve_device on torch's stream, CUDA events.
+  * e2e:    the same solve through the public host API (Solver.solve) from pinned host memory:
+            b host->device and x device->host inside the timed region.
+  * plain_fp64_ms: the reference's algorithm on the same GPU (FP64 MAS, true residual every 4,
+            convergence tested every 10 iterations) -- the denominator of the 2x target.
+  * roofline: the SpMV (the dominant kernel) from per-launch CUDA events in a profiled solve.
+  * cpu_baseline: the CPU MAS-PCG oracle (OpenMP C++ port) on this host, bounded sample.
+
+--impl reference runs the reference's algorithm on the host cores (the oracle port: the reference's
+CUDA MAS path cannot be built in this image), each step a bounded sample of PCG iterations scaled
+to a full solve.
+
+Multi-GPU: the path does not shard (one system per solve): N ranks run independent replicas;
+value = whole-job ms per solve = max-over-ranks time / (N * K).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "ms per solve to rel-residual 1e-8 at 1.6M DOF, chosen vs plain FP64 MAS-PCG"
+UNIT = "ms/solve"
+TOL = 1e-8
+
+CHOSEN = {"block_dim": 3, "relative_tolerance": TOL, "absolute_tolerance": 0.0, "max_iter": 5000,
+          "precision": "fp32", "true_residual_period": 50, "check_period": 1, "poll_period": 8}
+PLAIN = {"block_dim": 3, "relative_tolerance": TOL, "absolute_tolerance": 0.0, "max_iter": 5000,
+         "precision": "fp64", "true_residual_period": 4, "check_period": 10, "poll_period": 8}
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--grid", type=int, default=80)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--cpu-sample-iters", type=int, default=20)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def spmv_bytes(nnzb: int, n: int) -> int:
+    """Algorithmic bytes of one block SpMV: 3x3 FP64 values + int32 column per block, row
+    metadata, x read once and y written once."""
+    return nnzb * (72 + 4) + (n // 3 + 1) * 4 + 2 * 8 * n
+
+
+def mas_bytes(total_mats: int, n: int, value_bytes: int) -> int:
+    return total_mats * 4656 * value_bytes + 4 * 8 * n
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path).read().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def cpu_baseline_sample(system, padded, iterations: int, sample_iters: int) -> dict:
+    """CPU MAS-PCG (oracle port, OpenMP) on this host: time `sample_iters` reference-mode PCG
+    iterations on the same system and partition, scale to the solve's iteration count."""
+    from oracle import oracle as O
+
+    perm, offsets = O.partition_from_padded(padded)
+    t0 = time.time()
+    orc = O.MasOracle(system.outer, system.inner, system.vals, system.n, 3, perm, offsets)
+    fact_s = time.time() - t0
+    orc.time_iterations(2, 4)
+    sec = orc.time_iterations(sample_iters, 4)
+    per_iter_ms = sec * 1000.0 / sample_iters
+    return {"value": per_iter_ms * iterations, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "sample": f"{sample_iters} MAS-PCG iterations (FP64, true residual every 4) of the 80^3 system, "
+                      f"{per_iter_ms:.1f} ms/iteration x {iterations} iterations; factorize {fact_s:.1f} s "
+                      f"not included"}
+
+
+def run_ours(args) -> None:
+    import torch
+
+    from polysolve_b200 import Solver, synthetic
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist_mod
+
+        dist_mod.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=torch.device(f"cuda:{local}"))
+        dist = dist_mod
+
+    system = synthetic.workload_grid80(seed=args.seed, N=args.grid)
+    b = synthetic.rhs(system.n, seed=args.seed)
+    A = system.scipy()
+    n = system.n
+
+    def make(params):
+        s = Solver.create("MAS", "")
+        s.set_parameters({"MAS": params})
+        s.set_positions(system.positions)
+        s.analyze_pattern(A, n)
+        t0 = time.time()
+        s.factorize(A)
+        return s, time.time() - t0
+
+    chosen, fact_s = make(CHOSEN)
+    plain, _ = make(PLAIN)
+    stream = torch.cuda.current_stream()
+    chosen.set_stream(stream.cuda_stream)
+    plain.set_stream(stream.cuda_stream)
+
+    db = torch.tensor(b, device="cuda")
+    dx = torch.zeros_like(db)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # Warm-up
+    for _ in range(max(args.warmup, 3)):
+        chosen.solve_device(db.data_ptr(), dx.data_ptr(), n)
+    torch.cuda.synchronize()
+    launches0 = chosen.get_info()["kernel_launches_total"]
+
+    clocks = Clocks(local)
+    barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        chosen.solve_device(db.data_ptr(), dx.data_ptr(), n)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clk = clocks.stop()
+    total_ms = e0.elapsed_time(e1)
+    info = chosen.get_info()
+    gpu_launches = info["kernel_launches_total"] - launches0
+    t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_ms = float(t.item())
+    ms_per_step = max_ms / args.steps
+    value = max_ms / (args.steps * world)
+
+    x = dx.cpu().numpy()
+    relres = float(np.linalg.norm(A @ x - b) / np.linalg.norm(b))
+
+    # Plain FP64 (the reference's algorithm) on the same GPU.
+    plain.solve_device(db.data_ptr(), dx.data_ptr(), n)
+    torch.cuda.synchronize()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    psteps = max(1, min(args.steps, 3))
+    p0.record(stream)
+    for _ in range(psteps):
+        plain.solve_device(db.data_ptr(), dx.data_ptr(), n)
+    p1.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = p0.elapsed_time(p1) / psteps
+    pinfo = plain.get_info()
+    x_plain = dx.cpu().numpy()
+    relres_plain = float(np.linalg.norm(A @ x_plain - b) / np.linalg.norm(b))
+
+    # End to end through the public host API, pinned host buffers.
+    hb = torch.from_numpy(b).pin_memory()
+    hx = torch.zeros(n, dtype=torch.float64).pin_memory()
+    hb_np, hx_np = hb.numpy(), hx.numpy()
+    chosen.solve(hb_np, hx_np)
+    torch.cuda.synchronize()
+    barrier()
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    q0.record(stream)
+    for _ in range(args.steps):
+        chosen.solve(hb_np, hx_np)
+    q1.record(stream)
+    torch.cuda.synchronize()
+    te = torch.tensor([q0.elapsed_time(q1)], device="cuda", dtype=torch.float64)
+    if dist is not None:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = float(te.item()) / (args.steps * world)
+
+    # Roofline of the dominant kernel (SpMV) from per-launch events in a profiled solve.
+    chosen.set_parameters({"MAS": {"profile_kernels": True}})
+    chosen.solve_device(db.data_ptr(), dx.data_ptr(), n)
+    pinfo_k = chosen.get_info()
+    chosen.set_parameters({"MAS": {"profile_kernels": False}})
+    torch.cuda.synchronize()
+    sizes = chosen.sizes()
+    kms, kl = pinfo_k.get("kernel_ms", {}), pinfo_k.get("kernel_launches", {})
+    spmv_launch_ms = kms.get("spmv_pap", 0.0) / max(1, kl.get("spmv_pap", 1))
+    spmv_b = spmv_bytes(sizes["nnzb"], n)
+    peaks = {}
+    try:
+        peaks = json.load(open(ROOT / "MEASURED_PEAKS.json"))
+    except Exception:
+        pass
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = spmv_b / (spmv_launch_ms * 1e-3) / 1e9 if spmv_launch_ms > 0 else 0.0
+    symv_launch_ms = kms.get("mas_symv0", 0.0) / max(1, kl.get("mas_symv0", 1))
+    mas_b = mas_bytes(sizes["banks"], n, 4)
+    kernel_table = {k: {"launches": kl.get(k, 0), "ms_total": round(kms.get(k, 0.0), 4),
+                        "ms_per_launch": round(kms.get(k, 0.0) / max(1, kl.get(k, 1)), 5)} for k in kl}
+
+    out = {
+        "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": round(ms_per_step, 4), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 (SpMV, dots, updates) + f32 (MAS apply)",
+        "data": "synthetic (seeded 80^3 jittered tet elasticity, b ~ N(0,1))",
+        "config": {"workload": f"{args.grid}^3 jittered tet elasticity, {n} DOF, nnzb {sizes['nnzb']}, "
+                               f"{sizes['banks']} 32-vertex Morton subdomains, {sizes['level_num']} coarse levels",
+                   "chosen": "fp32 MAS, true residual every 50, convergence test every iteration, x0 = 0",
+                   "tolerance": TOL, "parallelism": f"replicas x{world}",
+                   "l2": "working set > L2 (A 560 MB + MAS 340 MB per solve iteration)"},
+        "iterations": info["solver_iter"], "relative_residual": relres,
+        "plain_fp64_ms": round(plain_ms, 4), "plain_fp64_iterations": pinfo["solver_iter"],
+        "plain_fp64_relative_residual": relres_plain, "speedup_vs_plain_fp64": round(plain_ms / ms_per_step, 3),
+        "factorize_s": round(fact_s, 3),
+        "e2e": {"value": round(e2e_value, 4), "unit": UNIT, "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
+        "gpu_launches": int(gpu_launches),
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None, "kernel": "spmv_pap",
+                     "algorithmic_bytes_per_launch": spmv_b, "launch_ms": round(spmv_launch_ms, 5),
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured copy)" if peaks else "fallback 6650 GB/s"},
+        "mas_symv0": {"launch_ms": round(symv_launch_ms, 5), "algorithmic_bytes_per_launch": mas_b,
+                      "achieved_gbs": round(mas_b / (symv_launch_ms * 1e-3) / 1e9, 1) if symv_launch_ms > 0 else None},
+        "kernels": kernel_table,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline_sample(system, chosen.ordering(), pinfo["solver_iter"],
+                                                  args.cpu_sample_iters)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    del chosen, plain
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def run_reference(args) -> None:
+    """The reference's algorithm (MAS-PCG, FP64, true residual every 4, check every 10) on the host
+    cores via the oracle port, each step a bounded sample of PCG iterations scaled to a solve."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    from polysolve_b200 import synthetic
+
+    system = synthetic.workload_grid80(seed=args.seed, N=args.grid)
+    iso = O.isolated_blocks(system.outer, system.inner, system.n, 3)
+    perm, offsets = O.morton_order(system.positions, iso)
+    t0 = time.time()
+    orc = O.MasOracle(system.outer, system.inner, system.vals, system.n, 3, perm, offsets)
+    fact_s = time.time() - t0
+    # Iteration count of the full reference-mode solve: run it once (warm-up) when affordable,
+    # otherwise scale by the count the same algorithm needs on this workload.
+    b = synthetic.rhs(system.n, seed=args.seed)
+    t0 = time.time()
+    _, info = orc.pcg(b, rel_tol=TOL, abs_tol=0.0, max_iter=5000)
+    full_solve_s = time.time() - t0
+    iterations = info["solver_iter"]
+    sample = max(1, args.cpu_sample_iters // 2)
+    for _ in range(max(args.warmup, 3) - 1):
+        orc.time_iterations(sample, 4)
+    times = []
+    for _ in range(args.steps):
+        sec = orc.time_iterations(sample, 4)
+        times.append(sec * 1000.0 / sample * iterations)
+    value = statistics.mean(times)
+    out = {"impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": round(value, 3),
+           "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded 80^3 jittered tet elasticity, b ~ N(0,1))",
+           "config": {"workload": f"{args.grid}^3 jittered tet elasticity, {system.n} DOF",
+                      "algorithm": "reference MAS-PCG (FP64, true residual every 4, check every 10)",
+                      "implementation": "CPU oracle port (OpenMP C++); the reference CUDA path needs CCCL 3.3, "
+                                        "Eigen, KaMinPar (absent)",
+                      "tolerance": TOL},
+           "iterations": iterations, "full_solve_s": round(full_solve_s, 2), "factorize_s": round(fact_s, 2),
+           "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                            "sample": f"{sample} PCG iterations per step scaled by {iterations} iterations"},
+           "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

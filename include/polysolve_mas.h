@@ -1,0 +1,149 @@
+/*
+ * polysolve_mas.h — C ABI of the B200 MAS-PCG solver.
+ *
+ * A drop-in for polysolve's "MAS" linear solver (src/polysolve/linear/MASSolver.hpp:35-72 behind
+ * the polysolve::linear::Solver interface, src/polysolve/linear/Solver.hpp:31-132). Plain C types
+ * only: no exceptions cross this boundary. Every call returns an int status (MAS_OK = 0); on a
+ * non-zero status mas_last_error() returns a message that starts with "[MAS]", as the reference's
+ * exceptions do. The C++ header include/polysolve/linear/MASSolver.hpp turns statuses back into
+ * the reference's exception types.
+ *
+ * Matrices are square CSC (column-major) with int32 indices, the layout of polysolve's
+ * StiffnessMatrix = Eigen::SparseMatrix<double, ColMajor, int> (src/polysolve/Types.hpp:11).
+ * A must be symmetric (CG requires it; the preconditioner reads only its upper triangle).
+ *
+ * Threading: a handle is used by one host thread at a time. All device work of a handle runs on
+ * the handle's own CUDA stream on the device that was current when the handle was created.
+ */
+#ifndef POLYSOLVE_MAS_H
+#define POLYSOLVE_MAS_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. */
+#define MAS_OK 0
+#define MAS_ERR_INVALID 1         /* bad argument or parameter (reference: std::runtime_error) */
+#define MAS_ERR_OOM 2             /* device allocation failed (reference: CudaOutOfMemoryError) */
+#define MAS_ERR_NOT_FACTORIZED 3  /* solve before factorize / size mismatch (MASSolver.cu:380-383) */
+#define MAS_ERR_CUDA 4            /* a CUDA runtime call failed */
+#define MAS_ERR_NONFINITE 5       /* NaN/inf initial residual (MASSolver.cu:483-486) */
+#define MAS_ERR_INVERSE 6         /* a subdomain inverse hit a zero/non-finite pivot (MASPreconditioner.cu:931-935) */
+#define MAS_ERR_TIMEOUT 7         /* a device-side wait hit its iteration limit */
+#define MAS_ERR_NO_DEVICE 8       /* no CUDA device (MASSolver.cu:188-191, "No Nvidia GPU!!") */
+
+/* Solver status after a solve, MASSolverStatus (MASSolver.hpp:10-16). */
+#define MAS_STATUS_RUNNING 0
+#define MAS_STATUS_REACH_RELATIVE_TOLERANCE 1
+#define MAS_STATUS_REACH_ABSOLUTE_TOLERANCE 2
+#define MAS_STATUS_REACH_MAX_ITERATIONS 3
+
+typedef struct mas_solver mas_solver;
+
+/* Solver::create(solver, precond) (Solver.cpp:310-499; "MAS" at :403-407). Only "MAS" is
+ * accepted; precond is ignored as in the reference. Parameters get the implementation defaults
+ * (MASSolver.cu:137-143): block_dim 1, max_iter 5000, relative_tolerance 1e-5,
+ * absolute_tolerance 1e-8, lazy_partitioning false, use_preconditioned_residual_norm false. */
+int mas_create(const char *solver, const char *precond, mas_solver **out);
+
+/* Solver::create(json params, logger, strict) (Solver.cpp:145-167): validates params against
+ * the /MAS spec (linear-solver-spec.json:456-509), injects the spec defaults (max_iter 10000,
+ * relative_tolerance 1e-4, lazy_partitioning true, ...) and calls set_parameters. */
+int mas_create_json(const char *params_json, int strict_validation, mas_solver **out);
+
+/* ~MASSolver. Safe on NULL. */
+void mas_destroy(mas_solver *h);
+
+/* MASSolver::set_parameters (MASSolver.cu:605-614, 198-212): reads the "MAS" object of the given
+ * JSON object and silently ignores the call when it is absent. Keys of the reference: block_dim,
+ * max_iter, relative_tolerance, absolute_tolerance, lazy_partitioning,
+ * use_preconditioned_residual_norm. Keys this implementation adds (ignored by the reference):
+ * precision ("fp64" | "fp32"), true_residual_period (int, reference 4), check_period (int,
+ * reference 10), initial_guess ("zero" | "input"; reference: zero), beta ("fletcher_reeves" |
+ * "polak_ribiere"), ordering ("auto" | "morton" | "graph" | "natural"), poll_period (int: iterations
+ * launched between looks at the device state), profile_kernels (bool: CUDA-event time per kernel
+ * kind, reported by get_info). */
+int mas_set_parameters(mas_solver *h, const char *params_json);
+
+/* MASSolver::get_info (MASSolver.cu:214-219): writes a JSON object with solver_iter,
+ * solver_error (absolute residual norm), solver_status (reference strings), plus extras.
+ * *needed receives strlen+1; the text is truncated to cap bytes (always NUL terminated). */
+int mas_get_info(const mas_solver *h, char *buf, size_t cap, size_t *needed);
+
+/* MASSolver::name() == "MAS" (MASSolver.cu:636-639). */
+const char *mas_name(void);
+
+/* MASSolver::analyze_pattern (MASSolver.cu:621-624): a no-op in the reference; here it only
+ * checks the arguments. */
+int mas_analyze_pattern(mas_solver *h, int n, const int *outer, const int *inner, int nnz, int precond_num);
+
+/* New, optional: vertex positions (xyz per block row, nverts = ceil(n / block_dim)) for the
+ * Morton subdomain ordering. Without positions factorize orders the blocks by graph bisection.
+ * The reference partitions with KaMinPar instead (MASSolver.cu:223-242). */
+int mas_set_positions(mas_solver *h, const double *xyz, int nverts);
+
+/* MASSolver::factorize(A) (MASSolver.cu:292-374): A as CSC host arrays outer[n+1], inner[nnz],
+ * vals[nnz]. Builds the subdomain ordering, the permuted block matrix and the MAS
+ * preconditioner on the device. With lazy_partitioning the ordering is reused while n is
+ * unchanged; when the sparsity pattern is also unchanged only the values are re-scattered. */
+int mas_factorize_csc(mas_solver *h, int n, const int *outer, const int *inner, const double *vals, int nnz);
+
+/* MASSolver::solve(b, x) (MASSolver.cu:376-409): host vectors of length n. With initial_guess
+ * "zero" (the reference's behaviour, MASSolver.cu:395-398) x is output only; with "input" x is
+ * also the starting guess. Synchronous. Non-convergence is not an error: see get_info. */
+int mas_solve(mas_solver *h, const double *b, double *x, int n);
+
+/* New: nrhs independent right-hand sides, column-major B[n * nrhs] / X[n * nrhs]. */
+int mas_solve_multi(mas_solver *h, const double *B, double *X, int n, int nrhs);
+
+/* New: solve with device pointers (length n, caller's order) on the handle's stream; the call
+ * returns when the solve has finished. */
+int mas_solve_device(mas_solver *h, const double *d_b, double *d_x, int n);
+
+/* New: run the handle's device work on the caller's CUDA stream (a cudaStream_t; NULL restores
+ * the handle's own stream). Calls still return only when their work has finished. */
+int mas_set_stream(mas_solver *h, void *stream);
+
+/* Last error message of the handle ("" if none). With h == NULL: the last mas_create error. */
+const char *mas_last_error(const mas_solver *h);
+
+/* ------------------------------------------------------------------------------------------
+ * Inspection entry points (new; used by parity tests and tools). Vectors here are in the
+ * solver's padded block order: node = bank * 32 + lane, length nodes * block_dim.
+ * ---------------------------------------------------------------------------------------- */
+
+/* sizes[0..11] = n, block_dim, V (block rows), banks, nodes (= banks*32), nnzb, level_num,
+ * total_mats, cco_nums[0..3]. */
+int mas_get_sizes(const mas_solver *h, int *sizes);
+
+/* padded[V]: padded node id of each original block row. */
+int mas_get_ordering(const mas_solver *h, int *padded, int V);
+
+/* Host-only (no device needed): the subdomain ordering factorize would compute. mode is "morton"
+ * (xyz required, one point per block row), "graph" or "natural". Writes padded[ceil(n/bd)] and
+ * *banks. Replaces the reference's KaMinPar partition (mas_utils/GraphPartition.cpp:176-289). */
+int mas_order_blocks(int n, const int *outer, const int *inner, int block_dim, const double *xyz, const char *mode,
+                     int *padded, int *banks);
+
+/* map[nodes * 4]: coarse-space id per padded node and level (-1 for virtual nodes and unused
+ * levels), the CoarseSpace map of MASPreconditioner.hpp:30-39 in padded order. */
+int mas_get_coarse_map(const mas_solver *h, int *map, int nodes);
+
+/* Inverse matrices in packed-upper row-major FP64 (MASPreconditioner.hpp:41-53 layout), matrix
+ * m at out + m * (N*(N+1)/2), N = 32 * block_dim, for all total_mats matrices. */
+int mas_get_inverses(const mas_solver *h, double *out, size_t count);
+
+/* y = A x on host vectors in padded order. */
+int mas_debug_spmv(mas_solver *h, const double *x, double *y, int len);
+
+/* z = M^-1 r (MAS apply) on host vectors in padded order. */
+int mas_debug_apply(mas_solver *h, const double *r, double *z, int len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* POLYSOLVE_MAS_H */

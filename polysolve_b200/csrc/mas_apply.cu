@@ -1,0 +1,560 @@
+// MAS preconditioner apply (sm_100a): z = sum_l P_l A_l^-1 P_l^T r.
+//
+// The reference (MASPreconditioner.cu:1099-1164) zeroes two multi-level vectors, restricts with
+// warp segmented sums plus FP64 atomics, multiplies every level's packed 96 x 96 inverse with one
+// 96-thread CTA each (symv_upper_packed, :665-705), and prolongs in a third kernel. Here:
+//
+//  * the level-0 restriction is fused into whichever kernel produced r (SpMV residual or the
+//    x/r update): per-bank sums of each connected component, deterministic;
+//  * k_coarse: one CTA per coarse matrix sums its components' level-0 sums (member lists) and
+//    multiplies with its inverse -> zc;
+//  * k_symv0: persistent warps stream the level-0 inverses through shared memory with
+//    cp.async.bulk (two stages per warp, mbarrier completion), multiply them with the bank's r,
+//    add the coarse corrections (prolongation), write z and reduce r . z; the last CTA then
+//    runs the PCG bookkeeping of the reference (convergence test, beta).
+//
+// Inverses are stored tile-packed (see mas_internal.h): the same N (N + 1) / 2 values as packed
+// upper storage, laid out so a warp reads every 32 x 32 tile conflict-free and uses each value
+// for both y_I += T x_J and y_J += T^T x_I; the transposed sums are combined across lanes with a
+// 31-shuffle reduce-transpose per column tile.
+
+#include "mas_common.cuh"
+
+namespace pmas
+{
+    namespace
+    {
+        template <class Real>
+        struct Vec4;
+        template <>
+        struct Vec4<float>
+        {
+            using type = float4;
+        };
+        template <>
+        struct Vec4<double>
+        {
+            using type = double4;
+        };
+
+        // Lane l receives sum over lanes of c[l]; c is destroyed. 31 shuffles.
+        template <class Real>
+        __device__ __forceinline__ Real transpose_sum32(Real (&c)[32], int lane)
+        {
+#pragma unroll
+            for (int s = 16; s >= 1; s >>= 1)
+            {
+                const bool upper = (lane & s) != 0;
+#pragma unroll
+                for (int i = 0; i < s; ++i)
+                {
+                    const Real send = upper ? c[i] : c[i + s];
+                    const Real keep = upper ? c[i + s] : c[i];
+                    c[i] = keep + __shfl_xor_sync(FULL, send, s);
+                }
+            }
+            return c[0];
+        }
+
+        // y = M x for one tile-packed symmetric matrix M (N = 32 * T) in shared memory, x in shared
+        // memory. Lane l returns y[32 t + l] in yr[t].
+        template <int T, class Real>
+        __device__ __forceinline__ void symv_tiles(const Real *__restrict__ M, const Real *__restrict__ xs, int lane,
+                                                   Real (&yr)[T])
+        {
+            using V4 = typename Vec4<Real>::type;
+#pragma unroll
+            for (int t = 0; t < T; ++t)
+                yr[t] = Real(0);
+            int off = 0;
+#pragma unroll
+            for (int J = 0; J < T; ++J)
+            {
+                Real cy[32];
+#pragma unroll
+                for (int j = 0; j < 32; ++j)
+                    cy[j] = Real(0);
+#pragma unroll
+                for (int I = 0; I < J; ++I)
+                {
+                    const Real *tile = M + off + I * 1024;
+                    const Real xI = xs[32 * I + lane];
+                    Real a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+#pragma unroll
+                    for (int j4 = 0; j4 < 8; ++j4)
+                    {
+                        const V4 v = *reinterpret_cast<const V4 *>(tile + j4 * 128 + lane * 4);
+                        const V4 xv = *reinterpret_cast<const V4 *>(xs + 32 * J + 4 * j4);
+                        a0 = fma(v.x, xv.x, a0);
+                        a1 = fma(v.y, xv.y, a1);
+                        a2 = fma(v.z, xv.z, a2);
+                        a3 = fma(v.w, xv.w, a3);
+                        cy[4 * j4 + 0] = fma(v.x, xI, cy[4 * j4 + 0]);
+                        cy[4 * j4 + 1] = fma(v.y, xI, cy[4 * j4 + 1]);
+                        cy[4 * j4 + 2] = fma(v.z, xI, cy[4 * j4 + 2]);
+                        cy[4 * j4 + 3] = fma(v.w, xI, cy[4 * j4 + 3]);
+                    }
+                    yr[I] += (a0 + a1) + (a2 + a3);
+                }
+                off += J * 1024;
+                // Diagonal tile, upper triangle by columns.
+                {
+                    const Real *dt = M + off;
+                    const Real xJ = xs[32 * J + lane];
+                    Real a0 = 0, a1 = 0;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j)
+                    {
+                        const Real v = (lane <= j) ? dt[j * (j + 1) / 2 + lane] : Real(0);
+                        const Real xj = xs[32 * J + j];
+                        if (j & 1)
+                            a1 = fma(v, xj, a1);
+                        else
+                            a0 = fma(v, xj, a0);
+                        cy[j] = fma((lane < j) ? v : Real(0), xJ, cy[j]);
+                    }
+                    yr[J] += a0 + a1;
+                    off += 528;
+                }
+                yr[J] += transpose_sum32<Real>(cy, lane);
+            }
+        }
+
+        // Finish of an iteration (last CTA of k_symv0): the reference's per-iteration scalar work
+        // and convergence test (MASSolver.cu:505, 526-583), on the device.
+        __device__ void pcg_finalize(PcgState *st, const PcgConfig &cfg, int iter, int mode, double rz, double rzcross)
+        {
+            if (mode == 1)
+            {
+                st->rz = rz;
+                st->rz0 = rz;
+                st->iter = 0;
+                if (isnan(rz) || !isfinite(rz))
+                {
+                    st->error = ERR_NONFINITE;
+                    st->done = 1;
+                }
+                return;
+            }
+            const double rz_old = st->rz;
+            st->rz_old = rz_old;
+            st->rz = rz;
+            st->rzold_cross = rzcross;
+            st->iter = iter;
+            bool conv = false;
+            if (iter % cfg.check_period == 0)
+            {
+                const double rel2 = cfg.rel_tol * cfg.rel_tol, abs2 = cfg.abs_tol * cfg.abs_tol;
+                if (cfg.use_prec_norm)
+                {
+                    st->res_norm = sqrt(rz);
+                    if (rz <= rel2 * st->rz0 || rz <= abs2)
+                    {
+                        st->status = (rz <= abs2) ? 2 : 1;
+                        conv = true;
+                    }
+                }
+                else
+                {
+                    const double rr = st->rr;
+                    st->res_norm = sqrt(rr);
+                    if (rr <= rel2 * st->rr0 || rr <= abs2)
+                    {
+                        st->status = (rr <= abs2) ? 2 : 1;
+                        conv = true;
+                    }
+                }
+            }
+            if (conv)
+                st->done = 1;
+            else if (cfg.polak_ribiere)
+            {
+                double beta = (fabs(rz_old) < 1e-20) ? 0.0 : (rz - rzcross) / rz_old;
+                st->beta = beta > 0.0 ? beta : 0.0;
+            }
+            else
+                st->beta = (fabs(rz_old) < 1e-20) ? 0.0 : rz / rz_old;
+            if (iter == cfg.max_iter)
+            {
+                st->status = 3;
+                st->done = 1;
+            }
+        }
+
+        template <int BD, class Real>
+        struct Symv0Layout
+        {
+            static constexpr int N = 32 * BD;
+            static constexpr int S = N * (N + 1) / 2;
+            static constexpr int STAGE_BYTES = S * (int)sizeof(Real);
+            static constexpr int XS_BYTES = ((N * (int)sizeof(Real)) + 15) / 16 * 16;
+            static constexpr int WARP_BYTES = 2 * STAGE_BYTES + XS_BYTES + 16;
+            static constexpr int SMEM_LIMIT = 232448;
+            static constexpr int W0 = SMEM_LIMIT / WARP_BYTES;
+            static constexpr int WARPS = W0 > 16 ? 16 : W0;
+            static_assert(STAGE_BYTES % 16 == 0, "bulk copies need 16-byte multiples");
+        };
+
+        // mode 0: plain apply; 1: initial PCG apply (rz0); 2: PCG iteration.
+        template <int BD, class Real, int MODE>
+        __global__ void __launch_bounds__(Symv0Layout<BD, Real>::WARPS * 32)
+            k_symv0(MasView mas, const double *__restrict__ r, double *__restrict__ z, PcgState *st, ReduceBuf red,
+                    PcgConfig cfg, int iter)
+        {
+            using L = Symv0Layout<BD, Real>;
+            constexpr int N = L::N, S = L::S, WARPS = L::WARPS;
+            constexpr int THREADS = WARPS * 32;
+            if (MODE != 0 && st->done)
+                return;
+            extern __shared__ __align__(128) unsigned char smem[];
+            const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+            unsigned char *base = smem + (size_t)w * L::WARP_BYTES;
+            Real *stage0 = reinterpret_cast<Real *>(base);
+            Real *stage1 = reinterpret_cast<Real *>(base + L::STAGE_BYTES);
+            Real *xs = reinterpret_cast<Real *>(base + 2 * L::STAGE_BYTES);
+            uint64_t *bar = reinterpret_cast<uint64_t *>(base + 2 * L::STAGE_BYTES + L::XS_BYTES);
+            const Real *inv = static_cast<const Real *>(mas.inv);
+            const int banks = mas.banks;
+            const int total_warps = gridDim.x * WARPS;
+            const int gw = blockIdx.x * WARPS + w;
+            int *errp = st ? &st->error : nullptr;
+
+            if (lane == 0)
+            {
+                mbar_init(&bar[0], 1);
+                mbar_init(&bar[1], 1);
+                fence_mbar_init();
+            }
+            __syncwarp();
+            if (lane == 0)
+            {
+                if (gw < banks)
+                    bulk_load(stage0, inv + (size_t)gw * S, L::STAGE_BYTES, &bar[0]);
+                if (gw + total_warps < banks)
+                    bulk_load(stage1, inv + (size_t)(gw + total_warps) * S, L::STAGE_BYTES, &bar[1]);
+            }
+            double part[2] = {0.0, 0.0};
+            uint32_t phase0 = 0, phase1 = 0;
+            int k = 0;
+            bool ok = true;
+            for (int m = gw; m < banks; m += total_warps, ++k)
+            {
+                const bool s1 = (k & 1) != 0;
+                Real *stage = s1 ? stage1 : stage0;
+                uint64_t *b = s1 ? &bar[1] : &bar[0];
+                double r64[BD];
+#pragma unroll
+                for (int t = 0; t < BD; ++t)
+                {
+                    r64[t] = r[(size_t)m * N + t * 32 + lane];
+                    xs[t * 32 + lane] = (Real)r64[t];
+                }
+                __syncwarp();
+                if (!mbar_wait_bounded(b, s1 ? phase1 : phase0, errp))
+                {
+                    ok = false;
+                    break;
+                }
+                if (s1)
+                    phase1 ^= 1u;
+                else
+                    phase0 ^= 1u;
+                Real yr[BD];
+                symv_tiles<BD, Real>(stage, xs, lane, yr);
+                __syncwarp();
+                const int mn = m + 2 * total_warps;
+                if (lane == 0 && mn < banks)
+                {
+                    fence_proxy_async_smem();
+                    bulk_load(stage, inv + (size_t)mn * S, L::STAGE_BYTES, b);
+                }
+#pragma unroll
+                for (int t = 0; t < BD; ++t)
+                {
+                    const int row = t * 32 + lane;
+                    const long long node = (long long)m * 32 + row / BD;
+                    const int comp = row % BD;
+                    double zv = (double)yr[t];
+                    const int4 cs = mas.cslot[node];
+                    if (cs.x >= 0)
+                        zv += mas.zc[(size_t)cs.x * BD + comp];
+                    if (cs.y >= 0)
+                        zv += mas.zc[(size_t)cs.y * BD + comp];
+                    if (cs.z >= 0)
+                        zv += mas.zc[(size_t)cs.z * BD + comp];
+                    if (cs.w >= 0)
+                        zv += mas.zc[(size_t)cs.w * BD + comp];
+                    const size_t idx = (size_t)m * N + row;
+                    if (MODE == 2 && cfg.polak_ribiere)
+                        part[1] = fma(z[idx], r64[t], part[1]);
+                    z[idx] = zv;
+                    part[0] = fma(zv, r64[t], part[0]);
+                }
+                __syncwarp();
+            }
+            if (!ok)
+            {
+                // Drain this warp's other outstanding copy (bounded) before leaving.
+                if (lane == 0)
+                {
+                    for (long long i = 0; i < MBAR_SPIN_LIMIT; ++i)
+                        if (mbar_try_wait(&bar[0], phase0) && mbar_try_wait(&bar[1], phase1))
+                            break;
+                }
+                __syncwarp();
+            }
+            if (MODE == 0)
+                return;
+            double tot[2];
+            if (grid_reduce<2, THREADS>(part, red.partials, &st->counter[2], tot) && threadIdx.x == 0)
+                pcg_finalize(st, cfg, iter, MODE, tot[0], tot[1]);
+        }
+
+        // One CTA per coarse matrix: gather the coarse residual of its 32 components from the
+        // level-0 component sums, multiply with the inverse, write zc.
+        template <int BD, class Real>
+        __global__ void __launch_bounds__(128) k_coarse(MasView mas, const PcgState *st)
+        {
+            constexpr int N = 32 * BD, S = N * (N + 1) / 2;
+            if (st && st->done)
+                return;
+            extern __shared__ __align__(128) unsigned char smem[];
+            Real *mat = reinterpret_cast<Real *>(smem);
+            Real *xs = reinterpret_cast<Real *>(smem + ((size_t)S * sizeof(Real) + 15) / 16 * 16);
+            __shared__ double red[4][BD];
+            const int g = blockIdx.x;
+            const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+            const int level0 = (g < mas.mat_counts[1]); // first coarse level uses the sums directly
+            const long long node0 = (long long)g * 32;
+
+            // Start the matrix load (global -> shared, 16-byte vectors).
+            const Real *src = static_cast<const Real *>(mas.inv) + (size_t)(mas.banks + g) * S;
+            {
+                const int4 *s4 = reinterpret_cast<const int4 *>(src);
+                int4 *d4 = reinterpret_cast<int4 *>(mat);
+                const int n4 = S * (int)sizeof(Real) / 16;
+                for (int i = tid; i < n4; i += 128)
+                    d4[i] = s4[i];
+            }
+            if (level0)
+            {
+                for (int i = tid; i < N; i += 128)
+                    xs[i] = (Real)mas.rc[node0 * BD + i];
+            }
+            else
+            {
+                // Small components: one warp each; large ones: the whole CTA.
+                for (int i = w; i < 32; i += 4)
+                {
+                    const long long cn = node0 + i;
+                    const int b = mas.member_ptr[cn], e = mas.member_ptr[cn + 1];
+                    if (e - b > 256)
+                        continue;
+                    double s[BD];
+#pragma unroll
+                    for (int c = 0; c < BD; ++c)
+                        s[c] = 0.0;
+                    for (int q = b + lane; q < e; q += 32)
+                    {
+                        const int c0 = mas.members[q];
+#pragma unroll
+                        for (int c = 0; c < BD; ++c)
+                            s[c] += mas.rc[(size_t)c0 * BD + c];
+                    }
+#pragma unroll
+                    for (int c = 0; c < BD; ++c)
+                    {
+                        s[c] = warp_sum(s[c]);
+                        if (lane == 0)
+                        {
+                            xs[i * BD + c] = (Real)s[c];
+                            mas.rc[(size_t)cn * BD + c] = s[c];
+                        }
+                    }
+                }
+                for (int i = 0; i < 32; ++i)
+                {
+                    const long long cn = node0 + i;
+                    const int b = mas.member_ptr[cn], e = mas.member_ptr[cn + 1];
+                    if (e - b <= 256)
+                        continue;
+                    double s[BD];
+#pragma unroll
+                    for (int c = 0; c < BD; ++c)
+                        s[c] = 0.0;
+                    for (int q = b + tid; q < e; q += 128)
+                    {
+                        const int c0 = mas.members[q];
+#pragma unroll
+                        for (int c = 0; c < BD; ++c)
+                            s[c] += mas.rc[(size_t)c0 * BD + c];
+                    }
+#pragma unroll
+                    for (int c = 0; c < BD; ++c)
+                    {
+                        s[c] = warp_sum(s[c]);
+                        if (lane == 0)
+                            red[w][c] = s[c];
+                    }
+                    __syncthreads();
+                    if (tid == 0)
+                    {
+#pragma unroll
+                        for (int c = 0; c < BD; ++c)
+                        {
+                            const double t = (red[0][c] + red[1][c]) + (red[2][c] + red[3][c]);
+                            xs[i * BD + c] = (Real)t;
+                            mas.rc[(size_t)cn * BD + c] = t;
+                        }
+                    }
+                    __syncthreads();
+                }
+            }
+            __syncthreads();
+            if (w == 0)
+            {
+                Real yr[BD];
+                symv_tiles<BD, Real>(mat, xs, lane, yr);
+#pragma unroll
+                for (int t = 0; t < BD; ++t)
+                    mas.zc[node0 * BD + t * 32 + lane] = (double)yr[t];
+            }
+        }
+
+        // Level-0 restriction of a plain vector (used outside the PCG loop).
+        template <int BD>
+        __global__ void k_restrict(int banks, const double *__restrict__ r, const int *__restrict__ lcco0,
+                                   const int *__restrict__ cco0_base, double *rc)
+        {
+            const int lane = threadIdx.x & 31;
+            const int bank = blockIdx.x * 8 + (threadIdx.x >> 5);
+            if (bank >= banks)
+                return;
+            const long long u = (long long)bank * 32 + lane;
+            double rv[BD];
+#pragma unroll
+            for (int i = 0; i < BD; ++i)
+                rv[i] = r[u * BD + i];
+            warp_segment_store<BD>(rv, lcco0[u], cco0_base[bank], rc);
+        }
+
+        template <int BD, class Real>
+        void coarse_launch(const MasView &mas, PcgState *st, cudaStream_t s)
+        {
+            if (mas.total_coarse == 0)
+                return;
+            constexpr int N = 32 * BD, S = N * (N + 1) / 2;
+            const size_t smem = ((size_t)S * sizeof(Real) + 15) / 16 * 16 + N * sizeof(Real);
+            static bool configured = false;
+            if (!configured)
+            {
+                cuda_check(cudaFuncSetAttribute(k_coarse<BD, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)smem),
+                           "coarse smem attribute");
+                configured = true;
+            }
+            k_coarse<BD, Real><<<mas.total_coarse, 128, smem, s>>>(mas, st);
+            cuda_check(cudaGetLastError(), "coarse launch");
+        }
+
+        template <int BD, class Real, int MODE>
+        void symv0_launch_mode(const MasView &mas, const double *r, double *z, PcgState *st, ReduceBuf red,
+                               PcgConfig cfg, int iter, cudaStream_t s)
+        {
+            using L = Symv0Layout<BD, Real>;
+            static bool configured = false;
+            const size_t smem = (size_t)L::WARPS * L::WARP_BYTES;
+            if (!configured)
+            {
+                cuda_check(cudaFuncSetAttribute(k_symv0<BD, Real, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                (int)smem),
+                           "symv0 smem attribute");
+                configured = true;
+            }
+            int sms = 148;
+            int dev = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            int grid = (mas.banks + L::WARPS - 1) / L::WARPS;
+            if (grid > sms)
+                grid = sms;
+            if (grid < 1)
+                grid = 1;
+            if (MODE != 0 && grid > red.capacity)
+                throw Error(ERR_INVALID, "[MAS] reduction scratch too small");
+            k_symv0<BD, Real, MODE><<<grid, L::WARPS * 32, smem, s>>>(mas, r, z, st, red, cfg, iter);
+            cuda_check(cudaGetLastError(), "symv0 launch");
+        }
+
+        template <int BD, class Real>
+        void symv0_launch(const MasView &mas, const double *r, double *z, PcgState *st, ReduceBuf red, PcgConfig cfg,
+                          int iter, int mode, cudaStream_t s)
+        {
+            if (mode == 0)
+                symv0_launch_mode<BD, Real, 0>(mas, r, z, st, red, cfg, iter, s);
+            else if (mode == 1)
+                symv0_launch_mode<BD, Real, 1>(mas, r, z, st, red, cfg, iter, s);
+            else
+                symv0_launch_mode<BD, Real, 2>(mas, r, z, st, red, cfg, iter, s);
+        }
+    } // namespace
+
+    void launch_coarse(const MasView &mas, PcgState *st, cudaStream_t s)
+    {
+        if (mas.fp32)
+        {
+            if (mas.bd == 1)
+                coarse_launch<1, float>(mas, st, s);
+            else if (mas.bd == 2)
+                coarse_launch<2, float>(mas, st, s);
+            else
+                coarse_launch<3, float>(mas, st, s);
+        }
+        else
+        {
+            if (mas.bd == 1)
+                coarse_launch<1, double>(mas, st, s);
+            else if (mas.bd == 2)
+                coarse_launch<2, double>(mas, st, s);
+            else
+                coarse_launch<3, double>(mas, st, s);
+        }
+    }
+
+    void launch_symv0(const MasView &mas, const double *r, double *z, PcgState *st, ReduceBuf red, PcgConfig cfg,
+                      int iter, int mode, cudaStream_t s)
+    {
+        if (mas.fp32)
+        {
+            if (mas.bd == 1)
+                symv0_launch<1, float>(mas, r, z, st, red, cfg, iter, mode, s);
+            else if (mas.bd == 2)
+                symv0_launch<2, float>(mas, r, z, st, red, cfg, iter, mode, s);
+            else
+                symv0_launch<3, float>(mas, r, z, st, red, cfg, iter, mode, s);
+        }
+        else
+        {
+            if (mas.bd == 1)
+                symv0_launch<1, double>(mas, r, z, st, red, cfg, iter, mode, s);
+            else if (mas.bd == 2)
+                symv0_launch<2, double>(mas, r, z, st, red, cfg, iter, mode, s);
+            else
+                symv0_launch<3, double>(mas, r, z, st, red, cfg, iter, mode, s);
+        }
+    }
+
+    void launch_restrict_plain(const BankedView &A, const MasView &mas, const double *r, cudaStream_t s)
+    {
+        const int grid = (A.banks + 7) / 8;
+        if (grid == 0)
+            return;
+        if (A.bd == 1)
+            k_restrict<1><<<grid, 256, 0, s>>>(A.banks, r, mas.lcco0, mas.cco0_base, mas.rc);
+        else if (A.bd == 2)
+            k_restrict<2><<<grid, 256, 0, s>>>(A.banks, r, mas.lcco0, mas.cco0_base, mas.rc);
+        else
+            k_restrict<3><<<grid, 256, 0, s>>>(A.banks, r, mas.lcco0, mas.cco0_base, mas.rc);
+        cuda_check(cudaGetLastError(), "restrict launch");
+    }
+} // namespace pmas

@@ -1,0 +1,609 @@
+// MAS preconditioner factorization on the device (sm_100a).
+//
+// Restates MASPreconditioner::factorize (MASPreconditioner.cu:982-1097) on the padded numbering:
+//  1. level-0 coarse space: connected components of each bank (32 nodes) from bitmask closure of
+//     the in-bank neighbour masks (:128-213), numbered by lowest lane, offset by an exclusive scan
+//     over banks (:323-340);
+//  2. levels 1..3: masks of neighbouring components inside banks of 32 consecutive component ids
+//     (:222-275), components again (:281-318), global ids (:345-363); stop when nothing merges
+//     (:464-469);
+//  3. subdomain matrices: level 0 straight from each bank's rows (upper triangle, no atomics);
+//     coarse levels accumulate the upper triangle with the reference's rules (same bank, row <=
+//     col, diagonal block upper only, A_ij + A_ij^T when two nodes collapse, :494-591) with FP64
+//     atomics into a staging buffer;
+//  4. zero diagonals -> 1 (:779-796) and an in-place symmetric sweep inverse in FP64 (the
+//     Beaton / Goodnight sweep operator, as in batched_invert_upper :799-900), with a device error
+//     flag instead of an exception; the result is stored tile-packed in FP64 or FP32.
+
+#include <cub/cub.cuh>
+#include <vector>
+
+#include "mas_common.cuh"
+
+namespace pmas
+{
+    MasView MasDevice::view(double *rc_override) const
+    {
+        MasView v{};
+        v.bd = bd;
+        v.banks = banks;
+        v.level_num = level_num;
+        v.total_coarse = total_coarse;
+        for (int i = 0; i < LEVELS; ++i)
+        {
+            v.mat_offsets[i] = mat_offsets[i];
+            v.mat_counts[i] = mat_counts[i];
+            v.coarse_level_of[i] = 0;
+        }
+        for (int i = 0; i < MAX_COARSE; ++i)
+            v.cco_nums[i] = cco_nums[i];
+        v.fp32 = fp32;
+        v.inv = fp32 ? (const void *)inv32.get() : (const void *)inv64.get();
+        v.lcco0 = lcco0.get();
+        v.cco0_base = cco0_base.get();
+        v.cslot = cslot.get();
+        v.member_ptr = member_ptr.get();
+        v.members = members.get();
+        v.rc = rc_override ? rc_override : rc.get();
+        v.zc = zc.get();
+        return v;
+    }
+
+    namespace
+    {
+        __device__ __forceinline__ int ctz32(unsigned x) { return __ffs(x) - 1; }
+
+        // Bitmask closure inside a warp; masks in shared memory (32 per warp). Returns the local
+        // component id of this lane (-1 if invalid) and writes the component count to *count.
+        __device__ __forceinline__ int warp_components(unsigned mask, bool valid, unsigned *sm, int *count)
+        {
+            const int lane = threadIdx.x & 31;
+            sm[lane] = valid ? mask : 0u;
+            __syncwarp();
+            unsigned conn = valid ? mask : 0u;
+            if (valid)
+            {
+                unsigned visited = 1u << lane;
+                unsigned todo = conn & ~visited;
+                while (todo)
+                {
+                    const int v = ctz32(todo);
+                    conn |= sm[v];
+                    visited |= 1u << v;
+                    todo = conn & ~visited;
+                }
+            }
+            const int lead = valid ? ctz32(conn) : -1;
+            const unsigned leads = __ballot_sync(FULL, valid && lead == lane);
+            __syncwarp();
+            *count = __popc(leads);
+            if (!valid)
+                return -1;
+            return __popc(leads & ((1u << lead) - 1u));
+        }
+
+        __global__ void k_cco_lv0(BankedView A, const int *__restrict__ node_real, int *lcco0, int *cnt)
+        {
+            __shared__ unsigned sm[8][32];
+            const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+            const int bank = blockIdx.x * 8 + w;
+            if (bank >= A.banks)
+                return;
+            const int u = bank * 32 + lane;
+            const bool real = node_real[u] != 0;
+            unsigned m = 1u << lane;
+            if (real)
+            {
+                const long long s0 = A.slice[bank];
+                const int len = A.rowlen[u];
+                for (int k = 0; k < len; ++k)
+                {
+                    const int c = A.cols[(s0 + k) * 32 + lane];
+                    if ((c >> 5) == bank && node_real[c])
+                        m |= 1u << (c & 31);
+                }
+            }
+            int count;
+            const int id = warp_components(m, real, sm[w], &count);
+            lcco0[u] = id;
+            if (lane == 0)
+                cnt[bank] = count;
+        }
+
+        __global__ void k_map_lv0(int nodes, const int *__restrict__ lcco0, const int *__restrict__ base, int *map)
+        {
+            const int u = blockIdx.x * blockDim.x + threadIdx.x;
+            if (u >= nodes)
+                return;
+            const int l = lcco0[u];
+            map[(long long)u * 4 + 0] = l >= 0 ? base[u >> 5] + l : -1;
+            map[(long long)u * 4 + 1] = -1;
+            map[(long long)u * 4 + 2] = -1;
+            map[(long long)u * 4 + 3] = -1;
+        }
+
+        __global__ void k_masks_lvx(BankedView A, const int *__restrict__ node_real, const int *__restrict__ map,
+                                    int lv, unsigned *masks)
+        {
+            const int u = blockIdx.x * blockDim.x + threadIdx.x;
+            if (u >= A.banks * 32 || !node_real[u])
+                return;
+            const int c = map[(long long)u * 4 + lv - 1];
+            unsigned m = 1u << (c & 31);
+            const long long s0 = A.slice[u >> 5];
+            const int lane = u & 31;
+            const int len = A.rowlen[u];
+            for (int k = 0; k < len; ++k)
+            {
+                const int wn = A.cols[(s0 + k) * 32 + lane];
+                if (!node_real[wn])
+                    continue;
+                const int cw = map[(long long)wn * 4 + lv - 1];
+                if ((c >> 5) == (cw >> 5))
+                    m |= 1u << (cw & 31);
+            }
+            atomicOr(&masks[c], m);
+        }
+
+        __global__ void k_cco_lvx(int C, const unsigned *__restrict__ masks, int *lid, int *cnt)
+        {
+            __shared__ unsigned sm[8][32];
+            const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+            const int bank = blockIdx.x * 8 + w;
+            const int c = bank * 32 + lane;
+            if (bank * 32 >= C)
+                return;
+            const bool valid = c < C;
+            int count;
+            const int id = warp_components(valid ? masks[c] : 0u, valid, sm[w], &count);
+            if (valid)
+                lid[c] = id;
+            if (lane == 0)
+                cnt[bank] = count;
+        }
+
+        __global__ void k_map_lvx(int nodes, int lv, const int *__restrict__ lid, const int *__restrict__ base, int *map)
+        {
+            const int u = blockIdx.x * blockDim.x + threadIdx.x;
+            if (u >= nodes)
+                return;
+            const int prev = map[(long long)u * 4 + lv - 1];
+            map[(long long)u * 4 + lv] = prev >= 0 ? base[prev >> 5] + lid[prev] : -1;
+        }
+
+        // ----------------------------------------------------------------------------------
+        // Dense symmetric work matrix in shared memory (N x N, FP64), sweep inverse, store.
+        // ----------------------------------------------------------------------------------
+        template <int BD, class Out>
+        __device__ void invert_and_store(double *A, double *col, Out *out, int *flag)
+        {
+            constexpr int N = 32 * BD;
+            const int tid = threadIdx.x, nt = blockDim.x;
+            __shared__ int bad;
+            if (tid == 0)
+                bad = 0;
+            for (int i = tid; i < N; i += nt)
+                if (A[i * N + i] == 0.0)
+                    A[i * N + i] = 1.0;
+            __syncthreads();
+            for (int p = 0; p < N; ++p)
+            {
+                const double piv = A[p * N + p];
+                if (tid == 0 && (!isfinite(piv) || piv == 0.0))
+                    bad = 1;
+                for (int t = tid; t < N; t += nt)
+                    col[t] = (t == p) ? 0.0 : A[t * N + p];
+                __syncthreads();
+                for (int e = tid; e < N * N; e += nt)
+                {
+                    const int t = e / N, c = e - t * N;
+                    if (t > c || t == p || c == p)
+                        continue;
+                    const double scale = col[t] / piv;
+                    const double u = A[t * N + c] - scale * col[c];
+                    if (!isfinite(u))
+                        bad = 1;
+                    A[t * N + c] = u;
+                    A[c * N + t] = u;
+                }
+                __syncthreads();
+                for (int t = tid; t < N; t += nt)
+                {
+                    const double u = (t == p) ? -1.0 / piv : col[t] / piv;
+                    if (!isfinite(u))
+                        bad = 1;
+                    else
+                    {
+                        A[t * N + p] = u;
+                        A[p * N + t] = u;
+                    }
+                }
+                __syncthreads();
+            }
+            // Store -A (the inverse) tile-packed.
+            constexpr int S = N * (N + 1) / 2;
+            for (int idx = tid; idx < S; idx += nt)
+            {
+                // Decode the tile-packed index.
+                int rem = idx, J = 0;
+                while (rem >= J * 1024 + 528)
+                {
+                    rem -= J * 1024 + 528;
+                    ++J;
+                }
+                int row, cl;
+                if (rem < J * 1024)
+                {
+                    const int I = rem >> 10, e = rem & 1023;
+                    const int j4 = e >> 7, l = (e & 127) >> 2, jj = e & 3;
+                    row = 32 * I + l;
+                    cl = 32 * J + 4 * j4 + jj;
+                }
+                else
+                {
+                    const int e = rem - J * 1024;
+                    int j = (int)((sqrt(8.0 * e + 1.0) - 1.0) * 0.5);
+                    while (j * (j + 1) / 2 > e)
+                        --j;
+                    while ((j + 1) * (j + 2) / 2 <= e)
+                        ++j;
+                    row = 32 * J + (e - j * (j + 1) / 2);
+                    cl = 32 * J + j;
+                }
+                const double v = -A[row * N + cl];
+                if (!isfinite(v))
+                    bad = 1;
+                out[idx] = (Out)v;
+            }
+            __syncthreads();
+            if (tid == 0 && bad)
+                atomicExch(flag, ERR_INVERSE);
+        }
+
+        template <int BD, class Out>
+        __global__ void __launch_bounds__(256) k_assemble_invert_lv0(BankedView A, const int *__restrict__ node_real,
+                                                                     Out *out, int *flag)
+        {
+            constexpr int N = 32 * BD, S = N * (N + 1) / 2;
+            extern __shared__ __align__(16) double dsm[];
+            double *M = dsm;
+            double *col = dsm + N * N;
+            const int bank = blockIdx.x;
+            for (int i = threadIdx.x; i < N * N; i += blockDim.x)
+                M[i] = 0.0;
+            __syncthreads();
+            // 8 threads per node, each walking a subset of the node's slots.
+            const int lane = threadIdx.x >> 3, sub = threadIdx.x & 7;
+            const int u = bank * 32 + lane;
+            if (node_real[u])
+            {
+                const long long s0 = A.slice[bank];
+                const int len = A.rowlen[u];
+                for (int k = sub; k < len; k += 8)
+                {
+                    const long long slot = s0 + k;
+                    const int w = A.cols[slot * 32 + lane];
+                    if ((w >> 5) != bank || !node_real[w])
+                        continue;
+                    const int lw = w & 31;
+                    if (lw < lane)
+                        continue; // upper triangle in node order (reference skips tid > j)
+#pragma unroll
+                    for (int bi = 0; bi < BD; ++bi)
+#pragma unroll
+                        for (int bj = 0; bj < BD; ++bj)
+                        {
+                            if (lw == lane && bi > bj)
+                                continue;
+                            const double v = A.vals[banked_value_index(slot, lane, bi * BD + bj, BD)];
+                            const int row = lane * BD + bi, cl = lw * BD + bj;
+                            M[row * N + cl] = v;
+                            M[cl * N + row] = v;
+                        }
+                }
+            }
+            __syncthreads();
+            invert_and_store<BD, Out>(M, col, out + (size_t)bank * S, flag);
+        }
+
+        // Coarse-level upper-triangle accumulation with FP64 atomics (order-dependent in the
+        // last bits, as in the reference).
+        template <int BD>
+        __global__ void k_assemble_coarse(BankedView A, const int *__restrict__ node_real, const int *__restrict__ map,
+                                          int level_num, int coff0, int coff1, int coff2, int coff3, double *staging)
+        {
+            constexpr int N = 32 * BD;
+            const int u = blockIdx.x * blockDim.x + threadIdx.x;
+            if (u >= A.banks * 32 || !node_real[u])
+                return;
+            const int coff[4] = {coff0, coff1, coff2, coff3};
+            const long long s0 = A.slice[u >> 5];
+            const int lane = u & 31;
+            const int len = A.rowlen[u];
+            for (int k = 0; k < len; ++k)
+            {
+                const long long slot = s0 + k;
+                const int w = A.cols[slot * 32 + lane];
+                if (w < u || !node_real[w])
+                    continue;
+                for (int lv = 0; lv < level_num; ++lv)
+                {
+                    const int ci = map[(long long)u * 4 + lv], cj = map[(long long)w * 4 + lv];
+                    if ((ci >> 5) != (cj >> 5))
+                        continue;
+                    const long long g = (coff[lv] + ci) >> 5;
+                    double *mat = staging + (size_t)g * N * N;
+                    const bool collapsed = (u != w) && (ci == cj);
+#pragma unroll
+                    for (int bi = 0; bi < BD; ++bi)
+#pragma unroll
+                        for (int bj = 0; bj < BD; ++bj)
+                        {
+                            const int row = (ci & 31) * BD + bi, cl = (cj & 31) * BD + bj;
+                            if (row > cl)
+                                continue;
+                            if (u == w && bi > bj)
+                                continue;
+                            double v = A.vals[banked_value_index(slot, lane, bi * BD + bj, BD)];
+                            if (collapsed)
+                                v += A.vals[banked_value_index(slot, lane, bj * BD + bi, BD)];
+                            atomicAdd(mat + row * N + cl, v);
+                        }
+                }
+            }
+        }
+
+        template <int BD, class Out>
+        __global__ void __launch_bounds__(256) k_invert_coarse(const double *__restrict__ staging, Out *out, int *flag)
+        {
+            constexpr int N = 32 * BD, S = N * (N + 1) / 2;
+            extern __shared__ __align__(16) double dsm[];
+            double *M = dsm;
+            double *col = dsm + N * N;
+            const double *src = staging + (size_t)blockIdx.x * N * N;
+            for (int e = threadIdx.x; e < N * N; e += blockDim.x)
+            {
+                const int r = e / N, c = e - r * N;
+                M[e] = (r <= c) ? src[r * N + c] : src[c * N + r];
+            }
+            __syncthreads();
+            invert_and_store<BD, Out>(M, col, out + (size_t)blockIdx.x * S, flag);
+        }
+
+        __global__ void k_cslot(int nodes, int level_num, const int *__restrict__ map, int coff0, int coff1, int coff2,
+                                int coff3, int4 *cslot)
+        {
+            const int u = blockIdx.x * blockDim.x + threadIdx.x;
+            if (u >= nodes)
+                return;
+            const int coff[4] = {coff0, coff1, coff2, coff3};
+            int v[4];
+#pragma unroll
+            for (int l = 0; l < 4; ++l)
+            {
+                const int c = map[(long long)u * 4 + l];
+                v[l] = (l < level_num && c >= 0) ? coff[l] + c : -1;
+            }
+            cslot[u] = make_int4(v[0], v[1], v[2], v[3]);
+        }
+
+        int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+        template <class T>
+        void exclusive_scan(const T *in, T *out, int n, cudaStream_t s)
+        {
+            size_t bytes = 0;
+            cuda_check(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, s), "scan size");
+            DevBuf<unsigned char> tmp;
+            tmp.alloc(bytes, "MAS coarse_space scan");
+            cuda_check(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, in, out, n, s), "scan");
+            cuda_check(cudaStreamSynchronize(s), "scan sync");
+        }
+
+        template <int BD, class Out>
+        void assemble_and_invert(MasDevice &M, const BankedMatrix &A, const int *d_node_real, Out *out, const int *coff,
+                                 cudaStream_t s)
+        {
+            constexpr int N = 32 * BD;
+            const size_t smem = (size_t)(N * N + N) * sizeof(double);
+            cuda_check(cudaFuncSetAttribute(k_assemble_invert_lv0<BD, Out>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem),
+                       "assemble smem attribute");
+            cuda_check(cudaFuncSetAttribute(k_invert_coarse<BD, Out>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem),
+                       "invert smem attribute");
+            if (M.banks > 0)
+            {
+                k_assemble_invert_lv0<BD, Out><<<M.banks, 256, smem, s>>>(A.view(), d_node_real, out, M.flag.get());
+                cuda_check(cudaGetLastError(), "assemble lv0 launch");
+            }
+            if (M.total_coarse > 0)
+            {
+                DevBuf<double> staging;
+                staging.alloc((size_t)M.total_coarse * N * N, "MAS coarse_matrices staging");
+                cuda_check(cudaMemsetAsync(staging.get(), 0, staging.bytes(), s), "memset");
+                k_assemble_coarse<BD><<<div_up(M.nodes, 256), 256, 0, s>>>(A.view(), d_node_real, M.map.get(),
+                                                                          M.level_num, coff[0], coff[1], coff[2],
+                                                                          coff[3], staging.get());
+                cuda_check(cudaGetLastError(), "assemble coarse launch");
+                constexpr int S = N * (N + 1) / 2;
+                k_invert_coarse<BD, Out><<<M.total_coarse, 256, smem, s>>>(staging.get(), out + (size_t)M.banks * S,
+                                                                          M.flag.get());
+                cuda_check(cudaGetLastError(), "invert coarse launch");
+                cuda_check(cudaStreamSynchronize(s), "coarse inverse");
+            }
+        }
+    } // namespace
+
+    void build_mas(MasDevice &M, const BankedMatrix &A, const int *d_node_real, int fp32, cudaStream_t s)
+    {
+        const int bd = A.bd, banks = A.banks, nodes = A.nodes;
+        M.bd = bd;
+        M.banks = banks;
+        M.nodes = nodes;
+        M.fp32 = fp32;
+        M.flag.alloc(1, "MAS flag");
+        cuda_check(cudaMemsetAsync(M.flag.get(), 0, sizeof(int), s), "memset");
+
+        // --- level 0 components
+        M.lcco0.alloc(nodes, "MAS coarse_space lcco0");
+        M.cco0_base.alloc(banks + 1, "MAS coarse_space base");
+        M.map.alloc((size_t)nodes * 4, "MAS coarse_space map");
+        DevBuf<int> cnt;
+        cnt.alloc(banks + 1, "MAS coarse_space counts");
+        cuda_check(cudaMemsetAsync(cnt.get(), 0, sizeof(int) * (banks + 1), s), "memset");
+        k_cco_lv0<<<div_up(banks, 8), 256, 0, s>>>(A.view(), d_node_real, M.lcco0.get(), cnt.get());
+        cuda_check(cudaGetLastError(), "cco lv0 launch");
+        exclusive_scan(cnt.get(), M.cco0_base.get(), banks + 1, s);
+        int C = 0;
+        cuda_check(cudaMemcpy(&C, M.cco0_base.get() + banks, sizeof(int), cudaMemcpyDeviceToHost), "count");
+        k_map_lv0<<<div_up(nodes, 256), 256, 0, s>>>(nodes, M.lcco0.get(), M.cco0_base.get(), M.map.get());
+        cuda_check(cudaGetLastError(), "map lv0 launch");
+        for (int i = 0; i < MAX_COARSE; ++i)
+            M.cco_nums[i] = 0;
+        M.cco_nums[0] = C;
+        M.level_num = 1;
+
+        // --- levels 1..3
+        DevBuf<unsigned> masks;
+        DevBuf<int> lid, lbase, lcnt;
+        masks.alloc(C > 0 ? C : 1, "MAS coarse_space masks");
+        lid.alloc(C > 0 ? C : 1, "MAS coarse_space lid");
+        for (int lv = 1; lv < MAX_COARSE && C > 0; ++lv)
+        {
+            const int cb = div_up(C, 32);
+            lcnt.alloc(cb + 1, "MAS coarse_space counts");
+            lbase.alloc(cb + 1, "MAS coarse_space base");
+            cuda_check(cudaMemsetAsync(masks.get(), 0, sizeof(unsigned) * C, s), "memset");
+            cuda_check(cudaMemsetAsync(lcnt.get(), 0, sizeof(int) * (cb + 1), s), "memset");
+            k_masks_lvx<<<div_up(nodes, 256), 256, 0, s>>>(A.view(), d_node_real, M.map.get(), lv, masks.get());
+            cuda_check(cudaGetLastError(), "masks launch");
+            k_cco_lvx<<<div_up(cb, 8), 256, 0, s>>>(C, masks.get(), lid.get(), lcnt.get());
+            cuda_check(cudaGetLastError(), "cco lvx launch");
+            exclusive_scan(lcnt.get(), lbase.get(), cb + 1, s);
+            int next = 0;
+            cuda_check(cudaMemcpy(&next, lbase.get() + cb, sizeof(int), cudaMemcpyDeviceToHost), "count");
+            k_map_lvx<<<div_up(nodes, 256), 256, 0, s>>>(nodes, lv, lid.get(), lbase.get(), M.map.get());
+            cuda_check(cudaGetLastError(), "map lvx launch");
+            if (next == C)
+                break;
+            C = next;
+            M.cco_nums[lv] = C;
+            M.level_num = lv + 1;
+        }
+        // Unused levels back to -1 (the early-stop level was written but is not used).
+        if (M.level_num < MAX_COARSE)
+        {
+            std::vector<int> hmap((size_t)nodes * 4);
+            cuda_check(cudaMemcpy(hmap.data(), M.map.get(), hmap.size() * sizeof(int), cudaMemcpyDeviceToHost), "map");
+            for (int u = 0; u < nodes; ++u)
+                for (int l = M.level_num; l < MAX_COARSE; ++l)
+                    hmap[(size_t)u * 4 + l] = -1;
+            cuda_check(cudaMemcpy(M.map.get(), hmap.data(), hmap.size() * sizeof(int), cudaMemcpyHostToDevice), "map");
+        }
+
+        // --- matrix counts and coarse vector layout
+        for (int i = 0; i < LEVELS; ++i)
+            M.mat_counts[i] = M.mat_offsets[i] = 0;
+        M.mat_counts[0] = banks;
+        M.total_mats = banks;
+        int coff[4] = {0, 0, 0, 0};
+        int cn = 0;
+        for (int l = 0; l < M.level_num; ++l)
+        {
+            M.mat_offsets[l + 1] = M.total_mats;
+            M.mat_counts[l + 1] = div_up(M.cco_nums[l], 32);
+            M.total_mats += M.mat_counts[l + 1];
+            coff[l] = cn;
+            cn += M.mat_counts[l + 1] * 32;
+        }
+        M.total_coarse = M.total_mats - banks;
+        M.coarse_nodes = cn;
+
+        M.cslot.alloc(nodes, "MAS coarse_space slots");
+        k_cslot<<<div_up(nodes, 256), 256, 0, s>>>(nodes, M.level_num, M.map.get(), coff[0], coff[1], coff[2], coff[3],
+                                                  M.cslot.get());
+        cuda_check(cudaGetLastError(), "cslot launch");
+
+        // Member lists (level-0 components of each coarse node of levels >= 1), built on the host.
+        {
+            std::vector<int> hmap((size_t)nodes * 4);
+            cuda_check(cudaMemcpy(hmap.data(), M.map.get(), hmap.size() * sizeof(int), cudaMemcpyDeviceToHost), "map");
+            const int C0 = M.cco_nums[0];
+            std::vector<int> up((size_t)C0 * 4, -1);
+            for (int u = 0; u < nodes; ++u)
+            {
+                const int c0 = hmap[(size_t)u * 4];
+                if (c0 < 0)
+                    continue;
+                for (int l = 1; l < M.level_num; ++l)
+                    up[(size_t)c0 * 4 + l] = hmap[(size_t)u * 4 + l];
+            }
+            std::vector<int> ptr((size_t)cn + 1, 0);
+            for (int c0 = 0; c0 < C0; ++c0)
+                for (int l = 1; l < M.level_num; ++l)
+                    ptr[(size_t)coff[l] + up[(size_t)c0 * 4 + l] + 1]++;
+            for (int i = 0; i < cn; ++i)
+                ptr[i + 1] += ptr[i];
+            std::vector<int> fillp(ptr.begin(), ptr.end() - 1);
+            std::vector<int> mem(ptr[cn] > 0 ? ptr[cn] : 1);
+            for (int c0 = 0; c0 < C0; ++c0)
+                for (int l = 1; l < M.level_num; ++l)
+                {
+                    const int node = coff[l] + up[(size_t)c0 * 4 + l];
+                    mem[fillp[node]++] = c0;
+                }
+            M.member_ptr.alloc(cn + 1, "MAS coarse_space members");
+            M.members.alloc(mem.size(), "MAS coarse_space members");
+            cuda_check(cudaMemcpy(M.member_ptr.get(), ptr.data(), ptr.size() * sizeof(int), cudaMemcpyHostToDevice),
+                       "members");
+            cuda_check(cudaMemcpy(M.members.get(), mem.data(), mem.size() * sizeof(int), cudaMemcpyHostToDevice),
+                       "members");
+        }
+
+        // Coarse vectors (zero once: slots past the component counts stay zero).
+        M.rc.alloc((size_t)(cn > 0 ? cn : 1) * bd, "MAS coarse_vectors r");
+        M.zc.alloc((size_t)(cn > 0 ? cn : 1) * bd, "MAS coarse_vectors z");
+        cuda_check(cudaMemsetAsync(M.rc.get(), 0, M.rc.bytes(), s), "memset");
+        cuda_check(cudaMemsetAsync(M.zc.get(), 0, M.zc.bytes(), s), "memset");
+
+        // --- matrices
+        const size_t S = (size_t)tile_packed_size(bd);
+        if (fp32)
+        {
+            M.inv64.reset();
+            M.inv32.alloc(S * M.total_mats, "MAS coarse_matrices");
+        }
+        else
+        {
+            M.inv32.reset();
+            M.inv64.alloc(S * M.total_mats, "MAS coarse_matrices");
+        }
+        switch (bd)
+        {
+        case 1:
+            if (fp32)
+                assemble_and_invert<1, float>(M, A, d_node_real, M.inv32.get(), coff, s);
+            else
+                assemble_and_invert<1, double>(M, A, d_node_real, M.inv64.get(), coff, s);
+            break;
+        case 2:
+            if (fp32)
+                assemble_and_invert<2, float>(M, A, d_node_real, M.inv32.get(), coff, s);
+            else
+                assemble_and_invert<2, double>(M, A, d_node_real, M.inv64.get(), coff, s);
+            break;
+        default:
+            if (fp32)
+                assemble_and_invert<3, float>(M, A, d_node_real, M.inv32.get(), coff, s);
+            else
+                assemble_and_invert<3, double>(M, A, d_node_real, M.inv64.get(), coff, s);
+            break;
+        }
+        int h_flag = 0;
+        cuda_check(cudaMemcpyAsync(&h_flag, M.flag.get(), sizeof(int), cudaMemcpyDeviceToHost, s), "flag");
+        cuda_check(cudaStreamSynchronize(s), "mas build");
+        if (h_flag)
+            throw Error(ERR_INVERSE, "[MAS] MAS packed inverse failed.");
+    }
+} // namespace pmas

@@ -1,0 +1,965 @@
+// Host side of the B200 MAS-PCG solver behind the C ABI (include/polysolve_mas.h).
+//
+// MasSolver mirrors MASSolver::MASSolverImpl (src/polysolve/linear/MASSolver.cu:134-595):
+// parameters and info, ordering + permutation, the permuted block matrix, the MAS
+// preconditioner and the PCG loop. Differences by design:
+//   * the ordering is Morton (positions given) or graph bisection instead of KaMinPar;
+//   * all scalars live on the device; the iteration is launched in chunks and the host only
+//     looks at the device state between chunks (one chunk ahead), instead of a blocking read
+//     every 10 iterations (MASSolver.cu:533-560);
+//   * extension parameters (precision, true_residual_period, check_period, initial_guess, beta,
+//     ordering) default to the reference's behaviour.
+
+#include "polysolve_mas.h"
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "mas_internal.h"
+#include "mas_json.h"
+#include "mas_ordering.h"
+
+using namespace pmas;
+
+namespace
+{
+    struct Params
+    {
+        // Reference keys (MASSolver.cu:137-143, impl defaults).
+        int block_dim = 1;
+        int max_iter = 5000;
+        double rel_tol = 1e-5;
+        double abs_tol = 1e-8;
+        bool lazy = false;
+        bool use_prec_norm = false;
+        // Extensions; defaults reproduce the reference's algorithm.
+        bool fp32 = false;
+        int true_residual_period = 4;
+        int check_period = 10;
+        bool initial_guess_input = false;
+        bool polak_ribiere = false;
+        std::string ordering = "auto";
+        int poll_period = 8;
+        bool profile = false; // time every kernel launch with CUDA events
+    };
+
+    const char *status_string(int s)
+    {
+        switch (s)
+        {
+        case MAS_STATUS_RUNNING:
+            return "Running";
+        case MAS_STATUS_REACH_RELATIVE_TOLERANCE:
+            return "Reach relative tolerance";
+        case MAS_STATUS_REACH_ABSOLUTE_TOLERANCE:
+            return "Reach absolute tolerance";
+        case MAS_STATUS_REACH_MAX_ITERATIONS:
+            return "Reach max iterations";
+        default:
+            return "Unknown";
+        }
+    }
+
+    int get_int(const Json &v, const char *key)
+    {
+        if (v.type != Json::Number || !v.is_integer)
+            throw Error(ERR_INVALID, std::string("[MAS] parameter ") + key + " must be an integer");
+        return (int)v.num;
+    }
+    double get_num(const Json &v, const char *key)
+    {
+        if (v.type != Json::Number)
+            throw Error(ERR_INVALID, std::string("[MAS] parameter ") + key + " must be a number");
+        return v.num;
+    }
+    bool get_bool(const Json &v, const char *key)
+    {
+        if (v.type != Json::Bool)
+            throw Error(ERR_INVALID, std::string("[MAS] parameter ") + key + " must be a boolean");
+        return v.b;
+    }
+    std::string get_str(const Json &v, const char *key)
+    {
+        if (v.type != Json::String)
+            throw Error(ERR_INVALID, std::string("[MAS] parameter ") + key + " must be a string");
+        return v.str;
+    }
+
+    const char *KNOWN_KEYS[] = {"block_dim", "max_iter", "relative_tolerance", "absolute_tolerance",
+                                "lazy_partitioning", "use_preconditioned_residual_norm", "precision",
+                                "true_residual_period", "check_period", "initial_guess", "beta", "ordering",
+                                "poll_period", "profile_kernels"};
+
+    // MASSolverImpl::set_parameters (MASSolver.cu:198-212) plus the extension keys.
+    void apply_mas_params(Params &p, const Json &m, bool strict)
+    {
+        if (m.type != Json::Object)
+            throw Error(ERR_INVALID, "[MAS] \"MAS\" parameters must be an object");
+        if (strict)
+            for (const auto &kv : m.obj)
+            {
+                bool ok = false;
+                for (const char *k : KNOWN_KEYS)
+                    ok = ok || kv.first == k;
+                if (!ok)
+                    throw Error(ERR_INVALID, "[MAS] invalid input json: unknown key /MAS/" + kv.first);
+            }
+        Params q = p;
+        if (auto *v = m.find("block_dim"))
+        {
+            q.block_dim = get_int(*v, "block_dim");
+            if (q.block_dim < 1 || q.block_dim > 3)
+                throw Error(ERR_INVALID, "[MAS] block_dim must be 1, 2 or 3");
+        }
+        if (auto *v = m.find("max_iter"))
+            q.max_iter = get_int(*v, "max_iter");
+        if (auto *v = m.find("relative_tolerance"))
+            q.rel_tol = get_num(*v, "relative_tolerance");
+        if (auto *v = m.find("absolute_tolerance"))
+            q.abs_tol = get_num(*v, "absolute_tolerance");
+        if (auto *v = m.find("lazy_partitioning"))
+            q.lazy = get_bool(*v, "lazy_partitioning");
+        if (auto *v = m.find("use_preconditioned_residual_norm"))
+            q.use_prec_norm = get_bool(*v, "use_preconditioned_residual_norm");
+        if (auto *v = m.find("precision"))
+        {
+            const std::string s = get_str(*v, "precision");
+            if (s != "fp64" && s != "fp32")
+                throw Error(ERR_INVALID, "[MAS] precision must be \"fp64\" or \"fp32\"");
+            q.fp32 = (s == "fp32");
+        }
+        if (auto *v = m.find("true_residual_period"))
+        {
+            q.true_residual_period = get_int(*v, "true_residual_period");
+            if (q.true_residual_period < 1)
+                throw Error(ERR_INVALID, "[MAS] true_residual_period must be >= 1");
+        }
+        if (auto *v = m.find("check_period"))
+        {
+            q.check_period = get_int(*v, "check_period");
+            if (q.check_period < 1)
+                throw Error(ERR_INVALID, "[MAS] check_period must be >= 1");
+        }
+        if (auto *v = m.find("initial_guess"))
+        {
+            const std::string s = get_str(*v, "initial_guess");
+            if (s != "zero" && s != "input")
+                throw Error(ERR_INVALID, "[MAS] initial_guess must be \"zero\" or \"input\"");
+            q.initial_guess_input = (s == "input");
+        }
+        if (auto *v = m.find("beta"))
+        {
+            const std::string s = get_str(*v, "beta");
+            if (s != "fletcher_reeves" && s != "polak_ribiere")
+                throw Error(ERR_INVALID, "[MAS] beta must be \"fletcher_reeves\" or \"polak_ribiere\"");
+            q.polak_ribiere = (s == "polak_ribiere");
+        }
+        if (auto *v = m.find("ordering"))
+        {
+            const std::string s = get_str(*v, "ordering");
+            if (s != "auto" && s != "morton" && s != "graph" && s != "natural")
+                throw Error(ERR_INVALID, "[MAS] ordering must be \"auto\", \"morton\", \"graph\" or \"natural\"");
+            q.ordering = s;
+        }
+        if (auto *v = m.find("profile_kernels"))
+            q.profile = get_bool(*v, "profile_kernels");
+        if (auto *v = m.find("poll_period"))
+        {
+            q.poll_period = get_int(*v, "poll_period");
+            if (q.poll_period < 1)
+                throw Error(ERR_INVALID, "[MAS] poll_period must be >= 1");
+        }
+        p = q;
+    }
+
+    std::string g_create_error;
+} // namespace
+
+struct mas_solver
+{
+    Params p;
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr; // own_stream or the caller's (mas_set_stream)
+    std::string last_error;
+
+    // Kernel accounting: launches per kind, and CUDA-event time per kind when profiling.
+    struct KStat
+    {
+        long long launches = 0;
+        double ms = 0.0;
+    };
+    std::vector<std::pair<std::string, KStat>> kstats;
+    long long total_launches = 0;
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
+    size_t ev_used = 0;
+
+    // Info of the last solve (MASSolver.cu:145-149).
+    int iterations = 0;
+    double residual_norm = 0.0;
+    int status = MAS_STATUS_RUNNING;
+    double rr0 = 0.0, rz0 = 0.0;
+    double solve_ms = 0.0, factorize_ms = 0.0;
+    int launched_iterations = 0;
+
+    std::vector<double> positions;
+
+    // Ordering / pattern state.
+    int n = 0, V = 0, banks = 0, bd = 0;
+    long long nnz = 0;
+    uint64_t pattern = 0;
+    std::string ordering_used;
+    std::vector<int> padded;
+    DevBuf<int> d_padded, d_node_real;
+    BankedMatrix A;
+    MasDevice mas;
+    bool factorized = false;
+
+    DevBuf<double> x, b, r, pv, z, Ap, io;
+    DevBuf<PcgState> st;
+    DevBuf<double> partials;
+    int red_capacity = 0;
+    PcgState *h_st = nullptr; // pinned, 2 slots
+
+    ~mas_solver()
+    {
+        if (stream)
+        {
+            cudaSetDevice(device);
+            cudaStreamSynchronize(stream);
+        }
+        for (cudaEvent_t e : ev_pool)
+            cudaEventDestroy(e);
+        if (h_st)
+            cudaFreeHost(h_st);
+        if (own_stream)
+            cudaStreamDestroy(own_stream);
+    }
+
+    int stat_index(const char *kind)
+    {
+        for (size_t i = 0; i < kstats.size(); ++i)
+            if (kstats[i].first == kind)
+                return (int)i;
+        kstats.emplace_back(kind, KStat{});
+        return (int)kstats.size() - 1;
+    }
+
+    cudaEvent_t pool_event()
+    {
+        if (ev_used == ev_pool.size())
+        {
+            cudaEvent_t e;
+            cuda_check(cudaEventCreate(&e), "event");
+            ev_pool.push_back(e);
+        }
+        return ev_pool[ev_used++];
+    }
+
+    // Launch through here: counts kernels (`kernels` per call) and, when profiling, brackets the
+    // launch with events on the launching stream.
+    template <class F>
+    void run(const char *kind, int kernels, F &&f)
+    {
+        const int idx = stat_index(kind);
+        kstats[idx].second.launches += kernels;
+        total_launches += kernels;
+        if (p.profile)
+        {
+            cudaEvent_t a = pool_event(), b = pool_event();
+            cuda_check(cudaEventRecord(a, stream), "event");
+            f();
+            cuda_check(cudaEventRecord(b, stream), "event");
+            ev_pending.push_back({idx, {a, b}});
+        }
+        else
+            f();
+    }
+
+    void collect_profile()
+    {
+        for (auto &e : ev_pending)
+        {
+            float ms = 0.f;
+            cuda_check(cudaEventElapsedTime(&ms, e.second.first, e.second.second), "event time");
+            kstats[e.first].second.ms += ms;
+        }
+        ev_pending.clear();
+        ev_used = 0;
+    }
+
+    void init_device()
+    {
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0)
+        {
+            cudaGetLastError();
+            throw Error(ERR_NO_DEVICE, "No Nvidia GPU!!");
+        }
+        cuda_check(cudaGetDevice(&device), "get device");
+        cuda_check(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking), "stream create");
+        stream = own_stream;
+        cuda_check(cudaMallocHost(&h_st, 2 * sizeof(PcgState)), "pinned state");
+    }
+
+    // MASSolverImpl::factorize (MASSolver.cu:292-374).
+    void factorize(int n_, const int *outer, const int *inner, const double *vals, long long nnz_)
+    {
+        auto t0 = std::chrono::steady_clock::now();
+        cuda_check(cudaSetDevice(device), "set device");
+        if (n_ <= 0 || !outer || !inner || !vals)
+            throw Error(ERR_INVALID, "[MAS] factorize: invalid matrix arguments.");
+        if (outer[0] != 0 || (long long)outer[n_] != nnz_ || nnz_ < 0)
+            throw Error(ERR_INVALID, "[MAS] factorize: outer index array is inconsistent with nnz.");
+        if (nnz_ > 2147483647LL)
+            throw Error(ERR_INVALID, "[MAS] A is too large. Non-zero number exceeding int32 max.");
+        const int bd_ = p.block_dim;
+        const int V_ = (n_ + bd_ - 1) / bd_;
+        const bool rebuild_order = !p.lazy || padded.size() != (size_t)V_ || bd_ != bd || n_ != n;
+        const uint64_t h = pattern_hash(n_, outer, inner, nnz_);
+        const bool same_pattern = factorized && !rebuild_order && h == pattern && nnz_ == nnz && bd_ == A.bd;
+
+        if (rebuild_order)
+        {
+            std::vector<uint8_t> iso = isolated_blocks(n_, outer, inner, bd_);
+            std::string mode = p.ordering;
+            if (mode == "auto")
+                mode = (positions.size() == (size_t)V_ * 3) ? "morton" : "graph";
+            int nb = 0;
+            if (mode == "morton")
+            {
+                if (positions.size() != (size_t)V_ * 3)
+                    throw Error(ERR_INVALID, "[MAS] ordering \"morton\" needs positions for every block row.");
+                padded = morton_padded(positions.data(), V_, iso, &nb);
+            }
+            else if (mode == "graph")
+                padded = graph_padded(n_, outer, inner, bd_, iso, &nb);
+            else
+                padded = natural_padded(V_, &nb);
+            ordering_used = mode;
+            banks = nb;
+            V = V_;
+            n = n_;
+            bd = bd_;
+            d_padded.alloc(V_, "MAS ordering");
+            cuda_check(cudaMemcpyAsync(d_padded.get(), padded.data(), sizeof(int) * V_, cudaMemcpyHostToDevice, stream),
+                       "upload ordering");
+            std::vector<int> real(banks * 32, 0);
+            for (int v = 0; v < V_; ++v)
+                real[padded[v]] = 1;
+            d_node_real.alloc(real.size(), "MAS ordering");
+            cuda_check(cudaMemcpyAsync(d_node_real.get(), real.data(), sizeof(int) * real.size(),
+                                       cudaMemcpyHostToDevice, stream),
+                       "upload ordering");
+            cuda_check(cudaStreamSynchronize(stream), "ordering");
+        }
+        factorized = false;
+        {
+            DevBuf<double> d_vals;
+            d_vals.alloc(nnz_ > 0 ? nnz_ : 1, "MAS permuted_bsr input_csc");
+            cuda_check(cudaMemcpyAsync(d_vals.get(), vals, sizeof(double) * nnz_, cudaMemcpyHostToDevice, stream),
+                       "upload values");
+            if (same_pattern)
+            {
+                rescatter_values(A, nnz_, d_vals.get(), stream);
+            }
+            else
+            {
+                DevBuf<int> d_outer, d_inner;
+                d_outer.alloc(n_ + 1, "MAS permuted_bsr input_csc");
+                d_inner.alloc(nnz_ > 0 ? nnz_ : 1, "MAS permuted_bsr input_csc");
+                cuda_check(cudaMemcpyAsync(d_outer.get(), outer, sizeof(int) * (n_ + 1), cudaMemcpyHostToDevice, stream),
+                           "upload outer");
+                cuda_check(cudaMemcpyAsync(d_inner.get(), inner, sizeof(int) * nnz_, cudaMemcpyHostToDevice, stream),
+                           "upload inner");
+                A.slice.reset();
+                A.cols.reset();
+                A.vals.reset();
+                A.scatter.reset();
+                build_banked(A, n_, nnz_, d_outer.get(), d_inner.get(), d_vals.get(), bd_, V_, banks, d_padded.get(),
+                             stream);
+            }
+            cuda_check(cudaStreamSynchronize(stream), "matrix upload");
+        }
+        nnz = nnz_;
+        pattern = h;
+
+        build_mas(mas, A, d_node_real.get(), p.fp32 ? 1 : 0, stream);
+
+        const size_t len = (size_t)banks * 32 * bd_;
+        x.alloc(len, "device_buffers x");
+        b.alloc(len, "device_buffers b");
+        r.alloc(len, "device_buffers r");
+        pv.alloc(len, "device_buffers p");
+        z.alloc(len, "device_buffers z");
+        Ap.alloc(len, "device_buffers Ap");
+        io.alloc((size_t)n_ > len ? (size_t)n_ : len, "device_buffers io");
+        st.alloc(1, "device_buffers scalars");
+        red_capacity = (banks + 7) / 8 + 160;
+        partials.alloc((size_t)red_capacity * 2, "device_buffers reduction");
+        cuda_check(cudaMemsetAsync(x.get(), 0, x.bytes(), stream), "memset");
+        cuda_check(cudaMemsetAsync(pv.get(), 0, pv.bytes(), stream), "memset");
+        cuda_check(cudaMemsetAsync(z.get(), 0, z.bytes(), stream), "memset");
+        cuda_check(cudaMemsetAsync(Ap.get(), 0, Ap.bytes(), stream), "memset");
+        cuda_check(cudaStreamSynchronize(stream), "factorize");
+        factorized = true;
+        factorize_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+
+    void require_factorized(int len)
+    {
+        if (!factorized || len != n || len <= 0)
+            throw Error(ERR_NOT_FACTORIZED, "[MAS] Size mismatch. Did you forget to call factorize?");
+    }
+
+    ReduceBuf red() { return ReduceBuf{partials.get(), red_capacity}; }
+
+    PcgConfig config() const
+    {
+        PcgConfig c;
+        c.max_iter = p.max_iter;
+        c.rel_tol = p.rel_tol;
+        c.abs_tol = p.abs_tol;
+        c.use_prec_norm = p.use_prec_norm ? 1 : 0;
+        c.check_period = p.check_period;
+        c.polak_ribiere = p.polak_ribiere ? 1 : 0;
+        return c;
+    }
+
+    // pcg_solve (MASSolver.cu:469-595) on device-resident b_ / x_ (padded order).
+    void pcg()
+    {
+        const BankedView Av = A.view();
+        const MasView mv = mas.view();
+        const PcgConfig cfg = config();
+        PcgState *S = st.get();
+        const int nodes = banks * 32;
+        cudaEvent_t e0, e1;
+        cuda_check(cudaEventCreate(&e0), "event");
+        cuda_check(cudaEventCreate(&e1), "event");
+        cuda_check(cudaEventRecord(e0, stream), "event");
+        launch_pcg_init_state(S, stream);
+        const int coarse_k = mas.total_coarse > 0 ? 1 : 0;
+        // r = b - A x, its level-0 restriction and rr0
+        run("spmv_residual", 1, [&] { launch_spmv(SPMV_RESIDUAL, Av, x.get(), r.get(), b.get(), &mv, S, red(), 0, stream); });
+        run("mas_coarse", coarse_k, [&] { launch_coarse(mv, S, stream); });
+        run("mas_symv0", 1, [&] { launch_symv0(mv, r.get(), z.get(), S, red(), cfg, 0, 1, stream); });
+        run("update_p", 1, [&] { launch_update_p(nodes, bd, pv.get(), z.get(), S, 1, stream); });
+        cuda_check(cudaMemcpyAsync(&h_st[0], S, sizeof(PcgState), cudaMemcpyDeviceToHost, stream), "state");
+        cuda_check(cudaStreamSynchronize(stream), "pcg init");
+        rz0 = h_st[0].rz0;
+        rr0 = h_st[0].rr0;
+        if (h_st[0].error == ERR_NONFINITE || std::isnan(rz0) || !std::isfinite(rz0))
+        {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            throw Error(ERR_NONFINITE, "[MAS] Invalid initial residual.");
+        }
+        status = MAS_STATUS_RUNNING;
+        const int P = p.true_residual_period;
+        const int chunk = p.poll_period;
+        int launched = 0;
+        bool stop = false;
+        int pending = -1; // slot holding the previous chunk's state copy
+        cudaEvent_t chunk_ev[2];
+        cuda_check(cudaEventCreateWithFlags(&chunk_ev[0], cudaEventDisableTiming), "event");
+        cuda_check(cudaEventCreateWithFlags(&chunk_ev[1], cudaEventDisableTiming), "event");
+        for (int k0 = 1; k0 <= p.max_iter && !stop; k0 += chunk)
+        {
+            const int k1 = std::min(p.max_iter, k0 + chunk - 1);
+            for (int k = k0; k <= k1; ++k)
+            {
+                run("spmv_pap", 1, [&] { launch_spmv(SPMV_PAP, Av, pv.get(), Ap.get(), nullptr, &mv, S, red(), k, stream); });
+                if (k % P == 0)
+                {
+                    run("update_x", 1, [&] { launch_update_x(nodes, bd, x.get(), pv.get(), S, stream); });
+                    run("spmv_residual", 1, [&] { launch_spmv(SPMV_RESIDUAL, Av, x.get(), r.get(), b.get(), &mv, S, red(), k, stream); });
+                }
+                else
+                    run("update_xr", 1, [&] { launch_update_xr(Av, mv, x.get(), r.get(), pv.get(), Ap.get(), S, red(), stream); });
+                run("mas_coarse", coarse_k, [&] { launch_coarse(mv, S, stream); });
+                run("mas_symv0", 1, [&] { launch_symv0(mv, r.get(), z.get(), S, red(), cfg, k, 2, stream); });
+                run("update_p", 1, [&] { launch_update_p(nodes, bd, pv.get(), z.get(), S, 0, stream); });
+            }
+            launched = k1;
+            const int slot = (k0 / chunk) & 1;
+            cuda_check(cudaMemcpyAsync(&h_st[slot], S, sizeof(PcgState), cudaMemcpyDeviceToHost, stream), "state");
+            cuda_check(cudaEventRecord(chunk_ev[slot], stream), "event");
+            // Look at the previous chunk's state while this chunk runs.
+            if (pending >= 0)
+            {
+                cuda_check(cudaEventSynchronize(chunk_ev[pending]), "chunk");
+                if (h_st[pending].done)
+                    stop = true;
+            }
+            pending = slot;
+        }
+        cuda_check(cudaEventRecord(e1, stream), "event");
+        cuda_check(cudaMemcpyAsync(&h_st[0], S, sizeof(PcgState), cudaMemcpyDeviceToHost, stream), "state");
+        cuda_check(cudaStreamSynchronize(stream), "pcg");
+        collect_profile();
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        solve_ms = ms;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaEventDestroy(chunk_ev[0]);
+        cudaEventDestroy(chunk_ev[1]);
+        launched_iterations = launched;
+        const PcgState &f = h_st[0];
+        if (f.error == ERR_TIMEOUT)
+            throw Error(ERR_TIMEOUT, "[MAS] a device-side wait timed out.");
+        if (p.max_iter >= 1)
+            iterations = f.iter;
+        residual_norm = f.res_norm;
+        status = f.status;
+        if (p.max_iter < 1 && iterations == p.max_iter)
+            status = MAS_STATUS_REACH_MAX_ITERATIONS;
+    }
+
+    void load_rhs_device(const double *d_src_b, const double *d_src_x)
+    {
+        const size_t len = (size_t)banks * 32 * bd;
+        run("permute_in", 2, [&] { launch_permute_in(n, bd, V, d_padded.get(), d_src_b, b.get(), len, stream); });
+        if (p.initial_guess_input && d_src_x)
+            run("permute_in", 2, [&] { launch_permute_in(n, bd, V, d_padded.get(), d_src_x, x.get(), len, stream); });
+        else
+            cuda_check(cudaMemsetAsync(x.get(), 0, x.bytes(), stream), "memset");
+    }
+
+    // MASSolverImpl::solve (MASSolver.cu:376-409).
+    void solve(const double *hb, double *hx, int len)
+    {
+        cuda_check(cudaSetDevice(device), "set device");
+        require_factorized(len);
+        if (!hb || !hx)
+            throw Error(ERR_INVALID, "[MAS] solve: null vector.");
+        cuda_check(cudaMemcpyAsync(io.get(), hb, sizeof(double) * n, cudaMemcpyHostToDevice, stream), "upload b");
+        const size_t blen = (size_t)banks * 32 * bd;
+        run("permute_in", 2, [&] { launch_permute_in(n, bd, V, d_padded.get(), io.get(), b.get(), blen, stream); });
+        if (p.initial_guess_input)
+        {
+            cuda_check(cudaMemcpyAsync(io.get(), hx, sizeof(double) * n, cudaMemcpyHostToDevice, stream), "upload x");
+            run("permute_in", 2, [&] { launch_permute_in(n, bd, V, d_padded.get(), io.get(), x.get(), blen, stream); });
+        }
+        else
+            cuda_check(cudaMemsetAsync(x.get(), 0, x.bytes(), stream), "memset");
+        pcg();
+        run("permute_out", 1, [&] { launch_permute_out(n, bd, V, d_padded.get(), x.get(), io.get(), stream); });
+        cuda_check(cudaMemcpyAsync(hx, io.get(), sizeof(double) * n, cudaMemcpyDeviceToHost, stream), "download x");
+        cuda_check(cudaStreamSynchronize(stream), "solve");
+    }
+
+    void solve_device(const double *d_b, double *d_x, int len)
+    {
+        cuda_check(cudaSetDevice(device), "set device");
+        require_factorized(len);
+        load_rhs_device(d_b, d_x);
+        pcg();
+        run("permute_out", 1, [&] { launch_permute_out(n, bd, V, d_padded.get(), x.get(), d_x, stream); });
+        cuda_check(cudaStreamSynchronize(stream), "solve");
+    }
+
+    std::string info_json() const
+    {
+        Json o;
+        o.type = Json::Object;
+        auto num = [](double v, bool integer) {
+            Json j;
+            j.type = Json::Number;
+            j.num = v;
+            j.is_integer = integer;
+            return j;
+        };
+        auto str = [](const std::string &s) {
+            Json j;
+            j.type = Json::String;
+            j.str = s;
+            return j;
+        };
+        o.obj.emplace_back("solver_iter", num(iterations, true));
+        o.obj.emplace_back("solver_error", num(residual_norm, false));
+        o.obj.emplace_back("solver_status", str(status_string(status)));
+        const double ref = p.use_prec_norm ? std::sqrt(std::fabs(rz0)) : std::sqrt(std::fabs(rr0));
+        o.obj.emplace_back("relative_residual", num(ref > 0 ? residual_norm / ref : 0.0, false));
+        o.obj.emplace_back("precision", str(p.fp32 ? "fp32" : "fp64"));
+        o.obj.emplace_back("x0_source", str(p.initial_guess_input ? "input" : "zero"));
+        o.obj.emplace_back("ordering", str(ordering_used));
+        o.obj.emplace_back("solve_ms", num(solve_ms, false));
+        o.obj.emplace_back("factorize_ms", num(factorize_ms, false));
+        o.obj.emplace_back("launched_iterations", num(launched_iterations, true));
+        o.obj.emplace_back("banks", num(banks, true));
+        o.obj.emplace_back("coarse_levels", num(mas.level_num, true));
+        o.obj.emplace_back("kernel_launches_total", num((double)total_launches, true));
+        Json kl, km;
+        kl.type = km.type = Json::Object;
+        for (const auto &ks : kstats)
+        {
+            kl.obj.emplace_back(ks.first, num((double)ks.second.launches, true));
+            km.obj.emplace_back(ks.first, num(ks.second.ms, false));
+        }
+        o.obj.emplace_back("kernel_launches", kl);
+        if (p.profile)
+            o.obj.emplace_back("kernel_ms", km);
+        o.obj.emplace_back("subdomain_matrices", num(mas.total_mats, true));
+        return o.dump();
+    }
+};
+
+// ------------------------------------------------------------------------------------------------
+// C ABI
+// ------------------------------------------------------------------------------------------------
+
+namespace
+{
+    template <class F>
+    int guarded(mas_solver *h, F &&f)
+    {
+        try
+        {
+            f();
+            if (h)
+                h->last_error.clear();
+            return MAS_OK;
+        }
+        catch (const Error &e)
+        {
+            if (h)
+                h->last_error = e.what();
+            else
+                g_create_error = e.what();
+            return e.code;
+        }
+        catch (const std::bad_alloc &)
+        {
+            if (h)
+                h->last_error = "[MAS] host allocation failed";
+            return ERR_OOM;
+        }
+        catch (const std::exception &e)
+        {
+            if (h)
+                h->last_error = std::string("[MAS] ") + e.what();
+            else
+                g_create_error = std::string("[MAS] ") + e.what();
+            return ERR_INVALID;
+        }
+    }
+
+    int create_common(Params p, mas_solver **out)
+    {
+        *out = nullptr;
+        auto *h = new mas_solver();
+        h->p = p;
+        int rc = guarded(nullptr, [&] { h->init_device(); });
+        if (rc != MAS_OK)
+        {
+            delete h;
+            return rc;
+        }
+        *out = h;
+        return MAS_OK;
+    }
+} // namespace
+
+extern "C" int mas_create(const char *solver, const char *precond, mas_solver **out)
+{
+    (void)precond;
+    if (!out)
+        return MAS_ERR_INVALID;
+    *out = nullptr;
+    if (!solver || std::strcmp(solver, "MAS") != 0)
+    {
+        g_create_error = std::string("[MAS] Unknown solver ") + (solver ? solver : "(null)") + "; this library provides \"MAS\".";
+        return MAS_ERR_INVALID;
+    }
+    g_create_error.clear();
+    return create_common(Params{}, out);
+}
+
+extern "C" int mas_create_json(const char *params_json, int strict_validation, mas_solver **out)
+{
+    if (!out)
+        return MAS_ERR_INVALID;
+    *out = nullptr;
+    Params p;
+    // Spec defaults injected by Solver::create(json) (linear-solver-spec.json:481-509).
+    p.max_iter = 10000;
+    p.rel_tol = 1e-4;
+    p.abs_tol = 1e-8;
+    p.lazy = true;
+    p.block_dim = 1;
+    p.use_prec_norm = false;
+    int rc = guarded(nullptr, [&] {
+        Json j = Json::parse(params_json ? params_json : "{}");
+        if (j.type != Json::Object)
+            throw Error(ERR_INVALID, "[MAS] invalid input json: parameters must be an object");
+        if (auto *s = j.find("solver"))
+        {
+            if (s->type != Json::String || s->str != "MAS")
+                throw Error(ERR_INVALID, "[MAS] invalid input json: this library provides only solver \"MAS\"");
+        }
+        if (strict_validation)
+            for (const auto &kv : j.obj)
+                if (kv.first != "solver" && kv.first != "precond" && kv.first != "MAS")
+                    throw Error(ERR_INVALID, "[MAS] invalid input json: unknown key /" + kv.first);
+        if (auto *m = j.find("MAS"))
+            if (m->type != Json::Null)
+                apply_mas_params(p, *m, strict_validation != 0);
+    });
+    if (rc != MAS_OK)
+        return rc;
+    g_create_error.clear();
+    return create_common(p, out);
+}
+
+extern "C" void mas_destroy(mas_solver *h)
+{
+    delete h;
+}
+
+extern "C" int mas_set_parameters(mas_solver *h, const char *params_json)
+{
+    if (!h)
+        return MAS_ERR_INVALID;
+    return guarded(h, [&] {
+        Json j = Json::parse(params_json ? params_json : "{}");
+        const Json *m = j.find("MAS");
+        if (!m)
+            return; // MASSolver::set_parameters returns silently (MASSolver.cu:607-611)
+        apply_mas_params(h->p, *m, false);
+    });
+}
+
+extern "C" int mas_get_info(const mas_solver *h, char *buf, size_t cap, size_t *needed)
+{
+    if (!h)
+        return MAS_ERR_INVALID;
+    const std::string s = h->info_json();
+    if (needed)
+        *needed = s.size() + 1;
+    if (buf && cap > 0)
+    {
+        const size_t k = std::min(cap - 1, s.size());
+        std::memcpy(buf, s.data(), k);
+        buf[k] = '\0';
+    }
+    return MAS_OK;
+}
+
+extern "C" const char *mas_name(void)
+{
+    return "MAS";
+}
+
+extern "C" int mas_analyze_pattern(mas_solver *h, int n, const int *outer, const int *inner, int nnz, int precond_num)
+{
+    (void)precond_num;
+    if (!h)
+        return MAS_ERR_INVALID;
+    return guarded(h, [&] {
+        if (n < 0 || (n > 0 && (!outer || !inner)) || nnz < 0)
+            throw Error(ERR_INVALID, "[MAS] analyze_pattern: invalid matrix arguments.");
+    });
+}
+
+extern "C" int mas_set_positions(mas_solver *h, const double *xyz, int nverts)
+{
+    if (!h)
+        return MAS_ERR_INVALID;
+    return guarded(h, [&] {
+        if (nverts < 0 || (nverts > 0 && !xyz))
+            throw Error(ERR_INVALID, "[MAS] set_positions: invalid arguments.");
+        h->positions.assign(xyz, xyz + (size_t)nverts * 3);
+        h->padded.clear(); // a new geometry invalidates a lazily kept ordering
+    });
+}
+
+extern "C" int mas_factorize_csc(mas_solver *h, int n, const int *outer, const int *inner, const double *vals, int nnz)
+{
+    if (!h)
+        return MAS_ERR_INVALID;
+    return guarded(h, [&] { h->factorize(n, outer, inner, vals, nnz); });
+}
+
+extern "C" int mas_solve(mas_solver *h, const double *b, double *x, int n)
+{
+    if (!h)
+        return MAS_ERR_INVALID;
+    return guarded(h, [&] { h->solve(b, x, n); });
+}
+
+extern "C" int mas_solve_multi(mas_solver *h, const double *B, double *X, int n, int nrhs)
+{
+    if (!h)
+        return MAS_ERR_INVALID;
+    return guarded(h, [&] {
+        if (nrhs < 0)
+            throw Error(ERR_INVALID, "[MAS] solve_multi: nrhs must be >= 0");
+        for (int c = 0; c < nrhs; ++c)
+            h->solve(B + (size_t)c * n, X + (size_t)c * n, n);
+    });
+}
+
+extern "C" int mas_solve_device(mas_solver *h, const double *d_b, double *d_x, int n)
+{
+    if (!h)
+        return MAS_ERR_INVALID;
+    return guarded(h, [&] { h->solve_device(d_b, d_x, n); });
+}
+
+extern "C" int mas_set_stream(mas_solver *h, void *stream)
+{
+    if (!h)
+        return MAS_ERR_INVALID;
+    return guarded(h, [&] {
+        cuda_check(cudaStreamSynchronize(h->stream), "stream switch");
+        h->stream = stream ? static_cast<cudaStream_t>(stream) : h->own_stream;
+    });
+}
+
+extern "C" const char *mas_last_error(const mas_solver *h)
+{
+    if (!h)
+        return g_create_error.c_str();
+    return h->last_error.c_str();
+}
+
+extern "C" int mas_get_sizes(const mas_solver *h, int *sizes)
+{
+    if (!h || !sizes)
+        return MAS_ERR_INVALID;
+    sizes[0] = h->n;
+    sizes[1] = h->bd;
+    sizes[2] = h->V;
+    sizes[3] = h->banks;
+    sizes[4] = h->banks * 32;
+    sizes[5] = h->A.nnzb;
+    sizes[6] = h->mas.level_num;
+    sizes[7] = h->mas.total_mats;
+    for (int i = 0; i < 4; ++i)
+        sizes[8 + i] = h->mas.cco_nums[i];
+    return MAS_OK;
+}
+
+extern "C" int mas_get_ordering(const mas_solver *h, int *padded, int V)
+{
+    if (!h || !padded || V != (int)h->padded.size())
+        return MAS_ERR_INVALID;
+    std::memcpy(padded, h->padded.data(), sizeof(int) * V);
+    return MAS_OK;
+}
+
+extern "C" int mas_order_blocks(int n, const int *outer, const int *inner, int block_dim, const double *xyz,
+                                const char *mode, int *padded, int *banks)
+{
+    if (n <= 0 || !outer || !inner || !padded || !banks || block_dim < 1 || block_dim > 3 || !mode)
+        return MAS_ERR_INVALID;
+    try
+    {
+        const int V = (n + block_dim - 1) / block_dim;
+        std::vector<uint8_t> iso = isolated_blocks(n, outer, inner, block_dim);
+        std::vector<int> p;
+        const std::string m = mode;
+        if (m == "morton")
+        {
+            if (!xyz)
+                return MAS_ERR_INVALID;
+            p = morton_padded(xyz, V, iso, banks);
+        }
+        else if (m == "graph")
+            p = graph_padded(n, outer, inner, block_dim, iso, banks);
+        else if (m == "natural")
+            p = natural_padded(V, banks);
+        else
+            return MAS_ERR_INVALID;
+        std::memcpy(padded, p.data(), sizeof(int) * V);
+        return MAS_OK;
+    }
+    catch (...)
+    {
+        return MAS_ERR_INVALID;
+    }
+}
+
+extern "C" int mas_get_coarse_map(const mas_solver *h, int *map, int nodes)
+{
+    if (!h || !map || !h->factorized || nodes != h->banks * 32)
+        return MAS_ERR_INVALID;
+    auto *hh = const_cast<mas_solver *>(h);
+    return guarded(hh, [&] {
+        cuda_check(cudaSetDevice(h->device), "set device");
+        cuda_check(cudaMemcpy(map, h->mas.map.get(), sizeof(int) * (size_t)nodes * 4, cudaMemcpyDeviceToHost), "map");
+    });
+}
+
+extern "C" int mas_get_inverses(const mas_solver *h, double *out, size_t count)
+{
+    if (!h || !out || !h->factorized)
+        return MAS_ERR_INVALID;
+    const int bd = h->bd;
+    const int N = 32 * bd;
+    const size_t S = (size_t)N * (N + 1) / 2;
+    if (count != S * h->mas.total_mats)
+        return MAS_ERR_INVALID;
+    auto *hh = const_cast<mas_solver *>(h);
+    return guarded(hh, [&] {
+        cuda_check(cudaSetDevice(h->device), "set device");
+        std::vector<double> tp(count);
+        if (h->mas.fp32)
+        {
+            std::vector<float> f(count);
+            cuda_check(cudaMemcpy(f.data(), h->mas.inv32.get(), sizeof(float) * count, cudaMemcpyDeviceToHost), "inv");
+            for (size_t i = 0; i < count; ++i)
+                tp[i] = f[i];
+        }
+        else
+            cuda_check(cudaMemcpy(tp.data(), h->mas.inv64.get(), sizeof(double) * count, cudaMemcpyDeviceToHost), "inv");
+        for (int m = 0; m < h->mas.total_mats; ++m)
+            for (int i = 0; i < N; ++i)
+                for (int j = i; j < N; ++j)
+                    out[(size_t)m * S + (size_t)i * N - (size_t)i * (i + 1) / 2 + j] =
+                        tp[(size_t)m * S + tile_packed_index(bd, i, j)];
+    });
+}
+
+extern "C" int mas_debug_spmv(mas_solver *h, const double *xin, double *y, int len)
+{
+    if (!h)
+        return MAS_ERR_INVALID;
+    return guarded(h, [&] {
+        cuda_check(cudaSetDevice(h->device), "set device");
+        if (!h->factorized || len != h->banks * 32 * h->bd)
+            throw Error(ERR_NOT_FACTORIZED, "[MAS] debug_spmv: size mismatch.");
+        cuda_check(cudaMemcpyAsync(h->x.get(), xin, sizeof(double) * len, cudaMemcpyHostToDevice, h->stream), "x");
+        launch_spmv(SPMV_PLAIN, h->A.view(), h->x.get(), h->Ap.get(), nullptr, nullptr, nullptr, h->red(), 0,
+                    h->stream);
+        cuda_check(cudaMemcpyAsync(y, h->Ap.get(), sizeof(double) * len, cudaMemcpyDeviceToHost, h->stream), "y");
+        cuda_check(cudaStreamSynchronize(h->stream), "spmv");
+    });
+}
+
+extern "C" int mas_debug_apply(mas_solver *h, const double *rin, double *zout, int len)
+{
+    if (!h)
+        return MAS_ERR_INVALID;
+    return guarded(h, [&] {
+        cuda_check(cudaSetDevice(h->device), "set device");
+        if (!h->factorized || len != h->banks * 32 * h->bd)
+            throw Error(ERR_NOT_FACTORIZED, "[MAS] debug_apply: size mismatch.");
+        cuda_check(cudaMemcpyAsync(h->r.get(), rin, sizeof(double) * len, cudaMemcpyHostToDevice, h->stream), "r");
+        const MasView mv = h->mas.view();
+        launch_restrict_plain(h->A.view(), mv, h->r.get(), h->stream);
+        launch_coarse(mv, nullptr, h->stream);
+        launch_symv0(mv, h->r.get(), h->z.get(), nullptr, h->red(), h->config(), 0, 0, h->stream);
+        cuda_check(cudaMemcpyAsync(zout, h->z.get(), sizeof(double) * len, cudaMemcpyDeviceToHost, h->stream), "z");
+        cuda_check(cudaStreamSynchronize(h->stream), "apply");
+    });
+}

@@ -1,0 +1,180 @@
+// Device helpers shared by the MAS-PCG kernels (sm_100a).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "mas_internal.h"
+
+namespace pmas
+{
+    constexpr unsigned FULL = 0xFFFFFFFFu;
+
+    __device__ __forceinline__ double warp_sum(double v)
+    {
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1)
+            v += __shfl_xor_sync(FULL, v, o);
+        return v;
+    }
+
+    __device__ __forceinline__ float warp_sum(float v)
+    {
+#pragma unroll
+        for (int o = 16; o >= 1; o >>= 1)
+            v += __shfl_xor_sync(FULL, v, o);
+        return v;
+    }
+
+    // Deterministic grid-wide sum of NV values per CTA: every CTA writes its block sum to
+    // partials[blockIdx.x * NV + i]; the last CTA to arrive (atomic ticket) adds the partials in
+    // a fixed order. Returns true in the last CTA, with tot[] the totals (valid in all its
+    // threads). Every thread of every CTA must call it.
+    template <int NV, int THREADS>
+    __device__ __forceinline__ bool grid_reduce(double (&v)[NV], double *partials, unsigned *counter, double (&tot)[NV])
+    {
+        constexpr int W = THREADS / 32;
+        __shared__ double sh[W][NV];
+        __shared__ int is_last;
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+        for (int i = 0; i < NV; ++i)
+            v[i] = warp_sum(v[i]);
+        if (lane == 0)
+#pragma unroll
+            for (int i = 0; i < NV; ++i)
+                sh[w][i] = v[i];
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+#pragma unroll
+            for (int i = 0; i < NV; ++i)
+            {
+                double s = 0.0;
+                for (int ww = 0; ww < W; ++ww)
+                    s += sh[ww][i];
+                partials[(size_t)blockIdx.x * NV + i] = s;
+            }
+            __threadfence();
+            unsigned t = atomicAdd(counter, 1u);
+            is_last = (t == gridDim.x - 1);
+        }
+        __syncthreads();
+        if (!is_last)
+            return false;
+        __threadfence();
+        double s[NV];
+#pragma unroll
+        for (int i = 0; i < NV; ++i)
+        {
+            s[i] = 0.0;
+            for (int b = threadIdx.x; b < (int)gridDim.x; b += THREADS)
+                s[i] += __ldcg(partials + (size_t)b * NV + i);
+            s[i] = warp_sum(s[i]);
+        }
+        __syncthreads();
+        if (lane == 0)
+#pragma unroll
+            for (int i = 0; i < NV; ++i)
+                sh[w][i] = s[i];
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < NV; ++i)
+        {
+            double t = 0.0;
+            for (int ww = 0; ww < W; ++ww)
+                t += sh[ww][i];
+            tot[i] = t;
+        }
+        if (threadIdx.x == 0)
+            *counter = 0u;
+        return true;
+    }
+
+    // Sum of a per-lane value over the lanes whose key equals each distinct key of the warp,
+    // written by lane 0 of each group to out[(base + key) * BD + i]. Keys < 0 are skipped.
+    // Order of additions is fixed (xor butterfly), so results are deterministic.
+    template <int BD>
+    __device__ __forceinline__ void warp_segment_store(const double (&val)[BD], int key, int base, double *out)
+    {
+        const int lane = threadIdx.x & 31;
+        unsigned pending = __ballot_sync(FULL, key >= 0);
+        while (pending)
+        {
+            const int leader = __ffs(pending) - 1;
+            const int k = __shfl_sync(FULL, key, leader);
+            const bool in = (key == k);
+#pragma unroll
+            for (int i = 0; i < BD; ++i)
+            {
+                double s = warp_sum(in ? val[i] : 0.0);
+                if (lane == 0)
+                    out[(size_t)(base + k) * BD + i] = s;
+            }
+            pending &= ~__ballot_sync(FULL, in);
+        }
+    }
+
+    // ---------------------------------------------------------------------------------------
+    // mbarrier + bulk copy (cp.async.bulk, the 1D TMA path) with bounded waits.
+    // ---------------------------------------------------------------------------------------
+    __device__ __forceinline__ uint32_t smem_addr(const void *p)
+    {
+        return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+    }
+
+    __device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
+    {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+    }
+
+    __device__ __forceinline__ void fence_mbar_init()
+    {
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+
+    __device__ __forceinline__ void fence_proxy_async_smem()
+    {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+
+    // Arm the barrier for `bytes` and start a global -> shared bulk copy completing on it.
+    // dst, src and bytes must be 16-byte aligned / multiples of 16.
+    __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+    {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                     : "memory");
+        asm volatile(
+            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                smem_addr(dst)),
+            "l"(src), "r"(bytes), "r"(smem_addr(bar))
+            : "memory");
+    }
+
+    __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+    {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(smem_addr(bar)), "r"(parity)
+            : "memory");
+        return ok != 0;
+    }
+
+    // Wait for phase `parity` of the barrier with an iteration limit. On timeout records
+    // ERR_TIMEOUT in *err and returns false.
+    constexpr long long MBAR_SPIN_LIMIT = 1LL << 24;
+
+    __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *err)
+    {
+        for (long long i = 0; i < MBAR_SPIN_LIMIT; ++i)
+            if (mbar_try_wait(bar, parity))
+                return true;
+        if (err)
+            atomicExch(err, ERR_TIMEOUT);
+        return false;
+    }
+} // namespace pmas

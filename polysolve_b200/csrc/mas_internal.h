@@ -1,0 +1,267 @@
+// Internal interfaces of the B200 MAS-PCG solver: device data layouts and the host-side launch
+// functions that the .cu files define. Plain host C++ can include this file (no CUDA syntax).
+//
+// Numbering. The solver works in a "padded" block order: node = bank * 32 + lane. A bank is one
+// 32-node subdomain of the MAS preconditioner (BANK_SIZE, mas_utils/MASPreconditioner.cu:33);
+// lanes of a bank not covered by a real block row are virtual (padding) nodes with empty rows.
+// Every vector inside the solver is node-major: value index = node * block_dim + component.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <cuda_runtime_api.h>
+
+namespace pmas
+{
+    constexpr int BANK = 32;
+    constexpr int MAX_COARSE = 4; // coarse levels (MASPreconditioner.hpp:11)
+    constexpr int LEVELS = MAX_COARSE + 1;
+
+    // Status codes (mirror include/polysolve_mas.h).
+    enum : int
+    {
+        OK = 0,
+        ERR_INVALID = 1,
+        ERR_OOM = 2,
+        ERR_NOT_FACTORIZED = 3,
+        ERR_CUDA = 4,
+        ERR_NONFINITE = 5,
+        ERR_INVERSE = 6,
+        ERR_TIMEOUT = 7,
+        ERR_NO_DEVICE = 8,
+    };
+
+    struct Error : std::runtime_error
+    {
+        int code;
+        Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+    };
+
+    void cuda_check(cudaError_t e, const char *what);
+    void *device_alloc(size_t bytes, const char *ctx); // throws Error(ERR_OOM) with MB figures
+    void device_free(void *p);
+
+    // Owning device buffer.
+    template <class T>
+    struct DevBuf
+    {
+        T *p = nullptr;
+        size_t n = 0;
+        DevBuf() = default;
+        DevBuf(const DevBuf &) = delete;
+        DevBuf &operator=(const DevBuf &) = delete;
+        ~DevBuf() { reset(); }
+        void reset()
+        {
+            if (p)
+                device_free(p);
+            p = nullptr;
+            n = 0;
+        }
+        void alloc(size_t count, const char *ctx)
+        {
+            if (count == n && p)
+                return;
+            reset();
+            if (count)
+                p = static_cast<T *>(device_alloc(count * sizeof(T), ctx));
+            n = count;
+        }
+        T *get() const { return p; }
+        size_t bytes() const { return n * sizeof(T); }
+    };
+
+    // ---------------------------------------------------------------------------------------
+    // Bank-sliced block matrix ("banked BSR"): every bank (32 block rows) is a slice of width
+    // w_b = max row length in the bank; slot s of the slice holds the s-th block of each of the
+    // 32 rows. Within a slot the bd*bd values of the 32 lanes are stored as value pairs
+    // (q = 2p, 2p+1) interleaved per lane (16 B per lane, 512 B per pair plane), then the odd
+    // last value (if bd*bd is odd) as a plane of 32 doubles: one warp reads a slot with
+    // coalesced 128-bit loads.
+    // ---------------------------------------------------------------------------------------
+    struct BankedView
+    {
+        int bd;
+        int banks;
+        const long long *slice; // banks + 1, in slots
+        const int *rowlen;      // nodes
+        const int *cols;        // slots * 32, padded node ids
+        const double *vals;     // slots * 32 * bd * bd
+    };
+
+    __host__ __device__ inline long long banked_value_index(long long slot, int lane, int q, int bd)
+    {
+        const int bs = bd * bd;
+        const int pairs = bs / 2;
+        const long long base = slot * 32LL * bs;
+        if (q < 2 * pairs)
+            return base + (long long)(q >> 1) * 64 + lane * 2 + (q & 1);
+        return base + (long long)pairs * 64 + lane;
+    }
+
+    // ---------------------------------------------------------------------------------------
+    // Subdomain matrix storage ("tile-packed"): an N x N symmetric matrix, N = 32 * bd, split
+    // into bd x bd tiles of 32 x 32. For each column tile J: the off-diagonal tiles (I, J), I < J,
+    // each 1024 values with element (l, j) of the tile at (j / 4) * 128 + l * 4 + j % 4; then the
+    // diagonal tile's upper triangle, column j holding rows 0..j at offset j (j + 1) / 2 + l.
+    // Total N (N + 1) / 2 values, the same count as the reference's packed upper storage.
+    // ---------------------------------------------------------------------------------------
+    __host__ __device__ inline int tile_packed_size(int bd) { return 32 * bd * (32 * bd + 1) / 2; }
+
+    // Position of element (row, col) of the symmetric matrix in tile-packed storage.
+    __host__ __device__ inline int tile_packed_index(int bd, int row, int col)
+    {
+        if (row > col)
+        {
+            int t = row;
+            row = col;
+            col = t;
+        }
+        const int I = row >> 5, J = col >> 5, l = row & 31, j = col & 31;
+        int off = 0;
+        for (int jj = 0; jj < J; ++jj)
+            off += jj * 1024 + 528;
+        if (I < J)
+            return off + I * 1024 + (j >> 2) * 128 + l * 4 + (j & 3);
+        return off + J * 1024 + j * (j + 1) / 2 + l;
+    }
+
+    // ---------------------------------------------------------------------------------------
+    // MAS preconditioner on the device.
+    // ---------------------------------------------------------------------------------------
+    struct MasView
+    {
+        int bd;
+        int banks;              // level-0 matrices
+        int level_num;          // coarse levels in use (0..4)
+        int total_coarse;       // coarse matrices (all levels >= 1)
+        int coarse_level_of[LEVELS];  // not used on device
+        int mat_offsets[LEVELS];      // first matrix of each matrix level (0 = banks)
+        int mat_counts[LEVELS];
+        int cco_nums[MAX_COARSE];
+        int fp32;               // storage precision of the inverses
+        const void *inv;        // total_mats * tile_packed_size(bd), float or double
+        const int *lcco0;       // nodes: bank-local level-0 component id, -1 virtual
+        const int *cco0_base;   // banks: first global level-0 component id of the bank
+        const int4 *cslot;      // nodes: coarse-vector node of each coarse level (-1 unused)
+        const int *member_ptr;  // coarse nodes + 1: CSR of level-0 components per coarse node
+        const int *members;
+        double *rc;             // coarse residual, coarse nodes * bd (level-0 components first)
+        double *zc;             // coarse correction, coarse nodes * bd
+    };
+
+    // Device-resident PCG state; all scalars of the reference (MASSolver.cu:178-183) plus control.
+    struct PcgState
+    {
+        double rz, rz_old, pAp, alpha, beta, rr, rr0, rz0, res_norm, rzold_cross;
+        int iter;      // last finished iteration
+        int done;      // 1: converged / stopped; kernels return immediately
+        int status;    // MAS_STATUS_*
+        int error;     // device-detected error code (ERR_NONFINITE, ERR_TIMEOUT)
+        unsigned int counter[8];
+    };
+
+    struct PcgConfig
+    {
+        int max_iter;
+        double rel_tol, abs_tol;
+        int use_prec_norm;
+        int check_period;
+        int polak_ribiere;
+    };
+
+    // Scratch for deterministic two-stage reductions: per-CTA partials.
+    struct ReduceBuf
+    {
+        double *partials; // capacity >= max grid * 2
+        int capacity;
+    };
+
+    // ---------------------------------------------------------------------------------------
+    // Launchers (defined in the .cu files). All take the solver's stream.
+    // ---------------------------------------------------------------------------------------
+
+    // mas_bsr.cu: CSC (device) -> banked matrix. padded_of_block[V] maps old block rows to
+    // padded nodes. Allocates the outputs. scatter[k] = value index of CSC entry k.
+    struct BankedMatrix
+    {
+        int bd = 0, banks = 0, nodes = 0;
+        long long slots = 0;
+        int nnzb = 0;
+        DevBuf<long long> slice;
+        DevBuf<int> rowlen;
+        DevBuf<int> cols;
+        DevBuf<double> vals;
+        DevBuf<long long> scatter; // per CSC entry
+        long long pad_index[3] = {-1, -1, -1}; // value slots padded with 1.0 (trailing block)
+        int npad = 0;
+        BankedView view() const
+        {
+            return BankedView{bd, banks, slice.get(), rowlen.get(), cols.get(), vals.get()};
+        }
+    };
+
+    void build_banked(BankedMatrix &M, int n, long long nnz, const int *d_outer, const int *d_inner,
+                      const double *d_vals, int bd, int V, int banks, const int *d_padded_of_block,
+                      cudaStream_t s);
+    void rescatter_values(BankedMatrix &M, long long nnz, const double *d_vals, cudaStream_t s);
+
+    // mas_spmv.cu
+    enum SpmvMode : int
+    {
+        SPMV_PLAIN = 0,    // y = A x
+        SPMV_PAP = 1,      // y = A p ; pAp = p . y ; alpha = rz / pAp
+        SPMV_RESIDUAL = 2, // y = b - A x ; restrict y to level-0 components ; rr = y . y
+    };
+    void launch_spmv(int mode, const BankedView &A, const double *x, double *y, const double *b, const MasView *mas,
+                     PcgState *st, ReduceBuf red, int iter, cudaStream_t s);
+
+    // mas_pcg.cu
+    void launch_update_xr(const BankedView &A, const MasView &mas, double *x, double *r, const double *p,
+                          const double *Ap, PcgState *st, ReduceBuf red, cudaStream_t s);
+    void launch_update_x(int nodes, int bd, double *x, const double *p, PcgState *st, cudaStream_t s);
+    void launch_update_p(int nodes, int bd, double *p, const double *z, PcgState *st, int first, cudaStream_t s);
+    void launch_permute_in(int n, int bd, int V, const int *padded_of_block, const double *src, double *dst,
+                           size_t dst_len, cudaStream_t s);
+    void launch_permute_out(int n, int bd, int V, const int *padded_of_block, const double *src, double *dst,
+                            cudaStream_t s);
+    void launch_pcg_init_state(PcgState *st, cudaStream_t s);
+
+    // mas_apply.cu
+    void launch_coarse(const MasView &mas, PcgState *st, cudaStream_t s);
+    void launch_symv0(const MasView &mas, const double *r, double *z, PcgState *st, ReduceBuf red, PcgConfig cfg,
+                      int iter, int mode, cudaStream_t s);
+    // mode for launch_symv0: 0 = plain apply (no PCG bookkeeping), 1 = initial (rz0), 2 = iteration
+    void launch_restrict_plain(const BankedView &A, const MasView &mas, const double *r, cudaStream_t s);
+
+    // mas_build.cu: the MAS hierarchy and inverses.
+    struct MasDevice
+    {
+        int bd = 0, banks = 0, nodes = 0;
+        int level_num = 0;
+        int cco_nums[MAX_COARSE] = {0, 0, 0, 0};
+        int mat_counts[LEVELS] = {0, 0, 0, 0, 0};
+        int mat_offsets[LEVELS] = {0, 0, 0, 0, 0};
+        int total_mats = 0, total_coarse = 0;
+        int coarse_nodes = 0;
+        int fp32 = 1;
+        DevBuf<int> node_real;   // nodes: 1 if the node is a real block row
+        DevBuf<int> map;         // nodes * 4
+        DevBuf<int> lcco0;
+        DevBuf<int> cco0_base;
+        DevBuf<int4> cslot;
+        DevBuf<int> member_ptr, members;
+        DevBuf<float> inv32;
+        DevBuf<double> inv64;
+        DevBuf<double> rc, zc;
+        DevBuf<int> flag;        // device error flag for the inverses
+        MasView view(double *rc_override = nullptr) const;
+    };
+
+    void build_mas(MasDevice &M, const BankedMatrix &A, const int *d_node_real, int fp32, cudaStream_t s);
+
+    // mas_pcg.cu: misc
+    void launch_zero(double *p, size_t n, cudaStream_t s);
+} // namespace pmas

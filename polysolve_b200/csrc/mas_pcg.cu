@@ -1,0 +1,218 @@
+// PCG vector kernels (sm_100a) and device-memory plumbing.
+//
+// The reference runs each vector step as its own launch (axpby / inner_product / scalar_division,
+// MASSolver.cu:46-81, InnerProduct.cu:16-45) with a memset and an FP64 atomicAdd per dot. Here:
+//   update_xr: x += alpha p ; r -= alpha Ap ; rr = r . r ; level-0 restriction of r   (one pass)
+//   update_x:  x += alpha p                       (true-residual steps; r = b - A x follows)
+//   update_p:  p = z + beta p                     (beta computed on the device by the MAS apply)
+// alpha / beta are read from the device-resident PcgState, and every dot is a deterministic
+// two-stage reduction, so no host round trip is needed inside the iteration.
+
+#include <cstdio>
+#include <string>
+
+#include "mas_common.cuh"
+
+namespace pmas
+{
+    void cuda_check(cudaError_t e, const char *what)
+    {
+        if (e != cudaSuccess)
+            throw Error(ERR_CUDA, std::string("[MAS] CUDA error in ") + what + ": " + cudaGetErrorString(e));
+    }
+
+    // Allocation with the reference's out-of-memory message (mas_utils/CudaUtils.cuh:68-79).
+    void *device_alloc(size_t bytes, const char *ctx)
+    {
+        void *p = nullptr;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if (e == cudaSuccess)
+            return p;
+        if (e != cudaErrorMemoryAllocation)
+            cuda_check(e, ctx);
+        cudaGetLastError();
+        size_t free_b = 0, total_b = 0;
+        cudaMemGetInfo(&free_b, &total_b);
+        const size_t mb = 1024ull * 1024ull;
+        throw Error(ERR_OOM, std::string("[MAS] Failed to allocate ") + std::to_string((bytes + mb - 1) / mb) +
+                                 " MB for " + (ctx ? ctx : "cuda allocation") + "; only " +
+                                 std::to_string(free_b / mb) + " MB free.");
+    }
+
+    void device_free(void *p)
+    {
+        if (p)
+            cudaFree(p);
+    }
+
+    namespace
+    {
+        constexpr int UPD_THREADS = 256;
+
+        template <int BD>
+        __global__ void __launch_bounds__(UPD_THREADS) k_update_xr(int banks, double *__restrict__ x, double *__restrict__ r,
+                                                                   const double *__restrict__ p,
+                                                                   const double *__restrict__ Ap,
+                                                                   const int *__restrict__ lcco0,
+                                                                   const int *__restrict__ cco0_base, double *rc,
+                                                                   PcgState *st, ReduceBuf red)
+        {
+            if (st->done)
+                return;
+            const double alpha = st->alpha;
+            const int lane = threadIdx.x & 31;
+            const int bank = blockIdx.x * (UPD_THREADS / 32) + (threadIdx.x >> 5);
+            double part = 0.0;
+            if (bank < banks)
+            {
+                const long long u = (long long)bank * 32 + lane;
+                double rv[BD];
+#pragma unroll
+                for (int i = 0; i < BD; ++i)
+                {
+                    const long long idx = u * BD + i;
+                    x[idx] = fma(alpha, p[idx], x[idx]);
+                    rv[i] = fma(-alpha, Ap[idx], r[idx]);
+                    r[idx] = rv[i];
+                    part = fma(rv[i], rv[i], part);
+                }
+                warp_segment_store<BD>(rv, lcco0[u], cco0_base[bank], rc);
+            }
+            double v1[1] = {part}, tot[1];
+            if (grid_reduce<1, UPD_THREADS>(v1, red.partials, &st->counter[1], tot) && threadIdx.x == 0)
+                st->rr = tot[0];
+        }
+
+        __global__ void k_update_x(long long len, double *__restrict__ x, const double *__restrict__ p,
+                                   const PcgState *st)
+        {
+            if (st->done)
+                return;
+            const double alpha = st->alpha;
+            for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len;
+                 i += (long long)gridDim.x * blockDim.x)
+                x[i] = fma(alpha, p[i], x[i]);
+        }
+
+        __global__ void k_update_p(long long len, double *__restrict__ p, const double *__restrict__ z,
+                                   const PcgState *st, int first)
+        {
+            if (st->done)
+                return;
+            const double beta = first ? 0.0 : st->beta;
+            if (first)
+            {
+                for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len;
+                     i += (long long)gridDim.x * blockDim.x)
+                    p[i] = z[i];
+                return;
+            }
+            for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len;
+                 i += (long long)gridDim.x * blockDim.x)
+                p[i] = fma(beta, p[i], z[i]);
+        }
+
+        // dst (padded, node-major, zero elsewhere) <- src (caller's order, length n)
+        __global__ void k_permute_in(int n, int bd, int V, const int *__restrict__ padded_of_block,
+                                     const double *__restrict__ src, double *__restrict__ dst)
+        {
+            const long long total = (long long)V * bd;
+            for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+                 i += (long long)gridDim.x * blockDim.x)
+            {
+                const int blk = (int)(i / bd), c = (int)(i % bd);
+                dst[(long long)padded_of_block[blk] * bd + c] = (i < n) ? src[i] : 0.0;
+            }
+        }
+
+        __global__ void k_permute_out(int n, int bd, const int *__restrict__ padded_of_block,
+                                      const double *__restrict__ src, double *__restrict__ dst)
+        {
+            for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+                 i += (long long)gridDim.x * blockDim.x)
+            {
+                const int blk = (int)(i / bd), c = (int)(i % bd);
+                dst[i] = src[(long long)padded_of_block[blk] * bd + c];
+            }
+        }
+
+        __global__ void k_zero(double *p, long long n)
+        {
+            for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+                 i += (long long)gridDim.x * blockDim.x)
+                p[i] = 0.0;
+        }
+
+        int grid_for(long long n, int threads = 256)
+        {
+            long long g = (n + threads - 1) / threads;
+            if (g > 148LL * 16)
+                g = 148LL * 16;
+            return (int)(g < 1 ? 1 : g);
+        }
+    } // namespace
+
+    void launch_update_xr(const BankedView &A, const MasView &mas, double *x, double *r, const double *p,
+                          const double *Ap, PcgState *st, ReduceBuf red, cudaStream_t s)
+    {
+        const int grid = (A.banks + UPD_THREADS / 32 - 1) / (UPD_THREADS / 32);
+        if (grid > red.capacity)
+            throw Error(ERR_INVALID, "[MAS] reduction scratch too small");
+        switch (A.bd)
+        {
+        case 1:
+            k_update_xr<1><<<grid, UPD_THREADS, 0, s>>>(A.banks, x, r, p, Ap, mas.lcco0, mas.cco0_base, mas.rc, st, red);
+            break;
+        case 2:
+            k_update_xr<2><<<grid, UPD_THREADS, 0, s>>>(A.banks, x, r, p, Ap, mas.lcco0, mas.cco0_base, mas.rc, st, red);
+            break;
+        default:
+            k_update_xr<3><<<grid, UPD_THREADS, 0, s>>>(A.banks, x, r, p, Ap, mas.lcco0, mas.cco0_base, mas.rc, st, red);
+            break;
+        }
+        cuda_check(cudaGetLastError(), "update_xr launch");
+    }
+
+    void launch_update_x(int nodes, int bd, double *x, const double *p, PcgState *st, cudaStream_t s)
+    {
+        const long long len = (long long)nodes * bd;
+        k_update_x<<<grid_for(len), 256, 0, s>>>(len, x, p, st);
+        cuda_check(cudaGetLastError(), "update_x launch");
+    }
+
+    void launch_update_p(int nodes, int bd, double *p, const double *z, PcgState *st, int first, cudaStream_t s)
+    {
+        const long long len = (long long)nodes * bd;
+        k_update_p<<<grid_for(len), 256, 0, s>>>(len, p, z, st, first);
+        cuda_check(cudaGetLastError(), "update_p launch");
+    }
+
+    void launch_permute_in(int n, int bd, int V, const int *padded_of_block, const double *src, double *dst,
+                           size_t dst_len, cudaStream_t s)
+    {
+        k_zero<<<grid_for((long long)dst_len), 256, 0, s>>>(dst, (long long)dst_len);
+        k_permute_in<<<grid_for((long long)V * bd), 256, 0, s>>>(n, bd, V, padded_of_block, src, dst);
+        cuda_check(cudaGetLastError(), "permute_in launch");
+    }
+
+    void launch_permute_out(int n, int bd, int V, const int *padded_of_block, const double *src, double *dst,
+                            cudaStream_t s)
+    {
+        (void)V;
+        k_permute_out<<<grid_for(n), 256, 0, s>>>(n, bd, padded_of_block, src, dst);
+        cuda_check(cudaGetLastError(), "permute_out launch");
+    }
+
+    void launch_zero(double *p, size_t n, cudaStream_t s)
+    {
+        if (n == 0)
+            return;
+        k_zero<<<grid_for((long long)n), 256, 0, s>>>(p, (long long)n);
+        cuda_check(cudaGetLastError(), "zero launch");
+    }
+
+    void launch_pcg_init_state(PcgState *st, cudaStream_t s)
+    {
+        cuda_check(cudaMemsetAsync(st, 0, sizeof(PcgState), s), "state reset");
+    }
+} // namespace pmas

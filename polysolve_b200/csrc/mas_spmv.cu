@@ -1,0 +1,171 @@
+// Block SpMV on the bank-sliced matrix (sm_100a), FP64.
+//
+// Replaces the reference's cusparseSpMV on a row-major BSR (MASSolver.cu:271-290,
+// CuSparseWrapper.hpp:141-154). One warp per bank: lane l owns block row bank * 32 + l and walks
+// the bank's slots; a slot is one block per lane, read with coalesced 128-bit loads (512 B per
+// value pair per warp), so every byte of A is read once, fully coalesced, with no reduction
+// across lanes. x is gathered by column (it stays L2-resident: 12.8 MB at 1.6 M DOF).
+//
+// Fused epilogues (one pass over A per PCG step):
+//   SPMV_PAP:      y = A p, pAp = p . y, alpha = rz / pAp (0 if |pAp| < 1e-20, MASSolver.cu:46-56)
+//   SPMV_RESIDUAL: y = b - A x, rr = y . y, and the level-0 restriction of y (per-bank sums of
+//                  each connected component, the first coarse level of the MAS apply).
+// The dot products are deterministic two-stage reductions (per-CTA partials, last CTA sums).
+
+#include "mas_common.cuh"
+
+namespace pmas
+{
+    namespace
+    {
+        constexpr int SPMV_THREADS = 256;
+        constexpr int BANKS_PER_CTA = SPMV_THREADS / 32;
+
+        template <int BD, int MODE>
+        __global__ void __launch_bounds__(SPMV_THREADS) k_spmv(BankedView A, const double *__restrict__ x,
+                                                               double *__restrict__ y, const double *__restrict__ b,
+                                                               const int *__restrict__ lcco0,
+                                                               const int *__restrict__ cco0_base, double *rc,
+                                                               PcgState *st, ReduceBuf red, int iter)
+        {
+            constexpr int BS = BD * BD;
+            constexpr int PAIRS = BS / 2;
+            if (MODE != SPMV_PLAIN && st->done)
+                return;
+            const int lane = threadIdx.x & 31;
+            const int bank = blockIdx.x * BANKS_PER_CTA + (threadIdx.x >> 5);
+            double part = 0.0, bb = 0.0;
+            if (bank < A.banks)
+            {
+                const int u = bank * 32 + lane;
+                const long long s0 = A.slice[bank];
+                const int len = A.rowlen[u];
+                const int *cp = A.cols + s0 * 32 + lane;
+                const double *vp = A.vals + s0 * 32 * BS;
+                double acc[BD];
+#pragma unroll
+                for (int i = 0; i < BD; ++i)
+                    acc[i] = 0.0;
+#pragma unroll 2
+                for (int k = 0; k < len; ++k)
+                {
+                    const int col = __ldg(cp + (long long)k * 32);
+                    const double *blk = vp + (long long)k * 32 * BS;
+                    double v[BS];
+#pragma unroll
+                    for (int p = 0; p < PAIRS; ++p)
+                    {
+                        const double2 t = __ldg(reinterpret_cast<const double2 *>(blk + p * 64 + lane * 2));
+                        v[2 * p] = t.x;
+                        v[2 * p + 1] = t.y;
+                    }
+                    if (BS & 1)
+                        v[BS - 1] = __ldg(blk + PAIRS * 64 + lane);
+                    double xc[BD];
+#pragma unroll
+                    for (int j = 0; j < BD; ++j)
+                        xc[j] = __ldg(x + (long long)col * BD + j);
+#pragma unroll
+                    for (int i = 0; i < BD; ++i)
+#pragma unroll
+                        for (int j = 0; j < BD; ++j)
+                            acc[i] = fma(v[i * BD + j], xc[j], acc[i]);
+                }
+                if (MODE == SPMV_PLAIN)
+                {
+#pragma unroll
+                    for (int i = 0; i < BD; ++i)
+                        y[(long long)u * BD + i] = acc[i];
+                }
+                else if (MODE == SPMV_PAP)
+                {
+#pragma unroll
+                    for (int i = 0; i < BD; ++i)
+                    {
+                        y[(long long)u * BD + i] = acc[i];
+                        part = fma(acc[i], x[(long long)u * BD + i], part);
+                    }
+                }
+                else
+                {
+                    double rv[BD];
+#pragma unroll
+                    for (int i = 0; i < BD; ++i)
+                    {
+                        const double bv = b[(long long)u * BD + i];
+                        rv[i] = bv - acc[i];
+                        y[(long long)u * BD + i] = rv[i];
+                        part = fma(rv[i], rv[i], part);
+                        bb = fma(bv, bv, bb);
+                    }
+                    warp_segment_store<BD>(rv, lcco0[u], cco0_base[bank], rc);
+                }
+            }
+            if (MODE == SPMV_PLAIN)
+                return;
+            // rr0 = ||b||^2: equal to the reference's r.r at x = 0 (MASSolver.cu:488-494), and keeps
+            // "relative" relative to ||b|| when an initial guess is used.
+            double v2[2] = {part, bb}, tot[2];
+            if (grid_reduce<2, SPMV_THREADS>(v2, red.partials, &st->counter[0], tot) && threadIdx.x == 0)
+            {
+                if (MODE == SPMV_PAP)
+                {
+                    st->pAp = tot[0];
+                    st->alpha = (fabs(tot[0]) < 1e-20) ? 0.0 : st->rz / tot[0];
+                }
+                else
+                {
+                    st->rr = tot[0];
+                    if (iter == 0)
+                        st->rr0 = tot[1];
+                }
+            }
+        }
+
+        template <int BD>
+        void launch_bd(int mode, const BankedView &A, const double *x, double *y, const double *b, const MasView *mas,
+                       PcgState *st, ReduceBuf red, int iter, cudaStream_t s)
+        {
+            const int grid = (A.banks + BANKS_PER_CTA - 1) / BANKS_PER_CTA;
+            if (grid == 0)
+                return;
+            if (mode != SPMV_PLAIN && grid > red.capacity)
+                throw Error(ERR_INVALID, "[MAS] reduction scratch too small");
+            const int *lcco0 = mas ? mas->lcco0 : nullptr;
+            const int *base = mas ? mas->cco0_base : nullptr;
+            double *rc = mas ? mas->rc : nullptr;
+            switch (mode)
+            {
+            case SPMV_PLAIN:
+                k_spmv<BD, SPMV_PLAIN><<<grid, SPMV_THREADS, 0, s>>>(A, x, y, b, lcco0, base, rc, st, red, iter);
+                break;
+            case SPMV_PAP:
+                k_spmv<BD, SPMV_PAP><<<grid, SPMV_THREADS, 0, s>>>(A, x, y, b, lcco0, base, rc, st, red, iter);
+                break;
+            default:
+                k_spmv<BD, SPMV_RESIDUAL><<<grid, SPMV_THREADS, 0, s>>>(A, x, y, b, lcco0, base, rc, st, red, iter);
+                break;
+            }
+            cuda_check(cudaGetLastError(), "spmv launch");
+        }
+    } // namespace
+
+    void launch_spmv(int mode, const BankedView &A, const double *x, double *y, const double *b, const MasView *mas,
+                     PcgState *st, ReduceBuf red, int iter, cudaStream_t s)
+    {
+        switch (A.bd)
+        {
+        case 1:
+            launch_bd<1>(mode, A, x, y, b, mas, st, red, iter, s);
+            break;
+        case 2:
+            launch_bd<2>(mode, A, x, y, b, mas, st, red, iter, s);
+            break;
+        case 3:
+            launch_bd<3>(mode, A, x, y, b, mas, st, red, iter, s);
+            break;
+        default:
+            throw Error(ERR_INVALID, "[MAS] block_dim must be 1, 2 or 3");
+        }
+    }
+} // namespace pmas
