@@ -4,18 +4,21 @@
 // warp segmented sums plus FP64 atomics, multiplies every level's packed 96 x 96 inverse with one
 // 96-thread CTA each (symv_upper_packed, :665-705), and prolongs in a third kernel. Here:
 //
-//  * the level-0 restriction is fused into whichever kernel produced r (SpMV residual or the
-//    x/r update): per-bank sums of each connected component, deterministic;
-//  * k_coarse: one CTA per coarse matrix sums its components' level-0 sums (member lists) and
-//    multiplies with its inverse -> zc;
+//  * the level-0 restriction (per-bank sums of each connected component) is fused into the
+//    kernel that produced r (SpMV residual or the x/r update), deterministic;
+//  * k_coarse_sum: coarse level l sums from level l-1 (every level-l component merges at most 32
+//    level-(l-1) components of one bank), one warp per component, one launch per level;
+//  * k_coarse_symv: one CTA per coarse matrix (one warp per column tile), zc = A_l^-1 rc, and
+//    rc . zc for the PCG dot (identity inverses -- banks of isolated rows -- skip the multiply);
 //  * k_symv0: persistent warps stream the level-0 inverses through shared memory with
-//    cp.async.bulk (two stages per warp, mbarrier completion), multiply them with the bank's r,
-//    add the coarse corrections (prolongation), write z and reduce r . z; the last CTA then
-//    runs the PCG bookkeeping of the reference (convergence test, beta).
+//    cp.async.bulk (two stages per warp, mbarrier completion) and write z0 = A_0^-1 r with r . z0;
+//    the last CTA runs the PCG bookkeeping of the reference (rz = r . z0 + rc . zc, convergence,
+//    beta). The prolongation z = z0 + P zc is fused into the p update (update_p), since PCG uses z
+//    only there and in r . z = r . z0 + (P^T r) . zc.
 //
-// Inverses are stored tile-packed (see mas_internal.h): the same N (N + 1) / 2 values as packed
-// upper storage, laid out so a warp reads every 32 x 32 tile conflict-free and uses each value
-// for both y_I += T x_J and y_J += T^T x_I; the transposed sums are combined across lanes with a
+// Inverses are stored tile-packed (mas_internal.h): the same N (N + 1) / 2 values as packed upper
+// storage, laid out so a warp reads every 32 x 32 tile conflict-free and uses each value for both
+// y_I += T x_J and y_J += T^T x_I; the transposed sums are combined across lanes with a
 // 31-shuffle reduce-transpose per column tile.
 
 #include "mas_common.cuh"
@@ -56,74 +59,85 @@ namespace pmas
             return c[0];
         }
 
-        // y = M x for one tile-packed symmetric matrix M (N = 32 * T) in shared memory, x in shared
-        // memory. Lane l returns y[32 t + l] in yr[t].
+        // Column tile J of y = M x for one tile-packed symmetric matrix (shared memory): adds the
+        // row contributions of tiles (I, J), I <= J, to yr[I] and the transposed contributions
+        // (rows of tile J) to yr[J]. Lane l owns rows 32 t + l.
+        template <int T, class Real>
+        __device__ __forceinline__ void symv_column(const Real *__restrict__ M, const Real *__restrict__ xs, int lane,
+                                                    int J, Real (&yr)[T])
+        {
+            using V4 = typename Vec4<Real>::type;
+            int off = 0;
+#pragma unroll
+            for (int jj = 0; jj < T; ++jj)
+                if (jj < J)
+                    off += jj * 1024 + 528;
+            Real cy[32];
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+                cy[j] = Real(0);
+#pragma unroll
+            for (int I = 0; I < T; ++I)
+            {
+                if (I >= J)
+                    break;
+                const Real *tile = M + off + I * 1024;
+                const Real xI = xs[32 * I + lane];
+                Real a0 = 0, a1 = 0, a2 = 0, a3 = 0;
+#pragma unroll
+                for (int j4 = 0; j4 < 8; ++j4)
+                {
+                    const V4 v = *reinterpret_cast<const V4 *>(tile + j4 * 128 + lane * 4);
+                    const V4 xv = *reinterpret_cast<const V4 *>(xs + 32 * J + 4 * j4);
+                    a0 = fma(v.x, xv.x, a0);
+                    a1 = fma(v.y, xv.y, a1);
+                    a2 = fma(v.z, xv.z, a2);
+                    a3 = fma(v.w, xv.w, a3);
+                    cy[4 * j4 + 0] = fma(v.x, xI, cy[4 * j4 + 0]);
+                    cy[4 * j4 + 1] = fma(v.y, xI, cy[4 * j4 + 1]);
+                    cy[4 * j4 + 2] = fma(v.z, xI, cy[4 * j4 + 2]);
+                    cy[4 * j4 + 3] = fma(v.w, xI, cy[4 * j4 + 3]);
+                }
+                yr[I] += (a0 + a1) + (a2 + a3);
+            }
+            // Diagonal tile, upper triangle by columns.
+            const Real *dt = M + off + J * 1024;
+            const Real xJ = xs[32 * J + lane];
+            Real a0 = 0, a1 = 0;
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+            {
+                const Real v = (lane <= j) ? dt[j * (j + 1) / 2 + lane] : Real(0);
+                const Real xj = xs[32 * J + j];
+                if (j & 1)
+                    a1 = fma(v, xj, a1);
+                else
+                    a0 = fma(v, xj, a0);
+                cy[j] = fma((lane < j) ? v : Real(0), xJ, cy[j]);
+            }
+            yr[J] += (a0 + a1) + transpose_sum32<Real>(cy, lane);
+        }
+
+        // y = M x by one warp (all column tiles).
         template <int T, class Real>
         __device__ __forceinline__ void symv_tiles(const Real *__restrict__ M, const Real *__restrict__ xs, int lane,
                                                    Real (&yr)[T])
         {
-            using V4 = typename Vec4<Real>::type;
 #pragma unroll
             for (int t = 0; t < T; ++t)
                 yr[t] = Real(0);
-            int off = 0;
 #pragma unroll
             for (int J = 0; J < T; ++J)
-            {
-                Real cy[32];
-#pragma unroll
-                for (int j = 0; j < 32; ++j)
-                    cy[j] = Real(0);
-#pragma unroll
-                for (int I = 0; I < J; ++I)
-                {
-                    const Real *tile = M + off + I * 1024;
-                    const Real xI = xs[32 * I + lane];
-                    Real a0 = 0, a1 = 0, a2 = 0, a3 = 0;
-#pragma unroll
-                    for (int j4 = 0; j4 < 8; ++j4)
-                    {
-                        const V4 v = *reinterpret_cast<const V4 *>(tile + j4 * 128 + lane * 4);
-                        const V4 xv = *reinterpret_cast<const V4 *>(xs + 32 * J + 4 * j4);
-                        a0 = fma(v.x, xv.x, a0);
-                        a1 = fma(v.y, xv.y, a1);
-                        a2 = fma(v.z, xv.z, a2);
-                        a3 = fma(v.w, xv.w, a3);
-                        cy[4 * j4 + 0] = fma(v.x, xI, cy[4 * j4 + 0]);
-                        cy[4 * j4 + 1] = fma(v.y, xI, cy[4 * j4 + 1]);
-                        cy[4 * j4 + 2] = fma(v.z, xI, cy[4 * j4 + 2]);
-                        cy[4 * j4 + 3] = fma(v.w, xI, cy[4 * j4 + 3]);
-                    }
-                    yr[I] += (a0 + a1) + (a2 + a3);
-                }
-                off += J * 1024;
-                // Diagonal tile, upper triangle by columns.
-                {
-                    const Real *dt = M + off;
-                    const Real xJ = xs[32 * J + lane];
-                    Real a0 = 0, a1 = 0;
-#pragma unroll
-                    for (int j = 0; j < 32; ++j)
-                    {
-                        const Real v = (lane <= j) ? dt[j * (j + 1) / 2 + lane] : Real(0);
-                        const Real xj = xs[32 * J + j];
-                        if (j & 1)
-                            a1 = fma(v, xj, a1);
-                        else
-                            a0 = fma(v, xj, a0);
-                        cy[j] = fma((lane < j) ? v : Real(0), xJ, cy[j]);
-                    }
-                    yr[J] += a0 + a1;
-                    off += 528;
-                }
-                yr[J] += transpose_sum32<Real>(cy, lane);
-            }
+                symv_column<T, Real>(M, xs, lane, J, yr);
         }
 
         // Finish of an iteration (last CTA of k_symv0): the reference's per-iteration scalar work
         // and convergence test (MASSolver.cu:505, 526-583), on the device.
-        __device__ void pcg_finalize(PcgState *st, const PcgConfig &cfg, int iter, int mode, double rz, double rzcross)
+        __device__ void pcg_finalize(PcgState *st, const PcgConfig &cfg, int iter, int mode, double rz_fine,
+                                     double rzx_fine)
         {
+            const double rz = rz_fine + st->rz_coarse;
+            const double rzcross = rzx_fine + st->rzx_coarse;
             if (mode == 1)
             {
                 st->rz = rz;
@@ -169,7 +183,7 @@ namespace pmas
                 st->done = 1;
             else if (cfg.polak_ribiere)
             {
-                double beta = (fabs(rz_old) < 1e-20) ? 0.0 : (rz - rzcross) / rz_old;
+                const double beta = (fabs(rz_old) < 1e-20) ? 0.0 : (rz - rzcross) / rz_old;
                 st->beta = beta > 0.0 ? beta : 0.0;
             }
             else
@@ -189,7 +203,7 @@ namespace pmas
             static constexpr int STAGE_BYTES = S * (int)sizeof(Real);
             static constexpr int XS_BYTES = ((N * (int)sizeof(Real)) + 15) / 16 * 16;
             static constexpr int WARP_BYTES = 2 * STAGE_BYTES + XS_BYTES + 16;
-            static constexpr int SMEM_LIMIT = 232448;
+            static constexpr int SMEM_LIMIT = 232448 - 1024; // leave room for static shared memory
             static constexpr int W0 = SMEM_LIMIT / WARP_BYTES;
             static constexpr int WARPS = W0 > 16 ? 16 : W0;
             static_assert(STAGE_BYTES % 16 == 0, "bulk copies need 16-byte multiples");
@@ -198,7 +212,7 @@ namespace pmas
         // mode 0: plain apply; 1: initial PCG apply (rz0); 2: PCG iteration.
         template <int BD, class Real, int MODE>
         __global__ void __launch_bounds__(Symv0Layout<BD, Real>::WARPS * 32)
-            k_symv0(MasView mas, const double *__restrict__ r, double *__restrict__ z, PcgState *st, ReduceBuf red,
+            k_symv0(MasView mas, const double *__restrict__ r, double *__restrict__ z0, PcgState *st, ReduceBuf red,
                     PcgConfig cfg, int iter)
         {
             using L = Symv0Layout<BD, Real>;
@@ -213,11 +227,12 @@ namespace pmas
             Real *stage1 = reinterpret_cast<Real *>(base + L::STAGE_BYTES);
             Real *xs = reinterpret_cast<Real *>(base + 2 * L::STAGE_BYTES);
             uint64_t *bar = reinterpret_cast<uint64_t *>(base + 2 * L::STAGE_BYTES + L::XS_BYTES);
-            const Real *inv = static_cast<const Real *>(mas.inv);
+            const Real *__restrict__ inv = static_cast<const Real *>(mas.inv);
             const int banks = mas.banks;
             const int total_warps = gridDim.x * WARPS;
             const int gw = blockIdx.x * WARPS + w;
             int *errp = st ? &st->error : nullptr;
+            const bool pr = (MODE == 2) && cfg.polak_ribiere;
 
             if (lane == 0)
             {
@@ -235,8 +250,14 @@ namespace pmas
             }
             double part[2] = {0.0, 0.0};
             uint32_t phase0 = 0, phase1 = 0;
-            int k = 0;
             bool ok = true;
+            // r of the current bank, prefetched one bank ahead.
+            double r_next[BD];
+            if (gw < banks)
+#pragma unroll
+                for (int t = 0; t < BD; ++t)
+                    r_next[t] = r[(size_t)gw * N + t * 32 + lane];
+            int k = 0;
             for (int m = gw; m < banks; m += total_warps, ++k)
             {
                 const bool s1 = (k & 1) != 0;
@@ -246,9 +267,19 @@ namespace pmas
 #pragma unroll
                 for (int t = 0; t < BD; ++t)
                 {
-                    r64[t] = r[(size_t)m * N + t * 32 + lane];
+                    r64[t] = r_next[t];
                     xs[t * 32 + lane] = (Real)r64[t];
                 }
+                const int mnext = m + total_warps;
+                if (mnext < banks)
+#pragma unroll
+                    for (int t = 0; t < BD; ++t)
+                        r_next[t] = r[(size_t)mnext * N + t * 32 + lane];
+                double zold[BD];
+                if (pr)
+#pragma unroll
+                    for (int t = 0; t < BD; ++t)
+                        zold[t] = z0[(size_t)m * N + t * 32 + lane];
                 __syncwarp();
                 if (!mbar_wait_bounded(b, s1 ? phase1 : phase0, errp))
                 {
@@ -271,26 +302,12 @@ namespace pmas
 #pragma unroll
                 for (int t = 0; t < BD; ++t)
                 {
-                    const int row = t * 32 + lane;
-                    const long long node = (long long)m * 32 + row / BD;
-                    const int comp = row % BD;
-                    double zv = (double)yr[t];
-                    const int4 cs = mas.cslot[node];
-                    if (cs.x >= 0)
-                        zv += mas.zc[(size_t)cs.x * BD + comp];
-                    if (cs.y >= 0)
-                        zv += mas.zc[(size_t)cs.y * BD + comp];
-                    if (cs.z >= 0)
-                        zv += mas.zc[(size_t)cs.z * BD + comp];
-                    if (cs.w >= 0)
-                        zv += mas.zc[(size_t)cs.w * BD + comp];
-                    const size_t idx = (size_t)m * N + row;
-                    if (MODE == 2 && cfg.polak_ribiere)
-                        part[1] = fma(z[idx], r64[t], part[1]);
-                    z[idx] = zv;
+                    const double zv = (double)yr[t];
+                    z0[(size_t)m * N + t * 32 + lane] = zv;
                     part[0] = fma(zv, r64[t], part[0]);
+                    if (pr)
+                        part[1] = fma(zold[t], r64[t], part[1]);
                 }
-                __syncwarp();
             }
             if (!ok)
             {
@@ -310,114 +327,120 @@ namespace pmas
                 pcg_finalize(st, cfg, iter, MODE, tot[0], tot[1]);
         }
 
-        // One CTA per coarse matrix: gather the coarse residual of its 32 components from the
-        // level-0 component sums, multiply with the inverse, write zc.
-        template <int BD, class Real>
-        __global__ void __launch_bounds__(128) k_coarse(MasView mas, const PcgState *st)
+        // Coarse level l sums: rc[node] = sum of rc over its <= 32 children (previous level).
+        template <int BD>
+        __global__ void k_coarse_sum(MasView mas, int first_node, int count, const PcgState *st)
+        {
+            if (st && st->done)
+                return;
+            const int lane = threadIdx.x & 31;
+            const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+            if (i >= count)
+                return;
+            const int cn = first_node + i;
+            const int b = mas.child_ptr[cn], e = mas.child_ptr[cn + 1];
+            double s[BD];
+#pragma unroll
+            for (int c = 0; c < BD; ++c)
+                s[c] = 0.0;
+            if (b + lane < e)
+            {
+                const int ch = mas.children[b + lane];
+#pragma unroll
+                for (int c = 0; c < BD; ++c)
+                    s[c] = mas.rc[(size_t)ch * BD + c];
+            }
+#pragma unroll
+            for (int c = 0; c < BD; ++c)
+            {
+                const double v = warp_sum(s[c]);
+                if (lane == 0)
+                    mas.rc[(size_t)cn * BD + c] = v;
+            }
+        }
+
+        // One CTA (BD warps, one per column tile) per coarse matrix: zc = A^-1 rc on its 32 coarse
+        // nodes; in PCG modes rc . zc (and rc . zc_old) reduced into the state.
+        template <int BD, class Real, int PCG>
+        __global__ void __launch_bounds__(BD * 32) k_coarse_symv(MasView mas, PcgState *st, ReduceBuf red, int pr)
         {
             constexpr int N = 32 * BD, S = N * (N + 1) / 2;
-            if (st && st->done)
+            if (PCG && st->done)
                 return;
             extern __shared__ __align__(128) unsigned char smem[];
             Real *mat = reinterpret_cast<Real *>(smem);
             Real *xs = reinterpret_cast<Real *>(smem + ((size_t)S * sizeof(Real) + 15) / 16 * 16);
-            __shared__ double red[4][BD];
+            __shared__ Real ypart[BD][N];
             const int g = blockIdx.x;
             const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-            const int level0 = (g < mas.mat_counts[1]); // first coarse level uses the sums directly
-            const long long node0 = (long long)g * 32;
-
-            // Start the matrix load (global -> shared, 16-byte vectors).
-            const Real *src = static_cast<const Real *>(mas.inv) + (size_t)(mas.banks + g) * S;
+            const size_t v0 = (size_t)g * N; // first coarse value of this matrix
+            double part[2] = {0.0, 0.0};
+            double rcv[BD], zold[BD];
+#pragma unroll
+            for (int t = 0; t < BD; ++t)
+                zold[t] = 0.0;
+            if (w == 0)
             {
-                const int4 *s4 = reinterpret_cast<const int4 *>(src);
-                int4 *d4 = reinterpret_cast<int4 *>(mat);
-                const int n4 = S * (int)sizeof(Real) / 16;
-                for (int i = tid; i < n4; i += 128)
-                    d4[i] = s4[i];
+#pragma unroll
+                for (int t = 0; t < BD; ++t)
+                {
+                    rcv[t] = mas.rc[v0 + t * 32 + lane];
+                    if (PCG && pr)
+                        zold[t] = mas.zc[v0 + t * 32 + lane];
+                }
             }
-            if (level0)
+            if (mas.identity[g])
             {
-                for (int i = tid; i < N; i += 128)
-                    xs[i] = (Real)mas.rc[node0 * BD + i];
+                if (w == 0)
+#pragma unroll
+                    for (int t = 0; t < BD; ++t)
+                    {
+                        mas.zc[v0 + t * 32 + lane] = rcv[t];
+                        part[0] = fma(rcv[t], rcv[t], part[0]);
+                        part[1] = fma(rcv[t], zold[t], part[1]);
+                    }
             }
             else
             {
-                // Small components: one warp each; large ones: the whole CTA.
-                for (int i = w; i < 32; i += 4)
-                {
-                    const long long cn = node0 + i;
-                    const int b = mas.member_ptr[cn], e = mas.member_ptr[cn + 1];
-                    if (e - b > 256)
-                        continue;
-                    double s[BD];
-#pragma unroll
-                    for (int c = 0; c < BD; ++c)
-                        s[c] = 0.0;
-                    for (int q = b + lane; q < e; q += 32)
-                    {
-                        const int c0 = mas.members[q];
-#pragma unroll
-                        for (int c = 0; c < BD; ++c)
-                            s[c] += mas.rc[(size_t)c0 * BD + c];
-                    }
-#pragma unroll
-                    for (int c = 0; c < BD; ++c)
-                    {
-                        s[c] = warp_sum(s[c]);
-                        if (lane == 0)
-                        {
-                            xs[i * BD + c] = (Real)s[c];
-                            mas.rc[(size_t)cn * BD + c] = s[c];
-                        }
-                    }
-                }
-                for (int i = 0; i < 32; ++i)
-                {
-                    const long long cn = node0 + i;
-                    const int b = mas.member_ptr[cn], e = mas.member_ptr[cn + 1];
-                    if (e - b <= 256)
-                        continue;
-                    double s[BD];
-#pragma unroll
-                    for (int c = 0; c < BD; ++c)
-                        s[c] = 0.0;
-                    for (int q = b + tid; q < e; q += 128)
-                    {
-                        const int c0 = mas.members[q];
-#pragma unroll
-                        for (int c = 0; c < BD; ++c)
-                            s[c] += mas.rc[(size_t)c0 * BD + c];
-                    }
-#pragma unroll
-                    for (int c = 0; c < BD; ++c)
-                    {
-                        s[c] = warp_sum(s[c]);
-                        if (lane == 0)
-                            red[w][c] = s[c];
-                    }
-                    __syncthreads();
-                    if (tid == 0)
-                    {
-#pragma unroll
-                        for (int c = 0; c < BD; ++c)
-                        {
-                            const double t = (red[0][c] + red[1][c]) + (red[2][c] + red[3][c]);
-                            xs[i * BD + c] = (Real)t;
-                            mas.rc[(size_t)cn * BD + c] = t;
-                        }
-                    }
-                    __syncthreads();
-                }
-            }
-            __syncthreads();
-            if (w == 0)
-            {
+                const Real *src = static_cast<const Real *>(mas.inv) + (size_t)(mas.banks + g) * S;
+                const int4 *s4 = reinterpret_cast<const int4 *>(src);
+                int4 *d4 = reinterpret_cast<int4 *>(mat);
+                const int n4 = S * (int)sizeof(Real) / 16;
+                for (int i = tid; i < n4; i += BD * 32)
+                    d4[i] = s4[i];
+                for (int i = tid; i < N; i += BD * 32)
+                    xs[i] = (Real)mas.rc[v0 + i];
+                __syncthreads();
                 Real yr[BD];
-                symv_tiles<BD, Real>(mat, xs, lane, yr);
 #pragma unroll
                 for (int t = 0; t < BD; ++t)
-                    mas.zc[node0 * BD + t * 32 + lane] = (double)yr[t];
+                    yr[t] = Real(0);
+                symv_column<BD, Real>(mat, xs, lane, w, yr);
+#pragma unroll
+                for (int t = 0; t < BD; ++t)
+                    ypart[w][t * 32 + lane] = (t <= w) ? yr[t] : Real(0);
+                __syncthreads();
+                if (w == 0)
+#pragma unroll
+                    for (int t = 0; t < BD; ++t)
+                    {
+                        Real y = Real(0);
+#pragma unroll
+                        for (int J = 0; J < BD; ++J)
+                            y += ypart[J][t * 32 + lane];
+                        const double zv = (double)y;
+                        mas.zc[v0 + t * 32 + lane] = zv;
+                        part[0] = fma(rcv[t], zv, part[0]);
+                        part[1] = fma(rcv[t], zold[t], part[1]);
+                    }
+            }
+            if (!PCG)
+                return;
+            double tot[2];
+            if (grid_reduce<2, BD * 32>(part, red.partials, &st->counter[3], tot) && threadIdx.x == 0)
+            {
+                st->rz_coarse = tot[0];
+                st->rzx_coarse = tot[1];
             }
         }
 
@@ -438,23 +461,74 @@ namespace pmas
             warp_segment_store<BD>(rv, lcco0[u], cco0_base[bank], rc);
         }
 
+        template <int BD>
+        __global__ void k_prolong(MasView mas, const double *__restrict__ z0, double *__restrict__ z)
+        {
+            const long long len = (long long)mas.banks * 32 * BD;
+            for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len;
+                 i += (long long)gridDim.x * blockDim.x)
+            {
+                const long long node = i / BD;
+                const int comp = (int)(i % BD);
+                const int4 cs = mas.cslot[node];
+                double v = z0[i];
+                if (cs.x >= 0)
+                    v += mas.zc[(size_t)cs.x * BD + comp];
+                if (cs.y >= 0)
+                    v += mas.zc[(size_t)cs.y * BD + comp];
+                if (cs.z >= 0)
+                    v += mas.zc[(size_t)cs.z * BD + comp];
+                if (cs.w >= 0)
+                    v += mas.zc[(size_t)cs.w * BD + comp];
+                z[i] = v;
+            }
+        }
+
         template <int BD, class Real>
-        void coarse_launch(const MasView &mas, PcgState *st, cudaStream_t s)
+        int coarse_launch(const MasView &mas, PcgState *st, ReduceBuf red, int mode, int pr, cudaStream_t s)
         {
             if (mas.total_coarse == 0)
-                return;
+            {
+                if (mode != 0)
+                    cuda_check(cudaMemsetAsync(&st->rz_coarse, 0, 2 * sizeof(double), s), "memset");
+                return 0;
+            }
+            int launches = 0;
+            for (int l = 1; l < mas.level_num; ++l)
+            {
+                const int count = mas.cco_nums[l];
+                if (count <= 0)
+                    continue;
+                k_coarse_sum<BD><<<(count + 7) / 8, 256, 0, s>>>(mas, mas.coff[l], count, mode ? st : nullptr);
+                ++launches;
+            }
             constexpr int N = 32 * BD, S = N * (N + 1) / 2;
             const size_t smem = ((size_t)S * sizeof(Real) + 15) / 16 * 16 + N * sizeof(Real);
-            static bool configured = false;
-            if (!configured)
+            static bool configured[2] = {false, false};
+            const int pcg = mode != 0 ? 1 : 0;
+            if (!configured[pcg])
             {
-                cuda_check(cudaFuncSetAttribute(k_coarse<BD, Real>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                (int)smem),
-                           "coarse smem attribute");
-                configured = true;
+                if (pcg)
+                    cuda_check(cudaFuncSetAttribute(k_coarse_symv<BD, Real, 1>,
+                                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                               "coarse smem attribute");
+                else
+                    cuda_check(cudaFuncSetAttribute(k_coarse_symv<BD, Real, 0>,
+                                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
+                               "coarse smem attribute");
+                configured[pcg] = true;
             }
-            k_coarse<BD, Real><<<mas.total_coarse, 128, smem, s>>>(mas, st);
+            if (pcg)
+            {
+                if (mas.total_coarse > red.capacity)
+                    throw Error(ERR_INVALID, "[MAS] reduction scratch too small");
+                k_coarse_symv<BD, Real, 1><<<mas.total_coarse, BD * 32, smem, s>>>(mas, st, red, pr);
+            }
+            else
+                k_coarse_symv<BD, Real, 0><<<mas.total_coarse, BD * 32, smem, s>>>(mas, st, red, 0);
+            ++launches;
             cuda_check(cudaGetLastError(), "coarse launch");
+            return launches;
         }
 
         template <int BD, class Real, int MODE>
@@ -463,18 +537,18 @@ namespace pmas
         {
             using L = Symv0Layout<BD, Real>;
             static bool configured = false;
+            static int sms = 0;
             const size_t smem = (size_t)L::WARPS * L::WARP_BYTES;
             if (!configured)
             {
                 cuda_check(cudaFuncSetAttribute(k_symv0<BD, Real, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                 (int)smem),
                            "symv0 smem attribute");
+                int dev = 0;
+                cudaGetDevice(&dev);
+                cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
                 configured = true;
             }
-            int sms = 148;
-            int dev = 0;
-            cudaGetDevice(&dev);
-            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
             int grid = (mas.banks + L::WARPS - 1) / L::WARPS;
             if (grid > sms)
                 grid = sms;
@@ -499,26 +573,21 @@ namespace pmas
         }
     } // namespace
 
-    void launch_coarse(const MasView &mas, PcgState *st, cudaStream_t s)
+    int launch_coarse(const MasView &mas, PcgState *st, ReduceBuf red, int mode, int pr, cudaStream_t s)
     {
         if (mas.fp32)
         {
             if (mas.bd == 1)
-                coarse_launch<1, float>(mas, st, s);
-            else if (mas.bd == 2)
-                coarse_launch<2, float>(mas, st, s);
-            else
-                coarse_launch<3, float>(mas, st, s);
+                return coarse_launch<1, float>(mas, st, red, mode, pr, s);
+            if (mas.bd == 2)
+                return coarse_launch<2, float>(mas, st, red, mode, pr, s);
+            return coarse_launch<3, float>(mas, st, red, mode, pr, s);
         }
-        else
-        {
-            if (mas.bd == 1)
-                coarse_launch<1, double>(mas, st, s);
-            else if (mas.bd == 2)
-                coarse_launch<2, double>(mas, st, s);
-            else
-                coarse_launch<3, double>(mas, st, s);
-        }
+        if (mas.bd == 1)
+            return coarse_launch<1, double>(mas, st, red, mode, pr, s);
+        if (mas.bd == 2)
+            return coarse_launch<2, double>(mas, st, red, mode, pr, s);
+        return coarse_launch<3, double>(mas, st, red, mode, pr, s);
     }
 
     void launch_symv0(const MasView &mas, const double *r, double *z, PcgState *st, ReduceBuf red, PcgConfig cfg,
@@ -556,5 +625,22 @@ namespace pmas
         else
             k_restrict<3><<<grid, 256, 0, s>>>(A.banks, r, mas.lcco0, mas.cco0_base, mas.rc);
         cuda_check(cudaGetLastError(), "restrict launch");
+    }
+
+    void launch_prolong(const MasView &mas, const double *z0, double *z, cudaStream_t s)
+    {
+        const long long len = (long long)mas.banks * 32 * mas.bd;
+        long long g = (len + 255) / 256;
+        if (g > 148 * 16)
+            g = 148 * 16;
+        if (g < 1)
+            g = 1;
+        if (mas.bd == 1)
+            k_prolong<1><<<(int)g, 256, 0, s>>>(mas, z0, z);
+        else if (mas.bd == 2)
+            k_prolong<2><<<(int)g, 256, 0, s>>>(mas, z0, z);
+        else
+            k_prolong<3><<<(int)g, 256, 0, s>>>(mas, z0, z);
+        cuda_check(cudaGetLastError(), "prolong launch");
     }
 } // namespace pmas

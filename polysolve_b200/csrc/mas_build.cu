@@ -33,17 +33,20 @@ namespace pmas
         {
             v.mat_offsets[i] = mat_offsets[i];
             v.mat_counts[i] = mat_counts[i];
-            v.coarse_level_of[i] = 0;
         }
         for (int i = 0; i < MAX_COARSE; ++i)
+        {
             v.cco_nums[i] = cco_nums[i];
+            v.coff[i] = coff[i];
+        }
         v.fp32 = fp32;
         v.inv = fp32 ? (const void *)inv32.get() : (const void *)inv64.get();
         v.lcco0 = lcco0.get();
         v.cco0_base = cco0_base.get();
         v.cslot = cslot.get();
-        v.member_ptr = member_ptr.get();
-        v.members = members.get();
+        v.child_ptr = child_ptr.get();
+        v.children = children.get();
+        v.identity = identity.get();
         v.rc = rc_override ? rc_override : rc.get();
         v.zc = zc.get();
         return v;
@@ -387,6 +390,45 @@ namespace pmas
             cslot[u] = make_int4(v[0], v[1], v[2], v[3]);
         }
 
+        // flag[g] = 1 if coarse inverse g is exactly the identity (a bank of isolated rows).
+        template <int BD, class Real>
+        __global__ void k_identity_flags(const Real *__restrict__ inv, int first, int count, int *flag)
+        {
+            constexpr int N = 32 * BD, S = N * (N + 1) / 2;
+            const int g = blockIdx.x;
+            if (g >= count)
+                return;
+            const Real *m = inv + (size_t)(first + g) * S;
+            __shared__ int is_id;
+            if (threadIdx.x == 0)
+                is_id = 1;
+            __syncthreads();
+            for (int idx = threadIdx.x; idx < S; idx += blockDim.x)
+            {
+                int rem = idx, J = 0;
+                while (rem >= J * 1024 + 528)
+                {
+                    rem -= J * 1024 + 528;
+                    ++J;
+                }
+                bool diag = false;
+                if (rem >= J * 1024)
+                {
+                    const int e = rem - J * 1024;
+                    int j = 0;
+                    while ((j + 1) * (j + 2) / 2 <= e)
+                        ++j;
+                    diag = (e - j * (j + 1) / 2) == j;
+                }
+                const Real want = diag ? Real(1) : Real(0);
+                if (m[idx] != want)
+                    is_id = 0;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0)
+                flag[g] = is_id;
+        }
+
         int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
 
         template <class T>
@@ -525,40 +567,41 @@ namespace pmas
                                                   M.cslot.get());
         cuda_check(cudaGetLastError(), "cslot launch");
 
-        // Member lists (level-0 components of each coarse node of levels >= 1), built on the host.
+        // Child lists: for each coarse node of level l >= 1, the (<= 32) level l-1 coarse nodes it
+        // merges, in increasing order; built on the host from the maps.
+        for (int l = 0; l < MAX_COARSE; ++l)
+            M.coff[l] = coff[l];
         {
             std::vector<int> hmap((size_t)nodes * 4);
             cuda_check(cudaMemcpy(hmap.data(), M.map.get(), hmap.size() * sizeof(int), cudaMemcpyDeviceToHost), "map");
-            const int C0 = M.cco_nums[0];
-            std::vector<int> up((size_t)C0 * 4, -1);
+            std::vector<int> parent((size_t)cn, -1); // coarse node -> next-level coarse node
             for (int u = 0; u < nodes; ++u)
-            {
-                const int c0 = hmap[(size_t)u * 4];
-                if (c0 < 0)
-                    continue;
                 for (int l = 1; l < M.level_num; ++l)
-                    up[(size_t)c0 * 4 + l] = hmap[(size_t)u * 4 + l];
-            }
+                {
+                    const int c = hmap[(size_t)u * 4 + l - 1], up = hmap[(size_t)u * 4 + l];
+                    if (c >= 0 && up >= 0)
+                        parent[(size_t)coff[l - 1] + c] = coff[l] + up;
+                }
             std::vector<int> ptr((size_t)cn + 1, 0);
-            for (int c0 = 0; c0 < C0; ++c0)
-                for (int l = 1; l < M.level_num; ++l)
-                    ptr[(size_t)coff[l] + up[(size_t)c0 * 4 + l] + 1]++;
+            for (int c = 0; c < cn; ++c)
+                if (parent[c] >= 0)
+                    ptr[(size_t)parent[c] + 1]++;
             for (int i = 0; i < cn; ++i)
                 ptr[i + 1] += ptr[i];
             std::vector<int> fillp(ptr.begin(), ptr.end() - 1);
-            std::vector<int> mem(ptr[cn] > 0 ? ptr[cn] : 1);
-            for (int c0 = 0; c0 < C0; ++c0)
-                for (int l = 1; l < M.level_num; ++l)
-                {
-                    const int node = coff[l] + up[(size_t)c0 * 4 + l];
-                    mem[fillp[node]++] = c0;
-                }
-            M.member_ptr.alloc(cn + 1, "MAS coarse_space members");
-            M.members.alloc(mem.size(), "MAS coarse_space members");
-            cuda_check(cudaMemcpy(M.member_ptr.get(), ptr.data(), ptr.size() * sizeof(int), cudaMemcpyHostToDevice),
-                       "members");
-            cuda_check(cudaMemcpy(M.members.get(), mem.data(), mem.size() * sizeof(int), cudaMemcpyHostToDevice),
-                       "members");
+            std::vector<int> ch(ptr[cn] > 0 ? ptr[cn] : 1);
+            for (int c = 0; c < cn; ++c)
+                if (parent[c] >= 0)
+                    ch[fillp[parent[c]]++] = c;
+            for (int i = 0; i < cn; ++i)
+                if (ptr[i + 1] - ptr[i] > 32)
+                    throw Error(ERR_INVALID, "[MAS] internal: coarse component with more than 32 children");
+            M.child_ptr.alloc(cn + 1, "MAS coarse_space children");
+            M.children.alloc(ch.size(), "MAS coarse_space children");
+            cuda_check(cudaMemcpy(M.child_ptr.get(), ptr.data(), ptr.size() * sizeof(int), cudaMemcpyHostToDevice),
+                       "children");
+            cuda_check(cudaMemcpy(M.children.get(), ch.data(), ch.size() * sizeof(int), cudaMemcpyHostToDevice),
+                       "children");
         }
 
         // Coarse vectors (zero once: slots past the component counts stay zero).
@@ -599,6 +642,30 @@ namespace pmas
             else
                 assemble_and_invert<3, double>(M, A, d_node_real, M.inv64.get(), coff, s);
             break;
+        }
+        M.identity.alloc(M.total_coarse > 0 ? M.total_coarse : 1, "MAS coarse_matrices identity");
+        cuda_check(cudaMemsetAsync(M.identity.get(), 0, M.identity.bytes(), s), "memset");
+        if (M.total_coarse > 0)
+        {
+            if (fp32)
+            {
+                if (bd == 1)
+                    k_identity_flags<1, float><<<M.total_coarse, 256, 0, s>>>(M.inv32.get(), banks, M.total_coarse, M.identity.get());
+                else if (bd == 2)
+                    k_identity_flags<2, float><<<M.total_coarse, 256, 0, s>>>(M.inv32.get(), banks, M.total_coarse, M.identity.get());
+                else
+                    k_identity_flags<3, float><<<M.total_coarse, 256, 0, s>>>(M.inv32.get(), banks, M.total_coarse, M.identity.get());
+            }
+            else
+            {
+                if (bd == 1)
+                    k_identity_flags<1, double><<<M.total_coarse, 256, 0, s>>>(M.inv64.get(), banks, M.total_coarse, M.identity.get());
+                else if (bd == 2)
+                    k_identity_flags<2, double><<<M.total_coarse, 256, 0, s>>>(M.inv64.get(), banks, M.total_coarse, M.identity.get());
+                else
+                    k_identity_flags<3, double><<<M.total_coarse, 256, 0, s>>>(M.inv64.get(), banks, M.total_coarse, M.identity.get());
+            }
+            cuda_check(cudaGetLastError(), "identity flags launch");
         }
         int h_flag = 0;
         cuda_check(cudaMemcpyAsync(&h_flag, M.flag.get(), sizeof(int), cudaMemcpyDeviceToHost, s), "flag");

@@ -12,11 +12,13 @@
 
 #include "polysolve_mas.h"
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -265,22 +267,29 @@ struct mas_solver
 
     // Launch through here: counts kernels (`kernels` per call) and, when profiling, brackets the
     // launch with events on the launching stream.
+    // f returns the number of kernels it launched (or void: `kernels`).
     template <class F>
     void run(const char *kind, int kernels, F &&f)
     {
         const int idx = stat_index(kind);
+        cudaEvent_t a = nullptr, b = nullptr;
+        if (p.profile)
+        {
+            a = pool_event();
+            b = pool_event();
+            cuda_check(cudaEventRecord(a, stream), "event");
+        }
+        if constexpr (std::is_same_v<decltype(f()), int>)
+            kernels = f();
+        else
+            f();
         kstats[idx].second.launches += kernels;
         total_launches += kernels;
         if (p.profile)
         {
-            cudaEvent_t a = pool_event(), b = pool_event();
-            cuda_check(cudaEventRecord(a, stream), "event");
-            f();
             cuda_check(cudaEventRecord(b, stream), "event");
             ev_pending.push_back({idx, {a, b}});
         }
-        else
-            f();
     }
 
     void collect_profile()
@@ -402,7 +411,7 @@ struct mas_solver
         Ap.alloc(len, "device_buffers Ap");
         io.alloc((size_t)n_ > len ? (size_t)n_ : len, "device_buffers io");
         st.alloc(1, "device_buffers scalars");
-        red_capacity = (banks + 7) / 8 + 160;
+        red_capacity = std::max((banks + 7) / 8, mas.total_coarse) + 160;
         partials.alloc((size_t)red_capacity * 2, "device_buffers reduction");
         cuda_check(cudaMemsetAsync(x.get(), 0, x.bytes(), stream), "memset");
         cuda_check(cudaMemsetAsync(pv.get(), 0, pv.bytes(), stream), "memset");
@@ -445,13 +454,15 @@ struct mas_solver
         cuda_check(cudaEventCreate(&e0), "event");
         cuda_check(cudaEventCreate(&e1), "event");
         cuda_check(cudaEventRecord(e0, stream), "event");
+        for (auto &ks : kstats) // per-solve kernel statistics
+            ks.second = KStat{};
         launch_pcg_init_state(S, stream);
-        const int coarse_k = mas.total_coarse > 0 ? 1 : 0;
+        const int pr = p.polak_ribiere ? 1 : 0;
         // r = b - A x, its level-0 restriction and rr0
         run("spmv_residual", 1, [&] { launch_spmv(SPMV_RESIDUAL, Av, x.get(), r.get(), b.get(), &mv, S, red(), 0, stream); });
-        run("mas_coarse", coarse_k, [&] { launch_coarse(mv, S, stream); });
+        run("mas_coarse", 0, [&] { return launch_coarse(mv, S, red(), 1, pr, stream); });
         run("mas_symv0", 1, [&] { launch_symv0(mv, r.get(), z.get(), S, red(), cfg, 0, 1, stream); });
-        run("update_p", 1, [&] { launch_update_p(nodes, bd, pv.get(), z.get(), S, 1, stream); });
+        run("update_p", 1, [&] { launch_update_p(mv, pv.get(), z.get(), S, 1, stream); });
         cuda_check(cudaMemcpyAsync(&h_st[0], S, sizeof(PcgState), cudaMemcpyDeviceToHost, stream), "state");
         cuda_check(cudaStreamSynchronize(stream), "pcg init");
         rz0 = h_st[0].rz0;
@@ -484,9 +495,9 @@ struct mas_solver
                 }
                 else
                     run("update_xr", 1, [&] { launch_update_xr(Av, mv, x.get(), r.get(), pv.get(), Ap.get(), S, red(), stream); });
-                run("mas_coarse", coarse_k, [&] { launch_coarse(mv, S, stream); });
+                run("mas_coarse", 0, [&] { return launch_coarse(mv, S, red(), 2, pr, stream); });
                 run("mas_symv0", 1, [&] { launch_symv0(mv, r.get(), z.get(), S, red(), cfg, k, 2, stream); });
-                run("update_p", 1, [&] { launch_update_p(nodes, bd, pv.get(), z.get(), S, 0, stream); });
+                run("update_p", 1, [&] { launch_update_p(mv, pv.get(), z.get(), S, 0, stream); });
             }
             launched = k1;
             const int slot = (k0 / chunk) & 1;
@@ -957,9 +968,10 @@ extern "C" int mas_debug_apply(mas_solver *h, const double *rin, double *zout, i
         cuda_check(cudaMemcpyAsync(h->r.get(), rin, sizeof(double) * len, cudaMemcpyHostToDevice, h->stream), "r");
         const MasView mv = h->mas.view();
         launch_restrict_plain(h->A.view(), mv, h->r.get(), h->stream);
-        launch_coarse(mv, nullptr, h->stream);
+        launch_coarse(mv, nullptr, h->red(), 0, 0, h->stream);
         launch_symv0(mv, h->r.get(), h->z.get(), nullptr, h->red(), h->config(), 0, 0, h->stream);
-        cuda_check(cudaMemcpyAsync(zout, h->z.get(), sizeof(double) * len, cudaMemcpyDeviceToHost, h->stream), "z");
+        launch_prolong(mv, h->z.get(), h->Ap.get(), h->stream);
+        cuda_check(cudaMemcpyAsync(zout, h->Ap.get(), sizeof(double) * len, cudaMemcpyDeviceToHost, h->stream), "z");
         cuda_check(cudaStreamSynchronize(h->stream), "apply");
     });
 }

@@ -166,7 +166,7 @@ namespace pmas
 
     // Wait for phase `parity` of the barrier with an iteration limit. On timeout records
     // ERR_TIMEOUT in *err and returns false.
-    constexpr long long MBAR_SPIN_LIMIT = 1LL << 24;
+    constexpr long long MBAR_SPIN_LIMIT = 1LL << 20;
 
     __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *err)
     {

@@ -137,7 +137,7 @@ namespace pmas
         int banks;              // level-0 matrices
         int level_num;          // coarse levels in use (0..4)
         int total_coarse;       // coarse matrices (all levels >= 1)
-        int coarse_level_of[LEVELS];  // not used on device
+        int coff[MAX_COARSE];   // first coarse node of each coarse level
         int mat_offsets[LEVELS];      // first matrix of each matrix level (0 = banks)
         int mat_counts[LEVELS];
         int cco_nums[MAX_COARSE];
@@ -146,8 +146,9 @@ namespace pmas
         const int *lcco0;       // nodes: bank-local level-0 component id, -1 virtual
         const int *cco0_base;   // banks: first global level-0 component id of the bank
         const int4 *cslot;      // nodes: coarse-vector node of each coarse level (-1 unused)
-        const int *member_ptr;  // coarse nodes + 1: CSR of level-0 components per coarse node
-        const int *members;
+        const int *child_ptr;   // coarse nodes + 1: CSR of the (<= 32) previous-level coarse nodes
+        const int *children;    //   merged into each coarse node of levels >= 1
+        const int *identity;    // coarse matrices: 1 if the inverse is exactly the identity
         double *rc;             // coarse residual, coarse nodes * bd (level-0 components first)
         double *zc;             // coarse correction, coarse nodes * bd
     };
@@ -156,6 +157,7 @@ namespace pmas
     struct PcgState
     {
         double rz, rz_old, pAp, alpha, beta, rr, rr0, rz0, res_norm, rzold_cross;
+        double rz_coarse, rzx_coarse; // rc . zc and rc . zc_old of the coarse levels
         int iter;      // last finished iteration
         int done;      // 1: converged / stopped; kernels return immediately
         int status;    // MAS_STATUS_*
@@ -222,19 +224,25 @@ namespace pmas
     void launch_update_xr(const BankedView &A, const MasView &mas, double *x, double *r, const double *p,
                           const double *Ap, PcgState *st, ReduceBuf red, cudaStream_t s);
     void launch_update_x(int nodes, int bd, double *x, const double *p, PcgState *st, cudaStream_t s);
-    void launch_update_p(int nodes, int bd, double *p, const double *z, PcgState *st, int first, cudaStream_t s);
+    // p = z0 + prolongation(zc) + beta p (z0: level-0 part of z = M^-1 r)
+    void launch_update_p(const MasView &mas, double *p, const double *z0, PcgState *st, int first, cudaStream_t s);
     void launch_permute_in(int n, int bd, int V, const int *padded_of_block, const double *src, double *dst,
                            size_t dst_len, cudaStream_t s);
     void launch_permute_out(int n, int bd, int V, const int *padded_of_block, const double *src, double *dst,
                             cudaStream_t s);
     void launch_pcg_init_state(PcgState *st, cudaStream_t s);
 
-    // mas_apply.cu
-    void launch_coarse(const MasView &mas, PcgState *st, cudaStream_t s);
-    void launch_symv0(const MasView &mas, const double *r, double *z, PcgState *st, ReduceBuf red, PcgConfig cfg,
+    // mas_apply.cu. mode: 0 = plain apply (no PCG bookkeeping), 1 = initial (rz0), 2 = iteration.
+    // Coarse levels: hierarchical sums of the level-0 component sums, then every coarse matrix
+    // times its residual (zc) and, in PCG modes, rc . zc (and rc . zc_old) into the state.
+    int launch_coarse(const MasView &mas, PcgState *st, ReduceBuf red, int mode, int polak_ribiere, cudaStream_t s);
+    // Level-0 subdomains: z0 = A_0^-1 r per bank; in PCG modes r . z0 and the iteration's
+    // bookkeeping (rz = r . z0 + rc . zc, convergence test, beta) in the last CTA.
+    void launch_symv0(const MasView &mas, const double *r, double *z0, PcgState *st, ReduceBuf red, PcgConfig cfg,
                       int iter, int mode, cudaStream_t s);
-    // mode for launch_symv0: 0 = plain apply (no PCG bookkeeping), 1 = initial (rz0), 2 = iteration
     void launch_restrict_plain(const BankedView &A, const MasView &mas, const double *r, cudaStream_t s);
+    // z = z0 + prolongation(zc) (outside the PCG loop).
+    void launch_prolong(const MasView &mas, const double *z0, double *z, cudaStream_t s);
 
     // mas_build.cu: the MAS hierarchy and inverses.
     struct MasDevice
@@ -252,7 +260,8 @@ namespace pmas
         DevBuf<int> lcco0;
         DevBuf<int> cco0_base;
         DevBuf<int4> cslot;
-        DevBuf<int> member_ptr, members;
+        DevBuf<int> child_ptr, children, identity;
+        int coff[MAX_COARSE] = {0, 0, 0, 0};
         DevBuf<float> inv32;
         DevBuf<double> inv64;
         DevBuf<double> rc, zc;

@@ -4,7 +4,8 @@
 // MASSolver.cu:46-81, InnerProduct.cu:16-45) with a memset and an FP64 atomicAdd per dot. Here:
 //   update_xr: x += alpha p ; r -= alpha Ap ; rr = r . r ; level-0 restriction of r   (one pass)
 //   update_x:  x += alpha p                       (true-residual steps; r = b - A x follows)
-//   update_p:  p = z + beta p                     (beta computed on the device by the MAS apply)
+//   update_p:  p = z0 + P zc + beta p             (the MAS prolongation fused in; beta from the
+//                                                  device state, set by the MAS apply)
 // alpha / beta are read from the device-resident PcgState, and every dot is a deterministic
 // two-stage reduction, so no host round trip is needed inside the iteration.
 
@@ -49,6 +50,9 @@ namespace pmas
     {
         constexpr int UPD_THREADS = 256;
 
+        // One warp per bank: the bank's 32 * BD contiguous values are read and written with
+        // coalesced accesses (value e = t * 32 + lane); the node view for the level-0 restriction
+        // goes through shared memory.
         template <int BD>
         __global__ void __launch_bounds__(UPD_THREADS) k_update_xr(int banks, double *__restrict__ x, double *__restrict__ r,
                                                                    const double *__restrict__ p,
@@ -57,30 +61,72 @@ namespace pmas
                                                                    const int *__restrict__ cco0_base, double *rc,
                                                                    PcgState *st, ReduceBuf red)
         {
+            __shared__ double sv[UPD_THREADS / 32][32 * BD];
             if (st->done)
                 return;
             const double alpha = st->alpha;
-            const int lane = threadIdx.x & 31;
-            const int bank = blockIdx.x * (UPD_THREADS / 32) + (threadIdx.x >> 5);
+            const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+            const int bank = blockIdx.x * (UPD_THREADS / 32) + w;
             double part = 0.0;
             if (bank < banks)
             {
-                const long long u = (long long)bank * 32 + lane;
-                double rv[BD];
+                const long long b0 = (long long)bank * 32 * BD;
+#pragma unroll
+                for (int t = 0; t < BD; ++t)
+                {
+                    const long long idx = b0 + t * 32 + lane;
+                    const double xv = fma(alpha, p[idx], x[idx]);
+                    const double rv = fma(-alpha, Ap[idx], r[idx]);
+                    x[idx] = xv;
+                    r[idx] = rv;
+                    part = fma(rv, rv, part);
+                    sv[w][t * 32 + lane] = rv;
+                }
+                __syncwarp();
+                double rn[BD];
 #pragma unroll
                 for (int i = 0; i < BD; ++i)
-                {
-                    const long long idx = u * BD + i;
-                    x[idx] = fma(alpha, p[idx], x[idx]);
-                    rv[i] = fma(-alpha, Ap[idx], r[idx]);
-                    r[idx] = rv[i];
-                    part = fma(rv[i], rv[i], part);
-                }
-                warp_segment_store<BD>(rv, lcco0[u], cco0_base[bank], rc);
+                    rn[i] = sv[w][lane * BD + i];
+                warp_segment_store<BD>(rn, lcco0[(long long)bank * 32 + lane], cco0_base[bank], rc);
             }
             double v1[1] = {part}, tot[1];
             if (grid_reduce<1, UPD_THREADS>(v1, red.partials, &st->counter[1], tot) && threadIdx.x == 0)
                 st->rr = tot[0];
+        }
+
+        // p = z0 + sum_l zc[cslot_l(node)] + beta p, one warp per bank, coalesced.
+        template <int BD>
+        __global__ void __launch_bounds__(UPD_THREADS) k_update_p(MasView mas, double *__restrict__ p,
+                                                                  const double *__restrict__ z0, const PcgState *st,
+                                                                  int first)
+        {
+            if (st->done)
+                return;
+            const double beta = first ? 0.0 : st->beta;
+            const int lane = threadIdx.x & 31;
+            const int bank = blockIdx.x * (UPD_THREADS / 32) + (threadIdx.x >> 5);
+            if (bank >= mas.banks)
+                return;
+            const long long b0 = (long long)bank * 32 * BD;
+            const double *__restrict__ zc = mas.zc;
+#pragma unroll
+            for (int t = 0; t < BD; ++t)
+            {
+                const int e = t * 32 + lane;
+                const int node = e / BD, comp = e - node * BD;
+                const int4 cs = mas.cslot[(long long)bank * 32 + node];
+                const long long idx = b0 + e;
+                double v = z0[idx];
+                if (cs.x >= 0)
+                    v += zc[(size_t)cs.x * BD + comp];
+                if (cs.y >= 0)
+                    v += zc[(size_t)cs.y * BD + comp];
+                if (cs.z >= 0)
+                    v += zc[(size_t)cs.z * BD + comp];
+                if (cs.w >= 0)
+                    v += zc[(size_t)cs.w * BD + comp];
+                p[idx] = first ? v : fma(beta, p[idx], v);
+            }
         }
 
         __global__ void k_update_x(long long len, double *__restrict__ x, const double *__restrict__ p,
@@ -92,24 +138,6 @@ namespace pmas
             for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len;
                  i += (long long)gridDim.x * blockDim.x)
                 x[i] = fma(alpha, p[i], x[i]);
-        }
-
-        __global__ void k_update_p(long long len, double *__restrict__ p, const double *__restrict__ z,
-                                   const PcgState *st, int first)
-        {
-            if (st->done)
-                return;
-            const double beta = first ? 0.0 : st->beta;
-            if (first)
-            {
-                for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len;
-                     i += (long long)gridDim.x * blockDim.x)
-                    p[i] = z[i];
-                return;
-            }
-            for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len;
-                 i += (long long)gridDim.x * blockDim.x)
-                p[i] = fma(beta, p[i], z[i]);
         }
 
         // dst (padded, node-major, zero elsewhere) <- src (caller's order, length n)
@@ -180,10 +208,23 @@ namespace pmas
         cuda_check(cudaGetLastError(), "update_x launch");
     }
 
-    void launch_update_p(int nodes, int bd, double *p, const double *z, PcgState *st, int first, cudaStream_t s)
+    void launch_update_p(const MasView &mas, double *p, const double *z0, PcgState *st, int first, cudaStream_t s)
     {
-        const long long len = (long long)nodes * bd;
-        k_update_p<<<grid_for(len), 256, 0, s>>>(len, p, z, st, first);
+        const int grid = (mas.banks + UPD_THREADS / 32 - 1) / (UPD_THREADS / 32);
+        if (grid == 0)
+            return;
+        switch (mas.bd)
+        {
+        case 1:
+            k_update_p<1><<<grid, UPD_THREADS, 0, s>>>(mas, p, z0, st, first);
+            break;
+        case 2:
+            k_update_p<2><<<grid, UPD_THREADS, 0, s>>>(mas, p, z0, st, first);
+            break;
+        default:
+            k_update_p<3><<<grid, UPD_THREADS, 0, s>>>(mas, p, z0, st, first);
+            break;
+        }
         cuda_check(cudaGetLastError(), "update_p launch");
     }
 
