@@ -402,15 +402,26 @@ namespace pmas
             }
             else
             {
+                // One bulk copy (cp.async.bulk) for the whole matrix, completing on an mbarrier.
+                __shared__ __align__(8) uint64_t bar;
                 const Real *src = static_cast<const Real *>(mas.inv) + (size_t)(mas.banks + g) * S;
-                const int4 *s4 = reinterpret_cast<const int4 *>(src);
-                int4 *d4 = reinterpret_cast<int4 *>(mat);
-                const int n4 = S * (int)sizeof(Real) / 16;
-                for (int i = tid; i < n4; i += BD * 32)
-                    d4[i] = s4[i];
+                if (tid == 0)
+                {
+                    mbar_init(&bar, 1);
+                    fence_mbar_init();
+                    bulk_load(mat, src, (uint32_t)(S * sizeof(Real)), &bar);
+                }
                 for (int i = tid; i < N; i += BD * 32)
                     xs[i] = (Real)mas.rc[v0 + i];
                 __syncthreads();
+                if (!mbar_wait_bounded(&bar, 0, PCG ? &st->error : nullptr))
+                {
+                    // Bounded second wait so the copy is not left writing shared memory, then give
+                    // up on this matrix (the host reports ERR_TIMEOUT).
+                    for (long long i = 0; i < MBAR_SPIN_LIMIT && !mbar_try_wait(&bar, 0); ++i)
+                    {
+                    }
+                }
                 Real yr[BD];
 #pragma unroll
                 for (int t = 0; t < BD; ++t)

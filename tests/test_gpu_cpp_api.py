@@ -24,7 +24,8 @@ def write_market(path, A) -> None:
 
 def test_cpp_api_all_and_pre_factor(tmp_path):
     exe = _build.build_cpp_test()
-    A = synthetic.elasticity(5, young_sigma=0.5, seed=13).scipy()
+    # scaled so the reference's absolute alpha guard (|p.Ap| < 1e-20) does not stall at abs 1e-8
+    A = (synthetic.elasticity(5, young_sigma=0.5, seed=13).scipy() * 1e-3).tocsc()
     path = tmp_path / "A.mtx"
     write_market(path, A)
     res = subprocess.run([str(exe), str(path)], stdout=subprocess.PIPE, stderr=subprocess.STDOUT, text=True,

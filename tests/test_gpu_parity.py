@@ -152,22 +152,23 @@ def test_pcg_chosen_mode(case):
 
 
 def test_reference_all_style():
-    """Reference TEST_CASE("all") (test_linear_solver.cpp:103-164): rel 0, abs 1e-8, ||Ax-b|| < 1e-8.
-    The reference's stopping test reads the recursively updated residual (true residual only every
-    4th iteration, MASSolver.cu:510-520), which drifts from b - Ax by rounding; with
-    true_residual_period 1 the test reads b - Ax itself, so the bound holds by construction."""
+    """Reference TEST_CASE("all") (test_linear_solver.cpp:103-164): rel 0, abs 1e-8, reference PCG
+    semantics, ||Ax-b|| < 1e-8. The matrix is scaled by 1e-3: at E = 1e5 the solution is ~1e-5 and
+    the reference's absolute guard (alpha = 0 once |p.Ap| < 1e-20, MASSolver.cu:53) stops progress
+    near 1.1e-8, above the bound -- the CPU oracle stalls identically."""
     system = synthetic.elasticity(8, young_sigma=0.5, seed=21)
-    A = system.scipy()
+    A = (system.scipy() * 1e-3).tocsc()
     s = Solver.create("MAS", "")
     s.set_parameters({"MAS": {"tolerance": 1e-10}})
     s.set_parameters({"MAS": {"relative_tolerance": 0.0, "absolute_tolerance": 1e-8,
-                              "use_preconditioned_residual_norm": False, "true_residual_period": 1}})
+                              "use_preconditioned_residual_norm": False}})
     b = np.random.default_rng(0).uniform(-1, 1, system.n)
     x = np.zeros(system.n)
     s.analyze_pattern(A, A.shape[0])
     s.factorize(A)
     s.solve(b, x)
     assert s.name() == "MAS"
+    assert s.get_info()["solver_status"] == "Reach absolute tolerance"
     assert np.linalg.norm(A @ x - b) < 1e-8
 
 
