@@ -45,7 +45,8 @@ UNIT = "ms/solve"
 TOL = 1e-8
 
 CHOSEN = {"block_dim": 3, "relative_tolerance": TOL, "absolute_tolerance": 0.0, "max_iter": 5000,
-          "precision": "fp32", "true_residual_period": 50, "check_period": 1, "poll_period": 8}
+          "precision": "fp32", "true_residual_period": 50, "check_period": 1, "poll_period": 8,
+          "cuda_graphs": True}
 PLAIN = {"block_dim": 3, "relative_tolerance": TOL, "absolute_tolerance": 0.0, "max_iter": 5000,
          "precision": "fp64", "true_residual_period": 4, "check_period": 10, "poll_period": 8}
 

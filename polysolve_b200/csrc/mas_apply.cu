@@ -150,6 +150,8 @@ namespace pmas
                 }
                 return;
             }
+            // Iteration number from the device state, so a captured chunk of iterations replays.
+            iter = st->iter + 1;
             const double rz_old = st->rz;
             st->rz_old = rz_old;
             st->rz = rz;
@@ -496,6 +498,31 @@ namespace pmas
         }
 
         template <int BD, class Real>
+        constexpr size_t coarse_smem()
+        {
+            constexpr int N = 32 * BD, S = N * (N + 1) / 2;
+            return ((size_t)S * sizeof(Real) + 15) / 16 * 16 + N * sizeof(Real);
+        }
+
+        template <int BD, class Real>
+        void prepare_variant()
+        {
+            using L = Symv0Layout<BD, Real>;
+            const int smem = L::WARPS * L::WARP_BYTES;
+            cuda_check(cudaFuncSetAttribute(k_symv0<BD, Real, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                       "symv0 smem attribute");
+            cuda_check(cudaFuncSetAttribute(k_symv0<BD, Real, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                       "symv0 smem attribute");
+            cuda_check(cudaFuncSetAttribute(k_symv0<BD, Real, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                       "symv0 smem attribute");
+            const int cs = (int)coarse_smem<BD, Real>();
+            cuda_check(cudaFuncSetAttribute(k_coarse_symv<BD, Real, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs),
+                       "coarse smem attribute");
+            cuda_check(cudaFuncSetAttribute(k_coarse_symv<BD, Real, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs),
+                       "coarse smem attribute");
+        }
+
+        template <int BD, class Real>
         int coarse_launch(const MasView &mas, PcgState *st, ReduceBuf red, int mode, int pr, cudaStream_t s)
         {
             if (mas.total_coarse == 0)
@@ -514,21 +541,8 @@ namespace pmas
                 ++launches;
             }
             constexpr int N = 32 * BD, S = N * (N + 1) / 2;
-            const size_t smem = ((size_t)S * sizeof(Real) + 15) / 16 * 16 + N * sizeof(Real);
-            static bool configured[2] = {false, false};
+            const size_t smem = coarse_smem<BD, Real>();
             const int pcg = mode != 0 ? 1 : 0;
-            if (!configured[pcg])
-            {
-                if (pcg)
-                    cuda_check(cudaFuncSetAttribute(k_coarse_symv<BD, Real, 1>,
-                                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                               "coarse smem attribute");
-                else
-                    cuda_check(cudaFuncSetAttribute(k_coarse_symv<BD, Real, 0>,
-                                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem),
-                               "coarse smem attribute");
-                configured[pcg] = true;
-            }
             if (pcg)
             {
                 if (mas.total_coarse > red.capacity)
@@ -547,19 +561,8 @@ namespace pmas
                                PcgConfig cfg, int iter, cudaStream_t s)
         {
             using L = Symv0Layout<BD, Real>;
-            static bool configured = false;
-            static int sms = 0;
+            const int sms = device_sm_count();
             const size_t smem = (size_t)L::WARPS * L::WARP_BYTES;
-            if (!configured)
-            {
-                cuda_check(cudaFuncSetAttribute(k_symv0<BD, Real, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                (int)smem),
-                           "symv0 smem attribute");
-                int dev = 0;
-                cudaGetDevice(&dev);
-                cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-                configured = true;
-            }
             int grid = (mas.banks + L::WARPS - 1) / L::WARPS;
             if (grid > sms)
                 grid = sms;
@@ -583,6 +586,44 @@ namespace pmas
                 symv0_launch_mode<BD, Real, 2>(mas, r, z, st, red, cfg, iter, s);
         }
     } // namespace
+
+    int device_sm_count()
+    {
+        static int cached_dev = -1, cached = 148;
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (dev != cached_dev)
+        {
+            int v = 0;
+            if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0)
+                cached = v;
+            cached_dev = dev;
+        }
+        return cached;
+    }
+
+    void prepare_kernels(int bd, int fp32)
+    {
+        device_sm_count();
+        if (fp32)
+        {
+            if (bd == 1)
+                prepare_variant<1, float>();
+            else if (bd == 2)
+                prepare_variant<2, float>();
+            else
+                prepare_variant<3, float>();
+        }
+        else
+        {
+            if (bd == 1)
+                prepare_variant<1, double>();
+            else if (bd == 2)
+                prepare_variant<2, double>();
+            else
+                prepare_variant<3, double>();
+        }
+    }
 
     int launch_coarse(const MasView &mas, PcgState *st, ReduceBuf red, int mode, int pr, cudaStream_t s)
     {

@@ -189,13 +189,15 @@ namespace pmas
                 if (A[i * N + i] == 0.0)
                     A[i * N + i] = 1.0;
             __syncthreads();
+            // Only the upper triangle (t <= c) is kept up to date: consecutive threads touch
+            // consecutive columns of one row, so shared-memory accesses are conflict-free.
             for (int p = 0; p < N; ++p)
             {
                 const double piv = A[p * N + p];
                 if (tid == 0 && (!isfinite(piv) || piv == 0.0))
                     bad = 1;
                 for (int t = tid; t < N; t += nt)
-                    col[t] = (t == p) ? 0.0 : A[t * N + p];
+                    col[t] = (t == p) ? 0.0 : (t < p ? A[t * N + p] : A[p * N + t]);
                 __syncthreads();
                 for (int e = tid; e < N * N; e += nt)
                 {
@@ -207,7 +209,6 @@ namespace pmas
                     if (!isfinite(u))
                         bad = 1;
                     A[t * N + c] = u;
-                    A[c * N + t] = u;
                 }
                 __syncthreads();
                 for (int t = tid; t < N; t += nt)
@@ -215,11 +216,10 @@ namespace pmas
                     const double u = (t == p) ? -1.0 / piv : col[t] / piv;
                     if (!isfinite(u))
                         bad = 1;
-                    else
-                    {
+                    else if (t <= p)
                         A[t * N + p] = u;
+                    else
                         A[p * N + t] = u;
-                    }
                 }
                 __syncthreads();
             }

@@ -49,6 +49,7 @@ namespace
         std::string ordering = "auto";
         int poll_period = 8;
         bool profile = false; // time every kernel launch with CUDA events
+        bool graphs = true;   // replay chunks of iterations as a CUDA graph
     };
 
     const char *status_string(int s)
@@ -96,7 +97,7 @@ namespace
     const char *KNOWN_KEYS[] = {"block_dim", "max_iter", "relative_tolerance", "absolute_tolerance",
                                 "lazy_partitioning", "use_preconditioned_residual_norm", "precision",
                                 "true_residual_period", "check_period", "initial_guess", "beta", "ordering",
-                                "poll_period", "profile_kernels"};
+                                "poll_period", "profile_kernels", "cuda_graphs"};
 
     // MASSolverImpl::set_parameters (MASSolver.cu:198-212) plus the extension keys.
     void apply_mas_params(Params &p, const Json &m, bool strict)
@@ -171,6 +172,8 @@ namespace
         }
         if (auto *v = m.find("profile_kernels"))
             q.profile = get_bool(*v, "profile_kernels");
+        if (auto *v = m.find("cuda_graphs"))
+            q.graphs = get_bool(*v, "cuda_graphs");
         if (auto *v = m.find("poll_period"))
         {
             q.poll_period = get_int(*v, "poll_period");
@@ -202,6 +205,12 @@ struct mas_solver
     std::vector<cudaEvent_t> ev_pool;
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
     size_t ev_used = 0;
+
+    // CUDA graph of `graph_chunk` PCG iterations, replayed until the device flags done.
+    cudaGraphExec_t graph_exec = nullptr;
+    uint64_t graph_key = 0;
+    bool capturing = false;
+    std::vector<std::pair<int, long long>> graph_counts; // kernels per kind in one replay
 
     // Info of the last solve (MASSolver.cu:145-149).
     int iterations = 0;
@@ -239,6 +248,8 @@ struct mas_solver
         }
         for (cudaEvent_t e : ev_pool)
             cudaEventDestroy(e);
+        if (graph_exec)
+            cudaGraphExecDestroy(graph_exec);
         if (h_st)
             cudaFreeHost(h_st);
         if (own_stream)
@@ -283,8 +294,23 @@ struct mas_solver
             kernels = f();
         else
             f();
-        kstats[idx].second.launches += kernels;
-        total_launches += kernels;
+        if (capturing)
+        {
+            bool found = false;
+            for (auto &gc : graph_counts)
+                if (gc.first == idx)
+                {
+                    gc.second += kernels;
+                    found = true;
+                }
+            if (!found)
+                graph_counts.push_back({idx, kernels});
+        }
+        else
+        {
+            kstats[idx].second.launches += kernels;
+            total_launches += kernels;
+        }
         if (p.profile)
         {
             cuda_check(cudaEventRecord(b, stream), "event");
@@ -401,6 +427,8 @@ struct mas_solver
         pattern = h;
 
         build_mas(mas, A, d_node_real.get(), p.fp32 ? 1 : 0, stream);
+        prepare_kernels(bd_, p.fp32 ? 1 : 0);
+        drop_graph();
 
         const size_t len = (size_t)banks * 32 * bd_;
         x.alloc(len, "device_buffers x");
@@ -442,6 +470,85 @@ struct mas_solver
         return c;
     }
 
+    // One PCG iteration's kernels (MASSolver.cu:498-583). With host_knows_k the true-residual
+    // SpMV is only launched on its iterations; in a captured graph it is always launched and
+    // returns at once unless (st->iter + 1) % P == 0.
+    void launch_iteration(const BankedView &Av, const MasView &mv, const PcgConfig &cfg, int P, int pr, bool host_knows_k,
+                          int k)
+    {
+        PcgState *S = st.get();
+        run("spmv_pap", 1, [&] { launch_spmv(SPMV_PAP, Av, pv.get(), Ap.get(), nullptr, &mv, S, red(), 1, 0, stream); });
+        run("update_xr", 1, [&] { launch_update_xr(Av, mv, x.get(), r.get(), pv.get(), Ap.get(), S, red(), P, stream); });
+        if (!host_knows_k || k % P == 0)
+            run("spmv_residual", 1,
+                [&] { launch_spmv(SPMV_RESIDUAL, Av, x.get(), r.get(), b.get(), &mv, S, red(), 1, P, stream); });
+        run("mas_coarse", 0, [&] { return launch_coarse(mv, S, red(), 2, pr, stream); });
+        run("mas_symv0", 1, [&] { launch_symv0(mv, r.get(), z.get(), S, red(), cfg, 0, 2, stream); });
+        run("update_p", 1, [&] { launch_update_p(mv, pv.get(), z.get(), S, 0, stream); });
+    }
+
+    void drop_graph()
+    {
+        if (graph_exec)
+            cudaGraphExecDestroy(graph_exec);
+        graph_exec = nullptr;
+        graph_key = 0;
+        graph_counts.clear();
+    }
+
+    void ensure_graph(const BankedView &Av, const MasView &mv, const PcgConfig &cfg, int P, int pr, int chunk)
+    {
+        uint64_t key = 1469598103934665603ull;
+        auto mix = [&key](uint64_t v) {
+            key ^= v;
+            key *= 1099511628211ull;
+        };
+        for (const void *ptr : {(const void *)x.get(), (const void *)b.get(), (const void *)r.get(),
+                                (const void *)pv.get(), (const void *)z.get(), (const void *)Ap.get(),
+                                (const void *)st.get(), (const void *)partials.get(), (const void *)Av.vals, mv.inv,
+                                (const void *)stream})
+            mix((uint64_t)(uintptr_t)ptr);
+        mix((uint64_t)cfg.max_iter);
+        mix((uint64_t)cfg.check_period);
+        mix((uint64_t)cfg.use_prec_norm);
+        mix((uint64_t)cfg.polak_ribiere);
+        uint64_t bits;
+        std::memcpy(&bits, &cfg.rel_tol, 8);
+        mix(bits);
+        std::memcpy(&bits, &cfg.abs_tol, 8);
+        mix(bits);
+        mix((uint64_t)P);
+        mix((uint64_t)pr);
+        mix((uint64_t)chunk);
+        if (graph_exec && key == graph_key)
+            return;
+        drop_graph();
+        cudaGraph_t graph = nullptr;
+        cuda_check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        capturing = true;
+        try
+        {
+            for (int i = 0; i < chunk; ++i)
+                launch_iteration(Av, mv, cfg, P, pr, false, 0);
+        }
+        catch (...)
+        {
+            capturing = false;
+            cudaStreamEndCapture(stream, &graph);
+            if (graph)
+                cudaGraphDestroy(graph);
+            cudaGetLastError();
+            graph_counts.clear();
+            throw;
+        }
+        capturing = false;
+        cuda_check(cudaStreamEndCapture(stream, &graph), "end capture");
+        cudaError_t e = cudaGraphInstantiate(&graph_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        cuda_check(e, "graph instantiate");
+        graph_key = key;
+    }
+
     // pcg_solve (MASSolver.cu:469-595) on device-resident b_ / x_ (padded order).
     void pcg()
     {
@@ -459,7 +566,7 @@ struct mas_solver
         launch_pcg_init_state(S, stream);
         const int pr = p.polak_ribiere ? 1 : 0;
         // r = b - A x, its level-0 restriction and rr0
-        run("spmv_residual", 1, [&] { launch_spmv(SPMV_RESIDUAL, Av, x.get(), r.get(), b.get(), &mv, S, red(), 0, stream); });
+        run("spmv_residual", 1, [&] { launch_spmv(SPMV_RESIDUAL, Av, x.get(), r.get(), b.get(), &mv, S, red(), 0, 0, stream); });
         run("mas_coarse", 0, [&] { return launch_coarse(mv, S, red(), 1, pr, stream); });
         run("mas_symv0", 1, [&] { launch_symv0(mv, r.get(), z.get(), S, red(), cfg, 0, 1, stream); });
         run("update_p", 1, [&] { launch_update_p(mv, pv.get(), z.get(), S, 1, stream); });
@@ -476,31 +583,33 @@ struct mas_solver
         status = MAS_STATUS_RUNNING;
         const int P = p.true_residual_period;
         const int chunk = p.poll_period;
+        const bool graphs = p.graphs && !p.profile;
+        if (graphs)
+            ensure_graph(Av, mv, cfg, P, pr, chunk);
         int launched = 0;
         bool stop = false;
         int pending = -1; // slot holding the previous chunk's state copy
         cudaEvent_t chunk_ev[2];
         cuda_check(cudaEventCreateWithFlags(&chunk_ev[0], cudaEventDisableTiming), "event");
         cuda_check(cudaEventCreateWithFlags(&chunk_ev[1], cudaEventDisableTiming), "event");
+        int slot_flip = 0;
         for (int k0 = 1; k0 <= p.max_iter && !stop; k0 += chunk)
         {
             const int k1 = std::min(p.max_iter, k0 + chunk - 1);
-            for (int k = k0; k <= k1; ++k)
+            if (graphs)
             {
-                run("spmv_pap", 1, [&] { launch_spmv(SPMV_PAP, Av, pv.get(), Ap.get(), nullptr, &mv, S, red(), k, stream); });
-                if (k % P == 0)
+                cuda_check(cudaGraphLaunch(graph_exec, stream), "graph launch");
+                for (auto &gc : graph_counts)
                 {
-                    run("update_x", 1, [&] { launch_update_x(nodes, bd, x.get(), pv.get(), S, stream); });
-                    run("spmv_residual", 1, [&] { launch_spmv(SPMV_RESIDUAL, Av, x.get(), r.get(), b.get(), &mv, S, red(), k, stream); });
+                    kstats[gc.first].second.launches += gc.second;
+                    total_launches += gc.second;
                 }
-                else
-                    run("update_xr", 1, [&] { launch_update_xr(Av, mv, x.get(), r.get(), pv.get(), Ap.get(), S, red(), stream); });
-                run("mas_coarse", 0, [&] { return launch_coarse(mv, S, red(), 2, pr, stream); });
-                run("mas_symv0", 1, [&] { launch_symv0(mv, r.get(), z.get(), S, red(), cfg, k, 2, stream); });
-                run("update_p", 1, [&] { launch_update_p(mv, pv.get(), z.get(), S, 0, stream); });
             }
+            else
+                for (int k = k0; k <= k1; ++k)
+                    launch_iteration(Av, mv, cfg, P, pr, true, k);
             launched = k1;
-            const int slot = (k0 / chunk) & 1;
+            const int slot = (slot_flip++) & 1;
             cuda_check(cudaMemcpyAsync(&h_st[slot], S, sizeof(PcgState), cudaMemcpyDeviceToHost, stream), "state");
             cuda_check(cudaEventRecord(chunk_ev[slot], stream), "event");
             // Look at the previous chunk's state while this chunk runs.
@@ -950,7 +1059,7 @@ extern "C" int mas_debug_spmv(mas_solver *h, const double *xin, double *y, int l
         if (!h->factorized || len != h->banks * 32 * h->bd)
             throw Error(ERR_NOT_FACTORIZED, "[MAS] debug_spmv: size mismatch.");
         cuda_check(cudaMemcpyAsync(h->x.get(), xin, sizeof(double) * len, cudaMemcpyHostToDevice, h->stream), "x");
-        launch_spmv(SPMV_PLAIN, h->A.view(), h->x.get(), h->Ap.get(), nullptr, nullptr, nullptr, h->red(), 0,
+        launch_spmv(SPMV_PLAIN, h->A.view(), h->x.get(), h->Ap.get(), nullptr, nullptr, nullptr, h->red(), 0, 0,
                     h->stream);
         cuda_check(cudaMemcpyAsync(y, h->Ap.get(), sizeof(double) * len, cudaMemcpyDeviceToHost, h->stream), "y");
         cuda_check(cudaStreamSynchronize(h->stream), "spmv");

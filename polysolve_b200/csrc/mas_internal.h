@@ -217,13 +217,15 @@ namespace pmas
         SPMV_PAP = 1,      // y = A p ; pAp = p . y ; alpha = rz / pAp
         SPMV_RESIDUAL = 2, // y = b - A x ; restrict y to level-0 components ; rr = y . y
     };
+    // period > 0 (SPMV_RESIDUAL in the PCG loop): runs only when (st->iter + 1) % period == 0.
     void launch_spmv(int mode, const BankedView &A, const double *x, double *y, const double *b, const MasView *mas,
-                     PcgState *st, ReduceBuf red, int iter, cudaStream_t s);
+                     PcgState *st, ReduceBuf red, int iter, int period, cudaStream_t s);
 
     // mas_pcg.cu
+    // x += alpha p; unless this iteration recomputes the true residual ((st->iter + 1) % period == 0):
+    // r -= alpha Ap, rr = r . r and the level-0 restriction of r.
     void launch_update_xr(const BankedView &A, const MasView &mas, double *x, double *r, const double *p,
-                          const double *Ap, PcgState *st, ReduceBuf red, cudaStream_t s);
-    void launch_update_x(int nodes, int bd, double *x, const double *p, PcgState *st, cudaStream_t s);
+                          const double *Ap, PcgState *st, ReduceBuf red, int period, cudaStream_t s);
     // p = z0 + prolongation(zc) + beta p (z0: level-0 part of z = M^-1 r)
     void launch_update_p(const MasView &mas, double *p, const double *z0, PcgState *st, int first, cudaStream_t s);
     void launch_permute_in(int n, int bd, int V, const int *padded_of_block, const double *src, double *dst,
@@ -243,6 +245,10 @@ namespace pmas
     void launch_restrict_plain(const BankedView &A, const MasView &mas, const double *r, cudaStream_t s);
     // z = z0 + prolongation(zc) (outside the PCG loop).
     void launch_prolong(const MasView &mas, const double *z0, double *z, cudaStream_t s);
+    // Set kernel attributes (large shared memory) for every variant used with this block size and
+    // precision, so launches inside a CUDA graph capture never touch function attributes.
+    void prepare_kernels(int bd, int fp32);
+    int device_sm_count();
 
     // mas_build.cu: the MAS hierarchy and inverses.
     struct MasDevice

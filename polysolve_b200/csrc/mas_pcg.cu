@@ -2,8 +2,8 @@
 //
 // The reference runs each vector step as its own launch (axpby / inner_product / scalar_division,
 // MASSolver.cu:46-81, InnerProduct.cu:16-45) with a memset and an FP64 atomicAdd per dot. Here:
-//   update_xr: x += alpha p ; r -= alpha Ap ; rr = r . r ; level-0 restriction of r   (one pass)
-//   update_x:  x += alpha p                       (true-residual steps; r = b - A x follows)
+//   update_xr: x += alpha p ; r -= alpha Ap ; rr = r . r ; level-0 restriction of r   (one pass;
+//              on true-residual iterations only x, then r = b - A x follows in the SpMV)
 //   update_p:  p = z0 + P zc + beta p             (the MAS prolongation fused in; beta from the
 //                                                  device state, set by the MAS apply)
 // alpha / beta are read from the device-resident PcgState, and every dot is a deterministic
@@ -50,27 +50,39 @@ namespace pmas
     {
         constexpr int UPD_THREADS = 256;
 
-        // One warp per bank: the bank's 32 * BD contiguous values are read and written with
-        // coalesced accesses (value e = t * 32 + lane); the node view for the level-0 restriction
-        // goes through shared memory.
+        // Warps stride over banks (about four CTAs per SM, so few CTAs contend for the reduction
+        // ticket); a bank's 32 * BD contiguous values are read and written with coalesced accesses
+        // (value e = t * 32 + lane); the node view for the level-0 restriction goes through shared
+        // memory. On a true-residual iteration only x is updated.
         template <int BD>
         __global__ void __launch_bounds__(UPD_THREADS) k_update_xr(int banks, double *__restrict__ x, double *__restrict__ r,
                                                                    const double *__restrict__ p,
                                                                    const double *__restrict__ Ap,
                                                                    const int *__restrict__ lcco0,
                                                                    const int *__restrict__ cco0_base, double *rc,
-                                                                   PcgState *st, ReduceBuf red)
+                                                                   PcgState *st, ReduceBuf red, int period)
         {
             __shared__ double sv[UPD_THREADS / 32][32 * BD];
             if (st->done)
                 return;
             const double alpha = st->alpha;
+            const bool due = period > 0 && (st->iter + 1) % period == 0;
             const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-            const int bank = blockIdx.x * (UPD_THREADS / 32) + w;
+            const int total_warps = gridDim.x * (UPD_THREADS / 32);
             double part = 0.0;
-            if (bank < banks)
+            for (int bank = blockIdx.x * (UPD_THREADS / 32) + w; bank < banks; bank += total_warps)
             {
                 const long long b0 = (long long)bank * 32 * BD;
+                if (due)
+                {
+#pragma unroll
+                    for (int t = 0; t < BD; ++t)
+                    {
+                        const long long idx = b0 + t * 32 + lane;
+                        x[idx] = fma(alpha, p[idx], x[idx]);
+                    }
+                    continue;
+                }
 #pragma unroll
                 for (int t = 0; t < BD; ++t)
                 {
@@ -87,14 +99,17 @@ namespace pmas
 #pragma unroll
                 for (int i = 0; i < BD; ++i)
                     rn[i] = sv[w][lane * BD + i];
+                __syncwarp();
                 warp_segment_store<BD>(rn, lcco0[(long long)bank * 32 + lane], cco0_base[bank], rc);
             }
+            if (due)
+                return;
             double v1[1] = {part}, tot[1];
             if (grid_reduce<1, UPD_THREADS>(v1, red.partials, &st->counter[1], tot) && threadIdx.x == 0)
                 st->rr = tot[0];
         }
 
-        // p = z0 + sum_l zc[cslot_l(node)] + beta p, one warp per bank, coalesced.
+        // p = z0 + sum_l zc[cslot_l(node)] + beta p; warps stride over banks, coalesced.
         template <int BD>
         __global__ void __launch_bounds__(UPD_THREADS) k_update_p(MasView mas, double *__restrict__ p,
                                                                   const double *__restrict__ z0, const PcgState *st,
@@ -104,40 +119,30 @@ namespace pmas
                 return;
             const double beta = first ? 0.0 : st->beta;
             const int lane = threadIdx.x & 31;
-            const int bank = blockIdx.x * (UPD_THREADS / 32) + (threadIdx.x >> 5);
-            if (bank >= mas.banks)
-                return;
-            const long long b0 = (long long)bank * 32 * BD;
+            const int total_warps = gridDim.x * (UPD_THREADS / 32);
             const double *__restrict__ zc = mas.zc;
-#pragma unroll
-            for (int t = 0; t < BD; ++t)
+            for (int bank = blockIdx.x * (UPD_THREADS / 32) + (threadIdx.x >> 5); bank < mas.banks; bank += total_warps)
             {
-                const int e = t * 32 + lane;
-                const int node = e / BD, comp = e - node * BD;
-                const int4 cs = mas.cslot[(long long)bank * 32 + node];
-                const long long idx = b0 + e;
-                double v = z0[idx];
-                if (cs.x >= 0)
-                    v += zc[(size_t)cs.x * BD + comp];
-                if (cs.y >= 0)
-                    v += zc[(size_t)cs.y * BD + comp];
-                if (cs.z >= 0)
-                    v += zc[(size_t)cs.z * BD + comp];
-                if (cs.w >= 0)
-                    v += zc[(size_t)cs.w * BD + comp];
-                p[idx] = first ? v : fma(beta, p[idx], v);
+                const long long b0 = (long long)bank * 32 * BD;
+#pragma unroll
+                for (int t = 0; t < BD; ++t)
+                {
+                    const int e = t * 32 + lane;
+                    const int node = e / BD, comp = e - node * BD;
+                    const int4 cs = mas.cslot[(long long)bank * 32 + node];
+                    const long long idx = b0 + e;
+                    double v = z0[idx];
+                    if (cs.x >= 0)
+                        v += zc[(size_t)cs.x * BD + comp];
+                    if (cs.y >= 0)
+                        v += zc[(size_t)cs.y * BD + comp];
+                    if (cs.z >= 0)
+                        v += zc[(size_t)cs.z * BD + comp];
+                    if (cs.w >= 0)
+                        v += zc[(size_t)cs.w * BD + comp];
+                    p[idx] = first ? v : fma(beta, p[idx], v);
+                }
             }
-        }
-
-        __global__ void k_update_x(long long len, double *__restrict__ x, const double *__restrict__ p,
-                                   const PcgState *st)
-        {
-            if (st->done)
-                return;
-            const double alpha = st->alpha;
-            for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < len;
-                 i += (long long)gridDim.x * blockDim.x)
-                x[i] = fma(alpha, p[i], x[i]);
         }
 
         // dst (padded, node-major, zero elsewhere) <- src (caller's order, length n)
@@ -180,37 +185,42 @@ namespace pmas
         }
     } // namespace
 
-    void launch_update_xr(const BankedView &A, const MasView &mas, double *x, double *r, const double *p,
-                          const double *Ap, PcgState *st, ReduceBuf red, cudaStream_t s)
+    namespace
     {
-        const int grid = (A.banks + UPD_THREADS / 32 - 1) / (UPD_THREADS / 32);
+        int bank_grid(int banks)
+        {
+            const int need = (banks + UPD_THREADS / 32 - 1) / (UPD_THREADS / 32);
+            const int cap = device_sm_count() * 4;
+            return need < cap ? need : cap;
+        }
+    } // namespace
+
+    void launch_update_xr(const BankedView &A, const MasView &mas, double *x, double *r, const double *p,
+                          const double *Ap, PcgState *st, ReduceBuf red, int period, cudaStream_t s)
+    {
+        const int grid = bank_grid(A.banks);
+        if (grid == 0)
+            return;
         if (grid > red.capacity)
             throw Error(ERR_INVALID, "[MAS] reduction scratch too small");
         switch (A.bd)
         {
         case 1:
-            k_update_xr<1><<<grid, UPD_THREADS, 0, s>>>(A.banks, x, r, p, Ap, mas.lcco0, mas.cco0_base, mas.rc, st, red);
+            k_update_xr<1><<<grid, UPD_THREADS, 0, s>>>(A.banks, x, r, p, Ap, mas.lcco0, mas.cco0_base, mas.rc, st, red, period);
             break;
         case 2:
-            k_update_xr<2><<<grid, UPD_THREADS, 0, s>>>(A.banks, x, r, p, Ap, mas.lcco0, mas.cco0_base, mas.rc, st, red);
+            k_update_xr<2><<<grid, UPD_THREADS, 0, s>>>(A.banks, x, r, p, Ap, mas.lcco0, mas.cco0_base, mas.rc, st, red, period);
             break;
         default:
-            k_update_xr<3><<<grid, UPD_THREADS, 0, s>>>(A.banks, x, r, p, Ap, mas.lcco0, mas.cco0_base, mas.rc, st, red);
+            k_update_xr<3><<<grid, UPD_THREADS, 0, s>>>(A.banks, x, r, p, Ap, mas.lcco0, mas.cco0_base, mas.rc, st, red, period);
             break;
         }
         cuda_check(cudaGetLastError(), "update_xr launch");
     }
 
-    void launch_update_x(int nodes, int bd, double *x, const double *p, PcgState *st, cudaStream_t s)
-    {
-        const long long len = (long long)nodes * bd;
-        k_update_x<<<grid_for(len), 256, 0, s>>>(len, x, p, st);
-        cuda_check(cudaGetLastError(), "update_x launch");
-    }
-
     void launch_update_p(const MasView &mas, double *p, const double *z0, PcgState *st, int first, cudaStream_t s)
     {
-        const int grid = (mas.banks + UPD_THREADS / 32 - 1) / (UPD_THREADS / 32);
+        const int grid = bank_grid(mas.banks);
         if (grid == 0)
             return;
         switch (mas.bd)

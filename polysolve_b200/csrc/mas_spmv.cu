@@ -26,11 +26,14 @@ namespace pmas
                                                                double *__restrict__ y, const double *__restrict__ b,
                                                                const int *__restrict__ lcco0,
                                                                const int *__restrict__ cco0_base, double *rc,
-                                                               PcgState *st, ReduceBuf red, int iter)
+                                                               PcgState *st, ReduceBuf red, int iter, int period)
         {
             constexpr int BS = BD * BD;
             constexpr int PAIRS = BS / 2;
             if (MODE != SPMV_PLAIN && st->done)
+                return;
+            // In-loop true residual: only every `period`-th iteration (iteration = st->iter + 1).
+            if (MODE == SPMV_RESIDUAL && period > 0 && (st->iter + 1) % period != 0)
                 return;
             const int lane = threadIdx.x & 31;
             const int bank = blockIdx.x * BANKS_PER_CTA + (threadIdx.x >> 5);
@@ -124,7 +127,7 @@ namespace pmas
 
         template <int BD>
         void launch_bd(int mode, const BankedView &A, const double *x, double *y, const double *b, const MasView *mas,
-                       PcgState *st, ReduceBuf red, int iter, cudaStream_t s)
+                       PcgState *st, ReduceBuf red, int iter, int period, cudaStream_t s)
         {
             const int grid = (A.banks + BANKS_PER_CTA - 1) / BANKS_PER_CTA;
             if (grid == 0)
@@ -137,13 +140,13 @@ namespace pmas
             switch (mode)
             {
             case SPMV_PLAIN:
-                k_spmv<BD, SPMV_PLAIN><<<grid, SPMV_THREADS, 0, s>>>(A, x, y, b, lcco0, base, rc, st, red, iter);
+                k_spmv<BD, SPMV_PLAIN><<<grid, SPMV_THREADS, 0, s>>>(A, x, y, b, lcco0, base, rc, st, red, iter, period);
                 break;
             case SPMV_PAP:
-                k_spmv<BD, SPMV_PAP><<<grid, SPMV_THREADS, 0, s>>>(A, x, y, b, lcco0, base, rc, st, red, iter);
+                k_spmv<BD, SPMV_PAP><<<grid, SPMV_THREADS, 0, s>>>(A, x, y, b, lcco0, base, rc, st, red, iter, period);
                 break;
             default:
-                k_spmv<BD, SPMV_RESIDUAL><<<grid, SPMV_THREADS, 0, s>>>(A, x, y, b, lcco0, base, rc, st, red, iter);
+                k_spmv<BD, SPMV_RESIDUAL><<<grid, SPMV_THREADS, 0, s>>>(A, x, y, b, lcco0, base, rc, st, red, iter, period);
                 break;
             }
             cuda_check(cudaGetLastError(), "spmv launch");
@@ -151,18 +154,18 @@ namespace pmas
     } // namespace
 
     void launch_spmv(int mode, const BankedView &A, const double *x, double *y, const double *b, const MasView *mas,
-                     PcgState *st, ReduceBuf red, int iter, cudaStream_t s)
+                     PcgState *st, ReduceBuf red, int iter, int period, cudaStream_t s)
     {
         switch (A.bd)
         {
         case 1:
-            launch_bd<1>(mode, A, x, y, b, mas, st, red, iter, s);
+            launch_bd<1>(mode, A, x, y, b, mas, st, red, iter, period, s);
             break;
         case 2:
-            launch_bd<2>(mode, A, x, y, b, mas, st, red, iter, s);
+            launch_bd<2>(mode, A, x, y, b, mas, st, red, iter, period, s);
             break;
         case 3:
-            launch_bd<3>(mode, A, x, y, b, mas, st, red, iter, s);
+            launch_bd<3>(mode, A, x, y, b, mas, st, red, iter, period, s);
             break;
         default:
             throw Error(ERR_INVALID, "[MAS] block_dim must be 1, 2 or 3");
