@@ -8,13 +8,15 @@
 //    kernel that produced r (SpMV residual or the x/r update), deterministic;
 //  * k_coarse_sum: coarse level l sums from level l-1 (every level-l component merges at most 32
 //    level-(l-1) components of one bank), one warp per component, one launch per level;
-//  * k_coarse_symv: one CTA per coarse matrix (one warp per column tile), zc = A_l^-1 rc, and
-//    rc . zc for the PCG dot (identity inverses -- banks of isolated rows -- skip the multiply);
+//  * k_coarse_symv: one CTA per coarse matrix (one warp per column tile, matrix read from global
+//    memory), zc = A_l^-1 rc, and rc . zc for the PCG dot (identity inverses -- banks of isolated
+//    rows -- skip the multiply);
 //  * k_symv0: persistent warps stream the level-0 inverses through shared memory with
-//    cp.async.bulk (two stages per warp, mbarrier completion) and write z0 = A_0^-1 r with r . z0;
-//    the last CTA runs the PCG bookkeeping of the reference (rz = r . z0 + rc . zc, convergence,
-//    beta). The prolongation z = z0 + P zc is fused into the p update (update_p), since PCG uses z
-//    only there and in r . z = r . z0 + (P^T r) . zc.
+//    cp.async.bulk (two stages per warp, mbarrier completion) and write z0 = A_0^-1 r with per-CTA
+//    r . z0. The coarse levels do not feed it, so the host runs them concurrently on a second
+//    stream; k_finalize (one CTA, after the join) sums the partials and runs the reference's PCG
+//    bookkeeping (rz = r . z0 + rc . zc, convergence, beta). The prolongation z = z0 + P zc is fused
+//    into the p update (update_p): PCG uses z only there and in r . z = r . z0 + (P^T r) . zc.
 //
 // Inverses are stored tile-packed (mas_internal.h): the same N (N + 1) / 2 values as packed upper
 // storage, laid out so a warp reads every 32 x 32 tile conflict-free and uses each value for both
@@ -133,9 +135,9 @@ namespace pmas
 
         // Finish of an iteration (last CTA of k_symv0): the reference's per-iteration scalar work
         // and convergence test (MASSolver.cu:505, 526-583), on the device.
-        __device__ void pcg_finalize(PcgState *st, const PcgConfig &cfg, int iter, int mode, double rz_fine,
-                                     double rzx_fine)
+        __device__ void pcg_finalize(PcgState *st, const PcgConfig &cfg, int mode, double rz_fine, double rzx_fine)
         {
+            int iter;
             const double rz = rz_fine + st->rz_coarse;
             const double rzcross = rzx_fine + st->rzx_coarse;
             if (mode == 1)
@@ -324,9 +326,49 @@ namespace pmas
             }
             if (MODE == 0)
                 return;
-            double tot[2];
-            if (grid_reduce<2, THREADS>(part, red.partials, &st->counter[2], tot) && threadIdx.x == 0)
-                pcg_finalize(st, cfg, iter, MODE, tot[0], tot[1]);
+            const double t0 = block_sum<THREADS>(part[0]);
+            const double t1 = block_sum<THREADS>(part[1]);
+            if (threadIdx.x == 0)
+            {
+                red.rz_parts[2 * blockIdx.x] = t0;
+                red.rz_parts[2 * blockIdx.x + 1] = t1;
+                if (blockIdx.x == 0)
+                    st->n_rz = gridDim.x;
+            }
+        }
+
+        // The iteration's bookkeeping in one CTA: sum the per-CTA partials in a fixed order.
+        constexpr int FIN_THREADS = 256;
+        __global__ void __launch_bounds__(FIN_THREADS) k_finalize(PcgState *st, ReduceBuf red, PcgConfig cfg, int mode)
+        {
+            if (st->done)
+                return;
+            const int n_rz = st->n_rz, n_co = st->n_co, n_rr = (mode == 2) ? st->n_rr : 0;
+            double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+            for (int i = threadIdx.x; i < n_rz; i += FIN_THREADS)
+            {
+                v[0] += __ldcg(red.rz_parts + 2 * i);
+                v[1] += __ldcg(red.rz_parts + 2 * i + 1);
+            }
+            for (int i = threadIdx.x; i < n_co; i += FIN_THREADS)
+            {
+                v[2] += __ldcg(red.co_parts + 2 * i);
+                v[3] += __ldcg(red.co_parts + 2 * i + 1);
+            }
+            for (int i = threadIdx.x; i < n_rr; i += FIN_THREADS)
+                v[4] += __ldcg(red.rr_parts + i);
+            double t[5];
+#pragma unroll
+            for (int i = 0; i < 5; ++i)
+                t[i] = block_sum<FIN_THREADS>(v[i]);
+            if (threadIdx.x == 0)
+            {
+                st->rz_coarse = t[2];
+                st->rzx_coarse = t[3];
+                if (mode == 2)
+                    st->rr = t[4];
+                pcg_finalize(st, cfg, mode, t[0], t[1]);
+            }
         }
 
         // Coarse level l sums: rc[node] = sum of rc over its <= 32 children (previous level).
@@ -362,16 +404,16 @@ namespace pmas
         }
 
         // One CTA (BD warps, one per column tile) per coarse matrix: zc = A^-1 rc on its 32 coarse
-        // nodes; in PCG modes rc . zc (and rc . zc_old) reduced into the state.
+        // nodes; in PCG modes per-CTA rc . zc (and rc . zc_old). The matrix is read straight from
+        // global memory (each warp's tile reads are coalesced), so a CTA needs only ~2 KB of shared
+        // memory and can run beside the level-0 kernel, which holds most of every SM's.
         template <int BD, class Real, int PCG>
         __global__ void __launch_bounds__(BD * 32) k_coarse_symv(MasView mas, PcgState *st, ReduceBuf red, int pr)
         {
             constexpr int N = 32 * BD, S = N * (N + 1) / 2;
             if (PCG && st->done)
                 return;
-            extern __shared__ __align__(128) unsigned char smem[];
-            Real *mat = reinterpret_cast<Real *>(smem);
-            Real *xs = reinterpret_cast<Real *>(smem + ((size_t)S * sizeof(Real) + 15) / 16 * 16);
+            __shared__ __align__(16) Real xs[N];
             __shared__ Real ypart[BD][N];
             const int g = blockIdx.x;
             const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
@@ -404,31 +446,15 @@ namespace pmas
             }
             else
             {
-                // One bulk copy (cp.async.bulk) for the whole matrix, completing on an mbarrier.
-                __shared__ __align__(8) uint64_t bar;
-                const Real *src = static_cast<const Real *>(mas.inv) + (size_t)(mas.banks + g) * S;
-                if (tid == 0)
-                {
-                    mbar_init(&bar, 1);
-                    fence_mbar_init();
-                    bulk_load(mat, src, (uint32_t)(S * sizeof(Real)), &bar);
-                }
+                const Real *M = static_cast<const Real *>(mas.inv) + (size_t)(mas.banks + g) * S;
                 for (int i = tid; i < N; i += BD * 32)
                     xs[i] = (Real)mas.rc[v0 + i];
                 __syncthreads();
-                if (!mbar_wait_bounded(&bar, 0, PCG ? &st->error : nullptr))
-                {
-                    // Bounded second wait so the copy is not left writing shared memory, then give
-                    // up on this matrix (the host reports ERR_TIMEOUT).
-                    for (long long i = 0; i < MBAR_SPIN_LIMIT && !mbar_try_wait(&bar, 0); ++i)
-                    {
-                    }
-                }
                 Real yr[BD];
 #pragma unroll
                 for (int t = 0; t < BD; ++t)
                     yr[t] = Real(0);
-                symv_column<BD, Real>(mat, xs, lane, w, yr);
+                symv_column<BD, Real>(M, xs, lane, w, yr);
 #pragma unroll
                 for (int t = 0; t < BD; ++t)
                     ypart[w][t * 32 + lane] = (t <= w) ? yr[t] : Real(0);
@@ -449,11 +475,14 @@ namespace pmas
             }
             if (!PCG)
                 return;
-            double tot[2];
-            if (grid_reduce<2, BD * 32>(part, red.partials, &st->counter[3], tot) && threadIdx.x == 0)
+            const double t0 = block_sum<BD * 32>(part[0]);
+            const double t1 = block_sum<BD * 32>(part[1]);
+            if (threadIdx.x == 0)
             {
-                st->rz_coarse = tot[0];
-                st->rzx_coarse = tot[1];
+                red.co_parts[2 * blockIdx.x] = t0;
+                red.co_parts[2 * blockIdx.x + 1] = t1;
+                if (blockIdx.x == 0)
+                    st->n_co = gridDim.x;
             }
         }
 
@@ -498,13 +527,6 @@ namespace pmas
         }
 
         template <int BD, class Real>
-        constexpr size_t coarse_smem()
-        {
-            constexpr int N = 32 * BD, S = N * (N + 1) / 2;
-            return ((size_t)S * sizeof(Real) + 15) / 16 * 16 + N * sizeof(Real);
-        }
-
-        template <int BD, class Real>
         void prepare_variant()
         {
             using L = Symv0Layout<BD, Real>;
@@ -515,11 +537,6 @@ namespace pmas
                        "symv0 smem attribute");
             cuda_check(cudaFuncSetAttribute(k_symv0<BD, Real, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
                        "symv0 smem attribute");
-            const int cs = (int)coarse_smem<BD, Real>();
-            cuda_check(cudaFuncSetAttribute(k_coarse_symv<BD, Real, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs),
-                       "coarse smem attribute");
-            cuda_check(cudaFuncSetAttribute(k_coarse_symv<BD, Real, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs),
-                       "coarse smem attribute");
         }
 
         template <int BD, class Real>
@@ -528,7 +545,7 @@ namespace pmas
             if (mas.total_coarse == 0)
             {
                 if (mode != 0)
-                    cuda_check(cudaMemsetAsync(&st->rz_coarse, 0, 2 * sizeof(double), s), "memset");
+                    cuda_check(cudaMemsetAsync(&st->n_co, 0, sizeof(int), s), "memset");
                 return 0;
             }
             int launches = 0;
@@ -540,17 +557,15 @@ namespace pmas
                 k_coarse_sum<BD><<<(count + 7) / 8, 256, 0, s>>>(mas, mas.coff[l], count, mode ? st : nullptr);
                 ++launches;
             }
-            constexpr int N = 32 * BD, S = N * (N + 1) / 2;
-            const size_t smem = coarse_smem<BD, Real>();
             const int pcg = mode != 0 ? 1 : 0;
             if (pcg)
             {
                 if (mas.total_coarse > red.capacity)
                     throw Error(ERR_INVALID, "[MAS] reduction scratch too small");
-                k_coarse_symv<BD, Real, 1><<<mas.total_coarse, BD * 32, smem, s>>>(mas, st, red, pr);
+                k_coarse_symv<BD, Real, 1><<<mas.total_coarse, BD * 32, 0, s>>>(mas, st, red, pr);
             }
             else
-                k_coarse_symv<BD, Real, 0><<<mas.total_coarse, BD * 32, smem, s>>>(mas, st, red, 0);
+                k_coarse_symv<BD, Real, 0><<<mas.total_coarse, BD * 32, 0, s>>>(mas, st, red, 0);
             ++launches;
             cuda_check(cudaGetLastError(), "coarse launch");
             return launches;
@@ -663,6 +678,12 @@ namespace pmas
             else
                 symv0_launch<3, double>(mas, r, z, st, red, cfg, iter, mode, s);
         }
+    }
+
+    void launch_finalize(PcgState *st, ReduceBuf red, PcgConfig cfg, int mode, cudaStream_t s)
+    {
+        k_finalize<<<1, FIN_THREADS, 0, s>>>(st, red, cfg, mode);
+        cuda_check(cudaGetLastError(), "finalize launch");
     }
 
     void launch_restrict_plain(const BankedView &A, const MasView &mas, const double *r, cudaStream_t s)

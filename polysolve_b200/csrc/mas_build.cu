@@ -197,15 +197,18 @@ namespace pmas
                 if (tid == 0 && (!isfinite(piv) || piv == 0.0))
                     bad = 1;
                 for (int t = tid; t < N; t += nt)
-                    col[t] = (t == p) ? 0.0 : (t < p ? A[t * N + p] : A[p * N + t]);
+                {
+                    const double ct = (t == p) ? 0.0 : (t < p ? A[t * N + p] : A[p * N + t]);
+                    col[t] = ct;
+                    col[N + t] = ct / piv; // the row scale, one division per row
+                }
                 __syncthreads();
                 for (int e = tid; e < N * N; e += nt)
                 {
                     const int t = e / N, c = e - t * N;
                     if (t > c || t == p || c == p)
                         continue;
-                    const double scale = col[t] / piv;
-                    const double u = A[t * N + c] - scale * col[c];
+                    const double u = A[t * N + c] - col[N + t] * col[c];
                     if (!isfinite(u))
                         bad = 1;
                     A[t * N + c] = u;
@@ -213,7 +216,7 @@ namespace pmas
                 __syncthreads();
                 for (int t = tid; t < N; t += nt)
                 {
-                    const double u = (t == p) ? -1.0 / piv : col[t] / piv;
+                    const double u = (t == p) ? -1.0 / piv : col[N + t];
                     if (!isfinite(u))
                         bad = 1;
                     else if (t <= p)
@@ -447,7 +450,7 @@ namespace pmas
                                  cudaStream_t s)
         {
             constexpr int N = 32 * BD;
-            const size_t smem = (size_t)(N * N + N) * sizeof(double);
+            const size_t smem = (size_t)(N * N + 2 * N) * sizeof(double);
             cuda_check(cudaFuncSetAttribute(k_assemble_invert_lv0<BD, Out>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)smem),
                        "assemble smem attribute");

@@ -192,6 +192,8 @@ struct mas_solver
     int device = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr; // own_stream or the caller's (mas_set_stream)
+    cudaStream_t side = nullptr;   // coarse levels, concurrent with the level-0 MAS kernel
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::string last_error;
 
     // Kernel accounting: launches per kind, and CUDA-event time per kind when profiling.
@@ -252,6 +254,12 @@ struct mas_solver
             cudaGraphExecDestroy(graph_exec);
         if (h_st)
             cudaFreeHost(h_st);
+        if (ev_fork)
+            cudaEventDestroy(ev_fork);
+        if (ev_join)
+            cudaEventDestroy(ev_join);
+        if (side)
+            cudaStreamDestroy(side);
         if (own_stream)
             cudaStreamDestroy(own_stream);
     }
@@ -282,13 +290,19 @@ struct mas_solver
     template <class F>
     void run(const char *kind, int kernels, F &&f)
     {
+        run_on(stream, kind, kernels, std::forward<F>(f));
+    }
+
+    template <class F>
+    void run_on(cudaStream_t on, const char *kind, int kernels, F &&f)
+    {
         const int idx = stat_index(kind);
         cudaEvent_t a = nullptr, b = nullptr;
         if (p.profile)
         {
             a = pool_event();
             b = pool_event();
-            cuda_check(cudaEventRecord(a, stream), "event");
+            cuda_check(cudaEventRecord(a, on), "event");
         }
         if constexpr (std::is_same_v<decltype(f()), int>)
             kernels = f();
@@ -313,9 +327,23 @@ struct mas_solver
         }
         if (p.profile)
         {
-            cuda_check(cudaEventRecord(b, stream), "event");
+            cuda_check(cudaEventRecord(b, on), "event");
             ev_pending.push_back({idx, {a, b}});
         }
+    }
+
+    // The MAS apply of r: coarse levels on the side stream, concurrent with the level-0 kernel,
+    // then the one-CTA finalize after the join. mode 1 = initial, 2 = iteration.
+    void apply_and_finalize(const MasView &mv, const PcgConfig &cfg, int pr, int mode)
+    {
+        PcgState *S = st.get();
+        cuda_check(cudaEventRecord(ev_fork, stream), "fork");
+        cuda_check(cudaStreamWaitEvent(side, ev_fork, 0), "fork");
+        run_on(side, "mas_coarse", 0, [&] { return launch_coarse(mv, S, red(), mode, pr, side); });
+        cuda_check(cudaEventRecord(ev_join, side), "join");
+        run("mas_symv0", 1, [&] { launch_symv0(mv, r.get(), z.get(), S, red(), cfg, 0, mode, stream); });
+        cuda_check(cudaStreamWaitEvent(stream, ev_join, 0), "join");
+        run("finalize", 1, [&] { launch_finalize(S, red(), cfg, mode, stream); });
     }
 
     void collect_profile()
@@ -340,6 +368,11 @@ struct mas_solver
         }
         cuda_check(cudaGetDevice(&device), "get device");
         cuda_check(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking), "stream create");
+        int lo = 0, hi = 0;
+        cuda_check(cudaDeviceGetStreamPriorityRange(&lo, &hi), "stream priorities");
+        cuda_check(cudaStreamCreateWithPriority(&side, cudaStreamNonBlocking, hi), "stream create");
+        cuda_check(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming), "event create");
+        cuda_check(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming), "event create");
         stream = own_stream;
         cuda_check(cudaMallocHost(&h_st, 2 * sizeof(PcgState)), "pinned state");
     }
@@ -439,8 +472,8 @@ struct mas_solver
         Ap.alloc(len, "device_buffers Ap");
         io.alloc((size_t)n_ > len ? (size_t)n_ : len, "device_buffers io");
         st.alloc(1, "device_buffers scalars");
-        red_capacity = std::max((banks + 7) / 8, mas.total_coarse) + 160;
-        partials.alloc((size_t)red_capacity * 2, "device_buffers reduction");
+        red_capacity = std::max({(banks + 7) / 8, mas.total_coarse, device_sm_count() * 8}) + 160;
+        partials.alloc((size_t)red_capacity * 7, "device_buffers reduction");
         cuda_check(cudaMemsetAsync(x.get(), 0, x.bytes(), stream), "memset");
         cuda_check(cudaMemsetAsync(pv.get(), 0, pv.bytes(), stream), "memset");
         cuda_check(cudaMemsetAsync(z.get(), 0, z.bytes(), stream), "memset");
@@ -456,7 +489,12 @@ struct mas_solver
             throw Error(ERR_NOT_FACTORIZED, "[MAS] Size mismatch. Did you forget to call factorize?");
     }
 
-    ReduceBuf red() { return ReduceBuf{partials.get(), red_capacity}; }
+    ReduceBuf red()
+    {
+        double *base = partials.get();
+        const size_t c = (size_t)red_capacity;
+        return ReduceBuf{base, red_capacity, base + 2 * c, base + 3 * c, base + 5 * c};
+    }
 
     PcgConfig config() const
     {
@@ -482,8 +520,7 @@ struct mas_solver
         if (!host_knows_k || k % P == 0)
             run("spmv_residual", 1,
                 [&] { launch_spmv(SPMV_RESIDUAL, Av, x.get(), r.get(), b.get(), &mv, S, red(), 1, P, stream); });
-        run("mas_coarse", 0, [&] { return launch_coarse(mv, S, red(), 2, pr, stream); });
-        run("mas_symv0", 1, [&] { launch_symv0(mv, r.get(), z.get(), S, red(), cfg, 0, 2, stream); });
+        apply_and_finalize(mv, cfg, pr, 2);
         run("update_p", 1, [&] { launch_update_p(mv, pv.get(), z.get(), S, 0, stream); });
     }
 
@@ -567,8 +604,7 @@ struct mas_solver
         const int pr = p.polak_ribiere ? 1 : 0;
         // r = b - A x, its level-0 restriction and rr0
         run("spmv_residual", 1, [&] { launch_spmv(SPMV_RESIDUAL, Av, x.get(), r.get(), b.get(), &mv, S, red(), 0, 0, stream); });
-        run("mas_coarse", 0, [&] { return launch_coarse(mv, S, red(), 1, pr, stream); });
-        run("mas_symv0", 1, [&] { launch_symv0(mv, r.get(), z.get(), S, red(), cfg, 0, 1, stream); });
+        apply_and_finalize(mv, cfg, pr, 1);
         run("update_p", 1, [&] { launch_update_p(mv, pv.get(), z.get(), S, 1, stream); });
         cuda_check(cudaMemcpyAsync(&h_st[0], S, sizeof(PcgState), cudaMemcpyDeviceToHost, stream), "state");
         cuda_check(cudaStreamSynchronize(stream), "pcg init");

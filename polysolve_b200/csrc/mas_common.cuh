@@ -26,6 +26,24 @@ namespace pmas
         return v;
     }
 
+    // Deterministic CTA-wide sum; the result is valid in thread 0. Every thread must call it.
+    template <int THREADS>
+    __device__ __forceinline__ double block_sum(double v)
+    {
+        __shared__ double sh[THREADS / 32];
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        v = warp_sum(v);
+        __syncthreads();
+        if (lane == 0)
+            sh[w] = v;
+        __syncthreads();
+        double t = 0.0;
+        if (threadIdx.x == 0)
+            for (int i = 0; i < THREADS / 32; ++i)
+                t += sh[i];
+        return t;
+    }
+
     // Deterministic grid-wide sum of NV values per CTA: every CTA writes its block sum to
     // partials[blockIdx.x * NV + i]; the last CTA to arrive (atomic ticket) adds the partials in
     // a fixed order. Returns true in the last CTA, with tot[] the totals (valid in all its

@@ -162,6 +162,7 @@ namespace pmas
         int done;      // 1: converged / stopped; kernels return immediately
         int status;    // MAS_STATUS_*
         int error;     // device-detected error code (ERR_NONFINITE, ERR_TIMEOUT)
+        int n_rr, n_rz, n_co; // CTAs that wrote rr_parts / rz_parts / co_parts this iteration
         unsigned int counter[8];
     };
 
@@ -175,10 +176,16 @@ namespace pmas
     };
 
     // Scratch for deterministic two-stage reductions: per-CTA partials.
+    // Per-CTA partial sums. The SpMV's p.Ap uses a ticket (its last CTA sums `partials`); the dots
+    // of the rest of an iteration are written per CTA and summed by the one-CTA finalize kernel, so
+    // short kernels never queue on a ticket counter.
     struct ReduceBuf
     {
-        double *partials; // capacity >= max grid * 2
-        int capacity;
+        double *partials; // 2 * capacity
+        int capacity;     // max CTAs of any reduced launch
+        double *rr_parts; // capacity: r.r from the kernel that produced r this iteration
+        double *rz_parts; // 2 * capacity: r.z0 and r.z0_old from the level-0 MAS kernel
+        double *co_parts; // 2 * capacity: rc.zc and rc.zc_old from the coarse kernel
     };
 
     // ---------------------------------------------------------------------------------------
@@ -238,10 +245,12 @@ namespace pmas
     // Coarse levels: hierarchical sums of the level-0 component sums, then every coarse matrix
     // times its residual (zc) and, in PCG modes, rc . zc (and rc . zc_old) into the state.
     int launch_coarse(const MasView &mas, PcgState *st, ReduceBuf red, int mode, int polak_ribiere, cudaStream_t s);
-    // Level-0 subdomains: z0 = A_0^-1 r per bank; in PCG modes r . z0 and the iteration's
-    // bookkeeping (rz = r . z0 + rc . zc, convergence test, beta) in the last CTA.
+    // Level-0 subdomains: z0 = A_0^-1 r per bank; in PCG modes per-CTA r . z0 (and r . z0_old).
     void launch_symv0(const MasView &mas, const double *r, double *z0, PcgState *st, ReduceBuf red, PcgConfig cfg,
                       int iter, int mode, cudaStream_t s);
+    // One CTA: sums the iteration's partials (rr, r.z0, rc.zc) and runs the reference's per-iteration
+    // bookkeeping (rz, convergence test, status, beta; MASSolver.cu:505, 526-583). mode 1 = initial.
+    void launch_finalize(PcgState *st, ReduceBuf red, PcgConfig cfg, int mode, cudaStream_t s);
     void launch_restrict_plain(const BankedView &A, const MasView &mas, const double *r, cudaStream_t s);
     // z = z0 + prolongation(zc) (outside the PCG loop).
     void launch_prolong(const MasView &mas, const double *z0, double *z, cudaStream_t s);

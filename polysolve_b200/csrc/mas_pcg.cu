@@ -50,10 +50,10 @@ namespace pmas
     {
         constexpr int UPD_THREADS = 256;
 
-        // Warps stride over banks (about four CTAs per SM, so few CTAs contend for the reduction
-        // ticket); a bank's 32 * BD contiguous values are read and written with coalesced accesses
-        // (value e = t * 32 + lane); the node view for the level-0 restriction goes through shared
-        // memory. On a true-residual iteration only x is updated.
+        // Warps stride over banks; a bank's 32 * BD contiguous values are read and written with
+        // coalesced accesses (value e = t * 32 + lane); the node view for the level-0 restriction
+        // goes through shared memory. r.r is written per CTA (summed by the finalize kernel). On a
+        // true-residual iteration only x is updated.
         template <int BD>
         __global__ void __launch_bounds__(UPD_THREADS) k_update_xr(int banks, double *__restrict__ x, double *__restrict__ r,
                                                                    const double *__restrict__ p,
@@ -104,9 +104,13 @@ namespace pmas
             }
             if (due)
                 return;
-            double v1[1] = {part}, tot[1];
-            if (grid_reduce<1, UPD_THREADS>(v1, red.partials, &st->counter[1], tot) && threadIdx.x == 0)
-                st->rr = tot[0];
+            const double rr = block_sum<UPD_THREADS>(part);
+            if (threadIdx.x == 0)
+            {
+                red.rr_parts[blockIdx.x] = rr;
+                if (blockIdx.x == 0)
+                    st->n_rr = gridDim.x;
+            }
         }
 
         // p = z0 + sum_l zc[cslot_l(node)] + beta p; warps stride over banks, coalesced.
@@ -190,7 +194,7 @@ namespace pmas
         int bank_grid(int banks)
         {
             const int need = (banks + UPD_THREADS / 32 - 1) / (UPD_THREADS / 32);
-            const int cap = device_sm_count() * 4;
+            const int cap = device_sm_count() * 8;
             return need < cap ? need : cap;
         }
     } // namespace

@@ -106,6 +106,18 @@ namespace pmas
             }
             if (MODE == SPMV_PLAIN)
                 return;
+            if (MODE == SPMV_RESIDUAL && period > 0)
+            {
+                // In-loop true residual: per-CTA r.r partials, summed by the finalize kernel.
+                const double rr = block_sum<SPMV_THREADS>(part);
+                if (threadIdx.x == 0)
+                {
+                    red.rr_parts[blockIdx.x] = rr;
+                    if (blockIdx.x == 0)
+                        st->n_rr = gridDim.x;
+                }
+                return;
+            }
             // rr0 = ||b||^2: equal to the reference's r.r at x = 0 (MASSolver.cu:488-494), and keeps
             // "relative" relative to ||b|| when an initial guess is used.
             double v2[2] = {part, bb}, tot[2];
