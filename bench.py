@@ -45,7 +45,7 @@ UNIT = "ms/solve"
 TOL = 1e-8
 
 CHOSEN = {"block_dim": 3, "relative_tolerance": TOL, "absolute_tolerance": 0.0, "max_iter": 5000,
-          "precision": "fp32", "true_residual_period": 50, "check_period": 1, "poll_period": 8,
+          "precision": "fp32", "true_residual_period": 50, "check_period": 1, "poll_period": 10,
           "cuda_graphs": True}
 # The reference's algorithm: FP64 MAS, true residual every 4, convergence test every 10 iterations,
 # iterations launched from the host (MASSolver.cu:498-583).

@@ -4,8 +4,8 @@
 // warp segmented sums plus FP64 atomics, multiplies every level's packed 96 x 96 inverse with one
 // 96-thread CTA each (symv_upper_packed, :665-705), and prolongs in a third kernel. Here:
 //
-//  * the level-0 restriction (per-bank sums of each connected component) is fused into the
-//    kernel that produced r (SpMV residual or the x/r update), deterministic;
+//  * k_restrict: the level-0 restriction (per-bank sums of each connected component),
+//    deterministic, first kernel of the coarse chain;
 //  * k_coarse_sum: coarse level l sums from level l-1 (every level-l component merges at most 32
 //    level-(l-1) components of one bank), one warp per component, one launch per level;
 //  * k_coarse_symv: one CTA per coarse matrix (one warp per column tile, matrix read from global
@@ -486,21 +486,32 @@ namespace pmas
             }
         }
 
-        // Level-0 restriction of a plain vector (used outside the PCG loop).
+        // Level-0 restriction: per bank, the sum of r over each connected component (first coarse
+        // level). One warp per bank; the bank's 32 * BD values are read coalesced and regrouped by
+        // node through shared memory; sums in a fixed order (deterministic).
         template <int BD>
-        __global__ void k_restrict(int banks, const double *__restrict__ r, const int *__restrict__ lcco0,
-                                   const int *__restrict__ cco0_base, double *rc)
+        __global__ void __launch_bounds__(256) k_restrict(int banks, const double *__restrict__ r,
+                                                          const int *__restrict__ lcco0,
+                                                          const int *__restrict__ cco0_base, double *rc,
+                                                          const PcgState *st)
         {
-            const int lane = threadIdx.x & 31;
-            const int bank = blockIdx.x * 8 + (threadIdx.x >> 5);
+            __shared__ double sv[8][32 * BD];
+            if (st && st->done)
+                return;
+            const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+            const int bank = blockIdx.x * 8 + w;
             if (bank >= banks)
                 return;
-            const long long u = (long long)bank * 32 + lane;
+            const long long b0 = (long long)bank * 32 * BD;
+#pragma unroll
+            for (int t = 0; t < BD; ++t)
+                sv[w][t * 32 + lane] = r[b0 + t * 32 + lane];
+            __syncwarp();
             double rv[BD];
 #pragma unroll
             for (int i = 0; i < BD; ++i)
-                rv[i] = r[u * BD + i];
-            warp_segment_store<BD>(rv, lcco0[u], cco0_base[bank], rc);
+                rv[i] = sv[w][lane * BD + i];
+            warp_segment_store<BD>(rv, lcco0[(long long)bank * 32 + lane], cco0_base[bank], rc);
         }
 
         template <int BD>
@@ -540,15 +551,22 @@ namespace pmas
         }
 
         template <int BD, class Real>
-        int coarse_launch(const MasView &mas, PcgState *st, ReduceBuf red, int mode, int pr, cudaStream_t s)
+        int coarse_launch(const MasView &mas, const double *r, PcgState *st, ReduceBuf red, int mode, int pr,
+                          cudaStream_t s)
         {
+            int launches = 0;
+            if (mas.banks > 0)
+            {
+                k_restrict<BD><<<(mas.banks + 7) / 8, 256, 0, s>>>(mas.banks, r, mas.lcco0, mas.cco0_base, mas.rc,
+                                                                  mode ? st : nullptr);
+                ++launches;
+            }
             if (mas.total_coarse == 0)
             {
                 if (mode != 0)
                     cuda_check(cudaMemsetAsync(&st->n_co, 0, sizeof(int), s), "memset");
-                return 0;
+                return launches;
             }
-            int launches = 0;
             for (int l = 1; l < mas.level_num; ++l)
             {
                 const int count = mas.cco_nums[l];
@@ -640,21 +658,22 @@ namespace pmas
         }
     }
 
-    int launch_coarse(const MasView &mas, PcgState *st, ReduceBuf red, int mode, int pr, cudaStream_t s)
+    int launch_coarse(const MasView &mas, const double *r, PcgState *st, ReduceBuf red, int mode, int pr,
+                      cudaStream_t s)
     {
         if (mas.fp32)
         {
             if (mas.bd == 1)
-                return coarse_launch<1, float>(mas, st, red, mode, pr, s);
+                return coarse_launch<1, float>(mas, r, st, red, mode, pr, s);
             if (mas.bd == 2)
-                return coarse_launch<2, float>(mas, st, red, mode, pr, s);
-            return coarse_launch<3, float>(mas, st, red, mode, pr, s);
+                return coarse_launch<2, float>(mas, r, st, red, mode, pr, s);
+            return coarse_launch<3, float>(mas, r, st, red, mode, pr, s);
         }
         if (mas.bd == 1)
-            return coarse_launch<1, double>(mas, st, red, mode, pr, s);
+            return coarse_launch<1, double>(mas, r, st, red, mode, pr, s);
         if (mas.bd == 2)
-            return coarse_launch<2, double>(mas, st, red, mode, pr, s);
-        return coarse_launch<3, double>(mas, st, red, mode, pr, s);
+            return coarse_launch<2, double>(mas, r, st, red, mode, pr, s);
+        return coarse_launch<3, double>(mas, r, st, red, mode, pr, s);
     }
 
     void launch_symv0(const MasView &mas, const double *r, double *z, PcgState *st, ReduceBuf red, PcgConfig cfg,
@@ -684,20 +703,6 @@ namespace pmas
     {
         k_finalize<<<1, FIN_THREADS, 0, s>>>(st, red, cfg, mode);
         cuda_check(cudaGetLastError(), "finalize launch");
-    }
-
-    void launch_restrict_plain(const BankedView &A, const MasView &mas, const double *r, cudaStream_t s)
-    {
-        const int grid = (A.banks + 7) / 8;
-        if (grid == 0)
-            return;
-        if (A.bd == 1)
-            k_restrict<1><<<grid, 256, 0, s>>>(A.banks, r, mas.lcco0, mas.cco0_base, mas.rc);
-        else if (A.bd == 2)
-            k_restrict<2><<<grid, 256, 0, s>>>(A.banks, r, mas.lcco0, mas.cco0_base, mas.rc);
-        else
-            k_restrict<3><<<grid, 256, 0, s>>>(A.banks, r, mas.lcco0, mas.cco0_base, mas.rc);
-        cuda_check(cudaGetLastError(), "restrict launch");
     }
 
     void launch_prolong(const MasView &mas, const double *z0, double *z, cudaStream_t s)

@@ -47,7 +47,7 @@ namespace
         bool initial_guess_input = false;
         bool polak_ribiere = false;
         std::string ordering = "auto";
-        int poll_period = 8;
+        int poll_period = 10;
         bool profile = false; // time every kernel launch with CUDA events
         bool graphs = true;   // replay chunks of iterations as a CUDA graph
     };
@@ -208,11 +208,16 @@ struct mas_solver
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
     size_t ev_used = 0;
 
-    // CUDA graph of `graph_chunk` PCG iterations, replayed until the device flags done.
-    cudaGraphExec_t graph_exec = nullptr;
+    // CUDA graphs of `chunk` PCG iterations, replayed until the device flags done. When the
+    // true-residual period is a multiple of the chunk, graph[0] has no true-residual SpMV and
+    // graph[1] recomputes it in its last iteration; otherwise graph[0] launches the (device-gated)
+    // true-residual SpMV in every iteration.
+    cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
     uint64_t graph_key = 0;
+    bool graph_aligned = false;
     bool capturing = false;
-    std::vector<std::pair<int, long long>> graph_counts; // kernels per kind in one replay
+    std::vector<std::pair<int, long long>> graph_counts[2]; // kernels per kind in one replay
+    int capture_slot = 0;
 
     // Info of the last solve (MASSolver.cu:145-149).
     int iterations = 0;
@@ -250,8 +255,9 @@ struct mas_solver
         }
         for (cudaEvent_t e : ev_pool)
             cudaEventDestroy(e);
-        if (graph_exec)
-            cudaGraphExecDestroy(graph_exec);
+        for (auto &g : graph_exec)
+            if (g)
+                cudaGraphExecDestroy(g);
         if (h_st)
             cudaFreeHost(h_st);
         if (ev_fork)
@@ -311,14 +317,14 @@ struct mas_solver
         if (capturing)
         {
             bool found = false;
-            for (auto &gc : graph_counts)
+            for (auto &gc : graph_counts[capture_slot])
                 if (gc.first == idx)
                 {
                     gc.second += kernels;
                     found = true;
                 }
             if (!found)
-                graph_counts.push_back({idx, kernels});
+                graph_counts[capture_slot].push_back({idx, kernels});
         }
         else
         {
@@ -339,7 +345,7 @@ struct mas_solver
         PcgState *S = st.get();
         cuda_check(cudaEventRecord(ev_fork, stream), "fork");
         cuda_check(cudaStreamWaitEvent(side, ev_fork, 0), "fork");
-        run_on(side, "mas_coarse", 0, [&] { return launch_coarse(mv, S, red(), mode, pr, side); });
+        run_on(side, "mas_coarse", 0, [&] { return launch_coarse(mv, r.get(), S, red(), mode, pr, side); });
         cuda_check(cudaEventRecord(ev_join, side), "join");
         run("mas_symv0", 1, [&] { launch_symv0(mv, r.get(), z.get(), S, red(), cfg, 0, mode, stream); });
         cuda_check(cudaStreamWaitEvent(stream, ev_join, 0), "join");
@@ -508,29 +514,59 @@ struct mas_solver
         return c;
     }
 
-    // One PCG iteration's kernels (MASSolver.cu:498-583). With host_knows_k the true-residual
-    // SpMV is only launched on its iterations; in a captured graph it is always launched and
-    // returns at once unless (st->iter + 1) % P == 0.
-    void launch_iteration(const BankedView &Av, const MasView &mv, const PcgConfig &cfg, int P, int pr, bool host_knows_k,
-                          int k)
+    // One PCG iteration's kernels (MASSolver.cu:498-583). residual: launch the true-residual SpMV
+    // (it also checks (st->iter + 1) % P == 0 on the device and returns at once otherwise).
+    void launch_iteration(const BankedView &Av, const MasView &mv, const PcgConfig &cfg, int P, int pr, bool residual)
     {
         PcgState *S = st.get();
-        run("spmv_pap", 1, [&] { launch_spmv(SPMV_PAP, Av, pv.get(), Ap.get(), nullptr, &mv, S, red(), 1, 0, stream); });
-        run("update_xr", 1, [&] { launch_update_xr(Av, mv, x.get(), r.get(), pv.get(), Ap.get(), S, red(), P, stream); });
-        if (!host_knows_k || k % P == 0)
+        run("spmv_pap", 1, [&] { launch_spmv(SPMV_PAP, Av, pv.get(), Ap.get(), nullptr, S, red(), 1, 0, stream); });
+        run("update_xr", 1, [&] { launch_update_xr(banks, bd, x.get(), r.get(), pv.get(), Ap.get(), S, red(), P, stream); });
+        if (residual)
             run("spmv_residual", 1,
-                [&] { launch_spmv(SPMV_RESIDUAL, Av, x.get(), r.get(), b.get(), &mv, S, red(), 1, P, stream); });
+                [&] { launch_spmv(SPMV_RESIDUAL, Av, x.get(), r.get(), b.get(), S, red(), 1, P, stream); });
         apply_and_finalize(mv, cfg, pr, 2);
         run("update_p", 1, [&] { launch_update_p(mv, pv.get(), z.get(), S, 0, stream); });
     }
 
     void drop_graph()
     {
-        if (graph_exec)
-            cudaGraphExecDestroy(graph_exec);
-        graph_exec = nullptr;
+        for (int i = 0; i < 2; ++i)
+        {
+            if (graph_exec[i])
+                cudaGraphExecDestroy(graph_exec[i]);
+            graph_exec[i] = nullptr;
+            graph_counts[i].clear();
+        }
         graph_key = 0;
-        graph_counts.clear();
+    }
+
+    void capture(int slot, const BankedView &Av, const MasView &mv, const PcgConfig &cfg, int P, int pr, int chunk,
+                 bool aligned)
+    {
+        cudaGraph_t graph = nullptr;
+        capture_slot = slot;
+        cuda_check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        capturing = true;
+        try
+        {
+            for (int i = 0; i < chunk; ++i)
+                launch_iteration(Av, mv, cfg, P, pr, aligned ? (slot == 1 && i == chunk - 1) : true);
+        }
+        catch (...)
+        {
+            capturing = false;
+            cudaStreamEndCapture(stream, &graph);
+            if (graph)
+                cudaGraphDestroy(graph);
+            cudaGetLastError();
+            graph_counts[slot].clear();
+            throw;
+        }
+        capturing = false;
+        cuda_check(cudaStreamEndCapture(stream, &graph), "end capture");
+        cudaError_t e = cudaGraphInstantiate(&graph_exec[slot], graph, 0);
+        cudaGraphDestroy(graph);
+        cuda_check(e, "graph instantiate");
     }
 
     void ensure_graph(const BankedView &Av, const MasView &mv, const PcgConfig &cfg, int P, int pr, int chunk)
@@ -557,32 +593,13 @@ struct mas_solver
         mix((uint64_t)P);
         mix((uint64_t)pr);
         mix((uint64_t)chunk);
-        if (graph_exec && key == graph_key)
+        if (graph_exec[0] && key == graph_key)
             return;
         drop_graph();
-        cudaGraph_t graph = nullptr;
-        cuda_check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
-        capturing = true;
-        try
-        {
-            for (int i = 0; i < chunk; ++i)
-                launch_iteration(Av, mv, cfg, P, pr, false, 0);
-        }
-        catch (...)
-        {
-            capturing = false;
-            cudaStreamEndCapture(stream, &graph);
-            if (graph)
-                cudaGraphDestroy(graph);
-            cudaGetLastError();
-            graph_counts.clear();
-            throw;
-        }
-        capturing = false;
-        cuda_check(cudaStreamEndCapture(stream, &graph), "end capture");
-        cudaError_t e = cudaGraphInstantiate(&graph_exec, graph, 0);
-        cudaGraphDestroy(graph);
-        cuda_check(e, "graph instantiate");
+        graph_aligned = (P % chunk == 0);
+        capture(0, Av, mv, cfg, P, pr, chunk, graph_aligned);
+        if (graph_aligned)
+            capture(1, Av, mv, cfg, P, pr, chunk, true);
         graph_key = key;
     }
 
@@ -603,7 +620,7 @@ struct mas_solver
         launch_pcg_init_state(S, stream);
         const int pr = p.polak_ribiere ? 1 : 0;
         // r = b - A x, its level-0 restriction and rr0
-        run("spmv_residual", 1, [&] { launch_spmv(SPMV_RESIDUAL, Av, x.get(), r.get(), b.get(), &mv, S, red(), 0, 0, stream); });
+        run("spmv_residual", 1, [&] { launch_spmv(SPMV_RESIDUAL, Av, x.get(), r.get(), b.get(), S, red(), 0, 0, stream); });
         apply_and_finalize(mv, cfg, pr, 1);
         run("update_p", 1, [&] { launch_update_p(mv, pv.get(), z.get(), S, 1, stream); });
         cuda_check(cudaMemcpyAsync(&h_st[0], S, sizeof(PcgState), cudaMemcpyDeviceToHost, stream), "state");
@@ -634,8 +651,9 @@ struct mas_solver
             const int k1 = std::min(p.max_iter, k0 + chunk - 1);
             if (graphs)
             {
-                cuda_check(cudaGraphLaunch(graph_exec, stream), "graph launch");
-                for (auto &gc : graph_counts)
+                const int g = (graph_aligned && (k0 + chunk - 1) % P == 0) ? 1 : 0;
+                cuda_check(cudaGraphLaunch(graph_exec[g], stream), "graph launch");
+                for (auto &gc : graph_counts[g])
                 {
                     kstats[gc.first].second.launches += gc.second;
                     total_launches += gc.second;
@@ -643,7 +661,7 @@ struct mas_solver
             }
             else
                 for (int k = k0; k <= k1; ++k)
-                    launch_iteration(Av, mv, cfg, P, pr, true, k);
+                    launch_iteration(Av, mv, cfg, P, pr, k % P == 0);
             launched = k1;
             const int slot = (slot_flip++) & 1;
             cuda_check(cudaMemcpyAsync(&h_st[slot], S, sizeof(PcgState), cudaMemcpyDeviceToHost, stream), "state");
@@ -1095,8 +1113,7 @@ extern "C" int mas_debug_spmv(mas_solver *h, const double *xin, double *y, int l
         if (!h->factorized || len != h->banks * 32 * h->bd)
             throw Error(ERR_NOT_FACTORIZED, "[MAS] debug_spmv: size mismatch.");
         cuda_check(cudaMemcpyAsync(h->x.get(), xin, sizeof(double) * len, cudaMemcpyHostToDevice, h->stream), "x");
-        launch_spmv(SPMV_PLAIN, h->A.view(), h->x.get(), h->Ap.get(), nullptr, nullptr, nullptr, h->red(), 0, 0,
-                    h->stream);
+        launch_spmv(SPMV_PLAIN, h->A.view(), h->x.get(), h->Ap.get(), nullptr, nullptr, h->red(), 0, 0, h->stream);
         cuda_check(cudaMemcpyAsync(y, h->Ap.get(), sizeof(double) * len, cudaMemcpyDeviceToHost, h->stream), "y");
         cuda_check(cudaStreamSynchronize(h->stream), "spmv");
     });
@@ -1112,8 +1129,7 @@ extern "C" int mas_debug_apply(mas_solver *h, const double *rin, double *zout, i
             throw Error(ERR_NOT_FACTORIZED, "[MAS] debug_apply: size mismatch.");
         cuda_check(cudaMemcpyAsync(h->r.get(), rin, sizeof(double) * len, cudaMemcpyHostToDevice, h->stream), "r");
         const MasView mv = h->mas.view();
-        launch_restrict_plain(h->A.view(), mv, h->r.get(), h->stream);
-        launch_coarse(mv, nullptr, h->red(), 0, 0, h->stream);
+        launch_coarse(mv, h->r.get(), nullptr, h->red(), 0, 0, h->stream);
         launch_symv0(mv, h->r.get(), h->z.get(), nullptr, h->red(), h->config(), 0, 0, h->stream);
         launch_prolong(mv, h->z.get(), h->Ap.get(), h->stream);
         cuda_check(cudaMemcpyAsync(zout, h->Ap.get(), sizeof(double) * len, cudaMemcpyDeviceToHost, h->stream), "z");

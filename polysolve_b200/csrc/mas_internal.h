@@ -225,14 +225,14 @@ namespace pmas
         SPMV_RESIDUAL = 2, // y = b - A x ; restrict y to level-0 components ; rr = y . y
     };
     // period > 0 (SPMV_RESIDUAL in the PCG loop): runs only when (st->iter + 1) % period == 0.
-    void launch_spmv(int mode, const BankedView &A, const double *x, double *y, const double *b, const MasView *mas,
-                     PcgState *st, ReduceBuf red, int iter, int period, cudaStream_t s);
+    void launch_spmv(int mode, const BankedView &A, const double *x, double *y, const double *b, PcgState *st,
+                     ReduceBuf red, int iter, int period, cudaStream_t s);
 
     // mas_pcg.cu
     // x += alpha p; unless this iteration recomputes the true residual ((st->iter + 1) % period == 0):
-    // r -= alpha Ap, rr = r . r and the level-0 restriction of r.
-    void launch_update_xr(const BankedView &A, const MasView &mas, double *x, double *r, const double *p,
-                          const double *Ap, PcgState *st, ReduceBuf red, int period, cudaStream_t s);
+    // r -= alpha Ap and per-CTA r . r.
+    void launch_update_xr(int banks, int bd, double *x, double *r, const double *p, const double *Ap, PcgState *st,
+                          ReduceBuf red, int period, cudaStream_t s);
     // p = z0 + prolongation(zc) + beta p (z0: level-0 part of z = M^-1 r)
     void launch_update_p(const MasView &mas, double *p, const double *z0, PcgState *st, int first, cudaStream_t s);
     void launch_permute_in(int n, int bd, int V, const int *padded_of_block, const double *src, double *dst,
@@ -242,16 +242,17 @@ namespace pmas
     void launch_pcg_init_state(PcgState *st, cudaStream_t s);
 
     // mas_apply.cu. mode: 0 = plain apply (no PCG bookkeeping), 1 = initial (rz0), 2 = iteration.
-    // Coarse levels: hierarchical sums of the level-0 component sums, then every coarse matrix
-    // times its residual (zc) and, in PCG modes, rc . zc (and rc . zc_old) into the state.
-    int launch_coarse(const MasView &mas, PcgState *st, ReduceBuf red, int mode, int polak_ribiere, cudaStream_t s);
+    // Coarse levels: level-0 restriction of r (per-bank component sums), hierarchical sums of the
+    // higher levels, then every coarse matrix times its residual (zc) and, in PCG modes, per-CTA
+    // rc . zc (and rc . zc_old). Returns the number of kernels launched.
+    int launch_coarse(const MasView &mas, const double *r, PcgState *st, ReduceBuf red, int mode, int polak_ribiere,
+                      cudaStream_t s);
     // Level-0 subdomains: z0 = A_0^-1 r per bank; in PCG modes per-CTA r . z0 (and r . z0_old).
     void launch_symv0(const MasView &mas, const double *r, double *z0, PcgState *st, ReduceBuf red, PcgConfig cfg,
                       int iter, int mode, cudaStream_t s);
     // One CTA: sums the iteration's partials (rr, r.z0, rc.zc) and runs the reference's per-iteration
     // bookkeeping (rz, convergence test, status, beta; MASSolver.cu:505, 526-583). mode 1 = initial.
     void launch_finalize(PcgState *st, ReduceBuf red, PcgConfig cfg, int mode, cudaStream_t s);
-    void launch_restrict_plain(const BankedView &A, const MasView &mas, const double *r, cudaStream_t s);
     // z = z0 + prolongation(zc) (outside the PCG loop).
     void launch_prolong(const MasView &mas, const double *z0, double *z, cudaStream_t s);
     // Set kernel attributes (large shared memory) for every variant used with this block size and

@@ -2,8 +2,8 @@
 //
 // The reference runs each vector step as its own launch (axpby / inner_product / scalar_division,
 // MASSolver.cu:46-81, InnerProduct.cu:16-45) with a memset and an FP64 atomicAdd per dot. Here:
-//   update_xr: x += alpha p ; r -= alpha Ap ; rr = r . r ; level-0 restriction of r   (one pass;
-//              on true-residual iterations only x, then r = b - A x follows in the SpMV)
+//   update_xr: x += alpha p ; r -= alpha Ap ; rr = r . r            (one pass; on true-residual
+//              iterations only x, then r = b - A x follows in the SpMV)
 //   update_p:  p = z0 + P zc + beta p             (the MAS prolongation fused in; beta from the
 //                                                  device state, set by the MAS apply)
 // alpha / beta are read from the device-resident PcgState, and every dot is a deterministic
@@ -50,60 +50,32 @@ namespace pmas
     {
         constexpr int UPD_THREADS = 256;
 
-        // Warps stride over banks; a bank's 32 * BD contiguous values are read and written with
-        // coalesced accesses (value e = t * 32 + lane); the node view for the level-0 restriction
-        // goes through shared memory. r.r is written per CTA (summed by the finalize kernel). On a
-        // true-residual iteration only x is updated.
-        template <int BD>
-        __global__ void __launch_bounds__(UPD_THREADS) k_update_xr(int banks, double *__restrict__ x, double *__restrict__ r,
-                                                                   const double *__restrict__ p,
-                                                                   const double *__restrict__ Ap,
-                                                                   const int *__restrict__ lcco0,
-                                                                   const int *__restrict__ cco0_base, double *rc,
-                                                                   PcgState *st, ReduceBuf red, int period)
+        // x += alpha p ; r -= alpha Ap ; per-CTA r . r (summed by the finalize kernel). Grid-stride
+        // over the vectors with coalesced accesses. On a true-residual iteration only x is updated.
+        __global__ void __launch_bounds__(UPD_THREADS) k_update_xr(long long len, double *__restrict__ x,
+                                                                   double *__restrict__ r, const double *__restrict__ p,
+                                                                   const double *__restrict__ Ap, PcgState *st,
+                                                                   ReduceBuf red, int period)
         {
-            __shared__ double sv[UPD_THREADS / 32][32 * BD];
             if (st->done)
                 return;
             const double alpha = st->alpha;
             const bool due = period > 0 && (st->iter + 1) % period == 0;
-            const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-            const int total_warps = gridDim.x * (UPD_THREADS / 32);
+            const long long stride = (long long)gridDim.x * UPD_THREADS;
             double part = 0.0;
-            for (int bank = blockIdx.x * (UPD_THREADS / 32) + w; bank < banks; bank += total_warps)
-            {
-                const long long b0 = (long long)bank * 32 * BD;
-                if (due)
-                {
-#pragma unroll
-                    for (int t = 0; t < BD; ++t)
-                    {
-                        const long long idx = b0 + t * 32 + lane;
-                        x[idx] = fma(alpha, p[idx], x[idx]);
-                    }
-                    continue;
-                }
-#pragma unroll
-                for (int t = 0; t < BD; ++t)
-                {
-                    const long long idx = b0 + t * 32 + lane;
-                    const double xv = fma(alpha, p[idx], x[idx]);
-                    const double rv = fma(-alpha, Ap[idx], r[idx]);
-                    x[idx] = xv;
-                    r[idx] = rv;
-                    part = fma(rv, rv, part);
-                    sv[w][t * 32 + lane] = rv;
-                }
-                __syncwarp();
-                double rn[BD];
-#pragma unroll
-                for (int i = 0; i < BD; ++i)
-                    rn[i] = sv[w][lane * BD + i];
-                __syncwarp();
-                warp_segment_store<BD>(rn, lcco0[(long long)bank * 32 + lane], cco0_base[bank], rc);
-            }
             if (due)
+            {
+                for (long long i = blockIdx.x * (long long)UPD_THREADS + threadIdx.x; i < len; i += stride)
+                    x[i] = fma(alpha, p[i], x[i]);
                 return;
+            }
+            for (long long i = blockIdx.x * (long long)UPD_THREADS + threadIdx.x; i < len; i += stride)
+            {
+                x[i] = fma(alpha, p[i], x[i]);
+                const double rv = fma(-alpha, Ap[i], r[i]);
+                r[i] = rv;
+                part = fma(rv, rv, part);
+            }
             const double rr = block_sum<UPD_THREADS>(part);
             if (threadIdx.x == 0)
             {
@@ -199,26 +171,19 @@ namespace pmas
         }
     } // namespace
 
-    void launch_update_xr(const BankedView &A, const MasView &mas, double *x, double *r, const double *p,
-                          const double *Ap, PcgState *st, ReduceBuf red, int period, cudaStream_t s)
+    void launch_update_xr(int banks, int bd, double *x, double *r, const double *p, const double *Ap, PcgState *st,
+                          ReduceBuf red, int period, cudaStream_t s)
     {
-        const int grid = bank_grid(A.banks);
-        if (grid == 0)
-            return;
-        if (grid > red.capacity)
+        const long long len = (long long)banks * 32 * bd;
+        long long g = (len + UPD_THREADS - 1) / UPD_THREADS;
+        const long long cap = (long long)device_sm_count() * 8;
+        if (g > cap)
+            g = cap;
+        if (g < 1)
+            g = 1;
+        if (g > red.capacity)
             throw Error(ERR_INVALID, "[MAS] reduction scratch too small");
-        switch (A.bd)
-        {
-        case 1:
-            k_update_xr<1><<<grid, UPD_THREADS, 0, s>>>(A.banks, x, r, p, Ap, mas.lcco0, mas.cco0_base, mas.rc, st, red, period);
-            break;
-        case 2:
-            k_update_xr<2><<<grid, UPD_THREADS, 0, s>>>(A.banks, x, r, p, Ap, mas.lcco0, mas.cco0_base, mas.rc, st, red, period);
-            break;
-        default:
-            k_update_xr<3><<<grid, UPD_THREADS, 0, s>>>(A.banks, x, r, p, Ap, mas.lcco0, mas.cco0_base, mas.rc, st, red, period);
-            break;
-        }
+        k_update_xr<<<(int)g, UPD_THREADS, 0, s>>>(len, x, r, p, Ap, st, red, period);
         cuda_check(cudaGetLastError(), "update_xr launch");
     }
 

@@ -8,8 +8,7 @@
 //
 // Fused epilogues (one pass over A per PCG step):
 //   SPMV_PAP:      y = A p, pAp = p . y, alpha = rz / pAp (0 if |pAp| < 1e-20, MASSolver.cu:46-56)
-//   SPMV_RESIDUAL: y = b - A x, rr = y . y, and the level-0 restriction of y (per-bank sums of
-//                  each connected component, the first coarse level of the MAS apply).
+//   SPMV_RESIDUAL: y = b - A x, rr = y . y (and ||b||^2 on the initial residual).
 // The dot products are deterministic two-stage reductions (per-CTA partials, last CTA sums).
 
 #include "mas_common.cuh"
@@ -24,8 +23,6 @@ namespace pmas
         template <int BD, int MODE>
         __global__ void __launch_bounds__(SPMV_THREADS) k_spmv(BankedView A, const double *__restrict__ x,
                                                                double *__restrict__ y, const double *__restrict__ b,
-                                                               const int *__restrict__ lcco0,
-                                                               const int *__restrict__ cco0_base, double *rc,
                                                                PcgState *st, ReduceBuf red, int iter, int period)
         {
             constexpr int BS = BD * BD;
@@ -101,7 +98,6 @@ namespace pmas
                         part = fma(rv[i], rv[i], part);
                         bb = fma(bv, bv, bb);
                     }
-                    warp_segment_store<BD>(rv, lcco0[u], cco0_base[bank], rc);
                 }
             }
             if (MODE == SPMV_PLAIN)
@@ -138,46 +134,43 @@ namespace pmas
         }
 
         template <int BD>
-        void launch_bd(int mode, const BankedView &A, const double *x, double *y, const double *b, const MasView *mas,
-                       PcgState *st, ReduceBuf red, int iter, int period, cudaStream_t s)
+        void launch_bd(int mode, const BankedView &A, const double *x, double *y, const double *b, PcgState *st,
+                       ReduceBuf red, int iter, int period, cudaStream_t s)
         {
             const int grid = (A.banks + BANKS_PER_CTA - 1) / BANKS_PER_CTA;
             if (grid == 0)
                 return;
             if (mode != SPMV_PLAIN && grid > red.capacity)
                 throw Error(ERR_INVALID, "[MAS] reduction scratch too small");
-            const int *lcco0 = mas ? mas->lcco0 : nullptr;
-            const int *base = mas ? mas->cco0_base : nullptr;
-            double *rc = mas ? mas->rc : nullptr;
             switch (mode)
             {
             case SPMV_PLAIN:
-                k_spmv<BD, SPMV_PLAIN><<<grid, SPMV_THREADS, 0, s>>>(A, x, y, b, lcco0, base, rc, st, red, iter, period);
+                k_spmv<BD, SPMV_PLAIN><<<grid, SPMV_THREADS, 0, s>>>(A, x, y, b, st, red, iter, period);
                 break;
             case SPMV_PAP:
-                k_spmv<BD, SPMV_PAP><<<grid, SPMV_THREADS, 0, s>>>(A, x, y, b, lcco0, base, rc, st, red, iter, period);
+                k_spmv<BD, SPMV_PAP><<<grid, SPMV_THREADS, 0, s>>>(A, x, y, b, st, red, iter, period);
                 break;
             default:
-                k_spmv<BD, SPMV_RESIDUAL><<<grid, SPMV_THREADS, 0, s>>>(A, x, y, b, lcco0, base, rc, st, red, iter, period);
+                k_spmv<BD, SPMV_RESIDUAL><<<grid, SPMV_THREADS, 0, s>>>(A, x, y, b, st, red, iter, period);
                 break;
             }
             cuda_check(cudaGetLastError(), "spmv launch");
         }
     } // namespace
 
-    void launch_spmv(int mode, const BankedView &A, const double *x, double *y, const double *b, const MasView *mas,
-                     PcgState *st, ReduceBuf red, int iter, int period, cudaStream_t s)
+    void launch_spmv(int mode, const BankedView &A, const double *x, double *y, const double *b, PcgState *st,
+                     ReduceBuf red, int iter, int period, cudaStream_t s)
     {
         switch (A.bd)
         {
         case 1:
-            launch_bd<1>(mode, A, x, y, b, mas, st, red, iter, period, s);
+            launch_bd<1>(mode, A, x, y, b, st, red, iter, period, s);
             break;
         case 2:
-            launch_bd<2>(mode, A, x, y, b, mas, st, red, iter, period, s);
+            launch_bd<2>(mode, A, x, y, b, st, red, iter, period, s);
             break;
         case 3:
-            launch_bd<3>(mode, A, x, y, b, mas, st, red, iter, period, s);
+            launch_bd<3>(mode, A, x, y, b, st, red, iter, period, s);
             break;
         default:
             throw Error(ERR_INVALID, "[MAS] block_dim must be 1, 2 or 3");
