@@ -337,24 +337,28 @@ namespace pmas
             }
         }
 
-        // The iteration's bookkeeping in one CTA: sum the per-CTA partials in a fixed order.
-        constexpr int FIN_THREADS = 256;
+        // The iteration's bookkeeping in one CTA: sum the per-CTA partials in a fixed order (1024
+        // threads, loads unrolled so each thread has its few loads in flight at once).
+        constexpr int FIN_THREADS = 1024;
         __global__ void __launch_bounds__(FIN_THREADS) k_finalize(PcgState *st, ReduceBuf red, PcgConfig cfg, int mode)
         {
             if (st->done)
                 return;
             const int n_rz = st->n_rz, n_co = st->n_co, n_rr = (mode == 2) ? st->n_rr : 0;
             double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll 4
             for (int i = threadIdx.x; i < n_rz; i += FIN_THREADS)
             {
                 v[0] += __ldcg(red.rz_parts + 2 * i);
                 v[1] += __ldcg(red.rz_parts + 2 * i + 1);
             }
+#pragma unroll 4
             for (int i = threadIdx.x; i < n_co; i += FIN_THREADS)
             {
                 v[2] += __ldcg(red.co_parts + 2 * i);
                 v[3] += __ldcg(red.co_parts + 2 * i + 1);
             }
+#pragma unroll 4
             for (int i = threadIdx.x; i < n_rr; i += FIN_THREADS)
                 v[4] += __ldcg(red.rr_parts + i);
             double t[5];
@@ -487,30 +491,42 @@ namespace pmas
         }
 
         // Level-0 restriction: per bank, the sum of r over each connected component (first coarse
-        // level). One warp per bank; the bank's 32 * BD values are read coalesced and regrouped by
-        // node through shared memory; sums in a fixed order (deterministic).
+        // level). One warp per bank; the bank's 32 * BD values are read coalesced (value e = t * 32
+        // + lane) and regrouped by node with shuffles -- no shared memory, so these CTAs fit beside
+        // the level-0 MAS kernel. Sums in a fixed order (deterministic).
         template <int BD>
         __global__ void __launch_bounds__(256) k_restrict(int banks, const double *__restrict__ r,
                                                           const int *__restrict__ lcco0,
                                                           const int *__restrict__ cco0_base, double *rc,
                                                           const PcgState *st)
         {
-            __shared__ double sv[8][32 * BD];
             if (st && st->done)
                 return;
-            const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-            const int bank = blockIdx.x * 8 + w;
+            const int lane = threadIdx.x & 31;
+            const int bank = blockIdx.x * 8 + (threadIdx.x >> 5);
             if (bank >= banks)
                 return;
             const long long b0 = (long long)bank * 32 * BD;
+            double reg[BD];
 #pragma unroll
             for (int t = 0; t < BD; ++t)
-                sv[w][t * 32 + lane] = r[b0 + t * 32 + lane];
-            __syncwarp();
+                reg[t] = r[b0 + t * 32 + lane];
             double rv[BD];
 #pragma unroll
             for (int i = 0; i < BD; ++i)
-                rv[i] = sv[w][lane * BD + i];
+            {
+                const int e = lane * BD + i; // this lane's node component i
+                const int src = e & 31, tsel = e >> 5;
+                double v = 0.0;
+#pragma unroll
+                for (int t = 0; t < BD; ++t)
+                {
+                    const double got = __shfl_sync(FULL, reg[t], src);
+                    if (t == tsel)
+                        v = got;
+                }
+                rv[i] = v;
+            }
             warp_segment_store<BD>(rv, lcco0[(long long)bank * 32 + lane], cco0_base[bank], rc);
         }
 
