@@ -207,6 +207,8 @@ struct mas_solver
     std::vector<cudaEvent_t> ev_pool;
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> ev_pending;
     size_t ev_used = 0;
+    cudaEvent_t ev_origin = nullptr; // solve start, for the profiled launch timeline
+    std::vector<std::pair<int, std::pair<float, float>>> timeline; // kind, start ms, end ms (profiled)
 
     // CUDA graphs of `chunk` PCG iterations, replayed until the device flags done. When the
     // true-residual period is a multiple of the chunk, graph[0] has no true-residual SpMV and
@@ -354,11 +356,19 @@ struct mas_solver
 
     void collect_profile()
     {
+        timeline.clear();
         for (auto &e : ev_pending)
         {
             float ms = 0.f;
             cuda_check(cudaEventElapsedTime(&ms, e.second.first, e.second.second), "event time");
             kstats[e.first].second.ms += ms;
+            if (ev_origin && timeline.size() < 400)
+            {
+                float t0 = 0.f, t1 = 0.f;
+                cudaEventElapsedTime(&t0, ev_origin, e.second.first);
+                cudaEventElapsedTime(&t1, ev_origin, e.second.second);
+                timeline.push_back({e.first, {t0, t1}});
+            }
         }
         ev_pending.clear();
         ev_used = 0;
@@ -615,6 +625,7 @@ struct mas_solver
         cuda_check(cudaEventCreate(&e0), "event");
         cuda_check(cudaEventCreate(&e1), "event");
         cuda_check(cudaEventRecord(e0, stream), "event");
+        ev_origin = e0;
         for (auto &ks : kstats) // per-solve kernel statistics
             ks.second = KStat{};
         launch_pcg_init_state(S, stream);
@@ -679,6 +690,7 @@ struct mas_solver
         cuda_check(cudaMemcpyAsync(&h_st[0], S, sizeof(PcgState), cudaMemcpyDeviceToHost, stream), "state");
         cuda_check(cudaStreamSynchronize(stream), "pcg");
         collect_profile();
+        ev_origin = nullptr;
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
         solve_ms = ms;
@@ -781,7 +793,21 @@ struct mas_solver
         }
         o.obj.emplace_back("kernel_launches", kl);
         if (p.profile)
+        {
             o.obj.emplace_back("kernel_ms", km);
+            Json tl;
+            tl.type = Json::Array;
+            for (const auto &t : timeline)
+            {
+                Json row;
+                row.type = Json::Array;
+                row.arr.push_back(str(kstats[t.first].first));
+                row.arr.push_back(num(t.second.first, false));
+                row.arr.push_back(num(t.second.second, false));
+                tl.arr.push_back(row);
+            }
+            o.obj.emplace_back("kernel_timeline", tl);
+        }
         o.obj.emplace_back("subdomain_matrices", num(mas.total_mats, true));
         return o.dump();
     }

@@ -112,11 +112,18 @@ namespace pmas
     // Sum of a per-lane value over the lanes whose key equals each distinct key of the warp,
     // written by lane 0 of each group to out[(base + key) * BD + i]. Keys < 0 are skipped.
     // Order of additions is fixed (xor butterfly), so results are deterministic.
+    // Keys held by a single lane (e.g. isolated rows, one component each) are stored directly.
     template <int BD>
     __device__ __forceinline__ void warp_segment_store(const double (&val)[BD], int key, int base, double *out)
     {
         const int lane = threadIdx.x & 31;
-        unsigned pending = __ballot_sync(FULL, key >= 0);
+        const unsigned group = __match_any_sync(FULL, key);
+        const bool single = (group == (1u << lane));
+        if (single && key >= 0)
+#pragma unroll
+            for (int i = 0; i < BD; ++i)
+                out[(size_t)(base + key) * BD + i] = val[i];
+        unsigned pending = __ballot_sync(FULL, key >= 0 && !single);
         while (pending)
         {
             const int leader = __ffs(pending) - 1;
