@@ -252,7 +252,7 @@ namespace pmas
                 if (gw + total_warps < banks)
                     bulk_load(stage1, inv + (size_t)(gw + total_warps) * S, L::STAGE_BYTES, &bar[1]);
             }
-            double part[2] = {0.0, 0.0};
+            double part[4] = {0.0, 0.0, 0.0, 0.0}; // r.z0, r.z0_old; the same over isolated banks
             uint32_t phase0 = 0, phase1 = 0;
             bool ok = true;
             // r of the current bank, prefetched one bank ahead.
@@ -303,14 +303,15 @@ namespace pmas
                     fence_proxy_async_smem();
                     bulk_load(stage, inv + (size_t)mn * S, L::STAGE_BYTES, b);
                 }
+                const int off = (m >= mas.first_iso_bank) ? 2 : 0;
 #pragma unroll
                 for (int t = 0; t < BD; ++t)
                 {
                     const double zv = (double)yr[t];
                     z0[(size_t)m * N + t * 32 + lane] = zv;
-                    part[0] = fma(zv, r64[t], part[0]);
+                    part[off] = fma(zv, r64[t], part[off]);
                     if (pr)
-                        part[1] = fma(zold[t], r64[t], part[1]);
+                        part[off + 1] = fma(zold[t], r64[t], part[off + 1]);
                 }
             }
             if (!ok)
@@ -326,12 +327,15 @@ namespace pmas
             }
             if (MODE == 0)
                 return;
-            const double t0 = block_sum<THREADS>(part[0]);
-            const double t1 = block_sum<THREADS>(part[1]);
+            double t[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+                t[i] = block_sum<THREADS>(part[i]);
             if (threadIdx.x == 0)
             {
-                red.rz_parts[2 * blockIdx.x] = t0;
-                red.rz_parts[2 * blockIdx.x + 1] = t1;
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    red.rz_parts[4 * blockIdx.x + i] = t[i];
                 if (blockIdx.x == 0)
                     st->n_rz = gridDim.x;
             }
@@ -345,12 +349,14 @@ namespace pmas
             if (st->done)
                 return;
             const int n_rz = st->n_rz, n_co = st->n_co, n_rr = (mode == 2) ? st->n_rr : 0;
-            double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+            double v[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
 #pragma unroll 4
             for (int i = threadIdx.x; i < n_rz; i += FIN_THREADS)
             {
-                v[0] += __ldcg(red.rz_parts + 2 * i);
-                v[1] += __ldcg(red.rz_parts + 2 * i + 1);
+                v[0] += __ldcg(red.rz_parts + 4 * i);
+                v[1] += __ldcg(red.rz_parts + 4 * i + 1);
+                v[5] += __ldcg(red.rz_parts + 4 * i + 2);
+                v[6] += __ldcg(red.rz_parts + 4 * i + 3);
             }
 #pragma unroll 4
             for (int i = threadIdx.x; i < n_co; i += FIN_THREADS)
@@ -361,17 +367,20 @@ namespace pmas
 #pragma unroll 4
             for (int i = threadIdx.x; i < n_rr; i += FIN_THREADS)
                 v[4] += __ldcg(red.rr_parts + i);
-            double t[5];
+            double t[7];
 #pragma unroll
-            for (int i = 0; i < 5; ++i)
+            for (int i = 0; i < 7; ++i)
                 t[i] = block_sum<FIN_THREADS>(v[i]);
             if (threadIdx.x == 0)
             {
-                st->rz_coarse = t[2];
-                st->rzx_coarse = t[3];
+                // Isolated rows: z = (1 + L) z0, so their r.z is (1 + L) r.z0 -- r.z0 is already in
+                // the level-0 sums, the coarse levels add L r.z0.
+                const double L = (double)cfg.level_num;
+                st->rz_coarse = t[2] + L * t[5];
+                st->rzx_coarse = t[3] + L * t[6];
                 if (mode == 2)
                     st->rr = t[4];
-                pcg_finalize(st, cfg, mode, t[0], t[1]);
+                pcg_finalize(st, cfg, mode, t[0] + t[5], t[1] + t[6]);
             }
         }
 
@@ -419,7 +428,7 @@ namespace pmas
                 return;
             __shared__ __align__(16) Real xs[N];
             __shared__ Real ypart[BD][N];
-            const int g = blockIdx.x;
+            const int g = mas.coarse_active[blockIdx.x];
             const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
             const size_t v0 = (size_t)g * N; // first coarse value of this matrix
             double part[2] = {0.0, 0.0};
@@ -539,6 +548,11 @@ namespace pmas
             {
                 const long long node = i / BD;
                 const int comp = (int)(i % BD);
+                if ((node >> 5) >= mas.first_iso_bank)
+                {
+                    z[i] = (1.0 + mas.level_num) * z0[i];
+                    continue;
+                }
                 const int4 cs = mas.cslot[node];
                 double v = z0[i];
                 if (cs.x >= 0)
@@ -571,10 +585,10 @@ namespace pmas
                           cudaStream_t s)
         {
             int launches = 0;
-            if (mas.banks > 0)
+            if (mas.first_iso_bank > 0)
             {
-                k_restrict<BD><<<(mas.banks + 7) / 8, 256, 0, s>>>(mas.banks, r, mas.lcco0, mas.cco0_base, mas.rc,
-                                                                  mode ? st : nullptr);
+                k_restrict<BD><<<(mas.first_iso_bank + 7) / 8, 256, 0, s>>>(mas.first_iso_bank, r, mas.lcco0,
+                                                                           mas.cco0_base, mas.rc, mode ? st : nullptr);
                 ++launches;
             }
             if (mas.total_coarse == 0)
@@ -585,7 +599,7 @@ namespace pmas
             }
             for (int l = 1; l < mas.level_num; ++l)
             {
-                const int count = mas.cco_nums[l];
+                const int count = mas.real_count[l];
                 if (count <= 0)
                     continue;
                 k_coarse_sum<BD><<<(count + 7) / 8, 256, 0, s>>>(mas, mas.coff[l], count, mode ? st : nullptr);
@@ -594,12 +608,15 @@ namespace pmas
             const int pcg = mode != 0 ? 1 : 0;
             if (pcg)
             {
-                if (mas.total_coarse > red.capacity)
+                if (mas.n_coarse_active > red.capacity)
                     throw Error(ERR_INVALID, "[MAS] reduction scratch too small");
-                k_coarse_symv<BD, Real, 1><<<mas.total_coarse, BD * 32, 0, s>>>(mas, st, red, pr);
+                if (mas.n_coarse_active > 0)
+                    k_coarse_symv<BD, Real, 1><<<mas.n_coarse_active, BD * 32, 0, s>>>(mas, st, red, pr);
+                else
+                    cuda_check(cudaMemsetAsync(&st->n_co, 0, sizeof(int), s), "memset");
             }
-            else
-                k_coarse_symv<BD, Real, 0><<<mas.total_coarse, BD * 32, 0, s>>>(mas, st, red, 0);
+            else if (mas.n_coarse_active > 0)
+                k_coarse_symv<BD, Real, 0><<<mas.n_coarse_active, BD * 32, 0, s>>>(mas, st, red, 0);
             ++launches;
             cuda_check(cudaGetLastError(), "coarse launch");
             return launches;

@@ -15,6 +15,7 @@
 //     Beaton / Goodnight sweep operator, as in batched_invert_upper :799-900), with a device error
 //     flag instead of an exception; the result is stored tile-packed in FP64 or FP32.
 
+#include <algorithm>
 #include <cub/cub.cuh>
 #include <vector>
 
@@ -40,6 +41,11 @@ namespace pmas
             v.coff[i] = coff[i];
         }
         v.fp32 = fp32;
+        v.first_iso_bank = first_iso_bank;
+        for (int i = 0; i < MAX_COARSE; ++i)
+            v.real_count[i] = real_count[i];
+        v.n_coarse_active = n_coarse_active;
+        v.coarse_active = coarse_active.get();
         v.inv = fp32 ? (const void *)inv32.get() : (const void *)inv64.get();
         v.lcco0 = lcco0.get();
         v.cco0_base = cco0_base.get();
@@ -480,7 +486,8 @@ namespace pmas
         }
     } // namespace
 
-    void build_mas(MasDevice &M, const BankedMatrix &A, const int *d_node_real, int fp32, cudaStream_t s)
+    void build_mas(MasDevice &M, const BankedMatrix &A, const int *d_node_real, int fp32, int first_iso_bank,
+                   cudaStream_t s)
     {
         const int bd = A.bd, banks = A.banks, nodes = A.nodes;
         M.bd = bd;
@@ -599,6 +606,53 @@ namespace pmas
             for (int i = 0; i < cn; ++i)
                 if (ptr[i + 1] - ptr[i] > 32)
                     throw Error(ERR_INVALID, "[MAS] internal: coarse component with more than 32 children");
+            // Isolated-row suffix: the components of the trailing isolated banks must be the
+            // largest ids at every level; otherwise the shortcut is off (first_iso_bank = banks).
+            int fib = first_iso_bank < banks ? first_iso_bank : banks;
+            for (int l = 0; l < MAX_COARSE; ++l)
+                M.real_count[l] = (l < M.level_num) ? M.cco_nums[l] : 0;
+            if (fib < banks)
+            {
+                std::vector<int> hreal((size_t)nodes);
+                cuda_check(cudaMemcpy(hreal.data(), d_node_real, sizeof(int) * nodes, cudaMemcpyDeviceToHost), "real");
+                int rc_l[MAX_COARSE];
+                bool ok = true;
+                for (int l = 0; l < M.level_num && ok; ++l)
+                {
+                    int first_iso = 1 << 30, last_real = -1;
+                    for (int u = 0; u < nodes; ++u)
+                    {
+                        if (!hreal[u])
+                            continue;
+                        const int c = hmap[(size_t)u * 4 + l];
+                        if ((u >> 5) >= fib)
+                            first_iso = std::min(first_iso, c);
+                        else
+                            last_real = std::max(last_real, c);
+                    }
+                    ok = last_real < first_iso;
+                    rc_l[l] = first_iso;
+                }
+                if (ok)
+                    for (int l = 0; l < M.level_num; ++l)
+                        M.real_count[l] = rc_l[l];
+                else
+                    fib = banks;
+            }
+            M.first_iso_bank = fib;
+            std::vector<int> active;
+            for (int l = 0; l < M.level_num; ++l)
+            {
+                const int need = div_up(M.real_count[l], 32);
+                for (int g = 0; g < need; ++g)
+                    active.push_back(M.mat_offsets[l + 1] - banks + g);
+            }
+            M.n_coarse_active = (int)active.size();
+            M.coarse_active.alloc(active.empty() ? 1 : active.size(), "MAS coarse_space active");
+            if (!active.empty())
+                cuda_check(cudaMemcpy(M.coarse_active.get(), active.data(), active.size() * sizeof(int),
+                                      cudaMemcpyHostToDevice),
+                           "active");
             M.child_ptr.alloc(cn + 1, "MAS coarse_space children");
             M.children.alloc(ch.size(), "MAS coarse_space children");
             cuda_check(cudaMemcpy(M.child_ptr.get(), ptr.data(), ptr.size() * sizeof(int), cudaMemcpyHostToDevice),

@@ -475,7 +475,18 @@ struct mas_solver
         nnz = nnz_;
         pattern = h;
 
-        build_mas(mas, A, d_node_real.get(), p.fp32 ? 1 : 0, stream);
+        // Trailing banks of isolated rows (no off-diagonal block): the coarse levels skip them.
+        int first_iso_bank = banks;
+        {
+            const std::vector<uint8_t> iso = isolated_blocks(n_, outer, inner, bd_);
+            for (int v = 0; v < V_; ++v)
+                if (iso[v])
+                    first_iso_bank = std::min(first_iso_bank, padded[v] / 32);
+            for (int v = 0; v < V_ && first_iso_bank < banks; ++v)
+                if (!iso[v] && padded[v] / 32 >= first_iso_bank)
+                    first_iso_bank = banks;
+        }
+        build_mas(mas, A, d_node_real.get(), p.fp32 ? 1 : 0, first_iso_bank, stream);
         prepare_kernels(bd_, p.fp32 ? 1 : 0);
         drop_graph();
 
@@ -489,7 +500,7 @@ struct mas_solver
         io.alloc((size_t)n_ > len ? (size_t)n_ : len, "device_buffers io");
         st.alloc(1, "device_buffers scalars");
         red_capacity = std::max({(banks + 7) / 8, mas.total_coarse, device_sm_count() * 8}) + 160;
-        partials.alloc((size_t)red_capacity * 7, "device_buffers reduction");
+        partials.alloc((size_t)red_capacity * 9, "device_buffers reduction");
         cuda_check(cudaMemsetAsync(x.get(), 0, x.bytes(), stream), "memset");
         cuda_check(cudaMemsetAsync(pv.get(), 0, pv.bytes(), stream), "memset");
         cuda_check(cudaMemsetAsync(z.get(), 0, z.bytes(), stream), "memset");
@@ -509,7 +520,7 @@ struct mas_solver
     {
         double *base = partials.get();
         const size_t c = (size_t)red_capacity;
-        return ReduceBuf{base, red_capacity, base + 2 * c, base + 3 * c, base + 5 * c};
+        return ReduceBuf{base, red_capacity, base + 2 * c, base + 3 * c, base + 7 * c};
     }
 
     PcgConfig config() const
@@ -521,6 +532,7 @@ struct mas_solver
         c.use_prec_norm = p.use_prec_norm ? 1 : 0;
         c.check_period = p.check_period;
         c.polak_ribiere = p.polak_ribiere ? 1 : 0;
+        c.level_num = mas.level_num;
         return c;
     }
 
@@ -809,6 +821,8 @@ struct mas_solver
             o.obj.emplace_back("kernel_timeline", tl);
         }
         o.obj.emplace_back("subdomain_matrices", num(mas.total_mats, true));
+        o.obj.emplace_back("coarse_matrices_active", num(mas.n_coarse_active, true));
+        o.obj.emplace_back("isolated_banks", num(banks - mas.first_iso_bank, true));
         return o.dump();
     }
 };

@@ -142,6 +142,14 @@ namespace pmas
         int mat_counts[LEVELS];
         int cco_nums[MAX_COARSE];
         int fp32;               // storage precision of the inverses
+        // Banks >= first_iso_bank hold only isolated rows (no off-diagonal block). Such a row is its
+        // own component at every level with coarse block A_uu, so z_u = (1 + level_num) z0_u and the
+        // coarse levels can skip it: only components < real_count[l] and the coarse matrices in
+        // coarse_active are processed.
+        int first_iso_bank;
+        int real_count[MAX_COARSE];
+        int n_coarse_active;
+        const int *coarse_active;
         const void *inv;        // total_mats * tile_packed_size(bd), float or double
         const int *lcco0;       // nodes: bank-local level-0 component id, -1 virtual
         const int *cco0_base;   // banks: first global level-0 component id of the bank
@@ -173,6 +181,7 @@ namespace pmas
         int use_prec_norm;
         int check_period;
         int polak_ribiere;
+        int level_num; // coarse levels in use (isolated rows: z = (1 + level_num) z0)
     };
 
     // Scratch for deterministic two-stage reductions: per-CTA partials.
@@ -184,7 +193,7 @@ namespace pmas
         double *partials; // 2 * capacity
         int capacity;     // max CTAs of any reduced launch
         double *rr_parts; // capacity: r.r from the kernel that produced r this iteration
-        double *rz_parts; // 2 * capacity: r.z0 and r.z0_old from the level-0 MAS kernel
+        double *rz_parts; // 4 * capacity: r.z0, r.z0_old, and both over isolated banks (MAS level 0)
         double *co_parts; // 2 * capacity: rc.zc and rc.zc_old from the coarse kernel
     };
 
@@ -277,6 +286,10 @@ namespace pmas
         DevBuf<int> cco0_base;
         DevBuf<int4> cslot;
         DevBuf<int> child_ptr, children, identity;
+        int first_iso_bank = 0;
+        int real_count[MAX_COARSE] = {0, 0, 0, 0};
+        DevBuf<int> coarse_active;
+        int n_coarse_active = 0;
         int coff[MAX_COARSE] = {0, 0, 0, 0};
         DevBuf<float> inv32;
         DevBuf<double> inv64;
@@ -285,7 +298,9 @@ namespace pmas
         MasView view(double *rc_override = nullptr) const;
     };
 
-    void build_mas(MasDevice &M, const BankedMatrix &A, const int *d_node_real, int fp32, cudaStream_t s);
+    // first_iso_bank: first bank of the trailing isolated rows (banks if none / not trailing).
+    void build_mas(MasDevice &M, const BankedMatrix &A, const int *d_node_real, int fp32, int first_iso_bank,
+                   cudaStream_t s);
 
     // mas_pcg.cu: misc
     void launch_zero(double *p, size_t n, cudaStream_t s);

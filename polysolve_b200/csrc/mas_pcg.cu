@@ -97,9 +97,22 @@ namespace pmas
             const int lane = threadIdx.x & 31;
             const int total_warps = gridDim.x * (UPD_THREADS / 32);
             const double *__restrict__ zc = mas.zc;
+            const double iso_scale = 1.0 + mas.level_num;
             for (int bank = blockIdx.x * (UPD_THREADS / 32) + (threadIdx.x >> 5); bank < mas.banks; bank += total_warps)
             {
                 const long long b0 = (long long)bank * 32 * BD;
+                if (bank >= mas.first_iso_bank)
+                {
+                    // Isolated rows: every coarse level adds z0 again (coarse block A_uu).
+#pragma unroll
+                    for (int t = 0; t < BD; ++t)
+                    {
+                        const long long idx = b0 + t * 32 + lane;
+                        const double v = iso_scale * z0[idx];
+                        p[idx] = first ? v : fma(beta, p[idx], v);
+                    }
+                    continue;
+                }
 #pragma unroll
                 for (int t = 0; t < BD; ++t)
                 {
