@@ -538,6 +538,22 @@ namespace
         }
     }
 
+    // Round a float to the nearest IEEE binary16 value (round to nearest even), returned as float.
+    float half_round(float f)
+    {
+        if (!std::isfinite(f) || f == 0.0f)
+            return f;
+        int e;
+        std::frexp(f, &e); // f = m 2^e, 0.5 <= |m| < 1
+        if (e > 16)
+            return std::copysign(65504.0f, f);
+        const int bits = (e - 1 >= -14) ? 11 : 11 - (-14 - (e - 1)); // normal: 11 significant bits
+        if (bits <= 0)
+            return 0.0f;
+        const float q = std::ldexp(1.0f, e - bits);
+        return std::nearbyint(f / q) * q;
+    }
+
     // Deterministic dot: fixed chunks, summed in chunk order.
     double dot(const double *a, const double *b, size_t n)
     {
@@ -570,7 +586,7 @@ extern "C"
         int true_residual_period; // reference: 4 (MASSolver.cu:139)
         int check_period;         // reference: 10 (MASSolver.cu:533)
         int use_initial_guess;    // reference: 0, x forced to zero (MASSolver.cu:395-398)
-        int mas_fp32;             // round the inverses to float (emulates FP32 storage)
+        int mas_fp32;             // emulate inverse storage: 1 = FP32, 16 = FP16 with a per-matrix scale
         int polak_ribiere;        // beta = r.(z - z_old) / rz_old instead of rz / rz_old
     };
 
@@ -693,8 +709,23 @@ extern "C"
         if (p.mas_fp32)
         {
             saved = o->mats;
-            for (double &v : o->mats)
-                v = (double)(float)v;
+            if (p.mas_fp32 == 16)
+            {
+                // FP16 storage with one scale per matrix (largest magnitude -> 2^14), FP32 math.
+                for (int m = 0; m < o->total_mats; ++m)
+                {
+                    double *mat = o->mats.data() + (size_t)m * o->storage;
+                    double amax = 0.0;
+                    for (long long i = 0; i < o->storage; ++i)
+                        amax = std::max(amax, std::fabs(mat[i]));
+                    const double sc = amax > 0.0 ? std::ldexp(1.0, 14 - std::ilogb(amax)) : 1.0;
+                    for (long long i = 0; i < o->storage; ++i)
+                        mat[i] = (double)(float)((double)half_round((float)(mat[i] * sc)) / sc);
+                }
+            }
+            else
+                for (double &v : o->mats)
+                    v = (double)(float)v;
         }
         // Permute b (and x) into block order; pad with zeros (MASSolver.cu:387-393).
         for (size_t nb = 0; nb < (size_t)o->V; ++nb)
