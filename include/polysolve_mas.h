@@ -107,6 +107,18 @@ int mas_solve_device(mas_solver *h, const double *d_b, double *d_x, int n);
  * the handle's own stream). Calls still return only when their work has finished. */
 int mas_set_stream(mas_solver *h, void *stream);
 
+/* New, no counterpart in the reference: y = A x and *d_dot = x . (A x) on the factorized matrix,
+ * with no device allocation at all, for callers that cannot allocate at call time (inside a CUDA
+ * stream capture, or in applications that reserve all device memory up front and forbid later
+ * allocations). d_x, d_y: device vectors of length len = nodes * block_dim in the solver's padded
+ * block order (see mas_get_sizes); d_dot: one device double. Runs on `stream` (a cudaStream_t, NULL
+ * = the handle's stream) without synchronizing. The reduction scratch is a static device array of
+ * 256 KB (held by every GPU that loads the library until exit), which limits the matrix to 262,144
+ * banks (8,388,608 block rows); larger matrices get MAS_ERR_INVALID. All calls share that scratch:
+ * calls that overlap on the GPU race. The first call on a device looks the scratch address up
+ * (cudaGetSymbolAddress); make it before any stream capture. */
+int mas_spmv_dot_noalloc(mas_solver *h, const double *d_x, double *d_y, double *d_dot, int len, void *stream);
+
 /* Last error message of the handle ("" if none). With h == NULL: the last mas_create error. */
 const char *mas_last_error(const mas_solver *h);
 

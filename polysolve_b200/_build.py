@@ -38,6 +38,7 @@ CU_SOURCES = [
     "mas_build.cu",
     "mas_apply.cu",
     "mas_pcg.cu",
+    "mas_noalloc.cu",
 ]
 CPP_SOURCES = ["mas_capi.cpp", "mas_ordering.cpp", "mas_json.cpp"]
 

@@ -1039,6 +1039,24 @@ extern "C" int mas_set_stream(mas_solver *h, void *stream)
     });
 }
 
+extern "C" int mas_spmv_dot_noalloc(mas_solver *h, const double *d_x, double *d_y, double *d_dot, int len,
+                                    void *stream)
+{
+    if (!h)
+        return MAS_ERR_INVALID;
+    return guarded(h, [&] {
+        if (!h->factorized)
+            throw Error(ERR_NOT_FACTORIZED, "[MAS] spmv_dot_noalloc: call factorize first.");
+        if (len != h->banks * 32 * h->bd)
+            throw Error(ERR_INVALID, "[MAS] spmv_dot_noalloc: len must be nodes * block_dim = " +
+                                         std::to_string(h->banks * 32 * h->bd) + ".");
+        if (!d_x || !d_y || !d_dot)
+            throw Error(ERR_INVALID, "[MAS] spmv_dot_noalloc: null device pointer.");
+        cuda_check(cudaSetDevice(h->device), "set device");
+        launch_spmv_dot_noalloc(h->A.view(), d_x, d_y, d_dot, stream ? static_cast<cudaStream_t>(stream) : h->stream);
+    });
+}
+
 extern "C" const char *mas_last_error(const mas_solver *h)
 {
     if (!h)

@@ -304,4 +304,9 @@ namespace pmas
 
     // mas_pcg.cu: misc
     void launch_zero(double *p, size_t n, cudaStream_t s);
+
+    // mas_noalloc.cu: y = A x and *dot = x . y with the reduction scratch in a static device array
+    // (no allocation). Throws Error(ERR_INVALID) beyond noalloc_max_banks() banks.
+    void launch_spmv_dot_noalloc(const BankedView &A, const double *x, double *y, double *dot, cudaStream_t s);
+    int noalloc_max_banks();
 } // namespace pmas

@@ -39,7 +39,7 @@ MAS_ERR_NO_DEVICE = 8
 EXPORTED_SYMBOLS = [
     "mas_create", "mas_create_json", "mas_destroy", "mas_set_parameters", "mas_get_info", "mas_name",
     "mas_analyze_pattern", "mas_set_positions", "mas_factorize_csc", "mas_solve", "mas_solve_multi",
-    "mas_solve_device", "mas_set_stream", "mas_last_error", "mas_get_sizes", "mas_get_ordering", "mas_order_blocks",
+    "mas_solve_device", "mas_set_stream", "mas_spmv_dot_noalloc", "mas_last_error", "mas_get_sizes", "mas_get_ordering", "mas_order_blocks",
     "mas_get_coarse_map", "mas_get_inverses", "mas_debug_spmv", "mas_debug_apply",
 ]
 
@@ -83,6 +83,7 @@ def library() -> ctypes.CDLL:
         L.mas_solve_multi.argtypes = [vp, vp, vp, i, i]
         L.mas_solve_device.argtypes = [vp, ctypes.c_void_p, ctypes.c_void_p, i]
         L.mas_set_stream.argtypes = [vp, vp]
+        L.mas_spmv_dot_noalloc.argtypes = [vp, vp, vp, vp, i, vp]
         L.mas_last_error.argtypes = [vp]
         L.mas_last_error.restype = ctypes.c_char_p
         L.mas_get_sizes.argtypes = [vp, ip]
@@ -239,6 +240,13 @@ class Solver:
     def set_stream(self, stream_handle: int | None) -> None:
         """New: run on the caller's CUDA stream (e.g. torch.cuda.current_stream().cuda_stream)."""
         _check(library().mas_set_stream(self._h, ctypes.c_void_p(stream_handle or 0)), self._h)
+
+    def spmv_dot_noalloc(self, d_x: int, d_y: int, d_dot: int, length: int, stream: int | None = None) -> None:
+        """New: y = A x and *d_dot = x . y on device pointers in padded block order, with no
+        device allocation (static scratch; for callers that cannot allocate at call time)."""
+        _check(library().mas_spmv_dot_noalloc(self._h, ctypes.c_void_p(d_x), ctypes.c_void_p(d_y),
+                                               ctypes.c_void_p(d_dot), int(length), ctypes.c_void_p(stream or 0)),
+               self._h)
 
     def name(self) -> str:
         return library().mas_name().decode()
