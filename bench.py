@@ -6,8 +6,10 @@ split, vertices jittered +-0.2h, E lognormal(ln 1e5, 1.0) per element, K + M/h^2
 Dirichlet on x = 0), BSR 3x3, 32-vertex Morton subdomains, b ~ N(0, 1). Synthetic, seeded.
 
 A step is one solve from x0 = 0 to ||b - A x|| <= 1e-8 ||b||.
-  * value:  the chosen configuration (FP32 MAS, true residual every 50, device-side convergence test
-            every iteration), inputs resident in HBM, solve_device on torch's stream, CUDA events.
+  * value:  the chosen configuration (MAS inverses stored in FP16 with a per-matrix scale and applied
+            in FP32 -- `--precision fp32` for FP32 storage --, true residual every 50, device-side
+            convergence test every iteration), inputs resident in HBM, solve_device on torch's
+            stream, CUDA events.
   * e2e:    the same solve through the public host API (Solver.solve) from pinned host memory:
             b host->device and x device->host inside the timed region.
   * plain_fp64_ms: the reference's algorithm on the same GPU (FP64 MAS, true residual every 4,
@@ -45,7 +47,7 @@ UNIT = "ms/solve"
 TOL = 1e-8
 
 CHOSEN = {"block_dim": 3, "relative_tolerance": TOL, "absolute_tolerance": 0.0, "max_iter": 5000,
-          "precision": "fp32", "true_residual_period": 50, "check_period": 1, "poll_period": 10,
+          "precision": "fp16", "true_residual_period": 50, "check_period": 1, "poll_period": 10,
           "cuda_graphs": True}
 # The reference's algorithm: FP64 MAS, true residual every 4, convergence test every 10 iterations,
 # iterations launched from the host (MASSolver.cu:498-583).
@@ -64,6 +66,8 @@ def parse_args():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cpu-sample-iters", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default=CHOSEN["precision"], choices=["fp16", "fp32", "fp64"],
+                    help="storage of the MAS inverses in the chosen configuration")
     return ap.parse_args()
 
 
@@ -73,8 +77,10 @@ def spmv_bytes(nnzb: int, n: int) -> int:
     return nnzb * (72 + 4) + (n // 3 + 1) * 4 + 2 * 8 * n
 
 
-def mas_bytes(total_mats: int, n: int, value_bytes: int) -> int:
-    return total_mats * 4656 * value_bytes + 4 * 8 * n
+def mas_bytes(mats: int, n: int, value_bytes: int) -> int:
+    """Algorithmic bytes of one MAS apply launch: every applied 96 x 96 packed inverse (4,656
+    values) once, r read and z0 written once (FP64)."""
+    return mats * 4656 * value_bytes + 2 * 8 * n
 
 
 class Clocks:
@@ -176,7 +182,7 @@ def run_ours(args) -> None:
         s.factorize(A)
         return s, time.time() - t0
 
-    chosen, fact_s = make(CHOSEN)
+    chosen, fact_s = make(dict(CHOSEN, precision=args.precision))
     plain, _ = make(PLAIN)
     stream = torch.cuda.current_stream()
     chosen.set_stream(stream.cuda_stream)
@@ -280,21 +286,24 @@ def run_ours(args) -> None:
         pass
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = spmv_b / (spmv_launch_ms * 1e-3) / 1e9 if spmv_launch_ms > 0 else 0.0
-    symv_launch_ms = kms.get("mas_symv0", 0.0) / max(1, kl.get("mas_symv0", 1))
-    mas_b = mas_bytes(sizes["banks"], n, 4)
+    symv_launch_ms = kms.get("mas_apply", 0.0) / max(1, kl.get("mas_apply", 1))
+    value_bytes = {"fp16": 2, "fp32": 4, "fp64": 8}[args.precision]
+    mas_b = mas_bytes(sizes["banks"] + info["coarse_matrices_active"], n, value_bytes)
     kernel_table = {k: {"launches": kl.get(k, 0), "ms_total": round(kms.get(k, 0.0), 4),
                         "ms_per_launch": round(kms.get(k, 0.0) / max(1, kl.get(k, 1)), 5)} for k in kl}
 
     out = {
         "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": max(args.warmup, 3), "ms_per_step": round(ms_per_step, 4), "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64 (SpMV, dots, updates) + f32 (MAS apply)",
+        "scaling": "weak", "vs_baseline": None, "dtype": f"f64 (SpMV, dots, updates) + {args.precision} storage / "
+                                    f"{'f64' if args.precision == 'fp64' else 'f32'} arithmetic (MAS apply)",
         "data": "synthetic (seeded 80^3 jittered tet elasticity, b ~ N(0,1))",
         "config": {"workload": f"{args.grid}^3 jittered tet elasticity, {n} DOF, nnzb {sizes['nnzb']}, "
                                f"{sizes['banks']} 32-vertex Morton subdomains, {sizes['level_num']} coarse levels",
-                   "chosen": "fp32 MAS, true residual every 50, convergence test every iteration, x0 = 0",
+                   "chosen": f"{args.precision} MAS inverses, true residual every 50, convergence test every "
+                             f"iteration, x0 = 0",
                    "tolerance": TOL, "parallelism": f"replicas x{world}",
-                   "l2": "working set > L2 (A 560 MB + MAS 340 MB per solve iteration)"},
+                   "l2": f"working set > L2 (A {spmv_b / 1e6:.0f} MB + MAS {mas_b / 1e6:.0f} MB per iteration)"},
         "iterations": info["solver_iter"], "relative_residual": relres,
         "plain_fp64_ms": round(plain_ms, 4), "plain_fp64_iterations": pinfo["solver_iter"],
         "plain_fp64_relative_residual": relres_plain, "speedup_vs_plain_fp64": round(plain_ms / ms_per_step, 3),
@@ -306,7 +315,7 @@ def run_ours(args) -> None:
                      "frac": round(achieved / peak, 4), "traffic": None, "kernel": "spmv_pap",
                      "algorithmic_bytes_per_launch": spmv_b, "launch_ms": round(spmv_launch_ms, 5),
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured copy)" if peaks else "fallback 6650 GB/s"},
-        "mas_symv0": {"launch_ms": round(symv_launch_ms, 5), "algorithmic_bytes_per_launch": mas_b,
+        "mas_apply": {"launch_ms": round(symv_launch_ms, 5), "algorithmic_bytes_per_launch": mas_b,
                       "achieved_gbs": round(mas_b / (symv_launch_ms * 1e-3) / 1e9, 1) if symv_launch_ms > 0 else None},
         "kernels": kernel_table,
         "clocks": clk,

@@ -61,7 +61,8 @@ void mas_destroy(mas_solver *h);
  * JSON object and silently ignores the call when it is absent. Keys of the reference: block_dim,
  * max_iter, relative_tolerance, absolute_tolerance, lazy_partitioning,
  * use_preconditioned_residual_norm. Keys this implementation adds (ignored by the reference):
- * precision ("fp64" | "fp32"), true_residual_period (int, reference 4), check_period (int,
+ * precision ("fp64" | "fp32" | "fp16": storage of the MAS inverses; fp16 keeps one power-of-two
+ * scale per matrix and multiplies in FP32), true_residual_period (int, reference 4), check_period (int,
  * reference 10), initial_guess ("zero" | "input"; reference: zero), beta ("fletcher_reeves" |
  * "polak_ribiere"), ordering ("auto" | "morton" | "graph" | "natural"), poll_period (int: iterations
  * launched between looks at the device state), profile_kernels (bool: CUDA-event time per kernel

@@ -539,19 +539,39 @@ namespace
     }
 
     // Round a float to the nearest IEEE binary16 value (round to nearest even), returned as float.
+    // Normal results keep 11 significant bits; below 2^-14 the step is the subnormal 2^-24.
     float half_round(float f)
     {
         if (!std::isfinite(f) || f == 0.0f)
             return f;
         int e;
         std::frexp(f, &e); // f = m 2^e, 0.5 <= |m| < 1
-        if (e > 16)
-            return std::copysign(65504.0f, f);
-        const int bits = (e - 1 >= -14) ? 11 : 11 - (-14 - (e - 1)); // normal: 11 significant bits
-        if (bits <= 0)
-            return 0.0f;
-        const float q = std::ldexp(1.0f, e - bits);
-        return std::nearbyint(f / q) * q;
+        const float q = std::ldexp(1.0f, std::max(e - 11, -24));
+        const float r = std::nearbyint(f / q) * q;
+        return std::fabs(r) > 65504.0f ? std::copysign(INFINITY, f) : r; // past the largest finite value
+    }
+
+    // Emulates storing the inverses in reduced precision (values rounded in place, arithmetic
+    // stays FP64): mode 1 = FP32; mode 16 = binary16 with one power-of-two scale per matrix that
+    // maps its largest magnitude into [2^14, 2^15).
+    void round_storage(Oracle &o, int mode)
+    {
+        if (mode == 16)
+        {
+            for (int m = 0; m < o.total_mats; ++m)
+            {
+                double *mat = o.mats.data() + (size_t)m * o.storage;
+                double amax = 0.0;
+                for (long long i = 0; i < o.storage; ++i)
+                    amax = std::max(amax, std::fabs(mat[i]));
+                const double sc = (amax > 0.0 && std::isfinite(amax)) ? std::ldexp(1.0, 14 - std::ilogb(amax)) : 1.0;
+                for (long long i = 0; i < o.storage; ++i)
+                    mat[i] = (double)half_round((float)(mat[i] * sc)) / sc;
+            }
+        }
+        else if (mode)
+            for (double &v : o.mats)
+                v = (double)(float)v;
     }
 
     // Deterministic dot: fixed chunks, summed in chunk order.
@@ -690,6 +710,30 @@ extern "C"
         return 0;
     }
 
+    // out[i] = half_round(in[i]) (checks the binary16 rounding against IEEE conversions).
+    int orc_half_round(const float *in, float *out, long long n)
+    {
+        for (long long i = 0; i < n; ++i)
+            out[i] = half_round(in[i]);
+        return 0;
+    }
+
+    // z = M^-1 r with the inverses stored as in round_storage(mode) (0 = FP64).
+    int orc_apply_storage(void *h, const double *r, double *z, int mode)
+    {
+        auto *o = static_cast<Oracle *>(h);
+        if (mode == 0)
+        {
+            mas_apply(*o, r, z);
+            return 0;
+        }
+        const std::vector<double> saved = o->mats;
+        round_storage(*o, mode);
+        mas_apply(*o, r, z);
+        o->mats = saved;
+        return 0;
+    }
+
     int orc_spmv(void *h, const double *x, double *y)
     {
         spmv(*static_cast<Oracle *>(h), x, y);
@@ -709,23 +753,7 @@ extern "C"
         if (p.mas_fp32)
         {
             saved = o->mats;
-            if (p.mas_fp32 == 16)
-            {
-                // FP16 storage with one scale per matrix (largest magnitude -> 2^14), FP32 math.
-                for (int m = 0; m < o->total_mats; ++m)
-                {
-                    double *mat = o->mats.data() + (size_t)m * o->storage;
-                    double amax = 0.0;
-                    for (long long i = 0; i < o->storage; ++i)
-                        amax = std::max(amax, std::fabs(mat[i]));
-                    const double sc = amax > 0.0 ? std::ldexp(1.0, 14 - std::ilogb(amax)) : 1.0;
-                    for (long long i = 0; i < o->storage; ++i)
-                        mat[i] = (double)(float)((double)half_round((float)(mat[i] * sc)) / sc);
-                }
-            }
-            else
-                for (double &v : o->mats)
-                    v = (double)(float)v;
+            round_storage(*o, p.mas_fp32);
         }
         // Permute b (and x) into block order; pad with zeros (MASSolver.cu:387-393).
         for (size_t nb = 0; nb < (size_t)o->V; ++nb)

@@ -89,6 +89,8 @@ def lib():
         L.orc_export_maps.argtypes = [vp, vp, vp]
         L.orc_export_inverses.argtypes = [vp, vp]
         L.orc_apply.argtypes = [vp, vp, vp]
+        L.orc_apply_storage.argtypes = [vp, vp, vp, ctypes.c_int]
+        L.orc_half_round.argtypes = [vp, vp, ctypes.c_longlong]
         L.orc_spmv.argtypes = [vp, vp, vp]
         L.orc_pcg.argtypes = [vp, vp, vp, ctypes.POINTER(PcgParams), ctypes.POINTER(PcgResult)]
         L.orc_time_iterations.restype = ctypes.c_double
@@ -267,10 +269,14 @@ class MasOracle:
         return out.reshape(self.s.total_mats, storage)
 
     # vectors below are in permuted block order (length V * bd)
-    def apply(self, r: np.ndarray) -> np.ndarray:
+    def apply(self, r: np.ndarray, storage: int = 0) -> np.ndarray:
+        """z = M^-1 r; storage 1 / 16 emulates FP32 / scaled binary16 inverses (FP64 arithmetic)."""
         r = np.ascontiguousarray(r, dtype=np.float64)
         z = np.empty_like(r)
-        lib().orc_apply(self.h, _p(r), _p(z))
+        if storage:
+            lib().orc_apply_storage(self.h, _p(r), _p(z), int(storage))
+        else:
+            lib().orc_apply(self.h, _p(r), _p(z))
         return z
 
     def spmv(self, x: np.ndarray) -> np.ndarray:
@@ -309,6 +315,14 @@ class MasOracle:
 
     def time_iterations(self, iterations: int, true_residual_period: int) -> float:
         return float(lib().orc_time_iterations(self.h, int(iterations), int(true_residual_period)))
+
+
+def half_round(v: np.ndarray) -> np.ndarray:
+    """The oracle's float -> nearest binary16 rounding (as float32), for checking it."""
+    v = np.ascontiguousarray(v, dtype=np.float32)
+    out = np.empty_like(v)
+    lib().orc_half_round(_p(v), _p(out), v.size)
+    return out
 
 
 def jacobi_pcg(outer, inner, vals, n: int, b: np.ndarray, tol: float = 1e-8, max_iter: int | None = None,

@@ -78,7 +78,7 @@ def build_mas(force: bool = False, verbose_ptxas: bool = False) -> Path:
         src = CSRC / name
         obj = BUILD / (name + ".o")
         if force or _stale(obj, [src] + hdrs):
-            cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-fopenmp",
+            cmd = [NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++20", "-Xcompiler", "-fPIC,-fopenmp",
                    "--expt-relaxed-constexpr", *common_inc, "-c", str(src), "-o", str(obj)]
             if verbose_ptxas:
                 cmd.insert(1, "-Xptxas=-v")

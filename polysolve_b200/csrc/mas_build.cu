@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <cub/cub.cuh>
+#include <type_traits>
 #include <vector>
 
 #include "mas_common.cuh"
@@ -40,18 +41,20 @@ namespace pmas
             v.cco_nums[i] = cco_nums[i];
             v.coff[i] = coff[i];
         }
-        v.fp32 = fp32;
+        v.storage = storage;
         v.first_iso_bank = first_iso_bank;
         for (int i = 0; i < MAX_COARSE; ++i)
             v.real_count[i] = real_count[i];
         v.n_coarse_active = n_coarse_active;
         v.coarse_active = coarse_active.get();
-        v.inv = fp32 ? (const void *)inv32.get() : (const void *)inv64.get();
+        v.inv = storage == STORE_F64 ? (const void *)inv64.get()
+                : (storage == STORE_F16 ? (const void *)inv16.get() : (const void *)inv32.get());
+        v.inv_scale = inv_scale.get();
         v.lcco0 = lcco0.get();
         v.cco0_base = cco0_base.get();
         v.cslot = cslot.get();
-        v.child_ptr = child_ptr.get();
-        v.children = children.get();
+        v.parent = parent.get();
+        v.ticket = ticket.get();
         v.identity = identity.get();
         v.rc = rc_override ? rc_override : rc.get();
         v.zc = zc.get();
@@ -183,8 +186,19 @@ namespace pmas
         // ----------------------------------------------------------------------------------
         // Dense symmetric work matrix in shared memory (N x N, FP64), sweep inverse, store.
         // ----------------------------------------------------------------------------------
+        __device__ __forceinline__ void store_value(double *o, double v, double) { *o = v; }
+        __device__ __forceinline__ void store_value(float *o, double v, double) { *o = (float)v; }
+        // Binary16: scaled by the matrix's power of two, rounded to FP32 and then to nearest-even.
+        __device__ __forceinline__ void store_value(__half *o, double v, double sc)
+        {
+            *o = __float2half_rn((float)(v * sc));
+        }
+
+        // Inverts the symmetric N x N matrix A (shared memory, upper triangle used) and stores the
+        // inverse tile-packed in `out`; *scale_out receives the factor that turns stored values
+        // back into matrix values (1 unless binary16).
         template <int BD, class Out>
-        __device__ void invert_and_store(double *A, double *col, Out *out, int *flag)
+        __device__ void invert_and_store(double *A, double *col, Out *out, double *scale_out, int *flag)
         {
             constexpr int N = 32 * BD;
             const int tid = threadIdx.x, nt = blockDim.x;
@@ -232,6 +246,32 @@ namespace pmas
                 }
                 __syncthreads();
             }
+            // Binary16 storage: one power-of-two scale per matrix maps the largest magnitude into
+            // [2^14, 2^15), well inside the format's range (max 65504) and clear of its subnormals.
+            double sc = 1.0;
+            if constexpr (StoreTraits<Out>::SCALED)
+            {
+                __shared__ unsigned long long amax_bits;
+                if (tid == 0)
+                    amax_bits = 0ull;
+                __syncthreads();
+                unsigned long long m = 0ull;
+                for (int e = tid; e < N * N; e += nt)
+                {
+                    const int t = e / N, c = e - t * N;
+                    if (t > c)
+                        continue;
+                    // Non-negative doubles order like their bit patterns.
+                    const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(A[e]));
+                    m = b > m ? b : m;
+                }
+                atomicMax(&amax_bits, m);
+                __syncthreads();
+                const double amax = __longlong_as_double((long long)amax_bits);
+                sc = (amax > 0.0 && isfinite(amax)) ? ldexp(1.0, 14 - ilogb(amax)) : 1.0;
+            }
+            if (tid == 0)
+                *scale_out = 1.0 / sc;
             // Store -A (the inverse) tile-packed.
             constexpr int S = N * (N + 1) / 2;
             for (int idx = tid; idx < S; idx += nt)
@@ -265,7 +305,7 @@ namespace pmas
                 const double v = -A[row * N + cl];
                 if (!isfinite(v))
                     bad = 1;
-                out[idx] = (Out)v;
+                store_value(out + idx, v, sc);
             }
             __syncthreads();
             if (tid == 0 && bad)
@@ -274,7 +314,7 @@ namespace pmas
 
         template <int BD, class Out>
         __global__ void __launch_bounds__(256) k_assemble_invert_lv0(BankedView A, const int *__restrict__ node_real,
-                                                                     Out *out, int *flag)
+                                                                     Out *out, double *scale, int *flag)
         {
             constexpr int N = 32 * BD, S = N * (N + 1) / 2;
             extern __shared__ __align__(16) double dsm[];
@@ -315,7 +355,7 @@ namespace pmas
                 }
             }
             __syncthreads();
-            invert_and_store<BD, Out>(M, col, out + (size_t)bank * S, flag);
+            invert_and_store<BD, Out>(M, col, out + (size_t)bank * S, scale + bank, flag);
         }
 
         // Coarse-level upper-triangle accumulation with FP64 atomics (order-dependent in the
@@ -366,7 +406,8 @@ namespace pmas
         }
 
         template <int BD, class Out>
-        __global__ void __launch_bounds__(256) k_invert_coarse(const double *__restrict__ staging, Out *out, int *flag)
+        __global__ void __launch_bounds__(256) k_invert_coarse(const double *__restrict__ staging, Out *out,
+                                                               double *scale, int *flag)
         {
             constexpr int N = 32 * BD, S = N * (N + 1) / 2;
             extern __shared__ __align__(16) double dsm[];
@@ -379,7 +420,7 @@ namespace pmas
                 M[e] = (r <= c) ? src[r * N + c] : src[c * N + r];
             }
             __syncthreads();
-            invert_and_store<BD, Out>(M, col, out + (size_t)blockIdx.x * S, flag);
+            invert_and_store<BD, Out>(M, col, out + (size_t)blockIdx.x * S, scale + blockIdx.x, flag);
         }
 
         __global__ void k_cslot(int nodes, int level_num, const int *__restrict__ map, int coff0, int coff1, int coff2,
@@ -400,14 +441,16 @@ namespace pmas
         }
 
         // flag[g] = 1 if coarse inverse g is exactly the identity (a bank of isolated rows).
-        template <int BD, class Real>
-        __global__ void k_identity_flags(const Real *__restrict__ inv, int first, int count, int *flag)
+        template <int BD, class Store>
+        __global__ void k_identity_flags(const Store *__restrict__ inv, const double *__restrict__ scale, int first,
+                                         int count, int *flag)
         {
             constexpr int N = 32 * BD, S = N * (N + 1) / 2;
             const int g = blockIdx.x;
             if (g >= count)
                 return;
-            const Real *m = inv + (size_t)(first + g) * S;
+            const Store *m = inv + (size_t)(first + g) * S;
+            const double sc = scale[first + g];
             __shared__ int is_id;
             if (threadIdx.x == 0)
                 is_id = 1;
@@ -429,8 +472,8 @@ namespace pmas
                         ++j;
                     diag = (e - j * (j + 1) / 2) == j;
                 }
-                const Real want = diag ? Real(1) : Real(0);
-                if (m[idx] != want)
+                const double want = diag ? 1.0 : 0.0;
+                if ((double)load1(m + idx) * sc != want)
                     is_id = 0;
             }
             __syncthreads();
@@ -455,6 +498,7 @@ namespace pmas
         void assemble_and_invert(MasDevice &M, const BankedMatrix &A, const int *d_node_real, Out *out, const int *coff,
                                  cudaStream_t s)
         {
+            double *scale = M.inv_scale.get();
             constexpr int N = 32 * BD;
             const size_t smem = (size_t)(N * N + 2 * N) * sizeof(double);
             cuda_check(cudaFuncSetAttribute(k_assemble_invert_lv0<BD, Out>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -465,7 +509,7 @@ namespace pmas
                        "invert smem attribute");
             if (M.banks > 0)
             {
-                k_assemble_invert_lv0<BD, Out><<<M.banks, 256, smem, s>>>(A.view(), d_node_real, out, M.flag.get());
+                k_assemble_invert_lv0<BD, Out><<<M.banks, 256, smem, s>>>(A.view(), d_node_real, out, scale, M.flag.get());
                 cuda_check(cudaGetLastError(), "assemble lv0 launch");
             }
             if (M.total_coarse > 0)
@@ -479,21 +523,21 @@ namespace pmas
                 cuda_check(cudaGetLastError(), "assemble coarse launch");
                 constexpr int S = N * (N + 1) / 2;
                 k_invert_coarse<BD, Out><<<M.total_coarse, 256, smem, s>>>(staging.get(), out + (size_t)M.banks * S,
-                                                                          M.flag.get());
+                                                                          scale + M.banks, M.flag.get());
                 cuda_check(cudaGetLastError(), "invert coarse launch");
                 cuda_check(cudaStreamSynchronize(s), "coarse inverse");
             }
         }
     } // namespace
 
-    void build_mas(MasDevice &M, const BankedMatrix &A, const int *d_node_real, int fp32, int first_iso_bank,
+    void build_mas(MasDevice &M, const BankedMatrix &A, const int *d_node_real, int storage, int first_iso_bank,
                    cudaStream_t s)
     {
         const int bd = A.bd, banks = A.banks, nodes = A.nodes;
         M.bd = bd;
         M.banks = banks;
         M.nodes = nodes;
-        M.fp32 = fp32;
+        M.storage = storage;
         M.flag.alloc(1, "MAS flag");
         cuda_check(cudaMemsetAsync(M.flag.get(), 0, sizeof(int), s), "memset");
 
@@ -577,8 +621,8 @@ namespace pmas
                                                   M.cslot.get());
         cuda_check(cudaGetLastError(), "cslot launch");
 
-        // Child lists: for each coarse node of level l >= 1, the (<= 32) level l-1 coarse nodes it
-        // merges, in increasing order; built on the host from the maps.
+        // Parents: for each coarse node of level l - 1, the level-l coarse node it merges into
+        // (every level-l node has at most 32 children, all in one group of 32 consecutive ids).
         for (int l = 0; l < MAX_COARSE; ++l)
             M.coff[l] = coff[l];
         {
@@ -592,20 +636,22 @@ namespace pmas
                     if (c >= 0 && up >= 0)
                         parent[(size_t)coff[l - 1] + c] = coff[l] + up;
                 }
-            std::vector<int> ptr((size_t)cn + 1, 0);
-            for (int c = 0; c < cn; ++c)
-                if (parent[c] >= 0)
-                    ptr[(size_t)parent[c] + 1]++;
-            for (int i = 0; i < cn; ++i)
-                ptr[i + 1] += ptr[i];
-            std::vector<int> fillp(ptr.begin(), ptr.end() - 1);
-            std::vector<int> ch(ptr[cn] > 0 ? ptr[cn] : 1);
-            for (int c = 0; c < cn; ++c)
-                if (parent[c] >= 0)
-                    ch[fillp[parent[c]]++] = c;
-            for (int i = 0; i < cn; ++i)
-                if (ptr[i + 1] - ptr[i] > 32)
-                    throw Error(ERR_INVALID, "[MAS] internal: coarse component with more than 32 children");
+            // The coarse-level sums rely on it: the children of every node share one 32-id group
+            // (so at most 32 children).
+            {
+                std::vector<int> group((size_t)cn, -1);
+                for (int c = 0; c < cn; ++c)
+                {
+                    const int pa = parent[c];
+                    if (pa < 0)
+                        continue;
+                    const int g = c >> 5; // coff[] are multiples of 32
+                    if (group[pa] < 0)
+                        group[pa] = g;
+                    else if (group[pa] != g)
+                        throw Error(ERR_INVALID, "[MAS] internal: coarse component spans two groups of 32");
+                }
+            }
             // Isolated-row suffix: the components of the trailing isolated banks must be the
             // largest ids at every level; otherwise the shortcut is off (first_iso_bank = banks).
             int fib = first_iso_bank < banks ? first_iso_bank : banks;
@@ -653,12 +699,12 @@ namespace pmas
                 cuda_check(cudaMemcpy(M.coarse_active.get(), active.data(), active.size() * sizeof(int),
                                       cudaMemcpyHostToDevice),
                            "active");
-            M.child_ptr.alloc(cn + 1, "MAS coarse_space children");
-            M.children.alloc(ch.size(), "MAS coarse_space children");
-            cuda_check(cudaMemcpy(M.child_ptr.get(), ptr.data(), ptr.size() * sizeof(int), cudaMemcpyHostToDevice),
-                       "children");
-            cuda_check(cudaMemcpy(M.children.get(), ch.data(), ch.size() * sizeof(int), cudaMemcpyHostToDevice),
-                       "children");
+            M.parent.alloc(cn > 0 ? cn : 1, "MAS coarse_space parents");
+            if (cn > 0)
+                cuda_check(cudaMemcpy(M.parent.get(), parent.data(), (size_t)cn * sizeof(int), cudaMemcpyHostToDevice),
+                           "parents");
+            M.ticket.alloc(1, "MAS coarse_space ticket");
+            cuda_check(cudaMemsetAsync(M.ticket.get(), 0, sizeof(unsigned), s), "memset");
         }
 
         // Coarse vectors (zero once: slots past the component counts stay zero).
@@ -669,61 +715,43 @@ namespace pmas
 
         // --- matrices
         const size_t S = (size_t)tile_packed_size(bd);
-        if (fp32)
-        {
-            M.inv64.reset();
-            M.inv32.alloc(S * M.total_mats, "MAS coarse_matrices");
-        }
-        else
-        {
-            M.inv32.reset();
+        M.inv64.reset();
+        M.inv32.reset();
+        M.inv16.reset();
+        if (storage == STORE_F64)
             M.inv64.alloc(S * M.total_mats, "MAS coarse_matrices");
-        }
-        switch (bd)
-        {
-        case 1:
-            if (fp32)
-                assemble_and_invert<1, float>(M, A, d_node_real, M.inv32.get(), coff, s);
-            else
-                assemble_and_invert<1, double>(M, A, d_node_real, M.inv64.get(), coff, s);
-            break;
-        case 2:
-            if (fp32)
-                assemble_and_invert<2, float>(M, A, d_node_real, M.inv32.get(), coff, s);
-            else
-                assemble_and_invert<2, double>(M, A, d_node_real, M.inv64.get(), coff, s);
-            break;
-        default:
-            if (fp32)
-                assemble_and_invert<3, float>(M, A, d_node_real, M.inv32.get(), coff, s);
-            else
-                assemble_and_invert<3, double>(M, A, d_node_real, M.inv64.get(), coff, s);
-            break;
-        }
+        else if (storage == STORE_F16)
+            M.inv16.alloc(S * M.total_mats, "MAS coarse_matrices");
+        else
+            M.inv32.alloc(S * M.total_mats, "MAS coarse_matrices");
+        M.inv_scale.alloc(M.total_mats > 0 ? M.total_mats : 1, "MAS coarse_matrices scales");
         M.identity.alloc(M.total_coarse > 0 ? M.total_coarse : 1, "MAS coarse_matrices identity");
         cuda_check(cudaMemsetAsync(M.identity.get(), 0, M.identity.bytes(), s), "memset");
-        if (M.total_coarse > 0)
-        {
-            if (fp32)
-            {
-                if (bd == 1)
-                    k_identity_flags<1, float><<<M.total_coarse, 256, 0, s>>>(M.inv32.get(), banks, M.total_coarse, M.identity.get());
-                else if (bd == 2)
-                    k_identity_flags<2, float><<<M.total_coarse, 256, 0, s>>>(M.inv32.get(), banks, M.total_coarse, M.identity.get());
-                else
-                    k_identity_flags<3, float><<<M.total_coarse, 256, 0, s>>>(M.inv32.get(), banks, M.total_coarse, M.identity.get());
-            }
+        auto run = [&](auto *out) {
+            using Out = std::remove_pointer_t<decltype(out)>;
+            auto per_bd = [&](auto bdc) {
+                constexpr int BD = decltype(bdc)::value;
+                assemble_and_invert<BD, Out>(M, A, d_node_real, out, coff, s);
+                if (M.total_coarse > 0)
+                {
+                    k_identity_flags<BD, Out><<<M.total_coarse, 256, 0, s>>>(out, M.inv_scale.get(), banks,
+                                                                            M.total_coarse, M.identity.get());
+                    cuda_check(cudaGetLastError(), "identity flags launch");
+                }
+            };
+            if (bd == 1)
+                per_bd(std::integral_constant<int, 1>{});
+            else if (bd == 2)
+                per_bd(std::integral_constant<int, 2>{});
             else
-            {
-                if (bd == 1)
-                    k_identity_flags<1, double><<<M.total_coarse, 256, 0, s>>>(M.inv64.get(), banks, M.total_coarse, M.identity.get());
-                else if (bd == 2)
-                    k_identity_flags<2, double><<<M.total_coarse, 256, 0, s>>>(M.inv64.get(), banks, M.total_coarse, M.identity.get());
-                else
-                    k_identity_flags<3, double><<<M.total_coarse, 256, 0, s>>>(M.inv64.get(), banks, M.total_coarse, M.identity.get());
-            }
-            cuda_check(cudaGetLastError(), "identity flags launch");
-        }
+                per_bd(std::integral_constant<int, 3>{});
+        };
+        if (storage == STORE_F64)
+            run(M.inv64.get());
+        else if (storage == STORE_F16)
+            run(reinterpret_cast<__half *>(M.inv16.get()));
+        else
+            run(M.inv32.get());
         int h_flag = 0;
         cuda_check(cudaMemcpyAsync(&h_flag, M.flag.get(), sizeof(int), cudaMemcpyDeviceToHost, s), "flag");
         cuda_check(cudaStreamSynchronize(s), "mas build");

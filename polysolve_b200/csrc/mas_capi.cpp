@@ -17,6 +17,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -41,7 +42,7 @@ namespace
         bool lazy = false;
         bool use_prec_norm = false;
         // Extensions; defaults reproduce the reference's algorithm.
-        bool fp32 = false;
+        int storage = STORE_F64; // precision of the stored MAS inverses
         int true_residual_period = 4;
         int check_period = 10;
         bool initial_guess_input = false;
@@ -133,9 +134,9 @@ namespace
         if (auto *v = m.find("precision"))
         {
             const std::string s = get_str(*v, "precision");
-            if (s != "fp64" && s != "fp32")
-                throw Error(ERR_INVALID, "[MAS] precision must be \"fp64\" or \"fp32\"");
-            q.fp32 = (s == "fp32");
+            if (s != "fp64" && s != "fp32" && s != "fp16")
+                throw Error(ERR_INVALID, "[MAS] precision must be \"fp64\", \"fp32\" or \"fp16\"");
+            q.storage = s == "fp64" ? STORE_F64 : (s == "fp32" ? STORE_F32 : STORE_F16);
         }
         if (auto *v = m.find("true_residual_period"))
         {
@@ -192,8 +193,6 @@ struct mas_solver
     int device = 0;
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr; // own_stream or the caller's (mas_set_stream)
-    cudaStream_t side = nullptr;   // coarse levels, concurrent with the level-0 MAS kernel
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     std::string last_error;
 
     // Kernel accounting: launches per kind, and CUDA-event time per kind when profiling.
@@ -262,12 +261,6 @@ struct mas_solver
                 cudaGraphExecDestroy(g);
         if (h_st)
             cudaFreeHost(h_st);
-        if (ev_fork)
-            cudaEventDestroy(ev_fork);
-        if (ev_join)
-            cudaEventDestroy(ev_join);
-        if (side)
-            cudaStreamDestroy(side);
         if (own_stream)
             cudaStreamDestroy(own_stream);
     }
@@ -340,18 +333,14 @@ struct mas_solver
         }
     }
 
-    // The MAS apply of r: coarse levels on the side stream, concurrent with the level-0 kernel,
-    // then the one-CTA finalize after the join. mode 1 = initial, 2 = iteration.
-    void apply_and_finalize(const MasView &mv, const PcgConfig &cfg, int pr, int mode)
+    // The MAS apply of the current r, whose level-0 restriction is already in rc: the coarse
+    // levels above the first, then every inverse (last CTA: PCG scalars). mode 1 = initial,
+    // 2 = iteration.
+    void apply_levels(const MasView &mv, const PcgConfig &cfg, int mode)
     {
         PcgState *S = st.get();
-        cuda_check(cudaEventRecord(ev_fork, stream), "fork");
-        cuda_check(cudaStreamWaitEvent(side, ev_fork, 0), "fork");
-        run_on(side, "mas_coarse", 0, [&] { return launch_coarse(mv, r.get(), S, red(), mode, pr, side); });
-        cuda_check(cudaEventRecord(ev_join, side), "join");
-        run("mas_symv0", 1, [&] { launch_symv0(mv, r.get(), z.get(), S, red(), cfg, 0, mode, stream); });
-        cuda_check(cudaStreamWaitEvent(stream, ev_join, 0), "join");
-        run("finalize", 1, [&] { launch_finalize(S, red(), cfg, mode, stream); });
+        run("coarse_levels", 0, [&] { return launch_coarse_levels(mv, S, stream); });
+        run("mas_apply", 1, [&] { launch_mas_apply(mv, r.get(), z.get(), S, red(), cfg, mode, stream); });
     }
 
     void collect_profile()
@@ -384,11 +373,6 @@ struct mas_solver
         }
         cuda_check(cudaGetDevice(&device), "get device");
         cuda_check(cudaStreamCreateWithFlags(&own_stream, cudaStreamNonBlocking), "stream create");
-        int lo = 0, hi = 0;
-        cuda_check(cudaDeviceGetStreamPriorityRange(&lo, &hi), "stream priorities");
-        cuda_check(cudaStreamCreateWithPriority(&side, cudaStreamNonBlocking, hi), "stream create");
-        cuda_check(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming), "event create");
-        cuda_check(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming), "event create");
         stream = own_stream;
         cuda_check(cudaMallocHost(&h_st, 2 * sizeof(PcgState)), "pinned state");
     }
@@ -486,8 +470,8 @@ struct mas_solver
                 if (!iso[v] && padded[v] / 32 >= first_iso_bank)
                     first_iso_bank = banks;
         }
-        build_mas(mas, A, d_node_real.get(), p.fp32 ? 1 : 0, first_iso_bank, stream);
-        prepare_kernels(bd_, p.fp32 ? 1 : 0);
+        build_mas(mas, A, d_node_real.get(), p.storage, first_iso_bank, stream);
+        prepare_kernels(bd_, p.storage);
         drop_graph();
 
         const size_t len = (size_t)banks * 32 * bd_;
@@ -520,7 +504,7 @@ struct mas_solver
     {
         double *base = partials.get();
         const size_t c = (size_t)red_capacity;
-        return ReduceBuf{base, red_capacity, base + 2 * c, base + 3 * c, base + 7 * c};
+        return ReduceBuf{base, red_capacity, base + 2 * c, base + 3 * c};
     }
 
     PcgConfig config() const
@@ -537,16 +521,20 @@ struct mas_solver
     }
 
     // One PCG iteration's kernels (MASSolver.cu:498-583). residual: launch the true-residual SpMV
-    // (it also checks (st->iter + 1) % P == 0 on the device and returns at once otherwise).
-    void launch_iteration(const BankedView &Av, const MasView &mv, const PcgConfig &cfg, int P, int pr, bool residual)
+    // and its restriction (both check (st->iter + 1) % P == 0 on the device and return at once
+    // otherwise; update_xr restricts r on the other iterations).
+    void launch_iteration(const BankedView &Av, const MasView &mv, const PcgConfig &cfg, int P, bool residual)
     {
         PcgState *S = st.get();
         run("spmv_pap", 1, [&] { launch_spmv(SPMV_PAP, Av, pv.get(), Ap.get(), nullptr, S, red(), 1, 0, stream); });
-        run("update_xr", 1, [&] { launch_update_xr(banks, bd, x.get(), r.get(), pv.get(), Ap.get(), S, red(), P, stream); });
+        run("update_xr", 1, [&] { launch_update_xr(mv, x.get(), r.get(), pv.get(), Ap.get(), S, red(), P, stream); });
         if (residual)
+        {
             run("spmv_residual", 1,
                 [&] { launch_spmv(SPMV_RESIDUAL, Av, x.get(), r.get(), b.get(), S, red(), 1, P, stream); });
-        apply_and_finalize(mv, cfg, pr, 2);
+            run("restrict", 0, [&] { return launch_restrict(mv, r.get(), S, P, stream); });
+        }
+        apply_levels(mv, cfg, 2);
         run("update_p", 1, [&] { launch_update_p(mv, pv.get(), z.get(), S, 0, stream); });
     }
 
@@ -562,7 +550,7 @@ struct mas_solver
         graph_key = 0;
     }
 
-    void capture(int slot, const BankedView &Av, const MasView &mv, const PcgConfig &cfg, int P, int pr, int chunk,
+    void capture(int slot, const BankedView &Av, const MasView &mv, const PcgConfig &cfg, int P, int chunk,
                  bool aligned)
     {
         cudaGraph_t graph = nullptr;
@@ -572,7 +560,7 @@ struct mas_solver
         try
         {
             for (int i = 0; i < chunk; ++i)
-                launch_iteration(Av, mv, cfg, P, pr, aligned ? (slot == 1 && i == chunk - 1) : true);
+                launch_iteration(Av, mv, cfg, P, aligned ? (slot == 1 && i == chunk - 1) : true);
         }
         catch (...)
         {
@@ -591,7 +579,7 @@ struct mas_solver
         cuda_check(e, "graph instantiate");
     }
 
-    void ensure_graph(const BankedView &Av, const MasView &mv, const PcgConfig &cfg, int P, int pr, int chunk)
+    void ensure_graph(const BankedView &Av, const MasView &mv, const PcgConfig &cfg, int P, int chunk)
     {
         uint64_t key = 1469598103934665603ull;
         auto mix = [&key](uint64_t v) {
@@ -613,15 +601,14 @@ struct mas_solver
         std::memcpy(&bits, &cfg.abs_tol, 8);
         mix(bits);
         mix((uint64_t)P);
-        mix((uint64_t)pr);
         mix((uint64_t)chunk);
         if (graph_exec[0] && key == graph_key)
             return;
         drop_graph();
         graph_aligned = (P % chunk == 0);
-        capture(0, Av, mv, cfg, P, pr, chunk, graph_aligned);
+        capture(0, Av, mv, cfg, P, chunk, graph_aligned);
         if (graph_aligned)
-            capture(1, Av, mv, cfg, P, pr, chunk, true);
+            capture(1, Av, mv, cfg, P, chunk, true);
         graph_key = key;
     }
 
@@ -641,10 +628,10 @@ struct mas_solver
         for (auto &ks : kstats) // per-solve kernel statistics
             ks.second = KStat{};
         launch_pcg_init_state(S, stream);
-        const int pr = p.polak_ribiere ? 1 : 0;
-        // r = b - A x, its level-0 restriction and rr0
+        // r = b - A x, rr0, the level-0 restriction of r, then z = M^-1 r
         run("spmv_residual", 1, [&] { launch_spmv(SPMV_RESIDUAL, Av, x.get(), r.get(), b.get(), S, red(), 0, 0, stream); });
-        apply_and_finalize(mv, cfg, pr, 1);
+        run("restrict", 0, [&] { return launch_restrict(mv, r.get(), S, 0, stream); });
+        apply_levels(mv, cfg, 1);
         run("update_p", 1, [&] { launch_update_p(mv, pv.get(), z.get(), S, 1, stream); });
         cuda_check(cudaMemcpyAsync(&h_st[0], S, sizeof(PcgState), cudaMemcpyDeviceToHost, stream), "state");
         cuda_check(cudaStreamSynchronize(stream), "pcg init");
@@ -661,7 +648,7 @@ struct mas_solver
         const int chunk = p.poll_period;
         const bool graphs = p.graphs && !p.profile;
         if (graphs)
-            ensure_graph(Av, mv, cfg, P, pr, chunk);
+            ensure_graph(Av, mv, cfg, P, chunk);
         int launched = 0;
         bool stop = false;
         int pending = -1; // slot holding the previous chunk's state copy
@@ -684,7 +671,7 @@ struct mas_solver
             }
             else
                 for (int k = k0; k <= k1; ++k)
-                    launch_iteration(Av, mv, cfg, P, pr, k % P == 0);
+                    launch_iteration(Av, mv, cfg, P, k % P == 0);
             launched = k1;
             const int slot = (slot_flip++) & 1;
             cuda_check(cudaMemcpyAsync(&h_st[slot], S, sizeof(PcgState), cudaMemcpyDeviceToHost, stream), "state");
@@ -787,7 +774,8 @@ struct mas_solver
         o.obj.emplace_back("solver_status", str(status_string(status)));
         const double ref = p.use_prec_norm ? std::sqrt(std::fabs(rz0)) : std::sqrt(std::fabs(rr0));
         o.obj.emplace_back("relative_residual", num(ref > 0 ? residual_norm / ref : 0.0, false));
-        o.obj.emplace_back("precision", str(p.fp32 ? "fp32" : "fp64"));
+        o.obj.emplace_back("precision",
+                           str(p.storage == STORE_F64 ? "fp64" : (p.storage == STORE_F32 ? "fp32" : "fp16")));
         o.obj.emplace_back("x0_source", str(p.initial_guess_input ? "input" : "zero"));
         o.obj.emplace_back("ordering", str(ordering_used));
         o.obj.emplace_back("solve_ms", num(solve_ms, false));
@@ -1132,6 +1120,23 @@ extern "C" int mas_get_coarse_map(const mas_solver *h, int *map, int nodes)
     });
 }
 
+namespace
+{
+    // IEEE binary16 bit pattern -> value.
+    double half_bits_to_double(uint16_t h)
+    {
+        const int sign = h >> 15, e = (h >> 10) & 31, m = h & 1023;
+        double v;
+        if (e == 0)
+            v = std::ldexp((double)m, -24);
+        else if (e == 31)
+            v = m ? std::numeric_limits<double>::quiet_NaN() : std::numeric_limits<double>::infinity();
+        else
+            v = std::ldexp((double)(m + 1024), e - 25);
+        return sign ? -v : v;
+    }
+} // namespace
+
 extern "C" int mas_get_inverses(const mas_solver *h, double *out, size_t count)
 {
     if (!h || !out || !h->factorized)
@@ -1145,12 +1150,24 @@ extern "C" int mas_get_inverses(const mas_solver *h, double *out, size_t count)
     return guarded(hh, [&] {
         cuda_check(cudaSetDevice(h->device), "set device");
         std::vector<double> tp(count);
-        if (h->mas.fp32)
+        if (h->mas.storage == STORE_F32)
         {
             std::vector<float> f(count);
             cuda_check(cudaMemcpy(f.data(), h->mas.inv32.get(), sizeof(float) * count, cudaMemcpyDeviceToHost), "inv");
             for (size_t i = 0; i < count; ++i)
                 tp[i] = f[i];
+        }
+        else if (h->mas.storage == STORE_F16)
+        {
+            std::vector<uint16_t> f(count);
+            std::vector<double> sc((size_t)h->mas.total_mats);
+            cuda_check(cudaMemcpy(f.data(), h->mas.inv16.get(), sizeof(uint16_t) * count, cudaMemcpyDeviceToHost),
+                       "inv");
+            cuda_check(cudaMemcpy(sc.data(), h->mas.inv_scale.get(), sizeof(double) * sc.size(),
+                                  cudaMemcpyDeviceToHost),
+                       "inv scale");
+            for (size_t i = 0; i < count; ++i)
+                tp[i] = half_bits_to_double(f[i]) * sc[i / S];
         }
         else
             cuda_check(cudaMemcpy(tp.data(), h->mas.inv64.get(), sizeof(double) * count, cudaMemcpyDeviceToHost), "inv");
@@ -1187,8 +1204,9 @@ extern "C" int mas_debug_apply(mas_solver *h, const double *rin, double *zout, i
             throw Error(ERR_NOT_FACTORIZED, "[MAS] debug_apply: size mismatch.");
         cuda_check(cudaMemcpyAsync(h->r.get(), rin, sizeof(double) * len, cudaMemcpyHostToDevice, h->stream), "r");
         const MasView mv = h->mas.view();
-        launch_coarse(mv, h->r.get(), nullptr, h->red(), 0, 0, h->stream);
-        launch_symv0(mv, h->r.get(), h->z.get(), nullptr, h->red(), h->config(), 0, 0, h->stream);
+        launch_restrict(mv, h->r.get(), nullptr, 0, h->stream);
+        launch_coarse_levels(mv, nullptr, h->stream);
+        launch_mas_apply(mv, h->r.get(), h->z.get(), nullptr, h->red(), h->config(), 0, h->stream);
         launch_prolong(mv, h->z.get(), h->Ap.get(), h->stream);
         cuda_check(cudaMemcpyAsync(zout, h->Ap.get(), sizeof(double) * len, cudaMemcpyDeviceToHost, h->stream), "z");
         cuda_check(cudaStreamSynchronize(h->stream), "apply");

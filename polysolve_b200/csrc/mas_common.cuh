@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "mas_internal.h"
@@ -9,6 +10,43 @@
 namespace pmas
 {
     constexpr unsigned FULL = 0xFFFFFFFFu;
+
+    // Inverse storage types: the arithmetic type of each and loads of one / four consecutive
+    // stored values converted to it. Binary16 values are read as IEEE bits (the buffers are
+    // uint16_t on the host) and multiplied in FP32.
+    template <class Store>
+    struct StoreTraits;
+    template <>
+    struct StoreTraits<double>
+    {
+        using Real = double;
+        static constexpr bool SCALED = false;
+    };
+    template <>
+    struct StoreTraits<float>
+    {
+        using Real = float;
+        static constexpr bool SCALED = false;
+    };
+    template <>
+    struct StoreTraits<__half>
+    {
+        using Real = float;
+        static constexpr bool SCALED = true;
+    };
+
+    __device__ __forceinline__ double4 load4(const double *p) { return *reinterpret_cast<const double4 *>(p); }
+    __device__ __forceinline__ float4 load4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+    __device__ __forceinline__ float4 load4(const __half *p)
+    {
+        const uint2 u = *reinterpret_cast<const uint2 *>(p);
+        const float2 a = __half22float2(*reinterpret_cast<const __half2 *>(&u.x));
+        const float2 b = __half22float2(*reinterpret_cast<const __half2 *>(&u.y));
+        return make_float4(a.x, a.y, b.x, b.y);
+    }
+    __device__ __forceinline__ double load1(const double *p) { return *p; }
+    __device__ __forceinline__ float load1(const float *p) { return *p; }
+    __device__ __forceinline__ float load1(const __half *p) { return __half2float(*p); }
 
     __device__ __forceinline__ double warp_sum(double v)
     {
@@ -138,6 +176,33 @@ namespace pmas
             }
             pending &= ~__ballot_sync(FULL, in);
         }
+    }
+
+    // Level-0 restriction of one bank: reg[t] holds the bank's values t * 32 + lane (coalesced
+    // layout); the values are regrouped by node with shuffles and summed per connected component
+    // of the bank into rc (first coarse level). Every lane of the warp must call it.
+    template <int BD>
+    __device__ __forceinline__ void bank_restrict(const double (&reg)[BD], int bank, const int *__restrict__ lcco0,
+                                                  const int *__restrict__ cco0_base, double *rc)
+    {
+        const int lane = threadIdx.x & 31;
+        double rv[BD];
+#pragma unroll
+        for (int i = 0; i < BD; ++i)
+        {
+            const int e = lane * BD + i; // this lane's node, component i
+            const int src = e & 31, tsel = e >> 5;
+            double v = 0.0;
+#pragma unroll
+            for (int t = 0; t < BD; ++t)
+            {
+                const double got = __shfl_sync(FULL, reg[t], src);
+                if (t == tsel)
+                    v = got;
+            }
+            rv[i] = v;
+        }
+        warp_segment_store<BD>(rv, lcco0[(long long)bank * 32 + lane], cco0_base[bank], rc);
     }
 
     // ---------------------------------------------------------------------------------------

@@ -19,6 +19,15 @@ namespace pmas
     constexpr int MAX_COARSE = 4; // coarse levels (MASPreconditioner.hpp:11)
     constexpr int LEVELS = MAX_COARSE + 1;
 
+    // Storage precision of the subdomain inverses. FP16 keeps one power-of-two scale per matrix
+    // (largest magnitude -> [2^14, 2^15)); products are formed in FP32 and scaled back in FP64.
+    enum : int
+    {
+        STORE_F64 = 0,
+        STORE_F32 = 1,
+        STORE_F16 = 2,
+    };
+
     // Status codes (mirror include/polysolve_mas.h).
     enum : int
     {
@@ -141,7 +150,7 @@ namespace pmas
         int mat_offsets[LEVELS];      // first matrix of each matrix level (0 = banks)
         int mat_counts[LEVELS];
         int cco_nums[MAX_COARSE];
-        int fp32;               // storage precision of the inverses
+        int storage;            // STORE_F64 / STORE_F32 / STORE_F16
         // Banks >= first_iso_bank hold only isolated rows (no off-diagonal block). Such a row is its
         // own component at every level with coarse block A_uu, so z_u = (1 + level_num) z0_u and the
         // coarse levels can skip it: only components < real_count[l] and the coarse matrices in
@@ -150,12 +159,13 @@ namespace pmas
         int real_count[MAX_COARSE];
         int n_coarse_active;
         const int *coarse_active;
-        const void *inv;        // total_mats * tile_packed_size(bd), float or double
+        const void *inv;        // total_mats * tile_packed_size(bd): double, float or binary16
+        const double *inv_scale; // total_mats: value = stored value * inv_scale (1 unless FP16)
         const int *lcco0;       // nodes: bank-local level-0 component id, -1 virtual
         const int *cco0_base;   // banks: first global level-0 component id of the bank
         const int4 *cslot;      // nodes: coarse-vector node of each coarse level (-1 unused)
-        const int *child_ptr;   // coarse nodes + 1: CSR of the (<= 32) previous-level coarse nodes
-        const int *children;    //   merged into each coarse node of levels >= 1
+        const int *parent;      // coarse nodes: the next level's coarse node it merges into (-1: none)
+        unsigned *ticket;       // arrival counter of the coarse-level kernel (zero between launches)
         const int *identity;    // coarse matrices: 1 if the inverse is exactly the identity
         double *rc;             // coarse residual, coarse nodes * bd (level-0 components first)
         double *zc;             // coarse correction, coarse nodes * bd
@@ -170,7 +180,8 @@ namespace pmas
         int done;      // 1: converged / stopped; kernels return immediately
         int status;    // MAS_STATUS_*
         int error;     // device-detected error code (ERR_NONFINITE, ERR_TIMEOUT)
-        int n_rr, n_rz, n_co; // CTAs that wrote rr_parts / rz_parts / co_parts this iteration
+        // Arrival tickets of the grid reductions: [0] SpMV p.Ap / initial residual, [1] update_xr,
+        // [2] in-loop true residual, [4] MAS apply. The last CTA resets its ticket to zero.
         unsigned int counter[8];
     };
 
@@ -184,17 +195,15 @@ namespace pmas
         int level_num; // coarse levels in use (isolated rows: z = (1 + level_num) z0)
     };
 
-    // Scratch for deterministic two-stage reductions: per-CTA partials.
-    // Per-CTA partial sums. The SpMV's p.Ap uses a ticket (its last CTA sums `partials`); the dots
-    // of the rest of an iteration are written per CTA and summed by the one-CTA finalize kernel, so
-    // short kernels never queue on a ticket counter.
+    // Scratch of the deterministic two-stage reductions: every CTA writes its partial sums, the
+    // last CTA to arrive (atomic ticket) adds them in a fixed order.
     struct ReduceBuf
     {
-        double *partials; // 2 * capacity
+        double *partials; // 2 * capacity: SpMV p.Ap (and b.b on the initial residual)
         int capacity;     // max CTAs of any reduced launch
         double *rr_parts; // capacity: r.r from the kernel that produced r this iteration
-        double *rz_parts; // 4 * capacity: r.z0, r.z0_old, and both over isolated banks (MAS level 0)
-        double *co_parts; // 2 * capacity: rc.zc and rc.zc_old from the coarse kernel
+        double *rz_parts; // 6 * capacity: the MAS apply's dots (r.z0, r.z0_old, the same over
+                          // isolated banks, rc.zc, rc.zc_old)
     };
 
     // ---------------------------------------------------------------------------------------
@@ -231,7 +240,7 @@ namespace pmas
     {
         SPMV_PLAIN = 0,    // y = A x
         SPMV_PAP = 1,      // y = A p ; pAp = p . y ; alpha = rz / pAp
-        SPMV_RESIDUAL = 2, // y = b - A x ; restrict y to level-0 components ; rr = y . y
+        SPMV_RESIDUAL = 2, // y = b - A x ; rr = y . y (iter 0: also rr0 = b . b)
     };
     // period > 0 (SPMV_RESIDUAL in the PCG loop): runs only when (st->iter + 1) % period == 0.
     void launch_spmv(int mode, const BankedView &A, const double *x, double *y, const double *b, PcgState *st,
@@ -239,8 +248,8 @@ namespace pmas
 
     // mas_pcg.cu
     // x += alpha p; unless this iteration recomputes the true residual ((st->iter + 1) % period == 0):
-    // r -= alpha Ap and per-CTA r . r.
-    void launch_update_xr(int banks, int bd, double *x, double *r, const double *p, const double *Ap, PcgState *st,
+    // r -= alpha Ap, rr = r . r and the level-0 restriction of r into rc.
+    void launch_update_xr(const MasView &mas, double *x, double *r, const double *p, const double *Ap, PcgState *st,
                           ReduceBuf red, int period, cudaStream_t s);
     // p = z0 + prolongation(zc) + beta p (z0: level-0 part of z = M^-1 r)
     void launch_update_p(const MasView &mas, double *p, const double *z0, PcgState *st, int first, cudaStream_t s);
@@ -250,23 +259,22 @@ namespace pmas
                             cudaStream_t s);
     void launch_pcg_init_state(PcgState *st, cudaStream_t s);
 
-    // mas_apply.cu. mode: 0 = plain apply (no PCG bookkeeping), 1 = initial (rz0), 2 = iteration.
-    // Coarse levels: level-0 restriction of r (per-bank component sums), hierarchical sums of the
-    // higher levels, then every coarse matrix times its residual (zc) and, in PCG modes, per-CTA
-    // rc . zc (and rc . zc_old). Returns the number of kernels launched.
-    int launch_coarse(const MasView &mas, const double *r, PcgState *st, ReduceBuf red, int mode, int polak_ribiere,
-                      cudaStream_t s);
-    // Level-0 subdomains: z0 = A_0^-1 r per bank; in PCG modes per-CTA r . z0 (and r . z0_old).
-    void launch_symv0(const MasView &mas, const double *r, double *z0, PcgState *st, ReduceBuf red, PcgConfig cfg,
-                      int iter, int mode, cudaStream_t s);
-    // One CTA: sums the iteration's partials (rr, r.z0, rc.zc) and runs the reference's per-iteration
-    // bookkeeping (rz, convergence test, status, beta; MASSolver.cu:505, 526-583). mode 1 = initial.
-    void launch_finalize(PcgState *st, ReduceBuf red, PcgConfig cfg, int mode, cudaStream_t s);
-    // z = z0 + prolongation(zc) (outside the PCG loop).
+    // mas_apply.cu: the MAS apply. The coarse residual rc is built by the level-0 restriction
+    // (fused into update_xr, or launch_restrict) and launch_coarse_levels; launch_mas_apply then
+    // multiplies every inverse.
+    // Level-0 restriction of r into rc (with period > 0: only on true-residual iterations);
+    // returns the number of kernels launched.
+    int launch_restrict(const MasView &mas, const double *r, const PcgState *st, int period, cudaStream_t s);
+    // Coarse levels >= 2 summed from the first coarse level; returns the number of kernels launched.
+    int launch_coarse_levels(const MasView &mas, const PcgState *st, cudaStream_t s);
+    // z0 = A_0^-1 r and zc = A_l^-1 rc for all coarse levels (rc must be complete); mode 1 / 2 also
+    // run the PCG scalar step in the last CTA (1: initial apply, 2: iteration).
+    void launch_mas_apply(const MasView &mas, const double *r, double *z0, PcgState *st, ReduceBuf red,
+                          PcgConfig cfg, int mode, cudaStream_t s);
     void launch_prolong(const MasView &mas, const double *z0, double *z, cudaStream_t s);
     // Set kernel attributes (large shared memory) for every variant used with this block size and
     // precision, so launches inside a CUDA graph capture never touch function attributes.
-    void prepare_kernels(int bd, int fp32);
+    void prepare_kernels(int bd, int storage);
     int device_sm_count();
 
     // mas_build.cu: the MAS hierarchy and inverses.
@@ -279,13 +287,14 @@ namespace pmas
         int mat_offsets[LEVELS] = {0, 0, 0, 0, 0};
         int total_mats = 0, total_coarse = 0;
         int coarse_nodes = 0;
-        int fp32 = 1;
+        int storage = STORE_F32;
         DevBuf<int> node_real;   // nodes: 1 if the node is a real block row
         DevBuf<int> map;         // nodes * 4
         DevBuf<int> lcco0;
         DevBuf<int> cco0_base;
         DevBuf<int4> cslot;
-        DevBuf<int> child_ptr, children, identity;
+        DevBuf<int> parent, identity;
+        DevBuf<unsigned> ticket;
         int first_iso_bank = 0;
         int real_count[MAX_COARSE] = {0, 0, 0, 0};
         DevBuf<int> coarse_active;
@@ -293,13 +302,15 @@ namespace pmas
         int coff[MAX_COARSE] = {0, 0, 0, 0};
         DevBuf<float> inv32;
         DevBuf<double> inv64;
+        DevBuf<uint16_t> inv16;  // IEEE binary16 bits
+        DevBuf<double> inv_scale;
         DevBuf<double> rc, zc;
         DevBuf<int> flag;        // device error flag for the inverses
         MasView view(double *rc_override = nullptr) const;
     };
 
     // first_iso_bank: first bank of the trailing isolated rows (banks if none / not trailing).
-    void build_mas(MasDevice &M, const BankedMatrix &A, const int *d_node_real, int fp32, int first_iso_bank,
+    void build_mas(MasDevice &M, const BankedMatrix &A, const int *d_node_real, int storage, int first_iso_bank,
                    cudaStream_t s);
 
     // mas_pcg.cu: misc

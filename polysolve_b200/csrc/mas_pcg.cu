@@ -2,15 +2,17 @@
 //
 // The reference runs each vector step as its own launch (axpby / inner_product / scalar_division,
 // MASSolver.cu:46-81, InnerProduct.cu:16-45) with a memset and an FP64 atomicAdd per dot. Here:
-//   update_xr: x += alpha p ; r -= alpha Ap ; rr = r . r            (one pass; on true-residual
-//              iterations only x, then r = b - A x follows in the SpMV)
+//   update_xr: x += alpha p ; r -= alpha Ap ; rr = r . r ; level-0 restriction of r  (one pass;
+//              on true-residual iterations only x, then r = b - A x follows in the SpMV)
 //   update_p:  p = z0 + P zc + beta p             (the MAS prolongation fused in; beta from the
 //                                                  device state, set by the MAS apply)
 // alpha / beta are read from the device-resident PcgState, and every dot is a deterministic
 // two-stage reduction, so no host round trip is needed inside the iteration.
 
 #include <cstdio>
+#include <mutex>
 #include <string>
+#include <unordered_map>
 
 #include "mas_common.cuh"
 
@@ -50,9 +52,12 @@ namespace pmas
     {
         constexpr int UPD_THREADS = 256;
 
-        // x += alpha p ; r -= alpha Ap ; per-CTA r . r (summed by the finalize kernel). Grid-stride
-        // over the vectors with coalesced accesses. On a true-residual iteration only x is updated.
-        __global__ void __launch_bounds__(UPD_THREADS) k_update_xr(long long len, double *__restrict__ x,
+        // x += alpha p ; r -= alpha Ap ; rr = r . r (ticket: the last CTA sums the partials) ; and
+        // the level-0 restriction of the new r (per-bank component sums, the MAS apply's first
+        // step). One warp per bank, its 32 * BD values read coalesced (value t * 32 + lane). On a
+        // true-residual iteration only x is updated: r, rr and the restriction follow the SpMV.
+        template <int BD>
+        __global__ void __launch_bounds__(UPD_THREADS) k_update_xr(MasView mas, double *__restrict__ x,
                                                                    double *__restrict__ r, const double *__restrict__ p,
                                                                    const double *__restrict__ Ap, PcgState *st,
                                                                    ReduceBuf red, int period)
@@ -61,28 +66,47 @@ namespace pmas
                 return;
             const double alpha = st->alpha;
             const bool due = period > 0 && (st->iter + 1) % period == 0;
-            const long long stride = (long long)gridDim.x * UPD_THREADS;
+            const int lane = threadIdx.x & 31;
+            const int total_warps = gridDim.x * (UPD_THREADS / 32);
+            const bool restrict_r = !due && mas.level_num > 0;
             double part = 0.0;
+            for (int bank = blockIdx.x * (UPD_THREADS / 32) + (threadIdx.x >> 5); bank < mas.banks; bank += total_warps)
+            {
+                const long long b0 = (long long)bank * 32 * BD + lane;
+                // All loads of the bank first (one memory round trip), then the updates.
+                double xv[BD], pv[BD], av[BD], rv[BD];
+#pragma unroll
+                for (int t = 0; t < BD; ++t)
+                {
+                    xv[t] = x[b0 + t * 32];
+                    pv[t] = p[b0 + t * 32];
+                    av[t] = 0.0;
+                    rv[t] = 0.0;
+                    if (!due)
+                    {
+                        av[t] = Ap[b0 + t * 32];
+                        rv[t] = r[b0 + t * 32];
+                    }
+                }
+#pragma unroll
+                for (int t = 0; t < BD; ++t)
+                {
+                    x[b0 + t * 32] = fma(alpha, pv[t], xv[t]);
+                    if (!due)
+                    {
+                        rv[t] = fma(-alpha, av[t], rv[t]);
+                        r[b0 + t * 32] = rv[t];
+                        part = fma(rv[t], rv[t], part);
+                    }
+                }
+                if (restrict_r && bank < mas.first_iso_bank)
+                    bank_restrict<BD>(rv, bank, mas.lcco0, mas.cco0_base, mas.rc);
+            }
             if (due)
-            {
-                for (long long i = blockIdx.x * (long long)UPD_THREADS + threadIdx.x; i < len; i += stride)
-                    x[i] = fma(alpha, p[i], x[i]);
                 return;
-            }
-            for (long long i = blockIdx.x * (long long)UPD_THREADS + threadIdx.x; i < len; i += stride)
-            {
-                x[i] = fma(alpha, p[i], x[i]);
-                const double rv = fma(-alpha, Ap[i], r[i]);
-                r[i] = rv;
-                part = fma(rv, rv, part);
-            }
-            const double rr = block_sum<UPD_THREADS>(part);
-            if (threadIdx.x == 0)
-            {
-                red.rr_parts[blockIdx.x] = rr;
-                if (blockIdx.x == 0)
-                    st->n_rr = gridDim.x;
-            }
+            double v1[1] = {part}, tot[1];
+            if (grid_reduce<1, UPD_THREADS>(v1, red.rr_parts, &st->counter[1], tot) && threadIdx.x == 0)
+                st->rr = tot[0];
         }
 
         // p = z0 + sum_l zc[cslot_l(node)] + beta p; warps stride over banks, coalesced.
@@ -113,23 +137,34 @@ namespace pmas
                     }
                     continue;
                 }
+                // Loads first (z0, p and the coarse slots), then the coarse-value gathers.
+                double zv[BD], pold[BD];
+                int4 cs[BD];
 #pragma unroll
                 for (int t = 0; t < BD; ++t)
                 {
                     const int e = t * 32 + lane;
-                    const int node = e / BD, comp = e - node * BD;
-                    const int4 cs = mas.cslot[(long long)bank * 32 + node];
-                    const long long idx = b0 + e;
-                    double v = z0[idx];
-                    if (cs.x >= 0)
-                        v += zc[(size_t)cs.x * BD + comp];
-                    if (cs.y >= 0)
-                        v += zc[(size_t)cs.y * BD + comp];
-                    if (cs.z >= 0)
-                        v += zc[(size_t)cs.z * BD + comp];
-                    if (cs.w >= 0)
-                        v += zc[(size_t)cs.w * BD + comp];
-                    p[idx] = first ? v : fma(beta, p[idx], v);
+                    const int node = e / BD;
+                    zv[t] = z0[b0 + e];
+                    pold[t] = first ? 0.0 : p[b0 + e];
+                    cs[t] = mas.cslot[(long long)bank * 32 + node];
+                }
+#pragma unroll
+                for (int t = 0; t < BD; ++t)
+                {
+                    const int e = t * 32 + lane;
+                    const int comp = e - (e / BD) * BD;
+                    // Unconditional loads (slot -1 reads zc[comp], then drops it): all in flight.
+                    const double g0 = zc[(size_t)max(cs[t].x, 0) * BD + comp];
+                    const double g1 = zc[(size_t)max(cs[t].y, 0) * BD + comp];
+                    const double g2 = zc[(size_t)max(cs[t].z, 0) * BD + comp];
+                    const double g3 = zc[(size_t)max(cs[t].w, 0) * BD + comp];
+                    double v = zv[t];
+                    v += cs[t].x >= 0 ? g0 : 0.0;
+                    v += cs[t].y >= 0 ? g1 : 0.0;
+                    v += cs[t].z >= 0 ? g2 : 0.0;
+                    v += cs[t].w >= 0 ? g3 : 0.0;
+                    p[b0 + e] = first ? v : fma(beta, pold[t], v);
                 }
             }
         }
@@ -176,47 +211,76 @@ namespace pmas
 
     namespace
     {
-        int bank_grid(int banks)
+        // CTAs of UPD_THREADS threads of `kernel` resident on the whole device at once.
+        template <class K>
+        int resident_ctas(K kernel)
+        {
+            static std::mutex mu;
+            static std::unordered_map<const void *, int> cache; // kernel -> CTAs per SM
+            int per_sm = 0;
+            {
+                std::lock_guard<std::mutex> lock(mu);
+                auto it = cache.find((const void *)kernel);
+                if (it != cache.end())
+                    per_sm = it->second;
+            }
+            if (per_sm == 0)
+            {
+                if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, UPD_THREADS, 0) != cudaSuccess ||
+                    per_sm < 1)
+                {
+                    cudaGetLastError();
+                    per_sm = 1;
+                }
+                std::lock_guard<std::mutex> lock(mu);
+                cache[(const void *)kernel] = per_sm;
+            }
+            return per_sm * device_sm_count();
+        }
+
+        template <class K>
+        int bank_grid(int banks, K kernel)
         {
             const int need = (banks + UPD_THREADS / 32 - 1) / (UPD_THREADS / 32);
-            const int cap = device_sm_count() * 8;
+            const int cap = resident_ctas(kernel);
             return need < cap ? need : cap;
         }
     } // namespace
 
-    void launch_update_xr(int banks, int bd, double *x, double *r, const double *p, const double *Ap, PcgState *st,
+    void launch_update_xr(const MasView &mas, double *x, double *r, const double *p, const double *Ap, PcgState *st,
                           ReduceBuf red, int period, cudaStream_t s)
     {
-        const long long len = (long long)banks * 32 * bd;
-        long long g = (len + UPD_THREADS - 1) / UPD_THREADS;
-        const long long cap = (long long)device_sm_count() * 8;
-        if (g > cap)
-            g = cap;
-        if (g < 1)
-            g = 1;
-        if (g > red.capacity)
-            throw Error(ERR_INVALID, "[MAS] reduction scratch too small");
-        k_update_xr<<<(int)g, UPD_THREADS, 0, s>>>(len, x, r, p, Ap, st, red, period);
+        auto go = [&](auto kernel) {
+            // One resident wave: as many CTAs as fit on the device at once.
+            int grid = bank_grid(mas.banks, kernel);
+            if (grid < 1)
+                grid = 1;
+            if (grid > red.capacity)
+                throw Error(ERR_INVALID, "[MAS] reduction scratch too small");
+            kernel<<<grid, UPD_THREADS, 0, s>>>(mas, x, r, p, Ap, st, red, period);
+        };
+        if (mas.bd == 1)
+            go(k_update_xr<1>);
+        else if (mas.bd == 2)
+            go(k_update_xr<2>);
+        else
+            go(k_update_xr<3>);
         cuda_check(cudaGetLastError(), "update_xr launch");
     }
 
     void launch_update_p(const MasView &mas, double *p, const double *z0, PcgState *st, int first, cudaStream_t s)
     {
-        const int grid = bank_grid(mas.banks);
-        if (grid == 0)
-            return;
-        switch (mas.bd)
-        {
-        case 1:
-            k_update_p<1><<<grid, UPD_THREADS, 0, s>>>(mas, p, z0, st, first);
-            break;
-        case 2:
-            k_update_p<2><<<grid, UPD_THREADS, 0, s>>>(mas, p, z0, st, first);
-            break;
-        default:
-            k_update_p<3><<<grid, UPD_THREADS, 0, s>>>(mas, p, z0, st, first);
-            break;
-        }
+        auto go = [&](auto kernel) {
+            const int grid = bank_grid(mas.banks, kernel);
+            if (grid > 0)
+                kernel<<<grid, UPD_THREADS, 0, s>>>(mas, p, z0, st, first);
+        };
+        if (mas.bd == 1)
+            go(k_update_p<1>);
+        else if (mas.bd == 2)
+            go(k_update_p<2>);
+        else
+            go(k_update_p<3>);
         cuda_check(cudaGetLastError(), "update_p launch");
     }
 

@@ -104,14 +104,10 @@ namespace pmas
                 return;
             if (MODE == SPMV_RESIDUAL && period > 0)
             {
-                // In-loop true residual: per-CTA r.r partials, summed by the finalize kernel.
-                const double rr = block_sum<SPMV_THREADS>(part);
-                if (threadIdx.x == 0)
-                {
-                    red.rr_parts[blockIdx.x] = rr;
-                    if (blockIdx.x == 0)
-                        st->n_rr = gridDim.x;
-                }
+                // In-loop true residual: rr = r . r (ticket on its own counter).
+                double v1[1] = {part}, t1[1];
+                if (grid_reduce<1, SPMV_THREADS>(v1, red.rr_parts, &st->counter[2], t1) && threadIdx.x == 0)
+                    st->rr = t1[0];
                 return;
             }
             // rr0 = ||b||^2: equal to the reference's r.r at x = 0 (MASSolver.cu:488-494), and keeps

@@ -101,6 +101,39 @@ def test_preconditioned_norm_and_modes():
         assert np.linalg.norm(A @ x - b) <= 1e-7 * np.linalg.norm(b), kw
 
 
+def test_half_round_is_ieee_nearest_even():
+    """The oracle's binary16 rounding equals IEEE conversion (numpy float32 -> float16), including
+    ties, subnormals and the smallest subnormal's half-way region."""
+    rng = np.random.default_rng(0)
+    v = np.concatenate([
+        rng.standard_normal(20000).astype(np.float32) * np.float32(2.0) ** rng.integers(-30, 16, 20000),
+        np.float32([2.0 ** -24, 2.0 ** -25, 1.5 * 2.0 ** -25, 0.75 * 2.0 ** -24, 2.0 ** -26, 1.0 + 2.0 ** -11,
+                    1.0 + 3 * 2.0 ** -11, 2048.0 + 1.0, 2048.0 + 3.0, 6.0e-5, -6.0e-8, 32767.0, 65504.0]),
+    ]).astype(np.float32)
+    got = O.half_round(v)
+    with np.errstate(over="ignore"):
+        want = v.astype(np.float16).astype(np.float32)
+    np.testing.assert_array_equal(got, want)
+
+
+def test_fp16_storage_apply_close_to_fp64():
+    """Scaled binary16 inverses change the MAS apply by about the format's precision (2^-11)."""
+    s, orc = _oracle(6, 3, young_sigma=1.0, jitter=0.2)
+    # r = A x: every row (stiff rows and unit Dirichlet rows alike) contributes O(|x|) to z.
+    r = orc.spmv(np.random.default_rng(3).standard_normal(orc.s.V * 3))
+    z64 = orc.apply(r)
+    z16 = orc.apply(r, storage=16)
+    z32 = orc.apply(r, storage=1)
+    e16 = np.linalg.norm(z16 - z64) / np.linalg.norm(z64)
+    e32 = np.linalg.norm(z32 - z64) / np.linalg.norm(z64)
+    assert 0 < e32 < 1e-6
+    assert 1e-6 < e16 < 2e-3
+    b = synthetic.rhs(s.n, 4)
+    x, info = orc.pcg(b, rel_tol=1e-9, abs_tol=0.0, true_residual_period=50, check_period=1, mas_fp32=16)
+    assert info["solver_status"] == "Reach relative tolerance"
+    assert np.linalg.norm(s.scipy() @ x - b) <= 1e-7 * np.linalg.norm(b)
+
+
 def test_initial_guess_is_used_when_asked():
     s, orc = _oracle(6, 3, young_sigma=1.0)
     b = synthetic.rhs(s.n, 5)

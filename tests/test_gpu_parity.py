@@ -78,7 +78,7 @@ def test_spmv_parity(case):
     assert np.linalg.norm(got - y_ref) <= 1e-12 * np.linalg.norm(y_ref)
 
 
-@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("fp32", 2e-5)])
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-9), ("fp32", 2e-5), ("fp16", 1e-3)])
 def test_inverse_parity(case, precision, tol):
     _, system, bd = case
     s = make_solver(system, bd, {"precision": precision})
@@ -93,7 +93,10 @@ def test_inverse_parity(case, precision, tol):
         assert np.linalg.norm(a - b) <= tol * np.linalg.norm(b), m
 
 
-@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("fp32", 2e-5)])
+STORAGE = {"fp64": 0, "fp32": 1, "fp16": 16}
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("fp32", 2e-5), ("fp16", 2e-5)])
 def test_apply_parity(case, precision, tol):
     _, system, bd = case
     s = make_solver(system, bd, {"precision": precision})
@@ -102,8 +105,13 @@ def test_apply_parity(case, precision, tol):
     nodes = s.sizes()["nodes"]
     for seed in (0, 1):
         r_real = np.random.default_rng(seed).standard_normal(orc.s.V * bd)
+        if seed == 1:
+            # r = A x: stiff rows contribute to z as much as unit (Dirichlet) rows.
+            r_real = orc.spmv(r_real)
         z = s.debug_apply(oracle_to_padded(r_real, r2p, bd, nodes))
-        z_ref = orc.apply(r_real)
+        # Reduced-precision storage is emulated in the oracle (same rounded inverses, FP64
+        # arithmetic), so the tolerance measures the FP32 arithmetic only.
+        z_ref = orc.apply(r_real, storage=STORAGE[precision])
         got = padded_to_oracle(z, r2p, bd)
         assert np.linalg.norm(got - z_ref) <= tol * np.linalg.norm(z_ref)
         # padding nodes stay zero
@@ -133,16 +141,19 @@ def test_pcg_reference_mode_parity(case):
     assert abs(info["solver_error"] - oinfo["solver_error"]) <= 2e-3 * oinfo["solver_error"]
 
 
-def test_pcg_chosen_mode(case):
-    """FP32 MAS, true residual every 50, convergence tested every iteration."""
+@pytest.mark.parametrize("precision", ["fp32", "fp16"])
+def test_pcg_chosen_mode(case, precision):
+    """Reduced-precision MAS, true residual every 50, convergence tested every iteration."""
     _, system, bd = case
-    s = make_solver(system, bd, {"precision": "fp32", "true_residual_period": 50, "check_period": 1})
+    s = make_solver(system, bd, {"precision": precision, "true_residual_period": 50, "check_period": 1})
     orc, _ = oracle_for(system, s, bd)
     b = synthetic.rhs(system.n, seed=12)
     x = np.zeros(system.n)
     s.solve(b, x)
     info = s.get_info({})
-    xo, oinfo = orc.pcg(b, rel_tol=1e-8, abs_tol=0.0, true_residual_period=50, check_period=1, mas_fp32=True)
+    assert info["precision"] == precision
+    xo, oinfo = orc.pcg(b, rel_tol=1e-8, abs_tol=0.0, true_residual_period=50, check_period=1,
+                        mas_fp32=STORAGE[precision])
     A = system.scipy()
     assert info["solver_status"] == "Reach relative tolerance"
     assert abs(info["solver_iter"] - oinfo["solver_iter"]) <= 2
