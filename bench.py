@@ -77,10 +77,12 @@ def spmv_bytes(nnzb: int, n: int) -> int:
     return nnzb * (72 + 4) + (n // 3 + 1) * 4 + 2 * 8 * n
 
 
-def mas_bytes(mats: int, n: int, value_bytes: int) -> int:
-    """Algorithmic bytes of one MAS apply launch: every applied 96 x 96 packed inverse (4,656
-    values) once, r read and z0 written once (FP64)."""
-    return mats * 4656 * value_bytes + 2 * 8 * n
+def mas_bytes(mats: int, n: int, precision: str) -> int:
+    """Bytes one MAS apply launch must move: every applied 96 x 96 inverse once as stored
+    (FP64 / FP32: 4,656 packed values; FP16: 4,992 values, the tensor-core block layout keeps
+    its 8 x 8 diagonal cores whole), r read and z0 written once (FP64)."""
+    values, vb = {"fp16": (4992, 2), "fp32": (4656, 4), "fp64": (4656, 8)}[precision]
+    return mats * values * vb + 2 * 8 * n
 
 
 class Clocks:
@@ -287,8 +289,7 @@ def run_ours(args) -> None:
     peak = float(peaks.get("hbm_gbs", 6650.0))
     achieved = spmv_b / (spmv_launch_ms * 1e-3) / 1e9 if spmv_launch_ms > 0 else 0.0
     symv_launch_ms = kms.get("mas_apply", 0.0) / max(1, kl.get("mas_apply", 1))
-    value_bytes = {"fp16": 2, "fp32": 4, "fp64": 8}[args.precision]
-    mas_b = mas_bytes(sizes["banks"] + info["coarse_matrices_active"], n, value_bytes)
+    mas_b = mas_bytes(sizes["banks"] + info["coarse_matrices_active"], n, args.precision)
     kernel_table = {k: {"launches": kl.get(k, 0), "ms_total": round(kms.get(k, 0.0), 4),
                         "ms_per_launch": round(kms.get(k, 0.0) / max(1, kl.get(k, 1)), 5)} for k in kl}
 

@@ -119,6 +119,99 @@ namespace pmas
                 symv_column<T, Store>(M, xs, lane, J, yr);
         }
 
+        // ---- Binary16 (mma16 layout): warp tensor-core products, m16n8k16, FP32 accumulation. ----
+        __device__ __forceinline__ void ldsm_x4(uint32_t (&a)[4], uint32_t addr)
+        {
+            asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
+                         : "=r"(a[0]), "=r"(a[1]), "=r"(a[2]), "=r"(a[3])
+                         : "r"(addr));
+        }
+        __device__ __forceinline__ void ldsm_x4_trans(uint32_t (&a)[4], uint32_t addr)
+        {
+            asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0, %1, %2, %3}, [%4];"
+                         : "=r"(a[0]), "=r"(a[1]), "=r"(a[2]), "=r"(a[3])
+                         : "r"(addr));
+        }
+        __device__ __forceinline__ uint32_t ldsm_x1(uint32_t addr)
+        {
+            uint32_t a;
+            asm volatile("ldmatrix.sync.aligned.m8n8.x1.shared.b16 {%0}, [%1];" : "=r"(a) : "r"(addr));
+            return a;
+        }
+        __device__ __forceinline__ void mma_16816(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1)
+        {
+            asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+                         "{%8, %9}, {%0, %1, %2, %3};"
+                         : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+        }
+
+        // y = M x for one mma16 matrix in shared memory, by one warp. x enters as two binary16
+        // columns (xh + xl = x scaled, ~22 significant bits), the B operand's columns 0 and 1; the
+        // FP32 products of column 0 and 1 are added back. Each 16 x 16 block above the diagonal
+        // is used twice: as stored for its block row and, loaded transposed, for its block
+        // column. The result goes through ys (shared, N floats): lane l gets rows 32 t + l.
+        template <int BD>
+        __device__ __forceinline__ void symv_mma16(const __half *M, const __half *xh, const __half *xl, float *ys,
+                                                   int lane, float (&yr)[BD])
+        {
+            constexpr int NS = 2 * BD, NB = NS * (NS - 1) / 2;
+            const int g = lane >> 2, q = lane & 3;
+            const int c = lane >> 3, rr = lane & 7; // ldmatrix: lanes 8c..8c+7 give the rows of core c
+            uint32_t bf[NS][2];
+            const __half *xsrc = (g == 0) ? xh : xl;
+#pragma unroll
+            for (int S = 0; S < NS; ++S)
+            {
+                bf[S][0] = g < 2 ? *reinterpret_cast<const uint32_t *>(xsrc + 16 * S + 2 * q) : 0u;
+                bf[S][1] = g < 2 ? *reinterpret_cast<const uint32_t *>(xsrc + 16 * S + 2 * q + 8) : 0u;
+            }
+            float d[NS][4];
+#pragma unroll
+            for (int R = 0; R < NS; ++R)
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    d[R][i] = 0.f;
+            const uint32_t mbase = smem_addr(M);
+            const int ct = (c == 1) ? 2 : (c == 2 ? 1 : c); // fragment c of a transposed block
+            const uint32_t row_off = (uint32_t)(rr * 16);
+#pragma unroll
+            for (int R = 0; R < NS; ++R)
+#pragma unroll
+                for (int S = R + 1; S < NS; ++S)
+                {
+                    const uint32_t blk = mbase + (uint32_t)((R * (2 * NS - R - 1) / 2 + (S - R - 1)) * 512);
+                    uint32_t a[4];
+                    ldsm_x4(a, blk + c * 128 + row_off);
+                    mma_16816(d[R], a, bf[S][0], bf[S][1]);
+                    ldsm_x4_trans(a, blk + ct * 128 + row_off);
+                    mma_16816(d[S], a, bf[R][0], bf[R][1]);
+                }
+            // Diagonal blocks [[D0, C], [C^T, D1]]: transposed loads of (D0, C, -, D1) give
+            // fragments 0, 1, 3 (D0, D1 are symmetric); fragment 2 (C) is a plain load.
+            const int cd = (c == 1) ? 1 : (c == 3 ? 2 : 0);
+#pragma unroll
+            for (int R = 0; R < NS; ++R)
+            {
+                const uint32_t blk = mbase + (uint32_t)((NB * 256 + R * 192) * 2);
+                uint32_t a[4];
+                ldsm_x4_trans(a, blk + cd * 128 + row_off);
+                a[2] = ldsm_x1(blk + 128 + row_off);
+                mma_16816(d[R], a, bf[R][0], bf[R][1]);
+            }
+            if (q == 0)
+#pragma unroll
+                for (int R = 0; R < NS; ++R)
+                {
+                    ys[16 * R + g] = d[R][0] + d[R][1];
+                    ys[16 * R + g + 8] = d[R][2] + d[R][3];
+                }
+            __syncwarp();
+#pragma unroll
+            for (int t = 0; t < BD; ++t)
+                yr[t] = ys[t * 32 + lane];
+        }
+
         // The reference's per-iteration scalar work and convergence test (MASSolver.cu:505,
         // 526-583), run by the last CTA of the apply. rz = r . z, rzcross = r . z_old (Polak-Ribiere).
         __device__ void pcg_finalize(PcgState *st, const PcgConfig &cfg, int mode, double rz, double rzcross)
@@ -187,9 +280,11 @@ namespace pmas
         {
             using Real = typename StoreTraits<Store>::Real;
             static constexpr int N = 32 * BD;
-            static constexpr int S = N * (N + 1) / 2;
+            static constexpr bool MMA = StoreTraits<Store>::SCALED; // binary16: mma16 layout
+            static constexpr int S = MMA ? (2 * BD) * (2 * BD - 1) / 2 * 256 + 2 * BD * 192 : N * (N + 1) / 2;
             static constexpr int STAGE_BYTES = S * (int)sizeof(Store);
-            static constexpr int XS_BYTES = ((N * (int)sizeof(Real)) + 15) / 16 * 16;
+            // x: Real values, or binary16 hi / lo columns plus the FP32 result rows.
+            static constexpr int XS_BYTES = MMA ? 8 * N : ((N * (int)sizeof(Real)) + 15) / 16 * 16;
             static constexpr int WARP_BYTES = 2 * STAGE_BYTES + XS_BYTES + 16;
             static constexpr int SMEM_LIMIT = 232448 - 1024; // leave room for static shared memory
             static constexpr int W0 = SMEM_LIMIT / WARP_BYTES;
@@ -221,6 +316,9 @@ namespace pmas
             Store *stage0 = reinterpret_cast<Store *>(base);
             Store *stage1 = reinterpret_cast<Store *>(base + L::STAGE_BYTES);
             Real *xs = reinterpret_cast<Real *>(base + 2 * L::STAGE_BYTES);
+            __half *xh = reinterpret_cast<__half *>(base + 2 * L::STAGE_BYTES);
+            __half *xl = xh + N;
+            float *ys = reinterpret_cast<float *>(base + 2 * L::STAGE_BYTES + 4 * N);
             uint64_t *bar = reinterpret_cast<uint64_t *>(base + 2 * L::STAGE_BYTES + L::XS_BYTES);
             const Store *__restrict__ inv = static_cast<const Store *>(mas.inv);
             const int banks = mas.banks;
@@ -276,9 +374,32 @@ namespace pmas
                 double r64[BD];
 #pragma unroll
                 for (int t = 0; t < BD; ++t)
-                {
                     r64[t] = r_next[t];
-                    xs[t * 32 + lane] = (Real)r64[t];
+                double xscale = 1.0; // binary16 input: x * xscale split into hi + lo
+                if constexpr (L::MMA)
+                {
+                    double amax = 0.0;
+#pragma unroll
+                    for (int t = 0; t < BD; ++t)
+                        amax = fmax(amax, fabs(r64[t]));
+#pragma unroll
+                    for (int o = 16; o >= 1; o >>= 1)
+                        amax = fmax(amax, __shfl_xor_sync(FULL, amax, o));
+                    xscale = (amax > 0.0 && isfinite(amax)) ? ldexp(1.0, 14 - ilogb(amax)) : 1.0;
+#pragma unroll
+                    for (int t = 0; t < BD; ++t)
+                    {
+                        const float v = (float)(r64[t] * xscale);
+                        const __half h = __float2half_rn(v);
+                        xh[t * 32 + lane] = h;
+                        xl[t * 32 + lane] = __float2half_rn(v - __half2float(h));
+                    }
+                }
+                else
+                {
+#pragma unroll
+                    for (int t = 0; t < BD; ++t)
+                        xs[t * 32 + lane] = (Real)r64[t];
                 }
                 const int mnext = m + total_warps;
                 if (mnext < items)
@@ -307,7 +428,12 @@ namespace pmas
                 const bool ident = coarse && mas.identity[mat - banks];
                 Real yr[BD];
                 if (!ident)
-                    symv_tiles<BD, Store>(stage, xs, lane, yr);
+                {
+                    if constexpr (L::MMA)
+                        symv_mma16<BD>(reinterpret_cast<const __half *>(stage), xh, xl, ys, lane, yr);
+                    else
+                        symv_tiles<BD, Store>(stage, xs, lane, yr);
+                }
                 __syncwarp();
                 const int mn = m + 2 * total_warps;
                 if (lane == 0 && mn < items)
@@ -315,7 +441,7 @@ namespace pmas
                     fence_proxy_async_smem();
                     bulk_load(stage, inv + (size_t)mat_of(mn) * S, L::STAGE_BYTES, b);
                 }
-                const double scale = StoreTraits<Store>::SCALED ? mas.inv_scale[mat] : 1.0;
+                const double scale = StoreTraits<Store>::SCALED ? mas.inv_scale[mat] / xscale : 1.0;
                 double d0 = 0.0, d1 = 0.0;
 #pragma unroll
                 for (int t = 0; t < BD; ++t)

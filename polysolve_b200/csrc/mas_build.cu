@@ -195,10 +195,12 @@ namespace pmas
         }
 
         // Inverts the symmetric N x N matrix A (shared memory, upper triangle used) and stores the
-        // inverse tile-packed in `out`; *scale_out receives the factor that turns stored values
-        // back into matrix values (1 unless binary16).
+        // inverse in `out` (tile-packed; binary16: mma16); *scale_out receives the factor that turns
+        // stored values back into matrix values (1 unless binary16); *ident_out (if given) 1 when
+        // the inverse is exactly the identity.
         template <int BD, class Out>
-        __device__ void invert_and_store(double *A, double *col, Out *out, double *scale_out, int *flag)
+        __device__ void invert_and_store(double *A, double *col, Out *out, double *scale_out, int *ident_out,
+                                         int *flag)
         {
             constexpr int N = 32 * BD;
             const int tid = threadIdx.x, nt = blockDim.x;
@@ -272,6 +274,41 @@ namespace pmas
             }
             if (tid == 0)
                 *scale_out = 1.0 / sc;
+            // Exactly the identity (a coarse matrix of isolated rows): the apply copies instead.
+            if (ident_out)
+            {
+                __shared__ int is_id;
+                if (tid == 0)
+                    is_id = 1;
+                __syncthreads();
+                for (int e = tid; e < N * N; e += nt)
+                {
+                    const int t = e / N, c = e - t * N;
+                    if (t <= c && -A[e] != (t == c ? 1.0 : 0.0))
+                        is_id = 0;
+                }
+                __syncthreads();
+                if (tid == 0)
+                    *ident_out = is_id;
+            }
+            if constexpr (StoreTraits<Out>::SCALED)
+            {
+                // Binary16: mma16 layout (tensor-core fragments).
+                constexpr int S16 = (2 * BD) * (2 * BD - 1) / 2 * 256 + 2 * BD * 192;
+                for (int idx = tid; idx < S16; idx += nt)
+                {
+                    int row, cl;
+                    mma16_rowcol(BD, idx, row, cl);
+                    const double v = -A[row * N + cl];
+                    if (!isfinite(v))
+                        bad = 1;
+                    store_value(out + idx, v, sc);
+                }
+                __syncthreads();
+                if (tid == 0 && bad)
+                    atomicExch(flag, ERR_INVERSE);
+                return;
+            }
             // Store -A (the inverse) tile-packed.
             constexpr int S = N * (N + 1) / 2;
             for (int idx = tid; idx < S; idx += nt)
@@ -316,7 +353,9 @@ namespace pmas
         __global__ void __launch_bounds__(256) k_assemble_invert_lv0(BankedView A, const int *__restrict__ node_real,
                                                                      Out *out, double *scale, int *flag)
         {
-            constexpr int N = 32 * BD, S = N * (N + 1) / 2;
+            constexpr int N = 32 * BD;
+            constexpr int S = StoreTraits<Out>::SCALED ? (2 * BD) * (2 * BD - 1) / 2 * 256 + 2 * BD * 192
+                                                       : N * (N + 1) / 2;
             extern __shared__ __align__(16) double dsm[];
             double *M = dsm;
             double *col = dsm + N * N;
@@ -355,7 +394,7 @@ namespace pmas
                 }
             }
             __syncthreads();
-            invert_and_store<BD, Out>(M, col, out + (size_t)bank * S, scale + bank, flag);
+            invert_and_store<BD, Out>(M, col, out + (size_t)bank * S, scale + bank, nullptr, flag);
         }
 
         // Coarse-level upper-triangle accumulation with FP64 atomics (order-dependent in the
@@ -407,9 +446,11 @@ namespace pmas
 
         template <int BD, class Out>
         __global__ void __launch_bounds__(256) k_invert_coarse(const double *__restrict__ staging, Out *out,
-                                                               double *scale, int *flag)
+                                                               double *scale, int *identity, int *flag)
         {
-            constexpr int N = 32 * BD, S = N * (N + 1) / 2;
+            constexpr int N = 32 * BD;
+            constexpr int S = StoreTraits<Out>::SCALED ? (2 * BD) * (2 * BD - 1) / 2 * 256 + 2 * BD * 192
+                                                       : N * (N + 1) / 2;
             extern __shared__ __align__(16) double dsm[];
             double *M = dsm;
             double *col = dsm + N * N;
@@ -420,7 +461,8 @@ namespace pmas
                 M[e] = (r <= c) ? src[r * N + c] : src[c * N + r];
             }
             __syncthreads();
-            invert_and_store<BD, Out>(M, col, out + (size_t)blockIdx.x * S, scale + blockIdx.x, flag);
+            invert_and_store<BD, Out>(M, col, out + (size_t)blockIdx.x * S, scale + blockIdx.x, identity + blockIdx.x,
+                                      flag);
         }
 
         __global__ void k_cslot(int nodes, int level_num, const int *__restrict__ map, int coff0, int coff1, int coff2,
@@ -438,47 +480,6 @@ namespace pmas
                 v[l] = (l < level_num && c >= 0) ? coff[l] + c : -1;
             }
             cslot[u] = make_int4(v[0], v[1], v[2], v[3]);
-        }
-
-        // flag[g] = 1 if coarse inverse g is exactly the identity (a bank of isolated rows).
-        template <int BD, class Store>
-        __global__ void k_identity_flags(const Store *__restrict__ inv, const double *__restrict__ scale, int first,
-                                         int count, int *flag)
-        {
-            constexpr int N = 32 * BD, S = N * (N + 1) / 2;
-            const int g = blockIdx.x;
-            if (g >= count)
-                return;
-            const Store *m = inv + (size_t)(first + g) * S;
-            const double sc = scale[first + g];
-            __shared__ int is_id;
-            if (threadIdx.x == 0)
-                is_id = 1;
-            __syncthreads();
-            for (int idx = threadIdx.x; idx < S; idx += blockDim.x)
-            {
-                int rem = idx, J = 0;
-                while (rem >= J * 1024 + 528)
-                {
-                    rem -= J * 1024 + 528;
-                    ++J;
-                }
-                bool diag = false;
-                if (rem >= J * 1024)
-                {
-                    const int e = rem - J * 1024;
-                    int j = 0;
-                    while ((j + 1) * (j + 2) / 2 <= e)
-                        ++j;
-                    diag = (e - j * (j + 1) / 2) == j;
-                }
-                const double want = diag ? 1.0 : 0.0;
-                if ((double)load1(m + idx) * sc != want)
-                    is_id = 0;
-            }
-            __syncthreads();
-            if (threadIdx.x == 0)
-                flag[g] = is_id;
         }
 
         int div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
@@ -521,9 +522,10 @@ namespace pmas
                                                                           M.level_num, coff[0], coff[1], coff[2],
                                                                           coff[3], staging.get());
                 cuda_check(cudaGetLastError(), "assemble coarse launch");
-                constexpr int S = N * (N + 1) / 2;
+                const size_t S = (size_t)inv_stride(BD, M.storage);
                 k_invert_coarse<BD, Out><<<M.total_coarse, 256, smem, s>>>(staging.get(), out + (size_t)M.banks * S,
-                                                                          scale + M.banks, M.flag.get());
+                                                                          scale + M.banks, M.identity.get(),
+                                                                          M.flag.get());
                 cuda_check(cudaGetLastError(), "invert coarse launch");
                 cuda_check(cudaStreamSynchronize(s), "coarse inverse");
             }
@@ -714,7 +716,7 @@ namespace pmas
         cuda_check(cudaMemsetAsync(M.zc.get(), 0, M.zc.bytes(), s), "memset");
 
         // --- matrices
-        const size_t S = (size_t)tile_packed_size(bd);
+        const size_t S = (size_t)inv_stride(bd, storage);
         M.inv64.reset();
         M.inv32.reset();
         M.inv16.reset();
@@ -732,12 +734,6 @@ namespace pmas
             auto per_bd = [&](auto bdc) {
                 constexpr int BD = decltype(bdc)::value;
                 assemble_and_invert<BD, Out>(M, A, d_node_real, out, coff, s);
-                if (M.total_coarse > 0)
-                {
-                    k_identity_flags<BD, Out><<<M.total_coarse, 256, 0, s>>>(out, M.inv_scale.get(), banks,
-                                                                            M.total_coarse, M.identity.get());
-                    cuda_check(cudaGetLastError(), "identity flags launch");
-                }
             };
             if (bd == 1)
                 per_bd(std::integral_constant<int, 1>{});

@@ -1149,33 +1149,38 @@ extern "C" int mas_get_inverses(const mas_solver *h, double *out, size_t count)
     auto *hh = const_cast<mas_solver *>(h);
     return guarded(hh, [&] {
         cuda_check(cudaSetDevice(h->device), "set device");
-        std::vector<double> tp(count);
-        if (h->mas.storage == STORE_F32)
+        const int storage = h->mas.storage;
+        const size_t Ss = (size_t)inv_stride(bd, storage); // stored values per matrix
+        const size_t stored = Ss * h->mas.total_mats;
+        std::vector<double> tp(stored);
+        if (storage == STORE_F32)
         {
-            std::vector<float> f(count);
-            cuda_check(cudaMemcpy(f.data(), h->mas.inv32.get(), sizeof(float) * count, cudaMemcpyDeviceToHost), "inv");
-            for (size_t i = 0; i < count; ++i)
+            std::vector<float> f(stored);
+            cuda_check(cudaMemcpy(f.data(), h->mas.inv32.get(), sizeof(float) * stored, cudaMemcpyDeviceToHost), "inv");
+            for (size_t i = 0; i < stored; ++i)
                 tp[i] = f[i];
         }
-        else if (h->mas.storage == STORE_F16)
+        else if (storage == STORE_F16)
         {
-            std::vector<uint16_t> f(count);
+            std::vector<uint16_t> f(stored);
             std::vector<double> sc((size_t)h->mas.total_mats);
-            cuda_check(cudaMemcpy(f.data(), h->mas.inv16.get(), sizeof(uint16_t) * count, cudaMemcpyDeviceToHost),
+            cuda_check(cudaMemcpy(f.data(), h->mas.inv16.get(), sizeof(uint16_t) * stored, cudaMemcpyDeviceToHost),
                        "inv");
             cuda_check(cudaMemcpy(sc.data(), h->mas.inv_scale.get(), sizeof(double) * sc.size(),
                                   cudaMemcpyDeviceToHost),
                        "inv scale");
-            for (size_t i = 0; i < count; ++i)
-                tp[i] = half_bits_to_double(f[i]) * sc[i / S];
+            for (size_t i = 0; i < stored; ++i)
+                tp[i] = half_bits_to_double(f[i]) * sc[i / Ss];
         }
         else
-            cuda_check(cudaMemcpy(tp.data(), h->mas.inv64.get(), sizeof(double) * count, cudaMemcpyDeviceToHost), "inv");
+            cuda_check(cudaMemcpy(tp.data(), h->mas.inv64.get(), sizeof(double) * stored, cudaMemcpyDeviceToHost),
+                       "inv");
         for (int m = 0; m < h->mas.total_mats; ++m)
             for (int i = 0; i < N; ++i)
                 for (int j = i; j < N; ++j)
                     out[(size_t)m * S + (size_t)i * N - (size_t)i * (i + 1) / 2 + j] =
-                        tp[(size_t)m * S + tile_packed_index(bd, i, j)];
+                        tp[(size_t)m * Ss +
+                           (storage == STORE_F16 ? mma16_index(bd, i, j) : tile_packed_index(bd, i, j))];
     });
 }
 

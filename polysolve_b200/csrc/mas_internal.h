@@ -138,6 +138,87 @@ namespace pmas
     }
 
     // ---------------------------------------------------------------------------------------
+    // Binary16 subdomain matrix storage ("mma16"): the N x N symmetric matrix (N = 32 * bd) in
+    // 16 x 16 blocks, NS = N / 16 block rows, laid out for warp tensor-core fragments. First the
+    // NS (NS - 1) / 2 blocks above the diagonal (block row R, block column S > R, row-major over
+    // (R, S)), 256 values each as four 8 x 8 cores [rows 0-7 | cols 0-7], [rows 8-15 | cols 0-7],
+    // [rows 0-7 | cols 8-15], [rows 8-15 | cols 8-15], each core row-major; then the NS diagonal
+    // blocks, 192 values each: the two diagonal cores stored full (symmetric) and the core
+    // [rows 0-7 | cols 8-15], as [D0 | C | D1]. The same blocks serve the rows below the diagonal
+    // through transposed fragment loads.
+    // ---------------------------------------------------------------------------------------
+    __host__ __device__ inline int mma16_size(int bd)
+    {
+        const int ns = 2 * bd;
+        return ns * (ns - 1) / 2 * 256 + ns * 192;
+    }
+
+    // Element of mma16 position idx (the row <= col one for symmetric pairs of a diagonal core).
+    __host__ __device__ inline void mma16_rowcol(int bd, int idx, int &row, int &col)
+    {
+        const int ns = 2 * bd, nb = ns * (ns - 1) / 2;
+        if (idx < nb * 256)
+        {
+            int blk = idx >> 8, R = 0;
+            while (blk >= ns - 1 - R)
+            {
+                blk -= ns - 1 - R;
+                ++R;
+            }
+            const int S = R + 1 + blk;
+            const int core = (idx & 255) >> 6, e = idx & 63;
+            row = 16 * R + (core & 1) * 8 + (e >> 3);
+            col = 16 * S + (core >> 1) * 8 + (e & 7);
+            return;
+        }
+        const int d = idx - nb * 256, R = d / 192, e = d % 192;
+        int i, j;
+        if (e < 64)
+            i = e >> 3, j = e & 7;
+        else if (e < 128)
+            i = (e - 64) >> 3, j = 8 + ((e - 64) & 7);
+        else
+            i = 8 + ((e - 128) >> 3), j = 8 + ((e - 128) & 7);
+        row = 16 * R + (i < j ? i : j);
+        col = 16 * R + (i < j ? j : i);
+    }
+
+    // Values stored per subdomain matrix for a storage precision.
+    __host__ __device__ inline int inv_stride(int bd, int storage)
+    {
+        return storage == STORE_F16 ? mma16_size(bd) : tile_packed_size(bd);
+    }
+
+    // Position of element (row, col) in mma16 storage (either triangle).
+    __host__ __device__ inline int mma16_index(int bd, int row, int col)
+    {
+        const int ns = 2 * bd;
+        int R = row >> 4, S = col >> 4, i = row & 15, j = col & 15;
+        if (R > S)
+        {
+            int t = R;
+            R = S;
+            S = t;
+            t = i;
+            i = j;
+            j = t;
+        }
+        if (R < S)
+        {
+            const int blk = R * (2 * ns - R - 1) / 2 + (S - R - 1);
+            const int core = (i >> 3) + 2 * (j >> 3);
+            return blk * 256 + core * 64 + (i & 7) * 8 + (j & 7);
+        }
+        const int base = ns * (ns - 1) / 2 * 256 + R * 192;
+        if (i < 8 && j < 8)
+            return base + i * 8 + j;
+        if (i >= 8 && j >= 8)
+            return base + 128 + (i - 8) * 8 + (j - 8);
+        const int a = i < j ? i : j, b = i < j ? j : i; // a < 8 <= b
+        return base + 64 + a * 8 + (b - 8);
+    }
+
+    // ---------------------------------------------------------------------------------------
     // MAS preconditioner on the device.
     // ---------------------------------------------------------------------------------------
     struct MasView
