@@ -353,14 +353,16 @@ namespace pmas
                 part[i] = 0.0;
             uint32_t phase0 = 0, phase1 = 0;
             bool ok = true;
-            // Input of the current item, prefetched one item ahead.
-            double r_next[BD];
+            // Input (and binary16 scale) of the current item, prefetched one item ahead.
+            double r_next[BD], scale_next = 1.0;
             if (gw < items)
             {
                 const double *in = in_of(gw);
 #pragma unroll
                 for (int t = 0; t < BD; ++t)
                     r_next[t] = in[t * 32 + lane];
+                if (StoreTraits<Store>::SCALED)
+                    scale_next = mas.inv_scale[mat_of(gw)];
             }
             int k = 0;
             for (int m = gw; m < items; m += total_warps, ++k)
@@ -375,6 +377,7 @@ namespace pmas
 #pragma unroll
                 for (int t = 0; t < BD; ++t)
                     r64[t] = r_next[t];
+                const double mscale = scale_next;
                 double xscale = 1.0; // binary16 input: x * xscale split into hi + lo
                 if constexpr (L::MMA)
                 {
@@ -408,6 +411,8 @@ namespace pmas
 #pragma unroll
                     for (int t = 0; t < BD; ++t)
                         r_next[t] = in[t * 32 + lane];
+                    if (StoreTraits<Store>::SCALED)
+                        scale_next = mas.inv_scale[mat_of(mnext)];
                 }
                 double zold[BD];
                 if (pr)
@@ -441,7 +446,7 @@ namespace pmas
                     fence_proxy_async_smem();
                     bulk_load(stage, inv + (size_t)mat_of(mn) * S, L::STAGE_BYTES, b);
                 }
-                const double scale = StoreTraits<Store>::SCALED ? mas.inv_scale[mat] / xscale : 1.0;
+                const double scale = StoreTraits<Store>::SCALED ? mscale / xscale : 1.0;
                 double d0 = 0.0, d1 = 0.0;
 #pragma unroll
                 for (int t = 0; t < BD; ++t)

@@ -238,6 +238,8 @@ namespace pmas
             return per_sm * device_sm_count();
         }
 
+        // Resident grid (one wave, warps loop over banks): update_xr, whose rr ticket then has
+        // few arrivals.
         template <class K>
         int bank_grid(int banks, K kernel)
         {
@@ -245,6 +247,10 @@ namespace pmas
             const int cap = resident_ctas(kernel);
             return need < cap ? need : cap;
         }
+
+        // One warp per bank: the hardware hands CTAs to SMs as others finish, which balances the
+        // end of a short streaming kernel without a reduction (update_p).
+        int bank_grid_all(int banks) { return (banks + UPD_THREADS / 32 - 1) / (UPD_THREADS / 32); }
     } // namespace
 
     void launch_update_xr(const MasView &mas, double *x, double *r, const double *p, const double *Ap, PcgState *st,
@@ -271,7 +277,7 @@ namespace pmas
     void launch_update_p(const MasView &mas, double *p, const double *z0, PcgState *st, int first, cudaStream_t s)
     {
         auto go = [&](auto kernel) {
-            const int grid = bank_grid(mas.banks, kernel);
+            const int grid = bank_grid_all(mas.banks);
             if (grid > 0)
                 kernel<<<grid, UPD_THREADS, 0, s>>>(mas, p, z0, st, first);
         };
