@@ -333,6 +333,7 @@ namespace pmas
                 return m < banks ? r + (size_t)m * N : mas.rc + (size_t)(mat_of(m) - banks) * N;
             };
 
+            const uint64_t pol = l2_evict_first_policy(); // the inverses stream, the vectors stay
             if (lane == 0)
             {
                 mbar_init(&bar[0], 1);
@@ -343,9 +344,9 @@ namespace pmas
             if (lane == 0)
             {
                 if (gw < items)
-                    bulk_load(stage0, inv + (size_t)mat_of(gw) * S, L::STAGE_BYTES, &bar[0]);
+                    bulk_load_stream(stage0, inv + (size_t)mat_of(gw) * S, L::STAGE_BYTES, &bar[0], pol);
                 if (gw + total_warps < items)
-                    bulk_load(stage1, inv + (size_t)mat_of(gw + total_warps) * S, L::STAGE_BYTES, &bar[1]);
+                    bulk_load_stream(stage1, inv + (size_t)mat_of(gw + total_warps) * S, L::STAGE_BYTES, &bar[1], pol);
             }
             double part[APPLY_PARTS];
 #pragma unroll
@@ -444,7 +445,7 @@ namespace pmas
                 if (lane == 0 && mn < items)
                 {
                     fence_proxy_async_smem();
-                    bulk_load(stage, inv + (size_t)mat_of(mn) * S, L::STAGE_BYTES, b);
+                    bulk_load_stream(stage, inv + (size_t)mat_of(mn) * S, L::STAGE_BYTES, b, pol);
                 }
                 const double scale = StoreTraits<Store>::SCALED ? mscale / xscale : 1.0;
                 double d0 = 0.0, d1 = 0.0;

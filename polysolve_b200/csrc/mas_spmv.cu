@@ -19,9 +19,14 @@ namespace pmas
     {
         constexpr int SPMV_THREADS = 256;
         constexpr int BANKS_PER_CTA = SPMV_THREADS / 32;
+        // Slots unrolled per loop trip (loads of both in flight; measured best of 1, 2, 4).
+        constexpr int SPMV_UNROLL = 2;
 
+        // Minimum one CTA per SM: the compiler then keeps both unrolled slots' loads in flight
+        // (80 registers, 3 CTAs per SM), measured faster than the occupancy-first 44-register
+        // build at 1.6 M DOF.
         template <int BD, int MODE>
-        __global__ void __launch_bounds__(SPMV_THREADS) k_spmv(BankedView A, const double *__restrict__ x,
+        __global__ void __launch_bounds__(SPMV_THREADS, 1) k_spmv(BankedView A, const double *__restrict__ x,
                                                                double *__restrict__ y, const double *__restrict__ b,
                                                                PcgState *st, ReduceBuf red, int iter, int period)
         {
@@ -46,21 +51,24 @@ namespace pmas
 #pragma unroll
                 for (int i = 0; i < BD; ++i)
                     acc[i] = 0.0;
-#pragma unroll 2
+                // The matrix streams through L2 with evict-first priority (x, the gathered vector,
+                // and the other PCG vectors stay resident); two slots' loads in flight per lane.
+                const uint64_t pol = l2_evict_first_policy();
+#pragma unroll SPMV_UNROLL
                 for (int k = 0; k < len; ++k)
                 {
-                    const int col = __ldg(cp + (long long)k * 32);
+                    const int col = ld_stream_s32(cp + (long long)k * 32, pol);
                     const double *blk = vp + (long long)k * 32 * BS;
                     double v[BS];
 #pragma unroll
                     for (int p = 0; p < PAIRS; ++p)
                     {
-                        const double2 t = __ldg(reinterpret_cast<const double2 *>(blk + p * 64 + lane * 2));
+                        const double2 t = ld_stream_f64x2(blk + p * 64 + lane * 2, pol);
                         v[2 * p] = t.x;
                         v[2 * p + 1] = t.y;
                     }
                     if (BS & 1)
-                        v[BS - 1] = __ldg(blk + PAIRS * 64 + lane);
+                        v[BS - 1] = ld_stream_f64(blk + PAIRS * 64 + lane, pol);
                     double xc[BD];
 #pragma unroll
                     for (int j = 0; j < BD; ++j)
