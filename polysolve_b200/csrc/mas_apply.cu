@@ -7,9 +7,9 @@
 //
 //  * the level-0 restriction (per-bank sums of each connected component) is fused into the kernel
 //    that produces r (update_xr; k_restrict after a true-residual SpMV);
-//  * k_coarse_levels: every coarse level above the first in one launch -- the second level spread
-//    over all CTAs (one warp per 32 consecutive components, deterministic segmented sums), the
-//    last CTA to finish (atomic ticket) the levels above it;
+//  * k_coarse_levels: every coarse level above the first in one launch -- one CTA per third-level
+//    node sums its second-level children (a warp each, lane per child) and then itself, so both
+//    levels take one round; the last CTA to finish (atomic ticket) sums a fourth level;
 //  * k_mas_apply: persistent warps stream every inverse -- the level-0 subdomain matrices, then
 //    the active coarse matrices -- through shared memory with cp.async.bulk (two stages per warp,
 //    mbarrier completion) and write z0 = A_0^-1 r and zc = A_l^-1 rc with per-CTA partial dots;
@@ -504,39 +504,33 @@ namespace pmas
             }
         }
 
-        // Sums of coarse level l (>= 1) from level l - 1, warps [first_warp, +nwarps) of the
-        // caller's: one warp per 32 consecutive level-(l-1) components (lane = component), which
-        // all merge into level-l components of the same 32-id group, so every sum is complete
-        // within the warp (segmented butterfly sums, deterministic).
+        // Coarse levels above the first from its components rc (level 0 of the coarse vector).
+        // Each real node of level l sums its (at most 32) children of level l - 1 in a warp
+        // (lane = child, in increasing order; deterministic). With three or more levels one CTA
+        // (32 warps) per level-2 node computes its level-1 children (a warp each) and then itself
+        // from them, so both levels take one round; a fourth level is summed by the last CTA to
+        // finish (atomic ticket).
+        constexpr int LEVEL_THREADS = 1024;
+
         template <int BD>
-        __device__ __forceinline__ void level_sums(const MasView &mas, int l, int first_warp, int nwarps)
+        __device__ __forceinline__ void kid_sum(const MasView &mas, int l, int i, bool cg, double (&v)[BD])
         {
             const int lane = threadIdx.x & 31;
-            const int count = mas.real_count[l - 1];
-            const int chunks = (count + 31) / 32;
-            for (int q = first_warp; q < chunks; q += nwarps)
+            const int b = mas.kid_ptr[l][i], e = mas.kid_ptr[l][i + 1];
+#pragma unroll
+            for (int c = 0; c < BD; ++c)
+                v[c] = 0.0;
+            if (b + lane < e)
             {
-                const int i = q * 32 + lane;
-                double v[BD];
-                int key = -1;
+                const size_t node = (size_t)mas.coff[l - 1] + mas.kids[b + lane];
 #pragma unroll
                 for (int c = 0; c < BD; ++c)
-                    v[c] = 0.0;
-                if (i < count)
-                {
-                    const int node = mas.coff[l - 1] + i;
-                    key = mas.parent[node];
-#pragma unroll
-                    for (int c = 0; c < BD; ++c)
-                        v[c] = __ldcg(mas.rc + (size_t)node * BD + c);
-                }
-                warp_segment_store<BD>(v, key, 0, mas.rc);
+                    v[c] = cg ? __ldcg(mas.rc + node * BD + c) : mas.rc[node * BD + c];
             }
+#pragma unroll
+            for (int c = 0; c < BD; ++c)
+                v[c] = warp_sum(v[c]);
         }
-
-        // 32 warps: the last CTA sums each higher level (at most a few dozen groups of 32) in
-        // one round.
-        constexpr int LEVEL_THREADS = 1024;
 
         template <int BD>
         __global__ void __launch_bounds__(LEVEL_THREADS) k_coarse_levels(MasView mas, const PcgState *st)
@@ -544,10 +538,50 @@ namespace pmas
             if (st && st->done)
                 return;
             constexpr int W = LEVEL_THREADS / 32;
-            const int w = threadIdx.x >> 5;
+            const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+            __shared__ double part[W][BD];
             __shared__ int is_last;
-            level_sums<BD>(mas, 1, blockIdx.x * W + w, gridDim.x * W);
-            if (mas.level_num <= 2)
+            if (mas.level_num == 2)
+            {
+                const int i = blockIdx.x * W + w;
+                if (i >= mas.real_count[1])
+                    return;
+                double v[BD];
+                kid_sum<BD>(mas, 1, i, false, v);
+                if (lane == 0)
+#pragma unroll
+                    for (int c = 0; c < BD; ++c)
+                        mas.rc[((size_t)mas.coff[1] + i) * BD + c] = v[c];
+                return;
+            }
+            // Level-2 node j = blockIdx.x; warp w: its w-th level-1 child.
+            const int j = blockIdx.x;
+            const int kb = mas.kid_ptr[2][j], ke = mas.kid_ptr[2][j + 1];
+            if (kb + w < ke)
+            {
+                const int i = mas.kids[kb + w];
+                double v[BD];
+                kid_sum<BD>(mas, 1, i, false, v);
+                if (lane == 0)
+#pragma unroll
+                    for (int c = 0; c < BD; ++c)
+                    {
+                        mas.rc[((size_t)mas.coff[1] + i) * BD + c] = v[c];
+                        part[w][c] = v[c];
+                    }
+            }
+            __syncthreads();
+            if (w == 0)
+            {
+#pragma unroll
+                for (int c = 0; c < BD; ++c)
+                {
+                    const double t = warp_sum(kb + lane < ke ? part[lane][c] : 0.0);
+                    if (lane == 0)
+                        mas.rc[((size_t)mas.coff[2] + j) * BD + c] = t;
+                }
+            }
+            if (mas.level_num <= 3)
                 return;
             __syncthreads();
             if (threadIdx.x == 0)
@@ -559,11 +593,14 @@ namespace pmas
             if (!is_last)
                 return;
             __threadfence();
-            for (int l = 2; l < mas.level_num; ++l)
+            for (int k = w; k < mas.real_count[3]; k += W)
             {
-                level_sums<BD>(mas, l, w, W);
-                __threadfence_block();
-                __syncthreads();
+                double v[BD];
+                kid_sum<BD>(mas, 3, k, true, v);
+                if (lane == 0)
+#pragma unroll
+                    for (int c = 0; c < BD; ++c)
+                        mas.rc[((size_t)mas.coff[3] + k) * BD + c] = v[c];
             }
             if (threadIdx.x == 0)
                 *mas.ticket = 0u;
@@ -728,10 +765,12 @@ namespace pmas
 
     int launch_coarse_levels(const MasView &mas, const PcgState *st, cudaStream_t s)
     {
-        if (mas.level_num <= 1 || mas.real_count[0] <= 0)
+        if (mas.level_num <= 1 || mas.real_count[1] <= 0)
             return 0;
-        const int chunks = (mas.real_count[0] + 31) / 32;
-        const int grid = (chunks + LEVEL_THREADS / 32 - 1) / (LEVEL_THREADS / 32);
+        const int grid = mas.level_num == 2 ? (mas.real_count[1] + LEVEL_THREADS / 32 - 1) / (LEVEL_THREADS / 32)
+                                            : mas.real_count[2];
+        if (grid <= 0)
+            return 0;
         dispatch_bd(mas.bd, [&]<int BD>() { k_coarse_levels<BD><<<grid, LEVEL_THREADS, 0, s>>>(mas, st); });
         cuda_check(cudaGetLastError(), "coarse levels launch");
         return 1;

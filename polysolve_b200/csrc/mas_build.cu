@@ -55,6 +55,9 @@ namespace pmas
         v.cslot = cslot.get();
         v.parent = parent.get();
         v.ticket = ticket.get();
+        for (int l = 0; l < MAX_COARSE; ++l)
+            v.kid_ptr[l] = kid_ptr_all.get() ? kid_ptr_all.get() + kid_ptr_off[l] : nullptr;
+        v.kids = kids.get();
         v.identity = identity.get();
         v.rc = rc_override ? rc_override : rc.get();
         v.zc = zc.get();
@@ -707,6 +710,40 @@ namespace pmas
                            "parents");
             M.ticket.alloc(1, "MAS coarse_space ticket");
             cuda_check(cudaMemsetAsync(M.ticket.get(), 0, sizeof(unsigned), s), "memset");
+            // Children lists (local ids) of the real nodes of levels 1..level_num-1.
+            {
+                std::vector<int> ptr_all, kid;
+                for (int l = 0; l < MAX_COARSE; ++l)
+                    M.kid_ptr_off[l] = 0;
+                for (int l = 1; l < M.level_num; ++l)
+                {
+                    std::vector<std::vector<int>> ch((size_t)M.real_count[l]);
+                    for (int i = 0; i < M.real_count[l - 1]; ++i)
+                    {
+                        const int pa = parent[(size_t)coff[l - 1] + i];
+                        if (pa >= 0 && pa - coff[l] < M.real_count[l])
+                            ch[(size_t)(pa - coff[l])].push_back(i);
+                    }
+                    M.kid_ptr_off[l] = (int)ptr_all.size();
+                    ptr_all.push_back((int)kid.size());
+                    for (auto &c : ch)
+                    {
+                        if (c.size() > 32)
+                            throw Error(ERR_INVALID, "[MAS] internal: coarse node with more than 32 children");
+                        kid.insert(kid.end(), c.begin(), c.end());
+                        ptr_all.push_back((int)kid.size());
+                    }
+                }
+                M.kid_ptr_all.alloc(ptr_all.empty() ? 1 : ptr_all.size(), "MAS coarse_space children");
+                M.kids.alloc(kid.empty() ? 1 : kid.size(), "MAS coarse_space children");
+                if (!ptr_all.empty())
+                    cuda_check(cudaMemcpy(M.kid_ptr_all.get(), ptr_all.data(), ptr_all.size() * sizeof(int),
+                                          cudaMemcpyHostToDevice),
+                               "children");
+                if (!kid.empty())
+                    cuda_check(cudaMemcpy(M.kids.get(), kid.data(), kid.size() * sizeof(int), cudaMemcpyHostToDevice),
+                               "children");
+            }
         }
 
         // Coarse vectors (zero once: slots past the component counts stay zero).

@@ -247,6 +247,10 @@ namespace pmas
         const int4 *cslot;      // nodes: coarse-vector node of each coarse level (-1 unused)
         const int *parent;      // coarse nodes: the next level's coarse node it merges into (-1: none)
         unsigned *ticket;       // arrival counter of the coarse-level kernel (zero between launches)
+        // Children of each real coarse node of levels 1..3 (local ids of the level below, in
+        // increasing order, at most 32): node i of level l has kids[kid_ptr[l][i] .. [i + 1]).
+        const int *kid_ptr[MAX_COARSE]; // [1..3] used
+        const int *kids;
         const int *identity;    // coarse matrices: 1 if the inverse is exactly the identity
         double *rc;             // coarse residual, coarse nodes * bd (level-0 components first)
         double *zc;             // coarse correction, coarse nodes * bd
@@ -376,6 +380,8 @@ namespace pmas
         DevBuf<int4> cslot;
         DevBuf<int> parent, identity;
         DevBuf<unsigned> ticket;
+        DevBuf<int> kid_ptr_all, kids; // kid_ptr of levels 1..3 back to back
+        int kid_ptr_off[MAX_COARSE] = {0, 0, 0, 0};
         int first_iso_bank = 0;
         int real_count[MAX_COARSE] = {0, 0, 0, 0};
         DevBuf<int> coarse_active;
