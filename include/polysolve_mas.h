@@ -102,6 +102,15 @@ int mas_solve_multi(mas_solver *h, const double *B, double *X, int n, int nrhs);
 
 /* New: solve with device pointers (length n, caller's order) on the handle's stream; the call
  * returns when the solve has finished. */
+/* Batched solves of independent systems (the 64-system workload; no reference counterpart in
+ * MASSolver, which solves one system per call): every handle must be factorized and distinct;
+ * b[i], x[i] have length n[i] (host arrays, or device arrays when device_pointers != 0). Each
+ * handle runs on its own CUDA stream from a pool of `threads` host threads (<= 0: one per
+ * hardware thread, at most 64), so small systems overlap on the GPU. statuses (optional, count
+ * entries) receives each handle's status; the return value is the first non-zero status. */
+int mas_solve_batch(mas_solver *const *handles, int count, const double *const *b, double *const *x,
+                    const int *n, int device_pointers, int threads, int *statuses);
+
 int mas_solve_device(mas_solver *h, const double *d_b, double *d_x, int n);
 
 /* New: run the handle's device work on the caller's CUDA stream (a cudaStream_t; NULL restores

@@ -732,7 +732,8 @@ namespace pmas
 
     int device_sm_count()
     {
-        static int cached_dev = -1, cached = 148;
+        // Per host thread: batched solves run handles on several threads at once.
+        static thread_local int cached_dev = -1, cached = 148;
         int dev = 0;
         cudaGetDevice(&dev);
         if (dev != cached_dev)

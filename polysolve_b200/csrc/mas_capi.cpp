@@ -17,7 +17,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <limits>
+#include <thread>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -1008,6 +1010,59 @@ extern "C" int mas_solve_multi(mas_solver *h, const double *B, double *X, int n,
         for (int c = 0; c < nrhs; ++c)
             h->solve(B + (size_t)c * n, X + (size_t)c * n, n);
     });
+}
+
+extern "C" int mas_solve_batch(mas_solver *const *handles, int count, const double *const *b, double *const *x,
+                               const int *n, int device_pointers, int threads, int *statuses)
+{
+    if (count < 0 || (count > 0 && (!handles || !b || !x || !n)))
+        return MAS_ERR_INVALID;
+    for (int i = 0; i < count; ++i)
+        if (!handles[i])
+            return MAS_ERR_INVALID;
+    for (int i = 0; i < count; ++i)
+        for (int j = i + 1; j < count; ++j)
+            if (handles[i] == handles[j])
+            {
+                handles[i]->last_error = "[MAS] solve_batch: the same handle appears twice.";
+                return MAS_ERR_INVALID;
+            }
+    int workers = threads > 0 ? threads : (int)std::thread::hardware_concurrency();
+    workers = std::max(1, std::min({workers, count, 64}));
+    std::atomic<int> next{0};
+    std::vector<int> rc((size_t)count, MAS_OK);
+    auto work = [&] {
+        for (int i = next.fetch_add(1); i < count; i = next.fetch_add(1))
+        {
+            mas_solver *h = handles[i];
+            rc[(size_t)i] = guarded(h, [&] {
+                if (device_pointers)
+                    h->solve_device(b[i], x[i], n[i]);
+                else
+                    h->solve(b[i], x[i], n[i]);
+            });
+        }
+    };
+    if (workers <= 1)
+        work();
+    else
+    {
+        std::vector<std::thread> pool;
+        pool.reserve((size_t)workers);
+        for (int w = 0; w < workers; ++w)
+            pool.emplace_back(work);
+        for (auto &t : pool)
+            t.join();
+    }
+    int first = MAS_OK;
+    for (int i = 0; i < count; ++i)
+    {
+        if (statuses)
+            statuses[i] = rc[(size_t)i];
+        if (first == MAS_OK && rc[(size_t)i] != MAS_OK)
+            first = rc[(size_t)i];
+    }
+    return first;
 }
 
 extern "C" int mas_solve_device(mas_solver *h, const double *d_b, double *d_x, int n)

@@ -39,7 +39,7 @@ MAS_ERR_NO_DEVICE = 8
 EXPORTED_SYMBOLS = [
     "mas_create", "mas_create_json", "mas_destroy", "mas_set_parameters", "mas_get_info", "mas_name",
     "mas_analyze_pattern", "mas_set_positions", "mas_factorize_csc", "mas_solve", "mas_solve_multi",
-    "mas_solve_device", "mas_set_stream", "mas_spmv_dot_noalloc", "mas_last_error", "mas_get_sizes", "mas_get_ordering", "mas_order_blocks",
+    "mas_solve_device", "mas_solve_batch", "mas_set_stream", "mas_spmv_dot_noalloc", "mas_last_error", "mas_get_sizes", "mas_get_ordering", "mas_order_blocks",
     "mas_get_coarse_map", "mas_get_inverses", "mas_debug_spmv", "mas_debug_apply",
 ]
 
@@ -82,6 +82,7 @@ def library() -> ctypes.CDLL:
         L.mas_solve.argtypes = [vp, vp, vp, i]
         L.mas_solve_multi.argtypes = [vp, vp, vp, i, i]
         L.mas_solve_device.argtypes = [vp, ctypes.c_void_p, ctypes.c_void_p, i]
+        L.mas_solve_batch.argtypes = [hp, i, hp, hp, ip, i, i, ip]
         L.mas_set_stream.argtypes = [vp, vp]
         L.mas_spmv_dot_noalloc.argtypes = [vp, vp, vp, vp, i, vp]
         L.mas_last_error.argtypes = [vp]
@@ -95,6 +96,53 @@ def library() -> ctypes.CDLL:
         L.mas_order_blocks.argtypes = [i, vp, vp, i, vp, ctypes.c_char_p, ip, ip]
         _LIB = L
     return _LIB
+
+
+def solve_batch(solvers: list, bs: list, xs: list | None = None, *, threads: int = 0) -> list:
+    """New: solve independent factorized systems concurrently (``mas_solve_batch``): solver i
+    solves A_i x_i = b_i on its own CUDA stream, from a pool of host threads. bs / xs hold float64
+    numpy arrays (written in place; allocated when xs is None). Returns xs. Raises the first
+    failing solver's error; every solver's status stays readable through its ``get_info``."""
+    count = len(solvers)
+    if len(bs) != count or (xs is not None and len(xs) != count):
+        raise ValueError("solvers, bs and xs must have the same length")
+    bs = [np.ascontiguousarray(b, dtype=np.float64) for b in bs]
+    if xs is None:
+        xs = [np.zeros_like(b) for b in bs]
+    for x, b in zip(xs, bs):
+        if not (isinstance(x, np.ndarray) and x.dtype == np.float64 and x.flags.c_contiguous) or x.size != b.size:
+            raise TypeError("each x must be a contiguous float64 numpy array of its b's size")
+    VP = ctypes.c_void_p
+    handles = (VP * max(count, 1))(*[s._h for s in solvers])
+    bp = (VP * max(count, 1))(*[b.ctypes.data for b in bs])
+    xp = (VP * max(count, 1))(*[x.ctypes.data for x in xs])
+    ns = np.array([b.size for b in bs] or [0], dtype=np.int32)
+    st = np.zeros(max(count, 1), dtype=np.int32)
+    rc = library().mas_solve_batch(handles, count, bp, xp, ns.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), 0,
+                                   int(threads), st.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+    if rc != MAS_OK:
+        bad = next((k for k in range(count) if st[k] != MAS_OK), None)
+        _check(int(rc), solvers[bad]._h if bad is not None else (solvers[0]._h if count else None))
+    return xs
+
+
+def solve_batch_device(solvers: list, b_ptrs: list, x_ptrs: list, ns: list, *, threads: int = 0) -> None:
+    """New: like ``solve_batch`` with device pointers (e.g. torch ``data_ptr()``) in each system's
+    caller order."""
+    count = len(solvers)
+    if not (len(b_ptrs) == len(x_ptrs) == len(ns) == count):
+        raise ValueError("solvers, b_ptrs, x_ptrs and ns must have the same length")
+    VP = ctypes.c_void_p
+    handles = (VP * max(count, 1))(*[s._h for s in solvers])
+    bp = (VP * max(count, 1))(*[int(p) for p in b_ptrs])
+    xp = (VP * max(count, 1))(*[int(p) for p in x_ptrs])
+    nn = np.array(list(ns) or [0], dtype=np.int32)
+    st = np.zeros(max(count, 1), dtype=np.int32)
+    rc = library().mas_solve_batch(handles, count, bp, xp, nn.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), 1,
+                                   int(threads), st.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+    if rc != MAS_OK:
+        bad = next((k for k in range(count) if st[k] != MAS_OK), None)
+        _check(int(rc), solvers[bad]._h if bad is not None else (solvers[0]._h if count else None))
 
 
 def order_blocks(A, block_dim: int, mode: str, positions: np.ndarray | None = None) -> tuple[np.ndarray, int]:
