@@ -163,6 +163,11 @@ int mas_debug_spmv(mas_solver *h, const double *x, double *y, int len);
 
 /* z = M^-1 r (MAS apply) on host vectors in padded order. */
 int mas_debug_apply(mas_solver *h, const double *r, double *z, int len);
+/* Test hooks of the several-right-hand-side kernels: padded block order with RHS_GROUP (4)
+ * interleaved columns (value index (node * bd + component) * 4 + column); len = padded length * 4.
+ * No reference counterpart. */
+int mas_debug_apply_multi(mas_solver *h, const double *rin, double *zout, int len);
+int mas_debug_spmv_multi(mas_solver *h, const double *xin, double *yout, int len);
 
 #ifdef __cplusplus
 }

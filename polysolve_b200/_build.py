@@ -39,6 +39,7 @@ CU_SOURCES = [
     "mas_apply.cu",
     "mas_pcg.cu",
     "mas_noalloc.cu",
+    "mas_multi.cu",
 ]
 CPP_SOURCES = ["mas_capi.cpp", "mas_ordering.cpp", "mas_json.cpp"]
 

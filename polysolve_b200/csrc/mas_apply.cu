@@ -504,6 +504,255 @@ namespace pmas
             }
         }
 
+        // ---- G right-hand sides at once (binary16 inverses only): the B operand's eight columns
+        // hold the hi / lo splits of the G = RHS_GROUP vectors, so one pass over an inverse and the
+        // same 36 MMAs serve all of them; every lane of a fragment quad holds a different
+        // right-hand side of the result. Vectors are interleaved (value e of right-hand side g at
+        // e * G + g). Per-right-hand-side dots and PCG steps; st[G] is the group record.
+        template <int BD>
+        struct ApplyLayoutG
+        {
+            static constexpr int N = 32 * BD;
+            static constexpr int G = RHS_GROUP;
+            static constexpr int S = (2 * BD) * (2 * BD - 1) / 2 * 256 + 2 * BD * 192;
+            static constexpr int STAGE_BYTES = S * 2;
+            static constexpr int XS_BYTES = 8 * G * N; // hi, lo (binary16) and the FP32 result rows
+            static constexpr int WARP_BYTES = 2 * STAGE_BYTES + XS_BYTES + 16;
+            static constexpr int SMEM_LIMIT = 232448 - 1024;
+            static constexpr int W0 = SMEM_LIMIT / WARP_BYTES;
+            static constexpr int WARPS = W0 > 16 ? 16 : W0;
+            static_assert(STAGE_BYTES % 16 == 0, "bulk copies need 16-byte multiples");
+            static_assert(2 * G == 8, "the B operand has eight columns: G hi / lo pairs");
+        };
+
+        template <int BD>
+        __device__ __forceinline__ void symv_mma16_g(const __half *M, const __half *xh, const __half *xl, float *ys,
+                                                     int lane)
+        {
+            constexpr int NS = 2 * BD, NB = NS * (NS - 1) / 2, N = 32 * BD;
+            const int g = lane >> 2, q = lane & 3;
+            const int c = lane >> 3, rr = lane & 7;
+            // B column n = g: right-hand side g / 2, hi (even) or lo (odd).
+            const __half *xsrc = ((g & 1) ? xl : xh) + (g >> 1) * N;
+            uint32_t bf[NS][2];
+#pragma unroll
+            for (int S = 0; S < NS; ++S)
+            {
+                bf[S][0] = *reinterpret_cast<const uint32_t *>(xsrc + 16 * S + 2 * q);
+                bf[S][1] = *reinterpret_cast<const uint32_t *>(xsrc + 16 * S + 2 * q + 8);
+            }
+            float d[NS][4];
+#pragma unroll
+            for (int R = 0; R < NS; ++R)
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    d[R][i] = 0.f;
+            const uint32_t mbase = smem_addr(M);
+            const int ct = (c == 1) ? 2 : (c == 2 ? 1 : c);
+            const uint32_t row_off = (uint32_t)(rr * 16);
+#pragma unroll
+            for (int R = 0; R < NS; ++R)
+#pragma unroll
+                for (int S = R + 1; S < NS; ++S)
+                {
+                    const uint32_t blk = mbase + (uint32_t)((R * (2 * NS - R - 1) / 2 + (S - R - 1)) * 512);
+                    uint32_t a[4];
+                    ldsm_x4(a, blk + c * 128 + row_off);
+                    mma_16816(d[R], a, bf[S][0], bf[S][1]);
+                    ldsm_x4_trans(a, blk + ct * 128 + row_off);
+                    mma_16816(d[S], a, bf[R][0], bf[R][1]);
+                }
+            const int cd = (c == 1) ? 1 : (c == 3 ? 2 : 0);
+#pragma unroll
+            for (int R = 0; R < NS; ++R)
+            {
+                const uint32_t blk = mbase + (uint32_t)((NB * 256 + R * 192) * 2);
+                uint32_t a[4];
+                ldsm_x4_trans(a, blk + cd * 128 + row_off);
+                a[2] = ldsm_x1(blk + 128 + row_off);
+                mma_16816(d[R], a, bf[R][0], bf[R][1]);
+            }
+            // Columns 2q, 2q + 1 of rows g, g + 8 of each block row: right-hand side q.
+#pragma unroll
+            for (int R = 0; R < NS; ++R)
+            {
+                ys[q * N + 16 * R + g] = d[R][0] + d[R][1];
+                ys[q * N + 16 * R + g + 8] = d[R][2] + d[R][3];
+            }
+            __syncwarp();
+        }
+
+        template <int BD, int MODE>
+        __global__ void __launch_bounds__(ApplyLayoutG<BD>::WARPS * 32)
+            k_mas_apply_g(MasView mas, const double *__restrict__ r, double *__restrict__ z0, PcgState *st,
+                          ReduceBuf red, PcgConfig cfg)
+        {
+            using L = ApplyLayoutG<BD>;
+            constexpr int N = L::N, S = L::S, WARPS = L::WARPS, G = L::G;
+            constexpr int THREADS = WARPS * 32;
+            PcgState *grp = st + G;
+            if (grp->done)
+                return;
+            extern __shared__ __align__(128) unsigned char smem[];
+            const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+            unsigned char *base = smem + (size_t)w * L::WARP_BYTES;
+            __half *stage0 = reinterpret_cast<__half *>(base);
+            __half *stage1 = reinterpret_cast<__half *>(base + L::STAGE_BYTES);
+            __half *xh = reinterpret_cast<__half *>(base + 2 * L::STAGE_BYTES);
+            __half *xl = xh + G * N;
+            float *ys = reinterpret_cast<float *>(base + 2 * L::STAGE_BYTES + 4 * G * N);
+            uint64_t *bar = reinterpret_cast<uint64_t *>(base + 2 * L::STAGE_BYTES + L::XS_BYTES);
+            const __half *__restrict__ inv = static_cast<const __half *>(mas.inv);
+            const int banks = mas.banks;
+            const int items = banks + mas.n_coarse_active;
+            const int total_warps = gridDim.x * WARPS;
+            const int gw = blockIdx.x * WARPS + w;
+            auto mat_of = [&](int m) { return m < banks ? m : banks + mas.coarse_active[m - banks]; };
+            auto in_of = [&](int m) -> const double * {
+                return m < banks ? r + (size_t)m * N * G : mas.rc + (size_t)(mat_of(m) - banks) * N * G;
+            };
+            const uint64_t pol = l2_evict_first_policy();
+            if (lane == 0)
+            {
+                mbar_init(&bar[0], 1);
+                mbar_init(&bar[1], 1);
+                fence_mbar_init();
+            }
+            __syncwarp();
+            if (lane == 0)
+            {
+                if (gw < items)
+                    bulk_load_stream(stage0, inv + (size_t)mat_of(gw) * S, L::STAGE_BYTES, &bar[0], pol);
+                if (gw + total_warps < items)
+                    bulk_load_stream(stage1, inv + (size_t)mat_of(gw + total_warps) * S, L::STAGE_BYTES, &bar[1],
+                                     pol);
+            }
+            double part[3 * G]; // per right-hand side: coupled banks, isolated banks, coarse
+#pragma unroll
+            for (int i = 0; i < 3 * G; ++i)
+                part[i] = 0.0;
+            uint32_t phase0 = 0, phase1 = 0;
+            bool ok = true;
+            int k = 0;
+            for (int m = gw; m < items; m += total_warps, ++k)
+            {
+                const bool s1 = (k & 1) != 0;
+                __half *stage = s1 ? stage1 : stage0;
+                uint64_t *b = s1 ? &bar[1] : &bar[0];
+                const bool coarse = m >= banks;
+                const int mat = mat_of(m);
+                const double *in = in_of(m);
+                double *out = coarse ? mas.zc + (size_t)(mat - banks) * N * G : z0 + (size_t)m * N * G;
+                double r64[BD][G];
+#pragma unroll
+                for (int t = 0; t < BD; ++t)
+#pragma unroll
+                    for (int h = 0; h < G / 2; ++h)
+                    {
+                        const double2 v = *reinterpret_cast<const double2 *>(in + (t * 32 + lane) * G + 2 * h);
+                        r64[t][2 * h] = v.x;
+                        r64[t][2 * h + 1] = v.y;
+                    }
+                double xscale[G];
+#pragma unroll
+                for (int gg = 0; gg < G; ++gg)
+                {
+                    double amax = 0.0;
+#pragma unroll
+                    for (int t = 0; t < BD; ++t)
+                        amax = fmax(amax, fabs(r64[t][gg]));
+#pragma unroll
+                    for (int o = 16; o >= 1; o >>= 1)
+                        amax = fmax(amax, __shfl_xor_sync(FULL, amax, o));
+                    xscale[gg] = (amax > 0.0 && isfinite(amax)) ? ldexp(1.0, 14 - ilogb(amax)) : 1.0;
+#pragma unroll
+                    for (int t = 0; t < BD; ++t)
+                    {
+                        const float v = (float)(r64[t][gg] * xscale[gg]);
+                        const __half h = __float2half_rn(v);
+                        xh[gg * N + t * 32 + lane] = h;
+                        xl[gg * N + t * 32 + lane] = __float2half_rn(v - __half2float(h));
+                    }
+                }
+                __syncwarp();
+                if (!mbar_wait_bounded(b, s1 ? phase1 : phase0, &grp->error))
+                {
+                    ok = false;
+                    break;
+                }
+                if (s1)
+                    phase1 ^= 1u;
+                else
+                    phase0 ^= 1u;
+                const bool ident = coarse && mas.identity[mat - banks];
+                if (!ident)
+                    symv_mma16_g<BD>(stage, xh, xl, ys, lane);
+                __syncwarp();
+                const int mn = m + 2 * total_warps;
+                if (lane == 0 && mn < items)
+                {
+                    fence_proxy_async_smem();
+                    bulk_load_stream(stage, inv + (size_t)mat_of(mn) * S, L::STAGE_BYTES, b, pol);
+                }
+                const double mscale = mas.inv_scale[mat];
+                const int slot = coarse ? 2 : ((m >= mas.first_iso_bank) ? 1 : 0);
+#pragma unroll
+                for (int t = 0; t < BD; ++t)
+                {
+                    double zv[G];
+#pragma unroll
+                    for (int gg = 0; gg < G; ++gg)
+                    {
+                        zv[gg] = ident ? r64[t][gg] : (double)ys[gg * N + t * 32 + lane] * (mscale / xscale[gg]);
+                        const double d = zv[gg] * r64[t][gg];
+                        if (slot == 0)
+                            part[gg] += d;
+                        else if (slot == 1)
+                            part[G + gg] += d;
+                        else
+                            part[2 * G + gg] += d;
+                    }
+#pragma unroll
+                    for (int h = 0; h < G / 2; ++h)
+                        *reinterpret_cast<double2 *>(out + (t * 32 + lane) * G + 2 * h) =
+                            make_double2(zv[2 * h], zv[2 * h + 1]);
+                }
+                __syncwarp();
+            }
+            if (!ok)
+            {
+                if (lane == 0)
+                {
+                    for (long long i = 0; i < MBAR_SPIN_LIMIT; ++i)
+                        if (mbar_try_wait(&bar[0], phase0) && mbar_try_wait(&bar[1], phase1))
+                            break;
+                }
+                __syncwarp();
+            }
+            double tot[3 * G];
+            if (grid_reduce<3 * G, THREADS>(part, red.rz_parts, &grp->counter[4], tot) && threadIdx.x == 0)
+            {
+                const double Lc = (double)cfg.level_num;
+                int all_done = 1;
+#pragma unroll
+                for (int gg = 0; gg < G; ++gg)
+                {
+                    PcgState *sg = st + gg;
+                    if (!sg->done)
+                    {
+                        sg->rz_coarse = tot[2 * G + gg] + Lc * tot[G + gg];
+                        pcg_finalize(sg, cfg, MODE, tot[gg] + tot[G + gg] + sg->rz_coarse, 0.0);
+                        if (sg->error)
+                            grp->error = sg->error;
+                    }
+                    all_done &= sg->done ? 1 : 0;
+                }
+                grp->iter = MODE == 1 ? 0 : grp->iter + 1;
+                if (all_done)
+                    grp->done = 1;
+            }
+        }
+
         // Coarse levels above the first from its components rc (level 0 of the coarse vector).
         // Each real node of level l sums its (at most 32) children of level l - 1 in a warp
         // (lane = child, in increasing order; deterministic). With three or more levels one CTA
@@ -774,6 +1023,55 @@ namespace pmas
             return 0;
         dispatch_bd(mas.bd, [&]<int BD>() { k_coarse_levels<BD><<<grid, LEVEL_THREADS, 0, s>>>(mas, st); });
         cuda_check(cudaGetLastError(), "coarse levels launch");
+        return 1;
+    }
+
+    void prepare_kernels_g(int bd)
+    {
+        dispatch_bd(bd, [&]<int BD>() {
+            using L = ApplyLayoutG<BD>;
+            const int smem = L::WARPS * L::WARP_BYTES;
+            cuda_check(cudaFuncSetAttribute(k_mas_apply_g<BD, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                       "apply smem attribute");
+            cuda_check(cudaFuncSetAttribute(k_mas_apply_g<BD, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                       "apply smem attribute");
+        });
+    }
+
+    void launch_mas_apply_g(const MasView &mas, const double *r, double *z, PcgState *st, ReduceBuf red, PcgConfig cfg,
+                            int mode, cudaStream_t s)
+    {
+        if (mas.storage != STORE_F16)
+            throw Error(ERR_INVALID, "[MAS] several right-hand sides at once need precision fp16");
+        dispatch_bd(mas.bd, [&]<int BD>() {
+            using L = ApplyLayoutG<BD>;
+            const int items = mas.banks + mas.n_coarse_active;
+            int grid = (items + L::WARPS - 1) / L::WARPS;
+            const int sms = device_sm_count();
+            grid = grid > sms ? sms : (grid < 1 ? 1 : grid);
+            if (grid * 3 * RHS_GROUP > red.capacity * 6)
+                throw Error(ERR_INVALID, "[MAS] reduction scratch too small");
+            const size_t smem = (size_t)L::WARPS * L::WARP_BYTES;
+            if (mode == 1)
+                k_mas_apply_g<BD, 1><<<grid, L::WARPS * 32, smem, s>>>(mas, r, z, st, red, cfg);
+            else
+                k_mas_apply_g<BD, 2><<<grid, L::WARPS * 32, smem, s>>>(mas, r, z, st, red, cfg);
+        });
+        cuda_check(cudaGetLastError(), "multi apply launch");
+    }
+
+    int launch_coarse_levels_g(const MasView &mas, cudaStream_t s)
+    {
+        if (mas.level_num <= 1 || mas.real_count[1] <= 0)
+            return 0;
+        const int grid = mas.level_num == 2 ? (mas.real_count[1] + LEVEL_THREADS / 32 - 1) / (LEVEL_THREADS / 32)
+                                            : mas.real_count[2];
+        if (grid <= 0)
+            return 0;
+        dispatch_bd(mas.bd, [&]<int BD>() {
+            k_coarse_levels<BD * RHS_GROUP><<<grid, LEVEL_THREADS, 0, s>>>(mas, nullptr);
+        });
+        cuda_check(cudaGetLastError(), "multi coarse levels launch");
         return 1;
     }
 

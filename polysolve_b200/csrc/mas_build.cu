@@ -24,7 +24,7 @@
 
 namespace pmas
 {
-    MasView MasDevice::view(double *rc_override) const
+    MasView MasDevice::view(double *rc_override, double *zc_override) const
     {
         MasView v{};
         v.bd = bd;
@@ -60,7 +60,7 @@ namespace pmas
         v.kids = kids.get();
         v.identity = identity.get();
         v.rc = rc_override ? rc_override : rc.get();
-        v.zc = zc.get();
+        v.zc = zc_override ? zc_override : zc.get();
         return v;
     }
 

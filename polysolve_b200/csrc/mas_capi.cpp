@@ -247,6 +247,18 @@ struct mas_solver
     DevBuf<PcgState> st;
     DevBuf<double> partials;
     int red_capacity = 0;
+
+    // Several right-hand sides at once: groups of RHS_GROUP interleaved vectors, one PcgState
+    // per right-hand side plus the group record, their own graphs.
+    DevBuf<double> gx, gb, gr, gp, gz, gAp, grc, gzc, gio, gpartials;
+    DevBuf<PcgState> gst;
+    cudaGraphExec_t ggraph[2] = {nullptr, nullptr};
+    std::vector<std::pair<int, long long>> ggraph_counts[2];
+    uint64_t ggraph_key = 0;
+    bool ggraph_aligned = false;
+    std::vector<int> rhs_iterations, rhs_status;
+    std::vector<double> rhs_error;
+    bool last_multi = false; // the last solve was a several-right-hand-side solve
     PcgState *h_st = nullptr; // pinned, 2 slots
 
     ~mas_solver()
@@ -259,6 +271,9 @@ struct mas_solver
         for (cudaEvent_t e : ev_pool)
             cudaEventDestroy(e);
         for (auto &g : graph_exec)
+            if (g)
+                cudaGraphExecDestroy(g);
+        for (auto &g : ggraph)
             if (g)
                 cudaGraphExecDestroy(g);
         if (h_st)
@@ -474,6 +489,8 @@ struct mas_solver
         }
         build_mas(mas, A, d_node_real.get(), p.storage, first_iso_bank, stream);
         prepare_kernels(bd_, p.storage);
+        if (p.storage == STORE_F16)
+            prepare_kernels_g(bd_);
         drop_graph();
 
         const size_t len = (size_t)banks * 32 * bd_;
@@ -548,8 +565,13 @@ struct mas_solver
                 cudaGraphExecDestroy(graph_exec[i]);
             graph_exec[i] = nullptr;
             graph_counts[i].clear();
+            if (ggraph[i])
+                cudaGraphExecDestroy(ggraph[i]);
+            ggraph[i] = nullptr;
+            ggraph_counts[i].clear();
         }
         graph_key = 0;
+        ggraph_key = 0;
     }
 
     void capture(int slot, const BankedView &Av, const MasView &mv, const PcgConfig &cfg, int P, int chunk,
@@ -721,11 +743,242 @@ struct mas_solver
             cuda_check(cudaMemsetAsync(x.get(), 0, x.bytes(), stream), "memset");
     }
 
+    // ---- Several right-hand sides at once (RHS_GROUP per group, binary16 inverses). ----------
+    bool multi_supported() const
+    {
+        return factorized && mas.storage == STORE_F16 && !p.polak_ribiere && !p.initial_guess_input;
+    }
+
+    void alloc_multi()
+    {
+        const size_t len = (size_t)banks * 32 * bd * RHS_GROUP;
+        for (DevBuf<double> *v : {&gx, &gb, &gr, &gp, &gz, &gAp})
+            v->alloc(len, "device_buffers several right-hand sides");
+        const size_t clen = (size_t)std::max(mas.coarse_nodes, 1) * bd * RHS_GROUP;
+        grc.alloc(clen, "MAS coarse_vectors several right-hand sides");
+        gzc.alloc(clen, "MAS coarse_vectors several right-hand sides");
+        gio.alloc((size_t)n * RHS_GROUP, "device_buffers several right-hand sides");
+        gpartials.alloc((size_t)red_capacity * 6 * RHS_GROUP, "device_buffers reduction");
+        gst.alloc(RHS_GROUP + 1, "device_buffers state");
+        // Coarse slots past the component counts are read by the coarse products and must be zero.
+        cuda_check(cudaMemsetAsync(grc.get(), 0, grc.bytes(), stream), "memset");
+        cuda_check(cudaMemsetAsync(gzc.get(), 0, gzc.bytes(), stream), "memset");
+    }
+
+    ReduceBuf red_g()
+    {
+        double *base = gpartials.get();
+        const size_t c = (size_t)red_capacity;
+        return ReduceBuf{base, red_capacity, base + 2 * RHS_GROUP * c, base + 3 * RHS_GROUP * c};
+    }
+
+    MasView view_g() const { return mas.view(grc.get(), gzc.get()); }
+
+    void launch_iteration_g(const BankedView &Av, const MasView &mv, const PcgConfig &cfg, int P, bool residual)
+    {
+        PcgState *S = gst.get();
+        PcgState *grp = S + RHS_GROUP;
+        run("spmv_pap", 1, [&] { launch_spmv_g(SPMV_PAP, Av, gp.get(), gAp.get(), nullptr, S, red_g(), 1, 0, stream); });
+        run("update_xr", 1,
+            [&] { launch_update_xr_g(mv, gx.get(), gr.get(), gp.get(), gAp.get(), S, red_g(), P, stream); });
+        if (residual)
+        {
+            run("spmv_residual", 1,
+                [&] { launch_spmv_g(SPMV_RESIDUAL, Av, gx.get(), gr.get(), gb.get(), S, red_g(), 1, P, stream); });
+            run("restrict", 0, [&] { return launch_restrict_g(mv, gr.get(), grp, P, stream); });
+        }
+        run("coarse_levels", 0, [&] { return launch_coarse_levels_g(mv, stream); });
+        run("mas_apply", 1, [&] { launch_mas_apply_g(mv, gr.get(), gz.get(), S, red_g(), cfg, 2, stream); });
+        run("update_p", 1, [&] { launch_update_p_g(mv, gp.get(), gz.get(), S, 0, stream); });
+    }
+
+    void capture_g(int slot, const BankedView &Av, const MasView &mv, const PcgConfig &cfg, int P, int chunk,
+                   bool aligned)
+    {
+        cudaGraph_t graph = nullptr;
+        capture_slot = slot;
+        cuda_check(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+        capturing = true;
+        auto saved = std::move(graph_counts[slot]);
+        graph_counts[slot].clear();
+        try
+        {
+            for (int i = 0; i < chunk; ++i)
+                launch_iteration_g(Av, mv, cfg, P, aligned ? (slot == 1 && i == chunk - 1) : true);
+        }
+        catch (...)
+        {
+            capturing = false;
+            cudaStreamEndCapture(stream, &graph);
+            if (graph)
+                cudaGraphDestroy(graph);
+            cudaGetLastError();
+            graph_counts[slot] = std::move(saved);
+            throw;
+        }
+        capturing = false;
+        ggraph_counts[slot] = std::move(graph_counts[slot]);
+        graph_counts[slot] = std::move(saved);
+        cuda_check(cudaStreamEndCapture(stream, &graph), "end capture");
+        cudaError_t e = cudaGraphInstantiate(&ggraph[slot], graph, 0);
+        cudaGraphDestroy(graph);
+        cuda_check(e, "graph instantiate");
+    }
+
+    void ensure_graph_g(const BankedView &Av, const MasView &mv, const PcgConfig &cfg, int P, int chunk)
+    {
+        uint64_t key = 1469598103934665603ull;
+        auto mix = [&key](uint64_t v) {
+            key ^= v;
+            key *= 1099511628211ull;
+        };
+        for (const void *ptr : {(const void *)gx.get(), (const void *)gb.get(), (const void *)gr.get(),
+                                (const void *)gp.get(), (const void *)gz.get(), (const void *)gAp.get(),
+                                (const void *)gst.get(), (const void *)gpartials.get(), (const void *)grc.get(),
+                                (const void *)Av.vals, mv.inv, (const void *)stream})
+            mix((uint64_t)(uintptr_t)ptr);
+        mix((uint64_t)cfg.max_iter);
+        mix((uint64_t)cfg.check_period);
+        mix((uint64_t)cfg.use_prec_norm);
+        uint64_t bits;
+        std::memcpy(&bits, &cfg.rel_tol, 8);
+        mix(bits);
+        std::memcpy(&bits, &cfg.abs_tol, 8);
+        mix(bits);
+        mix((uint64_t)P);
+        mix((uint64_t)chunk);
+        if (ggraph[0] && key == ggraph_key)
+            return;
+        for (int i = 0; i < 2; ++i)
+        {
+            if (ggraph[i])
+                cudaGraphExecDestroy(ggraph[i]);
+            ggraph[i] = nullptr;
+            ggraph_counts[i].clear();
+        }
+        ggraph_aligned = (P % chunk == 0);
+        capture_g(0, Av, mv, cfg, P, chunk, ggraph_aligned);
+        if (ggraph_aligned)
+            capture_g(1, Av, mv, cfg, P, chunk, true);
+        ggraph_key = key;
+    }
+
+    // The PCG loop of one group: `cols` live right-hand sides (the others start finished).
+    void pcg_multi(int cols)
+    {
+        const BankedView Av = A.view();
+        const MasView mv = view_g();
+        const PcgConfig cfg = config();
+        PcgState *S = gst.get();
+        PcgState hinit[RHS_GROUP + 1];
+        std::memset(hinit, 0, sizeof(hinit));
+        for (int g = cols; g < RHS_GROUP; ++g)
+            hinit[g].done = 1;
+        cuda_check(cudaMemcpyAsync(S, hinit, sizeof(hinit), cudaMemcpyHostToDevice, stream), "state");
+        run("spmv_residual", 1,
+            [&] { launch_spmv_g(SPMV_RESIDUAL, Av, gx.get(), gr.get(), gb.get(), S, red_g(), 0, 0, stream); });
+        run("restrict", 0, [&] { return launch_restrict_g(mv, gr.get(), S + RHS_GROUP, 0, stream); });
+        run("coarse_levels", 0, [&] { return launch_coarse_levels_g(mv, stream); });
+        run("mas_apply", 1, [&] { launch_mas_apply_g(mv, gr.get(), gz.get(), S, red_g(), cfg, 1, stream); });
+        run("update_p", 1, [&] { launch_update_p_g(mv, gp.get(), gz.get(), S, 1, stream); });
+        PcgState hs[RHS_GROUP + 1];
+        cuda_check(cudaMemcpyAsync(hs, S, sizeof(hs), cudaMemcpyDeviceToHost, stream), "state");
+        cuda_check(cudaStreamSynchronize(stream), "pcg init");
+        for (int g = 0; g < cols; ++g)
+            if (hs[g].error == ERR_NONFINITE || std::isnan(hs[g].rz0) || !std::isfinite(hs[g].rz0))
+                throw Error(ERR_NONFINITE, "[MAS] Invalid initial residual.");
+        const int P = p.true_residual_period;
+        const int chunk = p.poll_period;
+        const bool graphs = p.graphs && !p.profile;
+        if (graphs)
+            ensure_graph_g(Av, mv, cfg, P, chunk);
+        for (int k0 = 1; k0 <= p.max_iter; k0 += chunk)
+        {
+            const int k1 = std::min(p.max_iter, k0 + chunk - 1);
+            if (graphs)
+            {
+                const int g = (ggraph_aligned && (k0 + chunk - 1) % P == 0) ? 1 : 0;
+                cuda_check(cudaGraphLaunch(ggraph[g], stream), "graph launch");
+                for (auto &gc : ggraph_counts[g])
+                {
+                    kstats[gc.first].second.launches += gc.second;
+                    total_launches += gc.second;
+                }
+            }
+            else
+                for (int k = k0; k <= k1; ++k)
+                    launch_iteration_g(Av, mv, cfg, P, k % P == 0);
+            cuda_check(cudaMemcpyAsync(&hs[RHS_GROUP], S + RHS_GROUP, sizeof(PcgState), cudaMemcpyDeviceToHost,
+                                       stream),
+                       "state");
+            cuda_check(cudaStreamSynchronize(stream), "chunk");
+            if (hs[RHS_GROUP].done)
+                break;
+        }
+        cuda_check(cudaMemcpyAsync(hs, S, sizeof(hs), cudaMemcpyDeviceToHost, stream), "state");
+        cuda_check(cudaStreamSynchronize(stream), "pcg");
+        if (hs[RHS_GROUP].error == ERR_TIMEOUT)
+            throw Error(ERR_TIMEOUT, "[MAS] a device-side wait timed out.");
+        for (int g = 0; g < cols; ++g)
+        {
+            rhs_iterations.push_back(hs[g].iter);
+            rhs_status.push_back(hs[g].status == 0 ? MAS_STATUS_REACH_MAX_ITERATIONS : hs[g].status);
+            rhs_error.push_back(hs[g].res_norm);
+        }
+    }
+
+    // Column-major B (n x nrhs) -> X; groups of RHS_GROUP share every matrix and inverse read.
+    void solve_multi(const double *hB, double *hX, int len, int nrhs)
+    {
+        cuda_check(cudaSetDevice(device), "set device");
+        require_factorized(len);
+        if (!multi_supported())
+        {
+            for (int c = 0; c < nrhs; ++c)
+                solve(hB + (size_t)c * n, hX + (size_t)c * n, n);
+            return;
+        }
+        alloc_multi();
+        for (auto &ks : kstats)
+            ks.second = KStat{};
+        rhs_iterations.clear();
+        rhs_status.clear();
+        rhs_error.clear();
+        const size_t glen = (size_t)banks * 32 * bd * RHS_GROUP;
+        auto t0 = std::chrono::steady_clock::now();
+        for (int c0 = 0; c0 < nrhs; c0 += RHS_GROUP)
+        {
+            const int cols = std::min(RHS_GROUP, nrhs - c0);
+            cuda_check(cudaMemcpyAsync(gio.get(), hB + (size_t)c0 * n, sizeof(double) * (size_t)n * cols,
+                                       cudaMemcpyHostToDevice, stream),
+                       "upload B");
+            run("permute_in", 2,
+                [&] { launch_permute_in_g(n, bd, V, cols, d_padded.get(), gio.get(), gb.get(), glen, stream); });
+            cuda_check(cudaMemsetAsync(gx.get(), 0, gx.bytes(), stream), "memset");
+            pcg_multi(cols);
+            run("permute_out", 1,
+                [&] { launch_permute_out_g(n, bd, cols, d_padded.get(), gx.get(), gio.get(), stream); });
+            cuda_check(cudaMemcpyAsync(hX + (size_t)c0 * n, gio.get(), sizeof(double) * (size_t)n * cols,
+                                       cudaMemcpyDeviceToHost, stream),
+                       "download X");
+            cuda_check(cudaStreamSynchronize(stream), "solve multi");
+        }
+        solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        iterations = rhs_iterations.empty() ? 0 : *std::max_element(rhs_iterations.begin(), rhs_iterations.end());
+        residual_norm = rhs_error.empty() ? 0.0 : *std::max_element(rhs_error.begin(), rhs_error.end());
+        status = MAS_STATUS_REACH_RELATIVE_TOLERANCE;
+        for (int st_ : rhs_status)
+            if (st_ == MAS_STATUS_REACH_MAX_ITERATIONS)
+                status = MAS_STATUS_REACH_MAX_ITERATIONS;
+        last_multi = true;
+    }
+
     // MASSolverImpl::solve (MASSolver.cu:376-409).
     void solve(const double *hb, double *hx, int len)
     {
         cuda_check(cudaSetDevice(device), "set device");
         require_factorized(len);
+        last_multi = false;
         if (!hb || !hx)
             throw Error(ERR_INVALID, "[MAS] solve: null vector.");
         cuda_check(cudaMemcpyAsync(io.get(), hb, sizeof(double) * n, cudaMemcpyHostToDevice, stream), "upload b");
@@ -748,6 +1001,7 @@ struct mas_solver
     {
         cuda_check(cudaSetDevice(device), "set device");
         require_factorized(len);
+        last_multi = false;
         load_rhs_device(d_b, d_x);
         pcg();
         run("permute_out", 1, [&] { launch_permute_out(n, bd, V, d_padded.get(), x.get(), d_x, stream); });
@@ -771,6 +1025,20 @@ struct mas_solver
             j.str = s;
             return j;
         };
+        if (last_multi)
+        {
+            Json it, stv, er;
+            it.type = stv.type = er.type = Json::Array;
+            for (size_t i = 0; i < rhs_iterations.size(); ++i)
+            {
+                it.arr.push_back(num(rhs_iterations[i], true));
+                stv.arr.push_back(str(status_string(rhs_status[i])));
+                er.arr.push_back(num(rhs_error[i], false));
+            }
+            o.obj.emplace_back("rhs_iterations", it);
+            o.obj.emplace_back("rhs_status", stv);
+            o.obj.emplace_back("rhs_error", er);
+        }
         o.obj.emplace_back("solver_iter", num(iterations, true));
         o.obj.emplace_back("solver_error", num(residual_norm, false));
         o.obj.emplace_back("solver_status", str(status_string(status)));
@@ -1007,8 +1275,8 @@ extern "C" int mas_solve_multi(mas_solver *h, const double *B, double *X, int n,
     return guarded(h, [&] {
         if (nrhs < 0)
             throw Error(ERR_INVALID, "[MAS] solve_multi: nrhs must be >= 0");
-        for (int c = 0; c < nrhs; ++c)
-            h->solve(B + (size_t)c * n, X + (size_t)c * n, n);
+        if (nrhs > 0)
+            h->solve_multi(B, X, n, nrhs);
     });
 }
 
@@ -1270,5 +1538,96 @@ extern "C" int mas_debug_apply(mas_solver *h, const double *rin, double *zout, i
         launch_prolong(mv, h->z.get(), h->Ap.get(), h->stream);
         cuda_check(cudaMemcpyAsync(zout, h->Ap.get(), sizeof(double) * len, cudaMemcpyDeviceToHost, h->stream), "z");
         cuda_check(cudaStreamSynchronize(h->stream), "apply");
+    });
+}
+
+// Test hooks of the several-right-hand-side kernels (padded, interleaved vectors of
+// RHS_GROUP columns): z = M^-1 r, and y = A x.
+extern "C" int mas_debug_apply_multi(mas_solver *h, const double *rin, double *zout, int len)
+{
+    if (!h)
+        return MAS_ERR_INVALID;
+    return guarded(h, [&] {
+        cuda_check(cudaSetDevice(h->device), "set device");
+        if (!h->multi_supported() || len != h->banks * 32 * h->bd * RHS_GROUP)
+            throw Error(ERR_NOT_FACTORIZED, "[MAS] debug_apply_multi: size mismatch or not fp16.");
+        h->alloc_multi();
+        PcgState hinit[RHS_GROUP + 1];
+        std::memset(hinit, 0, sizeof(hinit));
+        cuda_check(cudaMemcpyAsync(h->gst.get(), hinit, sizeof(hinit), cudaMemcpyHostToDevice, h->stream), "state");
+        cuda_check(cudaMemcpyAsync(h->gr.get(), rin, sizeof(double) * len, cudaMemcpyHostToDevice, h->stream), "r");
+        const MasView mv = h->view_g();
+        launch_restrict_g(mv, h->gr.get(), h->gst.get() + RHS_GROUP, 0, h->stream);
+        launch_coarse_levels_g(mv, h->stream);
+        launch_mas_apply_g(mv, h->gr.get(), h->gz.get(), h->gst.get(), h->red_g(), h->config(), 1, h->stream);
+        launch_update_p_g(mv, h->gp.get(), h->gz.get(), h->gst.get(), 1, h->stream);
+        cuda_check(cudaMemcpyAsync(zout, h->gp.get(), sizeof(double) * len, cudaMemcpyDeviceToHost, h->stream), "z");
+        cuda_check(cudaStreamSynchronize(h->stream), "apply");
+    });
+}
+
+extern "C" int mas_debug_spmv_multi(mas_solver *h, const double *xin, double *yout, int len)
+{
+    if (!h)
+        return MAS_ERR_INVALID;
+    return guarded(h, [&] {
+        cuda_check(cudaSetDevice(h->device), "set device");
+        if (!h->multi_supported() || len != h->banks * 32 * h->bd * RHS_GROUP)
+            throw Error(ERR_NOT_FACTORIZED, "[MAS] debug_spmv_multi: size mismatch or not fp16.");
+        h->alloc_multi();
+        PcgState hinit[RHS_GROUP + 1];
+        std::memset(hinit, 0, sizeof(hinit));
+        cuda_check(cudaMemcpyAsync(h->gst.get(), hinit, sizeof(hinit), cudaMemcpyHostToDevice, h->stream), "state");
+        cuda_check(cudaMemcpyAsync(h->gp.get(), xin, sizeof(double) * len, cudaMemcpyHostToDevice, h->stream), "x");
+        launch_spmv_g(SPMV_PAP, h->A.view(), h->gp.get(), h->gAp.get(), nullptr, h->gst.get(), h->red_g(), 1, 0,
+                      h->stream);
+        cuda_check(cudaMemcpyAsync(yout, h->gAp.get(), sizeof(double) * len, cudaMemcpyDeviceToHost, h->stream), "y");
+        cuda_check(cudaStreamSynchronize(h->stream), "spmv");
+    });
+}
+
+// Test hook: the device vectors after `iters` iterations of the several-right-hand-side loop
+// (iters = 0: after the initial residual and apply), for the columns of a padded interleaved B.
+// out: x, r, p, z (each len values) and the RHS_GROUP + 1 states (raw bytes appended).
+extern "C" int mas_debug_multi_state(mas_solver *h, const double *Bpad, int len, int iters, double *out,
+                                     void *states)
+{
+    if (!h)
+        return MAS_ERR_INVALID;
+    return guarded(h, [&] {
+        cuda_check(cudaSetDevice(h->device), "set device");
+        if (!h->multi_supported() || len != h->banks * 32 * h->bd * RHS_GROUP)
+            throw Error(ERR_NOT_FACTORIZED, "[MAS] debug_multi_state: size mismatch or not fp16.");
+        h->alloc_multi();
+        cuda_check(cudaMemcpyAsync(h->gb.get(), Bpad, sizeof(double) * len, cudaMemcpyHostToDevice, h->stream), "b");
+        cuda_check(cudaMemsetAsync(h->gx.get(), 0, h->gx.bytes(), h->stream), "memset");
+        const int saved_max = h->p.max_iter;
+        const bool saved_graphs = h->p.graphs;
+        h->p.max_iter = iters;
+        h->p.graphs = false;
+        try
+        {
+            h->rhs_iterations.clear();
+            h->rhs_status.clear();
+            h->rhs_error.clear();
+            h->pcg_multi(RHS_GROUP);
+        }
+        catch (...)
+        {
+            h->p.max_iter = saved_max;
+            h->p.graphs = saved_graphs;
+            throw;
+        }
+        h->p.max_iter = saved_max;
+        h->p.graphs = saved_graphs;
+        const double *src[4] = {h->gx.get(), h->gr.get(), h->gp.get(), h->gz.get()};
+        for (int k = 0; k < 4; ++k)
+            cuda_check(cudaMemcpyAsync(out + (size_t)k * len, src[k], sizeof(double) * len, cudaMemcpyDeviceToHost,
+                                       h->stream),
+                       "state vectors");
+        cuda_check(cudaMemcpyAsync(states, h->gst.get(), sizeof(PcgState) * (RHS_GROUP + 1), cudaMemcpyDeviceToHost,
+                                   h->stream),
+                   "states");
+        cuda_check(cudaStreamSynchronize(h->stream), "debug");
     });
 }

@@ -18,6 +18,7 @@ namespace pmas
     constexpr int BANK = 32;
     constexpr int MAX_COARSE = 4; // coarse levels (MASPreconditioner.hpp:11)
     constexpr int LEVELS = MAX_COARSE + 1;
+    constexpr int RHS_GROUP = 4; // right-hand sides solved together (several-RHS solves)
 
     // Storage precision of the subdomain inverses. FP16 keeps one power-of-two scale per matrix
     // (largest magnitude -> [2^14, 2^15)); products are formed in FP32 and scaled back in FP64.
@@ -357,6 +358,24 @@ namespace pmas
     void launch_mas_apply(const MasView &mas, const double *r, double *z0, PcgState *st, ReduceBuf red,
                           PcgConfig cfg, int mode, cudaStream_t s);
     void launch_prolong(const MasView &mas, const double *z0, double *z, cudaStream_t s);
+
+    // Several right-hand sides (groups of RHS_GROUP, interleaved vectors, state array of
+    // RHS_GROUP + 1 entries: one per right-hand side, then the group record). mas_multi.cu and
+    // mas_apply.cu; the MAS apply needs binary16 inverses.
+    void launch_spmv_g(int mode, const BankedView &A, const double *x, double *y, const double *b, PcgState *st,
+                       ReduceBuf red, int iter, int period, cudaStream_t s);
+    void launch_update_xr_g(const MasView &mas, double *x, double *r, const double *p, const double *Ap,
+                            PcgState *st, ReduceBuf red, int period, cudaStream_t s);
+    void launch_update_p_g(const MasView &mas, double *p, const double *z0, PcgState *st, int first, cudaStream_t s);
+    int launch_restrict_g(const MasView &mas, const double *r, const PcgState *grp, int period, cudaStream_t s);
+    int launch_coarse_levels_g(const MasView &mas, cudaStream_t s);
+    void launch_mas_apply_g(const MasView &mas, const double *r, double *z0, PcgState *st, ReduceBuf red,
+                            PcgConfig cfg, int mode, cudaStream_t s);
+    void prepare_kernels_g(int bd);
+    void launch_permute_in_g(int n, int bd, int V, int cols, const int *padded_of_block, const double *B, double *dst,
+                             size_t dst_len, cudaStream_t s);
+    void launch_permute_out_g(int n, int bd, int cols, const int *padded_of_block, const double *src, double *X,
+                              cudaStream_t s);
     // Set kernel attributes (large shared memory) for every variant used with this block size and
     // precision, so launches inside a CUDA graph capture never touch function attributes.
     void prepare_kernels(int bd, int storage);
@@ -393,7 +412,7 @@ namespace pmas
         DevBuf<double> inv_scale;
         DevBuf<double> rc, zc;
         DevBuf<int> flag;        // device error flag for the inverses
-        MasView view(double *rc_override = nullptr) const;
+        MasView view(double *rc_override = nullptr, double *zc_override = nullptr) const;
     };
 
     // first_iso_bank: first bank of the trailing isolated rows (banks if none / not trailing).

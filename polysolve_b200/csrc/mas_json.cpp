@@ -265,6 +265,11 @@ namespace pmas
                 out += v.b ? "true" : "false";
                 break;
             case Json::Number:
+                if (!std::isfinite(v.num))
+                {
+                    out += "null"; // JSON has no NaN / infinity
+                    break;
+                }
                 if (v.is_integer && std::fabs(v.num) < 9e15)
                     std::snprintf(buf, sizeof(buf), "%lld", (long long)v.num);
                 else

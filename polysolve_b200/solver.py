@@ -40,7 +40,8 @@ EXPORTED_SYMBOLS = [
     "mas_create", "mas_create_json", "mas_destroy", "mas_set_parameters", "mas_get_info", "mas_name",
     "mas_analyze_pattern", "mas_set_positions", "mas_factorize_csc", "mas_solve", "mas_solve_multi",
     "mas_solve_device", "mas_solve_batch", "mas_set_stream", "mas_spmv_dot_noalloc", "mas_last_error", "mas_get_sizes", "mas_get_ordering", "mas_order_blocks",
-    "mas_get_coarse_map", "mas_get_inverses", "mas_debug_spmv", "mas_debug_apply",
+    "mas_get_coarse_map", "mas_get_inverses", "mas_debug_spmv", "mas_debug_apply", "mas_debug_apply_multi",
+    "mas_debug_spmv_multi",
 ]
 
 
@@ -93,6 +94,8 @@ def library() -> ctypes.CDLL:
         L.mas_get_inverses.argtypes = [vp, vp, ctypes.c_size_t]
         L.mas_debug_spmv.argtypes = [vp, vp, vp, i]
         L.mas_debug_apply.argtypes = [vp, vp, vp, i]
+        L.mas_debug_apply_multi.argtypes = [vp, vp, vp, i]
+        L.mas_debug_spmv_multi.argtypes = [vp, vp, vp, i]
         L.mas_order_blocks.argtypes = [i, vp, vp, i, vp, ctypes.c_char_p, ip, ip]
         _LIB = L
     return _LIB
@@ -340,6 +343,19 @@ class Solver:
         z = np.empty_like(r)
         _check(library().mas_debug_apply(self._h, r.ctypes.data, z.ctypes.data, int(r.size)), self._h)
         return z
+
+    def debug_apply_multi(self, R_padded: np.ndarray) -> np.ndarray:
+        """R_padded: (padded length, 4) columns; returns M^-1 applied to each (several-RHS kernels)."""
+        r = np.ascontiguousarray(R_padded, dtype=np.float64)
+        z = np.empty_like(r)
+        _check(library().mas_debug_apply_multi(self._h, r.ctypes.data, z.ctypes.data, int(r.size)), self._h)
+        return z
+
+    def debug_spmv_multi(self, X_padded: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(X_padded, dtype=np.float64)
+        y = np.empty_like(x)
+        _check(library().mas_debug_spmv_multi(self._h, x.ctypes.data, y.ctypes.data, int(x.size)), self._h)
+        return y
 
 
 MASSolver = Solver
