@@ -962,6 +962,7 @@ struct mas_solver
                                        cudaMemcpyDeviceToHost, stream),
                        "download X");
             cuda_check(cudaStreamSynchronize(stream), "solve multi");
+            collect_profile();
         }
         solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
         iterations = rhs_iterations.empty() ? 0 : *std::max_element(rhs_iterations.begin(), rhs_iterations.end());
