@@ -535,6 +535,59 @@ namespace pmas
         }
     } // namespace
 
+    namespace
+    {
+        // Level-0 and coarse matrices assembled from the current values of A and inverted in the
+        // storage precision (the coarse space in M must match A's pattern).
+        void build_inverses(MasDevice &M, const BankedMatrix &A, const int *d_node_real, int storage, const int *coff,
+                            cudaStream_t s)
+        {
+            const int bd = A.bd, banks = A.banks;
+            const size_t S = (size_t)inv_stride(bd, storage);
+            if (storage != STORE_F64)
+                M.inv64.reset();
+            if (storage != STORE_F32)
+                M.inv32.reset();
+            if (storage != STORE_F16)
+                M.inv16.reset();
+            M.storage = storage;
+            cuda_check(cudaMemsetAsync(M.flag.get(), 0, sizeof(int), s), "memset");
+            if (storage == STORE_F64)
+                M.inv64.alloc(S * M.total_mats, "MAS coarse_matrices");
+            else if (storage == STORE_F16)
+                M.inv16.alloc(S * M.total_mats, "MAS coarse_matrices");
+            else
+                M.inv32.alloc(S * M.total_mats, "MAS coarse_matrices");
+            M.inv_scale.alloc(M.total_mats > 0 ? M.total_mats : 1, "MAS coarse_matrices scales");
+            M.identity.alloc(M.total_coarse > 0 ? M.total_coarse : 1, "MAS coarse_matrices identity");
+            cuda_check(cudaMemsetAsync(M.identity.get(), 0, M.identity.bytes(), s), "memset");
+            auto run = [&](auto *out) {
+                using Out = std::remove_pointer_t<decltype(out)>;
+                auto per_bd = [&](auto bdc) {
+                    constexpr int BD = decltype(bdc)::value;
+                    assemble_and_invert<BD, Out>(M, A, d_node_real, out, coff, s);
+                };
+                if (bd == 1)
+                    per_bd(std::integral_constant<int, 1>{});
+                else if (bd == 2)
+                    per_bd(std::integral_constant<int, 2>{});
+                else
+                    per_bd(std::integral_constant<int, 3>{});
+            };
+            if (storage == STORE_F64)
+                run(M.inv64.get());
+            else if (storage == STORE_F16)
+                run(reinterpret_cast<__half *>(M.inv16.get()));
+            else
+                run(M.inv32.get());
+            int h_flag = 0;
+            cuda_check(cudaMemcpyAsync(&h_flag, M.flag.get(), sizeof(int), cudaMemcpyDeviceToHost, s), "flag");
+            cuda_check(cudaStreamSynchronize(s), "mas build");
+            if (h_flag)
+                throw Error(ERR_INVERSE, "[MAS] MAS packed inverse failed.");
+        }
+    } // namespace
+
     void build_mas(MasDevice &M, const BankedMatrix &A, const int *d_node_real, int storage, int first_iso_bank,
                    cudaStream_t s)
     {
@@ -752,43 +805,13 @@ namespace pmas
         cuda_check(cudaMemsetAsync(M.rc.get(), 0, M.rc.bytes(), s), "memset");
         cuda_check(cudaMemsetAsync(M.zc.get(), 0, M.zc.bytes(), s), "memset");
 
-        // --- matrices
-        const size_t S = (size_t)inv_stride(bd, storage);
-        M.inv64.reset();
-        M.inv32.reset();
-        M.inv16.reset();
-        if (storage == STORE_F64)
-            M.inv64.alloc(S * M.total_mats, "MAS coarse_matrices");
-        else if (storage == STORE_F16)
-            M.inv16.alloc(S * M.total_mats, "MAS coarse_matrices");
-        else
-            M.inv32.alloc(S * M.total_mats, "MAS coarse_matrices");
-        M.inv_scale.alloc(M.total_mats > 0 ? M.total_mats : 1, "MAS coarse_matrices scales");
-        M.identity.alloc(M.total_coarse > 0 ? M.total_coarse : 1, "MAS coarse_matrices identity");
-        cuda_check(cudaMemsetAsync(M.identity.get(), 0, M.identity.bytes(), s), "memset");
-        auto run = [&](auto *out) {
-            using Out = std::remove_pointer_t<decltype(out)>;
-            auto per_bd = [&](auto bdc) {
-                constexpr int BD = decltype(bdc)::value;
-                assemble_and_invert<BD, Out>(M, A, d_node_real, out, coff, s);
-            };
-            if (bd == 1)
-                per_bd(std::integral_constant<int, 1>{});
-            else if (bd == 2)
-                per_bd(std::integral_constant<int, 2>{});
-            else
-                per_bd(std::integral_constant<int, 3>{});
-        };
-        if (storage == STORE_F64)
-            run(M.inv64.get());
-        else if (storage == STORE_F16)
-            run(reinterpret_cast<__half *>(M.inv16.get()));
-        else
-            run(M.inv32.get());
-        int h_flag = 0;
-        cuda_check(cudaMemcpyAsync(&h_flag, M.flag.get(), sizeof(int), cudaMemcpyDeviceToHost, s), "flag");
-        cuda_check(cudaStreamSynchronize(s), "mas build");
-        if (h_flag)
-            throw Error(ERR_INVERSE, "[MAS] MAS packed inverse failed.");
+        build_inverses(M, A, d_node_real, storage, coff, s);
+    }
+
+    void refresh_mas_values(MasDevice &M, const BankedMatrix &A, const int *d_node_real, int storage, cudaStream_t s)
+    {
+        if (M.bd != A.bd || M.banks != A.banks || M.nodes != A.nodes)
+            throw Error(ERR_INVALID, "[MAS] internal: refresh with a different pattern");
+        build_inverses(M, A, d_node_real, storage, M.coff, s);
     }
 } // namespace pmas

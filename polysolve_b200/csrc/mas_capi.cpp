@@ -228,9 +228,15 @@ struct mas_solver
     int status = MAS_STATUS_RUNNING;
     double rr0 = 0.0, rz0 = 0.0;
     double solve_ms = 0.0, factorize_ms = 0.0;
+    std::vector<std::pair<std::string, double>> factorize_phases; // host-clock ms per phase
+    DevBuf<double> refresh_vals; // CSC values staging kept across values-only refactorizations
     int launched_iterations = 0;
 
     std::vector<double> positions;
+    long long positions_version = 0;  // bumped by set_positions
+    long long ordered_version = -1;   // positions_version the current ordering was built from
+    std::string ordered_mode;         // the ordering parameter it was built with
+    int first_iso_bank_cached = 0;
 
     // Ordering / pattern state.
     int n = 0, V = 0, banks = 0, bd = 0;
@@ -398,6 +404,13 @@ struct mas_solver
     void factorize(int n_, const int *outer, const int *inner, const double *vals, long long nnz_)
     {
         auto t0 = std::chrono::steady_clock::now();
+        auto tp = t0;
+        factorize_phases.clear();
+        auto phase = [&](const char *name) {
+            const auto now = std::chrono::steady_clock::now();
+            factorize_phases.emplace_back(name, std::chrono::duration<double, std::milli>(now - tp).count());
+            tp = now;
+        };
         cuda_check(cudaSetDevice(device), "set device");
         if (n_ <= 0 || !outer || !inner || !vals)
             throw Error(ERR_INVALID, "[MAS] factorize: invalid matrix arguments.");
@@ -407,9 +420,17 @@ struct mas_solver
             throw Error(ERR_INVALID, "[MAS] A is too large. Non-zero number exceeding int32 max.");
         const int bd_ = p.block_dim;
         const int V_ = (n_ + bd_ - 1) / bd_;
-        const bool rebuild_order = !p.lazy || padded.size() != (size_t)V_ || bd_ != bd || n_ != n;
         const uint64_t h = pattern_hash(n_, outer, inner, nnz_);
-        const bool same_pattern = factorized && !rebuild_order && h == pattern && nnz_ == nnz && bd_ == A.bd;
+        // The ordering is a pure function of the pattern, the positions and the ordering
+        // parameter: it is rebuilt only when one of them changed (lazy_partitioning keeps it even
+        // then, as the reference does, MASSolver.cu:304-320).
+        const bool shape_same = factorized && padded.size() == (size_t)V_ && bd_ == bd && n_ == n;
+        const bool inputs_same = shape_same && h == pattern && nnz_ == nnz && positions_version == ordered_version &&
+                                 p.ordering == ordered_mode;
+        const bool rebuild_order = !(shape_same && (p.lazy || inputs_same));
+        const bool same_pattern = factorized && !rebuild_order && h == pattern && nnz_ == nnz && bd_ == A.bd &&
+                                  mas.storage == p.storage;
+        phase("pattern_check");
 
         if (rebuild_order)
         {
@@ -429,6 +450,8 @@ struct mas_solver
             else
                 padded = natural_padded(V_, &nb);
             ordering_used = mode;
+            ordered_version = positions_version;
+            ordered_mode = p.ordering;
             banks = nb;
             V = V_;
             n = n_;
@@ -444,10 +467,14 @@ struct mas_solver
                                        cudaMemcpyHostToDevice, stream),
                        "upload ordering");
             cuda_check(cudaStreamSynchronize(stream), "ordering");
+            phase("ordering");
         }
         factorized = false;
         {
-            DevBuf<double> d_vals;
+            DevBuf<double> local_vals;
+            DevBuf<double> &d_vals = same_pattern ? refresh_vals : local_vals;
+            if (!same_pattern)
+                refresh_vals.reset();
             d_vals.alloc(nnz_ > 0 ? nnz_ : 1, "MAS permuted_bsr input_csc");
             cuda_check(cudaMemcpyAsync(d_vals.get(), vals, sizeof(double) * nnz_, cudaMemcpyHostToDevice, stream),
                        "upload values");
@@ -472,10 +499,20 @@ struct mas_solver
                              stream);
             }
             cuda_check(cudaStreamSynchronize(stream), "matrix upload");
+            phase("matrix_upload");
         }
         nnz = nnz_;
         pattern = h;
 
+        if (same_pattern)
+        {
+            // Values only: the coarse space, buffers and captured graphs stay valid.
+            refresh_mas_values(mas, A, d_node_real.get(), p.storage, stream); // syncs, checks pivots
+            phase("mas_inverses");
+            factorized = true;
+            factorize_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+            return;
+        }
         // Trailing banks of isolated rows (no off-diagonal block): the coarse levels skip them.
         int first_iso_bank = banks;
         {
@@ -488,6 +525,7 @@ struct mas_solver
                     first_iso_bank = banks;
         }
         build_mas(mas, A, d_node_real.get(), p.storage, first_iso_bank, stream);
+        phase("mas_build");
         prepare_kernels(bd_, p.storage);
         if (p.storage == STORE_F16)
             prepare_kernels_g(bd_);
@@ -509,6 +547,7 @@ struct mas_solver
         cuda_check(cudaMemsetAsync(z.get(), 0, z.bytes(), stream), "memset");
         cuda_check(cudaMemsetAsync(Ap.get(), 0, Ap.bytes(), stream), "memset");
         cuda_check(cudaStreamSynchronize(stream), "factorize");
+        phase("buffers");
         factorized = true;
         factorize_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     }
@@ -1051,6 +1090,13 @@ struct mas_solver
         o.obj.emplace_back("ordering", str(ordering_used));
         o.obj.emplace_back("solve_ms", num(solve_ms, false));
         o.obj.emplace_back("factorize_ms", num(factorize_ms, false));
+        {
+            Json fp;
+            fp.type = Json::Object;
+            for (const auto &ph : factorize_phases)
+                fp.obj.emplace_back(ph.first, num(ph.second, false));
+            o.obj.emplace_back("factorize_phases_ms", fp);
+        }
         o.obj.emplace_back("launched_iterations", num(launched_iterations, true));
         o.obj.emplace_back("banks", num(banks, true));
         o.obj.emplace_back("coarse_levels", num(mas.level_num, true));
@@ -1251,6 +1297,7 @@ extern "C" int mas_set_positions(mas_solver *h, const double *xyz, int nverts)
         if (nverts < 0 || (nverts > 0 && !xyz))
             throw Error(ERR_INVALID, "[MAS] set_positions: invalid arguments.");
         h->positions.assign(xyz, xyz + (size_t)nverts * 3);
+        ++h->positions_version;
         h->padded.clear(); // a new geometry invalidates a lazily kept ordering
     });
 }

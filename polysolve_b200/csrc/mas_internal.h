@@ -418,6 +418,8 @@ namespace pmas
     // first_iso_bank: first bank of the trailing isolated rows (banks if none / not trailing).
     void build_mas(MasDevice &M, const BankedMatrix &A, const int *d_node_real, int storage, int first_iso_bank,
                    cudaStream_t s);
+    // Same pattern, new values: re-assemble and re-invert only (the coarse space is kept).
+    void refresh_mas_values(MasDevice &M, const BankedMatrix &A, const int *d_node_real, int storage, cudaStream_t s);
 
     // mas_pcg.cu: misc
     void launch_zero(double *p, size_t n, cudaStream_t s);
