@@ -88,14 +88,33 @@ int mas_set_positions(mas_solver *h, const double *xyz, int nverts);
 
 /* MASSolver::factorize(A) (MASSolver.cu:292-374): A as CSC host arrays outer[n+1], inner[nnz],
  * vals[nnz]. Builds the subdomain ordering, the permuted block matrix and the MAS
- * preconditioner on the device. With lazy_partitioning the ordering is reused while n is
- * unchanged; when the sparsity pattern is also unchanged only the values are re-scattered. */
+ * preconditioner on the device. The ordering is reused while the pattern, the positions and the
+ * ordering parameter are unchanged (with lazy_partitioning: while n is unchanged); with the
+ * same pattern only the values are re-scattered and the inverses rebuilt (the coarse space,
+ * buffers and CUDA graphs are kept). */
 int mas_factorize_csc(mas_solver *h, int n, const int *outer, const int *inner, const double *vals, int nnz);
 
 /* MASSolver::solve(b, x) (MASSolver.cu:376-409): host vectors of length n. With initial_guess
  * "zero" (the reference's behaviour, MASSolver.cu:395-398) x is output only; with "input" x is
  * also the starting guess. Synchronous. Non-convergence is not an error: see get_info. */
 int mas_solve(mas_solver *h, const double *b, double *x, int n);
+
+/* New: learned warm start for sequences of systems with one pattern (initial_guess
+ * "learned"). The solver keeps its last two solutions on the device; the next solve starts from
+ * the energy-minimising combination of x_{k-1}, x_{k-1} - x_{k-2} and a message-passing
+ * network's correction (falling back to x_{k-1}), computed on the GPU from b, the diagonal
+ * blocks and the kept solutions. block_dim 3 only. The reference always starts from x0 = 0
+ * (MASSolver.cu:395-398); its caller refactorizes and solves every Newton step
+ * (Newton.cpp:173-214).
+ * params: MAS_WS_PARAMS float32 in the .psws order (polysolve_b200/warmstart.py). */
+#define MAS_WS_FEATURES 16
+#define MAS_WS_HIDDEN 64
+#define MAS_WS_LAYERS 3
+#define MAS_WS_PARAMS 26051
+int mas_set_warm_start_model(mas_solver *h, const float *params, long long count);
+/* Forget the kept solutions (the next solve starts from zero). A factorization with a new
+ * pattern or ordering also forgets them. */
+int mas_reset_warm_start(mas_solver *h);
 
 /* New: nrhs independent right-hand sides, column-major B[n * nrhs] / X[n * nrhs]. */
 int mas_solve_multi(mas_solver *h, const double *B, double *X, int n, int nrhs);
@@ -168,6 +187,13 @@ int mas_debug_apply(mas_solver *h, const double *r, double *z, int len);
  * No reference counterpart. */
 int mas_debug_apply_multi(mas_solver *h, const double *rin, double *zout, int len);
 int mas_debug_spmv_multi(mas_solver *h, const double *xin, double *yout, int len);
+/* Test hook of the learned warm start: the prediction for caller-order b, x1 (= x_{k-1}) and
+ * x2 (= x_{k-2}) without a solve. Outputs (each may be NULL): c_out[n] the network's correction,
+ * x0_out[n] the starting guess, features_out[nverts * 16] the raw per-vertex features,
+ * state_out[21] = feature sums (5), Galerkin matrix and right-hand side (9), coefficients (3),
+ * energy of x0, energy of x1, fallback flag, kept basis vectors. */
+int mas_debug_warm_start(mas_solver *h, const double *b, const double *x1, const double *x2, double *c_out,
+                         double *x0_out, float *features_out, double *state_out);
 
 #ifdef __cplusplus
 }

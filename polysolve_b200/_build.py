@@ -40,6 +40,7 @@ CU_SOURCES = [
     "mas_pcg.cu",
     "mas_noalloc.cu",
     "mas_multi.cu",
+    "mas_warmstart.cu",
 ]
 CPP_SOURCES = ["mas_capi.cpp", "mas_ordering.cpp", "mas_json.cpp"]
 

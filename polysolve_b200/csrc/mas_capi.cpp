@@ -48,6 +48,7 @@ namespace
         int true_residual_period = 4;
         int check_period = 10;
         bool initial_guess_input = false;
+        bool initial_guess_learned = false; // x0 from the solver's own last two solutions
         bool polak_ribiere = false;
         std::string ordering = "auto";
         int poll_period = 10;
@@ -155,9 +156,10 @@ namespace
         if (auto *v = m.find("initial_guess"))
         {
             const std::string s = get_str(*v, "initial_guess");
-            if (s != "zero" && s != "input")
-                throw Error(ERR_INVALID, "[MAS] initial_guess must be \"zero\" or \"input\"");
+            if (s != "zero" && s != "input" && s != "learned")
+                throw Error(ERR_INVALID, "[MAS] initial_guess must be \"zero\", \"input\" or \"learned\"");
             q.initial_guess_input = (s == "input");
+            q.initial_guess_learned = (s == "learned");
         }
         if (auto *v = m.find("beta"))
         {
@@ -260,6 +262,27 @@ struct mas_solver
     DevBuf<PcgState> gst;
     cudaGraphExec_t ggraph[2] = {nullptr, nullptr};
     std::vector<std::pair<int, long long>> ggraph_counts[2];
+
+    // Learned warm start: the last two solutions (padded order), the network's weights and
+    // scratch, and the record of the last prediction.
+    DevBuf<double> hist[2];
+    int hist_newest = 0, hist_count = 0;
+    DevBuf<float> ws_params;
+    DevBuf<uint16_t> ws_wl; // bf16 bits of the layer weights
+    bool ws_loaded = false;
+    DevBuf<int> ws_diag;
+    DevBuf<float> ws_wslot, ws_feat;
+    DevBuf<uint16_t> ws_h0, ws_h1;
+    DevBuf<double> ws_c, ws_y1, ws_y2, ws_y3, ws_partials;
+    DevBuf<WsState> ws_state;
+    WsState *h_ws = nullptr; // pinned copy of the last prediction's record
+    bool ws_graph_valid = false;
+    bool ws_predicted = false; // the last solve's x0 came from the network pipeline
+    std::string x0_source = "zero";
+    cudaEvent_t ws_ev[2] = {nullptr, nullptr};
+    double warm_start_ms = 0.0;
+    bool keep_stats = false; // the warm start's launches belong to the next solve's statistics
+    bool in_multi = false;
     uint64_t ggraph_key = 0;
     bool ggraph_aligned = false;
     std::vector<int> rhs_iterations, rhs_status;
@@ -284,6 +307,11 @@ struct mas_solver
                 cudaGraphExecDestroy(g);
         if (h_st)
             cudaFreeHost(h_st);
+        if (h_ws)
+            cudaFreeHost(h_ws);
+        for (cudaEvent_t e : ws_ev)
+            if (e)
+                cudaEventDestroy(e);
         if (own_stream)
             cudaStreamDestroy(own_stream);
     }
@@ -406,6 +434,7 @@ struct mas_solver
         auto t0 = std::chrono::steady_clock::now();
         auto tp = t0;
         factorize_phases.clear();
+        ws_graph_valid = false; // the neighbour weights follow the values
         auto phase = [&](const char *name) {
             const auto now = std::chrono::steady_clock::now();
             factorize_phases.emplace_back(name, std::chrono::duration<double, std::milli>(now - tp).count());
@@ -526,6 +555,7 @@ struct mas_solver
         }
         build_mas(mas, A, d_node_real.get(), p.storage, first_iso_bank, stream);
         phase("mas_build");
+        hist_count = 0; // a new pattern or ordering: the kept solutions no longer apply
         prepare_kernels(bd_, p.storage);
         if (p.storage == STORE_F16)
             prepare_kernels_g(bd_);
@@ -688,8 +718,10 @@ struct mas_solver
         cuda_check(cudaEventCreate(&e1), "event");
         cuda_check(cudaEventRecord(e0, stream), "event");
         ev_origin = e0;
-        for (auto &ks : kstats) // per-solve kernel statistics
-            ks.second = KStat{};
+        if (!keep_stats) // per-solve kernel statistics
+            for (auto &ks : kstats)
+                ks.second = KStat{};
+        keep_stats = false;
         launch_pcg_init_state(S, stream);
         // r = b - A x, rr0, the level-0 restriction of r, then z = M^-1 r
         run("spmv_residual", 1, [&] { launch_spmv(SPMV_RESIDUAL, Av, x.get(), r.get(), b.get(), S, red(), 0, 0, stream); });
@@ -780,6 +812,225 @@ struct mas_solver
             run("permute_in", 2, [&] { launch_permute_in(n, bd, V, d_padded.get(), d_src_x, x.get(), len, stream); });
         else
             cuda_check(cudaMemsetAsync(x.get(), 0, x.bytes(), stream), "memset");
+    }
+
+    // ---- Learned warm start ----------------------------------------------------------------
+    void set_warm_start_model(const float *prm, long long count)
+    {
+        cuda_check(cudaSetDevice(device), "set device");
+        if (!prm || count != WS_PARAMS)
+            throw Error(ERR_INVALID, "[MAS] warm start model: expected " + std::to_string(WS_PARAMS) +
+                                         " float32 parameters");
+        for (long long i = 0; i < count; ++i)
+            if (!std::isfinite(prm[i]))
+                throw Error(ERR_INVALID, "[MAS] warm start model: non-finite parameter");
+        // Layer weights to bf16 (round to nearest even) for the tensor-core products.
+        std::vector<uint16_t> wl((size_t)WS_LAYERS * WS_LAYER_WEIGHTS);
+        const int per_layer = WS_HIDDEN * 2 * WS_HIDDEN + WS_HIDDEN;
+        for (int l = 0; l < WS_LAYERS; ++l)
+        {
+            const float *src = prm + WS_HIDDEN * WS_FEATURES + WS_HIDDEN + (size_t)l * per_layer;
+            for (int i = 0; i < WS_LAYER_WEIGHTS; ++i)
+            {
+                uint32_t u;
+                std::memcpy(&u, src + i, 4);
+                u += 0x7FFFu + ((u >> 16) & 1u);
+                wl[(size_t)l * WS_LAYER_WEIGHTS + i] = (uint16_t)(u >> 16);
+            }
+        }
+        ws_params.alloc(WS_PARAMS, "warm start model");
+        ws_wl.alloc(wl.size(), "warm start model");
+        cuda_check(cudaMemcpyAsync(ws_params.get(), prm, sizeof(float) * WS_PARAMS, cudaMemcpyHostToDevice, stream),
+                   "upload model");
+        cuda_check(cudaMemcpyAsync(ws_wl.get(), wl.data(), sizeof(uint16_t) * wl.size(), cudaMemcpyHostToDevice,
+                                   stream),
+                   "upload model");
+        cuda_check(cudaStreamSynchronize(stream), "upload model");
+        ws_loaded = true;
+    }
+
+    WsBuffers ws_buffers()
+    {
+        const size_t nodes = (size_t)banks * 32;
+        const size_t len = nodes * 3;
+        ws_diag.alloc(nodes, "warm start scratch");
+        ws_wslot.alloc((size_t)std::max<long long>(A.slots, 1) * 32, "warm start scratch");
+        ws_feat.alloc(nodes * WS_FEATURES, "warm start scratch");
+        ws_h0.alloc(nodes * WS_HIDDEN, "warm start scratch");
+        ws_h1.alloc(nodes * WS_HIDDEN, "warm start scratch");
+        for (DevBuf<double> *v : {&ws_c, &ws_y1, &ws_y2, &ws_y3})
+            v->alloc(len, "warm start scratch");
+        const int capacity = std::max((int)((nodes + 255) / 256), ws_reduce_ctas());
+        if (ws_partials.n < (size_t)capacity * 9)
+            ws_partials.alloc((size_t)capacity * 9, "warm start scratch");
+        if (!ws_state.get())
+        {
+            ws_state.alloc(1, "warm start scratch");
+            cuda_check(cudaMemsetAsync(ws_state.get(), 0, sizeof(WsState), stream), "memset");
+        }
+        if (!h_ws)
+            cuda_check(cudaMallocHost(&h_ws, sizeof(WsState)), "pinned warm start record");
+        if (!ws_ev[0])
+        {
+            cuda_check(cudaEventCreate(&ws_ev[0]), "event");
+            cuda_check(cudaEventCreate(&ws_ev[1]), "event");
+        }
+        WsBuffers w;
+        w.params = ws_params.get();
+        w.wl = ws_wl.get();
+        w.diag_slot = ws_diag.get();
+        w.wslot = ws_wslot.get();
+        w.feat = ws_feat.get();
+        w.h[0] = ws_h0.get();
+        w.h[1] = ws_h1.get();
+        w.c = ws_c.get();
+        w.y1 = ws_y1.get();
+        w.y2 = ws_y2.get();
+        w.y3 = ws_y3.get();
+        w.st = ws_state.get();
+        w.partials = ws_partials.get();
+        w.capacity = (int)(ws_partials.n / 9);
+        return w;
+    }
+
+    bool learned_active() const { return p.initial_guess_learned && !in_multi; }
+
+    // x (padded order) for the next solve of a sequence: zero, the last solution, or the
+    // network's prediction combined with the last two solutions (b already loaded).
+    void warm_start_guess()
+    {
+        ws_predicted = false;
+        warm_start_ms = 0.0;
+        if (hist_count == 0)
+        {
+            cuda_check(cudaMemsetAsync(x.get(), 0, x.bytes(), stream), "memset");
+            x0_source = "zero";
+            return;
+        }
+        const double *x1 = hist[hist_newest].get();
+        if (hist_count < 2 || !ws_loaded || bd != 3)
+        {
+            cuda_check(cudaMemcpyAsync(x.get(), x1, x.bytes(), cudaMemcpyDeviceToDevice, stream), "copy x0");
+            x0_source = "previous";
+            return;
+        }
+        const double *x2 = hist[hist_newest ^ 1].get();
+        for (auto &ks : kstats)
+            ks.second = KStat{};
+        keep_stats = true;
+        WsBuffers w = ws_buffers();
+        cuda_check(cudaEventRecord(ws_ev[0], stream), "event");
+        ws_pipeline(w, x1, x2);
+        cuda_check(cudaEventRecord(ws_ev[1], stream), "event");
+        cuda_check(cudaMemcpyAsync(h_ws, ws_state.get(), sizeof(WsState), cudaMemcpyDeviceToHost, stream),
+                   "warm start record");
+        ws_predicted = true;
+        x0_source = "learned";
+    }
+
+    // The prediction: A x1, A x2, the network, A c, the Galerkin combination into x.
+    void ws_pipeline(const WsBuffers &w, const double *x1, const double *x2)
+    {
+        const size_t len = (size_t)banks * 32 * bd;
+        const BankedView Av = A.view();
+        if (!ws_graph_valid)
+        {
+            run("ws_graph", 1, [&] { launch_ws_graph(Av, w, stream); });
+            ws_graph_valid = true;
+        }
+        run("spmv_plain", 2, [&] {
+            launch_spmv(SPMV_PLAIN, Av, x1, w.y1, nullptr, nullptr, red(), 0, 0, stream);
+            launch_spmv(SPMV_PLAIN, Av, x2, w.y2, nullptr, nullptr, red(), 0, 0, stream);
+        });
+        run("ws_network", 0, [&] { return launch_ws_network(Av, w, b.get(), x1, x2, stream); });
+        run("spmv_plain", 1, [&] { launch_spmv(SPMV_PLAIN, Av, w.c, w.y3, nullptr, nullptr, red(), 0, 0, stream); });
+        run("ws_combine", 0, [&] { return launch_ws_combine(w, b.get(), x1, x2, x.get(), len, stream); });
+    }
+
+    // After a solve: keep x as the newest solution; read the prediction's record and time.
+    void finish_warm_start()
+    {
+        if (ws_predicted)
+        {
+            cuda_check(cudaStreamSynchronize(stream), "warm start");
+            float ms = 0.f;
+            cuda_check(cudaEventElapsedTime(&ms, ws_ev[0], ws_ev[1]), "event time");
+            warm_start_ms = ms;
+            if (h_ws->fallback)
+                x0_source = "previous (fallback)";
+        }
+        const size_t len = (size_t)banks * 32 * bd;
+        hist[0].alloc(len, "warm start history");
+        hist[1].alloc(len, "warm start history");
+        if (hist_count > 0)
+            hist_newest ^= 1;
+        cuda_check(cudaMemcpyAsync(hist[hist_newest].get(), x.get(), x.bytes(), cudaMemcpyDeviceToDevice, stream),
+                   "keep solution");
+        hist_count = std::min(hist_count + 1, 2);
+    }
+
+    // Tests: the prediction for caller-order b, x1, x2 without a solve; outputs in caller order
+    // (c, x0: n values; features: V * 16; state: sums 5, gram 9, coef 3, energy, energy of x1,
+    // fallback, rank).
+    void debug_warm_start(const double *hb, const double *hx1, const double *hx2, double *hc, double *hx0,
+                          float *hfeat, double *hstate)
+    {
+        cuda_check(cudaSetDevice(device), "set device");
+        require_factorized(n);
+        if (!ws_loaded || bd != 3)
+            throw Error(ERR_INVALID, "[MAS] warm start: no model loaded or block_dim is not 3");
+        if (!hb || !hx1 || !hx2)
+            throw Error(ERR_INVALID, "[MAS] warm start: null vector");
+        const size_t len = (size_t)banks * 32 * bd;
+        DevBuf<double> d1, d2;
+        d1.alloc(len, "debug");
+        d2.alloc(len, "debug");
+        const double *src[3] = {hb, hx1, hx2};
+        double *dst[3] = {b.get(), d1.get(), d2.get()};
+        for (int i = 0; i < 3; ++i)
+        {
+            cuda_check(cudaMemcpyAsync(io.get(), src[i], sizeof(double) * n, cudaMemcpyHostToDevice, stream), "upload");
+            launch_permute_in(n, bd, V, d_padded.get(), io.get(), dst[i], len, stream);
+        }
+        WsBuffers w = ws_buffers();
+        ws_pipeline(w, d1.get(), d2.get());
+        if (hc)
+        {
+            launch_permute_out(n, bd, V, d_padded.get(), w.c, io.get(), stream);
+            cuda_check(cudaMemcpyAsync(hc, io.get(), sizeof(double) * n, cudaMemcpyDeviceToHost, stream), "download");
+            cuda_check(cudaStreamSynchronize(stream), "debug warm start");
+        }
+        if (hx0)
+        {
+            launch_permute_out(n, bd, V, d_padded.get(), x.get(), io.get(), stream);
+            cuda_check(cudaMemcpyAsync(hx0, io.get(), sizeof(double) * n, cudaMemcpyDeviceToHost, stream), "download");
+            cuda_check(cudaStreamSynchronize(stream), "debug warm start");
+        }
+        if (hfeat)
+        {
+            DevBuf<float> f;
+            f.alloc((size_t)V * WS_FEATURES, "debug");
+            launch_ws_features_out(V, d_padded.get(), w.feat, f.get(), stream);
+            cuda_check(cudaMemcpyAsync(hfeat, f.get(), f.bytes(), cudaMemcpyDeviceToHost, stream), "download");
+            cuda_check(cudaStreamSynchronize(stream), "debug warm start");
+        }
+        WsState hs;
+        cuda_check(cudaMemcpyAsync(&hs, ws_state.get(), sizeof(WsState), cudaMemcpyDeviceToHost, stream), "download");
+        cuda_check(cudaStreamSynchronize(stream), "debug warm start");
+        if (hstate)
+        {
+            int k = 0;
+            for (double v : hs.sums)
+                hstate[k++] = v;
+            for (double v : hs.gram)
+                hstate[k++] = v;
+            for (double v : hs.coef)
+                hstate[k++] = v;
+            hstate[k++] = hs.energy;
+            hstate[k++] = hs.energy_prev;
+            hstate[k++] = hs.fallback;
+            hstate[k++] = hs.rank;
+        }
     }
 
     // ---- Several right-hand sides at once (RHS_GROUP per group, binary16 inverses). ----------
@@ -973,8 +1224,19 @@ struct mas_solver
         require_factorized(len);
         if (!multi_supported())
         {
-            for (int c = 0; c < nrhs; ++c)
-                solve(hB + (size_t)c * n, hX + (size_t)c * n, n);
+            // Each column from x0 = 0 (or the caller's x); the warm-start history is untouched.
+            in_multi = true;
+            try
+            {
+                for (int c = 0; c < nrhs; ++c)
+                    solve(hB + (size_t)c * n, hX + (size_t)c * n, n);
+            }
+            catch (...)
+            {
+                in_multi = false;
+                throw;
+            }
+            in_multi = false;
             return;
         }
         alloc_multi();
@@ -1024,16 +1286,26 @@ struct mas_solver
         cuda_check(cudaMemcpyAsync(io.get(), hb, sizeof(double) * n, cudaMemcpyHostToDevice, stream), "upload b");
         const size_t blen = (size_t)banks * 32 * bd;
         run("permute_in", 2, [&] { launch_permute_in(n, bd, V, d_padded.get(), io.get(), b.get(), blen, stream); });
-        if (p.initial_guess_input)
-        {
-            cuda_check(cudaMemcpyAsync(io.get(), hx, sizeof(double) * n, cudaMemcpyHostToDevice, stream), "upload x");
-            run("permute_in", 2, [&] { launch_permute_in(n, bd, V, d_padded.get(), io.get(), x.get(), blen, stream); });
-        }
+        if (learned_active())
+            warm_start_guess();
         else
-            cuda_check(cudaMemsetAsync(x.get(), 0, x.bytes(), stream), "memset");
+        {
+            if (p.initial_guess_input)
+            {
+                cuda_check(cudaMemcpyAsync(io.get(), hx, sizeof(double) * n, cudaMemcpyHostToDevice, stream),
+                           "upload x");
+                run("permute_in", 2,
+                    [&] { launch_permute_in(n, bd, V, d_padded.get(), io.get(), x.get(), blen, stream); });
+            }
+            else
+                cuda_check(cudaMemsetAsync(x.get(), 0, x.bytes(), stream), "memset");
+            x0_source = p.initial_guess_input ? "input" : "zero";
+        }
         pcg();
         run("permute_out", 1, [&] { launch_permute_out(n, bd, V, d_padded.get(), x.get(), io.get(), stream); });
         cuda_check(cudaMemcpyAsync(hx, io.get(), sizeof(double) * n, cudaMemcpyDeviceToHost, stream), "download x");
+        if (learned_active())
+            finish_warm_start();
         cuda_check(cudaStreamSynchronize(stream), "solve");
     }
 
@@ -1042,9 +1314,15 @@ struct mas_solver
         cuda_check(cudaSetDevice(device), "set device");
         require_factorized(len);
         last_multi = false;
-        load_rhs_device(d_b, d_x);
+        load_rhs_device(d_b, learned_active() ? nullptr : d_x);
+        if (learned_active())
+            warm_start_guess();
+        else
+            x0_source = p.initial_guess_input ? "input" : "zero";
         pcg();
         run("permute_out", 1, [&] { launch_permute_out(n, bd, V, d_padded.get(), x.get(), d_x, stream); });
+        if (learned_active())
+            finish_warm_start();
         cuda_check(cudaStreamSynchronize(stream), "solve");
     }
 
@@ -1063,6 +1341,12 @@ struct mas_solver
             Json j;
             j.type = Json::String;
             j.str = s;
+            return j;
+        };
+        auto boolean = [](bool v) {
+            Json j;
+            j.type = Json::Bool;
+            j.b = v;
             return j;
         };
         if (last_multi)
@@ -1086,7 +1370,26 @@ struct mas_solver
         o.obj.emplace_back("relative_residual", num(ref > 0 ? residual_norm / ref : 0.0, false));
         o.obj.emplace_back("precision",
                            str(p.storage == STORE_F64 ? "fp64" : (p.storage == STORE_F32 ? "fp32" : "fp16")));
-        o.obj.emplace_back("x0_source", str(p.initial_guess_input ? "input" : "zero"));
+        o.obj.emplace_back("x0_source", str(x0_source));
+        if (p.initial_guess_learned)
+        {
+            Json ws, cf;
+            ws.type = Json::Object;
+            cf.type = Json::Array;
+            const bool have = ws_predicted && h_ws;
+            for (int i = 0; i < 3; ++i)
+                cf.arr.push_back(num(have ? h_ws->coef[i] : 0.0, false));
+            ws.obj.emplace_back("model_loaded", boolean(ws_loaded));
+            ws.obj.emplace_back("history", num(hist_count, true));
+            ws.obj.emplace_back("predicted", boolean(have));
+            ws.obj.emplace_back("coefficients", cf);
+            ws.obj.emplace_back("energy", num(have ? h_ws->energy : 0.0, false));
+            ws.obj.emplace_back("energy_previous", num(have ? h_ws->energy_prev : 0.0, false));
+            ws.obj.emplace_back("fallback", boolean(have && h_ws->fallback));
+            ws.obj.emplace_back("rank", num(have ? h_ws->rank : 0, true));
+            ws.obj.emplace_back("ms", num(warm_start_ms, false));
+            o.obj.emplace_back("warm_start", ws);
+        }
         o.obj.emplace_back("ordering", str(ordering_used));
         o.obj.emplace_back("solve_ms", num(solve_ms, false));
         o.obj.emplace_back("factorize_ms", num(factorize_ms, false));
@@ -1300,6 +1603,28 @@ extern "C" int mas_set_positions(mas_solver *h, const double *xyz, int nverts)
         ++h->positions_version;
         h->padded.clear(); // a new geometry invalidates a lazily kept ordering
     });
+}
+
+extern "C" int mas_set_warm_start_model(mas_solver *h, const float *params, long long count)
+{
+    if (!h)
+        return MAS_ERR_INVALID;
+    return guarded(h, [&] { h->set_warm_start_model(params, count); });
+}
+
+extern "C" int mas_reset_warm_start(mas_solver *h)
+{
+    if (!h)
+        return MAS_ERR_INVALID;
+    return guarded(h, [&] { h->hist_count = 0; });
+}
+
+extern "C" int mas_debug_warm_start(mas_solver *h, const double *b, const double *x1, const double *x2, double *c_out,
+                                    double *x0_out, float *features_out, double *state_out)
+{
+    if (!h)
+        return MAS_ERR_INVALID;
+    return guarded(h, [&] { h->debug_warm_start(b, x1, x2, c_out, x0_out, features_out, state_out); });
 }
 
 extern "C" int mas_factorize_csc(mas_solver *h, int n, const int *outer, const int *inner, const double *vals, int nnz)

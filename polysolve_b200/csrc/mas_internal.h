@@ -424,6 +424,55 @@ namespace pmas
     // mas_pcg.cu: misc
     void launch_zero(double *p, size_t n, cudaStream_t s);
 
+    // ---------------------------------------------------------------------------------------
+    // mas_warmstart.cu: the learned starting guess for a sequence of systems (same pattern):
+    // a message-passing network over the vertex graph predicts a correction c of the
+    // extrapolated guess 2 x1 - x2 from the residual, the diagonal blocks and the last step;
+    // x0 is the energy-minimising combination of x1, x1 - x2 and c (x1 if that is not lower).
+    // Block size 3 only (three displacement components per vertex).
+    // ---------------------------------------------------------------------------------------
+    constexpr int WS_FEATURES = 16, WS_HIDDEN = 64, WS_LAYERS = 3;
+    constexpr int WS_PARAMS = WS_HIDDEN * WS_FEATURES + WS_HIDDEN +
+                              WS_LAYERS * (WS_HIDDEN * 2 * WS_HIDDEN + WS_HIDDEN) + 3 * WS_HIDDEN + 3;
+    constexpr int WS_LAYER_WEIGHTS = WS_HIDDEN * 2 * WS_HIDDEN; // bf16 values of one W_l
+
+    struct WsState
+    {
+        double sums[5];  // sum over real vertices of |q|^2, |v|^2, |p|^2, log trace, count
+        double gram[9];  // G11 G12 G13 G22 G23 G33 (v_i . A v_j) and g1 g2 g3 (v_i . b)
+        double coef[3];  // x0 = coef0 x1 + coef1 (x1 - x2) + coef2 c
+        double energy, energy_prev; // 1/2 x.Ax - x.b of x0 and of x1
+        int fallback;    // 1: x0 = x1 (the combination was degenerate or not lower)
+        int rank;        // basis vectors kept by the Galerkin solve
+        unsigned counter[2];
+    };
+
+    struct WsBuffers
+    {
+        const float *params;   // WS_PARAMS float32 (the .psws layout)
+        const uint16_t *wl;    // WS_LAYERS * WS_LAYER_WEIGHTS bf16 bits of the W_l
+        int *diag_slot;        // nodes: slot of the diagonal block in the node's row (-1: none)
+        float *wslot;          // slots * 32: neighbour weight of each stored block
+        float *feat;           // nodes * WS_FEATURES raw features
+        uint16_t *h[2];        // nodes * WS_HIDDEN bf16 hidden states (ping-pong)
+        double *c, *y1, *y2, *y3; // correction, A x1, A x2, A c (padded order, nodes * 3)
+        WsState *st;
+        double *partials;      // 9 * capacity
+        int capacity;          // CTAs of the reduced launches
+    };
+
+    // Neighbour weights and diagonal slots of the current values (once per factorization).
+    void launch_ws_graph(const BankedView &A, const WsBuffers &w, cudaStream_t s);
+    // Features .. correction c (needs y1 = A x1 and y2 = A x2 already in w). Returns kernels.
+    int launch_ws_network(const BankedView &A, const WsBuffers &w, const double *b, const double *x1,
+                          const double *x2, cudaStream_t s);
+    // Galerkin combination into x (needs w.y3 = A c). Returns kernels.
+    int launch_ws_combine(const WsBuffers &w, const double *b, const double *x1, const double *x2, double *x,
+                          size_t len, cudaStream_t s);
+    int ws_reduce_ctas();
+    // Features of the vertices in caller order (tests): out[v * 16 + f] = feat[padded[v] * 16 + f].
+    void launch_ws_features_out(int V, const int *padded_of_block, const float *feat, float *out, cudaStream_t s);
+
     // mas_noalloc.cu: y = A x and *dot = x . y with the reduction scratch in a static device array
     // (no allocation). Throws Error(ERR_INVALID) beyond noalloc_max_banks() banks.
     void launch_spmv_dot_noalloc(const BankedView &A, const double *x, double *y, double *dot, cudaStream_t s);

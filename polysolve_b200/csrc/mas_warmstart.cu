@@ -1,0 +1,637 @@
+// Learned starting guess for a sequence of systems with one pattern (sm_100a).
+//
+// The reference starts every PCG solve from x0 = 0 (MASSolver.cu:395-398) while its caller
+// (nonlinear::Newton, Newton.cpp:173-214) solves a matrix of the same pattern with new values at
+// every step. Here the solver keeps the last two solutions x1, x2 on the device and predicts x0:
+//
+//   k_ws_graph      once per factorization: each stored block's neighbour weight
+//                   ||A_ij||_F / sum_{j' != i} ||A_ij'||_F and the slot of the diagonal block.
+//   (SpMV x2)       y1 = A x1, y2 = A x2 (the plain SpMV kernel).
+//   k_ws_features   per vertex: q = D^-1 r_e (r_e = b - A (2 x1 - x2)), v = x1 - x2, p = D^-1 b,
+//                   the diagonal block scaled by trace / 3, log trace; the sums the
+//                   normalisation needs (deterministic grid reduction).
+//   k_ws_input      h = relu(W_in f + b_in) with the normalised features (FP32, BF16 out).
+//   k_ws_layer x3   m = sum_j w_ij h_j (gathered from L2 into shared memory), then
+//                   h += relu(W_l [h ; m] + b_l) on the tensor cores: BF16 mma.sync m16n8k16
+//                   with FP32 accumulation, 64 vertices x 64 outputs x K = 128 per CTA.
+//   k_ws_output     c = s_q (W_out h + b_out) (FP32 weights, FP64 out).
+//   (SpMV)          y3 = A c.
+//   k_ws_gram       the 3 x 3 Galerkin system of the basis {x1, x1 - x2, c} and its right-hand
+//                   side (9 dots, deterministic); the last CTA solves it with a pivoted
+//                   Cholesky that drops dependent vectors and falls back to x1 unless the
+//                   energy 1/2 x.Ax - x.b drops below that of x1.
+//   k_ws_combine    x0 = coef0 x1 + coef1 (x1 - x2) + coef2 c.
+//
+// All vectors are in the solver's padded (subdomain) order; nodes without a row (padding) get
+// zero features, zero hidden states and c = 0. The work is small next to a solve: at 680 K DOF
+// the three layers move about 30 MB of hidden states each (the gathers hit L2) and do
+// 3 x 2 x 227 K x 64 x 128 = 11 GFLOP on the tensor pipe.
+
+#include <cuda_bf16.h>
+
+#include "mas_common.cuh"
+
+namespace pmas
+{
+    namespace
+    {
+        constexpr int F = WS_FEATURES;
+        constexpr int H = WS_HIDDEN;
+        constexpr int WT = 256;         // threads of the per-vertex kernels
+        constexpr int TILE = 64;        // vertices per CTA of a layer
+        constexpr int LT = 128;         // threads of a layer CTA (4 warps x 16 vertices)
+        constexpr int TS = 2 * H + 8;   // shared row stride (bf16): 272 B, conflict-free ldmatrix
+
+        // Parameter offsets in the flat float32 vector (the .psws layout).
+        constexpr int OFF_WIN = 0;
+        constexpr int OFF_BIN = OFF_WIN + H * F;
+        __host__ __device__ constexpr int off_layer(int l) { return OFF_BIN + H + l * (H * 2 * H + H); }
+        constexpr int OFF_WOUT = off_layer(WS_LAYERS);
+        constexpr int OFF_BOUT = OFF_WOUT + 3 * H;
+        static_assert(OFF_BOUT + 3 == WS_PARAMS, "parameter layout");
+
+        __device__ __forceinline__ double block_entry(const BankedView &A, long long slot, int lane, int q)
+        {
+            return A.vals[banked_value_index(slot, lane, q, 3)];
+        }
+
+        __device__ __forceinline__ double block_fro(const BankedView &A, long long slot, int lane)
+        {
+            double s = 0.0;
+#pragma unroll
+            for (int q = 0; q < 9; ++q)
+            {
+                const double v = block_entry(A, slot, lane, q);
+                s = fma(v, v, s);
+            }
+            return sqrt(s);
+        }
+
+        // One thread per node (lanes of a warp = the 32 nodes of a bank: coalesced slot reads).
+        __global__ void __launch_bounds__(WT) k_ws_graph(BankedView A, int *__restrict__ diag_slot,
+                                                         float *__restrict__ wslot)
+        {
+            const int u = blockIdx.x * WT + threadIdx.x;
+            if (u >= A.banks * 32)
+                return;
+            const int bank = u >> 5, lane = u & 31;
+            const long long s0 = A.slice[bank];
+            const int len = A.rowlen[u];
+            double tot = 0.0;
+            int dslot = -1;
+            for (int k = 0; k < len; ++k)
+            {
+                const int col = A.cols[(s0 + k) * 32 + lane];
+                if (col == u)
+                    dslot = k;
+                else
+                    tot += block_fro(A, s0 + k, lane);
+            }
+            for (int k = 0; k < len; ++k)
+            {
+                const int col = A.cols[(s0 + k) * 32 + lane];
+                const float w = (col == u || !(tot > 0.0)) ? 0.f : (float)(block_fro(A, s0 + k, lane) / tot);
+                wslot[(s0 + k) * 32 + lane] = w;
+            }
+            diag_slot[u] = dslot;
+        }
+
+        // 3 x 3 inverse by cofactors; false if singular or not finite.
+        __device__ __forceinline__ bool inv3(const double (&d)[9], double (&o)[9])
+        {
+            const double c00 = d[4] * d[8] - d[5] * d[7];
+            const double c01 = d[5] * d[6] - d[3] * d[8];
+            const double c02 = d[3] * d[7] - d[4] * d[6];
+            const double det = d[0] * c00 + d[1] * c01 + d[2] * c02;
+            if (!(fabs(det) > 0.0) || !isfinite(det))
+                return false;
+            const double r = 1.0 / det;
+            o[0] = c00 * r;
+            o[1] = (d[2] * d[7] - d[1] * d[8]) * r;
+            o[2] = (d[1] * d[5] - d[2] * d[4]) * r;
+            o[3] = c01 * r;
+            o[4] = (d[0] * d[8] - d[2] * d[6]) * r;
+            o[5] = (d[2] * d[3] - d[0] * d[5]) * r;
+            o[6] = c02 * r;
+            o[7] = (d[1] * d[6] - d[0] * d[7]) * r;
+            o[8] = (d[0] * d[4] - d[1] * d[3]) * r;
+            return true;
+        }
+
+        __global__ void __launch_bounds__(WT)
+            k_ws_features(BankedView A, const int *__restrict__ diag_slot, const double *__restrict__ b,
+                          const double *__restrict__ x1, const double *__restrict__ x2,
+                          const double *__restrict__ y1, const double *__restrict__ y2, float *__restrict__ feat,
+                          WsState *ws, double *partials)
+        {
+            const int u = blockIdx.x * WT + threadIdx.x;
+            double sums[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+            if (u < A.banks * 32)
+            {
+                float f[F];
+#pragma unroll
+                for (int i = 0; i < F; ++i)
+                    f[i] = 0.f;
+                const int dslot = diag_slot[u];
+                if (A.rowlen[u] > 0 && dslot >= 0)
+                {
+                    const int bank = u >> 5, lane = u & 31;
+                    const long long slot = A.slice[bank] + dslot;
+                    double d[9], di[9];
+#pragma unroll
+                    for (int q = 0; q < 9; ++q)
+                        d[q] = block_entry(A, slot, lane, q);
+                    const double tr = d[0] + d[4] + d[8];
+                    if (tr > 0.0 && isfinite(tr) && inv3(d, di))
+                    {
+                        double re[3], bv[3], v[3];
+#pragma unroll
+                        for (int i = 0; i < 3; ++i)
+                        {
+                            const long long k = (long long)u * 3 + i;
+                            bv[i] = b[k];
+                            re[i] = bv[i] - (2.0 * y1[k] - y2[k]);
+                            v[i] = x1[k] - x2[k];
+                        }
+#pragma unroll
+                        for (int i = 0; i < 3; ++i)
+                        {
+                            const double q = di[3 * i] * re[0] + di[3 * i + 1] * re[1] + di[3 * i + 2] * re[2];
+                            const double p = di[3 * i] * bv[0] + di[3 * i + 1] * bv[1] + di[3 * i + 2] * bv[2];
+                            f[i] = (float)q;
+                            f[3 + i] = (float)v[i];
+                            f[6 + i] = (float)p;
+                            sums[0] = fma(q, q, sums[0]);
+                            sums[1] = fma(v[i], v[i], sums[1]);
+                            sums[2] = fma(p, p, sums[2]);
+                        }
+                        const double t = tr / 3.0;
+                        f[9] = (float)(d[0] / t);
+                        f[10] = (float)(d[4] / t);
+                        f[11] = (float)(d[8] / t);
+                        f[12] = (float)(d[1] / t);
+                        f[13] = (float)(d[2] / t);
+                        f[14] = (float)(d[5] / t);
+                        const double lt = log(tr);
+                        f[15] = (float)lt;
+                        sums[3] = lt;
+                        sums[4] = 1.0;
+                    }
+                }
+                float4 *dst = reinterpret_cast<float4 *>(feat + (long long)u * F);
+#pragma unroll
+                for (int i = 0; i < F / 4; ++i)
+                    dst[i] = make_float4(f[4 * i], f[4 * i + 1], f[4 * i + 2], f[4 * i + 3]);
+            }
+            double tot[5];
+            if (grid_reduce<5, WT>(sums, partials, &ws->counter[0], tot) && threadIdx.x == 0)
+                for (int i = 0; i < 5; ++i)
+                    ws->sums[i] = tot[i];
+        }
+
+        struct Norms
+        {
+            float iq, iv, ip, mlog; // 1 / rms (0 if the rms is 0) and the mean log trace
+        };
+
+        __device__ __forceinline__ Norms norms(const WsState *ws)
+        {
+            const double cnt = ws->sums[4];
+            Norms n{0.f, 0.f, 0.f, 0.f};
+            if (cnt > 0.0)
+            {
+                const double dofs = 3.0 * cnt;
+                const double sq = sqrt(ws->sums[0] / dofs), sv = sqrt(ws->sums[1] / dofs),
+                             sp = sqrt(ws->sums[2] / dofs);
+                n.iq = sq > 0.0 ? (float)(1.0 / sq) : 0.f;
+                n.iv = sv > 0.0 ? (float)(1.0 / sv) : 0.f;
+                n.ip = sp > 0.0 ? (float)(1.0 / sp) : 0.f;
+                n.mlog = (float)(ws->sums[3] / cnt);
+            }
+            return n;
+        }
+
+        __device__ __forceinline__ bool node_real(const int *rowlen, const int *diag_slot, int u)
+        {
+            return rowlen[u] > 0 && diag_slot[u] >= 0;
+        }
+
+        // One warp per bank: lane o computes hidden units 2 o and 2 o + 1 of each of the bank's
+        // 32 vertices (features broadcast from global), stores coalesced 128 B rows.
+        __global__ void __launch_bounds__(WT) k_ws_input(int nodes, const int *__restrict__ rowlen,
+                                                         const int *__restrict__ diag_slot,
+                                                         const float *__restrict__ feat, const float *__restrict__ prm,
+                                                         const WsState *ws, __nv_bfloat162 *__restrict__ h)
+        {
+            __shared__ float wsm[H * F + H];
+            for (int i = threadIdx.x; i < H * F + H; i += WT)
+                wsm[i] = prm[OFF_WIN + i];
+            __syncthreads();
+            const Norms nm = norms(ws);
+            const int lane = threadIdx.x & 31;
+            const int bank = blockIdx.x * (WT / 32) + (threadIdx.x >> 5);
+            if (bank * 32 >= nodes)
+                return;
+            const int o0 = 2 * lane, o1 = 2 * lane + 1;
+            for (int j = 0; j < 32; ++j)
+            {
+                const int u = bank * 32 + j;
+                float2 out = make_float2(0.f, 0.f);
+                if (node_real(rowlen, diag_slot, u))
+                {
+                    const float4 *fp = reinterpret_cast<const float4 *>(feat + (long long)u * F);
+                    float f[F];
+#pragma unroll
+                    for (int i = 0; i < F / 4; ++i)
+                    {
+                        const float4 t = fp[i];
+                        f[4 * i] = t.x;
+                        f[4 * i + 1] = t.y;
+                        f[4 * i + 2] = t.z;
+                        f[4 * i + 3] = t.w;
+                    }
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+                    {
+                        f[i] *= nm.iq;
+                        f[3 + i] *= nm.iv;
+                        f[6 + i] *= nm.ip;
+                    }
+                    f[15] -= nm.mlog;
+                    float a0 = wsm[H * F + o0], a1 = wsm[H * F + o1];
+#pragma unroll
+                    for (int i = 0; i < F; ++i)
+                    {
+                        a0 = fmaf(wsm[o0 * F + i], f[i], a0);
+                        a1 = fmaf(wsm[o1 * F + i], f[i], a1);
+                    }
+                    out = make_float2(fmaxf(a0, 0.f), fmaxf(a1, 0.f));
+                }
+                h[(long long)u * (H / 2) + lane] = __float22bfloat162_rn(out);
+            }
+        }
+
+        __device__ __forceinline__ void ldsm_x4(uint32_t (&a)[4], uint32_t addr)
+        {
+            asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
+                         : "=r"(a[0]), "=r"(a[1]), "=r"(a[2]), "=r"(a[3])
+                         : "r"(addr));
+        }
+
+        __device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1)
+        {
+            asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
+                         "{%8, %9}, {%0, %1, %2, %3};"
+                         : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+        }
+
+        // One message-passing layer for 64 vertices. Shared tile T[v] = [h_v ; m_v] (bf16,
+        // K = 128), W_l as rows of K (the mma's column-major B), then each warp multiplies its
+        // 16 vertices by W_l^T: 8 k-steps x 8 n-tiles of m16n8k16.
+        __global__ void __launch_bounds__(LT) k_ws_layer(BankedView A, const float *__restrict__ wslot,
+                                                         const __nv_bfloat16 *__restrict__ hin,
+                                                         const uint16_t *__restrict__ wl, const float *__restrict__ bl,
+                                                         const int *__restrict__ diag_slot,
+                                                         __nv_bfloat16 *__restrict__ hout)
+        {
+            __shared__ __align__(16) __nv_bfloat16 T[TILE * TS];
+            __shared__ __align__(16) __nv_bfloat16 Wsm[H * TS];
+            __shared__ float bias[H];
+            const int nodes = A.banks * 32;
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+            // W_l: 64 rows x 128 bf16 = 16 chunks of 16 B per row.
+            for (int i = threadIdx.x; i < H * 16; i += LT)
+            {
+                const int row = i >> 4, ch = i & 15;
+                *reinterpret_cast<uint4 *>(&Wsm[row * TS + ch * 8]) =
+                    __ldg(reinterpret_cast<const uint4 *>(wl + row * 2 * H) + ch);
+            }
+            if (threadIdx.x < H)
+                bias[threadIdx.x] = bl[threadIdx.x];
+            // Gather: warp w fills rows 16 w .. 16 w + 15; lane l holds hidden units 2 l, 2 l + 1.
+            const __nv_bfloat162 *h2 = reinterpret_cast<const __nv_bfloat162 *>(hin);
+            for (int rr = 0; rr < 16; ++rr)
+            {
+                const int r = warp * 16 + rr;
+                const int u = blockIdx.x * TILE + r;
+                __nv_bfloat162 self = __float2bfloat162_rn(0.f);
+                float2 acc = make_float2(0.f, 0.f);
+                if (u < nodes && node_real(A.rowlen, diag_slot, u))
+                {
+                    self = h2[(long long)u * (H / 2) + lane];
+                    const int bank = u >> 5, ln = u & 31;
+                    const long long s0 = A.slice[bank];
+                    const int len = A.rowlen[u];
+                    for (int k0 = 0; k0 < len; k0 += 32)
+                    {
+                        const int kk = k0 + lane;
+                        int col = 0;
+                        float w = 0.f;
+                        if (kk < len)
+                        {
+                            col = A.cols[(s0 + kk) * 32 + ln];
+                            w = wslot[(s0 + kk) * 32 + ln];
+                        }
+                        const int cnt = min(32, len - k0);
+#pragma unroll 4
+                        for (int j = 0; j < cnt; ++j)
+                        {
+                            const int cj = __shfl_sync(FULL, col, j);
+                            const float wj = __shfl_sync(FULL, w, j);
+                            if (wj != 0.f)
+                            {
+                                const float2 hv = __bfloat1622float2(h2[(long long)cj * (H / 2) + lane]);
+                                acc.x = fmaf(wj, hv.x, acc.x);
+                                acc.y = fmaf(wj, hv.y, acc.y);
+                            }
+                        }
+                    }
+                }
+                *reinterpret_cast<__nv_bfloat162 *>(&T[r * TS + 2 * lane]) = self;
+                *reinterpret_cast<__nv_bfloat162 *>(&T[r * TS + H + 2 * lane]) = __float22bfloat162_rn(acc);
+            }
+            __syncthreads();
+
+            // Tensor-core product of the warp's 16 rows with W_l^T.
+            float d[8][4];
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    d[nt][i] = 0.f;
+            const uint32_t tbase = smem_addr(T), wbase = smem_addr(Wsm);
+            const int arow = warp * 16 + (lane & 15), acol = (lane >> 4) * 8;
+            const int brow = (lane & 7) + ((lane >> 4) << 3), bcol = ((lane >> 3) & 1) * 8;
+#pragma unroll
+            for (int ks = 0; ks < (2 * H) / 16; ++ks)
+            {
+                uint32_t a[4];
+                ldsm_x4(a, tbase + (uint32_t)((arow * TS + ks * 16 + acol) * 2));
+#pragma unroll
+                for (int np = 0; np < 4; ++np)
+                {
+                    uint32_t bfr[4];
+                    ldsm_x4(bfr, wbase + (uint32_t)(((np * 16 + brow) * TS + ks * 16 + bcol) * 2));
+                    mma_bf16(d[2 * np], a, bfr[0], bfr[1]);
+                    mma_bf16(d[2 * np + 1], a, bfr[2], bfr[3]);
+                }
+            }
+            __syncwarp();
+            // Epilogue: h_out = h + relu(acc + b), written over the warp's own rows of T.
+            const int g = lane >> 2, c2 = (lane & 3) * 2;
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+                for (int half = 0; half < 2; ++half)
+                {
+                    const int r = warp * 16 + g + half * 8;
+                    const int col = nt * 8 + c2;
+                    __nv_bfloat162 *tp = reinterpret_cast<__nv_bfloat162 *>(&T[r * TS + col]);
+                    const float2 hs = __bfloat1622float2(*tp);
+                    const float v0 = hs.x + fmaxf(d[nt][2 * half] + bias[col], 0.f);
+                    const float v1 = hs.y + fmaxf(d[nt][2 * half + 1] + bias[col + 1], 0.f);
+                    *tp = __float22bfloat162_rn(make_float2(v0, v1));
+                }
+            __syncwarp();
+            __nv_bfloat162 *o2 = reinterpret_cast<__nv_bfloat162 *>(hout);
+            for (int rr = 0; rr < 16; ++rr)
+            {
+                const int r = warp * 16 + rr;
+                const int u = blockIdx.x * TILE + r;
+                if (u >= nodes)
+                    break;
+                __nv_bfloat162 v = __float2bfloat162_rn(0.f);
+                if (node_real(A.rowlen, diag_slot, u))
+                    v = *reinterpret_cast<const __nv_bfloat162 *>(&T[r * TS + 2 * lane]);
+                o2[(long long)u * (H / 2) + lane] = v;
+            }
+        }
+
+        // c = s_q (W_out h + b_out): one warp per bank, vertices in turn, lanes over hidden units.
+        __global__ void __launch_bounds__(WT) k_ws_output(int nodes, const int *__restrict__ rowlen,
+                                                          const int *__restrict__ diag_slot,
+                                                          const __nv_bfloat162 *__restrict__ h,
+                                                          const float *__restrict__ prm, const WsState *ws,
+                                                          double *__restrict__ c)
+        {
+            const int lane = threadIdx.x & 31;
+            const int bank = blockIdx.x * (WT / 32) + (threadIdx.x >> 5);
+            if (bank * 32 >= nodes)
+                return;
+            const double cnt = ws->sums[4];
+            const double sq = cnt > 0.0 ? sqrt(ws->sums[0] / (3.0 * cnt)) : 0.0;
+            float w[3][2];
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+            {
+                w[i][0] = prm[OFF_WOUT + i * H + 2 * lane];
+                w[i][1] = prm[OFF_WOUT + i * H + 2 * lane + 1];
+            }
+            const float b0 = prm[OFF_BOUT], b1 = prm[OFF_BOUT + 1], b2 = prm[OFF_BOUT + 2];
+            for (int j = 0; j < 32; ++j)
+            {
+                const int u = bank * 32 + j;
+                const bool real = node_real(rowlen, diag_slot, u);
+                const float2 hv = __bfloat1622float2(h[(long long)u * (H / 2) + lane]);
+                float s[3];
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    s[i] = warp_sum(fmaf(w[i][0], hv.x, w[i][1] * hv.y));
+                if (lane < 3)
+                {
+                    const float bo = lane == 0 ? b0 : (lane == 1 ? b1 : b2);
+                    const float si = lane == 0 ? s[0] : (lane == 1 ? s[1] : s[2]);
+                    c[(long long)u * 3 + lane] = real ? sq * (double)(si + bo) : 0.0;
+                }
+            }
+        }
+
+        constexpr int GRAM_CTAS_PER_SM = 4;
+
+        // The Galerkin system of {x1, x1 - x2, c}; the last CTA solves it.
+        __global__ void __launch_bounds__(WT)
+            k_ws_gram(const double *__restrict__ b, const double *__restrict__ x1, const double *__restrict__ x2,
+                      const double *__restrict__ c, const double *__restrict__ y1, const double *__restrict__ y2,
+                      const double *__restrict__ y3, size_t len, WsState *ws, double *partials)
+        {
+            double s[9];
+#pragma unroll
+            for (int i = 0; i < 9; ++i)
+                s[i] = 0.0;
+            for (size_t k = (size_t)blockIdx.x * WT + threadIdx.x; k < len; k += (size_t)gridDim.x * WT)
+            {
+                const double v1 = x1[k], v2 = x1[k] - x2[k], v3 = c[k];
+                const double a1 = y1[k], a2 = y1[k] - y2[k], a3 = y3[k], bk = b[k];
+                s[0] = fma(v1, a1, s[0]);
+                s[1] = fma(v1, a2, s[1]);
+                s[2] = fma(v1, a3, s[2]);
+                s[3] = fma(v2, a2, s[3]);
+                s[4] = fma(v2, a3, s[4]);
+                s[5] = fma(v3, a3, s[5]);
+                s[6] = fma(v1, bk, s[6]);
+                s[7] = fma(v2, bk, s[7]);
+                s[8] = fma(v3, bk, s[8]);
+            }
+            double t[9];
+            if (!grid_reduce<9, WT>(s, partials, &ws->counter[1], t) || threadIdx.x != 0)
+                return;
+            for (int i = 0; i < 9; ++i)
+                ws->gram[i] = t[i];
+            const double G[3][3] = {{t[0], t[1], t[2]}, {t[1], t[3], t[4]}, {t[2], t[4], t[5]}};
+            const double g[3] = {t[6], t[7], t[8]};
+            // Cholesky of the kept vectors, in order; a vector whose pivot is below 1e-10 of its
+            // diagonal (dependent on the kept ones) or not positive is dropped.
+            double L[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+            bool keep[3] = {false, false, false};
+            int rank = 0;
+            for (int i = 0; i < 3; ++i)
+            {
+                if (!(G[i][i] > 0.0) || !isfinite(G[i][i]))
+                    continue;
+                double dsum = G[i][i];
+                for (int j = 0; j < i; ++j)
+                {
+                    if (!keep[j])
+                        continue;
+                    double v = G[i][j];
+                    for (int k = 0; k < j; ++k)
+                        if (keep[k])
+                            v -= L[i][k] * L[j][k];
+                    L[i][j] = v / L[j][j];
+                    dsum -= L[i][j] * L[i][j];
+                }
+                if (dsum > 1e-10 * G[i][i] && isfinite(dsum))
+                {
+                    L[i][i] = sqrt(dsum);
+                    keep[i] = true;
+                    ++rank;
+                }
+                else
+                    for (int j = 0; j < i; ++j)
+                        L[i][j] = 0.0;
+            }
+            double y[3] = {0.0, 0.0, 0.0}, z[3] = {0.0, 0.0, 0.0};
+            for (int i = 0; i < 3; ++i) // L z = g
+                if (keep[i])
+                {
+                    double v = g[i];
+                    for (int j = 0; j < i; ++j)
+                        if (keep[j])
+                            v -= L[i][j] * z[j];
+                    z[i] = v / L[i][i];
+                }
+            for (int i = 2; i >= 0; --i) // L^T y = z
+                if (keep[i])
+                {
+                    double v = z[i];
+                    for (int j = i + 1; j < 3; ++j)
+                        if (keep[j])
+                            v -= L[j][i] * y[j];
+                    y[i] = v / L[i][i];
+                }
+            double e = 0.0; // 1/2 y.Gy - y.g
+            for (int i = 0; i < 3; ++i)
+            {
+                double gy = 0.0;
+                for (int j = 0; j < 3; ++j)
+                    gy += G[i][j] * y[j];
+                e += y[i] * (0.5 * gy - g[i]);
+            }
+            const double e1 = 0.5 * G[0][0] - g[0];
+            const bool ok = rank > 0 && isfinite(e) && isfinite(y[0]) && isfinite(y[1]) && isfinite(y[2]) && e < e1;
+            ws->fallback = ok ? 0 : 1;
+            ws->rank = rank;
+            ws->coef[0] = ok ? y[0] : 1.0;
+            ws->coef[1] = ok ? y[1] : 0.0;
+            ws->coef[2] = ok ? y[2] : 0.0;
+            ws->energy = ok ? e : e1;
+            ws->energy_prev = e1;
+        }
+
+        __global__ void __launch_bounds__(WT) k_ws_combine(const double *__restrict__ x1,
+                                                           const double *__restrict__ x2,
+                                                           const double *__restrict__ c, const WsState *ws,
+                                                           double *__restrict__ x, size_t len)
+        {
+            const double a = ws->coef[0], bcoef = ws->coef[1], g = ws->coef[2];
+            for (size_t k = (size_t)blockIdx.x * WT + threadIdx.x; k < len; k += (size_t)gridDim.x * WT)
+                x[k] = a * x1[k] + bcoef * (x1[k] - x2[k]) + g * c[k];
+        }
+
+        __global__ void k_ws_features_out(int V, const int *__restrict__ padded, const float *__restrict__ feat,
+                                          float *__restrict__ out)
+        {
+            const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+            if (i >= (long long)V * F)
+                return;
+            const int v = (int)(i / F), f = (int)(i % F);
+            out[i] = feat[(long long)padded[v] * F + f];
+        }
+    } // namespace
+
+    int ws_reduce_ctas() { return device_sm_count() * GRAM_CTAS_PER_SM; }
+
+    void launch_ws_graph(const BankedView &A, const WsBuffers &w, cudaStream_t s)
+    {
+        if (A.bd != 3)
+            throw Error(ERR_INVALID, "[MAS] the learned warm start needs block_dim 3");
+        const int nodes = A.banks * 32;
+        if (nodes == 0)
+            return;
+        k_ws_graph<<<(nodes + WT - 1) / WT, WT, 0, s>>>(A, w.diag_slot, w.wslot);
+        cuda_check(cudaGetLastError(), "warm start graph launch");
+    }
+
+    int launch_ws_network(const BankedView &A, const WsBuffers &w, const double *b, const double *x1,
+                          const double *x2, cudaStream_t s)
+    {
+        const int nodes = A.banks * 32;
+        if (nodes == 0)
+            return 0;
+        const int grid_v = (nodes + WT - 1) / WT;
+        if (grid_v > w.capacity)
+            throw Error(ERR_INVALID, "[MAS] warm start reduction scratch too small");
+        k_ws_features<<<grid_v, WT, 0, s>>>(A, w.diag_slot, b, x1, x2, w.y1, w.y2, w.feat, w.st, w.partials);
+        cuda_check(cudaGetLastError(), "warm start features launch");
+        const int grid_b = (A.banks + WT / 32 - 1) / (WT / 32);
+        k_ws_input<<<grid_b, WT, 0, s>>>(nodes, A.rowlen, w.diag_slot, w.feat, w.params, w.st,
+                                         reinterpret_cast<__nv_bfloat162 *>(w.h[0]));
+        cuda_check(cudaGetLastError(), "warm start input launch");
+        const int grid_t = (nodes + TILE - 1) / TILE;
+        for (int l = 0; l < WS_LAYERS; ++l)
+        {
+            k_ws_layer<<<grid_t, LT, 0, s>>>(A, w.wslot, reinterpret_cast<const __nv_bfloat16 *>(w.h[l & 1]),
+                                            w.wl + (size_t)l * WS_LAYER_WEIGHTS, w.params + off_layer(l) + H * 2 * H,
+                                            w.diag_slot, reinterpret_cast<__nv_bfloat16 *>(w.h[(l + 1) & 1]));
+            cuda_check(cudaGetLastError(), "warm start layer launch");
+        }
+        k_ws_output<<<grid_b, WT, 0, s>>>(nodes, A.rowlen, w.diag_slot,
+                                          reinterpret_cast<const __nv_bfloat162 *>(w.h[WS_LAYERS & 1]), w.params, w.st,
+                                          w.c);
+        cuda_check(cudaGetLastError(), "warm start output launch");
+        return 3 + WS_LAYERS;
+    }
+
+    int launch_ws_combine(const WsBuffers &w, const double *b, const double *x1, const double *x2, double *x,
+                          size_t len, cudaStream_t s)
+    {
+        const int grid = ws_reduce_ctas();
+        if (grid > w.capacity)
+            throw Error(ERR_INVALID, "[MAS] warm start reduction scratch too small");
+        k_ws_gram<<<grid, WT, 0, s>>>(b, x1, x2, w.c, w.y1, w.y2, w.y3, len, w.st, w.partials);
+        cuda_check(cudaGetLastError(), "warm start gram launch");
+        k_ws_combine<<<grid, WT, 0, s>>>(x1, x2, w.c, w.st, x, len);
+        cuda_check(cudaGetLastError(), "warm start combine launch");
+        return 2;
+    }
+
+    void launch_ws_features_out(int V, const int *padded_of_block, const float *feat, float *out, cudaStream_t s)
+    {
+        const long long total = (long long)V * F;
+        if (total == 0)
+            return;
+        k_ws_features_out<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(V, padded_of_block, feat, out);
+        cuda_check(cudaGetLastError(), "warm start features out launch");
+    }
+} // namespace pmas

@@ -10,13 +10,17 @@ it from the previous solutions:
   ``previous`` for the second step and to zero for the first.
 
 The relative tolerance stays relative to ||b_k||, so a good guess directly saves iterations.
+
+``learned`` leaves the guess to the solver (``initial_guess: "learned"``, a network loaded with
+``Solver.set_warm_start_model``): it keeps its last two solutions on the device and starts from
+the energy-minimising combination of x_{k-1}, x_{k-1} - x_{k-2} and the network's correction.
 """
 
 from __future__ import annotations
 
 import numpy as np
 
-MODES = ("zero", "previous", "extrapolate")
+MODES = ("zero", "previous", "extrapolate", "learned")
 
 
 class WarmStart:
@@ -28,7 +32,7 @@ class WarmStart:
 
     def guess(self, n: int) -> np.ndarray | None:
         """x0 for the next step (None: start from zero)."""
-        if self.mode == "zero" or not self._hist:
+        if self.mode in ("zero", "learned") or not self._hist:
             return None
         if self.mode == "previous" or len(self._hist) < 2:
             return self._hist[-1].copy()
@@ -44,7 +48,8 @@ class WarmStart:
 
 def solve_sequence(solver, systems, rhs, mode: str = "extrapolate", on_step=None, check: bool = True) -> list[dict]:
     """Factorize and solve each (A_k, b_k) with warm starts; returns per-step info (iterations,
-    status, relative residual). `solver` must have ``initial_guess: input`` for non-zero modes;
+    status, relative residual, x0 source). `solver` must have ``initial_guess: input`` for the
+    previous / extrapolate modes and ``initial_guess: learned`` for the learned mode;
     the pattern of every A_k must be the same (values-only refactorization). With ``check`` the
     relative residual ||A x - b|| / ||b|| is recomputed on the host (scipy); otherwise it is the
     solver's own reported relative residual."""
@@ -61,7 +66,8 @@ def solve_sequence(solver, systems, rhs, mode: str = "extrapolate", on_step=None
             rel = float(np.linalg.norm(A @ x - b) / np.linalg.norm(b))
         else:
             rel = float(info["relative_residual"])
-        out.append({"step": k, "iterations": info["solver_iter"], "status": info["solver_status"], "rel": rel})
+        out.append({"step": k, "iterations": info["solver_iter"], "status": info["solver_status"], "rel": rel,
+                    "x0_source": info.get("x0_source", "")})
         if on_step:
             on_step(k, x, info)
     return out

@@ -41,7 +41,7 @@ EXPORTED_SYMBOLS = [
     "mas_analyze_pattern", "mas_set_positions", "mas_factorize_csc", "mas_solve", "mas_solve_multi",
     "mas_solve_device", "mas_solve_batch", "mas_set_stream", "mas_spmv_dot_noalloc", "mas_last_error", "mas_get_sizes", "mas_get_ordering", "mas_order_blocks",
     "mas_get_coarse_map", "mas_get_inverses", "mas_debug_spmv", "mas_debug_apply", "mas_debug_apply_multi",
-    "mas_debug_spmv_multi",
+    "mas_debug_spmv_multi", "mas_set_warm_start_model", "mas_reset_warm_start", "mas_debug_warm_start",
 ]
 
 
@@ -96,6 +96,9 @@ def library() -> ctypes.CDLL:
         L.mas_debug_apply.argtypes = [vp, vp, vp, i]
         L.mas_debug_apply_multi.argtypes = [vp, vp, vp, i]
         L.mas_debug_spmv_multi.argtypes = [vp, vp, vp, i]
+        L.mas_set_warm_start_model.argtypes = [vp, vp, ctypes.c_longlong]
+        L.mas_reset_warm_start.argtypes = [vp]
+        L.mas_debug_warm_start.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
         L.mas_order_blocks.argtypes = [i, vp, vp, i, vp, ctypes.c_char_p, ip, ip]
         _LIB = L
     return _LIB
@@ -350,6 +353,39 @@ class Solver:
         z = np.empty_like(r)
         _check(library().mas_debug_apply_multi(self._h, r.ctypes.data, z.ctypes.data, int(r.size)), self._h)
         return z
+
+    def set_warm_start_model(self, params=None) -> None:
+        """New: the network of ``initial_guess: "learned"``: a float32 parameter vector, a path to
+        a ``.psws`` file, or None for the shipped weights (``polysolve_b200.warmstart``)."""
+        from . import warmstart
+
+        if params is None:
+            params = warmstart.default_weights()
+        elif not isinstance(params, np.ndarray):
+            params = warmstart.load(params)
+        prm = np.ascontiguousarray(params, dtype=np.float32)
+        _check(library().mas_set_warm_start_model(self._h, prm.ctypes.data, int(prm.size)), self._h)
+
+    def reset_warm_start(self) -> None:
+        """New: forget the kept solutions (the next learned-mode solve starts from zero)."""
+        _check(library().mas_reset_warm_start(self._h), self._h)
+
+    def debug_warm_start(self, b: np.ndarray, x1: np.ndarray, x2: np.ndarray) -> dict:
+        """Test hook: the learned starting guess for b given x_{k-1} = x1, x_{k-2} = x2 (caller
+        order), without a solve: c, x0, raw features (nverts, 16) and the reduction record."""
+        from . import warmstart
+
+        b, x1, x2 = (np.ascontiguousarray(v, dtype=np.float64) for v in (b, x1, x2))
+        n = b.size
+        c = np.empty(n)
+        x0 = np.empty(n)
+        feat = np.empty(((n + 2) // 3, warmstart.FEATURES), dtype=np.float32)
+        state = np.empty(21)
+        _check(library().mas_debug_warm_start(self._h, b.ctypes.data, x1.ctypes.data, x2.ctypes.data, c.ctypes.data,
+                                              x0.ctypes.data, feat.ctypes.data, state.ctypes.data), self._h)
+        return {"c": c, "x0": x0, "features": feat, "sums": state[0:5], "gram": state[5:14], "coef": state[14:17],
+                "energy": state[17], "energy_previous": state[18], "fallback": bool(state[19]),
+                "rank": int(state[20])}
 
     def debug_spmv_multi(self, X_padded: np.ndarray) -> np.ndarray:
         x = np.ascontiguousarray(X_padded, dtype=np.float64)

@@ -34,4 +34,7 @@ def test_warm_start_keeps_two_and_copies():
     ws.reset()
     assert ws.guess(2) is None
     with pytest.raises(ValueError):
-        WarmStart("learned")
+        WarmStart("quadratic")
+    learned = WarmStart("learned")  # the solver makes the guess itself
+    learned.record(x)
+    assert learned.guess(2) is None
