@@ -195,6 +195,27 @@ int mas_debug_spmv_multi(mas_solver *h, const double *xin, double *yout, int len
 int mas_debug_warm_start(mas_solver *h, const double *b, const double *x1, const double *x2, double *c_out,
                          double *x0_out, float *features_out, double *state_out);
 
+/* New: Matrix Market files for A and b, the format the reference's tests load with Eigen's
+ * loadMarket / loadMarketVector (tests/test_linear_solver.cpp:25-50, :211-213). Host only.
+ * mas_market_load reads "coordinate" (real / integer / pattern, general / symmetric: duplicates
+ * summed, symmetric files expanded to the full matrix) into CSC with sorted rows, or "array"
+ * files into a dense column-major array (a vector is n x 1). dims gives rows, cols, the CSC
+ * entry count (or rows * cols for arrays) and whether it is dense; copy_csc fills outer[cols+1],
+ * inner[nnz], vals[nnz]; copy_dense fills count = rows * cols values. Errors: MAS_ERR_INVALID
+ * with the message in mas_market_last_error() (per thread). */
+typedef struct mas_market mas_market;
+int mas_market_load(const char *path, mas_market **out);
+int mas_market_dims(const mas_market *m, int *rows, int *cols, long long *nnz, int *dense);
+int mas_market_copy_csc(const mas_market *m, int *outer, int *inner, double *vals);
+int mas_market_copy_dense(const mas_market *m, double *out, long long count);
+void mas_market_free(mas_market *m);
+const char *mas_market_last_error(void);
+/* Writes a square CSC matrix as "coordinate real general", or only its lower triangle as
+ * "coordinate real symmetric"; a vector as "array real general". 17 significant digits. */
+int mas_market_write_csc(const char *path, int n, const int *outer, const int *inner, const double *vals,
+                         int symmetric);
+int mas_market_write_vector(const char *path, const double *x, long long n);
+
 #ifdef __cplusplus
 }
 #endif

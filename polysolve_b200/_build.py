@@ -42,7 +42,7 @@ CU_SOURCES = [
     "mas_multi.cu",
     "mas_warmstart.cu",
 ]
-CPP_SOURCES = ["mas_capi.cpp", "mas_ordering.cpp", "mas_json.cpp"]
+CPP_SOURCES = ["mas_capi.cpp", "mas_ordering.cpp", "mas_json.cpp", "mas_market.cpp"]
 
 
 def _run(cmd: list[str]) -> None:

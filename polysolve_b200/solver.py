@@ -42,6 +42,8 @@ EXPORTED_SYMBOLS = [
     "mas_solve_device", "mas_solve_batch", "mas_set_stream", "mas_spmv_dot_noalloc", "mas_last_error", "mas_get_sizes", "mas_get_ordering", "mas_order_blocks",
     "mas_get_coarse_map", "mas_get_inverses", "mas_debug_spmv", "mas_debug_apply", "mas_debug_apply_multi",
     "mas_debug_spmv_multi", "mas_set_warm_start_model", "mas_reset_warm_start", "mas_debug_warm_start",
+    "mas_market_load", "mas_market_dims", "mas_market_copy_csc", "mas_market_copy_dense", "mas_market_free",
+    "mas_market_last_error", "mas_market_write_csc", "mas_market_write_vector",
 ]
 
 
