@@ -15,6 +15,8 @@
 //     (nlohmann::json), or a std::string holding JSON text.
 #pragma once
 
+#include <cstdio>
+#include <cstring>
 #include <memory>
 #include <stdexcept>
 #include <string>
@@ -172,6 +174,32 @@ namespace polysolve::linear
 
         /// New: vertex positions for the Morton subdomain ordering (xyz per block row).
         void set_positions(const double *xyz, int nverts) { check(mas_set_positions(h_, xyz, nverts)); }
+
+        /// New: the network of "initial_guess": "learned" (MAS_WS_PARAMS float32 values).
+        void set_warm_start_model(const std::vector<float> &params)
+        {
+            check(mas_set_warm_start_model(h_, params.data(), (long long)params.size()));
+        }
+        /// New: forget the kept solutions of a sequence.
+        void reset_warm_start() { check(mas_reset_warm_start(h_)); }
+        /// The parameters of a .psws weight file ("PSWSMPN1", four int32 dimensions, float32s).
+        static std::vector<float> load_warm_start_model(const std::string &path)
+        {
+            std::FILE *f = std::fopen(path.c_str(), "rb");
+            if (!f)
+                throw std::runtime_error("[MAS] cannot open " + path);
+            char magic[8];
+            int dims[4];
+            std::vector<float> prm(MAS_WS_PARAMS);
+            const bool ok = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, "PSWSMPN1", 8) == 0 &&
+                            std::fread(dims, sizeof(int), 4, f) == 4 && dims[0] == MAS_WS_FEATURES &&
+                            dims[1] == MAS_WS_HIDDEN && dims[2] == MAS_WS_LAYERS && dims[3] == MAS_WS_PARAMS &&
+                            std::fread(prm.data(), sizeof(float), prm.size(), f) == prm.size();
+            std::fclose(f);
+            if (!ok)
+                throw std::runtime_error("[MAS] not a warm-start weight file: " + path);
+            return prm;
+        }
 
         template <class M>
         void factorize(const M &A)
