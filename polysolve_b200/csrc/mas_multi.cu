@@ -20,8 +20,10 @@ namespace pmas
         constexpr int G = RHS_GROUP;
         constexpr int MT = 256; // threads per CTA of the multi kernels
 
+        // Two slots per loop trip with at most 128 registers (two CTAs per SM): both slots' loads
+        // and gathers in flight.
         template <int BD, int MODE>
-        __global__ void __launch_bounds__(MT) k_spmv_g(BankedView A, const double *__restrict__ x,
+        __global__ void __launch_bounds__(MT, 2) k_spmv_g(BankedView A, const double *__restrict__ x,
                                                       double *__restrict__ y, const double *__restrict__ b,
                                                       PcgState *st, ReduceBuf red, int iter, int period)
         {
@@ -52,6 +54,7 @@ namespace pmas
                     for (int g = 0; g < G; ++g)
                         acc[i][g] = 0.0;
                 const uint64_t pol = l2_evict_first_policy();
+#pragma unroll 2
                 for (int k = 0; k < len; ++k)
                 {
                     const int col = ld_stream_s32(cp + (long long)k * 32, pol);

@@ -1,5 +1,5 @@
-"""A system read from Matrix Market files (as polysolve's tests load theirs) solves exactly like
-the in-memory one."""
+"""A system read from Matrix Market files (as polysolve's tests load theirs) is the in-memory one
+bit for bit and solves to the same solution."""
 
 import numpy as np
 import pytest
@@ -14,10 +14,15 @@ def test_solve_from_matrix_market_files(tmp_path):
     system = synthetic.elasticity(9, young_sigma=1.0, jitter=0.2, seed=8)
     A = system.scipy()
     b = synthetic.rhs(system.n, seed=8)
-    scipy.io.mmwrite(tmp_path / "A.mtx", A, symmetry="symmetric", precision=17)
+    # general: every stored value round-trips exactly (a symmetric file keeps one triangle, and
+    # the assembled matrix is symmetric only to rounding)
+    scipy.io.mmwrite(tmp_path / "A.mtx", A, symmetry="general", precision=17)
     market.save_vector(tmp_path / "b.mtx", b)
     A2 = market.load_matrix(tmp_path / "A.mtx")
     b2 = market.load_vector(tmp_path / "b.mtx")
+    A.sort_indices()
+    assert np.array_equal(A2.indptr, A.indptr) and np.array_equal(A2.indices, A.indices)
+    assert np.array_equal(A2.data, A.data) and np.array_equal(b2, b)
     xs = []
     for M, rhs in ((A, b), (A2, b2)):
         s = Solver.create("MAS", "")
@@ -29,4 +34,5 @@ def test_solve_from_matrix_market_files(tmp_path):
         s.solve(rhs, x)
         xs.append(x)
         assert np.linalg.norm(M @ x - rhs) <= 1e-8 * np.linalg.norm(rhs)
-    assert np.array_equal(xs[0], xs[1])
+    # the coarse-level assembly sums with atomics, so two factorizations agree to rounding only
+    assert np.linalg.norm(xs[0] - xs[1]) <= 1e-6 * np.linalg.norm(xs[0])
