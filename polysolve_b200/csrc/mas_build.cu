@@ -8,9 +8,12 @@
 //     (:222-275), components again (:281-318), global ids (:345-363); stop when nothing merges
 //     (:464-469);
 //  3. subdomain matrices: level 0 straight from each bank's rows (upper triangle, no atomics);
-//     coarse levels accumulate the upper triangle with the reference's rules (same bank, row <=
-//     col, diagonal block upper only, A_ij + A_ij^T when two nodes collapse, :494-591) with FP64
-//     atomics into a staging buffer;
+//     coarse levels hold the reference's sums (same bank, row <= col, diagonal block upper only,
+//     A_ij + A_ij^T when two nodes collapse, :494-591) but build them hierarchically and without
+//     atomics: the Galerkin blocks S_0(a, b) = sum of the fine blocks A_uw with map(u) = a,
+//     map(w) = b, then S_(l+1)(A, B) = sum of S_l(a, b) over the children pairs, each a
+//     fixed-order sum over a record list sorted once per coarse space (deterministic: the same
+//     values give the same bits; the reference's FP64 atomics do not);
 //  4. zero diagonals -> 1 (:779-796) and an in-place symmetric sweep inverse in FP64 (the
 //     Beaton / Goodnight sweep operator, as in batched_invert_upper :799-900), with a device error
 //     flag instead of an exception; the result is stored tile-packed in FP64 or FP32.
@@ -400,53 +403,6 @@ namespace pmas
             invert_and_store<BD, Out>(M, col, out + (size_t)bank * S, scale + bank, nullptr, flag);
         }
 
-        // Coarse-level upper-triangle accumulation with FP64 atomics (order-dependent in the
-        // last bits, as in the reference).
-        template <int BD>
-        __global__ void k_assemble_coarse(BankedView A, const int *__restrict__ node_real, const int *__restrict__ map,
-                                          int level_num, int coff0, int coff1, int coff2, int coff3, double *staging)
-        {
-            constexpr int N = 32 * BD;
-            const int u = blockIdx.x * blockDim.x + threadIdx.x;
-            if (u >= A.banks * 32 || !node_real[u])
-                return;
-            const int coff[4] = {coff0, coff1, coff2, coff3};
-            const long long s0 = A.slice[u >> 5];
-            const int lane = u & 31;
-            const int len = A.rowlen[u];
-            for (int k = 0; k < len; ++k)
-            {
-                const long long slot = s0 + k;
-                const int w = A.cols[slot * 32 + lane];
-                if (w < u || !node_real[w])
-                    continue;
-                for (int lv = 0; lv < level_num; ++lv)
-                {
-                    const int ci = map[(long long)u * 4 + lv], cj = map[(long long)w * 4 + lv];
-                    if ((ci >> 5) != (cj >> 5))
-                        continue;
-                    const long long g = (coff[lv] + ci) >> 5;
-                    double *mat = staging + (size_t)g * N * N;
-                    const bool collapsed = (u != w) && (ci == cj);
-#pragma unroll
-                    for (int bi = 0; bi < BD; ++bi)
-#pragma unroll
-                        for (int bj = 0; bj < BD; ++bj)
-                        {
-                            const int row = (ci & 31) * BD + bi, cl = (cj & 31) * BD + bj;
-                            if (row > cl)
-                                continue;
-                            if (u == w && bi > bj)
-                                continue;
-                            double v = A.vals[banked_value_index(slot, lane, bi * BD + bj, BD)];
-                            if (collapsed)
-                                v += A.vals[banked_value_index(slot, lane, bj * BD + bi, BD)];
-                            atomicAdd(mat + row * N + cl, v);
-                        }
-                }
-            }
-        }
-
         template <int BD, class Out>
         __global__ void __launch_bounds__(256) k_invert_coarse(const double *__restrict__ staging, Out *out,
                                                                double *scale, int *identity, int *flag)
@@ -498,6 +454,276 @@ namespace pmas
             cuda_check(cudaStreamSynchronize(s), "scan sync");
         }
 
+
+        // ---- Deterministic hierarchical coarse assembly -------------------------------------
+        // Record rules: the source block X enters its target as X, X^T, or X + X^T (two distinct
+        // nodes collapsing into one coarse node).
+        constexpr int RULE_PLAIN = 0, RULE_TRANS = 1, RULE_SYM = 2;
+
+        __device__ __forceinline__ void pair_rule(long long a, long long b, bool same_source_node, long long cn,
+                                                  long long &key, int &rule)
+        {
+            if (a < b)
+            {
+                key = a * cn + b;
+                rule = RULE_PLAIN;
+            }
+            else if (a > b)
+            {
+                key = b * cn + a;
+                rule = RULE_TRANS;
+            }
+            else
+            {
+                key = a * cn + a;
+                rule = same_source_node ? RULE_PLAIN : RULE_SYM;
+            }
+        }
+
+        // Level 0 records: one per coupled fine pair (u <= w), both real.
+        __global__ void k_fine_pair_count(BankedView A, const int *__restrict__ node_real, long long *cnt)
+        {
+            const int u = blockIdx.x * blockDim.x + threadIdx.x;
+            if (u >= A.banks * 32)
+                return;
+            long long c = 0;
+            if (node_real[u])
+            {
+                const long long s0 = A.slice[u >> 5];
+                const int lane = u & 31, len = A.rowlen[u];
+                for (int k = 0; k < len; ++k)
+                {
+                    const int w = A.cols[(s0 + k) * 32 + lane];
+                    if (w >= u && node_real[w])
+                        ++c;
+                }
+            }
+            cnt[u] = c;
+        }
+
+        __global__ void k_fine_pair_emit(BankedView A, const int *__restrict__ node_real, const int *__restrict__ map,
+                                         const long long *__restrict__ off, long long cn, long long *keys,
+                                         long long *payload)
+        {
+            const int u = blockIdx.x * blockDim.x + threadIdx.x;
+            if (u >= A.banks * 32 || !node_real[u])
+                return;
+            const long long s0 = A.slice[u >> 5];
+            const int lane = u & 31, len = A.rowlen[u];
+            long long pos = off[u];
+            const long long a = map[(long long)u * 4];
+            for (int k = 0; k < len; ++k)
+            {
+                const long long slot = s0 + k;
+                const int w = A.cols[slot * 32 + lane];
+                if (w < u || !node_real[w])
+                    continue;
+                const long long b = map[(long long)w * 4];
+                long long key;
+                int rule;
+                pair_rule(a, b, w == u, cn, key, rule);
+                keys[pos] = key;
+                payload[pos] = ((slot * 32 + lane) << 2) | rule;
+                ++pos;
+            }
+        }
+
+        // Level l + 1 records: one per level-l target, through the parents.
+        __global__ void k_coarse_pair_emit(const int2 *__restrict__ pair, int targets, const int *__restrict__ parent,
+                                           long long cn, long long *keys, long long *payload)
+        {
+            const int t = blockIdx.x * blockDim.x + threadIdx.x;
+            if (t >= targets)
+                return;
+            const int2 p = pair[t];
+            long long key;
+            int rule;
+            pair_rule(parent[p.x], parent[p.y], p.x == p.y, cn, key, rule);
+            keys[t] = key;
+            payload[t] = ((long long)t << 2) | rule;
+        }
+
+        __global__ void k_key_heads(const long long *__restrict__ keys, long long n, int *head)
+        {
+            const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+            if (i < n)
+                head[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1 : 0;
+            else if (i == n)
+                head[i] = 0;
+        }
+
+        __global__ void k_key_targets(const long long *__restrict__ keys, const int *__restrict__ head,
+                                      const int *__restrict__ hidx, long long n, long long cn, int *ptr, int2 *pair)
+        {
+            const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+            if (i < n && head[i])
+            {
+                const int t = hidx[i];
+                ptr[t] = (int)i;
+                pair[t] = make_int2((int)(keys[i] / cn), (int)(keys[i] % cn));
+            }
+            if (i == n)
+                ptr[hidx[n]] = (int)n;
+        }
+
+        // One thread per target: the fixed-order sum of its records; same-bank pairs also go to
+        // the upper triangle of their coarse matrix in the staging buffer.
+        template <int BD>
+        __global__ void __launch_bounds__(256)
+            k_coarse_sum(bool fine, const long long *__restrict__ src, const int *__restrict__ ptr,
+                         const int2 *__restrict__ pair, int targets, BankedView A, const double *__restrict__ prev,
+                         double *__restrict__ vals, double *__restrict__ staging)
+        {
+            constexpr int BS = BD * BD, N = 32 * BD;
+            const int t = blockIdx.x * blockDim.x + threadIdx.x;
+            if (t >= targets)
+                return;
+            double acc[BS];
+#pragma unroll
+            for (int q = 0; q < BS; ++q)
+                acc[q] = 0.0;
+            const int r1 = ptr[t + 1];
+            for (int r = ptr[t]; r < r1; ++r)
+            {
+                const long long rec = src[r];
+                const int rule = (int)(rec & 3);
+                const long long idx = rec >> 2;
+                double x[BS];
+                if (fine)
+                {
+#pragma unroll
+                    for (int q = 0; q < BS; ++q)
+                        x[q] = A.vals[banked_value_index(idx >> 5, (int)(idx & 31), q, BD)];
+                }
+                else
+                {
+#pragma unroll
+                    for (int q = 0; q < BS; ++q)
+                        x[q] = prev[idx * BS + q];
+                }
+#pragma unroll
+                for (int i = 0; i < BD; ++i)
+#pragma unroll
+                    for (int j = 0; j < BD; ++j)
+                    {
+                        const double xt = x[j * BD + i];
+                        const double v = rule == RULE_PLAIN ? x[i * BD + j]
+                                                            : (rule == RULE_TRANS ? xt : x[i * BD + j] + xt);
+                        acc[i * BD + j] += v;
+                    }
+            }
+#pragma unroll
+            for (int q = 0; q < BS; ++q)
+                vals[(long long)t * BS + q] = acc[q];
+            const int2 p = pair[t];
+            if ((p.x >> 5) != (p.y >> 5))
+                return;
+            double *mat = staging + (size_t)(p.x >> 5) * N * N;
+#pragma unroll
+            for (int i = 0; i < BD; ++i)
+#pragma unroll
+                for (int j = 0; j < BD; ++j)
+                {
+                    const int row = (p.x & 31) * BD + i, col = (p.y & 31) * BD + j;
+                    if (row <= col)
+                        mat[row * N + col] = acc[i * BD + j];
+                }
+        }
+
+        int key_bits(long long cn)
+        {
+            const unsigned long long top = (unsigned long long)cn * (unsigned long long)cn;
+            int bits = 1;
+            while (bits < 64 && (top >> bits) != 0)
+                ++bits;
+            return bits;
+        }
+
+        // The record lists of every coarse level (once per coarse space).
+        void build_coarse_sums(MasDevice &M, const BankedMatrix &A, const int *d_node_real, cudaStream_t s)
+        {
+            const long long cn = std::max(M.coarse_nodes, 1);
+            const int nodes = A.banks * 32;
+            for (int l = 0; l < MAX_COARSE; ++l)
+            {
+                MasDevice::CoarseSum &cs = M.csum[l];
+                cs.src.reset();
+                cs.ptr.reset();
+                cs.pair.reset();
+                cs.vals.reset();
+                cs.targets = 0;
+                cs.records = 0;
+                if (l >= M.level_num)
+                    continue;
+                long long R = 0;
+                DevBuf<long long> keys, pay;
+                if (l == 0)
+                {
+                    DevBuf<long long> cnt, off;
+                    cnt.alloc((size_t)nodes + 1, "MAS coarse_sums");
+                    off.alloc((size_t)nodes + 1, "MAS coarse_sums");
+                    cuda_check(cudaMemsetAsync(cnt.get(), 0, cnt.bytes(), s), "memset");
+                    if (nodes > 0)
+                        k_fine_pair_count<<<div_up(nodes, 256), 256, 0, s>>>(A.view(), d_node_real, cnt.get());
+                    cuda_check(cudaGetLastError(), "pair count launch");
+                    exclusive_scan(cnt.get(), off.get(), nodes + 1, s);
+                    cuda_check(cudaMemcpy(&R, off.get() + nodes, sizeof(long long), cudaMemcpyDeviceToHost), "count");
+                    keys.alloc((size_t)std::max(R, 1LL), "MAS coarse_sums");
+                    pay.alloc((size_t)std::max(R, 1LL), "MAS coarse_sums");
+                    if (nodes > 0)
+                        k_fine_pair_emit<<<div_up(nodes, 256), 256, 0, s>>>(A.view(), d_node_real, M.map.get(), off.get(),
+                                                                            cn, keys.get(), pay.get());
+                    cuda_check(cudaGetLastError(), "pair emit launch");
+                }
+                else
+                {
+                    const MasDevice::CoarseSum &pv = M.csum[l - 1];
+                    R = pv.targets;
+                    keys.alloc((size_t)std::max(R, 1LL), "MAS coarse_sums");
+                    pay.alloc((size_t)std::max(R, 1LL), "MAS coarse_sums");
+                    if (R > 0)
+                        k_coarse_pair_emit<<<div_up((int)R, 256), 256, 0, s>>>(pv.pair.get(), pv.targets, M.parent.get(),
+                                                                               cn, keys.get(), pay.get());
+                    cuda_check(cudaGetLastError(), "coarse pair emit launch");
+                }
+                if (R == 0)
+                    continue;
+                if (R > 2147483000LL)
+                    throw Error(ERR_INVALID, "[MAS] coarse assembly: too many block pairs");
+                // Stable radix sort by target: records keep their emission order within a target.
+                DevBuf<long long> keys_s;
+                keys_s.alloc((size_t)R, "MAS coarse_sums");
+                cs.src.alloc((size_t)R, "MAS coarse_sums");
+                const int bits = key_bits(cn);
+                size_t tb = 0;
+                cuda_check(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys.get(), keys_s.get(), pay.get(), cs.src.get(),
+                                                           (int)R, 0, bits, s),
+                           "sort size");
+                DevBuf<unsigned char> tmp;
+                tmp.alloc(std::max<size_t>(tb, 1), "MAS coarse_sums sort");
+                cuda_check(cub::DeviceRadixSort::SortPairs(tmp.get(), tb, keys.get(), keys_s.get(), pay.get(), cs.src.get(),
+                                                           (int)R, 0, bits, s),
+                           "sort");
+                DevBuf<int> head, hidx;
+                head.alloc((size_t)R + 1, "MAS coarse_sums");
+                hidx.alloc((size_t)R + 1, "MAS coarse_sums");
+                const int g1 = (int)((R + 1 + 255) / 256);
+                k_key_heads<<<g1, 256, 0, s>>>(keys_s.get(), R, head.get());
+                cuda_check(cudaGetLastError(), "heads launch");
+                exclusive_scan(head.get(), hidx.get(), (int)R + 1, s);
+                int T = 0;
+                cuda_check(cudaMemcpy(&T, hidx.get() + R, sizeof(int), cudaMemcpyDeviceToHost), "targets");
+                cs.ptr.alloc((size_t)T + 1, "MAS coarse_sums");
+                cs.pair.alloc((size_t)std::max(T, 1), "MAS coarse_sums");
+                k_key_targets<<<g1, 256, 0, s>>>(keys_s.get(), head.get(), hidx.get(), R, cn, cs.ptr.get(), cs.pair.get());
+                cuda_check(cudaGetLastError(), "targets launch");
+                cs.vals.alloc((size_t)std::max(T, 1) * A.bd * A.bd, "MAS coarse_sums");
+                cs.targets = T;
+                cs.records = R;
+                cuda_check(cudaStreamSynchronize(s), "coarse sums");
+            }
+        }
+
         template <int BD, class Out>
         void assemble_and_invert(MasDevice &M, const BankedMatrix &A, const int *d_node_real, Out *out, const int *coff,
                                  cudaStream_t s)
@@ -521,10 +747,16 @@ namespace pmas
                 DevBuf<double> staging;
                 staging.alloc((size_t)M.total_coarse * N * N, "MAS coarse_matrices staging");
                 cuda_check(cudaMemsetAsync(staging.get(), 0, staging.bytes(), s), "memset");
-                k_assemble_coarse<BD><<<div_up(M.nodes, 256), 256, 0, s>>>(A.view(), d_node_real, M.map.get(),
-                                                                          M.level_num, coff[0], coff[1], coff[2],
-                                                                          coff[3], staging.get());
-                cuda_check(cudaGetLastError(), "assemble coarse launch");
+                for (int l = 0; l < M.level_num; ++l)
+                {
+                    const MasDevice::CoarseSum &cs = M.csum[l];
+                    if (cs.targets == 0)
+                        continue;
+                    k_coarse_sum<BD><<<div_up(cs.targets, 256), 256, 0, s>>>(
+                        l == 0, cs.src.get(), cs.ptr.get(), cs.pair.get(), cs.targets, A.view(),
+                        l > 0 ? M.csum[l - 1].vals.get() : nullptr, cs.vals.get(), staging.get());
+                    cuda_check(cudaGetLastError(), "coarse sum launch");
+                }
                 const size_t S = (size_t)inv_stride(BD, M.storage);
                 k_invert_coarse<BD, Out><<<M.total_coarse, 256, smem, s>>>(staging.get(), out + (size_t)M.banks * S,
                                                                           scale + M.banks, M.identity.get(),
@@ -805,6 +1037,7 @@ namespace pmas
         cuda_check(cudaMemsetAsync(M.rc.get(), 0, M.rc.bytes(), s), "memset");
         cuda_check(cudaMemsetAsync(M.zc.get(), 0, M.zc.bytes(), s), "memset");
 
+        build_coarse_sums(M, A, d_node_real, s);
         build_inverses(M, A, d_node_real, storage, coff, s);
     }
 

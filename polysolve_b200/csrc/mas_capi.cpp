@@ -25,6 +25,7 @@
 #include <vector>
 
 #include <cuda_runtime.h>
+#include <omp.h>
 
 #include "mas_internal.h"
 #include "mas_json.h"
@@ -232,6 +233,10 @@ struct mas_solver
     double solve_ms = 0.0, factorize_ms = 0.0;
     std::vector<std::pair<std::string, double>> factorize_phases; // host-clock ms per phase
     DevBuf<double> refresh_vals; // CSC values staging kept across values-only refactorizations
+    // Pinned double buffer for large uploads from pageable host memory (the CSC values).
+    static constexpr size_t STAGE_BYTES = (size_t)16 << 20;
+    char *h_stage = nullptr;
+    cudaEvent_t stage_ev[2] = {nullptr, nullptr};
     int launched_iterations = 0;
 
     std::vector<double> positions;
@@ -309,6 +314,11 @@ struct mas_solver
             cudaFreeHost(h_st);
         if (h_ws)
             cudaFreeHost(h_ws);
+        if (h_stage)
+            cudaFreeHost(h_stage);
+        for (cudaEvent_t e : stage_ev)
+            if (e)
+                cudaEventDestroy(e);
         for (cudaEvent_t e : ws_ev)
             if (e)
                 cudaEventDestroy(e);
@@ -428,6 +438,45 @@ struct mas_solver
         cuda_check(cudaMallocHost(&h_st, 2 * sizeof(PcgState)), "pinned state");
     }
 
+    // Host -> device copy of a large pageable array: host threads copy 16 MB chunks into a pinned
+    // double buffer while the previous chunk's DMA runs (a plain pageable copy goes through one
+    // staging thread of the driver). Small arrays take the plain path.
+    void upload_pageable(void *dst, const void *src, size_t bytes)
+    {
+        if (bytes < 2 * STAGE_BYTES)
+        {
+            cuda_check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream), "upload");
+            return;
+        }
+        if (!h_stage)
+        {
+            cuda_check(cudaMallocHost(&h_stage, 2 * STAGE_BYTES), "pinned staging");
+            for (cudaEvent_t &e : stage_ev)
+                cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+        }
+        const int threads = std::max(1, std::min(8, omp_get_max_threads()));
+        bool used[2] = {false, false};
+        for (size_t off = 0, i = 0; off < bytes; off += STAGE_BYTES, ++i)
+        {
+            const int slot = (int)(i & 1);
+            const size_t len = std::min(STAGE_BYTES, bytes - off);
+            if (used[slot])
+                cuda_check(cudaEventSynchronize(stage_ev[slot]), "staging");
+            char *buf = h_stage + slot * STAGE_BYTES;
+            const char *from = static_cast<const char *>(src) + off;
+#pragma omp parallel for num_threads(threads) schedule(static)
+            for (int t = 0; t < threads; ++t)
+            {
+                const size_t a = len * t / threads, z = len * (t + 1) / threads;
+                std::memcpy(buf + a, from + a, z - a);
+            }
+            cuda_check(cudaMemcpyAsync(static_cast<char *>(dst) + off, buf, len, cudaMemcpyHostToDevice, stream),
+                       "upload");
+            cuda_check(cudaEventRecord(stage_ev[slot], stream), "event");
+            used[slot] = true;
+        }
+    }
+
     // MASSolverImpl::factorize (MASSolver.cu:292-374).
     void factorize(int n_, const int *outer, const int *inner, const double *vals, long long nnz_)
     {
@@ -505,8 +554,7 @@ struct mas_solver
             if (!same_pattern)
                 refresh_vals.reset();
             d_vals.alloc(nnz_ > 0 ? nnz_ : 1, "MAS permuted_bsr input_csc");
-            cuda_check(cudaMemcpyAsync(d_vals.get(), vals, sizeof(double) * nnz_, cudaMemcpyHostToDevice, stream),
-                       "upload values");
+            upload_pageable(d_vals.get(), vals, sizeof(double) * (size_t)nnz_);
             if (same_pattern)
             {
                 rescatter_values(A, nnz_, d_vals.get(), stream);

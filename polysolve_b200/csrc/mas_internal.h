@@ -412,6 +412,20 @@ namespace pmas
         DevBuf<double> inv_scale;
         DevBuf<double> rc, zc;
         DevBuf<int> flag;        // device error flag for the inverses
+        // Deterministic coarse assembly (pattern-dependent, built once per coarse space): at
+        // coarse level l, the blocks of the Galerkin operator S_l over coupled pairs (a <= b) of
+        // level-l nodes (global coarse ids), each the fixed-order sum of its sources (records):
+        // level 0 from the fine blocks of A, level l + 1 from the level-l pairs via the parents.
+        struct CoarseSum
+        {
+            DevBuf<long long> src; // records sorted by target: source index << 2 | rule
+            DevBuf<int> ptr;       // targets + 1 record offsets
+            DevBuf<int2> pair;     // (a, b) of each target
+            DevBuf<double> vals;   // targets * bd * bd block values (refreshed with the values)
+            int targets = 0;
+            long long records = 0;
+        };
+        CoarseSum csum[MAX_COARSE];
         MasView view(double *rc_override = nullptr, double *zc_override = nullptr) const;
     };
 

@@ -426,3 +426,20 @@ def test_isolated_rows_with_general_blocks(ordering):
     xo, oinfo = orc.pcg(b, rel_tol=1e-8, abs_tol=0.0)
     assert s.get_info()["solver_iter"] == oinfo["solver_iter"]
     assert np.linalg.norm(x - xo) <= 1e-6 * np.linalg.norm(xo)
+
+
+def test_factorize_is_deterministic():
+    """The coarse matrices are fixed-order sums (no atomics): two factorizations of the same
+    matrix give bit-identical inverses and solutions."""
+    system = synthetic.elasticity(12, young_sigma=1.0, jitter=0.2, seed=21)
+    b = synthetic.rhs(system.n, seed=21)
+    invs, xs = [], []
+    for _ in range(2):
+        s = make_solver(system, 3)
+        s.factorize(system.scipy())
+        invs.append(s.inverses())
+        x = np.zeros(system.n)
+        s.solve(b, x)
+        xs.append(x)
+    assert np.array_equal(invs[0], invs[1])
+    assert np.array_equal(xs[0], xs[1])
