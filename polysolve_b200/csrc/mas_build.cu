@@ -19,6 +19,7 @@
 //     flag instead of an exception; the result is stored tile-packed in FP64 or FP32.
 
 #include <algorithm>
+#include <mutex>
 #include <cub/cub.cuh>
 #include <type_traits>
 #include <vector>
@@ -69,6 +70,12 @@ namespace pmas
 
     namespace
     {
+        // Upper-triangle element lists of the 32-, 64- and 96-row subdomain matrices, packed
+        // (row << 8 | col) in row-major order: the sweep visits exactly the kept elements without
+        // index arithmetic. Filled once per device (ensure_tri_table).
+        constexpr int TRI_1 = 32 * 33 / 2, TRI_2 = 64 * 65 / 2, TRI_3 = 96 * 97 / 2;
+        __device__ uint16_t g_tri[TRI_1 + TRI_2 + TRI_3];
+        __host__ __device__ constexpr int tri_offset(int bd) { return bd == 1 ? 0 : (bd == 2 ? TRI_1 : TRI_1 + TRI_2); }
         __device__ __forceinline__ int ctz32(unsigned x) { return __ffs(x) - 1; }
 
         // Bitmask closure inside a warp; masks in shared memory (32 per warp). Returns the local
@@ -231,10 +238,12 @@ namespace pmas
                     col[N + t] = ct / piv; // the row scale, one division per row
                 }
                 __syncthreads();
-                for (int e = tid; e < N * N; e += nt)
+                const uint16_t *tri = g_tri + tri_offset(BD);
+                for (int k = tid; k < N * (N + 1) / 2; k += nt)
                 {
-                    const int t = e / N, c = e - t * N;
-                    if (t > c || t == p || c == p)
+                    const unsigned tc = __ldg(tri + k);
+                    const int t = (int)(tc >> 8), c = (int)(tc & 255u);
+                    if (t == p || c == p)
                         continue;
                     const double u = A[t * N + c] - col[N + t] * col[c];
                     if (!isfinite(u))
@@ -820,9 +829,37 @@ namespace pmas
         }
     } // namespace
 
+    namespace
+    {
+        // The element lists, once per device (module data is per device).
+        void ensure_tri_table(cudaStream_t s)
+        {
+            static std::mutex mu;
+            static std::vector<int> done;
+            int dev = 0;
+            cuda_check(cudaGetDevice(&dev), "get device");
+            std::lock_guard<std::mutex> lock(mu);
+            if ((int)done.size() > dev && done[dev])
+                return;
+            std::vector<uint16_t> h;
+            h.reserve(TRI_1 + TRI_2 + TRI_3);
+            for (int n : {32, 64, 96})
+                for (int t = 0; t < n; ++t)
+                    for (int c = t; c < n; ++c)
+                        h.push_back((uint16_t)((t << 8) | c));
+            cuda_check(cudaMemcpyToSymbolAsync(g_tri, h.data(), h.size() * sizeof(uint16_t), 0, cudaMemcpyHostToDevice, s),
+                       "element lists");
+            cuda_check(cudaStreamSynchronize(s), "element lists");
+            if ((int)done.size() <= dev)
+                done.resize(dev + 1, 0);
+            done[dev] = 1;
+        }
+    } // namespace
+
     void build_mas(MasDevice &M, const BankedMatrix &A, const int *d_node_real, int storage, int first_iso_bank,
                    cudaStream_t s)
     {
+        ensure_tri_table(s);
         const int bd = A.bd, banks = A.banks, nodes = A.nodes;
         M.bd = bd;
         M.banks = banks;
