@@ -72,7 +72,9 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seq-steps", type=int, default=20, help="sequence60: steps of the sequence")
     ap.add_argument("--seq-grid", type=int, default=60, help="sequence60: grid edge N (N^3 cells)")
-    ap.add_argument("--workload", default="grid80", choices=["grid80", "batch64", "contact16", "sequence60"],
+    ap.add_argument("--seq-modes", default="all",
+                    help="sequence60: comma-separated starting-guess modes to run (default all)")
+    ap.add_argument("--workload", default="grid80", choices=["grid80", "batch64", "contact16", "sequence60", "refactor60"],
                     help="grid80: the headline 1.6 M DOF solve; batch64: 64 independent uneven systems; "
                          "contact16: the 80^3 mesh with 20,000 contact pairs and 16 right-hand sides; "
                          "sequence60: a 60^3 sequence (new values each step) with warm starts")
@@ -572,6 +574,9 @@ def run_sequence(args) -> None:
     modes = {"plain_fp64": ("zero", None), "zero": ("input", None), "previous": ("input", None),
              "extrapolate": ("input", None), "projection": ("learned", np.zeros(W.PARAMS, dtype=np.float32)),
              "learned": ("learned", W.default_weights())}
+    if args.seq_modes != "all":
+        keep = set(args.seq_modes.split(","))
+        modes = {m: v for m, v in modes.items() if m in keep or m in ("learned",)}
     for mode, (guess, model) in modes.items():
         sv = Solver.create("MAS", "")
         base = PLAIN if mode == "plain_fp64" else CHOSEN
@@ -607,7 +612,8 @@ def run_sequence(args) -> None:
                      "worst_rel": max(r["rel"] for r in out),
                      "factorize_phases_ms_per_step": {k: float(f"{v:.4g}") for k, v in phases.items()}}
         del sv
-    lrn, prev, zero = res["learned"], res["previous"], res["zero"]
+    lrn = res["learned"]
+    prev, zero = res.get("previous", lrn), res.get("zero", lrn)
     out = {
         "metric": SEQ_METRIC, "value": round(lrn["wall_ms"] / S, 3), "unit": "ms/step", "n_gpus": 1, "steps": S,
         "warmup": 3, "ms_per_step": round(lrn["wall_ms"] / S, 3), "higher_is_better": False, "scaling": "weak",
@@ -626,10 +632,62 @@ def run_sequence(args) -> None:
         # solve time per step (warm-start pipeline included) of the chosen configuration against
         # the reference's algorithm (FP64 MAS, x0 = 0) on the same systems and GPU
         "solve_speedup_vs_plain_fp64": round(res["plain_fp64"]["solve_ms"] /
-                                             max(lrn["solve_ms"] + lrn["warm_start_ms"], 1e-9), 3),
+                                             max(lrn["solve_ms"] + lrn["warm_start_ms"], 1e-9), 3)
+        if "plain_fp64" in res else None,
         "e2e": {"value": round(lrn["wall_ms"] / S, 3), "unit": "ms/step",
                 "h2d_bytes_per_step": int(8 * systems[0].shape[0] + 12 * systems[0].nnz),
                 "d2h_bytes_per_step": int(8 * systems[0].shape[0])},
+    }
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def run_refactor(args) -> None:
+    """The Newton-step factorization: steps 0 and 1 of the 60^3 sequence (same pattern, new
+    values), one full factorize, then W + K values-only refactorizations alternating between the
+    two (host arrays, as the reference's factorize(A) takes them); value = ms per values-only
+    factorize (host clock, the call is synchronous), with the per-phase split."""
+    import torch
+
+    from polysolve_b200 import Solver, synthetic
+
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    rank = int(os.environ.get("RANK", "0"))
+    N = args.seq_grid
+    s0, _ = synthetic.workload_sequence60(0, seed=args.seed, N=N)
+    s1, _ = synthetic.workload_sequence60(1, seed=args.seed, N=N)
+    A = [s0.scipy(), s1.scipy()]
+    sv = Solver.create("MAS", "")
+    sv.set_parameters({"MAS": dict(CHOSEN)})
+    sv.set_positions(s0.positions)
+    sv.analyze_pattern(A[0], A[0].shape[0])
+    t0 = time.perf_counter()
+    sv.factorize(A[0])
+    full_ms = (time.perf_counter() - t0) * 1000.0
+    full_phases = sv.get_info({})["factorize_phases_ms"]
+    for k in range(args.warmup):
+        sv.factorize(A[(k + 1) % 2])
+    times, phases = [], {}
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        sv.factorize(A[(args.warmup + k + 1) % 2])
+        times.append((time.perf_counter() - t0) * 1000.0)
+        for name, ms in sv.get_info({})["factorize_phases_ms"].items():
+            phases[name] = phases.get(name, 0.0) + ms / args.steps
+    ms = sum(times) / len(times)
+    nnz = A[0].nnz
+    out = {
+        "metric": "ms per values-only refactorization (same pattern, new values) at 680K DOF",
+        "value": round(ms, 3), "unit": "ms/factorize", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms, 3), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64 values, fp16 inverses", "data": "synthetic (60^3 sequence steps 0 and 1)",
+        "config": {"workload": f"{N}^3 sequence, {A[0].shape[0]} DOF, nnz {nnz}",
+                   "timing": "host clock around the synchronous factorize call, host CSC arrays"},
+        "phases_ms": {k: round(v, 3) for k, v in phases.items()},
+        "first_factorize_ms": round(full_ms, 3),
+        "first_factorize_phases_ms": {k: round(v, 3) for k, v in full_phases.items()},
+        "e2e": {"value": round(ms, 3), "unit": "ms/factorize", "h2d_bytes_per_step": int(8 * nnz),
+                "d2h_bytes_per_step": 0},
     }
     if rank == 0:
         print(json.dumps(out), flush=True)
@@ -691,6 +749,9 @@ def main():
         return
     if args.workload == "sequence60" and args.impl != "reference":
         run_sequence(args)
+        return
+    if args.workload == "refactor60" and args.impl != "reference":
+        run_refactor(args)
         return
     if args.impl == "reference":
         run_reference(args)
