@@ -354,7 +354,7 @@ def run_batch(args) -> None:
     one stream (the reference's one-solve-per-call pattern) on this rank's share."""
     import torch
 
-    from polysolve_b200 import Solver, batch, solve_batch, solve_batch_device, synthetic
+    from polysolve_b200 import Solver, autotune, batch, solve_batch, solve_batch_device, synthetic
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -396,8 +396,11 @@ def run_batch(args) -> None:
         if dist is not None:
             dist.barrier()
 
+    # graph length and host threads for these systems (untimed)
+    tuned = autotune.tune_batch(solvers, bptr, xptr, ns, repeats=2)
+    threads = int(tuned["threads"])
     for _ in range(max(args.warmup, 3)):
-        solve_batch_device(solvers, bptr, xptr, ns)
+        solve_batch_device(solvers, bptr, xptr, ns, threads=threads)
     torch.cuda.synchronize()
     launches0 = sum(sv.get_info()["kernel_launches_total"] for sv in solvers)
     clocks = Clocks(local)
@@ -406,7 +409,7 @@ def run_batch(args) -> None:
     clocks.start()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        solve_batch_device(solvers, bptr, xptr, ns)
+        solve_batch_device(solvers, bptr, xptr, ns, threads=threads)
     torch.cuda.synchronize()
     dt_ms = (time.perf_counter() - t0) * 1000.0
     barrier()
@@ -432,7 +435,7 @@ def run_batch(args) -> None:
     hbs = [b for _, _, b in systems]
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        solve_batch(solvers, hbs)
+        solve_batch(solvers, hbs, threads=threads)
     e2e_ms = (time.perf_counter() - t0) * 1000.0 / args.steps
     te = torch.tensor([e2e_ms, seq_ms], device="cuda", dtype=torch.float64)
     if dist is not None:
@@ -455,6 +458,8 @@ def run_batch(args) -> None:
         "e2e": {"value": round(float(te[0].item()), 3), "unit": "ms/batch",
                 "h2d_bytes_per_step": int(8 * sum(ns)), "d2h_bytes_per_step": int(8 * sum(ns))},
         "gpu_launches": int(gpu_launches), "clocks": clk,
+        "autotune": {"poll_period": tuned["poll_period"], "threads": threads,
+                     "tables": tuned.get("tables", {})},
     }
     if rank == 0:
         print(json.dumps(out), flush=True)

@@ -746,14 +746,19 @@ namespace pmas
             cuda_check(cudaFuncSetAttribute(k_invert_coarse<BD, Out>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)smem),
                        "invert smem attribute");
+            if (!M.inv_ev[0])
+                for (cudaEvent_t &e : M.inv_ev)
+                    cuda_check(cudaEventCreate(&e), "event");
+            cuda_check(cudaEventRecord(M.inv_ev[0], s), "event");
             if (M.banks > 0)
             {
                 k_assemble_invert_lv0<BD, Out><<<M.banks, 256, smem, s>>>(A.view(), d_node_real, out, scale, M.flag.get());
                 cuda_check(cudaGetLastError(), "assemble lv0 launch");
             }
+            cuda_check(cudaEventRecord(M.inv_ev[1], s), "event");
             if (M.total_coarse > 0)
             {
-                DevBuf<double> staging;
+                DevBuf<double> &staging = M.staging;
                 staging.alloc((size_t)M.total_coarse * N * N, "MAS coarse_matrices staging");
                 cuda_check(cudaMemsetAsync(staging.get(), 0, staging.bytes(), s), "memset");
                 for (int l = 0; l < M.level_num; ++l)
@@ -766,13 +771,16 @@ namespace pmas
                         l > 0 ? M.csum[l - 1].vals.get() : nullptr, cs.vals.get(), staging.get());
                     cuda_check(cudaGetLastError(), "coarse sum launch");
                 }
+                cuda_check(cudaEventRecord(M.inv_ev[2], s), "event");
                 const size_t S = (size_t)inv_stride(BD, M.storage);
                 k_invert_coarse<BD, Out><<<M.total_coarse, 256, smem, s>>>(staging.get(), out + (size_t)M.banks * S,
                                                                           scale + M.banks, M.identity.get(),
                                                                           M.flag.get());
                 cuda_check(cudaGetLastError(), "invert coarse launch");
-                cuda_check(cudaStreamSynchronize(s), "coarse inverse");
             }
+            else
+                cuda_check(cudaEventRecord(M.inv_ev[2], s), "event");
+            cuda_check(cudaEventRecord(M.inv_ev[3], s), "event");
         }
     } // namespace
 
@@ -824,6 +832,8 @@ namespace pmas
             int h_flag = 0;
             cuda_check(cudaMemcpyAsync(&h_flag, M.flag.get(), sizeof(int), cudaMemcpyDeviceToHost, s), "flag");
             cuda_check(cudaStreamSynchronize(s), "mas build");
+            for (int i = 0; i < 3; ++i)
+                cuda_check(cudaEventElapsedTime(&M.inverse_ms[i], M.inv_ev[i], M.inv_ev[i + 1]), "event time");
             if (h_flag)
                 throw Error(ERR_INVERSE, "[MAS] MAS packed inverse failed.");
         }

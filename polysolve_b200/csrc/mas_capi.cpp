@@ -586,6 +586,9 @@ struct mas_solver
             // Values only: the coarse space, buffers and captured graphs stay valid.
             refresh_mas_values(mas, A, d_node_real.get(), p.storage, stream); // syncs, checks pivots
             phase("mas_inverses");
+            factorize_phases.emplace_back("gpu_level0_inverses", mas.inverse_ms[0]);
+            factorize_phases.emplace_back("gpu_coarse_sums", mas.inverse_ms[1]);
+            factorize_phases.emplace_back("gpu_coarse_inverses", mas.inverse_ms[2]);
             factorized = true;
             factorize_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
             return;

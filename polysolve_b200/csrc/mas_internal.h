@@ -426,6 +426,16 @@ namespace pmas
             long long records = 0;
         };
         CoarseSum csum[MAX_COARSE];
+        DevBuf<double> staging;  // coarse matrices before inversion (kept across refreshes)
+        // GPU time of the last assembly + inversion: level 0, coarse sums, coarse inverses (ms).
+        float inverse_ms[3] = {0.f, 0.f, 0.f};
+        cudaEvent_t inv_ev[4] = {nullptr, nullptr, nullptr, nullptr};
+        ~MasDevice()
+        {
+            for (cudaEvent_t &e : inv_ev)
+                if (e)
+                    cudaEventDestroy(e);
+        }
         MasView view(double *rc_override = nullptr, double *zc_override = nullptr) const;
     };
 

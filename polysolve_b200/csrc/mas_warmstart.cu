@@ -223,9 +223,12 @@ namespace pmas
                                                          const float *__restrict__ feat, const float *__restrict__ prm,
                                                          const WsState *ws, __nv_bfloat162 *__restrict__ h)
         {
+            // W_in transposed (wsm[f * H + o]): lanes read consecutive words, no bank conflicts.
             __shared__ float wsm[H * F + H];
-            for (int i = threadIdx.x; i < H * F + H; i += WT)
-                wsm[i] = prm[OFF_WIN + i];
+            for (int i = threadIdx.x; i < H * F; i += WT)
+                wsm[(i % F) * H + i / F] = prm[OFF_WIN + i];
+            for (int i = threadIdx.x; i < H; i += WT)
+                wsm[H * F + i] = prm[OFF_BIN + i];
             __syncthreads();
             const Norms nm = norms(ws);
             const int lane = threadIdx.x & 31;
@@ -262,8 +265,9 @@ namespace pmas
 #pragma unroll
                     for (int i = 0; i < F; ++i)
                     {
-                        a0 = fmaf(wsm[o0 * F + i], f[i], a0);
-                        a1 = fmaf(wsm[o1 * F + i], f[i], a1);
+                        const float2 wv = *reinterpret_cast<const float2 *>(&wsm[i * H + o0]);
+                        a0 = fmaf(wv.x, f[i], a0);
+                        a1 = fmaf(wv.y, f[i], a1);
                     }
                     out = make_float2(fmaxf(a0, 0.f), fmaxf(a1, 0.f));
                 }
@@ -309,47 +313,74 @@ namespace pmas
             }
             if (threadIdx.x < H)
                 bias[threadIdx.x] = bl[threadIdx.x];
-            // Gather: warp w fills rows 16 w .. 16 w + 15; lane l holds hidden units 2 l, 2 l + 1.
-            const __nv_bfloat162 *h2 = reinterpret_cast<const __nv_bfloat162 *>(hin);
-            for (int rr = 0; rr < 16; ++rr)
+            // Gather: warp w fills rows 16 w .. 16 w + 15, four at a time: lane group q = lane / 8
+            // takes one row, lane gl = lane % 8 its hidden units 8 gl .. 8 gl + 7 (16-byte loads),
+            // so four rows' neighbour loads are in flight together. Every lane runs the warp's
+            // longest row; slots past a row's end carry w = 0 and the row's own (valid) index.
+            const uint4 *h8 = reinterpret_cast<const uint4 *>(hin);
+            const int gq = lane >> 3, gl = lane & 7;
+            int my_len = 0;
+            long long my_s0 = 0;
             {
-                const int r = warp * 16 + rr;
-                const int u = blockIdx.x * TILE + r;
-                __nv_bfloat162 self = __float2bfloat162_rn(0.f);
-                float2 acc = make_float2(0.f, 0.f);
+                const int u = blockIdx.x * TILE + warp * 16 + (lane & 15);
                 if (u < nodes && node_real(A.rowlen, diag_slot, u))
                 {
-                    self = h2[(long long)u * (H / 2) + lane];
-                    const int bank = u >> 5, ln = u & 31;
-                    const long long s0 = A.slice[bank];
-                    const int len = A.rowlen[u];
-                    for (int k0 = 0; k0 < len; k0 += 32)
+                    my_len = A.rowlen[u];
+                    my_s0 = A.slice[u >> 5];
+                }
+            }
+            for (int rb = 0; rb < 16; rb += 4)
+            {
+                const int rl = rb + gq;
+                const int r = warp * 16 + rl;
+                const int u = blockIdx.x * TILE + r;
+                const int len = __shfl_sync(FULL, my_len, rl);
+                const long long s0 = __shfl_sync(FULL, my_s0, rl);
+                int maxlen = len;
+#pragma unroll
+                for (int o = 8; o < 32; o <<= 1)
+                    maxlen = max(maxlen, __shfl_xor_sync(FULL, maxlen, o));
+                float acc[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i)
+                    acc[i] = 0.f;
+                uint4 self = make_uint4(0u, 0u, 0u, 0u);
+                if (len > 0)
+                    self = h8[(long long)u * (H / 8) + gl];
+                const int uu = (u < nodes) ? u : 0;
+                for (int k0 = 0; k0 < maxlen; k0 += 8)
+                {
+                    const int kk = k0 + gl;
+                    int col = uu;
+                    float w = 0.f;
+                    if (kk < len)
                     {
-                        const int kk = k0 + lane;
-                        int col = 0;
-                        float w = 0.f;
-                        if (kk < len)
+                        col = A.cols[(s0 + kk) * 32 + (u & 31)];
+                        w = wslot[(s0 + kk) * 32 + (u & 31)];
+                    }
+#pragma unroll
+                    for (int j = 0; j < 8; ++j)
+                    {
+                        const int cj = __shfl_sync(FULL, col, j, 8);
+                        const float wj = __shfl_sync(FULL, w, j, 8);
+                        const uint4 hv = h8[(long long)cj * (H / 8) + gl];
+                        const __nv_bfloat162 *hb = reinterpret_cast<const __nv_bfloat162 *>(&hv);
+#pragma unroll
+                        for (int i = 0; i < 4; ++i)
                         {
-                            col = A.cols[(s0 + kk) * 32 + ln];
-                            w = wslot[(s0 + kk) * 32 + ln];
-                        }
-                        const int cnt = min(32, len - k0);
-#pragma unroll 4
-                        for (int j = 0; j < cnt; ++j)
-                        {
-                            const int cj = __shfl_sync(FULL, col, j);
-                            const float wj = __shfl_sync(FULL, w, j);
-                            if (wj != 0.f)
-                            {
-                                const float2 hv = __bfloat1622float2(h2[(long long)cj * (H / 2) + lane]);
-                                acc.x = fmaf(wj, hv.x, acc.x);
-                                acc.y = fmaf(wj, hv.y, acc.y);
-                            }
+                            const float2 f2 = __bfloat1622float2(hb[i]);
+                            acc[2 * i] = fmaf(wj, f2.x, acc[2 * i]);
+                            acc[2 * i + 1] = fmaf(wj, f2.y, acc[2 * i + 1]);
                         }
                     }
                 }
-                *reinterpret_cast<__nv_bfloat162 *>(&T[r * TS + 2 * lane]) = self;
-                *reinterpret_cast<__nv_bfloat162 *>(&T[r * TS + H + 2 * lane]) = __float22bfloat162_rn(acc);
+                uint4 m8;
+                __nv_bfloat162 *mb = reinterpret_cast<__nv_bfloat162 *>(&m8);
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    mb[i] = __float22bfloat162_rn(make_float2(acc[2 * i], acc[2 * i + 1]));
+                *reinterpret_cast<uint4 *>(&T[r * TS + 8 * gl]) = self;
+                *reinterpret_cast<uint4 *>(&T[r * TS + H + 8 * gl]) = m8;
             }
             __syncthreads();
 

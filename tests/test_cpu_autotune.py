@@ -1,0 +1,39 @@
+"""The autotuner's search and cache logic with stand-in solvers and timed callables (no GPU)."""
+
+import time
+
+from polysolve_b200 import autotune
+
+
+class FakeSolver:
+    def __init__(self):
+        self.params = {}
+
+    def set_parameters(self, p):
+        self.params.update(p["MAS"])
+
+
+def test_poll_period_picks_the_fastest_and_leaves_it_set():
+    solvers = [FakeSolver(), FakeSolver()]
+    cost = {5: 0.03, 10: 0.005, 20: 0.02}
+
+    def run():
+        time.sleep(cost[solvers[0].params["poll_period"]])
+
+    res = autotune.tune_poll_period(solvers, run, candidates=(5, 10, 20), repeats=2)
+    assert res["best"] == 10 and set(res["ms"]) == {5, 10, 20}
+    assert all(s.params["poll_period"] == 10 for s in solvers)
+
+
+def test_threads_pick_the_fastest():
+    res = autotune.tune_batch_threads(lambda t: time.sleep(0.004 * abs(t - 8) + 0.002), candidates=(2, 8, 32),
+                                      repeats=2)
+    assert res["best"] == 8
+
+
+def test_cache_round_trip(tmp_path):
+    path = tmp_path / "tune.json"
+    cache = {autotune.signature([30, 10]): {"poll_period": 20, "threads": 16, "tables": {}}}
+    autotune._store_cache(str(path), cache)
+    assert autotune._load_cache(str(path)) == cache
+    assert autotune.signature([10, 30]) == autotune.signature([30, 10])
