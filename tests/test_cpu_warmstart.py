@@ -39,8 +39,6 @@ def test_weight_file_round_trip(tmp_path):
 
 
 def test_shipped_weights_load():
-    if not W.DEFAULT_WEIGHTS.exists():
-        pytest.skip("shipped weights not generated yet")
     prm = W.default_weights()
     assert prm.shape == (W.PARAMS,) and np.all(np.isfinite(prm))
 

@@ -46,8 +46,6 @@ def test_prediction_matches_oracle(params):
     b, x1, x2 = rhs[2], xs[1], xs[0]
     s = _solver(systems[2])
     s.factorize(systems[2].scipy())
-    if params == "shipped" and not W.DEFAULT_WEIGHTS.exists():
-        pytest.skip("shipped weights not generated yet")
     prm = _random_params(5) if params == "random" else W.default_weights()
     s.set_warm_start_model(prm)
     d = s.debug_warm_start(b, x1, x2)
@@ -69,8 +67,6 @@ def test_prediction_matches_oracle(params):
 
 
 def test_learned_sequence_converges_and_beats_extrapolation():
-    if not W.DEFAULT_WEIGHTS.exists():
-        pytest.skip("shipped weights not generated yet")
     N, steps, seed = 12, 8, 3
     systems = [synthetic.workload_sequence60(k, seed=seed, N=N) for k in range(steps)]
     mats, rhs = [s.scipy() for s, _ in systems], [b for _, b in systems]
