@@ -264,6 +264,15 @@ def run_ours(args) -> None:
     plain_graph_ms = p0.elapsed_time(p1) / psteps
     x_plain = dx.cpu().numpy()
     relres_plain = float(np.linalg.norm(A @ x_plain - b) / np.linalg.norm(b))
+    # FP64 reference solution (CHOLMOD is unavailable on this box): the plain FP64 MAS-PCG to a
+    # relative residual of 1e-13; the chosen solution's relative error against it.
+    plain.set_parameters({"MAS": {"relative_tolerance": 1e-13, "max_iter": 20000}})
+    plain.solve_device(db.data_ptr(), dx.data_ptr(), n)
+    torch.cuda.synchronize()
+    x_ref = dx.cpu().numpy()
+    relres_ref = float(np.linalg.norm(A @ x_ref - b) / np.linalg.norm(b))
+    sol_err = float(np.linalg.norm(x - x_ref) / np.linalg.norm(x_ref))
+    sol_err_plain = float(np.linalg.norm(x_plain - x_ref) / np.linalg.norm(x_ref))
 
     # End to end through the public host API, pinned host buffers.
     hb = torch.from_numpy(b).pin_memory()
@@ -321,6 +330,9 @@ def run_ours(args) -> None:
         "plain_fp64_ms": round(plain_ms, 4), "plain_fp64_iterations": pinfo["solver_iter"],
         "plain_fp64_relative_residual": relres_plain, "speedup_vs_plain_fp64": round(plain_ms / ms_per_step, 3),
         "plain_fp64_graphs_ms": round(plain_graph_ms, 4),
+        "solution_relative_error": sol_err, "plain_fp64_solution_relative_error": sol_err_plain,
+        "fp64_reference": f"plain FP64 MAS-PCG to relative residual 1e-13 (reached {relres_ref:.1e}); "
+                          "CHOLMOD unavailable on this box",
         "factorize_s": round(fact_s, 3),
         "e2e": {"value": round(e2e_value, 4), "unit": UNIT, "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
         "gpu_launches": int(gpu_launches),
@@ -521,6 +533,18 @@ def run_contact16(args) -> None:
     for c in range(R):
         sv.solve(B[c], x)
     seq = (time.perf_counter() - t0) * 1000.0
+    # FP64 reference solutions (CHOLMOD is unavailable on this box): plain FP64 MAS-PCG to a
+    # relative residual of 1e-13 for every right-hand side; the worst relative solution error.
+    ref = Solver.create("MAS", "")
+    ref.set_parameters({"MAS": dict(PLAIN, relative_tolerance=1e-13, max_iter=20000)})
+    ref.set_positions(system.positions)
+    ref.analyze_pattern(A, n)
+    ref.factorize(A)
+    sol_err = 0.0
+    for c in range(R):
+        ref.solve(B[c], x)
+        sol_err = max(sol_err, float(np.linalg.norm(X[c] - x) / np.linalg.norm(x)))
+    del ref
     t = torch.tensor([dt, seq], device="cuda", dtype=torch.float64)
     if dist is not None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -534,6 +558,9 @@ def run_contact16(args) -> None:
         "config": {"workload": f"{args.grid}^3 + contact, {n} DOF, 16 right-hand sides in groups of 4",
                    "parallelism": f"replicas x{world}", "timing": "host clock around the public call (host arrays)"},
         "rhs_iterations": info.get("rhs_iterations"), "worst_relative_residual": worst,
+        "worst_solution_relative_error": sol_err,
+        "fp64_reference": "plain FP64 MAS-PCG to relative residual 1e-13 per right-hand side "
+                          "(CHOLMOD unavailable on this box)",
         "one_by_one_ms": round(float(t[1].item()), 3),
         "speedup_vs_one_by_one": round(float(t[1].item()) / float(t[0].item()), 3),
         "e2e": {"value": round(value, 3), "unit": "ms/16 RHS", "h2d_bytes_per_step": int(8 * n * R),
