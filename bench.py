@@ -337,7 +337,12 @@ def run_ours(args) -> None:
         "e2e": {"value": round(e2e_value, 4), "unit": UNIT, "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
         "gpu_launches": int(gpu_launches),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": None, "kernel": "spmv_pap",
+                     "frac": round(achieved / peak, 4),
+                     # DRAM read + write of one spmv_pap launch on this workload from an ncu capture
+                     # (dram__bytes_read.sum + dram__bytes_write.sum: 613.98 + 5.58 MB)
+                     "traffic": 619.56e6 if args.grid == 80 else None,
+                     "traffic_source": "ncu capture of k_spmv<3,PAP> on the 80^3 workload" if args.grid == 80 else None,
+                     "kernel": "spmv_pap",
                      "algorithmic_bytes_per_launch": spmv_b, "launch_ms": round(spmv_launch_ms, 5),
                      "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured copy)" if peaks else "fallback 6650 GB/s"},
         "mas_apply": {"launch_ms": round(symv_launch_ms, 5), "algorithmic_bytes_per_launch": mas_b,
