@@ -224,42 +224,121 @@ namespace pmas
                 if (A[i * N + i] == 0.0)
                     A[i * N + i] = 1.0;
             __syncthreads();
-            // Only the upper triangle (t <= c) is kept up to date: consecutive threads touch
-            // consecutive columns of one row, so shared-memory accesses are conflict-free.
-            for (int p = 0; p < N; ++p)
+            // Blocked sweep (KB pivots per block; both triangles kept exactly symmetric):
+            //  1. warp 0 sweeps the KB x KB pivot block pivot by pivot and records, per pivot q, its
+            //     value d_q, pivot-row entries r_t = A[q][t] and scaled entries s_t = r_t / d_q;
+            //  2. every column c outside the block replays those pivots on its KB panel entries
+            //     (one thread per column, registers) with the single-pivot rule;
+            //  3. every thread applies the block's rank-KB update A[t][c] -= sum_q A[t][q] W[q][c]
+            //     to the upper triangle outside the block (A[t][q]: the block's columns, untouched
+            //     so far; W: the swept panel) and mirrors it; 4. the panel is mirrored into the
+            //     block's columns. The same operator as N single pivots (upper-triangle products
+            //     for both triangles), with N / KB rounds of block-wide barriers instead of N.
+            constexpr int KB = 8;
+            constexpr int NCOEF = KB * (2 * KB + 1);
+            static_assert(N % KB == 0, "pivot blocks");
+            // The pivot records live in col (2 N doubles) when it is large enough.
+            __shared__ double coef_extra[2 * N >= NCOEF ? 1 : NCOEF];
+            double *coef = 2 * N >= NCOEF ? col : coef_extra;
+            const int lane = tid & 31, warp = tid >> 5;
+            const uint16_t *tri = g_tri + tri_offset(BD);
+            double *cd = coef;                // [KB] pivots
+            double *cr = coef + KB;           // [KB][KB] pivot-row entries (0 at the pivot)
+            double *cs = coef + KB + KB * KB; // [KB][KB] scaled entries
+            for (int b0 = 0; b0 < N; b0 += KB)
             {
-                const double piv = A[p * N + p];
-                if (tid == 0 && (!isfinite(piv) || piv == 0.0))
-                    bad = 1;
-                for (int t = tid; t < N; t += nt)
+                if (warp == 0)
                 {
-                    const double ct = (t == p) ? 0.0 : (t < p ? A[t * N + p] : A[p * N + t]);
-                    col[t] = ct;
-                    col[N + t] = ct / piv; // the row scale, one division per row
+                    for (int qq = 0; qq < KB; ++qq)
+                    {
+                        const int q = b0 + qq;
+                        const double d = A[q * N + q];
+                        if (lane == 0 && (!isfinite(d) || d == 0.0))
+                            bad = 1;
+                        if (lane < KB)
+                        {
+                            const double rq = (lane == qq) ? 0.0 : A[q * N + b0 + lane];
+                            cr[qq * KB + lane] = rq;
+                            cs[qq * KB + lane] = rq / d; // the row scale, one division per row
+                        }
+                        if (lane == 0)
+                            cd[qq] = d;
+                        __syncwarp();
+                        for (int e = lane; e < KB * KB; e += 32)
+                        {
+                            const int ti = e / KB, ci = e % KB;
+                            double u;
+                            if (ti == qq)
+                                u = (ci == qq) ? -1.0 / d : cs[qq * KB + ci];
+                            else if (ci == qq)
+                                u = cs[qq * KB + ti];
+                            else
+                                u = A[(b0 + ti) * N + b0 + ci] -
+                                    (ti <= ci ? cs[qq * KB + ti] * cr[qq * KB + ci] : cs[qq * KB + ci] * cr[qq * KB + ti]);
+                            if (!isfinite(u))
+                                bad = 1;
+                            A[(b0 + ti) * N + b0 + ci] = u;
+                        }
+                        __syncwarp();
+                    }
                 }
                 __syncthreads();
-                const uint16_t *tri = g_tri + tri_offset(BD);
+                for (int c = tid; c < N; c += nt)
+                {
+                    if ((unsigned)(c - b0) < (unsigned)KB)
+                        continue;
+                    double v[KB];
+#pragma unroll
+                    for (int i = 0; i < KB; ++i)
+                        v[i] = A[(b0 + i) * N + c];
+                    int badc = 0;
+#pragma unroll
+                    for (int qq = 0; qq < KB; ++qq)
+                    {
+                        const double d = cd[qq];
+                        const double a = v[qq];      // A[q][c] before pivot q
+                        const double as = a / d;     // its row scale
+#pragma unroll
+                        for (int i = 0; i < KB; ++i)
+                        {
+                            const int t = b0 + i;
+                            if (i == qq)
+                                v[i] = as;
+                            else
+                                v[i] = v[i] - (t <= c ? cs[qq * KB + i] * a : as * cr[qq * KB + i]);
+                        }
+                    }
+#pragma unroll
+                    for (int i = 0; i < KB; ++i)
+                    {
+                        badc |= !isfinite(v[i]);
+                        A[(b0 + i) * N + c] = v[i];
+                    }
+                    if (badc)
+                        bad = 1;
+                }
+                __syncthreads();
                 for (int k = tid; k < N * (N + 1) / 2; k += nt)
                 {
                     const unsigned tc = __ldg(tri + k);
                     const int t = (int)(tc >> 8), c = (int)(tc & 255u);
-                    if (t == p || c == p)
+                    if ((unsigned)(t - b0) < (unsigned)KB || (unsigned)(c - b0) < (unsigned)KB)
                         continue;
-                    const double u = A[t * N + c] - col[N + t] * col[c];
+                    double u = A[t * N + c];
+#pragma unroll
+                    for (int qq = 0; qq < KB; ++qq)
+                        u -= A[t * N + b0 + qq] * A[(b0 + qq) * N + c];
                     if (!isfinite(u))
                         bad = 1;
                     A[t * N + c] = u;
+                    A[c * N + t] = u;
                 }
                 __syncthreads();
-                for (int t = tid; t < N; t += nt)
+                for (int e = tid; e < KB * N; e += nt)
                 {
-                    const double u = (t == p) ? -1.0 / piv : col[N + t];
-                    if (!isfinite(u))
-                        bad = 1;
-                    else if (t <= p)
-                        A[t * N + p] = u;
-                    else
-                        A[p * N + t] = u;
+                    const int q = b0 + e / N, t = e % N;
+                    if ((unsigned)(t - b0) >= (unsigned)KB)
+                        A[t * N + q] = A[q * N + t];
                 }
                 __syncthreads();
             }
