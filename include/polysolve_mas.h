@@ -100,10 +100,10 @@ int mas_factorize_csc(mas_solver *h, int n, const int *outer, const int *inner, 
 int mas_solve(mas_solver *h, const double *b, double *x, int n);
 
 /* New: learned warm start for sequences of systems with one pattern (initial_guess
- * "learned"). The solver keeps its last two solutions on the device; the next solve starts from
- * the energy-minimising combination of x_{k-1}, x_{k-1} - x_{k-2} and a message-passing
- * network's correction (falling back to x_{k-1}), computed on the GPU from b, the diagonal
- * blocks and the kept solutions. block_dim 3 only. The reference always starts from x0 = 0
+ * "learned"). The solver keeps its last four solutions on the device; the next solve starts
+ * from the energy-minimising combination of x_{k-1}, the differences x_{k-i} - x_{k-i-1} and a
+ * message-passing network's correction (falling back to x_{k-1}), computed on the GPU from b,
+ * the diagonal blocks and the kept solutions. block_dim 3 only. The reference always starts from x0 = 0
  * (MASSolver.cu:395-398); its caller refactorizes and solves every Newton step
  * (Newton.cpp:173-214).
  * params: MAS_WS_PARAMS float32 in the .psws order (polysolve_b200/warmstart.py). */
@@ -187,12 +187,13 @@ int mas_debug_apply(mas_solver *h, const double *r, double *z, int len);
  * No reference counterpart. */
 int mas_debug_apply_multi(mas_solver *h, const double *rin, double *zout, int len);
 int mas_debug_spmv_multi(mas_solver *h, const double *xin, double *yout, int len);
-/* Test hook of the learned warm start: the prediction for caller-order b, x1 (= x_{k-1}) and
- * x2 (= x_{k-2}) without a solve. Outputs (each may be NULL): c_out[n] the network's correction,
- * x0_out[n] the starting guess, features_out[nverts * 16] the raw per-vertex features,
- * state_out[21] = feature sums (5), Galerkin matrix and right-hand side (9), coefficients (3),
- * energy of x0, energy of x1, fallback flag, kept basis vectors. */
-int mas_debug_warm_start(mas_solver *h, const double *b, const double *x1, const double *x2, double *c_out,
+/* Test hook of the learned warm start: the prediction for caller-order b and nhist (2 to 4) kept
+ * solutions history[j * n ..] (x_{k-1} first) without a solve. Outputs (each may be NULL):
+ * c_out[n] the network's correction, x0_out[n] the starting guess, features_out[nverts * 16] the
+ * raw per-vertex features, state_out[34] = feature sums (5), Galerkin matrix (upper triangle by
+ * rows, 15) and right-hand side (5) of the basis {x1, x1 - x2, x2 - x3, x3 - x4, c},
+ * coefficients (5), energy of x0, energy of x1, fallback flag, kept basis vectors. */
+int mas_debug_warm_start(mas_solver *h, const double *b, const double *history, int nhist, double *c_out,
                          double *x0_out, float *features_out, double *state_out);
 
 /* New: Matrix Market files for A and b, the format the reference's tests load with Eigen's

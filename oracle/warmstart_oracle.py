@@ -12,7 +12,8 @@ solver's own (features, network, Galerkin combination):
                   states and layer weights with float32 accumulation, float32 output layer);
 * ``forward64`` / ``backward64``: the same network in float64 with its reverse pass, checked
                   against finite differences (it is the reference for the training code);
-* ``galerkin``:   the energy-minimising combination of {x1, x1 - x2, c} with the fallback to x1.
+* ``galerkin``:   the energy-minimising combination of {x1, x1 - x2, x2 - x3, x3 - x4, c} (missing
+                  kept solutions give zero vectors, which are dropped) with the fallback to x1.
 
 Only ``tests/`` import this.
 """
@@ -179,27 +180,42 @@ def backward64(cache, g_out):
     return flat
 
 
-def galerkin(A, b, x1, x2, c):
-    """(coef[3], energy, energy of x1, fallback, rank) of the solver's combination rule."""
-    V = [x1, x1 - x2, c]
+def galerkin_basis(history, c):
+    """The solver's basis: x1, the differences of consecutive kept solutions (x_{k-1} first; a
+    missing one is zero), then c."""
+    hist = list(history)
+    V = [hist[0]]
+    for i in range(1, 4):
+        V.append(hist[i - 1] - hist[i] if i < len(hist) else np.zeros_like(hist[0]))
+    V.append(c)
+    return V
+
+
+def galerkin(A, b, x1, x2, c, *older):
+    """(coef[5], energy, energy of x1, fallback, rank) of the solver's combination rule over the
+    basis of ``galerkin_basis((x1, x2, *older), c)``."""
+    V = galerkin_basis((x1, x2) + tuple(older), c)
     AV = [A @ v for v in V]
-    G = np.array([[V[i] @ AV[j] for j in range(3)] for i in range(3)])
+    nb = len(V)
+    G = np.array([[V[i] @ AV[j] for j in range(nb)] for i in range(nb)])
     G = 0.5 * (G + G.T)
     g = np.array([v @ b for v in V])
     keep = []
-    for i in range(3):
+    for i in range(nb):
         if not (G[i, i] > 0 and np.isfinite(G[i, i])):
             continue
         S = keep
         d = G[i, i] - (G[i, S] @ np.linalg.solve(G[np.ix_(S, S)], G[S, i]) if S else 0.0)
         if d > 1e-10 * G[i, i] and np.isfinite(d):
             keep.append(i)
-    y = np.zeros(3)
+    y = np.zeros(nb)
     if keep:
         y[keep] = np.linalg.solve(G[np.ix_(keep, keep)], g[keep])
     e = 0.5 * y @ G @ y - y @ g
     e1 = 0.5 * G[0, 0] - g[0]
     ok = bool(keep) and np.isfinite(e) and e < e1
     if not ok:
-        return np.array([1.0, 0.0, 0.0]), e1, e1, True, len(keep)
+        y0 = np.zeros(nb)
+        y0[0] = 1.0
+        return y0, e1, e1, True, len(keep)
     return y, e, e1, False, len(keep)

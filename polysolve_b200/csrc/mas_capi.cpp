@@ -270,7 +270,7 @@ struct mas_solver
 
     // Learned warm start: the last two solutions (padded order), the network's weights and
     // scratch, and the record of the last prediction.
-    DevBuf<double> hist[2];
+    DevBuf<double> hist[WS_HISTORY]; // ring: hist[hist_newest] is the last solution
     int hist_newest = 0, hist_count = 0;
     DevBuf<float> ws_params;
     DevBuf<uint16_t> ws_wl; // bf16 bits of the layer weights
@@ -278,7 +278,7 @@ struct mas_solver
     DevBuf<int> ws_diag;
     DevBuf<float> ws_wslot, ws_feat;
     DevBuf<uint16_t> ws_h0, ws_h1;
-    DevBuf<double> ws_c, ws_y1, ws_y2, ws_y3, ws_partials;
+    DevBuf<double> ws_c, ws_yc, ws_y[WS_HISTORY], ws_partials;
     DevBuf<WsState> ws_state;
     WsState *h_ws = nullptr; // pinned copy of the last prediction's record
     bool ws_graph_valid = false;
@@ -909,11 +909,13 @@ struct mas_solver
         ws_feat.alloc(nodes * WS_FEATURES, "warm start scratch");
         ws_h0.alloc(nodes * WS_HIDDEN, "warm start scratch");
         ws_h1.alloc(nodes * WS_HIDDEN, "warm start scratch");
-        for (DevBuf<double> *v : {&ws_c, &ws_y1, &ws_y2, &ws_y3})
-            v->alloc(len, "warm start scratch");
+        ws_c.alloc(len, "warm start scratch");
+        ws_yc.alloc(len, "warm start scratch");
+        for (DevBuf<double> &v : ws_y)
+            v.alloc(len, "warm start scratch");
         const int capacity = std::max((int)((nodes + 255) / 256), ws_reduce_ctas());
-        if (ws_partials.n < (size_t)capacity * 9)
-            ws_partials.alloc((size_t)capacity * 9, "warm start scratch");
+        if (ws_partials.n < (size_t)capacity * WS_GRAM)
+            ws_partials.alloc((size_t)capacity * WS_GRAM, "warm start scratch");
         if (!ws_state.get())
         {
             ws_state.alloc(1, "warm start scratch");
@@ -935,12 +937,10 @@ struct mas_solver
         w.h[0] = ws_h0.get();
         w.h[1] = ws_h1.get();
         w.c = ws_c.get();
-        w.y1 = ws_y1.get();
-        w.y2 = ws_y2.get();
-        w.y3 = ws_y3.get();
+        w.yc = ws_yc.get();
         w.st = ws_state.get();
         w.partials = ws_partials.get();
-        w.capacity = (int)(ws_partials.n / 9);
+        w.capacity = (int)(ws_partials.n / WS_GRAM);
         return w;
     }
 
@@ -965,13 +965,15 @@ struct mas_solver
             x0_source = "previous";
             return;
         }
-        const double *x2 = hist[hist_newest ^ 1].get();
+        const double *xs[WS_HISTORY];
+        for (int j = 0; j < hist_count; ++j)
+            xs[j] = hist[(hist_newest - j + WS_HISTORY) % WS_HISTORY].get();
         for (auto &ks : kstats)
             ks.second = KStat{};
         keep_stats = true;
         WsBuffers w = ws_buffers();
         cuda_check(cudaEventRecord(ws_ev[0], stream), "event");
-        ws_pipeline(w, x1, x2);
+        ws_pipeline(w, xs, hist_count);
         cuda_check(cudaEventRecord(ws_ev[1], stream), "event");
         cuda_check(cudaMemcpyAsync(h_ws, ws_state.get(), sizeof(WsState), cudaMemcpyDeviceToHost, stream),
                    "warm start record");
@@ -979,8 +981,9 @@ struct mas_solver
         x0_source = "learned";
     }
 
-    // The prediction: A x1, A x2, the network, A c, the Galerkin combination into x.
-    void ws_pipeline(const WsBuffers &w, const double *x1, const double *x2)
+    // The prediction from the kept solutions xs[0] (newest) .. xs[count - 1], count >= 2: their
+    // products with A, the network, A c, the Galerkin combination into x.
+    void ws_pipeline(const WsBuffers &w, const double *const *xs, int count)
     {
         const size_t len = (size_t)banks * 32 * bd;
         const BankedView Av = A.view();
@@ -989,13 +992,21 @@ struct mas_solver
             run("ws_graph", 1, [&] { launch_ws_graph(Av, w, stream); });
             ws_graph_valid = true;
         }
-        run("spmv_plain", 2, [&] {
-            launch_spmv(SPMV_PLAIN, Av, x1, w.y1, nullptr, nullptr, red(), 0, 0, stream);
-            launch_spmv(SPMV_PLAIN, Av, x2, w.y2, nullptr, nullptr, red(), 0, 0, stream);
+        WsHistory h;
+        const int have = std::min(count, WS_HISTORY);
+        for (int j = 0; j < WS_HISTORY; ++j)
+        {
+            const int src = std::min(j, have - 1); // missing: repeat the oldest (zero difference)
+            h.x[j] = xs[src];
+            h.y[j] = ws_y[src].get();
+        }
+        run("spmv_plain", have, [&] {
+            for (int j = 0; j < have; ++j)
+                launch_spmv(SPMV_PLAIN, Av, xs[j], ws_y[j].get(), nullptr, nullptr, red(), 0, 0, stream);
         });
-        run("ws_network", 0, [&] { return launch_ws_network(Av, w, b.get(), x1, x2, stream); });
-        run("spmv_plain", 1, [&] { launch_spmv(SPMV_PLAIN, Av, w.c, w.y3, nullptr, nullptr, red(), 0, 0, stream); });
-        run("ws_combine", 0, [&] { return launch_ws_combine(w, b.get(), x1, x2, x.get(), len, stream); });
+        run("ws_network", 0, [&] { return launch_ws_network(Av, w, b.get(), h, stream); });
+        run("spmv_plain", 1, [&] { launch_spmv(SPMV_PLAIN, Av, w.c, w.yc, nullptr, nullptr, red(), 0, 0, stream); });
+        run("ws_combine", 0, [&] { return launch_ws_combine(w, b.get(), h, x.get(), len, stream); });
     }
 
     // After a solve: keep x as the newest solution; read the prediction's record and time.
@@ -1011,40 +1022,44 @@ struct mas_solver
                 x0_source = "previous (fallback)";
         }
         const size_t len = (size_t)banks * 32 * bd;
-        hist[0].alloc(len, "warm start history");
-        hist[1].alloc(len, "warm start history");
+        for (DevBuf<double> &hb : hist)
+            hb.alloc(len, "warm start history");
         if (hist_count > 0)
-            hist_newest ^= 1;
+            hist_newest = (hist_newest + 1) % WS_HISTORY;
         cuda_check(cudaMemcpyAsync(hist[hist_newest].get(), x.get(), x.bytes(), cudaMemcpyDeviceToDevice, stream),
                    "keep solution");
-        hist_count = std::min(hist_count + 1, 2);
+        hist_count = std::min(hist_count + 1, WS_HISTORY);
     }
 
-    // Tests: the prediction for caller-order b, x1, x2 without a solve; outputs in caller order
-    // (c, x0: n values; features: V * 16; state: sums 5, gram 9, coef 3, energy, energy of x1,
-    // fallback, rank).
-    void debug_warm_start(const double *hb, const double *hx1, const double *hx2, double *hc, double *hx0,
+    // Tests: the prediction for caller-order b and kept solutions hhist[j * n ..] (newest first,
+    // 2 <= nhist <= 4) without a solve; outputs in caller order (c, x0: n values; features:
+    // V * 16; state: sums 5, Galerkin matrix and right-hand side WS_GRAM, coefficients WS_BASIS,
+    // energy, energy of x1, fallback, rank).
+    void debug_warm_start(const double *hb, const double *hhist, int nhist, double *hc, double *hx0,
                           float *hfeat, double *hstate)
     {
         cuda_check(cudaSetDevice(device), "set device");
         require_factorized(n);
         if (!ws_loaded || bd != 3)
             throw Error(ERR_INVALID, "[MAS] warm start: no model loaded or block_dim is not 3");
-        if (!hb || !hx1 || !hx2)
-            throw Error(ERR_INVALID, "[MAS] warm start: null vector");
+        if (!hb || !hhist || nhist < 2 || nhist > WS_HISTORY)
+            throw Error(ERR_INVALID, "[MAS] warm start: b and 2 to 4 kept solutions are needed");
         const size_t len = (size_t)banks * 32 * bd;
-        DevBuf<double> d1, d2;
-        d1.alloc(len, "debug");
-        d2.alloc(len, "debug");
-        const double *src[3] = {hb, hx1, hx2};
-        double *dst[3] = {b.get(), d1.get(), d2.get()};
-        for (int i = 0; i < 3; ++i)
+        DevBuf<double> dh[WS_HISTORY];
+        const double *xs[WS_HISTORY];
+        cuda_check(cudaMemcpyAsync(io.get(), hb, sizeof(double) * n, cudaMemcpyHostToDevice, stream), "upload");
+        launch_permute_in(n, bd, V, d_padded.get(), io.get(), b.get(), len, stream);
+        for (int j = 0; j < nhist; ++j)
         {
-            cuda_check(cudaMemcpyAsync(io.get(), src[i], sizeof(double) * n, cudaMemcpyHostToDevice, stream), "upload");
-            launch_permute_in(n, bd, V, d_padded.get(), io.get(), dst[i], len, stream);
+            dh[j].alloc(len, "debug");
+            cuda_check(cudaMemcpyAsync(io.get(), hhist + (size_t)j * n, sizeof(double) * n, cudaMemcpyHostToDevice,
+                                       stream),
+                       "upload");
+            launch_permute_in(n, bd, V, d_padded.get(), io.get(), dh[j].get(), len, stream);
+            xs[j] = dh[j].get();
         }
         WsBuffers w = ws_buffers();
-        ws_pipeline(w, d1.get(), d2.get());
+        ws_pipeline(w, xs, nhist);
         if (hc)
         {
             launch_permute_out(n, bd, V, d_padded.get(), w.c, io.get(), stream);
@@ -1428,7 +1443,7 @@ struct mas_solver
             ws.type = Json::Object;
             cf.type = Json::Array;
             const bool have = ws_predicted && h_ws;
-            for (int i = 0; i < 3; ++i)
+            for (int i = 0; i < WS_BASIS; ++i)
                 cf.arr.push_back(num(have ? h_ws->coef[i] : 0.0, false));
             ws.obj.emplace_back("model_loaded", boolean(ws_loaded));
             ws.obj.emplace_back("history", num(hist_count, true));
@@ -1670,12 +1685,12 @@ extern "C" int mas_reset_warm_start(mas_solver *h)
     return guarded(h, [&] { h->hist_count = 0; });
 }
 
-extern "C" int mas_debug_warm_start(mas_solver *h, const double *b, const double *x1, const double *x2, double *c_out,
+extern "C" int mas_debug_warm_start(mas_solver *h, const double *b, const double *history, int nhist, double *c_out,
                                     double *x0_out, float *features_out, double *state_out)
 {
     if (!h)
         return MAS_ERR_INVALID;
-    return guarded(h, [&] { h->debug_warm_start(b, x1, x2, c_out, x0_out, features_out, state_out); });
+    return guarded(h, [&] { h->debug_warm_start(b, history, nhist, c_out, x0_out, features_out, state_out); });
 }
 
 extern "C" int mas_factorize_csc(mas_solver *h, int n, const int *outer, const int *inner, const double *vals, int nnz)

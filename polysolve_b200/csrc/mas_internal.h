@@ -452,23 +452,34 @@ namespace pmas
     // mas_warmstart.cu: the learned starting guess for a sequence of systems (same pattern):
     // a message-passing network over the vertex graph predicts a correction c of the
     // extrapolated guess 2 x1 - x2 from the residual, the diagonal blocks and the last step;
-    // x0 is the energy-minimising combination of x1, x1 - x2 and c (x1 if that is not lower).
-    // Block size 3 only (three displacement components per vertex).
+    // x0 is the energy-minimising combination of the kept solutions x1 .. x4 (as x1 and the
+    // differences x_i - x_(i+1)) and c, x1 if that is not lower. Block size 3 only.
     // ---------------------------------------------------------------------------------------
     constexpr int WS_FEATURES = 16, WS_HIDDEN = 64, WS_LAYERS = 3;
     constexpr int WS_PARAMS = WS_HIDDEN * WS_FEATURES + WS_HIDDEN +
                               WS_LAYERS * (WS_HIDDEN * 2 * WS_HIDDEN + WS_HIDDEN) + 3 * WS_HIDDEN + 3;
     constexpr int WS_LAYER_WEIGHTS = WS_HIDDEN * 2 * WS_HIDDEN; // bf16 values of one W_l
+    constexpr int WS_HISTORY = 4;              // kept solutions x1 (newest) .. x4
+    constexpr int WS_BASIS = WS_HISTORY + 1;   // x1, x1 - x2, x2 - x3, x3 - x4, c
+    constexpr int WS_GRAM = WS_BASIS * (WS_BASIS + 1) / 2 + WS_BASIS;
 
     struct WsState
     {
-        double sums[5];  // sum over real vertices of |q|^2, |v|^2, |p|^2, log trace, count
-        double gram[9];  // G11 G12 G13 G22 G23 G33 (v_i . A v_j) and g1 g2 g3 (v_i . b)
-        double coef[3];  // x0 = coef0 x1 + coef1 (x1 - x2) + coef2 c
+        double sums[5];       // sum over real vertices of |q|^2, |v|^2, |p|^2, log trace, count
+        double gram[WS_GRAM]; // v_i . A v_j (i <= j, row by row), then v_i . b
+        double coef[WS_BASIS]; // x0 = sum_i coef_i v_i
         double energy, energy_prev; // 1/2 x.Ax - x.b of x0 and of x1
         int fallback;    // 1: x0 = x1 (the combination was degenerate or not lower)
         int rank;        // basis vectors kept by the Galerkin solve
         unsigned counter[2];
+    };
+
+    // The kept solutions (newest first) and their products with the current A; a missing one
+    // repeats the oldest present, so its difference is zero and the Galerkin solve drops it.
+    struct WsHistory
+    {
+        const double *x[WS_HISTORY];
+        const double *y[WS_HISTORY];
     };
 
     struct WsBuffers
@@ -479,20 +490,20 @@ namespace pmas
         float *wslot;          // slots * 32: neighbour weight of each stored block
         float *feat;           // nodes * WS_FEATURES raw features
         uint16_t *h[2];        // nodes * WS_HIDDEN bf16 hidden states (ping-pong)
-        double *c, *y1, *y2, *y3; // correction, A x1, A x2, A c (padded order, nodes * 3)
+        double *c, *yc;        // correction and A c (padded order, nodes * 3)
         WsState *st;
-        double *partials;      // 9 * capacity
+        double *partials;      // WS_GRAM * capacity
         int capacity;          // CTAs of the reduced launches
     };
 
     // Neighbour weights and diagonal slots of the current values (once per factorization).
     void launch_ws_graph(const BankedView &A, const WsBuffers &w, cudaStream_t s);
-    // Features .. correction c (needs y1 = A x1 and y2 = A x2 already in w). Returns kernels.
-    int launch_ws_network(const BankedView &A, const WsBuffers &w, const double *b, const double *x1,
-                          const double *x2, cudaStream_t s);
-    // Galerkin combination into x (needs w.y3 = A c). Returns kernels.
-    int launch_ws_combine(const WsBuffers &w, const double *b, const double *x1, const double *x2, double *x,
-                          size_t len, cudaStream_t s);
+    // Features .. correction c (needs hist.y[0], hist.y[1] = A x1, A x2). Returns kernels.
+    int launch_ws_network(const BankedView &A, const WsBuffers &w, const double *b, const WsHistory &hist,
+                          cudaStream_t s);
+    // Galerkin combination into x (needs w.yc = A c). Returns kernels.
+    int launch_ws_combine(const WsBuffers &w, const double *b, const WsHistory &hist, double *x, size_t len,
+                          cudaStream_t s);
     int ws_reduce_ctas();
     // Features of the vertices in caller order (tests): out[v * 16 + f] = feat[padded[v] * 16 + f].
     void launch_ws_features_out(int V, const int *padded_of_block, const float *feat, float *out, cudaStream_t s);

@@ -2,11 +2,12 @@
 //
 // The reference starts every PCG solve from x0 = 0 (MASSolver.cu:395-398) while its caller
 // (nonlinear::Newton, Newton.cpp:173-214) solves a matrix of the same pattern with new values at
-// every step. Here the solver keeps the last two solutions x1, x2 on the device and predicts x0:
+// every step. Here the solver keeps the last four solutions x1 (newest) .. x4 on the device and
+// predicts x0:
 //
 //   k_ws_graph      once per factorization: each stored block's neighbour weight
 //                   ||A_ij||_F / sum_{j' != i} ||A_ij'||_F and the slot of the diagonal block.
-//   (SpMV x2)       y1 = A x1, y2 = A x2 (the plain SpMV kernel).
+//   (SpMV x4)       y_i = A x_i for the kept solutions (the plain SpMV kernel).
 //   k_ws_features   per vertex: q = D^-1 r_e (r_e = b - A (2 x1 - x2)), v = x1 - x2, p = D^-1 b,
 //                   the diagonal block scaled by trace / 3, log trace; the sums the
 //                   normalisation needs (deterministic grid reduction).
@@ -16,11 +17,13 @@
 //                   with FP32 accumulation, 64 vertices x 64 outputs x K = 128 per CTA.
 //   k_ws_output     c = s_q (W_out h + b_out) (FP32 weights, FP64 out).
 //   (SpMV)          y3 = A c.
-//   k_ws_gram       the 3 x 3 Galerkin system of the basis {x1, x1 - x2, c} and its right-hand
-//                   side (9 dots, deterministic); the last CTA solves it with a pivoted
-//                   Cholesky that drops dependent vectors and falls back to x1 unless the
-//                   energy 1/2 x.Ax - x.b drops below that of x1.
-//   k_ws_combine    x0 = coef0 x1 + coef1 (x1 - x2) + coef2 c.
+//   k_ws_gram       the 5 x 5 Galerkin system of the basis {x1, x1 - x2, x2 - x3, x3 - x4, c}
+//                   and its right-hand side (20 dots, deterministic); the last CTA solves it
+//                   with a pivoted Cholesky that drops dependent (or missing) vectors and falls
+//                   back to x1 unless the energy 1/2 x.Ax - x.b drops below that of x1. The
+//                   differences of past solutions carry their trend in k: the combination is a
+//                   polynomial extrapolation in the step index, fitted in the energy norm;
+//   k_ws_combine    x0 = sum_i coef_i v_i.
 //
 // All vectors are in the solver's padded (subdomain) order; nodes without a row (padding) get
 // zero features, zero hidden states and c = 0. The work is small next to a solve: at 680 K DOF
@@ -479,44 +482,82 @@ namespace pmas
         }
 
         constexpr int GRAM_CTAS_PER_SM = 4;
+        constexpr int NB = WS_BASIS;
 
-        // The Galerkin system of {x1, x1 - x2, c}; the last CTA solves it.
-        __global__ void __launch_bounds__(WT)
-            k_ws_gram(const double *__restrict__ b, const double *__restrict__ x1, const double *__restrict__ x2,
-                      const double *__restrict__ c, const double *__restrict__ y1, const double *__restrict__ y2,
-                      const double *__restrict__ y3, size_t len, WsState *ws, double *partials)
+        // Basis vector i and its product with A at element k.
+        __device__ __forceinline__ void basis_at(const WsHistory &h, const double *__restrict__ c,
+                                                 const double *__restrict__ yc, size_t k, double (&v)[NB],
+                                                 double (&av)[NB])
         {
-            double s[9];
+            v[0] = h.x[0][k];
+            av[0] = h.y[0][k];
 #pragma unroll
-            for (int i = 0; i < 9; ++i)
+            for (int i = 1; i < WS_HISTORY; ++i)
+            {
+                v[i] = h.x[i - 1][k] - h.x[i][k];
+                av[i] = h.y[i - 1][k] - h.y[i][k];
+            }
+            v[NB - 1] = c[k];
+            av[NB - 1] = yc[k];
+        }
+
+        // The Galerkin system of the basis; the last CTA solves it.
+        __global__ void __launch_bounds__(WT)
+            k_ws_gram(const double *__restrict__ b, WsHistory h, const double *__restrict__ c,
+                      const double *__restrict__ yc, size_t len, WsState *ws, double *partials)
+        {
+            double s[WS_GRAM];
+#pragma unroll
+            for (int i = 0; i < WS_GRAM; ++i)
                 s[i] = 0.0;
             for (size_t k = (size_t)blockIdx.x * WT + threadIdx.x; k < len; k += (size_t)gridDim.x * WT)
             {
-                const double v1 = x1[k], v2 = x1[k] - x2[k], v3 = c[k];
-                const double a1 = y1[k], a2 = y1[k] - y2[k], a3 = y3[k], bk = b[k];
-                s[0] = fma(v1, a1, s[0]);
-                s[1] = fma(v1, a2, s[1]);
-                s[2] = fma(v1, a3, s[2]);
-                s[3] = fma(v2, a2, s[3]);
-                s[4] = fma(v2, a3, s[4]);
-                s[5] = fma(v3, a3, s[5]);
-                s[6] = fma(v1, bk, s[6]);
-                s[7] = fma(v2, bk, s[7]);
-                s[8] = fma(v3, bk, s[8]);
+                double v[NB], av[NB];
+                basis_at(h, c, yc, k, v, av);
+                const double bk = b[k];
+                int e = 0;
+#pragma unroll
+                for (int i = 0; i < NB; ++i)
+#pragma unroll
+                    for (int j = i; j < NB; ++j)
+                    {
+                        s[e] = fma(v[i], av[j], s[e]);
+                        ++e;
+                    }
+#pragma unroll
+                for (int i = 0; i < NB; ++i)
+                    s[e + i] = fma(v[i], bk, s[e + i]);
             }
-            double t[9];
-            if (!grid_reduce<9, WT>(s, partials, &ws->counter[1], t) || threadIdx.x != 0)
+            double t[WS_GRAM];
+            if (!grid_reduce<WS_GRAM, WT>(s, partials, &ws->counter[1], t) || threadIdx.x != 0)
                 return;
-            for (int i = 0; i < 9; ++i)
+            for (int i = 0; i < WS_GRAM; ++i)
                 ws->gram[i] = t[i];
-            const double G[3][3] = {{t[0], t[1], t[2]}, {t[1], t[3], t[4]}, {t[2], t[4], t[5]}};
-            const double g[3] = {t[6], t[7], t[8]};
+            double G[NB][NB], g[NB];
+            {
+                int e = 0;
+                for (int i = 0; i < NB; ++i)
+                    for (int j = i; j < NB; ++j)
+                    {
+                        G[i][j] = t[e];
+                        G[j][i] = t[e];
+                        ++e;
+                    }
+                for (int i = 0; i < NB; ++i)
+                    g[i] = t[e + i];
+            }
             // Cholesky of the kept vectors, in order; a vector whose pivot is below 1e-10 of its
             // diagonal (dependent on the kept ones) or not positive is dropped.
-            double L[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-            bool keep[3] = {false, false, false};
+            double L[NB][NB];
+            bool keep[NB];
             int rank = 0;
-            for (int i = 0; i < 3; ++i)
+            for (int i = 0; i < NB; ++i)
+            {
+                keep[i] = false;
+                for (int j = 0; j < NB; ++j)
+                    L[i][j] = 0.0;
+            }
+            for (int i = 0; i < NB; ++i)
             {
                 if (!(G[i][i] > 0.0) || !isfinite(G[i][i]))
                     continue;
@@ -542,8 +583,10 @@ namespace pmas
                     for (int j = 0; j < i; ++j)
                         L[i][j] = 0.0;
             }
-            double y[3] = {0.0, 0.0, 0.0}, z[3] = {0.0, 0.0, 0.0};
-            for (int i = 0; i < 3; ++i) // L z = g
+            double y[NB], z[NB];
+            for (int i = 0; i < NB; ++i)
+                y[i] = z[i] = 0.0;
+            for (int i = 0; i < NB; ++i) // L z = g
                 if (keep[i])
                 {
                     double v = g[i];
@@ -552,42 +595,50 @@ namespace pmas
                             v -= L[i][j] * z[j];
                     z[i] = v / L[i][i];
                 }
-            for (int i = 2; i >= 0; --i) // L^T y = z
+            for (int i = NB - 1; i >= 0; --i) // L^T y = z
                 if (keep[i])
                 {
                     double v = z[i];
-                    for (int j = i + 1; j < 3; ++j)
+                    for (int j = i + 1; j < NB; ++j)
                         if (keep[j])
                             v -= L[j][i] * y[j];
                     y[i] = v / L[i][i];
                 }
             double e = 0.0; // 1/2 y.Gy - y.g
-            for (int i = 0; i < 3; ++i)
+            bool finite = true;
+            for (int i = 0; i < NB; ++i)
             {
                 double gy = 0.0;
-                for (int j = 0; j < 3; ++j)
+                for (int j = 0; j < NB; ++j)
                     gy += G[i][j] * y[j];
                 e += y[i] * (0.5 * gy - g[i]);
+                finite = finite && isfinite(y[i]);
             }
             const double e1 = 0.5 * G[0][0] - g[0];
-            const bool ok = rank > 0 && isfinite(e) && isfinite(y[0]) && isfinite(y[1]) && isfinite(y[2]) && e < e1;
+            const bool ok = rank > 0 && finite && isfinite(e) && e < e1;
             ws->fallback = ok ? 0 : 1;
             ws->rank = rank;
-            ws->coef[0] = ok ? y[0] : 1.0;
-            ws->coef[1] = ok ? y[1] : 0.0;
-            ws->coef[2] = ok ? y[2] : 0.0;
+            for (int i = 0; i < NB; ++i)
+                ws->coef[i] = ok ? y[i] : (i == 0 ? 1.0 : 0.0);
             ws->energy = ok ? e : e1;
             ws->energy_prev = e1;
         }
 
-        __global__ void __launch_bounds__(WT) k_ws_combine(const double *__restrict__ x1,
-                                                           const double *__restrict__ x2,
-                                                           const double *__restrict__ c, const WsState *ws,
-                                                           double *__restrict__ x, size_t len)
+        __global__ void __launch_bounds__(WT) k_ws_combine(WsHistory h, const double *__restrict__ c,
+                                                           const WsState *ws, double *__restrict__ x, size_t len)
         {
-            const double a = ws->coef[0], bcoef = ws->coef[1], g = ws->coef[2];
+            double cf[NB];
+#pragma unroll
+            for (int i = 0; i < NB; ++i)
+                cf[i] = ws->coef[i];
             for (size_t k = (size_t)blockIdx.x * WT + threadIdx.x; k < len; k += (size_t)gridDim.x * WT)
-                x[k] = a * x1[k] + bcoef * (x1[k] - x2[k]) + g * c[k];
+            {
+                double v = cf[0] * h.x[0][k];
+#pragma unroll
+                for (int i = 1; i < WS_HISTORY; ++i)
+                    v += cf[i] * (h.x[i - 1][k] - h.x[i][k]);
+                x[k] = v + cf[NB - 1] * c[k];
+            }
         }
 
         __global__ void k_ws_features_out(int V, const int *__restrict__ padded, const float *__restrict__ feat,
@@ -614,16 +665,18 @@ namespace pmas
         cuda_check(cudaGetLastError(), "warm start graph launch");
     }
 
-    int launch_ws_network(const BankedView &A, const WsBuffers &w, const double *b, const double *x1,
-                          const double *x2, cudaStream_t s)
+    int launch_ws_network(const BankedView &A, const WsBuffers &w, const double *b, const WsHistory &hist,
+                          cudaStream_t s)
     {
+        const double *x1 = hist.x[0], *x2 = hist.x[1];
         const int nodes = A.banks * 32;
         if (nodes == 0)
             return 0;
         const int grid_v = (nodes + WT - 1) / WT;
         if (grid_v > w.capacity)
             throw Error(ERR_INVALID, "[MAS] warm start reduction scratch too small");
-        k_ws_features<<<grid_v, WT, 0, s>>>(A, w.diag_slot, b, x1, x2, w.y1, w.y2, w.feat, w.st, w.partials);
+        k_ws_features<<<grid_v, WT, 0, s>>>(A, w.diag_slot, b, x1, x2, hist.y[0], hist.y[1], w.feat, w.st,
+                                            w.partials);
         cuda_check(cudaGetLastError(), "warm start features launch");
         const int grid_b = (A.banks + WT / 32 - 1) / (WT / 32);
         k_ws_input<<<grid_b, WT, 0, s>>>(nodes, A.rowlen, w.diag_slot, w.feat, w.params, w.st,
@@ -644,15 +697,15 @@ namespace pmas
         return 3 + WS_LAYERS;
     }
 
-    int launch_ws_combine(const WsBuffers &w, const double *b, const double *x1, const double *x2, double *x,
-                          size_t len, cudaStream_t s)
+    int launch_ws_combine(const WsBuffers &w, const double *b, const WsHistory &hist, double *x, size_t len,
+                          cudaStream_t s)
     {
         const int grid = ws_reduce_ctas();
         if (grid > w.capacity)
             throw Error(ERR_INVALID, "[MAS] warm start reduction scratch too small");
-        k_ws_gram<<<grid, WT, 0, s>>>(b, x1, x2, w.c, w.y1, w.y2, w.y3, len, w.st, w.partials);
+        k_ws_gram<<<grid, WT, 0, s>>>(b, hist, w.c, w.yc, len, w.st, w.partials);
         cuda_check(cudaGetLastError(), "warm start gram launch");
-        k_ws_combine<<<grid, WT, 0, s>>>(x1, x2, w.c, w.st, x, len);
+        k_ws_combine<<<grid, WT, 0, s>>>(hist, w.c, w.st, x, len);
         cuda_check(cudaGetLastError(), "warm start combine launch");
         return 2;
     }

@@ -100,7 +100,7 @@ def library() -> ctypes.CDLL:
         L.mas_debug_spmv_multi.argtypes = [vp, vp, vp, i]
         L.mas_set_warm_start_model.argtypes = [vp, vp, ctypes.c_longlong]
         L.mas_reset_warm_start.argtypes = [vp]
-        L.mas_debug_warm_start.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
+        L.mas_debug_warm_start.argtypes = [vp, vp, vp, i, vp, vp, vp, vp]
         L.mas_order_blocks.argtypes = [i, vp, vp, i, vp, ctypes.c_char_p, ip, ip]
         _LIB = L
     return _LIB
@@ -372,22 +372,28 @@ class Solver:
         """New: forget the kept solutions (the next learned-mode solve starts from zero)."""
         _check(library().mas_reset_warm_start(self._h), self._h)
 
-    def debug_warm_start(self, b: np.ndarray, x1: np.ndarray, x2: np.ndarray) -> dict:
-        """Test hook: the learned starting guess for b given x_{k-1} = x1, x_{k-2} = x2 (caller
-        order), without a solve: c, x0, raw features (nverts, 16) and the reduction record."""
+    def debug_warm_start(self, b: np.ndarray, *history: np.ndarray) -> dict:
+        """Test hook: the learned starting guess for b given 2 to 4 kept solutions (x_{k-1} first,
+        caller order), without a solve: c, x0, raw features (nverts, 16) and the reduction record
+        (Galerkin matrix / right-hand side of the basis {x1, x1 - x2, x2 - x3, x3 - x4, c})."""
         from . import warmstart
 
-        b, x1, x2 = (np.ascontiguousarray(v, dtype=np.float64) for v in (b, x1, x2))
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        hist = np.ascontiguousarray(np.stack([np.asarray(h, dtype=np.float64) for h in history]))
         n = b.size
         c = np.empty(n)
         x0 = np.empty(n)
         feat = np.empty(((n + 2) // 3, warmstart.FEATURES), dtype=np.float32)
-        state = np.empty(21)
-        _check(library().mas_debug_warm_start(self._h, b.ctypes.data, x1.ctypes.data, x2.ctypes.data, c.ctypes.data,
-                                              x0.ctypes.data, feat.ctypes.data, state.ctypes.data), self._h)
-        return {"c": c, "x0": x0, "features": feat, "sums": state[0:5], "gram": state[5:14], "coef": state[14:17],
-                "energy": state[17], "energy_previous": state[18], "fallback": bool(state[19]),
-                "rank": int(state[20])}
+        nb = warmstart.BASIS
+        ng = nb * (nb + 1) // 2 + nb
+        state = np.empty(5 + ng + nb + 4)
+        _check(library().mas_debug_warm_start(self._h, b.ctypes.data, hist.ctypes.data, int(hist.shape[0]),
+                                              c.ctypes.data, x0.ctypes.data, feat.ctypes.data, state.ctypes.data),
+               self._h)
+        e = 5 + ng
+        return {"c": c, "x0": x0, "features": feat, "sums": state[0:5], "gram": state[5:e], "coef": state[e:e + nb],
+                "energy": state[e + nb], "energy_previous": state[e + nb + 1], "fallback": bool(state[e + nb + 2]),
+                "rank": int(state[e + nb + 3])}
 
     def debug_spmv_multi(self, X_padded: np.ndarray) -> np.ndarray:
         x = np.ascontiguousarray(X_padded, dtype=np.float64)

@@ -1,6 +1,6 @@
 """Learned warm start: the message-passing network's definition and weight file format.
 
-The solver's ``initial_guess: "learned"`` mode keeps the last two solutions of a sequence of
+The solver's ``initial_guess: "learned"`` mode keeps the last four solutions of a sequence of
 systems on the device and predicts the next starting guess from them, b and the diagonal blocks
 (all on the GPU, ``csrc/mas_warmstart.cu``):
 
@@ -27,10 +27,12 @@ systems on the device and predicts the next starting guess from them, b and the 
 
    On the GPU the hidden states and the layer weights W_l are BF16 (tensor-core products,
    FP32 accumulation); W_in, W_out and the biases stay FP32;
-4. the starting guess is the Galerkin (energy-minimising) combination of x_{k-1},
-   x_{k-1} - x_{k-2} and c; if its energy is not below that of x_{k-1} (or the system is
-   degenerate), the guess falls back to x_{k-1}. PCG then runs to the tolerance as usual, so
-   every accepted solve meets the same relative residual as a cold start.
+4. the starting guess is the Galerkin (energy-minimising) combination of x_{k-1}, the
+   differences x_{k-1} - x_{k-2}, x_{k-2} - x_{k-3}, x_{k-3} - x_{k-4} of the kept solutions
+   (a polynomial extrapolation in the step index, fitted in the energy norm; missing ones are
+   dropped) and c; if its energy is not below that of x_{k-1} (or the system is degenerate),
+   the guess falls back to x_{k-1}. PCG then runs to the tolerance as usual, so every accepted
+   solve meets the same relative residual as a cold start.
 
 Weight file (``.psws``): 8 bytes ``PSWSMPN1``, four little-endian int32 (features 16,
 hidden 64, layers 3, parameter count), then the parameters as little-endian float32 in the
@@ -48,6 +50,8 @@ import numpy as np
 FEATURES = 16
 HIDDEN = 64
 LAYERS = 3
+HISTORY = 4            # kept solutions
+BASIS = HISTORY + 1    # Galerkin basis: x1, x1 - x2, x2 - x3, x3 - x4, c
 MAGIC = b"PSWSMPN1"
 
 
@@ -118,5 +122,5 @@ def default_weights() -> np.ndarray:
     return load(DEFAULT_WEIGHTS)
 
 
-__all__ = ["FEATURES", "HIDDEN", "LAYERS", "PARAMS", "layout", "unpack", "save", "load", "default_weights",
-           "DEFAULT_WEIGHTS"]
+__all__ = ["FEATURES", "HIDDEN", "LAYERS", "HISTORY", "BASIS", "PARAMS", "layout", "unpack", "save", "load",
+           "default_weights", "DEFAULT_WEIGHTS"]

@@ -41,14 +41,14 @@ def _random_params(seed):
 
 @pytest.mark.parametrize("params", ["random", "shipped"])
 def test_prediction_matches_oracle(params):
-    systems, rhs, xs = _exact_sequence(7, 3, seed=11)
-    A = systems[2].scipy().tocsr()
-    b, x1, x2 = rhs[2], xs[1], xs[0]
-    s = _solver(systems[2])
-    s.factorize(systems[2].scipy())
+    systems, rhs, xs = _exact_sequence(7, 5, seed=11)
+    A = systems[4].scipy().tocsr()
+    b, x1, x2, x3, x4 = rhs[4], xs[3], xs[2], xs[1], xs[0]
+    s = _solver(systems[4])
+    s.factorize(systems[4].scipy())
     prm = _random_params(5) if params == "random" else W.default_weights()
     s.set_warm_start_model(prm)
-    d = s.debug_warm_start(b, x1, x2)
+    d = s.debug_warm_start(b, x1, x2, x3, x4)
 
     src, dst, w, D = WO.graph(A)
     raw, sums = WO.features(A, b, x1, x2, D)
@@ -58,12 +58,19 @@ def test_prediction_matches_oracle(params):
     # bf16 hidden states: the tolerance covers rounding-boundary flips from the summation order
     c_orc = WO.forward_device(prm, raw.astype(np.float32), sums, src, dst, w).reshape(-1)
     assert np.linalg.norm(d["c"] - c_orc) <= 2e-2 * np.linalg.norm(c_orc)
-    y, e, e1, fb, rank = WO.galerkin(A, b, x1, x2, d["c"])
+    y, e, e1, fb, rank = WO.galerkin(A, b, x1, x2, d["c"], x3, x4)
     assert d["fallback"] == fb and d["rank"] == rank
-    assert np.allclose(d["coef"], y, rtol=1e-6, atol=1e-9)
-    x0 = y[0] * x1 + y[1] * (x1 - x2) + y[2] * d["c"]
-    assert np.linalg.norm(d["x0"] - x0) <= 1e-9 * np.linalg.norm(x0)
+    # the 5 x 5 system can be ill-conditioned (the differences shrink with the step): compare the
+    # starting guesses and their energies rather than the coefficients
+    x0 = sum(yi * vi for yi, vi in zip(y, WO.galerkin_basis((x1, x2, x3, x4), d["c"])))
+    assert np.linalg.norm(d["x0"] - x0) <= 1e-7 * np.linalg.norm(x0)
+    assert abs(d["energy"] - e) <= 1e-7 * abs(e)
     assert d["energy"] <= d["energy_previous"]
+    # fewer kept solutions: the missing differences are dropped
+    d2 = s.debug_warm_start(b, x1, x2)
+    y2, e2, _, _, rank2 = WO.galerkin(A, b, x1, x2, d2["c"])
+    assert d2["rank"] == rank2 <= 3 and abs(d2["energy"] - e2) <= 1e-7 * abs(e2)
+    assert d["energy"] <= d2["energy"] + 1e-12 * abs(d2["energy"])
 
 
 def test_learned_sequence_converges_and_beats_extrapolation():
