@@ -49,7 +49,7 @@ namespace
         int true_residual_period = 4;
         int check_period = 10;
         bool initial_guess_input = false;
-        bool initial_guess_learned = false; // x0 from the solver's own last two solutions
+        bool initial_guess_learned = false; // x0 from the solver's own kept solutions
         bool polak_ribiere = false;
         std::string ordering = "auto";
         int poll_period = 10;
@@ -268,7 +268,7 @@ struct mas_solver
     cudaGraphExec_t ggraph[2] = {nullptr, nullptr};
     std::vector<std::pair<int, long long>> ggraph_counts[2];
 
-    // Learned warm start: the last two solutions (padded order), the network's weights and
+    // Learned warm start: the last four solutions (padded order), the network's weights and
     // scratch, and the record of the last prediction.
     DevBuf<double> hist[WS_HISTORY]; // ring: hist[hist_newest] is the last solution
     int hist_newest = 0, hist_count = 0;
@@ -947,7 +947,7 @@ struct mas_solver
     bool learned_active() const { return p.initial_guess_learned && !in_multi; }
 
     // x (padded order) for the next solve of a sequence: zero, the last solution, or the
-    // network's prediction combined with the last two solutions (b already loaded).
+    // network's prediction combined with the kept solutions (b already loaded).
     void warm_start_guess()
     {
         ws_predicted = false;

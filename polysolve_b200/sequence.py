@@ -12,8 +12,9 @@ it from the previous solutions:
 The relative tolerance stays relative to ||b_k||, so a good guess directly saves iterations.
 
 ``learned`` leaves the guess to the solver (``initial_guess: "learned"``, a network loaded with
-``Solver.set_warm_start_model``): it keeps its last two solutions on the device and starts from
-the energy-minimising combination of x_{k-1}, x_{k-1} - x_{k-2} and the network's correction.
+``Solver.set_warm_start_model``): it keeps its last four solutions on the device and starts from
+the energy-minimising combination of x_{k-1}, the differences of consecutive kept solutions and
+the network's correction.
 """
 
 from __future__ import annotations
