@@ -232,7 +232,7 @@ struct mas_solver
     double rr0 = 0.0, rz0 = 0.0;
     double solve_ms = 0.0, factorize_ms = 0.0;
     std::vector<std::pair<std::string, double>> factorize_phases; // host-clock ms per phase
-    DevBuf<double> refresh_vals; // CSC values staging kept across values-only refactorizations
+    DevBuf<double> refresh_vals; // CSC values on the device (kept: nnz doubles)
     // Pinned double buffer for large uploads from pageable host memory (the CSC values).
     static constexpr size_t STAGE_BYTES = (size_t)16 << 20;
     char *h_stage = nullptr;
@@ -498,7 +498,21 @@ struct mas_solver
             throw Error(ERR_INVALID, "[MAS] A is too large. Non-zero number exceeding int32 max.");
         const int bd_ = p.block_dim;
         const int V_ = (n_ + bd_ - 1) / bd_;
-        const uint64_t h = pattern_hash(n_, outer, inner, nnz_);
+        // The pattern hash (host threads) runs while the values go to the device: both paths
+        // below need them there.
+        uint64_t h = 0;
+        std::thread hasher([&] { h = pattern_hash(n_, outer, inner, nnz_); });
+        try
+        {
+            refresh_vals.alloc(nnz_ > 0 ? nnz_ : 1, "MAS permuted_bsr input_csc");
+            upload_pageable(refresh_vals.get(), vals, sizeof(double) * (size_t)nnz_);
+        }
+        catch (...)
+        {
+            hasher.join();
+            throw;
+        }
+        hasher.join();
         // The ordering is a pure function of the pattern, the positions and the ordering
         // parameter: it is rebuilt only when one of them changed (lazy_partitioning keeps it even
         // then, as the reference does, MASSolver.cu:304-320).
@@ -508,7 +522,7 @@ struct mas_solver
         const bool rebuild_order = !(shape_same && (p.lazy || inputs_same));
         const bool same_pattern = factorized && !rebuild_order && h == pattern && nnz_ == nnz && bd_ == A.bd &&
                                   mas.storage == p.storage;
-        phase("pattern_check");
+        phase("pattern_check_and_upload");
 
         if (rebuild_order)
         {
@@ -549,12 +563,7 @@ struct mas_solver
         }
         factorized = false;
         {
-            DevBuf<double> local_vals;
-            DevBuf<double> &d_vals = same_pattern ? refresh_vals : local_vals;
-            if (!same_pattern)
-                refresh_vals.reset();
-            d_vals.alloc(nnz_ > 0 ? nnz_ : 1, "MAS permuted_bsr input_csc");
-            upload_pageable(d_vals.get(), vals, sizeof(double) * (size_t)nnz_);
+            DevBuf<double> &d_vals = refresh_vals; // uploaded above
             if (same_pattern)
             {
                 rescatter_values(A, nnz_, d_vals.get(), stream);
