@@ -337,7 +337,7 @@ def run_ours(args) -> None:
         "e2e": {"value": round(e2e_value, 4), "unit": UNIT, "h2d_bytes_per_step": 8 * n, "d2h_bytes_per_step": 8 * n},
         "gpu_launches": int(gpu_launches),
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4),
+                     "frac": round(achieved / peak, 4), "frac_of_nominal_8000": round(achieved / 8000.0, 4),
                      # DRAM read + write of one spmv_pap launch on this workload from an ncu capture
                      # (dram__bytes_read.sum + dram__bytes_write.sum: 613.98 + 5.58 MB)
                      "traffic": 619.56e6 if args.grid == 80 else None,
