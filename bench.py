@@ -70,6 +70,8 @@ def parse_args():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cpu-sample-iters", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-sequence", action="store_true",
+                    help="grid80: skip the 8-step sequence run of the learned warm start")
     ap.add_argument("--seq-steps", type=int, default=20, help="sequence60: steps of the sequence")
     ap.add_argument("--seq-grid", type=int, default=60, help="sequence60: grid edge N (N^3 cells)")
     ap.add_argument("--seq-modes", default="all",
@@ -350,6 +352,21 @@ def run_ours(args) -> None:
         "kernels": kernel_table,
         "clocks": clk,
     }
+    if world == 1 and not args.no_sequence:
+        # The chosen configuration's learned warm start needs a sequence of systems: the same mesh
+        # size through 8 steps of the sequence workload (refactorized values each step), against
+        # plain FP64 MAS-PCG from x0 = 0 on the same systems.
+        sres, sdof, _ = sequence_modes(args.grid, 8, args.seed, "plain_fp64")
+        lrn, pl = sres["learned"], sres["plain_fp64"]
+        out["sequence"] = {
+            "workload": f"{args.grid}^3 sequence ({sdof} DOF), 8 steps after a 3-step warm-up",
+            "chosen_solve_ms_per_step": round((lrn["solve_ms"] + lrn["warm_start_ms"]) / 8, 3),
+            "chosen_iterations": lrn["iterations"],
+            "plain_fp64_solve_ms_per_step": round(pl["solve_ms"] / 8, 3),
+            "plain_fp64_iterations": pl["iterations"],
+            "speedup_vs_plain_fp64": round(pl["solve_ms"] / max(lrn["solve_ms"] + lrn["warm_start_ms"], 1e-9), 3),
+            "worst_relative_residual": lrn["worst_rel"],
+            "timing": "GPU events: PCG solve plus the warm-start prediction per step (factorize excluded)"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline_sample(system, chosen.ordering(), pinfo["solver_iter"],
                                                   args.cpu_sample_iters)
@@ -582,13 +599,9 @@ def run_contact16(args) -> None:
 SEQ_METRIC = "ms per step of a 60^3 sequence (refactorize values + solve to 1e-8), learned warm start"
 
 
-def run_sequence(args) -> None:
-    """Steps k = 0..S-1 of the 60^3 sequence (E_k = E_0 (1 + 0.3 sin(2 pi k / 50 + phase)), b_k a
-    sum of drifting Gaussian bumps): each step refactorizes the new values (same pattern) and
-    solves. Starting guesses: zero, the previous solution (the learned mode's fallback), the linear
-    extrapolation, the Galerkin combination of the last two solutions alone ("projection": the
-    learned pipeline with an all-zero network) and the learned warm start. A timed step is the
-    whole sequence for one mode; value = ms per sequence step of the learned warm start."""
+def sequence_modes(N: int, S: int, seed: int, mode_filter: str = "all") -> tuple[dict, int, int]:
+    """Runs the N^3 sequence (steps 0..S-1) once per starting-guess mode, after a 3-step warm-up;
+    returns ({mode: totals}, DOF, nnz)."""
     import numpy as np
     import torch
 
@@ -596,23 +609,18 @@ def run_sequence(args) -> None:
     from polysolve_b200 import warmstart as W
     from polysolve_b200.sequence import solve_sequence
 
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    rank = int(os.environ.get("RANK", "0"))
-    torch.cuda.set_device(local)
-    S = args.seq_steps
-    N = args.seq_grid
     systems, rhs = [], []
     for k in range(S):
-        sk, bk = synthetic.workload_sequence60(k, seed=args.seed, N=N)
+        sk, bk = synthetic.workload_sequence60(k, seed=seed, N=N)
         systems.append(sk.scipy())
         rhs.append(bk)
-    pos = synthetic.workload_sequence60(0, seed=args.seed, N=N)[0].positions
+    pos = synthetic.workload_sequence60(0, seed=seed, N=N)[0].positions
     res = {}
     modes = {"plain_fp64": ("zero", None), "zero": ("input", None), "previous": ("input", None),
              "extrapolate": ("input", None), "projection": ("learned", np.zeros(W.PARAMS, dtype=np.float32)),
              "learned": ("learned", W.default_weights())}
-    if args.seq_modes != "all":
-        keep = set(args.seq_modes.split(","))
+    if mode_filter != "all":
+        keep = set(mode_filter.split(","))
         modes = {m: v for m, v in modes.items() if m in keep or m in ("learned",)}
     for mode, (guess, model) in modes.items():
         sv = Solver.create("MAS", "")
@@ -649,6 +657,29 @@ def run_sequence(args) -> None:
                      "worst_rel": max(r["rel"] for r in out),
                      "factorize_phases_ms_per_step": {k: float(f"{v:.4g}") for k, v in phases.items()}}
         del sv
+    return res, systems[0].shape[0], systems[0].nnz
+
+
+def run_sequence(args) -> None:
+    """Steps k = 0..S-1 of the 60^3 sequence (E_k = E_0 (1 + 0.3 sin(2 pi k / 50 + phase)), b_k a
+    sum of drifting Gaussian bumps): each step refactorizes the new values (same pattern) and
+    solves. Starting guesses: zero, the previous solution (the learned mode's fallback), the linear
+    extrapolation, the Galerkin combination of the last two solutions alone ("projection": the
+    learned pipeline with an all-zero network) and the learned warm start. A timed step is the
+    whole sequence for one mode; value = ms per sequence step of the learned warm start."""
+    import numpy as np
+    import torch
+
+    from polysolve_b200 import Solver, synthetic
+    from polysolve_b200 import warmstart as W
+    from polysolve_b200.sequence import solve_sequence
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(local)
+    S = args.seq_steps
+    N = args.seq_grid
+    res, ndof, nnz = sequence_modes(N, S, args.seed, args.seq_modes)
     lrn = res["learned"]
     prev, zero = res.get("previous", lrn), res.get("zero", lrn)
     out = {
@@ -656,7 +687,7 @@ def run_sequence(args) -> None:
         "warmup": 3, "ms_per_step": round(lrn["wall_ms"] / S, 3), "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64 (SpMV, dots, updates) + fp16 storage (MAS apply) + bf16 network",
         "data": "synthetic (seeded 60^3 sequence: sinusoidal E_k, drifting Gaussian-bump b_k)",
-        "config": {"workload": f"{N}^3 sequence, {systems[0].shape[0]} DOF, {S} steps",
+        "config": {"workload": f"{N}^3 sequence, {ndof} DOF, {S} steps",
                    "warm_start": "learned (network + Galerkin over x_{k-1}, x_{k-1} - x_{k-2}) vs projection "
                                  "(no network) vs 2 x_{k-1} - x_{k-2} vs x_{k-1} (fallback) vs zero",
                    "timing": "host clock around factorize + solve of every step"},
@@ -672,8 +703,8 @@ def run_sequence(args) -> None:
                                              max(lrn["solve_ms"] + lrn["warm_start_ms"], 1e-9), 3)
         if "plain_fp64" in res else None,
         "e2e": {"value": round(lrn["wall_ms"] / S, 3), "unit": "ms/step",
-                "h2d_bytes_per_step": int(8 * systems[0].shape[0] + 12 * systems[0].nnz),
-                "d2h_bytes_per_step": int(8 * systems[0].shape[0])},
+                "h2d_bytes_per_step": int(8 * ndof + 8 * nnz),
+                "d2h_bytes_per_step": int(8 * ndof)},
     }
     if rank == 0:
         print(json.dumps(out), flush=True)
