@@ -136,3 +136,16 @@ def test_bad_model_rejected():
     bad[7] = np.nan
     with pytest.raises(Exception):
         s.set_warm_start_model(bad)
+
+
+def test_learned_mode_other_block_sizes_fall_back_to_previous():
+    """The network is defined for three displacement components per vertex: with block_dim 1
+    the learned mode starts from the previous solution and still meets the tolerance."""
+    systems = [synthetic.workload_sequence60(k, seed=6, N=5) for k in range(3)]
+    s = Solver.create("MAS", "")
+    s.set_parameters({"MAS": dict(PARAMS, block_dim=1, initial_guess="learned")})
+    s.analyze_pattern(systems[0][0].scipy(), systems[0][0].n)
+    s.set_warm_start_model()
+    res = solve_sequence(s, [sk.scipy() for sk, _ in systems], [bk for _, bk in systems], "learned")
+    assert [r["x0_source"] for r in res] == ["zero", "previous", "previous"]
+    assert all(r["rel"] <= 5e-8 for r in res)
