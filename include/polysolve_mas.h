@@ -190,9 +190,10 @@ int mas_debug_spmv_multi(mas_solver *h, const double *xin, double *yout, int len
 /* Test hook of the learned warm start: the prediction for caller-order b and nhist (2 to 4) kept
  * solutions history[j * n ..] (x_{k-1} first) without a solve. Outputs (each may be NULL):
  * c_out[n] the network's correction, x0_out[n] the starting guess, features_out[nverts * 16] the
- * raw per-vertex features, state_out[34] = feature sums (5), Galerkin matrix (upper triangle by
+ * raw per-vertex features, state_out[39] = feature sums (5), Galerkin matrix (upper triangle by
  * rows, 15) and right-hand side (5) of the basis {x1, x1 - x2, x2 - x3, x3 - x4, c},
- * coefficients (5), energy of x0, energy of x1, fallback flag, kept basis vectors. */
+ * coefficients (5), energy of x0, energy of x1, fallback flag, kept basis vectors, and the
+ * coefficients of x_g, the first pass over the basis without c (5). */
 int mas_debug_warm_start(mas_solver *h, const double *b, const double *history, int nhist, double *c_out,
                          double *x0_out, float *features_out, double *state_out);
 

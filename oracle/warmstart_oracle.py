@@ -7,7 +7,8 @@ solver's own (features, network, Galerkin combination):
 
 * ``graph``:      neighbour weights w_ij = ||A_ij||_F / sum_{j' != i} ||A_ij'||_F over the
                   3x3 block pattern and the diagonal blocks;
-* ``features``:   the 16 raw per-vertex features and the five normalisation sums;
+* ``features``:   the 16 raw per-vertex features (from the residual of the history guess x_g)
+                  and the five normalisation sums;
 * ``forward_device``: the network as the GPU evaluates it (float32 input layer, bf16 hidden
                   states and layer weights with float32 accumulation, float32 output layer);
 * ``forward64`` / ``backward64``: the same network in float64 with its reverse pass, checked
@@ -75,10 +76,11 @@ def graph(A, bd=3):
     return src, dst, w, D
 
 
-def features(A, b, x1, x2, D):
-    """(raw features float64 [V,16], sums[5]) with r_e = b - A (2 x1 - x2)."""
+def features(A, b, x1, x2, D, xg=None):
+    """(raw features float64 [V,16], sums[5]) with the residual r_g = b - A x_g of the history
+    guess x_g (the solver's first Galerkin pass; default: the linear extrapolation 2 x1 - x2)."""
     V = D.shape[0]
-    re = b - A @ (2.0 * x1 - x2)
+    re = b - A @ ((2.0 * x1 - x2) if xg is None else xg)
     Dinv = np.linalg.inv(D)
     q = np.einsum("vij,vj->vi", Dinv, re.reshape(V, 3))
     v = (x1 - x2).reshape(V, 3)

@@ -278,7 +278,7 @@ struct mas_solver
     DevBuf<int> ws_diag;
     DevBuf<float> ws_wslot, ws_feat;
     DevBuf<uint16_t> ws_h0, ws_h1;
-    DevBuf<double> ws_c, ws_yc, ws_y[WS_HISTORY], ws_partials;
+    DevBuf<double> ws_c, ws_yc, ws_rg, ws_y[WS_HISTORY], ws_partials;
     DevBuf<WsState> ws_state;
     WsState *h_ws = nullptr; // pinned copy of the last prediction's record
     bool ws_graph_valid = false;
@@ -920,6 +920,7 @@ struct mas_solver
         ws_h1.alloc(nodes * WS_HIDDEN, "warm start scratch");
         ws_c.alloc(len, "warm start scratch");
         ws_yc.alloc(len, "warm start scratch");
+        ws_rg.alloc(len, "warm start scratch");
         for (DevBuf<double> &v : ws_y)
             v.alloc(len, "warm start scratch");
         const int capacity = std::max((int)((nodes + 255) / 256), ws_reduce_ctas());
@@ -947,6 +948,7 @@ struct mas_solver
         w.h[1] = ws_h1.get();
         w.c = ws_c.get();
         w.yc = ws_yc.get();
+        w.rg = ws_rg.get();
         w.st = ws_state.get();
         w.partials = ws_partials.get();
         w.capacity = (int)(ws_partials.n / WS_GRAM);
@@ -1013,7 +1015,7 @@ struct mas_solver
             for (int j = 0; j < have; ++j)
                 launch_spmv(SPMV_PLAIN, Av, xs[j], ws_y[j].get(), nullptr, nullptr, red(), 0, 0, stream);
         });
-        run("ws_network", 0, [&] { return launch_ws_network(Av, w, b.get(), h, stream); });
+        run("ws_network", 0, [&] { return launch_ws_network(Av, w, b.get(), h, len, stream); });
         run("spmv_plain", 1, [&] { launch_spmv(SPMV_PLAIN, Av, w.c, w.yc, nullptr, nullptr, red(), 0, 0, stream); });
         run("ws_combine", 0, [&] { return launch_ws_combine(w, b.get(), h, x.get(), len, stream); });
     }
@@ -1105,6 +1107,8 @@ struct mas_solver
             hstate[k++] = hs.energy_prev;
             hstate[k++] = hs.fallback;
             hstate[k++] = hs.rank;
+            for (double v : hs.coef_hist)
+                hstate[k++] = v;
         }
     }
 

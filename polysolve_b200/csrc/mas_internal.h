@@ -450,10 +450,11 @@ namespace pmas
 
     // ---------------------------------------------------------------------------------------
     // mas_warmstart.cu: the learned starting guess for a sequence of systems (same pattern):
-    // a message-passing network over the vertex graph predicts a correction c of the
-    // extrapolated guess 2 x1 - x2 from the residual, the diagonal blocks and the last step;
-    // x0 is the energy-minimising combination of the kept solutions x1 .. x4 (as x1 and the
-    // differences x_i - x_(i+1)) and c, x1 if that is not lower. Block size 3 only.
+    // x_g, the energy-minimising combination of the kept solutions x1 .. x4 (as x1 and the
+    // differences x_i - x_(i+1)); a message-passing network over the vertex graph predicts a
+    // correction c of x_g from its residual, the diagonal blocks and the last step; x0 is the
+    // energy-minimising combination of the same basis and c, x1 if that is not lower. Block size
+    // 3 only.
     // ---------------------------------------------------------------------------------------
     constexpr int WS_FEATURES = 16, WS_HIDDEN = 64, WS_LAYERS = 3;
     constexpr int WS_PARAMS = WS_HIDDEN * WS_FEATURES + WS_HIDDEN +
@@ -472,6 +473,7 @@ namespace pmas
         int fallback;    // 1: x0 = x1 (the combination was degenerate or not lower)
         int rank;        // basis vectors kept by the Galerkin solve
         unsigned counter[2];
+        double coef_hist[WS_BASIS]; // x_g = sum_i coef_hist_i v_i (the basis without c)
     };
 
     // The kept solutions (newest first) and their products with the current A; a missing one
@@ -491,6 +493,7 @@ namespace pmas
         float *feat;           // nodes * WS_FEATURES raw features
         uint16_t *h[2];        // nodes * WS_HIDDEN bf16 hidden states (ping-pong)
         double *c, *yc;        // correction and A c (padded order, nodes * 3)
+        double *rg;            // b - A x_g, the residual the network's features start from
         WsState *st;
         double *partials;      // WS_GRAM * capacity
         int capacity;          // CTAs of the reduced launches
@@ -498,9 +501,10 @@ namespace pmas
 
     // Neighbour weights and diagonal slots of the current values (once per factorization).
     void launch_ws_graph(const BankedView &A, const WsBuffers &w, cudaStream_t s);
-    // Features .. correction c (needs hist.y[0], hist.y[1] = A x1, A x2). Returns kernels.
+    // x_g's residual (Galerkin over the kept solutions only) into w.rg, then features ..
+    // correction c (needs hist.y = A x_i). Returns kernels.
     int launch_ws_network(const BankedView &A, const WsBuffers &w, const double *b, const WsHistory &hist,
-                          cudaStream_t s);
+                          size_t len, cudaStream_t s);
     // Galerkin combination into x (needs w.yc = A c). Returns kernels.
     int launch_ws_combine(const WsBuffers &w, const double *b, const WsHistory &hist, double *x, size_t len,
                           cudaStream_t s);

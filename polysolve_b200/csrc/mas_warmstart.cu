@@ -8,16 +8,18 @@
 //   k_ws_graph      once per factorization: each stored block's neighbour weight
 //                   ||A_ij||_F / sum_{j' != i} ||A_ij'||_F and the slot of the diagonal block.
 //   (SpMV x4)       y_i = A x_i for the kept solutions (the plain SpMV kernel).
-//   k_ws_features   per vertex: q = D^-1 r_e (r_e = b - A (2 x1 - x2)), v = x1 - x2, p = D^-1 b,
-//                   the diagonal block scaled by trace / 3, log trace; the sums the
-//                   normalisation needs (deterministic grid reduction).
+//   k_ws_gram       (first pass, without c) the Galerkin combination x_g of the kept solutions;
+//   k_ws_residual   r_g = b - A x_g from the products already at hand (no SpMV).
+//   k_ws_features   per vertex: q = D^-1 r_g, v = x1 - x2, p = D^-1 b, the diagonal block scaled
+//                   by trace / 3, log trace; the sums the normalisation needs (deterministic
+//                   grid reduction).
 //   k_ws_input      h = relu(W_in f + b_in) with the normalised features (FP32, BF16 out).
 //   k_ws_layer x3   m = sum_j w_ij h_j (gathered from L2 into shared memory), then
 //                   h += relu(W_l [h ; m] + b_l) on the tensor cores: BF16 mma.sync m16n8k16
 //                   with FP32 accumulation, 64 vertices x 64 outputs x K = 128 per CTA.
 //   k_ws_output     c = s_q (W_out h + b_out) (FP32 weights, FP64 out).
 //   (SpMV)          y3 = A c.
-//   k_ws_gram       the 5 x 5 Galerkin system of the basis {x1, x1 - x2, x2 - x3, x3 - x4, c}
+//   k_ws_gram       (second pass) the 5 x 5 Galerkin system of the basis {x1, x1 - x2, x2 - x3, x3 - x4, c}
 //                   and its right-hand side (20 dots, deterministic); the last CTA solves it
 //                   with a pivoted Cholesky that drops dependent (or missing) vectors and falls
 //                   back to x1 unless the energy 1/2 x.Ax - x.b drops below that of x1. The
@@ -123,9 +125,8 @@ namespace pmas
 
         __global__ void __launch_bounds__(WT)
             k_ws_features(BankedView A, const int *__restrict__ diag_slot, const double *__restrict__ b,
-                          const double *__restrict__ x1, const double *__restrict__ x2,
-                          const double *__restrict__ y1, const double *__restrict__ y2, float *__restrict__ feat,
-                          WsState *ws, double *partials)
+                          const double *__restrict__ rg, const double *__restrict__ x1,
+                          const double *__restrict__ x2, float *__restrict__ feat, WsState *ws, double *partials)
         {
             const int u = blockIdx.x * WT + threadIdx.x;
             double sums[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
@@ -153,7 +154,7 @@ namespace pmas
                         {
                             const long long k = (long long)u * 3 + i;
                             bv[i] = b[k];
-                            re[i] = bv[i] - (2.0 * y1[k] - y2[k]);
+                            re[i] = rg[k];
                             v[i] = x1[k] - x2[k];
                         }
 #pragma unroll
@@ -497,8 +498,8 @@ namespace pmas
                 v[i] = h.x[i - 1][k] - h.x[i][k];
                 av[i] = h.y[i - 1][k] - h.y[i][k];
             }
-            v[NB - 1] = c[k];
-            av[NB - 1] = yc[k];
+            v[NB - 1] = c ? c[k] : 0.0; // first pass: no c yet
+            av[NB - 1] = c ? yc[k] : 0.0;
         }
 
         // The Galerkin system of the basis; the last CTA solves it.
@@ -641,6 +642,27 @@ namespace pmas
             }
         }
 
+        // r_g = b - A x_g with x_g the first pass's combination (A x_g from the y_i); also keeps
+        // the first pass's coefficients.
+        __global__ void __launch_bounds__(WT) k_ws_residual(const double *__restrict__ b, WsHistory h,
+                                                            WsState *ws, double *__restrict__ rg, size_t len)
+        {
+            double cf[NB];
+#pragma unroll
+            for (int i = 0; i < NB; ++i)
+                cf[i] = ws->coef[i];
+            for (size_t k = (size_t)blockIdx.x * WT + threadIdx.x; k < len; k += (size_t)gridDim.x * WT)
+            {
+                double ax = cf[0] * h.y[0][k];
+#pragma unroll
+                for (int i = 1; i < WS_HISTORY; ++i)
+                    ax += cf[i] * (h.y[i - 1][k] - h.y[i][k]);
+                rg[k] = b[k] - ax;
+            }
+            if (blockIdx.x == 0 && threadIdx.x < NB)
+                ws->coef_hist[threadIdx.x] = cf[threadIdx.x];
+        }
+
         __global__ void k_ws_features_out(int V, const int *__restrict__ padded, const float *__restrict__ feat,
                                           float *__restrict__ out)
         {
@@ -666,17 +688,22 @@ namespace pmas
     }
 
     int launch_ws_network(const BankedView &A, const WsBuffers &w, const double *b, const WsHistory &hist,
-                          cudaStream_t s)
+                          size_t len, cudaStream_t s)
     {
         const double *x1 = hist.x[0], *x2 = hist.x[1];
         const int nodes = A.banks * 32;
         if (nodes == 0)
             return 0;
         const int grid_v = (nodes + WT - 1) / WT;
-        if (grid_v > w.capacity)
+        const int grid_r = ws_reduce_ctas();
+        if (grid_v > w.capacity || grid_r > w.capacity)
             throw Error(ERR_INVALID, "[MAS] warm start reduction scratch too small");
-        k_ws_features<<<grid_v, WT, 0, s>>>(A, w.diag_slot, b, x1, x2, hist.y[0], hist.y[1], w.feat, w.st,
-                                            w.partials);
+        // First pass: x_g over the kept solutions alone, and its residual.
+        k_ws_gram<<<grid_r, WT, 0, s>>>(b, hist, nullptr, nullptr, len, w.st, w.partials);
+        cuda_check(cudaGetLastError(), "warm start gram launch");
+        k_ws_residual<<<grid_r, WT, 0, s>>>(b, hist, w.st, w.rg, len);
+        cuda_check(cudaGetLastError(), "warm start residual launch");
+        k_ws_features<<<grid_v, WT, 0, s>>>(A, w.diag_slot, b, w.rg, x1, x2, w.feat, w.st, w.partials);
         cuda_check(cudaGetLastError(), "warm start features launch");
         const int grid_b = (A.banks + WT / 32 - 1) / (WT / 32);
         k_ws_input<<<grid_b, WT, 0, s>>>(nodes, A.rowlen, w.diag_slot, w.feat, w.params, w.st,
@@ -694,7 +721,7 @@ namespace pmas
                                           reinterpret_cast<const __nv_bfloat162 *>(w.h[WS_LAYERS & 1]), w.params, w.st,
                                           w.c);
         cuda_check(cudaGetLastError(), "warm start output launch");
-        return 3 + WS_LAYERS;
+        return 5 + WS_LAYERS;
     }
 
     int launch_ws_combine(const WsBuffers &w, const double *b, const WsHistory &hist, double *x, size_t len,

@@ -375,7 +375,8 @@ class Solver:
     def debug_warm_start(self, b: np.ndarray, *history: np.ndarray) -> dict:
         """Test hook: the learned starting guess for b given 2 to 4 kept solutions (x_{k-1} first,
         caller order), without a solve: c, x0, raw features (nverts, 16) and the reduction record
-        (Galerkin matrix / right-hand side of the basis {x1, x1 - x2, x2 - x3, x3 - x4, c})."""
+        (Galerkin matrix / right-hand side of the basis {x1, x1 - x2, x2 - x3, x3 - x4, c}; the
+        coefficients of x_g, the first pass without c, in ``coef_history``)."""
         from . import warmstart
 
         b = np.ascontiguousarray(b, dtype=np.float64)
@@ -386,14 +387,14 @@ class Solver:
         feat = np.empty(((n + 2) // 3, warmstart.FEATURES), dtype=np.float32)
         nb = warmstart.BASIS
         ng = nb * (nb + 1) // 2 + nb
-        state = np.empty(5 + ng + nb + 4)
+        state = np.empty(5 + ng + nb + 4 + nb)
         _check(library().mas_debug_warm_start(self._h, b.ctypes.data, hist.ctypes.data, int(hist.shape[0]),
                                               c.ctypes.data, x0.ctypes.data, feat.ctypes.data, state.ctypes.data),
                self._h)
         e = 5 + ng
         return {"c": c, "x0": x0, "features": feat, "sums": state[0:5], "gram": state[5:e], "coef": state[e:e + nb],
                 "energy": state[e + nb], "energy_previous": state[e + nb + 1], "fallback": bool(state[e + nb + 2]),
-                "rank": int(state[e + nb + 3])}
+                "rank": int(state[e + nb + 3]), "coef_history": state[e + nb + 4:e + 2 * nb + 4]}
 
     def debug_spmv_multi(self, X_padded: np.ndarray) -> np.ndarray:
         x = np.ascontiguousarray(X_padded, dtype=np.float64)

@@ -4,13 +4,17 @@ The solver's ``initial_guess: "learned"`` mode keeps the last four solutions of 
 systems on the device and predicts the next starting guess from them, b and the diagonal blocks
 (all on the GPU, ``csrc/mas_warmstart.cu``):
 
-1. ``x_e = 2 x_{k-1} - x_{k-2}`` and ``r_e = b - A x_e`` (two SpMVs);
+1. ``y_j = A x_{k-j}`` for the kept solutions (one SpMV each), the history guess ``x_g``: the
+   Galerkin (energy-minimising) combination of x_{k-1} and the differences
+   x_{k-1} - x_{k-2}, x_{k-2} - x_{k-3}, x_{k-3} - x_{k-4} (a polynomial extrapolation in the
+   step index fitted in the energy norm; missing ones are dropped), and ``r_g = b - A x_g``
+   (from the y_j, no SpMV);
 2. per vertex i, with D_i the 3x3 diagonal block and t_i = trace(D_i) / 3, the 16 input features
 
    ====== =====================================  ==========================================
    index  raw value                               normalisation
    ====== =====================================  ==========================================
-   0-2    q_i = D_i^-1 r_e,i                      / s_q = rms of q over all real DOFs
+   0-2    q_i = D_i^-1 r_g,i                      / s_q = rms of q over all real DOFs
    3-5    v_i = x_{k-1,i} - x_{k-2,i}             / s_v = rms of v
    6-8    p_i = D_i^-1 b_i                        / s_p = rms of p
    9-11   D_i[0,0], D_i[1,1], D_i[2,2]            / t_i
@@ -27,12 +31,11 @@ systems on the device and predicts the next starting guess from them, b and the 
 
    On the GPU the hidden states and the layer weights W_l are BF16 (tensor-core products,
    FP32 accumulation); W_in, W_out and the biases stay FP32;
-4. the starting guess is the Galerkin (energy-minimising) combination of x_{k-1}, the
-   differences x_{k-1} - x_{k-2}, x_{k-2} - x_{k-3}, x_{k-3} - x_{k-4} of the kept solutions
-   (a polynomial extrapolation in the step index, fitted in the energy norm; missing ones are
-   dropped) and c; if its energy is not below that of x_{k-1} (or the system is degenerate),
-   the guess falls back to x_{k-1}. PCG then runs to the tolerance as usual, so every accepted
-   solve meets the same relative residual as a cold start.
+4. the starting guess is the Galerkin combination of the same basis plus c (the network is
+   trained on the error of x_g, so c is the part the history cannot extrapolate); if its energy
+   is not below that of x_{k-1} (or the system is degenerate), the guess falls back to x_{k-1}.
+   PCG then runs to the tolerance as usual, so every accepted solve meets the same relative
+   residual as a cold start.
 
 Weight file (``.psws``): 8 bytes ``PSWSMPN1``, four little-endian int32 (features 16,
 hidden 64, layers 3, parameter count), then the parameters as little-endian float32 in the

@@ -6,11 +6,12 @@ residual of 1e-12 on the host (a sparse LU of the first step's matrix preconditi
 following steps, whose matrices differ by a few percent). A sample is step k of a sequence with
 the two previous solutions: (A_k, b_k, x_{k-1}, x_{k-2}, x_k).
 
-Objective: the network's correction c should point along the error of the extrapolated guess,
-e = x_k - x_e, in the energy norm. With the optimal step along c (the solver's Galerkin
-combination does at least as well), the remaining squared energy error is
-||e||_A^2 (1 - rho) with rho = (c . r_e)^2 / ((c . A c) (e . r_e)), r_e = A e. The loss is the
-mean of 1 - rho, which is invariant to the scale of c.
+Objective: the network's correction c should point along the error of the history guess
+x_g (the energy-minimising combination of the kept solutions x_{k-1} .. x_{k-4}, as the solver
+computes it before the network), e = x_k - x_g, in the energy norm. With the optimal step along c
+(the solver's final Galerkin combination does at least as well), the remaining squared energy
+error is ||e||_A^2 (1 - rho) with rho = (c . r_g)^2 / ((c . A c) (e . r_g)), r_g = A e. The loss
+is the mean of 1 - rho, which is invariant to the scale of c.
 
 Run ``python -m polysolve_b200.warmstart_train --out polysolve_b200/data/warm_start_mpnn.psws``
 to regenerate the shipped weights (seeded; data generation and training take tens of minutes
@@ -59,10 +60,32 @@ def block_graph(A, bd: int = 3):
     return src.astype(np.int64), dst.astype(np.int64), w, D
 
 
-def features(A, b, x1, x2, D):
-    """(f[V, 16] float64, s_q, r_e, x_e) of the definitions in ``polysolve_b200.warmstart``."""
+def history_guess(A, b, hist):
+    """x_g: the energy-minimising combination of x1 and the differences of consecutive kept
+    solutions (``hist`` newest first, 2 to 4 of them), with the solver's rule of dropping
+    vectors whose Cholesky pivot falls below 1e-10 of their diagonal."""
+    V = [hist[0]] + [hist[i - 1] - hist[i] for i in range(1, len(hist))]
+    AV = [A @ v for v in V]
+    G = np.array([[vi @ avj for avj in AV] for vi in V])
+    g = np.array([v @ b for v in V])
+    keep = []
+    for i in range(len(V)):
+        if not G[i, i] > 0:
+            continue
+        d = G[i, i] - (G[i, keep] @ np.linalg.solve(G[np.ix_(keep, keep)], G[keep, i]) if keep else 0.0)
+        if d > 1e-10 * G[i, i]:
+            keep.append(i)
+    y = np.zeros(len(V))
+    if keep:
+        y[keep] = np.linalg.solve(G[np.ix_(keep, keep)], g[keep])
+    return sum(yi * vi for yi, vi in zip(y, V))
+
+
+def features(A, b, x1, x2, D, xg=None):
+    """(f[V, 16] float64, s_q, r_g, x_g) of the definitions in ``polysolve_b200.warmstart``;
+    x_g defaults to the linear extrapolation 2 x1 - x2."""
     V = D.shape[0]
-    xe = 2.0 * x1 - x2
+    xe = 2.0 * x1 - x2 if xg is None else xg
     re = b - A @ xe
     Dinv = np.linalg.inv(D)
     q = np.einsum("vij,vj->vi", Dinv, re.reshape(V, 3))
@@ -129,8 +152,10 @@ def make_samples(job):
     for k in range(2, steps):
         A = systems[k]
         src, dst, w, D = block_graph(A)
-        f, s_q, re, xe = features(A, rhs[k], xs[k - 1], xs[k - 2], D)
-        e = xs[k] - xe
+        hist = [xs[k - j] for j in range(1, min(k, W.HISTORY) + 1)]
+        xg = history_guess(A, rhs[k], hist)
+        f, s_q, re, _ = features(A, rhs[k], xs[k - 1], xs[k - 2], D, xg)
+        e = xs[k] - xg
         out.append({
             "N": N, "f": f.astype(np.float32), "src": src, "dst": dst, "w": w.astype(np.float32),
             "A_indptr": A.indptr.astype(np.int32), "A_indices": A.indices.astype(np.int32),

@@ -99,13 +99,19 @@ def test_training_features_match_oracle():
     rng = np.random.default_rng(5)
     x1, x2 = rng.standard_normal(s0.n), rng.standard_normal(s0.n)
     src, dst, w, D = T.block_graph(A)
-    f, sq, _, _ = T.features(A, b, x1, x2, D)
+    x3 = rng.standard_normal(s0.n)
+    xg = T.history_guess(A, b, [x1, x2, x3])
+    f, sq, _, _ = T.features(A, b, x1, x2, D, xg)
     src_o, dst_o, w_o, D_o = WO.graph(A)
     order_t = np.lexsort((src, dst))
     order_o = np.lexsort((src_o, dst_o))
     assert np.array_equal(src[order_t], src_o[order_o]) and np.array_equal(dst[order_t], dst_o[order_o])
     assert np.allclose(w[order_t], w_o[order_o], rtol=1e-14)
-    raw, sums = WO.features(A, b, x1, x2, D_o)
+    raw, sums = WO.features(A, b, x1, x2, D_o, xg)
+    # the training's history guess follows the oracle's Galerkin rule (no c)
+    y, _, _, _, _ = WO.galerkin(A, b, x1, x2, np.zeros_like(b), x3)
+    xg_o = sum(yi * vi for yi, vi in zip(y, WO.galerkin_basis((x1, x2, x3), np.zeros_like(b))))
+    assert np.linalg.norm(xg - xg_o) <= 1e-8 * np.linalg.norm(xg_o)
     fo = WO.normalise(raw, sums)
     assert np.allclose(f, fo, rtol=1e-10, atol=1e-12)
     assert abs(sq - WO.s_q(sums)) <= 1e-12 * sq

@@ -51,7 +51,14 @@ def test_prediction_matches_oracle(params):
     d = s.debug_warm_start(b, x1, x2, x3, x4)
 
     src, dst, w, D = WO.graph(A)
-    raw, sums = WO.features(A, b, x1, x2, D)
+    # the first pass (history only) against the oracle's Galerkin rule, then the features from
+    # the device's x_g
+    basis = WO.galerkin_basis((x1, x2, x3, x4), np.zeros_like(b))
+    yh, _, _, _, _ = WO.galerkin(A, b, x1, x2, np.zeros_like(b), x3, x4)
+    xg_orc = sum(yi * vi for yi, vi in zip(yh, basis))
+    xg = sum(yi * vi for yi, vi in zip(d["coef_history"], basis))
+    assert np.linalg.norm(xg - xg_orc) <= 1e-7 * np.linalg.norm(xg_orc)
+    raw, sums = WO.features(A, b, x1, x2, D, xg)
     scale = np.maximum(np.abs(raw).max(axis=0), 1e-300)
     assert np.all(np.abs(d["features"] - raw) <= 1e-6 * scale + 1e-6 * np.abs(raw))
     assert np.allclose(d["sums"], sums, rtol=1e-10)
