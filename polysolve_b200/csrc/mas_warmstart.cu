@@ -82,22 +82,26 @@ namespace pmas
             const int bank = u >> 5, lane = u & 31;
             const long long s0 = A.slice[bank];
             const int len = A.rowlen[u];
+            // One pass over the row's blocks (norms kept in wslot), then the normalisation.
             double tot = 0.0;
             int dslot = -1;
             for (int k = 0; k < len; ++k)
             {
                 const int col = A.cols[(s0 + k) * 32 + lane];
+                float nrm = 0.f;
                 if (col == u)
                     dslot = k;
                 else
-                    tot += block_fro(A, s0 + k, lane);
+                {
+                    const double f = block_fro(A, s0 + k, lane);
+                    tot += f;
+                    nrm = (float)f;
+                }
+                wslot[(s0 + k) * 32 + lane] = nrm;
             }
+            const float inv = (tot > 0.0) ? (float)(1.0 / tot) : 0.f;
             for (int k = 0; k < len; ++k)
-            {
-                const int col = A.cols[(s0 + k) * 32 + lane];
-                const float w = (col == u || !(tot > 0.0)) ? 0.f : (float)(block_fro(A, s0 + k, lane) / tot);
-                wslot[(s0 + k) * 32 + lane] = w;
-            }
+                wslot[(s0 + k) * 32 + lane] *= inv;
             diag_slot[u] = dslot;
         }
 
