@@ -1011,9 +1011,11 @@ struct mas_solver
             h.x[j] = xs[src];
             h.y[j] = ws_y[src].get();
         }
-        run("spmv_plain", have, [&] {
+        run("spmv_vectors", 1, [&] {
+            double *ys[WS_HISTORY];
             for (int j = 0; j < have; ++j)
-                launch_spmv(SPMV_PLAIN, Av, xs[j], ws_y[j].get(), nullptr, nullptr, red(), 0, 0, stream);
+                ys[j] = ws_y[j].get();
+            launch_spmv_vectors(Av, xs, ys, have, stream); // one pass over A for all kept solutions
         });
         run("ws_network", 0, [&] { return launch_ws_network(Av, w, b.get(), h, len, stream); });
         run("spmv_plain", 1, [&] { launch_spmv(SPMV_PLAIN, Av, w.c, w.yc, nullptr, nullptr, red(), 0, 0, stream); });

@@ -331,6 +331,9 @@ namespace pmas
     // period > 0 (SPMV_RESIDUAL in the PCG loop): runs only when (st->iter + 1) % period == 0.
     void launch_spmv(int mode, const BankedView &A, const double *x, double *y, const double *b, PcgState *st,
                      ReduceBuf red, int iter, int period, cudaStream_t s);
+    // y_v = A x_v for count (1..4) separate vectors in one pass over A.
+    constexpr int SPMV_MAX_VECTORS = 4;
+    void launch_spmv_vectors(const BankedView &A, const double *const *x, double *const *y, int count, cudaStream_t s);
 
     // mas_pcg.cu
     // x += alpha p; unless this iteration recomputes the true residual ((st->iter + 1) % period == 0):

@@ -160,7 +160,120 @@ namespace pmas
             }
             cuda_check(cudaGetLastError(), "spmv launch");
         }
+        struct VecPtrs
+        {
+            const double *x[SPMV_MAX_VECTORS];
+            double *y[SPMV_MAX_VECTORS];
+        };
+
+        // y_v = A x_v for NV separate vectors: each block of A is read once and applied to all of
+        // them (the learned warm start's products with the kept solutions).
+        template <int BD, int NV>
+        __global__ void __launch_bounds__(SPMV_THREADS, 1) k_spmv_vectors(BankedView A, VecPtrs v)
+        {
+            constexpr int BS = BD * BD;
+            constexpr int PAIRS = BS / 2;
+            const int lane = threadIdx.x & 31;
+            const int bank = blockIdx.x * BANKS_PER_CTA + (threadIdx.x >> 5);
+            if (bank >= A.banks)
+                return;
+            const int u = bank * 32 + lane;
+            const long long s0 = A.slice[bank];
+            const int len = A.rowlen[u];
+            const int *cp = A.cols + s0 * 32 + lane;
+            const double *vp = A.vals + s0 * 32 * BS;
+            double acc[NV][BD];
+#pragma unroll
+            for (int q = 0; q < NV; ++q)
+#pragma unroll
+                for (int i = 0; i < BD; ++i)
+                    acc[q][i] = 0.0;
+            const uint64_t pol = l2_evict_first_policy();
+            for (int k = 0; k < len; ++k)
+            {
+                const int col = ld_stream_s32(cp + (long long)k * 32, pol);
+                const double *blk = vp + (long long)k * 32 * BS;
+                double m[BS];
+#pragma unroll
+                for (int p = 0; p < PAIRS; ++p)
+                {
+                    const double2 t = ld_stream_f64x2(blk + p * 64 + lane * 2, pol);
+                    m[2 * p] = t.x;
+                    m[2 * p + 1] = t.y;
+                }
+                if (BS & 1)
+                    m[BS - 1] = ld_stream_f64(blk + PAIRS * 64 + lane, pol);
+#pragma unroll
+                for (int q = 0; q < NV; ++q)
+                {
+                    double xc[BD];
+#pragma unroll
+                    for (int j = 0; j < BD; ++j)
+                        xc[j] = __ldg(v.x[q] + (long long)col * BD + j);
+#pragma unroll
+                    for (int i = 0; i < BD; ++i)
+#pragma unroll
+                        for (int j = 0; j < BD; ++j)
+                            acc[q][i] = fma(m[i * BD + j], xc[j], acc[q][i]);
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < NV; ++q)
+#pragma unroll
+                for (int i = 0; i < BD; ++i)
+                    v.y[q][(long long)u * BD + i] = acc[q][i];
+        }
+
+        template <int BD>
+        void launch_vectors_bd(const BankedView &A, const VecPtrs &v, int count, cudaStream_t s)
+        {
+            const int grid = (A.banks + BANKS_PER_CTA - 1) / BANKS_PER_CTA;
+            if (grid == 0)
+                return;
+            switch (count)
+            {
+            case 1:
+                k_spmv_vectors<BD, 1><<<grid, SPMV_THREADS, 0, s>>>(A, v);
+                break;
+            case 2:
+                k_spmv_vectors<BD, 2><<<grid, SPMV_THREADS, 0, s>>>(A, v);
+                break;
+            case 3:
+                k_spmv_vectors<BD, 3><<<grid, SPMV_THREADS, 0, s>>>(A, v);
+                break;
+            default:
+                k_spmv_vectors<BD, 4><<<grid, SPMV_THREADS, 0, s>>>(A, v);
+                break;
+            }
+            cuda_check(cudaGetLastError(), "spmv vectors launch");
+        }
     } // namespace
+
+    void launch_spmv_vectors(const BankedView &A, const double *const *x, double *const *y, int count, cudaStream_t s)
+    {
+        if (count < 1 || count > SPMV_MAX_VECTORS)
+            throw Error(ERR_INVALID, "[MAS] internal: 1 to 4 vectors per SpMV pass");
+        VecPtrs v{};
+        for (int q = 0; q < count; ++q)
+        {
+            v.x[q] = x[q];
+            v.y[q] = y[q];
+        }
+        switch (A.bd)
+        {
+        case 1:
+            launch_vectors_bd<1>(A, v, count, s);
+            break;
+        case 2:
+            launch_vectors_bd<2>(A, v, count, s);
+            break;
+        case 3:
+            launch_vectors_bd<3>(A, v, count, s);
+            break;
+        default:
+            throw Error(ERR_INVALID, "[MAS] block_dim must be 1, 2 or 3");
+        }
+    }
 
     void launch_spmv(int mode, const BankedView &A, const double *x, double *y, const double *b, PcgState *st,
                      ReduceBuf red, int iter, int period, cudaStream_t s)
