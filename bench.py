@@ -618,14 +618,17 @@ def sequence_modes(N: int, S: int, seed: int, mode_filter: str = "all") -> tuple
     res = {}
     modes = {"plain_fp64": ("zero", None), "zero": ("input", None), "previous": ("input", None),
              "extrapolate": ("input", None), "projection": ("learned", np.zeros(W.PARAMS, dtype=np.float32)),
-             "learned": ("learned", W.default_weights())}
+             "learned": ("learned", W.default_weights()),
+             # the same with the MAS inverses rebuilt every third step only
+             "learned_refresh3": ("learned", W.default_weights())}
     if mode_filter != "all":
         keep = set(mode_filter.split(","))
         modes = {m: v for m, v in modes.items() if m in keep or m in ("learned",)}
     for mode, (guess, model) in modes.items():
         sv = Solver.create("MAS", "")
         base = PLAIN if mode == "plain_fp64" else CHOSEN
-        sv.set_parameters({"MAS": dict(base, initial_guess="zero" if guess == "zero" else guess)})
+        extra = {"preconditioner_refresh": 3} if mode == "learned_refresh3" else {}
+        sv.set_parameters({"MAS": dict(base, initial_guess="zero" if guess == "zero" else guess, **extra)})
         sv.set_positions(pos)
         sv.analyze_pattern(systems[0], systems[0].shape[0])
         if model is not None:

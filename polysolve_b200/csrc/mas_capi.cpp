@@ -53,6 +53,10 @@ namespace
         bool polak_ribiere = false;
         std::string ordering = "auto";
         int poll_period = 10;
+        // Values-only refactorizations rebuild the MAS inverses every this many calls (1: every
+        // call, as the reference); in between PCG runs with the current A and the last inverses,
+        // a valid preconditioner all the same (the tolerance is met as usual).
+        int preconditioner_refresh = 1;
         bool profile = false; // time every kernel launch with CUDA events
         bool graphs = true;   // replay chunks of iterations as a CUDA graph
     };
@@ -102,7 +106,7 @@ namespace
     const char *KNOWN_KEYS[] = {"block_dim", "max_iter", "relative_tolerance", "absolute_tolerance",
                                 "lazy_partitioning", "use_preconditioned_residual_norm", "precision",
                                 "true_residual_period", "check_period", "initial_guess", "beta", "ordering",
-                                "poll_period", "profile_kernels", "cuda_graphs"};
+                                "poll_period", "profile_kernels", "cuda_graphs", "preconditioner_refresh"};
 
     // MASSolverImpl::set_parameters (MASSolver.cu:198-212) plus the extension keys.
     void apply_mas_params(Params &p, const Json &m, bool strict)
@@ -186,6 +190,12 @@ namespace
             if (q.poll_period < 1)
                 throw Error(ERR_INVALID, "[MAS] poll_period must be >= 1");
         }
+        if (auto *v = m.find("preconditioner_refresh"))
+        {
+            q.preconditioner_refresh = get_int(*v, "preconditioner_refresh");
+            if (q.preconditioner_refresh < 1)
+                throw Error(ERR_INVALID, "[MAS] preconditioner_refresh must be >= 1");
+        }
         p = q;
     }
 
@@ -244,6 +254,8 @@ struct mas_solver
     long long ordered_version = -1;   // positions_version the current ordering was built from
     std::string ordered_mode;         // the ordering parameter it was built with
     int first_iso_bank_cached = 0;
+    int refreshes_skipped = 0;      // values-only refactorizations since the inverses were rebuilt
+    bool preconditioner_current = true;
 
     // Ordering / pattern state.
     int n = 0, V = 0, banks = 0, bd = 0;
@@ -593,11 +605,21 @@ struct mas_solver
         if (same_pattern)
         {
             // Values only: the coarse space, buffers and captured graphs stay valid.
-            refresh_mas_values(mas, A, d_node_real.get(), p.storage, stream); // syncs, checks pivots
-            phase("mas_inverses");
-            factorize_phases.emplace_back("gpu_level0_inverses", mas.inverse_ms[0]);
-            factorize_phases.emplace_back("gpu_coarse_sums", mas.inverse_ms[1]);
-            factorize_phases.emplace_back("gpu_coarse_inverses", mas.inverse_ms[2]);
+            if (refreshes_skipped + 1 >= p.preconditioner_refresh)
+            {
+                refresh_mas_values(mas, A, d_node_real.get(), p.storage, stream); // syncs, checks pivots
+                phase("mas_inverses");
+                factorize_phases.emplace_back("gpu_level0_inverses", mas.inverse_ms[0]);
+                factorize_phases.emplace_back("gpu_coarse_sums", mas.inverse_ms[1]);
+                factorize_phases.emplace_back("gpu_coarse_inverses", mas.inverse_ms[2]);
+                refreshes_skipped = 0;
+                preconditioner_current = true;
+            }
+            else
+            {
+                ++refreshes_skipped; // PCG uses the new A with the previous inverses
+                preconditioner_current = false;
+            }
             factorized = true;
             factorize_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
             return;
@@ -616,6 +638,8 @@ struct mas_solver
         build_mas(mas, A, d_node_real.get(), p.storage, first_iso_bank, stream);
         phase("mas_build");
         hist_count = 0; // a new pattern or ordering: the kept solutions no longer apply
+        refreshes_skipped = 0;
+        preconditioner_current = true;
         prepare_kernels(bd_, p.storage);
         if (p.storage == STORE_F16)
             prepare_kernels_g(bd_);
@@ -1474,6 +1498,7 @@ struct mas_solver
         o.obj.emplace_back("ordering", str(ordering_used));
         o.obj.emplace_back("solve_ms", num(solve_ms, false));
         o.obj.emplace_back("factorize_ms", num(factorize_ms, false));
+        o.obj.emplace_back("preconditioner_current", boolean(preconditioner_current));
         {
             Json fp;
             fp.type = Json::Object;

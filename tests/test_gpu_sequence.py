@@ -61,3 +61,34 @@ def test_values_only_refactorize_matches_fresh_solver():
     fresh(s1).solve(b, x2)
     assert not np.array_equal(x0, x1)
     assert np.array_equal(x1, x2)
+
+
+def test_preconditioner_refresh_period():
+    """preconditioner_refresh 3: two of three values-only refactorizations keep the previous
+    inverses (PCG still uses the new matrix), every solve meets the tolerance, and the iteration
+    count stays close to rebuilding every time."""
+    steps = [synthetic.workload_sequence60(k, seed=9, N=9) for k in range(7)]
+    totals, flags = {}, []
+    for period in (1, 3):
+        s = Solver.create("MAS", "")
+        s.set_parameters({"MAS": {"block_dim": 3, "relative_tolerance": 1e-8, "absolute_tolerance": 0.0,
+                                  "precision": "fp16", "preconditioner_refresh": period}})
+        s.set_positions(steps[0][0].positions)
+        s.analyze_pattern(steps[0][0].scipy(), steps[0][0].n)
+        it = 0
+        for sk, bk in steps:
+            A = sk.scipy()
+            s.factorize(A)
+            x = np.zeros(sk.n)
+            s.solve(bk, x)
+            info = s.get_info({})
+            assert info["solver_status"] == "Reach relative tolerance"
+            assert np.linalg.norm(A @ x - bk) <= 2e-8 * np.linalg.norm(bk)
+            it += info["solver_iter"]
+            if period == 3:
+                flags.append(info["preconditioner_current"])
+        totals[period] = it
+    assert flags == [True, False, False, True, False, False, True]
+    assert totals[3] <= 1.3 * totals[1], totals
+    with pytest.raises(Exception):
+        s.set_parameters({"MAS": {"preconditioner_refresh": 0}})
