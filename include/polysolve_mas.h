@@ -63,10 +63,12 @@ void mas_destroy(mas_solver *h);
  * use_preconditioned_residual_norm. Keys this implementation adds (ignored by the reference):
  * precision ("fp64" | "fp32" | "fp16": storage of the MAS inverses; fp16 keeps one power-of-two
  * scale per matrix and multiplies in FP32), true_residual_period (int, reference 4), check_period (int,
- * reference 10), initial_guess ("zero" | "input"; reference: zero), beta ("fletcher_reeves" |
- * "polak_ribiere"), ordering ("auto" | "morton" | "graph" | "natural"), poll_period (int: iterations
- * launched between looks at the device state), profile_kernels (bool: CUDA-event time per kernel
- * kind, reported by get_info). */
+ * reference 10), initial_guess ("zero" | "input" | "learned"; reference: zero), beta
+ * ("fletcher_reeves" | "polak_ribiere"), ordering ("auto" | "morton" | "graph" | "natural"),
+ * poll_period (int: iterations launched between looks at the device state), cuda_graphs (bool),
+ * preconditioner_refresh (int k: values-only refactorizations rebuild the MAS inverses every k-th
+ * time; 1, every time, as the reference), profile_kernels (bool: CUDA-event time per kernel kind,
+ * reported by get_info). */
 int mas_set_parameters(mas_solver *h, const char *params_json);
 
 /* MASSolver::get_info (MASSolver.cu:214-219): writes a JSON object with solver_iter,
