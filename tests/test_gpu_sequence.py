@@ -92,3 +92,24 @@ def test_preconditioner_refresh_period():
     assert totals[3] <= 1.3 * totals[1], totals
     with pytest.raises(Exception):
         s.set_parameters({"MAS": {"preconditioner_refresh": 0}})
+
+
+def test_pipelined_value_upload_on_a_large_system():
+    """nnz x 8 bytes above two 16 MB staging chunks: the CSC values go through the pinned double
+    buffer (full and values-only factorizations); both solves meet the tolerance against the
+    matrices on the host."""
+    s0, b0 = synthetic.workload_sequence60(0, seed=12, N=40)
+    s1, b1 = synthetic.workload_sequence60(1, seed=12, N=40)
+    assert s0.vals.size * 8 > 2 * (16 << 20)
+    s = Solver.create("MAS", "")
+    s.set_parameters({"MAS": {"block_dim": 3, "relative_tolerance": 1e-8, "absolute_tolerance": 0.0,
+                              "precision": "fp16"}})
+    s.set_positions(s0.positions)
+    s.analyze_pattern(s0.scipy(), s0.n)
+    for sk, bk in ((s0, b0), (s1, b1)):
+        A = sk.scipy()
+        s.factorize(A)
+        x = np.zeros(sk.n)
+        s.solve(bk, x)
+        assert np.linalg.norm(A @ x - bk) <= 2e-8 * np.linalg.norm(bk)
+    assert "mas_inverses" in s.get_info({})["factorize_phases_ms"]  # the second one was values-only
