@@ -224,62 +224,68 @@ namespace pmas
             return rowlen[u] > 0 && diag_slot[u] >= 0;
         }
 
-        // One warp per bank: lane o computes hidden units 2 o and 2 o + 1 of each of the bank's
-        // 32 vertices (features broadcast from global), stores coalesced 128 B rows.
+        // One thread per vertex: its 16 normalised features against W_in (shared memory, every
+        // lane reading the same weight: broadcast), 64 hidden units written as eight 16-byte
+        // stores.
         __global__ void __launch_bounds__(WT) k_ws_input(int nodes, const int *__restrict__ rowlen,
                                                          const int *__restrict__ diag_slot,
                                                          const float *__restrict__ feat, const float *__restrict__ prm,
                                                          const WsState *ws, __nv_bfloat162 *__restrict__ h)
         {
-            // W_in transposed (wsm[f * H + o]): lanes read consecutive words, no bank conflicts.
-            __shared__ float wsm[H * F + H];
-            for (int i = threadIdx.x; i < H * F; i += WT)
-                wsm[(i % F) * H + i / F] = prm[OFF_WIN + i];
-            for (int i = threadIdx.x; i < H; i += WT)
-                wsm[H * F + i] = prm[OFF_BIN + i];
+            __shared__ __align__(16) float wsm[H * F + H];
+            for (int i = threadIdx.x; i < H * F + H; i += WT)
+                wsm[i] = prm[OFF_WIN + i];
             __syncthreads();
-            const Norms nm = norms(ws);
-            const int lane = threadIdx.x & 31;
-            const int bank = blockIdx.x * (WT / 32) + (threadIdx.x >> 5);
-            if (bank * 32 >= nodes)
+            const int u = blockIdx.x * WT + threadIdx.x;
+            if (u >= nodes)
                 return;
-            const int o0 = 2 * lane, o1 = 2 * lane + 1;
-            for (int j = 0; j < 32; ++j)
+            uint4 *dst = reinterpret_cast<uint4 *>(h + (long long)u * (H / 2));
+            if (!node_real(rowlen, diag_slot, u))
             {
-                const int u = bank * 32 + j;
-                float2 out = make_float2(0.f, 0.f);
-                if (node_real(rowlen, diag_slot, u))
+#pragma unroll
+                for (int i = 0; i < H / 8; ++i)
+                    dst[i] = make_uint4(0u, 0u, 0u, 0u);
+                return;
+            }
+            const Norms nm = norms(ws);
+            const float4 *fp = reinterpret_cast<const float4 *>(feat + (long long)u * F);
+            float f[F];
+#pragma unroll
+            for (int i = 0; i < F / 4; ++i)
+            {
+                const float4 t = fp[i];
+                f[4 * i] = t.x;
+                f[4 * i + 1] = t.y;
+                f[4 * i + 2] = t.z;
+                f[4 * i + 3] = t.w;
+            }
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+            {
+                f[i] *= nm.iq;
+                f[3 + i] *= nm.iv;
+                f[6 + i] *= nm.ip;
+            }
+            f[15] -= nm.mlog;
+#pragma unroll
+            for (int c = 0; c < H / 8; ++c)
+            {
+                uint4 out;
+                __nv_bfloat162 *ob = reinterpret_cast<__nv_bfloat162 *>(&out);
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
                 {
-                    const float4 *fp = reinterpret_cast<const float4 *>(feat + (long long)u * F);
-                    float f[F];
-#pragma unroll
-                    for (int i = 0; i < F / 4; ++i)
-                    {
-                        const float4 t = fp[i];
-                        f[4 * i] = t.x;
-                        f[4 * i + 1] = t.y;
-                        f[4 * i + 2] = t.z;
-                        f[4 * i + 3] = t.w;
-                    }
-#pragma unroll
-                    for (int i = 0; i < 3; ++i)
-                    {
-                        f[i] *= nm.iq;
-                        f[3 + i] *= nm.iv;
-                        f[6 + i] *= nm.ip;
-                    }
-                    f[15] -= nm.mlog;
+                    const int o0 = c * 8 + 2 * k, o1 = o0 + 1;
                     float a0 = wsm[H * F + o0], a1 = wsm[H * F + o1];
 #pragma unroll
                     for (int i = 0; i < F; ++i)
                     {
-                        const float2 wv = *reinterpret_cast<const float2 *>(&wsm[i * H + o0]);
-                        a0 = fmaf(wv.x, f[i], a0);
-                        a1 = fmaf(wv.y, f[i], a1);
+                        a0 = fmaf(wsm[o0 * F + i], f[i], a0);
+                        a1 = fmaf(wsm[o1 * F + i], f[i], a1);
                     }
-                    out = make_float2(fmaxf(a0, 0.f), fmaxf(a1, 0.f));
+                    ob[k] = __float22bfloat162_rn(make_float2(fmaxf(a0, 0.f), fmaxf(a1, 0.f)));
                 }
-                h[(long long)u * (H / 2) + lane] = __float22bfloat162_rn(out);
+                dst[c] = out;
             }
         }
 
@@ -447,43 +453,50 @@ namespace pmas
             }
         }
 
-        // c = s_q (W_out h + b_out): one warp per bank, vertices in turn, lanes over hidden units.
+        // c = s_q (W_out h + b_out): one thread per vertex (eight 16-byte loads of its hidden row,
+        // W_out broadcast from shared memory).
         __global__ void __launch_bounds__(WT) k_ws_output(int nodes, const int *__restrict__ rowlen,
                                                           const int *__restrict__ diag_slot,
                                                           const __nv_bfloat162 *__restrict__ h,
                                                           const float *__restrict__ prm, const WsState *ws,
                                                           double *__restrict__ c)
         {
-            const int lane = threadIdx.x & 31;
-            const int bank = blockIdx.x * (WT / 32) + (threadIdx.x >> 5);
-            if (bank * 32 >= nodes)
+            __shared__ float wo[3 * H + 3];
+            for (int i = threadIdx.x; i < 3 * H + 3; i += WT)
+                wo[i] = prm[OFF_WOUT + i];
+            __syncthreads();
+            const int u = blockIdx.x * WT + threadIdx.x;
+            if (u >= nodes)
                 return;
-            const double cnt = ws->sums[4];
-            const double sq = cnt > 0.0 ? sqrt(ws->sums[0] / (3.0 * cnt)) : 0.0;
-            float w[3][2];
-#pragma unroll
-            for (int i = 0; i < 3; ++i)
+            if (!node_real(rowlen, diag_slot, u))
             {
-                w[i][0] = prm[OFF_WOUT + i * H + 2 * lane];
-                w[i][1] = prm[OFF_WOUT + i * H + 2 * lane + 1];
-            }
-            const float b0 = prm[OFF_BOUT], b1 = prm[OFF_BOUT + 1], b2 = prm[OFF_BOUT + 2];
-            for (int j = 0; j < 32; ++j)
-            {
-                const int u = bank * 32 + j;
-                const bool real = node_real(rowlen, diag_slot, u);
-                const float2 hv = __bfloat1622float2(h[(long long)u * (H / 2) + lane]);
-                float s[3];
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
-                    s[i] = warp_sum(fmaf(w[i][0], hv.x, w[i][1] * hv.y));
-                if (lane < 3)
+                    c[(long long)u * 3 + i] = 0.0;
+                return;
+            }
+            const double cnt = ws->sums[4];
+            const double sq = cnt > 0.0 ? sqrt(ws->sums[0] / (3.0 * cnt)) : 0.0;
+            const uint4 *src = reinterpret_cast<const uint4 *>(h + (long long)u * (H / 2));
+            float s3[3] = {wo[3 * H], wo[3 * H + 1], wo[3 * H + 2]};
+#pragma unroll
+            for (int ch = 0; ch < H / 8; ++ch)
+            {
+                const uint4 q = src[ch];
+                const __nv_bfloat162 *qb = reinterpret_cast<const __nv_bfloat162 *>(&q);
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
                 {
-                    const float bo = lane == 0 ? b0 : (lane == 1 ? b1 : b2);
-                    const float si = lane == 0 ? s[0] : (lane == 1 ? s[1] : s[2]);
-                    c[(long long)u * 3 + lane] = real ? sq * (double)(si + bo) : 0.0;
+                    const float2 hv = __bfloat1622float2(qb[k]);
+                    const int o = ch * 8 + 2 * k;
+#pragma unroll
+                    for (int i = 0; i < 3; ++i)
+                        s3[i] = fmaf(wo[i * H + o + 1], hv.y, fmaf(wo[i * H + o], hv.x, s3[i]));
                 }
             }
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                c[(long long)u * 3 + i] = sq * (double)s3[i];
         }
 
         constexpr int GRAM_CTAS_PER_SM = 4;
@@ -709,9 +722,8 @@ namespace pmas
         cuda_check(cudaGetLastError(), "warm start residual launch");
         k_ws_features<<<grid_v, WT, 0, s>>>(A, w.diag_slot, b, w.rg, x1, x2, w.feat, w.st, w.partials);
         cuda_check(cudaGetLastError(), "warm start features launch");
-        const int grid_b = (A.banks + WT / 32 - 1) / (WT / 32);
-        k_ws_input<<<grid_b, WT, 0, s>>>(nodes, A.rowlen, w.diag_slot, w.feat, w.params, w.st,
-                                         reinterpret_cast<__nv_bfloat162 *>(w.h[0]));
+        k_ws_input<<<(nodes + WT - 1) / WT, WT, 0, s>>>(nodes, A.rowlen, w.diag_slot, w.feat, w.params, w.st,
+                                                        reinterpret_cast<__nv_bfloat162 *>(w.h[0]));
         cuda_check(cudaGetLastError(), "warm start input launch");
         const int grid_t = (nodes + TILE - 1) / TILE;
         for (int l = 0; l < WS_LAYERS; ++l)
@@ -721,7 +733,7 @@ namespace pmas
                                             w.diag_slot, reinterpret_cast<__nv_bfloat16 *>(w.h[(l + 1) & 1]));
             cuda_check(cudaGetLastError(), "warm start layer launch");
         }
-        k_ws_output<<<grid_b, WT, 0, s>>>(nodes, A.rowlen, w.diag_slot,
+        k_ws_output<<<(nodes + WT - 1) / WT, WT, 0, s>>>(nodes, A.rowlen, w.diag_slot,
                                           reinterpret_cast<const __nv_bfloat162 *>(w.h[WS_LAYERS & 1]), w.params, w.st,
                                           w.c);
         cuda_check(cudaGetLastError(), "warm start output launch");
