@@ -43,8 +43,8 @@ namespace pmas
         constexpr int F = WS_FEATURES;
         constexpr int H = WS_HIDDEN;
         constexpr int WT = 256;         // threads of the per-vertex kernels
-        constexpr int TILE = 64;        // vertices per CTA of a layer
-        constexpr int LT = 128;         // threads of a layer CTA (4 warps x 16 vertices)
+        constexpr int TILE = 128;       // vertices per CTA of a layer
+        constexpr int LT = 256;         // threads of a layer CTA (8 warps x 16 vertices)
         constexpr int TS = 2 * H + 8;   // shared row stride (bf16): 272 B, conflict-free ldmatrix
 
         // Parameter offsets in the flat float32 vector (the .psws layout).
@@ -307,15 +307,17 @@ namespace pmas
         // One message-passing layer for 64 vertices. Shared tile T[v] = [h_v ; m_v] (bf16,
         // K = 128), W_l as rows of K (the mma's column-major B), then each warp multiplies its
         // 16 vertices by W_l^T: 8 k-steps x 8 n-tiles of m16n8k16.
-        __global__ void __launch_bounds__(LT) k_ws_layer(BankedView A, const float *__restrict__ wslot,
+        __global__ void __launch_bounds__(LT, 4) k_ws_layer(BankedView A, const float *__restrict__ wslot,
                                                          const __nv_bfloat16 *__restrict__ hin,
                                                          const uint16_t *__restrict__ wl, const float *__restrict__ bl,
                                                          const int *__restrict__ diag_slot,
                                                          __nv_bfloat16 *__restrict__ hout)
         {
-            __shared__ __align__(16) __nv_bfloat16 T[TILE * TS];
-            __shared__ __align__(16) __nv_bfloat16 Wsm[H * TS];
-            __shared__ float bias[H];
+            // Dynamic shared memory (52 KB: four CTAs, 32 warps per SM): the tile, W_l, the bias.
+            extern __shared__ __align__(16) unsigned char layer_smem[];
+            __nv_bfloat16 *T = reinterpret_cast<__nv_bfloat16 *>(layer_smem);
+            __nv_bfloat16 *Wsm = T + TILE * TS;
+            float *bias = reinterpret_cast<float *>(Wsm + H * TS);
             const int nodes = A.banks * 32;
             const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
             // W_l: 64 rows x 128 bf16 = 16 chunks of 16 B per row.
@@ -726,9 +728,13 @@ namespace pmas
                                                         reinterpret_cast<__nv_bfloat162 *>(w.h[0]));
         cuda_check(cudaGetLastError(), "warm start input launch");
         const int grid_t = (nodes + TILE - 1) / TILE;
+        constexpr int LAYER_SMEM = (TILE + H) * TS * 2 + H * 4;
+        static_assert((TILE * TS * 2) % 16 == 0 && ((TILE + H) * TS * 2) % 16 == 0, "shared layout");
+        cuda_check(cudaFuncSetAttribute(k_ws_layer, cudaFuncAttributeMaxDynamicSharedMemorySize, LAYER_SMEM),
+                   "layer smem attribute");
         for (int l = 0; l < WS_LAYERS; ++l)
         {
-            k_ws_layer<<<grid_t, LT, 0, s>>>(A, w.wslot, reinterpret_cast<const __nv_bfloat16 *>(w.h[l & 1]),
+            k_ws_layer<<<grid_t, LT, LAYER_SMEM, s>>>(A, w.wslot, reinterpret_cast<const __nv_bfloat16 *>(w.h[l & 1]),
                                             w.wl + (size_t)l * WS_LAYER_WEIGHTS, w.params + off_layer(l) + H * 2 * H,
                                             w.diag_slot, reinterpret_cast<__nv_bfloat16 *>(w.h[(l + 1) & 1]));
             cuda_check(cudaGetLastError(), "warm start layer launch");
