@@ -93,7 +93,9 @@ int mas_set_positions(mas_solver *h, const double *xyz, int nverts);
  * preconditioner on the device. The ordering is reused while the pattern, the positions and the
  * ordering parameter are unchanged (with lazy_partitioning: while n is unchanged); with the
  * same pattern only the values are re-scattered and the inverses rebuilt (the coarse space,
- * buffers and CUDA graphs are kept). */
+ * buffers and CUDA graphs are kept). Row order inside a column is free; row indices outside
+ * [0, n), decreasing column pointers or outer[n] != nnz give MAS_ERR_INVALID before the pattern
+ * is used (checked in the same host pass that hashes the pattern). */
 int mas_factorize_csc(mas_solver *h, int n, const int *outer, const int *inner, const double *vals, int nnz);
 
 /* MASSolver::solve(b, x) (MASSolver.cu:376-409): host vectors of length n. With initial_guess

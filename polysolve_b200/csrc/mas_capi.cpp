@@ -513,7 +513,8 @@ struct mas_solver
         // The pattern hash (host threads) runs while the values go to the device: both paths
         // below need them there.
         uint64_t h = 0;
-        std::thread hasher([&] { h = pattern_hash(n_, outer, inner, nnz_); });
+        bool pattern_ok = false;
+        std::thread hasher([&] { h = pattern_hash(n_, outer, inner, nnz_, &pattern_ok); });
         try
         {
             refresh_vals.alloc(nnz_ > 0 ? nnz_ : 1, "MAS permuted_bsr input_csc");
@@ -525,6 +526,8 @@ struct mas_solver
             throw;
         }
         hasher.join();
+        if (!pattern_ok)
+            throw Error(ERR_INVALID, "[MAS] Invalid CSC: row index out of range or decreasing column pointers.");
         // The ordering is a pure function of the pattern, the positions and the ordering
         // parameter: it is rebuilt only when one of them changed (lazy_partitioning keeps it even
         // then, as the reference does, MASSolver.cu:304-320).
@@ -1887,6 +1890,10 @@ extern "C" int mas_order_blocks(int n, const int *outer, const int *inner, int b
     try
     {
         const int V = (n + block_dim - 1) / block_dim;
+        bool pattern_ok = false;
+        pattern_hash(n, outer, inner, outer[n], &pattern_ok);
+        if (!pattern_ok)
+            return MAS_ERR_INVALID;
         std::vector<uint8_t> iso = isolated_blocks(n, outer, inner, block_dim);
         std::vector<int> p;
         const std::string m = mode;

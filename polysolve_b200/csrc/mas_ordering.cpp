@@ -270,33 +270,44 @@ namespace pmas
         return padded;
     }
 
-    uint64_t pattern_hash(int n, const int *outer, const int *inner, long long nnz)
+    uint64_t pattern_hash(int n, const int *outer, const int *inner, long long nnz, bool *valid)
     {
         const int chunks = 256;
         std::vector<uint64_t> part(chunks, 0);
+        std::vector<uint8_t> bad(chunks, 0);
 #pragma omp parallel for schedule(static)
         for (int c = 0; c < chunks; ++c)
         {
             const long long lo = nnz * c / chunks, hi = nnz * (c + 1) / chunks;
             uint64_t h = 1469598103934665603ull ^ (uint64_t)c;
+            uint32_t out_of_range = 0; // negative rows wrap to large unsigned values
             for (long long k = lo; k < hi; ++k)
             {
-                h ^= (uint64_t)(uint32_t)inner[k];
+                const uint32_t i = (uint32_t)inner[k];
+                out_of_range |= (uint32_t)(i >= (uint32_t)n);
+                h ^= (uint64_t)i;
                 h *= 1099511628211ull;
             }
             part[c] = h;
+            bad[c] = (uint8_t)out_of_range;
         }
         uint64_t h = 1469598103934665603ull ^ (uint64_t)n ^ ((uint64_t)nnz << 20);
+        bool ok = outer[0] == 0 && (long long)outer[n] == nnz;
         for (int j = 0; j <= n; ++j)
         {
             h ^= (uint64_t)(uint32_t)outer[j];
             h *= 1099511628211ull;
+            if (j > 0 && outer[j] < outer[j - 1])
+                ok = false;
         }
         for (int c = 0; c < chunks; ++c)
         {
             h ^= part[c];
             h *= 1099511628211ull;
+            ok = ok && !bad[c];
         }
+        if (valid)
+            *valid = ok;
         return h;
     }
 } // namespace pmas

@@ -27,6 +27,8 @@ namespace pmas
                                   const std::vector<uint8_t> &isolated, int *banks);
     std::vector<int> natural_padded(int V, int *banks);
 
-    // 64-bit FNV-1a style hash of a CSC pattern (n, outer, inner), OpenMP-parallel.
-    uint64_t pattern_hash(int n, const int *outer, const int *inner, long long nnz);
+    // 64-bit FNV-1a style hash of a CSC pattern (n, outer, inner), OpenMP-parallel. The same pass
+    // checks the pattern: *valid (if given) is false unless outer runs from 0 to nnz without
+    // decreasing and every row index lies in [0, n). Row order inside a column is free.
+    uint64_t pattern_hash(int n, const int *outer, const int *inner, long long nnz, bool *valid = nullptr);
 } // namespace pmas

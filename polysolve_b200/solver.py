@@ -190,8 +190,9 @@ def _csc_arrays(A) -> tuple[int, np.ndarray, np.ndarray, np.ndarray]:
         Ac = A.tocsc()
         if Ac.shape[0] != Ac.shape[1]:
             raise ValueError("[MAS] A must be square")
-        if not Ac.has_sorted_indices:
-            Ac = Ac.sorted_indices()
+        # Row order inside a column is free, and the library checks the row range and the
+        # column pointers itself in its pattern pass (scipy's sortedness scan of a new matrix
+        # costs more than a values-only refactorization).
         n = int(Ac.shape[0])
         outer, inner, vals = Ac.indptr, Ac.indices, Ac.data
     if np.asarray(outer)[-1] >= 2 ** 31:

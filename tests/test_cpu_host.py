@@ -86,6 +86,35 @@ def test_orderings_are_valid(mode):
     assert np.all(np.diff(offsets) <= 32) and np.all(np.diff(offsets) >= 1)
 
 
+class _Csc:
+    def __init__(self, n, outer, inner, vals):
+        self.n, self.outer, self.inner, self.vals = n, outer, inner, vals
+
+
+def test_invalid_patterns_are_rejected_on_the_host():
+    """The pattern pass (shared with factorize) rejects row indices outside [0, n) and
+    decreasing column pointers before anything reads through them; row order inside a column
+    does not change the ordering."""
+    s = synthetic.elasticity(6, young_sigma=1.0)
+    ref, ref_banks = order_blocks(s, 3, "graph")
+    inner_rev = s.inner.copy()
+    for j in range(s.n):
+        inner_rev[s.outer[j]:s.outer[j + 1]] = s.inner[s.outer[j]:s.outer[j + 1]][::-1]
+    got, banks = order_blocks(_Csc(s.n, s.outer, inner_rev, s.vals), 3, "graph")
+    np.testing.assert_array_equal(got, ref)
+    assert banks == ref_banks
+    for bad_row in (s.n, -1, 2 ** 31 - 1):
+        inner = s.inner.copy()
+        inner[len(inner) // 2] = bad_row
+        with pytest.raises(MasError):
+            order_blocks(_Csc(s.n, s.outer, inner, s.vals), 3, "graph")
+    outer = s.outer.copy()
+    j = s.n // 2
+    outer[j] = outer[j + 1] + 1  # column j - 1 runs past column j's start
+    with pytest.raises(MasError):
+        order_blocks(_Csc(s.n, outer, s.inner, s.vals), 3, "natural")
+
+
 def test_graph_ordering_is_local():
     """Graph bisection banks are mostly connected (few level-0 components per bank)."""
     s = synthetic.elasticity(12, young_sigma=1.0)

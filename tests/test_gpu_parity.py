@@ -300,6 +300,36 @@ def test_errors():
         Solver.create("Eigen::ConjugateGradient", "")
 
 
+def test_invalid_pattern_and_unsorted_rows():
+    """factorize rejects out-of-range rows and decreasing column pointers on the host (the solver
+    stays usable), and a CSC with the rows of every column reversed gives the same solution."""
+    import scipy.sparse as sp
+
+    system = synthetic.elasticity(5, seed=2, young_sigma=1.0)
+    s = make_solver(system, 3)
+    b = np.random.default_rng(0).standard_normal(system.n)
+    x_ref = np.zeros(system.n)
+    s.solve(b, x_ref)
+    inner = system.inner.copy()
+    inner[7] = system.n
+    with pytest.raises(MasError) as e:
+        s.factorize(sp.csc_matrix((system.vals, inner, system.outer), shape=(system.n, system.n)))
+    assert "Invalid CSC" in str(e.value)
+    outer = system.outer.copy()
+    outer[10] = outer[11] + 1
+    with pytest.raises(MasError):
+        s.factorize(sp.csc_matrix((system.vals, system.inner, outer), shape=(system.n, system.n)))
+    inner_rev, vals_rev = system.inner.copy(), system.vals.copy()
+    for j in range(system.n):
+        lo, hi = system.outer[j], system.outer[j + 1]
+        inner_rev[lo:hi] = system.inner[lo:hi][::-1]
+        vals_rev[lo:hi] = system.vals[lo:hi][::-1]
+    s.factorize(sp.csc_matrix((vals_rev, inner_rev, system.outer), shape=(system.n, system.n)))
+    x = np.zeros(system.n)
+    s.solve(b, x)
+    np.testing.assert_array_equal(x, x_ref)
+
+
 def test_create_json_defaults():
     s = Solver.create({"solver": "MAS", "MAS": {"block_dim": 3}})
     system = synthetic.elasticity(5, seed=2)
