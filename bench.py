@@ -615,6 +615,7 @@ def sequence_modes(N: int, S: int, seed: int, mode_filter: str = "all") -> tuple
         systems.append(sk.scipy())
         rhs.append(bk)
     pos = synthetic.workload_sequence60(0, seed=seed, N=N)[0].positions
+    torch.cuda.synchronize()  # torch's own CUDA set-up happens here, not inside the first timed step
     res = {}
     modes = {"plain_fp64": ("zero", None), "zero": ("input", None), "previous": ("input", None),
              "extrapolate": ("input", None), "projection": ("learned", np.zeros(W.PARAMS, dtype=np.float32)),
@@ -637,12 +638,13 @@ def sequence_modes(N: int, S: int, seed: int, mode_filter: str = "all") -> tuple
         solve_sequence(sv, systems[:3], rhs[:3], seq_mode)  # warm-up (first factorize, graphs)
         if guess == "learned":
             sv.reset_warm_start()
-        acc = {"solve_ms": 0.0, "factorize_ms": 0.0, "warm_start_ms": 0.0, "fallbacks": 0}
+        acc = {"solve_ms": 0.0, "factorize_ms": 0.0, "warm_start_ms": 0.0, "fallbacks": 0, "per_step": []}
         phases: dict[str, float] = {}
 
         def on_step(k, x, info, acc=acc, phases=phases):
             acc["solve_ms"] += info["solve_ms"]
             acc["factorize_ms"] += info["factorize_ms"]
+            acc["per_step"].append(round(float(info["factorize_ms"]), 2))
             ws = info.get("warm_start")
             if ws and ws.get("predicted"):
                 acc["warm_start_ms"] += ws["ms"]
@@ -656,6 +658,7 @@ def sequence_modes(N: int, S: int, seed: int, mode_filter: str = "all") -> tuple
         wall = (time.perf_counter() - t0) * 1000.0
         res[mode] = {"iterations": sum(r["iterations"] for r in out), "wall_ms": wall,
                      "solve_ms": acc["solve_ms"], "factorize_ms": acc["factorize_ms"],
+                     "factorize_ms_each_step": acc["per_step"],
                      "warm_start_ms": acc["warm_start_ms"], "fallbacks": acc["fallbacks"],
                      "worst_rel": max(r["rel"] for r in out),
                      "factorize_phases_ms_per_step": {k: float(f"{v:.4g}") for k, v in phases.items()}}
