@@ -68,7 +68,9 @@ void mas_destroy(mas_solver *h);
  * poll_period (int: iterations launched between looks at the device state), cuda_graphs (bool),
  * preconditioner_refresh (int k: values-only refactorizations rebuild the MAS inverses every k-th
  * time; 1, every time, as the reference), profile_kernels (bool: CUDA-event time per kernel kind,
- * reported by get_info). */
+ * reported by get_info), device_wait_limit (int >= 0: iterations of each bounded device-side wait
+ * before the solve stops with MAS_ERR_TIMEOUT; default 1048576, 0 makes every wait give up at
+ * once, which tests the timeout path). */
 int mas_set_parameters(mas_solver *h, const char *params_json);
 
 /* MASSolver::get_info (MASSolver.cu:214-219): writes a JSON object with solver_iter,
@@ -123,8 +125,6 @@ int mas_reset_warm_start(mas_solver *h);
 /* New: nrhs independent right-hand sides, column-major B[n * nrhs] / X[n * nrhs]. */
 int mas_solve_multi(mas_solver *h, const double *B, double *X, int n, int nrhs);
 
-/* New: solve with device pointers (length n, caller's order) on the handle's stream; the call
- * returns when the solve has finished. */
 /* Batched solves of independent systems (the 64-system workload; no reference counterpart in
  * MASSolver, which solves one system per call): every handle must be factorized and distinct;
  * b[i], x[i] have length n[i] (host arrays, or device arrays when device_pointers != 0). Each
@@ -134,6 +134,8 @@ int mas_solve_multi(mas_solver *h, const double *B, double *X, int n, int nrhs);
 int mas_solve_batch(mas_solver *const *handles, int count, const double *const *b, double *const *x,
                     const int *n, int device_pointers, int threads, int *statuses);
 
+/* New: solve with device pointers (length n, caller's order) on the handle's stream; the call
+ * returns when the solve has finished. */
 int mas_solve_device(mas_solver *h, const double *d_b, double *d_x, int n);
 
 /* New: run the handle's device work on the caller's CUDA stream (a cudaStream_t; NULL restores
@@ -144,13 +146,22 @@ int mas_set_stream(mas_solver *h, void *stream);
  * with no device allocation at all, for callers that cannot allocate at call time (inside a CUDA
  * stream capture, or in applications that reserve all device memory up front and forbid later
  * allocations). d_x, d_y: device vectors of length len = nodes * block_dim in the solver's padded
- * block order (see mas_get_sizes); d_dot: one device double. Runs on `stream` (a cudaStream_t, NULL
- * = the handle's stream) without synchronizing. The reduction scratch is a static device array of
- * 256 KB (held by every GPU that loads the library until exit), which limits the matrix to 262,144
+ * block order (see mas_get_sizes); d_dot: one device double. The three buffers must not overlap
+ * (MAS_ERR_INVALID otherwise). Runs on `stream` (a cudaStream_t, NULL = the handle's stream)
+ * without synchronizing. The reduction scratch is a static device array of 256 KB + 8 B (held by
+ * every GPU where the library's module is loaded, until exit), which limits the matrix to 262,144
  * banks (8,388,608 block rows); larger matrices get MAS_ERR_INVALID. All calls share that scratch:
- * calls that overlap on the GPU race. The first call on a device looks the scratch address up
- * (cudaGetSymbolAddress); make it before any stream capture. */
+ * calls that overlap on the GPU race. The first call on a device (and the first after a
+ * cudaDeviceReset) looks the scratch address up (cudaGetSymbolAddress), which under CUDA's lazy
+ * module loading also loads the module and its array onto the device: make it before any stream
+ * capture and before reserving the rest of the device's memory. */
 int mas_spmv_dot_noalloc(mas_solver *h, const double *d_x, double *d_y, double *d_dot, int len, void *stream);
+
+/* Test hook, process-wide (no reference counterpart; the reference's allocation failure is
+ * mas::CudaOutOfMemoryError, mas_utils/CudaUtils.cuh:41-124): after `after` more successful device
+ * allocations the next one fails as if the device were out of memory, once, and the call that made
+ * it returns MAS_ERR_OOM with the requested and free MB in its message. Negative: off. */
+int mas_debug_fail_allocation(long long after);
 
 /* Last error message of the handle ("" if none). With h == NULL: the last mas_create error. */
 const char *mas_last_error(const mas_solver *h);

@@ -871,48 +871,6 @@ extern "C"
         return 0;
     }
 
-    // Time k PCG iterations' worth of kernels (SpMV + MAS apply + vector passes) on the host,
-    // for a bounded CPU-baseline sample; returns seconds.
-    double orc_time_iterations(void *h, int iterations, int true_residual_period)
-    {
-        auto *o = static_cast<Oracle *>(h);
-        const size_t N = (size_t)o->V * o->bd;
-        std::vector<double> x(N, 0.0), r(N, 1.0), z(N), pv(N, 1.0), Ap(N), b(N, 1.0);
-        double t0 = omp_get_wtime();
-        double rz = dot(r.data(), r.data(), N);
-        for (int k = 1; k <= iterations; ++k)
-        {
-            spmv(*o, pv.data(), Ap.data());
-            double pAp = dot(pv.data(), Ap.data(), N);
-            double alpha = rz / (pAp + 1e-300) * 1e-3;
-#pragma omp parallel for schedule(static)
-            for (long long i = 0; i < (long long)N; ++i)
-                x[i] += alpha * pv[i];
-            if (true_residual_period > 0 && k % true_residual_period == 0)
-            {
-                spmv(*o, x.data(), r.data());
-#pragma omp parallel for schedule(static)
-                for (long long i = 0; i < (long long)N; ++i)
-                    r[i] = b[i] - r[i];
-            }
-            else
-            {
-#pragma omp parallel for schedule(static)
-                for (long long i = 0; i < (long long)N; ++i)
-                    r[i] -= alpha * Ap[i];
-            }
-            mas_apply(*o, r.data(), z.data());
-            double rz_old = rz;
-            rz = dot(r.data(), z.data(), N);
-            double beta = rz / (rz_old + 1e-300);
-            beta = std::min(std::fabs(beta), 1.0);
-#pragma omp parallel for schedule(static)
-            for (long long i = 0; i < (long long)N; ++i)
-                pv[i] = z[i] + beta * pv[i];
-        }
-        return omp_get_wtime() - t0;
-    }
-
     // Jacobi-preconditioned CG, restating the algorithm of Eigen::ConjugateGradient with its
     // default DiagonalPreconditioner (the reference's CPU CG path, Solver.cpp:294-303,
     // 436-438): stop when ||r||^2 < tol^2 ||b||^2. CSC of a symmetric matrix = its CSR.

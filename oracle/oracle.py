@@ -93,8 +93,6 @@ def lib():
         L.orc_half_round.argtypes = [vp, vp, ctypes.c_longlong]
         L.orc_spmv.argtypes = [vp, vp, vp]
         L.orc_pcg.argtypes = [vp, vp, vp, ctypes.POINTER(PcgParams), ctypes.POINTER(PcgResult)]
-        L.orc_time_iterations.restype = ctypes.c_double
-        L.orc_time_iterations.argtypes = [vp, ctypes.c_int, ctypes.c_int]
         L.orc_jacobi_pcg.argtypes = [ctypes.c_int, vp, vp, vp, vp, vp, ctypes.c_double, ctypes.c_int,
                                      ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
         _LIB = L
@@ -312,9 +310,6 @@ class MasOracle:
                     solver_status=STATUS_NAMES.get(res.status, "Unknown"), status_code=res.status, rz0=res.rz0,
                     rr0=res.rr0, rc=rc)
         return x, info
-
-    def time_iterations(self, iterations: int, true_residual_period: int) -> float:
-        return float(lib().orc_time_iterations(self.h, int(iterations), int(true_residual_period)))
 
 
 def half_round(v: np.ndarray) -> np.ndarray:

@@ -216,6 +216,12 @@ namespace pmas
         // 526-583), run by the last CTA of the apply. rz = r . z, rzcross = r . z_old (Polak-Ribiere).
         __device__ void pcg_finalize(PcgState *st, const PcgConfig &cfg, int mode, double rz, double rzcross)
         {
+            if (st->error == ERR_TIMEOUT)
+            {
+                // A bounded wait gave up in this apply: z is incomplete, stop the solve here.
+                st->done = 1;
+                return;
+            }
             if (mode == 1)
             {
                 st->rz = rz;
@@ -348,6 +354,8 @@ namespace pmas
                 if (gw + total_warps < items)
                     bulk_load_stream(stage1, inv + (size_t)mat_of(gw + total_warps) * S, L::STAGE_BYTES, &bar[1], pol);
             }
+            // Copies issued and not yet consumed, per stage (drained if a wait gives up).
+            bool pending[2] = {gw < items, gw + total_warps < items};
             double part[APPLY_PARTS];
 #pragma unroll
             for (int i = 0; i < APPLY_PARTS; ++i)
@@ -421,11 +429,12 @@ namespace pmas
                     for (int t = 0; t < BD; ++t)
                         zold[t] = out[t * 32 + lane];
                 __syncwarp();
-                if (!mbar_wait_bounded(b, s1 ? phase1 : phase0, errp))
+                if (!mbar_wait_bounded(b, s1 ? phase1 : phase0, errp, cfg.wait_limit))
                 {
                     ok = false;
                     break;
                 }
+                pending[s1 ? 1 : 0] = false;
                 if (s1)
                     phase1 ^= 1u;
                 else
@@ -442,10 +451,14 @@ namespace pmas
                 }
                 __syncwarp();
                 const int mn = m + 2 * total_warps;
-                if (lane == 0 && mn < items)
+                if (mn < items)
                 {
-                    fence_proxy_async_smem();
-                    bulk_load_stream(stage, inv + (size_t)mat_of(mn) * S, L::STAGE_BYTES, b, pol);
+                    if (lane == 0)
+                    {
+                        fence_proxy_async_smem();
+                        bulk_load_stream(stage, inv + (size_t)mat_of(mn) * S, L::STAGE_BYTES, b, pol);
+                    }
+                    pending[s1 ? 1 : 0] = true;
                 }
                 const double scale = StoreTraits<Store>::SCALED ? mscale / xscale : 1.0;
                 double d0 = 0.0, d1 = 0.0;
@@ -481,13 +494,9 @@ namespace pmas
             }
             if (!ok)
             {
-                // Drain this warp's other outstanding copy (bounded) before leaving.
+                // Drain this warp's outstanding copies (bounded) before leaving.
                 if (lane == 0)
-                {
-                    for (long long i = 0; i < MBAR_SPIN_LIMIT; ++i)
-                        if (mbar_try_wait(&bar[0], phase0) && mbar_try_wait(&bar[1], phase1))
-                            break;
-                }
+                    mbar_drain(bar, pending, {phase0, phase1});
                 __syncwarp();
             }
             if (MODE == 0)
@@ -627,6 +636,7 @@ namespace pmas
                     bulk_load_stream(stage1, inv + (size_t)mat_of(gw + total_warps) * S, L::STAGE_BYTES, &bar[1],
                                      pol);
             }
+            bool pending[2] = {gw < items, gw + total_warps < items};
             double part[3 * G]; // per right-hand side: coupled banks, isolated banks, coarse
 #pragma unroll
             for (int i = 0; i < 3 * G; ++i)
@@ -675,11 +685,12 @@ namespace pmas
                     }
                 }
                 __syncwarp();
-                if (!mbar_wait_bounded(b, s1 ? phase1 : phase0, &grp->error))
+                if (!mbar_wait_bounded(b, s1 ? phase1 : phase0, &grp->error, cfg.wait_limit))
                 {
                     ok = false;
                     break;
                 }
+                pending[s1 ? 1 : 0] = false;
                 if (s1)
                     phase1 ^= 1u;
                 else
@@ -689,10 +700,14 @@ namespace pmas
                     symv_mma16_g<BD>(stage, xh, xl, ys, lane);
                 __syncwarp();
                 const int mn = m + 2 * total_warps;
-                if (lane == 0 && mn < items)
+                if (mn < items)
                 {
-                    fence_proxy_async_smem();
-                    bulk_load_stream(stage, inv + (size_t)mat_of(mn) * S, L::STAGE_BYTES, b, pol);
+                    if (lane == 0)
+                    {
+                        fence_proxy_async_smem();
+                        bulk_load_stream(stage, inv + (size_t)mat_of(mn) * S, L::STAGE_BYTES, b, pol);
+                    }
+                    pending[s1 ? 1 : 0] = true;
                 }
                 const double mscale = mas.inv_scale[mat];
                 const int slot = coarse ? 2 : ((m >= mas.first_iso_bank) ? 1 : 0);
@@ -722,11 +737,7 @@ namespace pmas
             if (!ok)
             {
                 if (lane == 0)
-                {
-                    for (long long i = 0; i < MBAR_SPIN_LIMIT; ++i)
-                        if (mbar_try_wait(&bar[0], phase0) && mbar_try_wait(&bar[1], phase1))
-                            break;
-                }
+                    mbar_drain(bar, pending, {phase0, phase1});
                 __syncwarp();
             }
             double tot[3 * G];
@@ -748,7 +759,7 @@ namespace pmas
                     all_done &= sg->done ? 1 : 0;
                 }
                 grp->iter = MODE == 1 ? 0 : grp->iter + 1;
-                if (all_done)
+                if (all_done || grp->error)
                     grp->done = 1;
             }
         }

@@ -59,6 +59,9 @@ namespace
         int preconditioner_refresh = 1;
         bool profile = false; // time every kernel launch with CUDA events
         bool graphs = true;   // replay chunks of iterations as a CUDA graph
+        // Iterations of each bounded device-side wait before the solve stops with MAS_ERR_TIMEOUT
+        // (0: every wait gives up at once -- the test of the timeout path).
+        long long wait_limit = MBAR_SPIN_LIMIT_DEFAULT;
     };
 
     const char *status_string(int s)
@@ -106,7 +109,8 @@ namespace
     const char *KNOWN_KEYS[] = {"block_dim", "max_iter", "relative_tolerance", "absolute_tolerance",
                                 "lazy_partitioning", "use_preconditioned_residual_norm", "precision",
                                 "true_residual_period", "check_period", "initial_guess", "beta", "ordering",
-                                "poll_period", "profile_kernels", "cuda_graphs", "preconditioner_refresh"};
+                                "poll_period", "profile_kernels", "cuda_graphs", "preconditioner_refresh",
+                                "device_wait_limit"};
 
     // MASSolverImpl::set_parameters (MASSolver.cu:198-212) plus the extension keys.
     void apply_mas_params(Params &p, const Json &m, bool strict)
@@ -195,6 +199,12 @@ namespace
             q.preconditioner_refresh = get_int(*v, "preconditioner_refresh");
             if (q.preconditioner_refresh < 1)
                 throw Error(ERR_INVALID, "[MAS] preconditioner_refresh must be >= 1");
+        }
+        if (auto *v = m.find("device_wait_limit"))
+        {
+            q.wait_limit = get_int(*v, "device_wait_limit");
+            if (q.wait_limit < 0)
+                throw Error(ERR_INVALID, "[MAS] device_wait_limit must be >= 0");
         }
         p = q;
     }
@@ -692,6 +702,7 @@ struct mas_solver
         c.check_period = p.check_period;
         c.polak_ribiere = p.polak_ribiere ? 1 : 0;
         c.level_num = mas.level_num;
+        c.wait_limit = p.wait_limit;
         return c;
     }
 
@@ -775,6 +786,7 @@ struct mas_solver
         mix((uint64_t)cfg.check_period);
         mix((uint64_t)cfg.use_prec_norm);
         mix((uint64_t)cfg.polak_ribiere);
+        mix((uint64_t)cfg.wait_limit);
         uint64_t bits;
         std::memcpy(&bits, &cfg.rel_tol, 8);
         mix(bits);
@@ -819,6 +831,12 @@ struct mas_solver
         cuda_check(cudaStreamSynchronize(stream), "pcg init");
         rz0 = h_st[0].rz0;
         rr0 = h_st[0].rr0;
+        if (h_st[0].error == ERR_TIMEOUT)
+        {
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            throw Error(ERR_TIMEOUT, "[MAS] a device-side wait timed out.");
+        }
         if (h_st[0].error == ERR_NONFINITE || std::isnan(rz0) || !std::isfinite(rz0))
         {
             cudaEventDestroy(e0);
@@ -1238,6 +1256,7 @@ struct mas_solver
         mix((uint64_t)cfg.max_iter);
         mix((uint64_t)cfg.check_period);
         mix((uint64_t)cfg.use_prec_norm);
+        mix((uint64_t)cfg.wait_limit);
         uint64_t bits;
         std::memcpy(&bits, &cfg.rel_tol, 8);
         mix(bits);
@@ -1282,6 +1301,8 @@ struct mas_solver
         PcgState hs[RHS_GROUP + 1];
         cuda_check(cudaMemcpyAsync(hs, S, sizeof(hs), cudaMemcpyDeviceToHost, stream), "state");
         cuda_check(cudaStreamSynchronize(stream), "pcg init");
+        if (hs[RHS_GROUP].error == ERR_TIMEOUT)
+            throw Error(ERR_TIMEOUT, "[MAS] a device-side wait timed out.");
         for (int g = 0; g < cols; ++g)
             if (hs[g].error == ERR_NONFINITE || std::isnan(hs[g].rz0) || !std::isfinite(hs[g].rz0))
                 throw Error(ERR_NONFINITE, "[MAS] Invalid initial residual.");
@@ -1845,9 +1866,22 @@ extern "C" int mas_spmv_dot_noalloc(mas_solver *h, const double *d_x, double *d_
                                          std::to_string(h->banks * 32 * h->bd) + ".");
         if (!d_x || !d_y || !d_dot)
             throw Error(ERR_INVALID, "[MAS] spmv_dot_noalloc: null device pointer.");
+        // The kernel reads x while other warps write y (and x . y into *d_dot): the three buffers
+        // must not overlap, or y and the dot come out wrong without any error.
+        const uintptr_t x0 = reinterpret_cast<uintptr_t>(d_x), y0 = reinterpret_cast<uintptr_t>(d_y);
+        const uintptr_t bytes = sizeof(double) * (uintptr_t)len, dot = reinterpret_cast<uintptr_t>(d_dot);
+        auto inside = [](uintptr_t p, uintptr_t lo, uintptr_t nbytes) { return p + sizeof(double) > lo && p < lo + nbytes; };
+        if ((x0 < y0 + bytes && y0 < x0 + bytes) || inside(dot, x0, bytes) || inside(dot, y0, bytes))
+            throw Error(ERR_INVALID, "[MAS] spmv_dot_noalloc: d_x, d_y and d_dot must not overlap.");
         cuda_check(cudaSetDevice(h->device), "set device");
         launch_spmv_dot_noalloc(h->A.view(), d_x, d_y, d_dot, stream ? static_cast<cudaStream_t>(stream) : h->stream);
     });
+}
+
+extern "C" int mas_debug_fail_allocation(long long after)
+{
+    set_alloc_failure(after);
+    return MAS_OK;
 }
 
 extern "C" const char *mas_last_error(const mas_solver *h)

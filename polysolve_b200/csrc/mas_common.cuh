@@ -300,17 +300,36 @@ namespace pmas
         return ok != 0;
     }
 
-    // Wait for phase `parity` of the barrier with an iteration limit. On timeout records
-    // ERR_TIMEOUT in *err and returns false.
-    constexpr long long MBAR_SPIN_LIMIT = 1LL << 20;
+    // Default iteration limit of a bounded device-side wait (PcgConfig::wait_limit; the solver
+    // parameter device_wait_limit lowers it, down to 0 = give up at once, to test the timeout path).
+    constexpr long long MBAR_SPIN_LIMIT = MBAR_SPIN_LIMIT_DEFAULT;
 
-    __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *err)
+    // Wait for phase `parity` of the barrier with an iteration limit; warp-collective (all 32 lanes
+    // call it and get the same answer: the phase counts as complete only when every lane saw it,
+    // so every lane has acquired the copied data). On timeout records ERR_TIMEOUT in *err and
+    // returns false.
+    __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *err,
+                                                      long long limit = MBAR_SPIN_LIMIT)
     {
-        for (long long i = 0; i < MBAR_SPIN_LIMIT; ++i)
-            if (mbar_try_wait(bar, parity))
+        for (long long i = 0; i < limit; ++i)
+            if (__all_sync(FULL, mbar_try_wait(bar, parity)))
                 return true;
-        if (err)
+        if (err && (threadIdx.x & 31) == 0)
             atomicExch(err, ERR_TIMEOUT);
         return false;
+    }
+
+    // After a wait gave up: wait (bounded by the default limit, whatever the caller's limit was)
+    // for the copies this warp still has in flight, so none lands in shared memory after the CTA
+    // has left. pending[s]: a copy was issued to stage s and not consumed; phase[s]: its parity.
+    // Called by lane 0.
+    __device__ __forceinline__ void mbar_drain(uint64_t *bar, const bool (&pending)[2], const uint32_t (&phase)[2])
+    {
+#pragma unroll
+        for (int s = 0; s < 2; ++s)
+            if (pending[s])
+                for (long long i = 0; i < MBAR_SPIN_LIMIT; ++i)
+                    if (mbar_try_wait(&bar[s], phase[s]))
+                        break;
     }
 } // namespace pmas

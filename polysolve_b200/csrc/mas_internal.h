@@ -52,6 +52,9 @@ namespace pmas
     void cuda_check(cudaError_t e, const char *what);
     void *device_alloc(size_t bytes, const char *ctx); // throws Error(ERR_OOM) with MB figures
     void device_free(void *p);
+    // Test hook: after `after` more successful device allocations the next one fails as if the
+    // device were out of memory (once); negative: off.
+    void set_alloc_failure(long long after);
 
     // Owning device buffer.
     template <class T>
@@ -271,6 +274,9 @@ namespace pmas
         unsigned int counter[8];
     };
 
+    // Default iteration limit of a bounded device-side wait (an mbarrier wait of a bulk copy).
+    constexpr long long MBAR_SPIN_LIMIT_DEFAULT = 1LL << 20;
+
     struct PcgConfig
     {
         int max_iter;
@@ -279,6 +285,7 @@ namespace pmas
         int check_period;
         int polak_ribiere;
         int level_num; // coarse levels in use (isolated rows: z = (1 + level_num) z0)
+        long long wait_limit; // iterations of each bounded device-side wait before ERR_TIMEOUT
     };
 
     // Scratch of the deterministic two-stage reductions: every CTA writes its partial sums, the

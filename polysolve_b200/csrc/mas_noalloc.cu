@@ -8,14 +8,25 @@
 // the last CTA) in a file-scope static __device__ array instead of memory the solver allocates.
 //
 // Limits and rules:
-//   * the array holds NOALLOC_MAX_CTAS partials (256 KB + 8 B on every GPU that loads this
-//     library, held until the process exits): at most NOALLOC_MAX_CTAS * 8 banks, i.e. 262,144
+//   * the array holds NOALLOC_MAX_CTAS partials plus one double for the ticket (256 KB + 8 B on
+//     every GPU where this module is loaded, held until the process exits): at most
+//     NOALLOC_MAX_CTAS * 8 banks, i.e. 262,144
 //     banks = 8,388,608 block rows; larger matrices are rejected with an error;
 //   * every call shares the array: calls that overlap on the GPU (on different streams, or from
 //     different handles on one device) race and must be serialized by the caller;
 //   * the ticket is cleared before each launch; the partials need no clearing;
+//   * x, y and the dot must be distinct, non-overlapping device buffers (the kernel reads x while
+//     other warps write y); overlapping pointers are rejected by the entry point;
 //   * the first call on a device looks the array's device address up (cudaGetSymbolAddress with
-//     that device current) -- make that first call before any stream capture.
+//     that device current). Under CUDA's lazy module loading (the default) that lookup is also what
+//     loads this module onto the device and gives the array its 256 KB of device memory, so the
+//     first call must come before any stream capture and before the application reserves the rest
+//     of the device's memory;
+//   * the address is cached per device together with the id of the CUDA context it was looked up
+//     in; after a cudaDeviceReset (a new primary context) the next call looks it up again, which
+//     loads the module into the new context -- the same "first call" rule applies then.
+
+#include <cuda.h>
 
 #include <mutex>
 #include <string>
@@ -87,10 +98,39 @@ namespace pmas
                 *dot = tot[0];
         }
 
-        // Device address of the scratch array, looked up once per device.
+        // Device address of the scratch array per device, with the id of the context it belongs to.
         constexpr int MAX_DEVICES = 64;
         std::mutex g_lookup_mutex;
         double *g_scratch_addr[MAX_DEVICES] = {nullptr};
+        unsigned long long g_scratch_ctx[MAX_DEVICES] = {0};
+
+        // Unique id of the current CUDA context (driver entry points cuCtxGetCurrent / cuCtxGetId,
+        // looked up through the runtime); 0 when they are unavailable.
+        unsigned long long current_context_id()
+        {
+            using GetCurrent = CUresult (*)(CUcontext *);
+            using GetId = CUresult (*)(CUcontext, unsigned long long *);
+            static GetCurrent get_current = nullptr;
+            static GetId get_id = nullptr;
+            static std::once_flag once;
+            std::call_once(once, [] {
+                void *f = nullptr;
+                cudaDriverEntryPointQueryResult q;
+                if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+                    q == cudaDriverEntryPointSuccess)
+                    get_current = reinterpret_cast<GetCurrent>(f);
+                f = nullptr;
+                if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+                    q == cudaDriverEntryPointSuccess)
+                    get_id = reinterpret_cast<GetId>(f);
+                cudaGetLastError();
+            });
+            CUcontext ctx = nullptr;
+            unsigned long long id = 0;
+            if (get_current && get_id && get_current(&ctx) == CUDA_SUCCESS && ctx && get_id(ctx, &id) == CUDA_SUCCESS)
+                return id;
+            return 0;
+        }
     } // namespace
 
     int noalloc_max_banks() { return NOALLOC_MAX_CTAS * NOALLOC_BANKS_PER_CTA; }
@@ -108,12 +148,14 @@ namespace pmas
             throw Error(ERR_INVALID, "[MAS] spmv_dot_noalloc: device index out of range");
         double *scratch = nullptr;
         {
+            const unsigned long long ctx = current_context_id();
             std::lock_guard<std::mutex> lock(g_lookup_mutex);
-            if (!g_scratch_addr[dev])
+            if (!g_scratch_addr[dev] || g_scratch_ctx[dev] != ctx)
             {
                 void *p = nullptr;
                 cuda_check(cudaGetSymbolAddress(&p, g_noalloc_scratch), "scratch symbol address");
                 g_scratch_addr[dev] = static_cast<double *>(p);
+                g_scratch_ctx[dev] = ctx;
             }
             scratch = g_scratch_addr[dev];
         }

@@ -9,6 +9,7 @@
 // alpha / beta are read from the device-resident PcgState, and every dot is a deterministic
 // two-stage reduction, so no host round trip is needed inside the iteration.
 
+#include <atomic>
 #include <cstdio>
 #include <mutex>
 #include <string>
@@ -24,11 +25,30 @@ namespace pmas
             throw Error(ERR_CUDA, std::string("[MAS] CUDA error in ") + what + ": " + cudaGetErrorString(e));
     }
 
+    // Test hook (mas_debug_fail_allocation): the number of device allocations still to succeed
+    // before one fails as if the device were out of memory; -1 = off.
+    static std::atomic<long long> g_alloc_fail_after{-1};
+
+    void set_alloc_failure(long long after) { g_alloc_fail_after.store(after < 0 ? -1 : after); }
+
     // Allocation with the reference's out-of-memory message (mas_utils/CudaUtils.cuh:68-79).
     void *device_alloc(size_t bytes, const char *ctx)
     {
         void *p = nullptr;
-        cudaError_t e = cudaMalloc(&p, bytes);
+        cudaError_t e = cudaErrorMemoryAllocation;
+        long long left = g_alloc_fail_after.load();
+        bool injected = false;
+        while (left >= 0)
+        {
+            // left == 0: this allocation fails (once); otherwise count it down.
+            if (g_alloc_fail_after.compare_exchange_weak(left, left - 1))
+            {
+                injected = (left == 0);
+                break;
+            }
+        }
+        if (!injected)
+            e = cudaMalloc(&p, bytes);
         if (e == cudaSuccess)
             return p;
         if (e != cudaErrorMemoryAllocation)

@@ -43,7 +43,7 @@ EXPORTED_SYMBOLS = [
     "mas_get_coarse_map", "mas_get_inverses", "mas_debug_spmv", "mas_debug_apply", "mas_debug_apply_multi",
     "mas_debug_spmv_multi", "mas_set_warm_start_model", "mas_reset_warm_start", "mas_debug_warm_start",
     "mas_market_load", "mas_market_dims", "mas_market_copy_csc", "mas_market_copy_dense", "mas_market_free",
-    "mas_market_last_error", "mas_market_write_csc", "mas_market_write_vector",
+    "mas_market_last_error", "mas_market_write_csc", "mas_market_write_vector", "mas_debug_fail_allocation",
 ]
 
 
@@ -102,6 +102,7 @@ def library() -> ctypes.CDLL:
         L.mas_reset_warm_start.argtypes = [vp]
         L.mas_debug_warm_start.argtypes = [vp, vp, vp, i, vp, vp, vp, vp]
         L.mas_order_blocks.argtypes = [i, vp, vp, i, vp, ctypes.c_char_p, ip, ip]
+        L.mas_debug_fail_allocation.argtypes = [ctypes.c_longlong]
         _LIB = L
     return _LIB
 
@@ -151,6 +152,13 @@ def solve_batch_device(solvers: list, b_ptrs: list, x_ptrs: list, ns: list, *, t
     if rc != MAS_OK:
         bad = next((k for k in range(count) if st[k] != MAS_OK), None)
         _check(int(rc), solvers[bad]._h if bad is not None else (solvers[0]._h if count else None))
+
+
+def debug_fail_allocation(after: int) -> None:
+    """Test hook (process-wide): after ``after`` more successful device allocations the next one
+    fails as if the device were out of memory, once (the solver raises CudaOutOfMemoryError with
+    the requested and free MB, as mas_utils/CudaUtils.cuh:68-79). Negative: off."""
+    library().mas_debug_fail_allocation(int(after))
 
 
 def order_blocks(A, block_dim: int, mode: str, positions: np.ndarray | None = None) -> tuple[np.ndarray, int]:

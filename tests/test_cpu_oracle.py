@@ -203,3 +203,26 @@ def test_golden_generator_inputs_stable():
     np.testing.assert_array_equal(s.outer, d["outer"])
     np.testing.assert_array_equal(s.inner, d["inner"])
     np.testing.assert_array_equal(s.vals, d["vals"])
+
+
+def test_cpu20_oracle_matches_sparse_lu():
+    """The CPU-runnable configuration (20^3, 27,783 DOF, E 1e5, Dirichlet x = 0, b ~ N(0,1)): the
+    oracle's reference-mode PCG and the Jacobi-PCG baseline both reach 1e-8 and agree with an FP64
+    sparse LU (the CHOLMOD stand-in) to 1e-6."""
+    import scipy.sparse.linalg as sla
+
+    s = synthetic.workload_cpu20()
+    b = synthetic.rhs(s.n, seed=0)
+    A = s.scipy().tocsc()
+    x_lu = sla.splu(A).solve(b)
+    iso = O.isolated_blocks(s.outer, s.inner, s.n, 3)
+    perm, off = O.morton_order(s.positions, iso)
+    orc = O.MasOracle(s.outer, s.inner, s.vals, s.n, 3, perm, off)
+    x, info = orc.pcg(b, rel_tol=1e-8, abs_tol=0.0)
+    assert info["solver_status"] == "Reach relative tolerance"
+    assert info["solver_iter"] % 10 == 0
+    assert np.linalg.norm(A @ x - b) <= 1e-8 * np.linalg.norm(b)
+    assert np.linalg.norm(x - x_lu) <= 1e-6 * np.linalg.norm(x_lu)
+    xj, itj, rel = O.jacobi_pcg(s.outer, s.inner, s.vals, s.n, b, 1e-8)
+    assert rel <= 1e-8 and itj > info["solver_iter"]
+    assert np.linalg.norm(xj - x_lu) <= 1e-6 * np.linalg.norm(x_lu)
