@@ -17,7 +17,7 @@ A step is one solve from x0 = 0 to ||b - A x|| <= 1e-8 ||b||.
   * roofline: the SpMV (the dominant kernel) from per-launch CUDA events in a profiled solve.
   * cpu_baseline: the CPU MAS-PCG oracle (OpenMP C++ port) on this host, two whole solves timed;
             the same oracle checks the GPU's plain FP64 solve (iterations, solution) and, driven to
-            1e-12, gives the FP64 reference solution for `solution_relative_error`.
+            1e-11, gives the FP64 reference solution for `solution_relative_error`.
 
 --impl reference runs the reference's algorithm on the host cores (the oracle port: the reference's
 CUDA MAS path cannot be built in this image), each step one whole solve timed on the host clock.
@@ -153,7 +153,7 @@ def oracle_checks(system, padded, b, plain_iterations: int, x_chosen, x_plain, s
     system, partition and b: (1) `solves` timed whole reference-mode solves (FP64, true residual
     every 4, test every 10, x0 = 0) -- the CPU baseline, no extrapolation; (2) parity of the GPU's
     plain FP64 solve with the oracle's (iteration count, solution); (3) the oracle driven to a
-    relative residual of 1e-12, the FP64 reference solution the GPU solutions' errors are measured
+    relative residual of 1e-11, the FP64 reference solution the GPU solutions' errors are measured
     against (CHOLMOD is unavailable on this box)."""
     from oracle import oracle as O
 
@@ -167,7 +167,8 @@ def oracle_checks(system, padded, b, plain_iterations: int, x_chosen, x_plain, s
         xo, oinfo = orc.pcg(b, rel_tol=TOL, abs_tol=0.0, max_iter=5000)
         times.append((time.perf_counter() - t0) * 1000.0)
     value = statistics.median(times)
-    x_tight, tinfo = orc.pcg(b, rel_tol=1e-12, abs_tol=0.0, max_iter=20000)
+    # 1e-11: the recursive residual of FP64 PCG on this system stalls near 3e-12.
+    x_tight, tinfo = orc.pcg(b, rel_tol=1e-11, abs_tol=0.0, max_iter=1000)
     A = system.scipy()
     rel_tight = float(np.linalg.norm(A @ x_tight - b) / np.linalg.norm(b))
     # Eigen::ConjugateGradient's algorithm (Jacobi-PCG, the reference's CPU CG path), one whole solve.
@@ -193,7 +194,7 @@ def oracle_checks(system, padded, b, plain_iterations: int, x_chosen, x_plain, s
                                    "Solver.cpp:273-303, 436-438), OpenMP, host clock"},
         "solution_relative_error": err(x_chosen),
         "plain_fp64_solution_relative_error": err(x_plain),
-        "fp64_reference": f"CPU oracle MAS-PCG to relative residual 1e-12 (reached {rel_tight:.1e}, "
+        "fp64_reference": f"CPU oracle MAS-PCG to relative residual 1e-11 (reached {rel_tight:.1e}, "
                           f"{tinfo['solver_iter']} iterations); CHOLMOD unavailable on this box",
     }
 

@@ -122,6 +122,32 @@ int mas_set_warm_start_model(mas_solver *h, const float *params, long long count
  * pattern or ordering also forgets them. */
 int mas_reset_warm_start(mas_solver *h);
 
+/* New, no reference counterpart: training of the learned warm start's network on the GPU with this
+ * library's own forward and reverse-pass kernels (BF16 tensor-core products, FP32 accumulation and
+ * FP32 Adam state). A sample is one step of a sequence of systems with one pattern: add it from a
+ * solver factorized with that step's matrix, with b, 2 to 4 kept solutions history[j * n ..]
+ * (x_{k-1} first) and the exact solution x_exact (all caller order, length n); the trainer runs the
+ * solver's own prediction pipeline up to the features and keeps the sample in device memory. The
+ * loss of a sample is 1 - rho, rho = (c . r_g)^2 / ((c . A c) (e . r_g)) with r_g the residual of the
+ * kept solutions' Galerkin combination x_g and e = x_exact - x_g.
+ *   create:   initial parameters (MAS_WS_PARAMS float32, the .psws order); Adam moments start at 0.
+ *   train:    one Adam step (beta1 0.9, beta2 0.999, eps 1e-8) per listed sample, in order, with the
+ *             given learning rates; losses (optional) receives each step's loss before its update.
+ *   evaluate: rho of each listed sample under the current parameters.
+ *   gradient: the loss and its gradient (MAS_WS_PARAMS floats) for one sample; no update. */
+typedef struct mas_ws_trainer mas_ws_trainer;
+int mas_ws_trainer_create(const float *params, long long count, mas_ws_trainer **out);
+void mas_ws_trainer_destroy(mas_ws_trainer *t);
+int mas_ws_trainer_add_sample(mas_ws_trainer *t, mas_solver *h, const double *b, const double *history, int nhist,
+                              const double *x_exact, int n);
+int mas_ws_trainer_sample_count(const mas_ws_trainer *t);
+int mas_ws_trainer_train(mas_ws_trainer *t, const int *samples, const float *lr, int count, double *losses);
+int mas_ws_trainer_evaluate(mas_ws_trainer *t, const int *samples, int count, double *rho);
+int mas_ws_trainer_gradient(mas_ws_trainer *t, int sample, float *grad, long long count, double *loss);
+int mas_ws_trainer_get_params(const mas_ws_trainer *t, float *params, long long count);
+/* Last error of the trainer ("" if none); with t == NULL the last mas_ws_trainer_create error. */
+const char *mas_ws_trainer_last_error(const mas_ws_trainer *t);
+
 /* New: nrhs independent right-hand sides, column-major B[n * nrhs] / X[n * nrhs]. */
 int mas_solve_multi(mas_solver *h, const double *B, double *X, int n, int nrhs);
 

@@ -13,6 +13,8 @@ solver's own (features, network, Galerkin combination):
                   states and layer weights with float32 accumulation, float32 output layer);
 * ``forward64`` / ``backward64``: the same network in float64 with its reverse pass, checked
                   against finite differences (it is the reference for the training code);
+* ``train_gradient_device``: the GPU training pass's loss and gradient with its rounding points
+                  (bf16 where the GPU multiplies on tensor cores), for a tight check of its kernels;
 * ``galerkin``:   the energy-minimising combination of {x1, x1 - x2, x2 - x3, x3 - x4, c} (missing
                   kept solutions give zero vectors, which are dropped) with the fallback to x1.
 
@@ -180,6 +182,64 @@ def backward64(cache, g_out):
     for k, (o, s) in lay.items():
         flat[o:o + int(np.prod(s))] = grads[k].reshape(-1)
     return flat
+
+
+def loss_and_output_gradient(out, A, re, s_q, ere):
+    """(loss, rho, dL/dout) of the training objective 1 - rho, rho = (c . r_g)^2 / ((c . A c) (e . r_g)),
+    c = s_q out (float64; the GPU's k_tr_spmv_loss and k_tr_out_bwd)."""
+    c = s_q * np.asarray(out, dtype=np.float64).reshape(-1)
+    Ac = A @ c
+    a, q = float(c @ re), float(c @ Ac)
+    if not (q > 0 and ere > 0):
+        return 1.0, 0.0, np.zeros_like(np.asarray(out, dtype=np.float64))
+    rho = a * a / (q * ere)
+    g_c = -2.0 * a / (q * ere) * re + 2.0 * a * a / (q * q * ere) * Ac
+    return 1.0 - rho, rho, (s_q * g_c).reshape(-1, 3)
+
+
+def train_gradient_device(params, f, src, dst, w, A, re, s_q, ere):
+    """(loss, flat gradient) of one training sample with the GPU training pass's rounding points
+    (polysolve_b200/csrc/mas_ws_train.cu): the forward as ``forward_device`` (bf16 hidden states,
+    messages and layer weights, float32 elsewhere) on normalised float32 features f; the reverse pass
+    rounds gz = dL/dh' * [z > 0] and W_l to bf16 for the two tensor-core products, everything else
+    float32 (sums here in float64). Messages m_i = sum_j w_ij h_j over edges j -> i."""
+    P = {k: np.asarray(v, dtype=np.float32) for k, v in unpack(params).items()}
+    f = np.asarray(f, dtype=np.float32)
+    w32 = np.asarray(w, dtype=np.float32)
+    z0 = f @ P["w_in"].T + P["b_in"]
+    h = bf16(np.maximum(z0, 0.0))
+    hs, ts, zs = [h], [], []
+    for lv in range(LAYERS):
+        m = np.zeros_like(h)
+        np.add.at(m, dst, w32[:, None] * h[src])
+        t = np.concatenate([h, bf16(m)], axis=1)
+        z = t @ bf16(P[f"w_{lv}"]).T + P[f"b_{lv}"]
+        h = bf16(h + np.maximum(z, 0.0))
+        ts.append(t)
+        zs.append(z)
+        hs.append(h)
+    out = (h @ P["w_out"].T + P["b_out"]).astype(np.float32)
+    loss, _, g_out = loss_and_output_gradient(out, A, re, s_q, ere)
+    g_out = g_out.astype(np.float32).astype(np.float64)
+    grads = {"w_out": g_out.T @ hs[-1], "b_out": g_out.sum(axis=0)}
+    gh = (g_out @ P["w_out"].astype(np.float64)).astype(np.float32).astype(np.float64)
+    for lv in reversed(range(LAYERS)):
+        gz = gh * (zs[lv] > 0)
+        gzb = bf16(gz.astype(np.float32)).astype(np.float64)
+        grads[f"w_{lv}"] = gzb.T @ ts[lv].astype(np.float64)
+        grads[f"b_{lv}"] = gz.sum(axis=0)
+        gt = gzb @ bf16(P[f"w_{lv}"]).astype(np.float64)
+        gh_prev = gh + gt[:, :HIDDEN]
+        np.add.at(gh_prev, src, w32[:, None].astype(np.float64) * gt[dst, HIDDEN:])
+        gh = gh_prev.astype(np.float32).astype(np.float64)
+    gz0 = gh * (z0 > 0)
+    grads["w_in"] = gz0.T @ f.astype(np.float64)
+    grads["b_in"] = gz0.sum(axis=0)
+    lay, total = layout()
+    flat = np.zeros(total)
+    for k, (o, sh) in lay.items():
+        flat[o:o + int(np.prod(sh))] = grads[k].reshape(-1)
+    return loss, flat
 
 
 def galerkin_basis(history, c):

@@ -6,6 +6,8 @@ recipe (``_build.py``), the Python mirror of polysolve's ``Solver`` interface (`
 seeded synthetic elasticity workloads (``synthetic.py``).
 """
 
-from .solver import CudaOutOfMemoryError, MasError, MASSolver, Solver, library, solve_batch, solve_batch_device
+from .solver import (CudaOutOfMemoryError, MasError, MASSolver, Solver, WarmStartTrainer, library, solve_batch,
+                     solve_batch_device)
 
-__all__ = ["Solver", "MASSolver", "MasError", "CudaOutOfMemoryError", "library", "solve_batch", "solve_batch_device"]
+__all__ = ["Solver", "MASSolver", "MasError", "CudaOutOfMemoryError", "WarmStartTrainer", "library", "solve_batch",
+           "solve_batch_device"]

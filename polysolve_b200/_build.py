@@ -6,7 +6,7 @@
 * ``mas_cpp_test``          - a C++ program that drives the solver through the C++ header
   ``include/polysolve/linear/MASSolver.hpp`` the way polysolve's own tests drive ``Solver``.
 
-The oracle under ``oracle/`` has its own recipe (``oracle/build.py``).
+The oracle under ``oracle/`` (test infrastructure) has its own recipe: ``oracle.oracle.build()``.
 Everything is compiled for sm_100a only (``-gencode arch=compute_100a,code=sm_100a``).
 """
 
@@ -41,8 +41,9 @@ CU_SOURCES = [
     "mas_noalloc.cu",
     "mas_multi.cu",
     "mas_warmstart.cu",
+    "mas_ws_train.cu",
 ]
-CPP_SOURCES = ["mas_capi.cpp", "mas_ordering.cpp", "mas_json.cpp", "mas_market.cpp"]
+CPP_SOURCES = ["mas_capi.cpp", "mas_trainer.cpp", "mas_ordering.cpp", "mas_json.cpp", "mas_market.cpp"]
 
 
 def _run(cmd: list[str]) -> None:

@@ -30,6 +30,7 @@
 #include "mas_internal.h"
 #include "mas_json.h"
 #include "mas_ordering.h"
+#include "mas_trainer.h"
 
 using namespace pmas;
 
@@ -1159,6 +1160,64 @@ struct mas_solver
         }
     }
 
+    // One training sample for the warm-start network: the prediction pipeline up to the features
+    // (x_g over the kept solutions, r_g, raw features and their sums) for caller-order b and nhist
+    // (2 to 4) kept solutions history[j * n ..] (x_{k-1} first), and the exact solution x_k.
+    void collect_training_sample(mas_ws_trainer &t, const double *hb, const double *hhist, int nhist,
+                                 const double *hx, int len_in)
+    {
+        cuda_check(cudaSetDevice(device), "set device");
+        require_factorized(len_in);
+        if (t.device != device)
+            throw Error(ERR_INVALID, "[MAS] warm start trainer: the solver and the trainer are on different devices");
+        if (bd != 3)
+            throw Error(ERR_INVALID, "[MAS] the learned warm start needs block_dim 3");
+        if (!hb || !hhist || !hx || nhist < 2 || nhist > WS_HISTORY)
+            throw Error(ERR_INVALID, "[MAS] warm start trainer: b, x and 2 to 4 kept solutions are needed");
+        const size_t len = (size_t)banks * 32 * bd;
+        DevBuf<double> dh[WS_HISTORY], dxe;
+        const double *xs[WS_HISTORY];
+        cuda_check(cudaMemcpyAsync(io.get(), hb, sizeof(double) * n, cudaMemcpyHostToDevice, stream), "upload");
+        launch_permute_in(n, bd, V, d_padded.get(), io.get(), b.get(), len, stream);
+        for (int j = 0; j < nhist; ++j)
+        {
+            dh[j].alloc(len, "warm start trainer collection");
+            cuda_check(cudaMemcpyAsync(io.get(), hhist + (size_t)j * n, sizeof(double) * n, cudaMemcpyHostToDevice,
+                                       stream),
+                       "upload");
+            launch_permute_in(n, bd, V, d_padded.get(), io.get(), dh[j].get(), len, stream);
+            xs[j] = dh[j].get();
+        }
+        dxe.alloc(len, "warm start trainer collection");
+        cuda_check(cudaMemcpyAsync(io.get(), hx, sizeof(double) * n, cudaMemcpyHostToDevice, stream), "upload");
+        launch_permute_in(n, bd, V, d_padded.get(), io.get(), dxe.get(), len, stream);
+        WsBuffers w = ws_buffers();
+        const BankedView Av = A.view();
+        if (!ws_graph_valid)
+        {
+            launch_ws_graph(Av, w, stream);
+            ws_graph_valid = true;
+        }
+        WsHistory h;
+        for (int j = 0; j < WS_HISTORY; ++j)
+        {
+            const int src = std::min(j, nhist - 1);
+            h.x[j] = xs[src];
+            h.y[j] = ws_y[src].get();
+        }
+        {
+            double *ys[WS_HISTORY];
+            for (int j = 0; j < nhist; ++j)
+                ys[j] = ws_y[j].get();
+            launch_spmv_vectors(Av, xs, ys, nhist, stream);
+        }
+        launch_ws_features(Av, w, b.get(), h, len, stream);
+        const uint64_t key = pattern ^ ((uint64_t)ordered_version * 0x9E3779B97F4A7C15ull) ^ (uint64_t)nnz;
+        const int pat = t.pattern_for(this, key, A, w.diag_slot, stream);
+        t.add_sample(pat, A, w.wslot, w.feat, w.st, w.rg, h, dxe.get(), len, stream);
+        cuda_check(cudaStreamSynchronize(stream), "warm start trainer collection");
+    }
+
     // ---- Several right-hand sides at once (RHS_GROUP per group, binary16 inverses). ----------
     bool multi_supported() const
     {
@@ -1876,6 +1935,16 @@ extern "C" int mas_spmv_dot_noalloc(mas_solver *h, const double *d_x, double *d_
         cuda_check(cudaSetDevice(h->device), "set device");
         launch_spmv_dot_noalloc(h->A.view(), d_x, d_y, d_dot, stream ? static_cast<cudaStream_t>(stream) : h->stream);
     });
+}
+
+extern "C" int mas_ws_trainer_add_sample(mas_ws_trainer *t, mas_solver *h, const double *b, const double *history,
+                                         int nhist, const double *x_exact, int n)
+{
+    if (!h || !t)
+        return MAS_ERR_INVALID;
+    const int rc = guarded(h, [&] { h->collect_training_sample(*t, b, history, nhist, x_exact, n); });
+    t->last_error = h->last_error;
+    return rc;
 }
 
 extern "C" int mas_debug_fail_allocation(long long after)

@@ -522,6 +522,72 @@ namespace pmas
     // Features of the vertices in caller order (tests): out[v * 16 + f] = feat[padded[v] * 16 + f].
     void launch_ws_features_out(int V, const int *padded_of_block, const float *feat, float *out, cudaStream_t s);
 
+    // ---------------------------------------------------------------------------------------
+    // mas_ws_train.cu: training of the warm start's network on the GPU (forward, reverse pass,
+    // Adam). A sample is stored in the solver's padded block order: the banked pattern of its
+    // sequence plus its own values, weights, features, r_g and scalars (s_q, e . r_g).
+    // ---------------------------------------------------------------------------------------
+    struct WsTrainState
+    {
+        double a, q;        // c . r_g and c . A c
+        double rho, loss;   // rho = a^2 / (q e.r_g), loss = 1 - rho
+        double kr, ka;      // dL/dc = kr r_g + ka A c
+        unsigned counter[2];
+    };
+
+    struct WsTrainView
+    {
+        int banks;
+        const long long *slice;
+        const int *rowlen;
+        const int *cols;
+        const int *diag_slot;
+        const uint8_t *real;   // nodes: 1 for the network's vertices (a row with a diagonal block)
+        const float *vals32;   // slots * 288: block values [slot][q][lane]
+        const float *wslot;    // slots * 32: neighbour weight w_ij of row i's entry for j
+        const float *wT;       // slots * 32: the mirrored weight w_ji of the same entry
+        const float *feat;     // nodes * 16 normalised features
+        const double *re;      // nodes * 3: r_g
+        const double *sc;      // [0] s_q, [1] e . r_g
+    };
+
+    struct WsTrainScratch
+    {
+        float *z0;                      // nodes * 64 input-layer pre-activation
+        float *z[WS_LAYERS];            // layer pre-activations
+        uint16_t *h[WS_LAYERS + 1];     // bf16 hidden states h0 .. h3
+        uint16_t *m[WS_LAYERS];         // bf16 messages
+        double *c, *Ac;                 // nodes * 3
+        float *gh, *g1, *gm;            // nodes * 64 gradients
+        float *partials;                // ctas * WS_PARAMS
+        double *red;                    // reduction scratch of the loss
+        WsTrainState *st;
+    };
+
+    int ws_train_ctas(int nodes);
+    // Mirror map and real-vertex mask of a pattern (mirror: slots * 32 ints).
+    void launch_tr_pattern(const BankedView &A, const int *diag_slot, long long slots, int *mirror, uint8_t *real,
+                           cudaStream_t s);
+    // One sample from the solver's prediction buffers (features, r_g, WsState after the first
+    // Galerkin pass) and the exact solution; writes the sample's arrays and sc = {s_q, e . r_g}.
+    void launch_tr_sample(const BankedView &A, long long slots, const int *mirror, const uint8_t *real,
+                          const float *wslot, const float *feat_raw, const WsState *ws, const double *rg,
+                          const WsHistory &hist, const double *x_exact, size_t len, float *vals32, float *wslot_out,
+                          float *wT, float *feat, double *re, double *sc, double *partials, unsigned *counter,
+                          int capacity, cudaStream_t s);
+    // Forward pass and loss (into scratch.st); returns the kernels launched.
+    int launch_tr_forward(const WsTrainView &S, const float *prm, const uint16_t *wl, const WsTrainScratch &w,
+                          cudaStream_t s);
+    // Reverse pass after launch_tr_forward: the gradient of the loss (WS_PARAMS floats).
+    int launch_tr_backward(const WsTrainView &S, const float *prm, const uint16_t *wl, const WsTrainScratch &w,
+                           float *grad, cudaStream_t s);
+    void launch_tr_adam(float *prm, float *m, float *v, const float *grad, uint16_t *wl, float lr, long long step,
+                        cudaStream_t s);
+    void launch_tr_weights_bf16(const float *prm, uint16_t *wl, cudaStream_t s);
+    // First pass of the prediction only (x_g, r_g, raw features and their sums; no network).
+    int launch_ws_features(const BankedView &A, const WsBuffers &w, const double *b, const WsHistory &hist,
+                           size_t len, cudaStream_t s);
+
     // mas_noalloc.cu: y = A x and *dot = x . y with the reduction scratch in a static device array
     // (no allocation). Throws Error(ERR_INVALID) beyond noalloc_max_banks() banks.
     void launch_spmv_dot_noalloc(const BankedView &A, const double *x, double *y, double *dot, cudaStream_t s);

@@ -32,29 +32,12 @@
 // the three layers move about 30 MB of hidden states each (the gathers hit L2) and do
 // 3 x 2 x 227 K x 64 x 128 = 11 GFLOP on the tensor pipe.
 
-#include <cuda_bf16.h>
-
-#include "mas_common.cuh"
+#include "mas_ws_common.cuh"
 
 namespace pmas
 {
     namespace
     {
-        constexpr int F = WS_FEATURES;
-        constexpr int H = WS_HIDDEN;
-        constexpr int WT = 256;         // threads of the per-vertex kernels
-        constexpr int TILE = 128;       // vertices per CTA of a layer
-        constexpr int LT = 256;         // threads of a layer CTA (8 warps x 16 vertices)
-        constexpr int TS = 2 * H + 8;   // shared row stride (bf16): 272 B, conflict-free ldmatrix
-
-        // Parameter offsets in the flat float32 vector (the .psws layout).
-        constexpr int OFF_WIN = 0;
-        constexpr int OFF_BIN = OFF_WIN + H * F;
-        __host__ __device__ constexpr int off_layer(int l) { return OFF_BIN + H + l * (H * 2 * H + H); }
-        constexpr int OFF_WOUT = off_layer(WS_LAYERS);
-        constexpr int OFF_BOUT = OFF_WOUT + 3 * H;
-        static_assert(OFF_BOUT + 3 == WS_PARAMS, "parameter layout");
-
         __device__ __forceinline__ double block_entry(const BankedView &A, long long slot, int lane, int q)
         {
             return A.vals[banked_value_index(slot, lane, q, 3)];
@@ -197,33 +180,6 @@ namespace pmas
                     ws->sums[i] = tot[i];
         }
 
-        struct Norms
-        {
-            float iq, iv, ip, mlog; // 1 / rms (0 if the rms is 0) and the mean log trace
-        };
-
-        __device__ __forceinline__ Norms norms(const WsState *ws)
-        {
-            const double cnt = ws->sums[4];
-            Norms n{0.f, 0.f, 0.f, 0.f};
-            if (cnt > 0.0)
-            {
-                const double dofs = 3.0 * cnt;
-                const double sq = sqrt(ws->sums[0] / dofs), sv = sqrt(ws->sums[1] / dofs),
-                             sp = sqrt(ws->sums[2] / dofs);
-                n.iq = sq > 0.0 ? (float)(1.0 / sq) : 0.f;
-                n.iv = sv > 0.0 ? (float)(1.0 / sv) : 0.f;
-                n.ip = sp > 0.0 ? (float)(1.0 / sp) : 0.f;
-                n.mlog = (float)(ws->sums[3] / cnt);
-            }
-            return n;
-        }
-
-        __device__ __forceinline__ bool node_real(const int *rowlen, const int *diag_slot, int u)
-        {
-            return rowlen[u] > 0 && diag_slot[u] >= 0;
-        }
-
         // One thread per vertex: its 16 normalised features against W_in (shared memory, every
         // lane reading the same weight: broadcast), 64 hidden units written as eight 16-byte
         // stores.
@@ -286,172 +242,6 @@ namespace pmas
                     ob[k] = __float22bfloat162_rn(make_float2(fmaxf(a0, 0.f), fmaxf(a1, 0.f)));
                 }
                 dst[c] = out;
-            }
-        }
-
-        __device__ __forceinline__ void ldsm_x4(uint32_t (&a)[4], uint32_t addr)
-        {
-            asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0, %1, %2, %3}, [%4];"
-                         : "=r"(a[0]), "=r"(a[1]), "=r"(a[2]), "=r"(a[3])
-                         : "r"(addr));
-        }
-
-        __device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1)
-        {
-            asm volatile("mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
-                         "{%8, %9}, {%0, %1, %2, %3};"
-                         : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
-                         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-        }
-
-        // One message-passing layer for 64 vertices. Shared tile T[v] = [h_v ; m_v] (bf16,
-        // K = 128), W_l as rows of K (the mma's column-major B), then each warp multiplies its
-        // 16 vertices by W_l^T: 8 k-steps x 8 n-tiles of m16n8k16.
-        __global__ void __launch_bounds__(LT, 4) k_ws_layer(BankedView A, const float *__restrict__ wslot,
-                                                         const __nv_bfloat16 *__restrict__ hin,
-                                                         const uint16_t *__restrict__ wl, const float *__restrict__ bl,
-                                                         const int *__restrict__ diag_slot,
-                                                         __nv_bfloat16 *__restrict__ hout)
-        {
-            // Dynamic shared memory (52 KB: four CTAs, 32 warps per SM): the tile, W_l, the bias.
-            extern __shared__ __align__(16) unsigned char layer_smem[];
-            __nv_bfloat16 *T = reinterpret_cast<__nv_bfloat16 *>(layer_smem);
-            __nv_bfloat16 *Wsm = T + TILE * TS;
-            float *bias = reinterpret_cast<float *>(Wsm + H * TS);
-            const int nodes = A.banks * 32;
-            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-            // W_l: 64 rows x 128 bf16 = 16 chunks of 16 B per row.
-            for (int i = threadIdx.x; i < H * 16; i += LT)
-            {
-                const int row = i >> 4, ch = i & 15;
-                *reinterpret_cast<uint4 *>(&Wsm[row * TS + ch * 8]) =
-                    __ldg(reinterpret_cast<const uint4 *>(wl + row * 2 * H) + ch);
-            }
-            if (threadIdx.x < H)
-                bias[threadIdx.x] = bl[threadIdx.x];
-            // Gather: warp w fills rows 16 w .. 16 w + 15, four at a time: lane group q = lane / 8
-            // takes one row, lane gl = lane % 8 its hidden units 8 gl .. 8 gl + 7 (16-byte loads),
-            // so four rows' neighbour loads are in flight together. Every lane runs the warp's
-            // longest row; slots past a row's end carry w = 0 and the row's own (valid) index.
-            const uint4 *h8 = reinterpret_cast<const uint4 *>(hin);
-            const int gq = lane >> 3, gl = lane & 7;
-            int my_len = 0;
-            long long my_s0 = 0;
-            {
-                const int u = blockIdx.x * TILE + warp * 16 + (lane & 15);
-                if (u < nodes && node_real(A.rowlen, diag_slot, u))
-                {
-                    my_len = A.rowlen[u];
-                    my_s0 = A.slice[u >> 5];
-                }
-            }
-            for (int rb = 0; rb < 16; rb += 4)
-            {
-                const int rl = rb + gq;
-                const int r = warp * 16 + rl;
-                const int u = blockIdx.x * TILE + r;
-                const int len = __shfl_sync(FULL, my_len, rl);
-                const long long s0 = __shfl_sync(FULL, my_s0, rl);
-                int maxlen = len;
-#pragma unroll
-                for (int o = 8; o < 32; o <<= 1)
-                    maxlen = max(maxlen, __shfl_xor_sync(FULL, maxlen, o));
-                float acc[8];
-#pragma unroll
-                for (int i = 0; i < 8; ++i)
-                    acc[i] = 0.f;
-                uint4 self = make_uint4(0u, 0u, 0u, 0u);
-                if (len > 0)
-                    self = h8[(long long)u * (H / 8) + gl];
-                const int uu = (u < nodes) ? u : 0;
-                for (int k0 = 0; k0 < maxlen; k0 += 8)
-                {
-                    const int kk = k0 + gl;
-                    int col = uu;
-                    float w = 0.f;
-                    if (kk < len)
-                    {
-                        col = A.cols[(s0 + kk) * 32 + (u & 31)];
-                        w = wslot[(s0 + kk) * 32 + (u & 31)];
-                    }
-#pragma unroll
-                    for (int j = 0; j < 8; ++j)
-                    {
-                        const int cj = __shfl_sync(FULL, col, j, 8);
-                        const float wj = __shfl_sync(FULL, w, j, 8);
-                        const uint4 hv = h8[(long long)cj * (H / 8) + gl];
-                        const __nv_bfloat162 *hb = reinterpret_cast<const __nv_bfloat162 *>(&hv);
-#pragma unroll
-                        for (int i = 0; i < 4; ++i)
-                        {
-                            const float2 f2 = __bfloat1622float2(hb[i]);
-                            acc[2 * i] = fmaf(wj, f2.x, acc[2 * i]);
-                            acc[2 * i + 1] = fmaf(wj, f2.y, acc[2 * i + 1]);
-                        }
-                    }
-                }
-                uint4 m8;
-                __nv_bfloat162 *mb = reinterpret_cast<__nv_bfloat162 *>(&m8);
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-                    mb[i] = __float22bfloat162_rn(make_float2(acc[2 * i], acc[2 * i + 1]));
-                *reinterpret_cast<uint4 *>(&T[r * TS + 8 * gl]) = self;
-                *reinterpret_cast<uint4 *>(&T[r * TS + H + 8 * gl]) = m8;
-            }
-            __syncthreads();
-
-            // Tensor-core product of the warp's 16 rows with W_l^T.
-            float d[8][4];
-#pragma unroll
-            for (int nt = 0; nt < 8; ++nt)
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-                    d[nt][i] = 0.f;
-            const uint32_t tbase = smem_addr(T), wbase = smem_addr(Wsm);
-            const int arow = warp * 16 + (lane & 15), acol = (lane >> 4) * 8;
-            const int brow = (lane & 7) + ((lane >> 4) << 3), bcol = ((lane >> 3) & 1) * 8;
-#pragma unroll
-            for (int ks = 0; ks < (2 * H) / 16; ++ks)
-            {
-                uint32_t a[4];
-                ldsm_x4(a, tbase + (uint32_t)((arow * TS + ks * 16 + acol) * 2));
-#pragma unroll
-                for (int np = 0; np < 4; ++np)
-                {
-                    uint32_t bfr[4];
-                    ldsm_x4(bfr, wbase + (uint32_t)(((np * 16 + brow) * TS + ks * 16 + bcol) * 2));
-                    mma_bf16(d[2 * np], a, bfr[0], bfr[1]);
-                    mma_bf16(d[2 * np + 1], a, bfr[2], bfr[3]);
-                }
-            }
-            __syncwarp();
-            // Epilogue: h_out = h + relu(acc + b), written over the warp's own rows of T.
-            const int g = lane >> 2, c2 = (lane & 3) * 2;
-#pragma unroll
-            for (int nt = 0; nt < 8; ++nt)
-#pragma unroll
-                for (int half = 0; half < 2; ++half)
-                {
-                    const int r = warp * 16 + g + half * 8;
-                    const int col = nt * 8 + c2;
-                    __nv_bfloat162 *tp = reinterpret_cast<__nv_bfloat162 *>(&T[r * TS + col]);
-                    const float2 hs = __bfloat1622float2(*tp);
-                    const float v0 = hs.x + fmaxf(d[nt][2 * half] + bias[col], 0.f);
-                    const float v1 = hs.y + fmaxf(d[nt][2 * half + 1] + bias[col + 1], 0.f);
-                    *tp = __float22bfloat162_rn(make_float2(v0, v1));
-                }
-            __syncwarp();
-            __nv_bfloat162 *o2 = reinterpret_cast<__nv_bfloat162 *>(hout);
-            for (int rr = 0; rr < 16; ++rr)
-            {
-                const int r = warp * 16 + rr;
-                const int u = blockIdx.x * TILE + r;
-                if (u >= nodes)
-                    break;
-                __nv_bfloat162 v = __float2bfloat162_rn(0.f);
-                if (node_real(A.rowlen, diag_slot, u))
-                    v = *reinterpret_cast<const __nv_bfloat162 *>(&T[r * TS + 2 * lane]);
-                o2[(long long)u * (H / 2) + lane] = v;
             }
         }
 
@@ -706,6 +496,25 @@ namespace pmas
         cuda_check(cudaGetLastError(), "warm start graph launch");
     }
 
+    int launch_ws_features(const BankedView &A, const WsBuffers &w, const double *b, const WsHistory &hist,
+                           size_t len, cudaStream_t s)
+    {
+        const int nodes = A.banks * 32;
+        if (nodes == 0)
+            return 0;
+        const int grid_v = (nodes + WT - 1) / WT;
+        const int grid_r = ws_reduce_ctas();
+        if (grid_v > w.capacity || grid_r > w.capacity)
+            throw Error(ERR_INVALID, "[MAS] warm start reduction scratch too small");
+        k_ws_gram<<<grid_r, WT, 0, s>>>(b, hist, nullptr, nullptr, len, w.st, w.partials);
+        cuda_check(cudaGetLastError(), "warm start gram launch");
+        k_ws_residual<<<grid_r, WT, 0, s>>>(b, hist, w.st, w.rg, len);
+        cuda_check(cudaGetLastError(), "warm start residual launch");
+        k_ws_features<<<grid_v, WT, 0, s>>>(A, w.diag_slot, b, w.rg, hist.x[0], hist.x[1], w.feat, w.st, w.partials);
+        cuda_check(cudaGetLastError(), "warm start features launch");
+        return 3;
+    }
+
     int launch_ws_network(const BankedView &A, const WsBuffers &w, const double *b, const WsHistory &hist,
                           size_t len, cudaStream_t s)
     {
@@ -730,13 +539,14 @@ namespace pmas
         const int grid_t = (nodes + TILE - 1) / TILE;
         constexpr int LAYER_SMEM = (TILE + H) * TS * 2 + H * 4;
         static_assert((TILE * TS * 2) % 16 == 0 && ((TILE + H) * TS * 2) % 16 == 0, "shared layout");
-        cuda_check(cudaFuncSetAttribute(k_ws_layer, cudaFuncAttributeMaxDynamicSharedMemorySize, LAYER_SMEM),
+        cuda_check(cudaFuncSetAttribute(k_ws_layer<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, LAYER_SMEM),
                    "layer smem attribute");
         for (int l = 0; l < WS_LAYERS; ++l)
         {
-            k_ws_layer<<<grid_t, LT, LAYER_SMEM, s>>>(A, w.wslot, reinterpret_cast<const __nv_bfloat16 *>(w.h[l & 1]),
-                                            w.wl + (size_t)l * WS_LAYER_WEIGHTS, w.params + off_layer(l) + H * 2 * H,
-                                            w.diag_slot, reinterpret_cast<__nv_bfloat16 *>(w.h[(l + 1) & 1]));
+            k_ws_layer<false><<<grid_t, LT, LAYER_SMEM, s>>>(
+                A, w.wslot, reinterpret_cast<const __nv_bfloat16 *>(w.h[l & 1]), w.wl + (size_t)l * WS_LAYER_WEIGHTS,
+                w.params + off_layer(l) + H * 2 * H, w.diag_slot, reinterpret_cast<__nv_bfloat16 *>(w.h[(l + 1) & 1]),
+                nullptr, nullptr);
             cuda_check(cudaGetLastError(), "warm start layer launch");
         }
         k_ws_output<<<(nodes + WT - 1) / WT, WT, 0, s>>>(nodes, A.rowlen, w.diag_slot,

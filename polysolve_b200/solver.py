@@ -44,6 +44,9 @@ EXPORTED_SYMBOLS = [
     "mas_debug_spmv_multi", "mas_set_warm_start_model", "mas_reset_warm_start", "mas_debug_warm_start",
     "mas_market_load", "mas_market_dims", "mas_market_copy_csc", "mas_market_copy_dense", "mas_market_free",
     "mas_market_last_error", "mas_market_write_csc", "mas_market_write_vector", "mas_debug_fail_allocation",
+    "mas_ws_trainer_create", "mas_ws_trainer_destroy", "mas_ws_trainer_add_sample", "mas_ws_trainer_sample_count",
+    "mas_ws_trainer_train", "mas_ws_trainer_evaluate", "mas_ws_trainer_gradient", "mas_ws_trainer_get_params",
+    "mas_ws_trainer_last_error",
 ]
 
 
@@ -103,6 +106,17 @@ def library() -> ctypes.CDLL:
         L.mas_debug_warm_start.argtypes = [vp, vp, vp, i, vp, vp, vp, vp]
         L.mas_order_blocks.argtypes = [i, vp, vp, i, vp, ctypes.c_char_p, ip, ip]
         L.mas_debug_fail_allocation.argtypes = [ctypes.c_longlong]
+        L.mas_ws_trainer_create.argtypes = [vp, ctypes.c_longlong, hp]
+        L.mas_ws_trainer_destroy.argtypes = [vp]
+        L.mas_ws_trainer_destroy.restype = None
+        L.mas_ws_trainer_add_sample.argtypes = [vp, vp, vp, vp, i, vp, i]
+        L.mas_ws_trainer_sample_count.argtypes = [vp]
+        L.mas_ws_trainer_train.argtypes = [vp, vp, vp, i, vp]
+        L.mas_ws_trainer_evaluate.argtypes = [vp, vp, i, vp]
+        L.mas_ws_trainer_gradient.argtypes = [vp, i, vp, ctypes.c_longlong, vp]
+        L.mas_ws_trainer_get_params.argtypes = [vp, vp, ctypes.c_longlong]
+        L.mas_ws_trainer_last_error.argtypes = [vp]
+        L.mas_ws_trainer_last_error.restype = ctypes.c_char_p
         _LIB = L
     return _LIB
 
@@ -413,3 +427,85 @@ class Solver:
 
 
 MASSolver = Solver
+
+
+class WarmStartTrainer:
+    """New: GPU training of the learned warm start's network (``mas_ws_trainer_*``): the library's own
+    forward / reverse-pass kernels and Adam, samples resident in device memory."""
+
+    def __init__(self, params: np.ndarray):
+        p = np.ascontiguousarray(params, dtype=np.float32)
+        h = ctypes.c_void_p()
+        rc = library().mas_ws_trainer_create(p.ctypes.data, p.size, ctypes.byref(h))
+        if rc != MAS_OK:
+            msg = library().mas_ws_trainer_last_error(None).decode()
+            if rc == MAS_ERR_OOM:
+                raise CudaOutOfMemoryError(msg)
+            raise MasError(rc, msg or f"[MAS] error {rc}")
+        self._t = h
+
+    def __del__(self):
+        t = getattr(self, "_t", None)
+        if t is not None and t.value:
+            try:
+                library().mas_ws_trainer_destroy(t)
+            except Exception:
+                pass
+            self._t = None
+
+    def _check(self, rc: int) -> None:
+        if rc == MAS_OK:
+            return
+        msg = library().mas_ws_trainer_last_error(self._t).decode()
+        if rc == MAS_ERR_OOM:
+            raise CudaOutOfMemoryError(msg)
+        raise MasError(rc, msg or f"[MAS] error {rc}")
+
+    def add_sample(self, solver: "Solver", b: np.ndarray, history, x_exact: np.ndarray) -> int:
+        """Sample from ``solver`` (factorized with this step's matrix): b, the kept solutions (newest
+        first, 2 to 4) and the exact solution, caller order. Returns the sample index."""
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        hist = np.ascontiguousarray(np.stack([np.asarray(h, dtype=np.float64) for h in history]))
+        x = np.ascontiguousarray(x_exact, dtype=np.float64)
+        self._check(library().mas_ws_trainer_add_sample(self._t, solver._h, b.ctypes.data, hist.ctypes.data,
+                                                         hist.shape[0], x.ctypes.data, b.size))
+        return self.sample_count - 1
+
+    @property
+    def sample_count(self) -> int:
+        return int(library().mas_ws_trainer_sample_count(self._t))
+
+    def train(self, samples, lrs) -> np.ndarray:
+        """One Adam step per listed sample (in order) with the given learning rates; the losses."""
+        idx = np.ascontiguousarray(samples, dtype=np.int32)
+        lr = np.ascontiguousarray(np.broadcast_to(np.asarray(lrs, dtype=np.float32), idx.shape))
+        out = np.zeros(idx.size)
+        self._check(library().mas_ws_trainer_train(self._t, idx.ctypes.data, lr.ctypes.data, idx.size,
+                                                    out.ctypes.data))
+        return out
+
+    def evaluate(self, samples) -> np.ndarray:
+        """rho of each listed sample under the current parameters."""
+        idx = np.ascontiguousarray(samples, dtype=np.int32)
+        out = np.zeros(idx.size)
+        self._check(library().mas_ws_trainer_evaluate(self._t, idx.ctypes.data, idx.size, out.ctypes.data))
+        return out
+
+    def gradient(self, sample: int) -> tuple[float, np.ndarray]:
+        """(loss, gradient) of one sample; no update."""
+        g = np.zeros(_ws_params(), dtype=np.float32)
+        loss = ctypes.c_double()
+        self._check(library().mas_ws_trainer_gradient(self._t, int(sample), g.ctypes.data, g.size,
+                                                       ctypes.byref(loss)))
+        return loss.value, g
+
+    def params(self) -> np.ndarray:
+        p = np.zeros(_ws_params(), dtype=np.float32)
+        self._check(library().mas_ws_trainer_get_params(self._t, p.ctypes.data, p.size))
+        return p
+
+
+def _ws_params() -> int:
+    from . import warmstart
+
+    return warmstart.PARAMS

@@ -1,6 +1,6 @@
 """Learned warm start on the host: the weight file format, the network's parameter layout, the
-float64 oracle's reverse pass against finite differences, and the training code against the
-oracle (the definitions the GPU kernels follow)."""
+float64 oracle's reverse pass and training objective against finite differences, and the oracle's
+emulation of the GPU training pass against the plain float64 one."""
 
 import re
 from pathlib import Path
@@ -78,46 +78,76 @@ def test_oracle_backward_matches_finite_differences():
         assert abs(fd - grad[i]) <= 1e-5 * max(1.0, abs(fd)), (i, fd, grad[i])
 
 
-def test_training_model_matches_oracle_forward():
-    torch = pytest.importorskip("torch")
+def _spd(V, seed):
+    import scipy.sparse as sp
+
+    rng = np.random.default_rng(seed)
+    M = sp.random(3 * V, 3 * V, density=0.05, random_state=rng)
+    return (M @ M.T + 3 * V * sp.eye(3 * V)).tocsr()
+
+
+def test_loss_gradient_matches_finite_differences():
+    """The training objective 1 - rho through the float64 network: its reverse pass (backward64 of
+    dL/dout) against central differences of the loss."""
+    f, src, dst, w = _small_graph(V=30, seed=7)
+    rng = np.random.default_rng(8)
+    prm = 0.3 * rng.standard_normal(W.PARAMS)
+    A = _spd(30, 9)
+    e = rng.standard_normal(90)
+    re = A @ e
+    ere, s_q = float(e @ re), 0.7
+
+    def loss_of(p):
+        out, _ = WO.forward64(p, f, src, dst, w)
+        return WO.loss_and_output_gradient(out, A, re, s_q, ere)[0]
+
+    out, cache = WO.forward64(prm, f, src, dst, w)
+    loss, rho, g_out = WO.loss_and_output_gradient(out, A, re, s_q, ere)
+    assert 0.0 <= rho <= 1.0 + 1e-12 and abs(loss - (1 - rho)) < 1e-15
+    grad = WO.backward64(cache, g_out)
+    lay, _ = WO.layout()
+    eps = 1e-6
+    for name, (o, shape) in lay.items():
+        for i in o + rng.choice(int(np.prod(shape)), size=2, replace=False):
+            p1, p2 = prm.copy(), prm.copy()
+            p1[i] += eps
+            p2[i] -= eps
+            fd = (loss_of(p1) - loss_of(p2)) / (2 * eps)
+            assert abs(fd - grad[i]) <= 1e-5 * max(1.0, abs(fd)), (name, fd, grad[i])
+
+
+def test_device_training_emulation_close_to_float64():
+    """The emulation of the GPU training pass (bf16 at the tensor-core products) stays within BF16
+    error of the plain float64 gradient, tensor by tensor."""
     from polysolve_b200 import warmstart_train as T
 
-    f, src, dst, w = _small_graph(seed=3)
-    prm = 0.3 * np.random.default_rng(4).standard_normal(W.PARAMS)
-    model = T.build_model().double()
-    model.load_flat(prm)
-    out = model(torch.from_numpy(f), torch.from_numpy(src), torch.from_numpy(dst), torch.from_numpy(w))
-    ref, _ = WO.forward64(prm, f, src, dst, w)
-    assert np.allclose(out.detach().numpy(), ref, rtol=1e-12, atol=1e-12)
+    f, src, dst, w = _small_graph(V=60, seed=10)
+    rng = np.random.default_rng(11)
+    prm = T.initial_params(2)  # the training's initial scale (BF16 error grows with random large weights)
+    o = W.layout()["w_out"][0]
+    prm[o:o + 3 * W.HIDDEN] *= 10.0
+    A = _spd(60, 12)
+    e = rng.standard_normal(180)
+    re = A @ e
+    ere, s_q = float(e @ re), 1.3
+    loss_d, grad_d = WO.train_gradient_device(prm, f.astype(np.float32), src, dst, w, A, re, s_q, ere)
+    out, cache = WO.forward64(prm.astype(np.float64), f.astype(np.float32).astype(np.float64), src, dst, w)
+    loss, _, g_out = WO.loss_and_output_gradient(out, A, re, s_q, ere)
+    grad = WO.backward64(cache, g_out)
+    assert abs(loss_d - loss) <= 2e-2
+    for name, (o, shape) in WO.layout()[0].items():
+        a, b = grad_d[o:o + int(np.prod(shape))], grad[o:o + int(np.prod(shape))]
+        assert np.linalg.norm(a - b) <= 6e-2 * np.linalg.norm(b), name
 
 
-def test_training_features_match_oracle():
+def test_initial_parameters_are_seeded_and_scaled():
     from polysolve_b200 import warmstart_train as T
 
-    s0, b = synthetic.workload_sequence60(3, seed=2, N=5)
-    A = s0.scipy().tocsr()
-    rng = np.random.default_rng(5)
-    x1, x2 = rng.standard_normal(s0.n), rng.standard_normal(s0.n)
-    src, dst, w, D = T.block_graph(A)
-    x3 = rng.standard_normal(s0.n)
-    xg = T.history_guess(A, b, [x1, x2, x3])
-    f, sq, _, _ = T.features(A, b, x1, x2, D, xg)
-    src_o, dst_o, w_o, D_o = WO.graph(A)
-    order_t = np.lexsort((src, dst))
-    order_o = np.lexsort((src_o, dst_o))
-    assert np.array_equal(src[order_t], src_o[order_o]) and np.array_equal(dst[order_t], dst_o[order_o])
-    assert np.allclose(w[order_t], w_o[order_o], rtol=1e-14)
-    raw, sums = WO.features(A, b, x1, x2, D_o, xg)
-    # the training's history guess follows the oracle's Galerkin rule (no c)
-    y, _, _, _, _ = WO.galerkin(A, b, x1, x2, np.zeros_like(b), x3)
-    xg_o = sum(yi * vi for yi, vi in zip(y, WO.galerkin_basis((x1, x2, x3), np.zeros_like(b))))
-    assert np.linalg.norm(xg - xg_o) <= 1e-8 * np.linalg.norm(xg_o)
-    fo = WO.normalise(raw, sums)
-    assert np.allclose(f, fo, rtol=1e-10, atol=1e-12)
-    assert abs(sq - WO.s_q(sums)) <= 1e-12 * sq
-    # normalised q, v, p have unit rms
-    for k in range(3):
-        assert abs(np.sqrt(np.mean(fo[:, 3 * k:3 * k + 3] ** 2)) - 1.0) < 1e-12
+    p1, p2 = T.initial_params(3), T.initial_params(3)
+    assert np.array_equal(p1, p2) and p1.dtype == np.float32 and p1.size == W.PARAMS
+    t = W.unpack(p1)
+    assert np.abs(t["w_in"]).max() <= 1 / 4 and np.abs(t["w_0"]).max() <= 0.5 / np.sqrt(128)
+    assert np.abs(t["w_out"]).max() <= 0.1 / 8
 
 
 def test_galerkin_oracle_is_never_worse_than_previous():

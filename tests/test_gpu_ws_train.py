@@ -1,0 +1,138 @@
+"""GPU training of the learned warm start (``WarmStartTrainer``, ``csrc/mas_ws_train.cu``).
+
+* The gradient of one sample from the library's own forward / reverse-pass kernels against the
+  float64 oracle: tightly against the oracle's emulation of the GPU pass's rounding points
+  (``train_gradient_device``), and within BF16 tolerance against the plain float64 reverse pass
+  (``backward64``, itself checked against finite differences on the CPU).
+* The gradient is deterministic (fixed-order sums, no atomics).
+* Adam steps on a few sequences raise rho on held-out samples.
+* The shipped network (trained on the GPU by these kernels) beats the method without it: the same
+  Galerkin combination of the kept solutions with all network weights zero.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import warmstart_oracle as WO
+from polysolve_b200 import Solver, WarmStartTrainer, synthetic
+from polysolve_b200 import warmstart as W
+from polysolve_b200 import warmstart_train as WT
+
+pytestmark = pytest.mark.gpu
+
+
+def _tensor_errors(got, ref):
+    errs = {}
+    for name, (o, shape) in W.layout().items():
+        a, b = got[o:o + int(np.prod(shape))], ref[o:o + int(np.prod(shape))]
+        errs[name] = float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+    return errs
+
+
+@pytest.fixture(scope="module")
+def sample7():
+    """One sample on a 7^3 sequence (step 4: four kept solutions) and its host-side definition."""
+    N, seed = 7, 11
+    solver = Solver.create("MAS", "")
+    solver.set_parameters({"MAS": dict(WT.SOLVE_PARAMS)})
+    seq = []
+    for k in range(5):
+        sk, bk = synthetic.workload_sequence60(k + 3, seed=seed, N=N)
+        if k == 0:
+            solver.set_positions(sk.positions)
+        solver.factorize(sk.scipy())
+        x = seq[-1][2].copy() if seq else np.zeros(sk.n)
+        solver.solve(bk, x)
+        seq.append((sk, bk, x))
+    prm = WT.initial_params(seed=3)
+    # a trained-like spread of output weights, so the loss is not near its random-direction value
+    prm[W.layout()["w_out"][0]:W.layout()["w_out"][0] + 3 * W.HIDDEN] *= 10.0
+    trainer = WarmStartTrainer(prm)
+    sk, bk, xk = seq[4]
+    hist = [seq[3][2], seq[2][2], seq[1][2], seq[0][2]]
+    trainer.add_sample(solver, bk, hist, xk)
+    A = sk.scipy().tocsr()
+    src, dst, w, D = WO.graph(A)
+    y, _, _, _, _ = WO.galerkin(A, bk, hist[0], hist[1], np.zeros_like(bk), hist[2], hist[3])
+    xg = sum(yi * vi for yi, vi in zip(y, WO.galerkin_basis(tuple(hist), np.zeros_like(bk))))
+    raw, sums = WO.features(A, bk, hist[0], hist[1], D, xg)
+    f32 = WO.normalise(raw.astype(np.float32), sums, dtype=np.float32)
+    re = bk - A @ xg
+    ere = float((xk - xg) @ re)
+    return trainer, prm, dict(A=A, src=src, dst=dst, w=w, f32=f32, f64=WO.normalise(raw, sums), re=re,
+                              s_q=WO.s_q(sums), ere=ere)
+
+
+def test_gradient_matches_oracle(sample7):
+    trainer, prm, d = sample7
+    loss, grad = trainer.gradient(0)
+    loss_e, grad_e = WO.train_gradient_device(prm, d["f32"], d["src"], d["dst"], d["w"], d["A"], d["re"], d["s_q"],
+                                              d["ere"])
+    assert abs(loss - loss_e) <= 1e-4 * max(1.0, abs(loss_e)), (loss, loss_e)
+    tight = _tensor_errors(grad.astype(np.float64), grad_e)
+    assert max(tight.values()) <= 5e-3, tight
+    # plain float64 reverse pass (no bf16 rounding anywhere)
+    out, cache = WO.forward64(prm.astype(np.float64), d["f64"], d["src"], d["dst"], d["w"])
+    loss64, _, g_out = WO.loss_and_output_gradient(out, d["A"], d["re"], d["s_q"], d["ere"])
+    grad64 = WO.backward64(cache, g_out)
+    loose = _tensor_errors(grad.astype(np.float64), grad64)
+    assert max(loose.values()) <= 6e-2, loose
+    assert abs(loss - loss64) <= 2e-2
+
+
+def test_gradient_is_deterministic(sample7):
+    trainer, _, _ = sample7
+    l1, g1 = trainer.gradient(0)
+    l2, g2 = trainer.gradient(0)
+    assert l1 == l2
+    assert np.array_equal(g1, g2)
+
+
+def test_adam_steps_raise_held_out_rho():
+    trainer = WarmStartTrainer(WT.initial_params(seed=1))
+    jobs = [(8, 101, 10, 10), (9, 102, 40, 10), (10, 103, 80, 10), (8, 104, 120, 10)]
+    idx = WT.collect(trainer, jobs)
+    assert len(idx) == 4 * 8
+    rep = WT.train(trainer, idx, epochs=12, lr=3e-3, seed=0, val_fraction=0.25, log=lambda s: None)
+    assert rep["val_rho"] > rep["val_rho_initial"] + 0.2, rep
+    assert rep["val_rho"] > 0.4, rep
+
+
+def test_trainer_rejects_bad_input():
+    from polysolve_b200 import MasError
+
+    with pytest.raises(MasError):
+        WarmStartTrainer(np.zeros(10, dtype=np.float32))
+    trainer = WarmStartTrainer(WT.initial_params())
+    with pytest.raises(MasError):
+        trainer.gradient(0)  # no samples yet
+
+
+def test_shipped_network_beats_galerkin_history_alone():
+    """The method without the network: the same Galerkin combination of the kept solutions with every
+    network weight zero (c = 0 is dropped). The shipped network's correction must remove
+    iterations on a sequence it was not trained on."""
+    N, seed, k0, steps = 20, 777, 60, 12
+    base = {"block_dim": 3, "relative_tolerance": 1e-8, "absolute_tolerance": 0.0, "precision": "fp16",
+            "true_residual_period": 50, "check_period": 1, "initial_guess": "learned"}
+    its = {}
+    for name, prm in (("learned", W.default_weights()), ("history_only", np.zeros(W.PARAMS, dtype=np.float32))):
+        s = Solver.create("MAS", "")
+        s.set_parameters({"MAS": base})
+        s.set_warm_start_model(prm)
+        total = 0
+        for k in range(k0, k0 + steps):
+            sk, bk = synthetic.workload_sequence60(k, seed=seed, N=N)
+            if k == k0:
+                s.set_positions(sk.positions)
+            s.factorize(sk.scipy())
+            x = np.zeros(sk.n)
+            s.solve(bk, x)
+            info = s.get_info()
+            assert info["solver_status"] == "Reach relative tolerance"
+            if k >= k0 + 4:  # full history from here on
+                total += info["solver_iter"]
+        its[name] = total
+    assert its["learned"] < its["history_only"], its
