@@ -440,13 +440,14 @@ namespace pmas
                 }
                 bsum[grp * H + k] = bs;
             }
-            for (int i = threadIdx.x; i < TILE * 32; i += LB_THREADS)
+            // [h ; m] rows: 16 chunks of 8 bf16 (eight of h, eight of m) per vertex.
+            for (int i = threadIdx.x; i < TILE * 16; i += LB_THREADS)
             {
-                const int row = i >> 5, ch = i & 31, u = base + row;
+                const int row = i >> 4, ch = i & 15, u = base + row;
                 uint4 v = make_uint4(0u, 0u, 0u, 0u);
                 if (u < nodes)
-                    v = ch < 16 ? *reinterpret_cast<const uint4 *>(hl + (long long)u * H + ch * 8)
-                                : *reinterpret_cast<const uint4 *>(ml + (long long)u * H + (ch - 16) * 8);
+                    v = ch < 8 ? *reinterpret_cast<const uint4 *>(hl + (long long)u * H + ch * 8)
+                               : *reinterpret_cast<const uint4 *>(ml + (long long)u * H + (ch - 8) * 8);
                 *reinterpret_cast<uint4 *>(&T[row * TS + ch * 8]) = v;
             }
             for (int i = threadIdx.x; i < H * 16; i += LB_THREADS)
