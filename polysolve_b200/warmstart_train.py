@@ -2,7 +2,7 @@
 
 Data: seeded elasticity sequences built like the 60^3 sequence workload
 (``synthetic.workload_sequence60``) on 12^3 to 28^3 grids, 100 sequences of 22 steps. Every step is
-solved by the plain FP64 MAS-PCG on the GPU to a relative residual of 1e-12 (from the previous
+solved by the plain FP64 MAS-PCG on the GPU to a relative residual of 1e-10 (from the previous
 step's solution); a sample is step k >= 2 with its kept solutions x_{k-1} .. x_{k-4} and the exact
 solution x_k. The trainer (``WarmStartTrainer``, C ABI ``mas_ws_trainer_*``) runs the solver's own
 prediction pipeline up to the features for each sample and keeps the sample in device memory.
@@ -61,7 +61,9 @@ def default_jobs(seed0: int = 1000, steps: int = 22):
     return jobs
 
 
-SOLVE_PARAMS = {"block_dim": 3, "relative_tolerance": 1e-12, "absolute_tolerance": 0.0, "max_iter": 5000,
+# 1e-10: FP64 PCG's recursive residual on these systems stalls a little above 1e-12; the history
+# guess's error e = x_k - x_g is some 1e-3 of x_k, far above the solve's error.
+SOLVE_PARAMS = {"block_dim": 3, "relative_tolerance": 1e-10, "absolute_tolerance": 0.0, "max_iter": 5000,
                 "precision": "fp64", "true_residual_period": 10, "check_period": 1, "initial_guess": "input"}
 
 

@@ -46,13 +46,14 @@ def sample7():
         x = seq[-1][2].copy() if seq else np.zeros(sk.n)
         solver.solve(bk, x)
         seq.append((sk, bk, x))
-    prm = WT.initial_params(seed=3)
-    # a trained-like spread of output weights, so the loss is not near its random-direction value
-    prm[W.layout()["w_out"][0]:W.layout()["w_out"][0] + 3 * W.HIDDEN] *= 10.0
-    trainer = WarmStartTrainer(prm)
+    # the shipped (trained) network, where the loss is well away from its random-direction value 1,
+    # and the training's initial parameters
+    trainers = {"shipped": (WarmStartTrainer(W.default_weights()), W.default_weights()),
+                "initial": (WarmStartTrainer(WT.initial_params(seed=3)), WT.initial_params(seed=3))}
     sk, bk, xk = seq[4]
     hist = [seq[3][2], seq[2][2], seq[1][2], seq[0][2]]
-    trainer.add_sample(solver, bk, hist, xk)
+    for trainer, _ in trainers.values():
+        trainer.add_sample(solver, bk, hist, xk)
     A = sk.scipy().tocsr()
     src, dst, w, D = WO.graph(A)
     y, _, _, _, _ = WO.galerkin(A, bk, hist[0], hist[1], np.zeros_like(bk), hist[2], hist[3])
@@ -61,29 +62,44 @@ def sample7():
     f32 = WO.normalise(raw.astype(np.float32), sums, dtype=np.float32)
     re = bk - A @ xg
     ere = float((xk - xg) @ re)
-    return trainer, prm, dict(A=A, src=src, dst=dst, w=w, f32=f32, f64=WO.normalise(raw, sums), re=re,
-                              s_q=WO.s_q(sums), ere=ere)
+    return trainers, dict(A=A, src=src, dst=dst, w=w, f32=f32, f64=WO.normalise(raw, sums), re=re,
+                          s_q=WO.s_q(sums), ere=ere)
 
 
-def test_gradient_matches_oracle(sample7):
-    trainer, prm, d = sample7
+@pytest.mark.parametrize("which", ["shipped", "initial"])
+def test_gradient_matches_oracle_emulation(sample7, which):
+    """Tight: the oracle restates the GPU pass's rounding points (bf16 at the tensor-core products),
+    so what remains is FP32 summation order."""
+    trainers, d = sample7
+    trainer, prm = trainers[which]
     loss, grad = trainer.gradient(0)
     loss_e, grad_e = WO.train_gradient_device(prm, d["f32"], d["src"], d["dst"], d["w"], d["A"], d["re"], d["s_q"],
                                               d["ere"])
     assert abs(loss - loss_e) <= 1e-4 * max(1.0, abs(loss_e)), (loss, loss_e)
     tight = _tensor_errors(grad.astype(np.float64), grad_e)
     assert max(tight.values()) <= 5e-3, tight
-    # plain float64 reverse pass (no bf16 rounding anywhere)
+
+
+def test_gradient_matches_float64_reverse_pass(sample7):
+    """Against the plain float64 network and reverse pass (no bf16 anywhere) with the trained weights:
+    within BF16 error (measured on the CPU for this sample: 0.75 % for the whole vector, at most 3.2 %
+    per tensor)."""
+    trainers, d = sample7
+    trainer, prm = trainers["shipped"]
+    loss, grad = trainer.gradient(0)
     out, cache = WO.forward64(prm.astype(np.float64), d["f64"], d["src"], d["dst"], d["w"])
     loss64, _, g_out = WO.loss_and_output_gradient(out, d["A"], d["re"], d["s_q"], d["ere"])
     grad64 = WO.backward64(cache, g_out)
-    loose = _tensor_errors(grad.astype(np.float64), grad64)
+    g = grad.astype(np.float64)
+    assert np.linalg.norm(g - grad64) <= 2e-2 * np.linalg.norm(grad64)
+    assert g @ grad64 >= 0.999 * np.linalg.norm(g) * np.linalg.norm(grad64)
+    loose = _tensor_errors(g, grad64)
     assert max(loose.values()) <= 6e-2, loose
-    assert abs(loss - loss64) <= 2e-2
+    assert abs(loss - loss64) <= 1e-3
 
 
 def test_gradient_is_deterministic(sample7):
-    trainer, _, _ = sample7
+    trainer, _ = sample7[0]["initial"]
     l1, g1 = trainer.gradient(0)
     l2, g2 = trainer.gradient(0)
     assert l1 == l2
