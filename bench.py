@@ -527,8 +527,9 @@ MULTI_METRIC = "ms per 16-right-hand-side solve to rel-residual 1e-8 at 1.6M DOF
 
 def run_contact16(args) -> None:
     """The 80^3 jittered mesh plus 20,000 contact couplings, 16 right-hand sides b ~ N(0, 1). A
-    step is one `solve_multi` of all 16 (groups of four sharing every matrix and inverse read), host
-    arrays in and out (the public call). Also reported: the same 16 solved one by one."""
+    step is one `solve_multi` of all 16 (one group of sixteen sharing every matrix and inverse read),
+    host arrays in and out (the public call). Also reported: the same 16 in groups of four, and
+    solved one by one."""
     import torch
 
     from polysolve_b200 import Solver, synthetic
@@ -575,10 +576,18 @@ def run_contact16(args) -> None:
     for c in range(R):
         sv.solve(B[c], x)
     seq = (time.perf_counter() - t0) * 1000.0
+    # The same right-hand sides in four groups of four.
+    sv.set_parameters({"MAS": {"rhs_group": 4}})
+    sv.solve_multi(B)
+    t0 = time.perf_counter()
+    sv.solve_multi(B)
+    g4_ms = (time.perf_counter() - t0) * 1000.0
+    sv.set_parameters({"MAS": {"rhs_group": 0}})
     # FP64 reference solutions (CHOLMOD is unavailable on this box): plain FP64 MAS-PCG to a
-    # relative residual of 1e-13 for every right-hand side; the worst relative solution error.
+    # relative residual of 1e-11 (FP64 PCG stalls near 3e-12 here) for every right-hand side; the
+    # worst relative solution error.
     ref = Solver.create("MAS", "")
-    ref.set_parameters({"MAS": dict(PLAIN, relative_tolerance=1e-13, max_iter=20000)})
+    ref.set_parameters({"MAS": dict(PLAIN, relative_tolerance=1e-11, max_iter=2000)})
     ref.set_positions(system.positions)
     ref.analyze_pattern(A, n)
     ref.factorize(A)
@@ -597,12 +606,13 @@ def run_contact16(args) -> None:
         "scaling": "weak", "vs_baseline": None,
         "dtype": "f64 (SpMV, dots, updates) + fp16 storage / f32 tensor-core products (MAS apply)",
         "data": "synthetic (seeded 80^3 jittered tet elasticity + 20,000 contact pairs, 16 b ~ N(0,1))",
-        "config": {"workload": f"{args.grid}^3 + contact, {n} DOF, 16 right-hand sides in groups of 4",
+        "config": {"workload": f"{args.grid}^3 + contact, {n} DOF, 16 right-hand sides in one group of 16",
                    "parallelism": f"replicas x{world}", "timing": "host clock around the public call (host arrays)"},
         "rhs_iterations": info.get("rhs_iterations"), "worst_relative_residual": worst,
         "worst_solution_relative_error": sol_err,
-        "fp64_reference": "plain FP64 MAS-PCG to relative residual 1e-13 per right-hand side "
+        "fp64_reference": "plain FP64 MAS-PCG to relative residual 1e-11 per right-hand side "
                           "(CHOLMOD unavailable on this box)",
+        "groups_of_4_ms": round(g4_ms, 3),
         "one_by_one_ms": round(float(t[1].item()), 3),
         "speedup_vs_one_by_one": round(float(t[1].item()) / float(t[0].item()), 3),
         "e2e": {"value": round(value, 3), "unit": "ms/16 RHS", "h2d_bytes_per_step": int(8 * n * R),

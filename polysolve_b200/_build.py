@@ -40,6 +40,7 @@ CU_SOURCES = [
     "mas_pcg.cu",
     "mas_noalloc.cu",
     "mas_multi.cu",
+    "mas_multi16.cu",
     "mas_warmstart.cu",
     "mas_ws_train.cu",
 ]

@@ -534,15 +534,16 @@ namespace pmas
             static_assert(2 * G == 8, "the B operand has eight columns: G hi / lo pairs");
         };
 
-        template <int BD>
+        // XS, YS: strides (values) between consecutive right-hand sides in xh / xl and in ys.
+        template <int BD, int XS = 32 * BD, int YS = 32 * BD>
         __device__ __forceinline__ void symv_mma16_g(const __half *M, const __half *xh, const __half *xl, float *ys,
                                                      int lane)
         {
-            constexpr int NS = 2 * BD, NB = NS * (NS - 1) / 2, N = 32 * BD;
+            constexpr int NS = 2 * BD, NB = NS * (NS - 1) / 2;
             const int g = lane >> 2, q = lane & 3;
             const int c = lane >> 3, rr = lane & 7;
             // B column n = g: right-hand side g / 2, hi (even) or lo (odd).
-            const __half *xsrc = ((g & 1) ? xl : xh) + (g >> 1) * N;
+            const __half *xsrc = ((g & 1) ? xl : xh) + (g >> 1) * XS;
             uint32_t bf[NS][2];
 #pragma unroll
             for (int S = 0; S < NS; ++S)
@@ -585,8 +586,8 @@ namespace pmas
 #pragma unroll
             for (int R = 0; R < NS; ++R)
             {
-                ys[q * N + 16 * R + g] = d[R][0] + d[R][1];
-                ys[q * N + 16 * R + g + 8] = d[R][2] + d[R][3];
+                ys[q * YS + 16 * R + g] = d[R][0] + d[R][1];
+                ys[q * YS + 16 * R + g + 8] = d[R][2] + d[R][3];
             }
             __syncwarp();
         }
@@ -764,6 +765,200 @@ namespace pmas
             }
         }
 
+        // ---- RHS_WIDE (16) right-hand sides at once (block size 3, binary16 inverses): the B operand
+        // of each m16n8k16 holds four right-hand sides' hi / lo splits, so each inverse is multiplied in
+        // four n-tiles (symv_mma16_g per tile) and read from memory once for all sixteen. Lane l loads,
+        // splits and stores right-hand side g = l % 16 (values e = 2 t + l / 16 of the matrix's 96), so
+        // every load and store of the interleaved vectors is 128 B per 16 lanes. xh / xl and ys use
+        // padded strides per right-hand side (100 halves, 97 floats) that spread the 16 lanes' words
+        // over the shared-memory banks.
+        struct ApplyLayoutW
+        {
+            static constexpr int BD = 3, N = 96, G = RHS_WIDE;
+            static constexpr int XS = N + 4, YS = N + 1;
+            static constexpr int S = (2 * BD) * (2 * BD - 1) / 2 * 256 + 2 * BD * 192;
+            static constexpr int STAGE_BYTES = S * 2;
+            static constexpr int XS_BYTES = 2 * 2 * G * XS + 4 * G * YS; // hi, lo, FP32 result
+            static constexpr int WARP_BYTES = 2 * STAGE_BYTES + XS_BYTES + 16;
+            static constexpr int SMEM_LIMIT = 232448 - 2048; // static shared memory: the grid sum's groups
+            static constexpr int W0 = SMEM_LIMIT / WARP_BYTES;
+            static constexpr int WARPS = W0 > 16 ? 16 : W0;
+            static_assert(STAGE_BYTES % 16 == 0 && WARP_BYTES % 16 == 0 && XS_BYTES % 8 == 0, "alignment");
+            static_assert((WARPS + 2) * 3 * G * 8 <= WARP_BYTES, "the final sums reuse the first warp's area");
+        };
+
+        template <int MODE>
+        __global__ void __launch_bounds__(ApplyLayoutW::WARPS * 32)
+            k_mas_apply_w(MasView mas, const double *__restrict__ r, double *__restrict__ z0, PcgState *st,
+                          ReduceBuf red, PcgConfig cfg)
+        {
+            using L = ApplyLayoutW;
+            constexpr int N = L::N, S = L::S, WARPS = L::WARPS, G = L::G, XS = L::XS, YS = L::YS;
+            constexpr int THREADS = WARPS * 32;
+            constexpr int VW = N / 2; // values of a matrix per lane (two lanes per right-hand side)
+            PcgState *grp = st + G;
+            if (grp->done)
+                return;
+            extern __shared__ __align__(128) unsigned char smem[];
+            const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+            unsigned char *base = smem + (size_t)w * L::WARP_BYTES;
+            __half *stage0 = reinterpret_cast<__half *>(base);
+            __half *stage1 = reinterpret_cast<__half *>(base + L::STAGE_BYTES);
+            __half *xh = reinterpret_cast<__half *>(base + 2 * L::STAGE_BYTES);
+            __half *xl = xh + G * XS;
+            float *ys = reinterpret_cast<float *>(base + 2 * L::STAGE_BYTES + 4 * G * XS);
+            uint64_t *bar = reinterpret_cast<uint64_t *>(base + 2 * L::STAGE_BYTES + L::XS_BYTES);
+            const __half *__restrict__ inv = static_cast<const __half *>(mas.inv);
+            const int banks = mas.banks;
+            const int items = banks + mas.n_coarse_active;
+            const int total_warps = gridDim.x * WARPS;
+            const int gw = blockIdx.x * WARPS + w;
+            auto mat_of = [&](int m) { return m < banks ? m : banks + mas.coarse_active[m - banks]; };
+            auto in_of = [&](int m) -> const double * {
+                return m < banks ? r + (size_t)m * N * G : mas.rc + (size_t)(mat_of(m) - banks) * N * G;
+            };
+            const uint64_t pol = l2_evict_first_policy();
+            if (lane == 0)
+            {
+                mbar_init(&bar[0], 1);
+                mbar_init(&bar[1], 1);
+                fence_mbar_init();
+            }
+            __syncwarp();
+            if (lane == 0)
+            {
+                if (gw < items)
+                    bulk_load_stream(stage0, inv + (size_t)mat_of(gw) * S, L::STAGE_BYTES, &bar[0], pol);
+                if (gw + total_warps < items)
+                    bulk_load_stream(stage1, inv + (size_t)mat_of(gw + total_warps) * S, L::STAGE_BYTES, &bar[1],
+                                     pol);
+            }
+            bool pending[2] = {gw < items, gw + total_warps < items};
+            const int g = lane & (G - 1), half = lane >> 4;
+            double part[3] = {0.0, 0.0, 0.0}; // this lane's right-hand side: coupled, isolated, coarse
+            uint32_t phase0 = 0, phase1 = 0;
+            bool ok = true;
+            int k = 0;
+            for (int m = gw; m < items; m += total_warps, ++k)
+            {
+                const bool s1 = (k & 1) != 0;
+                __half *stage = s1 ? stage1 : stage0;
+                uint64_t *b = s1 ? &bar[1] : &bar[0];
+                const bool coarse = m >= banks;
+                const int mat = mat_of(m);
+                const double *in = in_of(m);
+                double *out = coarse ? mas.zc + (size_t)(mat - banks) * N * G : z0 + (size_t)m * N * G;
+                double r64[VW];
+#pragma unroll
+                for (int t = 0; t < VW; ++t)
+                    r64[t] = in[(2 * t + half) * G + g];
+                double amax = 0.0;
+#pragma unroll
+                for (int t = 0; t < VW; ++t)
+                    amax = fmax(amax, fabs(r64[t]));
+                amax = fmax(amax, __shfl_xor_sync(FULL, amax, 16));
+                const double xscale = (amax > 0.0 && isfinite(amax)) ? ldexp(1.0, 14 - ilogb(amax)) : 1.0;
+#pragma unroll
+                for (int t = 0; t < VW; ++t)
+                {
+                    const float v = (float)(r64[t] * xscale);
+                    const __half h = __float2half_rn(v);
+                    xh[g * XS + 2 * t + half] = h;
+                    xl[g * XS + 2 * t + half] = __float2half_rn(v - __half2float(h));
+                }
+                __syncwarp();
+                if (!mbar_wait_bounded(b, s1 ? phase1 : phase0, &grp->error, cfg.wait_limit))
+                {
+                    ok = false;
+                    break;
+                }
+                pending[s1 ? 1 : 0] = false;
+                if (s1)
+                    phase1 ^= 1u;
+                else
+                    phase0 ^= 1u;
+                const bool ident = coarse && mas.identity[mat - banks];
+                if (!ident)
+#pragma unroll
+                    for (int nt = 0; nt < G / 4; ++nt)
+                        symv_mma16_g<3, XS, YS>(stage, xh + 4 * nt * XS, xl + 4 * nt * XS, ys + 4 * nt * YS, lane);
+                __syncwarp();
+                const int mn = m + 2 * total_warps;
+                if (mn < items)
+                {
+                    if (lane == 0)
+                    {
+                        fence_proxy_async_smem();
+                        bulk_load_stream(stage, inv + (size_t)mat_of(mn) * S, L::STAGE_BYTES, b, pol);
+                    }
+                    pending[s1 ? 1 : 0] = true;
+                }
+                const double sc = mas.inv_scale[mat] / xscale;
+                double d = 0.0;
+#pragma unroll
+                for (int t = 0; t < VW; ++t)
+                {
+                    const int e = 2 * t + half;
+                    const double zv = ident ? r64[t] : (double)ys[g * YS + e] * sc;
+                    out[e * G + g] = zv;
+                    d = fma(zv, r64[t], d);
+                }
+                if (coarse)
+                    part[2] += d;
+                else if (m >= mas.first_iso_bank)
+                    part[1] += d;
+                else
+                    part[0] += d;
+                __syncwarp();
+            }
+            if (!ok)
+            {
+                if (lane == 0)
+                    mbar_drain(bar, pending, {phase0, phase1});
+                __syncwarp();
+            }
+            // Every warp is past its last stage (no copy in flight): the first warp's area holds the
+            // per-warp sums, the CTA's sums and the totals.
+            __syncthreads();
+            double *wsum = reinterpret_cast<double *>(smem);
+            double *cta = wsum + WARPS * 3 * G, *tot = cta + 3 * G;
+#pragma unroll
+            for (int i = 0; i < 3; ++i)
+                part[i] += __shfl_xor_sync(FULL, part[i], 16);
+            if (lane < G)
+#pragma unroll
+                for (int i = 0; i < 3; ++i)
+                    wsum[w * 3 * G + i * G + lane] = part[i];
+            __syncthreads();
+            if (threadIdx.x < 3 * G)
+            {
+                double s = 0.0;
+                for (int ww = 0; ww < WARPS; ++ww)
+                    s += wsum[ww * 3 * G + threadIdx.x];
+                cta[threadIdx.x] = s;
+            }
+            if (grid_reduce_cta<3 * G, THREADS>(cta, red.rz_parts, &grp->counter[4], tot) && threadIdx.x == 0)
+            {
+                const double Lc = (double)cfg.level_num;
+                int all_done = 1;
+                for (int gg = 0; gg < G; ++gg)
+                {
+                    PcgState *sg = st + gg;
+                    if (!sg->done)
+                    {
+                        sg->rz_coarse = tot[2 * G + gg] + Lc * tot[G + gg];
+                        pcg_finalize(sg, cfg, MODE, tot[gg] + tot[G + gg] + sg->rz_coarse, 0.0);
+                        if (sg->error)
+                            grp->error = sg->error;
+                    }
+                    all_done &= sg->done ? 1 : 0;
+                }
+                grp->iter = MODE == 1 ? 0 : grp->iter + 1;
+                if (all_done || grp->error)
+                    grp->done = 1;
+            }
+        }
+
         // Coarse levels above the first from its components rc (level 0 of the coarse vector).
         // Each real node of level l sums its (at most 32) children of level l - 1 in a warp
         // (lane = child, in increasing order; deterministic). With three or more levels one CTA
@@ -862,6 +1057,110 @@ namespace pmas
                     for (int c = 0; c < BD; ++c)
                         mas.rc[((size_t)mas.coff[3] + k) * BD + c] = v[c];
             }
+            if (threadIdx.x == 0)
+                *mas.ticket = 0u;
+        }
+
+        // The coarse levels for nodes of NC components (the wide groups: 3 components x 16 right-hand
+        // sides), the same sums as k_coarse_levels in chunks of CH components, so the registers do not
+        // grow with NC.
+        template <int NC, int CH>
+        __device__ __forceinline__ void kid_sum_chunk(const MasView &mas, int l, int i, bool cg, int c0,
+                                                      double (&v)[CH])
+        {
+            const int lane = threadIdx.x & 31;
+            const int b = mas.kid_ptr[l][i], e = mas.kid_ptr[l][i + 1];
+#pragma unroll
+            for (int c = 0; c < CH; ++c)
+                v[c] = 0.0;
+            if (b + lane < e)
+            {
+                const size_t node = (size_t)mas.coff[l - 1] + mas.kids[b + lane];
+#pragma unroll
+                for (int c = 0; c < CH; ++c)
+                    v[c] = cg ? __ldcg(mas.rc + node * NC + c0 + c) : mas.rc[node * NC + c0 + c];
+            }
+#pragma unroll
+            for (int c = 0; c < CH; ++c)
+                v[c] = warp_sum(v[c]);
+        }
+
+        template <int NC, int CH>
+        __global__ void __launch_bounds__(LEVEL_THREADS) k_coarse_levels_c(MasView mas, const PcgState *grp)
+        {
+            static_assert(NC % CH == 0, "whole chunks");
+            if (grp && grp->done)
+                return;
+            constexpr int W = LEVEL_THREADS / 32;
+            const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+            __shared__ double part[W][NC];
+            __shared__ int is_last;
+            if (mas.level_num == 2)
+            {
+                const int i = blockIdx.x * W + w;
+                if (i >= mas.real_count[1])
+                    return;
+                for (int c0 = 0; c0 < NC; c0 += CH)
+                {
+                    double v[CH];
+                    kid_sum_chunk<NC, CH>(mas, 1, i, false, c0, v);
+                    if (lane == 0)
+#pragma unroll
+                        for (int c = 0; c < CH; ++c)
+                            mas.rc[((size_t)mas.coff[1] + i) * NC + c0 + c] = v[c];
+                }
+                return;
+            }
+            const int j = blockIdx.x;
+            const int kb = mas.kid_ptr[2][j], ke = mas.kid_ptr[2][j + 1];
+            if (kb + w < ke)
+            {
+                const int i = mas.kids[kb + w];
+                for (int c0 = 0; c0 < NC; c0 += CH)
+                {
+                    double v[CH];
+                    kid_sum_chunk<NC, CH>(mas, 1, i, false, c0, v);
+                    if (lane == 0)
+#pragma unroll
+                        for (int c = 0; c < CH; ++c)
+                        {
+                            mas.rc[((size_t)mas.coff[1] + i) * NC + c0 + c] = v[c];
+                            part[w][c0 + c] = v[c];
+                        }
+                }
+            }
+            __syncthreads();
+            if (w == 0)
+            {
+                for (int c = 0; c < NC; ++c)
+                {
+                    const double t = warp_sum(kb + lane < ke ? part[lane][c] : 0.0);
+                    if (lane == 0)
+                        mas.rc[((size_t)mas.coff[2] + j) * NC + c] = t;
+                }
+            }
+            if (mas.level_num <= 3)
+                return;
+            __syncthreads();
+            if (threadIdx.x == 0)
+            {
+                __threadfence();
+                is_last = atomicAdd(mas.ticket, 1u) == gridDim.x - 1;
+            }
+            __syncthreads();
+            if (!is_last)
+                return;
+            __threadfence();
+            for (int k = w; k < mas.real_count[3]; k += W)
+                for (int c0 = 0; c0 < NC; c0 += CH)
+                {
+                    double v[CH];
+                    kid_sum_chunk<NC, CH>(mas, 3, k, true, c0, v);
+                    if (lane == 0)
+#pragma unroll
+                        for (int c = 0; c < CH; ++c)
+                            mas.rc[((size_t)mas.coff[3] + k) * NC + c0 + c] = v[c];
+                }
             if (threadIdx.x == 0)
                 *mas.ticket = 0u;
         }
@@ -1047,6 +1346,14 @@ namespace pmas
             cuda_check(cudaFuncSetAttribute(k_mas_apply_g<BD, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
                        "apply smem attribute");
         });
+        if (bd == 3)
+        {
+            const int smem = ApplyLayoutW::WARPS * ApplyLayoutW::WARP_BYTES;
+            cuda_check(cudaFuncSetAttribute(k_mas_apply_w<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                       "wide apply smem attribute");
+            cuda_check(cudaFuncSetAttribute(k_mas_apply_w<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                       "wide apply smem attribute");
+        }
     }
 
     void launch_mas_apply_g(const MasView &mas, const double *r, double *z, PcgState *st, ReduceBuf red, PcgConfig cfg,
@@ -1084,6 +1391,39 @@ namespace pmas
         });
         cuda_check(cudaGetLastError(), "multi coarse levels launch");
         return 1;
+    }
+
+    int launch_coarse_levels_w(const MasView &mas, const PcgState *grp, cudaStream_t s)
+    {
+        if (mas.level_num <= 1 || mas.real_count[1] <= 0)
+            return 0;
+        const int grid = mas.level_num == 2 ? (mas.real_count[1] + LEVEL_THREADS / 32 - 1) / (LEVEL_THREADS / 32)
+                                            : mas.real_count[2];
+        if (grid <= 0)
+            return 0;
+        k_coarse_levels_c<3 * RHS_WIDE, 8><<<grid, LEVEL_THREADS, 0, s>>>(mas, grp);
+        cuda_check(cudaGetLastError(), "wide coarse levels launch");
+        return 1;
+    }
+
+    void launch_mas_apply_w(const MasView &mas, const double *r, double *z, PcgState *st, ReduceBuf red,
+                            PcgConfig cfg, int mode, cudaStream_t s)
+    {
+        using L = ApplyLayoutW;
+        if (mas.bd != 3 || mas.storage != STORE_F16)
+            throw Error(ERR_INVALID, "[MAS] sixteen right-hand sides need block_dim 3 and fp16 inverses");
+        const int items = mas.banks + mas.n_coarse_active;
+        int grid = (items + L::WARPS - 1) / L::WARPS;
+        const int sms = device_sm_count();
+        grid = grid > sms ? sms : (grid < 1 ? 1 : grid);
+        if (grid > red.capacity)
+            throw Error(ERR_INVALID, "[MAS] reduction scratch too small");
+        const size_t smem = (size_t)L::WARPS * L::WARP_BYTES;
+        if (mode == 1)
+            k_mas_apply_w<1><<<grid, L::WARPS * 32, smem, s>>>(mas, r, z, st, red, cfg);
+        else
+            k_mas_apply_w<2><<<grid, L::WARPS * 32, smem, s>>>(mas, r, z, st, red, cfg);
+        cuda_check(cudaGetLastError(), "wide apply launch");
     }
 
     void launch_mas_apply(const MasView &mas, const double *r, double *z, PcgState *st, ReduceBuf red, PcgConfig cfg,

@@ -63,6 +63,9 @@ namespace
         // Iterations of each bounded device-side wait before the solve stops with MAS_ERR_TIMEOUT
         // (0: every wait gives up at once -- the test of the timeout path).
         long long wait_limit = MBAR_SPIN_LIMIT_DEFAULT;
+        // Right-hand sides per group of several-right-hand-side solves: 0 = 16 for more than four
+        // right-hand sides with block_dim 3, else 4; or 4 / 16 explicitly.
+        int rhs_group = 0;
     };
 
     const char *status_string(int s)
@@ -111,7 +114,7 @@ namespace
                                 "lazy_partitioning", "use_preconditioned_residual_norm", "precision",
                                 "true_residual_period", "check_period", "initial_guess", "beta", "ordering",
                                 "poll_period", "profile_kernels", "cuda_graphs", "preconditioner_refresh",
-                                "device_wait_limit"};
+                                "device_wait_limit", "rhs_group"};
 
     // MASSolverImpl::set_parameters (MASSolver.cu:198-212) plus the extension keys.
     void apply_mas_params(Params &p, const Json &m, bool strict)
@@ -200,6 +203,12 @@ namespace
             q.preconditioner_refresh = get_int(*v, "preconditioner_refresh");
             if (q.preconditioner_refresh < 1)
                 throw Error(ERR_INVALID, "[MAS] preconditioner_refresh must be >= 1");
+        }
+        if (auto *v = m.find("rhs_group"))
+        {
+            q.rhs_group = get_int(*v, "rhs_group");
+            if (q.rhs_group != 0 && q.rhs_group != RHS_GROUP && q.rhs_group != RHS_WIDE)
+                throw Error(ERR_INVALID, "[MAS] rhs_group must be 0, 4 or 16");
         }
         if (auto *v = m.find("device_wait_limit"))
         {
@@ -656,7 +665,11 @@ struct mas_solver
         preconditioner_current = true;
         prepare_kernels(bd_, p.storage);
         if (p.storage == STORE_F16)
+        {
             prepare_kernels_g(bd_);
+            if (bd_ == 3)
+                prepare_kernels_w();
+        }
         drop_graph();
 
         const size_t len = (size_t)banks * 32 * bd_;
@@ -1224,17 +1237,26 @@ struct mas_solver
         return factorized && mas.storage == STORE_F16 && !p.polak_ribiere && !p.initial_guess_input;
     }
 
-    void alloc_multi()
+    // Group width w (RHS_GROUP or RHS_WIDE) of the several-right-hand-side buffers and kernels.
+    int gwidth = RHS_GROUP;
+    bool wide() const { return gwidth == RHS_WIDE; }
+    int red_capacity_g() const { return wide() ? wide_reduce_ctas() : red_capacity; }
+
+    void alloc_multi(int width = RHS_GROUP)
     {
-        const size_t len = (size_t)banks * 32 * bd * RHS_GROUP;
+        if (width != gwidth)
+            for (DevBuf<double> *v : {&gx, &gb, &gr, &gp, &gz, &gAp, &grc, &gzc, &gio, &gpartials})
+                v->reset(); // other sizes; the captured graphs go with them (their key has the pointers)
+        gwidth = width;
+        const size_t len = (size_t)banks * 32 * bd * width;
         for (DevBuf<double> *v : {&gx, &gb, &gr, &gp, &gz, &gAp})
             v->alloc(len, "device_buffers several right-hand sides");
-        const size_t clen = (size_t)std::max(mas.coarse_nodes, 1) * bd * RHS_GROUP;
+        const size_t clen = (size_t)std::max(mas.coarse_nodes, 1) * bd * width;
         grc.alloc(clen, "MAS coarse_vectors several right-hand sides");
         gzc.alloc(clen, "MAS coarse_vectors several right-hand sides");
-        gio.alloc((size_t)n * RHS_GROUP, "device_buffers several right-hand sides");
-        gpartials.alloc((size_t)red_capacity * 6 * RHS_GROUP, "device_buffers reduction");
-        gst.alloc(RHS_GROUP + 1, "device_buffers state");
+        gio.alloc((size_t)n * width, "device_buffers several right-hand sides");
+        gpartials.alloc((size_t)red_capacity_g() * 6 * width, "device_buffers reduction");
+        gst.alloc(RHS_WIDE + 1, "device_buffers state");
         // Coarse slots past the component counts are read by the coarse products and must be zero.
         cuda_check(cudaMemsetAsync(grc.get(), 0, grc.bytes(), stream), "memset");
         cuda_check(cudaMemsetAsync(gzc.get(), 0, gzc.bytes(), stream), "memset");
@@ -1243,8 +1265,8 @@ struct mas_solver
     ReduceBuf red_g()
     {
         double *base = gpartials.get();
-        const size_t c = (size_t)red_capacity;
-        return ReduceBuf{base, red_capacity, base + 2 * RHS_GROUP * c, base + 3 * RHS_GROUP * c};
+        const size_t c = (size_t)red_capacity_g();
+        return ReduceBuf{base, red_capacity_g(), base + 2 * gwidth * c, base + 3 * gwidth * c};
     }
 
     MasView view_g() const { return mas.view(grc.get(), gzc.get()); }
@@ -1252,7 +1274,25 @@ struct mas_solver
     void launch_iteration_g(const BankedView &Av, const MasView &mv, const PcgConfig &cfg, int P, bool residual)
     {
         PcgState *S = gst.get();
-        PcgState *grp = S + RHS_GROUP;
+        PcgState *grp = S + gwidth;
+        if (wide())
+        {
+            run("spmv_pap", 1,
+                [&] { launch_spmv_w(SPMV_PAP, Av, gp.get(), gAp.get(), nullptr, S, red_g(), 1, 0, stream); });
+            run("update_xr", 1,
+                [&] { launch_update_xr_w(mv, gx.get(), gr.get(), gp.get(), gAp.get(), S, red_g(), P, stream); });
+            if (residual)
+            {
+                run("spmv_residual", 1, [&] {
+                    launch_spmv_w(SPMV_RESIDUAL, Av, gx.get(), gr.get(), gb.get(), S, red_g(), 1, P, stream);
+                });
+                run("restrict", 0, [&] { return launch_restrict_w(mv, gr.get(), grp, P, stream); });
+            }
+            run("coarse_levels", 0, [&] { return launch_coarse_levels_w(mv, grp, stream); });
+            run("mas_apply", 1, [&] { launch_mas_apply_w(mv, gr.get(), gz.get(), S, red_g(), cfg, 2, stream); });
+            run("update_p", 1, [&] { launch_update_p_w(mv, gp.get(), gz.get(), S, 0, stream); });
+            return;
+        }
         run("spmv_pap", 1, [&] { launch_spmv_g(SPMV_PAP, Av, gp.get(), gAp.get(), nullptr, S, red_g(), 1, 0, stream); });
         run("update_xr", 1,
             [&] { launch_update_xr_g(mv, gx.get(), gr.get(), gp.get(), gAp.get(), S, red_g(), P, stream); });
@@ -1316,6 +1356,7 @@ struct mas_solver
         mix((uint64_t)cfg.check_period);
         mix((uint64_t)cfg.use_prec_norm);
         mix((uint64_t)cfg.wait_limit);
+        mix((uint64_t)gwidth);
         uint64_t bits;
         std::memcpy(&bits, &cfg.rel_tol, 8);
         mix(bits);
@@ -1345,22 +1386,35 @@ struct mas_solver
         const BankedView Av = A.view();
         const MasView mv = view_g();
         const PcgConfig cfg = config();
+        const int W = gwidth;
         PcgState *S = gst.get();
-        PcgState hinit[RHS_GROUP + 1];
-        std::memset(hinit, 0, sizeof(hinit));
-        for (int g = cols; g < RHS_GROUP; ++g)
+        std::vector<PcgState> hinit((size_t)W + 1), hs((size_t)W + 1);
+        std::memset(hinit.data(), 0, sizeof(PcgState) * hinit.size());
+        for (int g = cols; g < W; ++g)
             hinit[g].done = 1;
-        cuda_check(cudaMemcpyAsync(S, hinit, sizeof(hinit), cudaMemcpyHostToDevice, stream), "state");
-        run("spmv_residual", 1,
-            [&] { launch_spmv_g(SPMV_RESIDUAL, Av, gx.get(), gr.get(), gb.get(), S, red_g(), 0, 0, stream); });
-        run("restrict", 0, [&] { return launch_restrict_g(mv, gr.get(), S + RHS_GROUP, 0, stream); });
-        run("coarse_levels", 0, [&] { return launch_coarse_levels_g(mv, stream); });
-        run("mas_apply", 1, [&] { launch_mas_apply_g(mv, gr.get(), gz.get(), S, red_g(), cfg, 1, stream); });
-        run("update_p", 1, [&] { launch_update_p_g(mv, gp.get(), gz.get(), S, 1, stream); });
-        PcgState hs[RHS_GROUP + 1];
-        cuda_check(cudaMemcpyAsync(hs, S, sizeof(hs), cudaMemcpyDeviceToHost, stream), "state");
+        cuda_check(cudaMemcpyAsync(S, hinit.data(), sizeof(PcgState) * (W + 1), cudaMemcpyHostToDevice, stream),
+                   "state");
+        if (wide())
+        {
+            run("spmv_residual", 1,
+                [&] { launch_spmv_w(SPMV_RESIDUAL, Av, gx.get(), gr.get(), gb.get(), S, red_g(), 0, 0, stream); });
+            run("restrict", 0, [&] { return launch_restrict_w(mv, gr.get(), S + W, 0, stream); });
+            run("coarse_levels", 0, [&] { return launch_coarse_levels_w(mv, S + W, stream); });
+            run("mas_apply", 1, [&] { launch_mas_apply_w(mv, gr.get(), gz.get(), S, red_g(), cfg, 1, stream); });
+            run("update_p", 1, [&] { launch_update_p_w(mv, gp.get(), gz.get(), S, 1, stream); });
+        }
+        else
+        {
+            run("spmv_residual", 1,
+                [&] { launch_spmv_g(SPMV_RESIDUAL, Av, gx.get(), gr.get(), gb.get(), S, red_g(), 0, 0, stream); });
+            run("restrict", 0, [&] { return launch_restrict_g(mv, gr.get(), S + W, 0, stream); });
+            run("coarse_levels", 0, [&] { return launch_coarse_levels_g(mv, stream); });
+            run("mas_apply", 1, [&] { launch_mas_apply_g(mv, gr.get(), gz.get(), S, red_g(), cfg, 1, stream); });
+            run("update_p", 1, [&] { launch_update_p_g(mv, gp.get(), gz.get(), S, 1, stream); });
+        }
+        cuda_check(cudaMemcpyAsync(hs.data(), S, sizeof(PcgState) * (W + 1), cudaMemcpyDeviceToHost, stream), "state");
         cuda_check(cudaStreamSynchronize(stream), "pcg init");
-        if (hs[RHS_GROUP].error == ERR_TIMEOUT)
+        if (hs[W].error == ERR_TIMEOUT)
             throw Error(ERR_TIMEOUT, "[MAS] a device-side wait timed out.");
         for (int g = 0; g < cols; ++g)
             if (hs[g].error == ERR_NONFINITE || std::isnan(hs[g].rz0) || !std::isfinite(hs[g].rz0))
@@ -1386,16 +1440,14 @@ struct mas_solver
             else
                 for (int k = k0; k <= k1; ++k)
                     launch_iteration_g(Av, mv, cfg, P, k % P == 0);
-            cuda_check(cudaMemcpyAsync(&hs[RHS_GROUP], S + RHS_GROUP, sizeof(PcgState), cudaMemcpyDeviceToHost,
-                                       stream),
-                       "state");
+            cuda_check(cudaMemcpyAsync(&hs[W], S + W, sizeof(PcgState), cudaMemcpyDeviceToHost, stream), "state");
             cuda_check(cudaStreamSynchronize(stream), "chunk");
-            if (hs[RHS_GROUP].done)
+            if (hs[W].done)
                 break;
         }
-        cuda_check(cudaMemcpyAsync(hs, S, sizeof(hs), cudaMemcpyDeviceToHost, stream), "state");
+        cuda_check(cudaMemcpyAsync(hs.data(), S, sizeof(PcgState) * (W + 1), cudaMemcpyDeviceToHost, stream), "state");
         cuda_check(cudaStreamSynchronize(stream), "pcg");
-        if (hs[RHS_GROUP].error == ERR_TIMEOUT)
+        if (hs[W].error == ERR_TIMEOUT)
             throw Error(ERR_TIMEOUT, "[MAS] a device-side wait timed out.");
         for (int g = 0; g < cols; ++g)
         {
@@ -1405,7 +1457,18 @@ struct mas_solver
         }
     }
 
-    // Column-major B (n x nrhs) -> X; groups of RHS_GROUP share every matrix and inverse read.
+    // Group width of a several-right-hand-side solve (the rhs_group parameter; automatic: sixteen
+    // for more than four right-hand sides with block_dim 3).
+    int group_width(int nrhs) const
+    {
+        if (p.rhs_group == RHS_WIDE && bd == 3)
+            return RHS_WIDE;
+        if (p.rhs_group == 0 && bd == 3 && nrhs > RHS_GROUP)
+            return RHS_WIDE;
+        return RHS_GROUP;
+    }
+
+    // Column-major B (n x nrhs) -> X; each group of right-hand sides shares every matrix and inverse read.
     void solve_multi(const double *hB, double *hX, int len, int nrhs)
     {
         cuda_check(cudaSetDevice(device), "set device");
@@ -1427,26 +1490,35 @@ struct mas_solver
             in_multi = false;
             return;
         }
-        alloc_multi();
+        const int W = group_width(nrhs);
+        alloc_multi(W);
         for (auto &ks : kstats)
             ks.second = KStat{};
         rhs_iterations.clear();
         rhs_status.clear();
         rhs_error.clear();
-        const size_t glen = (size_t)banks * 32 * bd * RHS_GROUP;
+        const size_t glen = (size_t)banks * 32 * bd * W;
         auto t0 = std::chrono::steady_clock::now();
-        for (int c0 = 0; c0 < nrhs; c0 += RHS_GROUP)
+        for (int c0 = 0; c0 < nrhs; c0 += W)
         {
-            const int cols = std::min(RHS_GROUP, nrhs - c0);
+            const int cols = std::min(W, nrhs - c0);
             cuda_check(cudaMemcpyAsync(gio.get(), hB + (size_t)c0 * n, sizeof(double) * (size_t)n * cols,
                                        cudaMemcpyHostToDevice, stream),
                        "upload B");
-            run("permute_in", 2,
-                [&] { launch_permute_in_g(n, bd, V, cols, d_padded.get(), gio.get(), gb.get(), glen, stream); });
+            run("permute_in", 2, [&] {
+                if (wide())
+                    launch_permute_in_w(n, V, cols, d_padded.get(), gio.get(), gb.get(), glen, stream);
+                else
+                    launch_permute_in_g(n, bd, V, cols, d_padded.get(), gio.get(), gb.get(), glen, stream);
+            });
             cuda_check(cudaMemsetAsync(gx.get(), 0, gx.bytes(), stream), "memset");
             pcg_multi(cols);
-            run("permute_out", 1,
-                [&] { launch_permute_out_g(n, bd, cols, d_padded.get(), gx.get(), gio.get(), stream); });
+            run("permute_out", 1, [&] {
+                if (wide())
+                    launch_permute_out_w(n, cols, d_padded.get(), gx.get(), gio.get(), stream);
+                else
+                    launch_permute_out_g(n, bd, cols, d_padded.get(), gx.get(), gio.get(), stream);
+            });
             cuda_check(cudaMemcpyAsync(hX + (size_t)c0 * n, gio.get(), sizeof(double) * (size_t)n * cols,
                                        cudaMemcpyDeviceToHost, stream),
                        "download X");

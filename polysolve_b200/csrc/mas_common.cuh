@@ -147,6 +147,52 @@ namespace pmas
         return true;
     }
 
+    // Deterministic grid-wide sum of NV values per CTA already summed into shared memory (vals, NV
+    // doubles, written before the call by the CTA; every thread must call it). Each CTA writes its
+    // row of partials; the last CTA to arrive (atomic ticket) sums the rows in a fixed order: THREADS /
+    // NV thread groups take strided subsets of the CTAs, then thread i adds the groups' sums of value i
+    // in group order. Returns true in the last CTA, with tot (shared memory, NV doubles) filled.
+    template <int NV, int THREADS>
+    __device__ __forceinline__ bool grid_reduce_cta(const double *vals, double *partials, unsigned *counter,
+                                                    double *tot)
+    {
+        static_assert(NV <= THREADS, "one thread per value at least");
+        constexpr int GROUPS = THREADS / NV;
+        __shared__ double gsum[GROUPS][NV];
+        __shared__ int is_last;
+        __syncthreads();
+        for (int i = threadIdx.x; i < NV; i += THREADS)
+            partials[(size_t)blockIdx.x * NV + i] = vals[i];
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0)
+            is_last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+        __syncthreads();
+        if (!is_last)
+            return false;
+        __threadfence();
+        const int i = threadIdx.x % NV, grp = threadIdx.x / NV;
+        if (grp < GROUPS)
+        {
+            double s = 0.0;
+            for (int c = grp; c < (int)gridDim.x; c += GROUPS)
+                s += __ldcg(partials + (size_t)c * NV + i);
+            gsum[grp][i] = s;
+        }
+        __syncthreads();
+        if (threadIdx.x < NV)
+        {
+            double t = 0.0;
+            for (int g = 0; g < GROUPS; ++g)
+                t += gsum[g][threadIdx.x];
+            tot[threadIdx.x] = t;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+            *counter = 0u;
+        return true;
+    }
+
     // Sum of a per-lane value over the lanes whose key equals each distinct key of the warp,
     // written by lane 0 of each group to out[(base + key) * BD + i]. Keys < 0 are skipped.
     // Order of additions is fixed (xor butterfly), so results are deterministic.

@@ -386,6 +386,27 @@ namespace pmas
                              size_t dst_len, cudaStream_t s);
     void launch_permute_out_g(int n, int bd, int cols, const int *padded_of_block, const double *src, double *X,
                               cudaStream_t s);
+    // The same group kernels for RHS_WIDE right-hand sides (block size 3, binary16 inverses only):
+    // mas_multi16.cu (SpMV, vector updates, restriction, permutations) and mas_apply.cu (coarse levels,
+    // MAS apply). Vectors interleaved as above with G = RHS_WIDE; state array of RHS_WIDE + 1 entries.
+    // Reductions: red.partials holds 2 RHS_WIDE, red.rr_parts RHS_WIDE and red.rz_parts 3 RHS_WIDE
+    // values per CTA of wide_reduce_ctas() CTAs at most.
+    constexpr int RHS_WIDE = 16;
+    int wide_reduce_ctas();
+    void launch_spmv_w(int mode, const BankedView &A, const double *x, double *y, const double *b, PcgState *st,
+                       ReduceBuf red, int iter, int period, cudaStream_t s);
+    void launch_update_xr_w(const MasView &mas, double *x, double *r, const double *p, const double *Ap,
+                            PcgState *st, ReduceBuf red, int period, cudaStream_t s);
+    void launch_update_p_w(const MasView &mas, double *p, const double *z0, PcgState *st, int first, cudaStream_t s);
+    int launch_restrict_w(const MasView &mas, const double *r, const PcgState *grp, int period, cudaStream_t s);
+    int launch_coarse_levels_w(const MasView &mas, const PcgState *grp, cudaStream_t s);
+    void launch_mas_apply_w(const MasView &mas, const double *r, double *z0, PcgState *st, ReduceBuf red,
+                            PcgConfig cfg, int mode, cudaStream_t s);
+    void launch_permute_in_w(int n, int V, int cols, const int *padded_of_block, const double *B, double *dst,
+                             size_t dst_len, cudaStream_t s);
+    void launch_permute_out_w(int n, int cols, const int *padded_of_block, const double *src, double *X,
+                              cudaStream_t s);
+    void prepare_kernels_w();
     // Set kernel attributes (large shared memory) for every variant used with this block size and
     // precision, so launches inside a CUDA graph capture never touch function attributes.
     void prepare_kernels(int bd, int storage);

@@ -106,10 +106,11 @@ def test_device_wait_timeout_is_reported_and_handle_recovers(precision, graphs):
     np.testing.assert_array_equal(x, x_ref)
 
 
-def test_device_wait_timeout_several_right_hand_sides():
+@pytest.mark.parametrize("group", [4, 16])
+def test_device_wait_timeout_several_right_hand_sides(group):
     system = synthetic.elasticity(8, young_sigma=1.0, jitter=0.2, seed=52)
     B = synthetic.rhs(system.n, seed=52, count=4)
-    params = {"precision": "fp16", "check_period": 1, "true_residual_period": 50}
+    params = {"precision": "fp16", "check_period": 1, "true_residual_period": 50, "rhs_group": group}
     s = _solver(system, params)
     s.factorize(system.scipy())
     X_ref = s.solve_multi(B)

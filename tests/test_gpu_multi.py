@@ -1,6 +1,7 @@
-"""Several right-hand sides at once (`mas_solve_multi`): groups of four independent PCG solves
-that share every read of the matrix and of the binary16 MAS inverses, against one-at-a-time
-solves and the CPU oracle."""
+"""Several right-hand sides at once (`mas_solve_multi`): groups of four or sixteen independent PCG
+solves that share every read of the matrix and of the binary16 MAS inverses, against one-at-a-time
+solves and the CPU oracle. The group width is the ``rhs_group`` parameter (automatic: sixteen for
+more than four right-hand sides with block_dim 3)."""
 
 from __future__ import annotations
 
@@ -33,10 +34,10 @@ def contact_system():
                                 contact_sigma=1.5)
 
 
-@pytest.mark.parametrize("nrhs", [1, 4, 6])
-def test_multi_matches_single_solves_and_oracle(contact_system, nrhs):
+@pytest.mark.parametrize("group,nrhs", [(4, 1), (4, 4), (4, 6), (16, 1), (16, 6), (16, 16), (0, 17)])
+def test_multi_matches_single_solves_and_oracle(contact_system, group, nrhs):
     system = contact_system
-    s = _solver(system, CHOSEN)
+    s = _solver(system, dict(CHOSEN, rhs_group=group))
     A = system.scipy()
     B = np.stack([synthetic.rhs(system.n, seed=40 + c) for c in range(nrhs)])
     X = s.solve_multi(B)
@@ -59,16 +60,17 @@ def test_multi_matches_single_solves_and_oracle(contact_system, nrhs):
         assert np.linalg.norm(X[c] - xo) <= 1e-5 * np.linalg.norm(xo)
 
 
-def test_multi_repeatable_and_graph_free_equal(contact_system):
+@pytest.mark.parametrize("group", [4, 16])
+def test_multi_repeatable_and_graph_free_equal(contact_system, group):
     """Deterministic: the same block of right-hand sides twice gives identical results, with and
     without graph replay of the iterations."""
     system = contact_system
     B = np.stack([synthetic.rhs(system.n, seed=70 + c) for c in range(5)])
-    s = _solver(system, CHOSEN)
+    s = _solver(system, dict(CHOSEN, rhs_group=group))
     X1 = s.solve_multi(B)
     X2 = s.solve_multi(B)
     np.testing.assert_array_equal(X1, X2)
-    s2 = _solver(system, dict(CHOSEN, cuda_graphs=False))
+    s2 = _solver(system, dict(CHOSEN, cuda_graphs=False, rhs_group=group))
     X3 = s2.solve_multi(B)
     np.testing.assert_array_equal(X1, X3)
 
@@ -85,11 +87,34 @@ def test_multi_falls_back_to_single_solves_without_fp16(contact_system):
         np.testing.assert_array_equal(X[c], x1)
 
 
-def test_multi_max_iterations(contact_system):
+@pytest.mark.parametrize("group", [4, 16])
+def test_multi_max_iterations(contact_system, group):
     system = contact_system
-    s = _solver(system, dict(CHOSEN, max_iter=7))
+    s = _solver(system, dict(CHOSEN, max_iter=7, rhs_group=group))
     B = np.stack([synthetic.rhs(system.n, seed=3 + c) for c in range(4)])
     s.solve_multi(B)
     info = s.get_info({})
     assert info["rhs_iterations"] == [7, 7, 7, 7]
     assert all(st == "Reach max iterations" for st in info["rhs_status"])
+
+
+def test_wide_and_narrow_groups_agree(contact_system):
+    """Groups of sixteen and of four are the same algorithm per right-hand side (the sums run in
+    another order): every column within 1e-6 and iteration counts within two."""
+    system = contact_system
+    B = np.stack([synthetic.rhs(system.n, seed=120 + c) for c in range(12)])
+    s4 = _solver(system, dict(CHOSEN, rhs_group=4))
+    s16 = _solver(system, dict(CHOSEN, rhs_group=16))
+    X4, X16 = s4.solve_multi(B), s16.solve_multi(B)
+    i4, i16 = s4.get_info()["rhs_iterations"], s16.get_info()["rhs_iterations"]
+    for c in range(12):
+        assert np.linalg.norm(X16[c] - X4[c]) <= 1e-6 * np.linalg.norm(X4[c])
+        assert abs(i4[c] - i16[c]) <= 2
+
+
+def test_rhs_group_is_validated():
+    from polysolve_b200 import MasError
+
+    s = Solver.create("MAS", "")
+    with pytest.raises(MasError):
+        s.set_parameters({"MAS": {"rhs_group": 8}})
