@@ -1130,14 +1130,12 @@ namespace pmas
                 }
             }
             __syncthreads();
-            if (w == 0)
+            // The level-2 node's components, one per warp (in the same order as one warp would sum them).
+            for (int c = w; c < NC; c += W)
             {
-                for (int c = 0; c < NC; ++c)
-                {
-                    const double t = warp_sum(kb + lane < ke ? part[lane][c] : 0.0);
-                    if (lane == 0)
-                        mas.rc[((size_t)mas.coff[2] + j) * NC + c] = t;
-                }
+                const double t = warp_sum(kb + lane < ke ? part[lane][c] : 0.0);
+                if (lane == 0)
+                    mas.rc[((size_t)mas.coff[2] + j) * NC + c] = t;
             }
             if (mas.level_num <= 3)
                 return;

@@ -1416,6 +1416,8 @@ struct mas_solver
         cuda_check(cudaStreamSynchronize(stream), "pcg init");
         if (hs[W].error == ERR_TIMEOUT)
             throw Error(ERR_TIMEOUT, "[MAS] a device-side wait timed out.");
+        if (hs[W].error == ERR_CUDA)
+            throw Error(ERR_CUDA, "[MAS] a kernel's self-check rejected a memory access.");
         for (int g = 0; g < cols; ++g)
             if (hs[g].error == ERR_NONFINITE || std::isnan(hs[g].rz0) || !std::isfinite(hs[g].rz0))
                 throw Error(ERR_NONFINITE, "[MAS] Invalid initial residual.");
@@ -1449,6 +1451,8 @@ struct mas_solver
         cuda_check(cudaStreamSynchronize(stream), "pcg");
         if (hs[W].error == ERR_TIMEOUT)
             throw Error(ERR_TIMEOUT, "[MAS] a device-side wait timed out.");
+        if (hs[W].error == ERR_CUDA)
+            throw Error(ERR_CUDA, "[MAS] a kernel's self-check rejected a memory access.");
         for (int g = 0; g < cols; ++g)
         {
             rhs_iterations.push_back(hs[g].iter);

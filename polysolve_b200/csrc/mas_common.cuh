@@ -333,6 +333,31 @@ namespace pmas
         return v;
     }
 
+    // Asynchronous global -> shared copies (cp.async, completion tracked per thread by commit / wait
+    // groups): 16 bytes cached in L1 and L2 (.ca) or in L2 only (.cg), and 8 bytes (.ca).
+    __device__ __forceinline__ void cp_async16_ca(void *dst, const void *src)
+    {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+    }
+
+    __device__ __forceinline__ void cp_async16_cg(void *dst, const void *src)
+    {
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+    }
+
+    __device__ __forceinline__ void cp_async8_ca(void *dst, const void *src)
+    {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+    }
+
+    __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+    template <int N>
+    __device__ __forceinline__ void cp_async_wait()
+    {
+        asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+    }
+
     __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     {
         uint32_t ok;

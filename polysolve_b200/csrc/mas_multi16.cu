@@ -39,11 +39,29 @@ namespace pmas
         static_assert(G == 16, "the lane mappings below assume 16 right-hand sides");
 
         // ---- SpMV: y = A x (PAP: p.Ap, alpha) or y = b - A x (RESIDUAL: r.r, b.b) ------------
+        // Slots (stored blocks) of the warp's four rows go through a ring of SP_STAGES shared-memory
+        // stages filled by cp.async SP_STAGES - 1 slots ahead: each lane copies the three 16-byte x
+        // pieces it multiplies (x[col][j][2 gq .. 2 gq + 1]) and lanes 0-4 of each row the block's
+        // values (four 16-byte pairs, one 8-byte value). The copies need no registers, so a warp keeps
+        // five slots of gathers in flight; the columns come from registers loaded at the bank's start
+        // (slots gq + 8 i of the row in lane gq's register i, up to SP_MAXLEN slots; longer rows take
+        // the plain loop).
+        constexpr int SP_STAGES = 6;
+        constexpr int SP_XB = 32 * 3 * 16;       // x pieces of the 32 lanes
+        constexpr int SP_MB = 4 * 5 * 16;        // block values of the four rows
+        constexpr int SP_SB = SP_XB + SP_MB;     // one stage
+        constexpr int SP_WARP = SP_STAGES * SP_SB;
+        constexpr int SP_SMEM = WW * SP_WARP;
+        constexpr int SP_REGS = 8;
+        constexpr int SP_MAXLEN = 8 * SP_REGS;
+        static_assert(SP_SB % 16 == 0, "16-byte aligned stages");
+
         template <int MODE>
         __global__ void __launch_bounds__(WT_) k_spmv_w(BankedView A, const double *__restrict__ x,
                                                         double *__restrict__ y, const double *__restrict__ b,
                                                         PcgState *st, ReduceBuf red, int iter, int period)
         {
+            extern __shared__ __align__(16) unsigned char sp_smem[];
             PcgState *grp = st + G;
             if (grp->done)
                 return;
@@ -53,6 +71,8 @@ namespace pmas
             const int rs = lane >> 3, gq = lane & 7; // row of the warp's four, pair of right-hand sides
             const int rb = w * 4 + rs;               // row within the bank
             const uint64_t pol = l2_evict_first_policy();
+            unsigned char *wbase = sp_smem + (size_t)w * SP_WARP;
+            const long long nodes = (long long)A.banks * 32;
             double part[2] = {0.0, 0.0}, bb[2] = {0.0, 0.0};
             for (int bank = blockIdx.x; bank < A.banks; bank += gridDim.x)
             {
@@ -65,43 +85,128 @@ namespace pmas
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
                     acc[i][0] = acc[i][1] = 0.0;
-                for (int k = 0; k < maxlen; ++k)
+                if (maxlen <= SP_MAXLEN)
                 {
-                    double v[9];
-                    long long col = u;
-                    if (k < len)
-                    {
-                        const long long slot = s0 + k;
-                        col = ld_stream_s32(A.cols + slot * 32 + rb, pol);
-                        const double *blk = A.vals + slot * 32 * 9;
+                    int colr[SP_REGS];
 #pragma unroll
-                        for (int q = 0; q < 4; ++q)
+                    for (int i = 0; i < SP_REGS; ++i)
+                    {
+                        const int sl = gq + 8 * i;
+                        colr[i] = sl < len ? ld_stream_s32(A.cols + (s0 + sl) * 32 + rb, pol) : (int)u;
+                    }
+                    // Copies of slot sl (warp-uniform) into its stage.
+                    auto issue = [&](int sl) {
+                        int reg = colr[0];
+#pragma unroll
+                        for (int i = 1; i < SP_REGS; ++i)
+                            if ((sl >> 3) == i)
+                                reg = colr[i];
+                        const long long col = __shfl_sync(FULL, reg, (lane & ~7) | (sl & 7));
+                        if (sl < len)
                         {
-                            const double2 t = ld_stream_f64x2(blk + q * 64 + rb * 2, pol);
-                            v[2 * q] = t.x;
-                            v[2 * q + 1] = t.y;
+                            unsigned char *sp = wbase + (sl % SP_STAGES) * SP_SB;
+                            const double *blk = A.vals + (s0 + sl) * 32 * 9;
+                            const double *xs = x + (col * 3) * G + 2 * gq;
+                            // Self-check of every copy's source (column range, 16-byte alignment):
+                            // a bad one is recorded in the group's error word and skipped.
+                            const bool bad = col < 0 || col >= nodes ||
+                                             ((reinterpret_cast<uintptr_t>(xs) | reinterpret_cast<uintptr_t>(blk) |
+                                               reinterpret_cast<uintptr_t>(sp)) & 15) != 0;
+                            if (bad)
+                                atomicExch(&grp->error, ERR_CUDA);
+                            else
+                            {
+#pragma unroll
+                                for (int j = 0; j < 3; ++j)
+                                    cp_async16_ca(sp + (lane * 3 + j) * 16, xs + j * G);
+                                if (gq < 4)
+                                    cp_async16_cg(sp + SP_XB + (rs * 5 + gq) * 16, blk + gq * 64 + rb * 2);
+                                else if (gq == 4)
+                                    cp_async8_ca(sp + SP_XB + (rs * 5 + 4) * 16, blk + 256 + rb);
+                            }
                         }
-                        v[8] = ld_stream_f64(blk + 256 + rb, pol);
-                    }
-                    else
+                    };
+#pragma unroll
+                    for (int d = 0; d < SP_STAGES - 1; ++d)
                     {
-#pragma unroll
-                        for (int q = 0; q < 9; ++q)
-                            v[q] = 0.0;
+                        if (d < maxlen)
+                            issue(d);
+                        cp_async_commit();
                     }
-#pragma unroll
-                    for (int j = 0; j < 3; ++j)
+                    for (int k = 0; k < maxlen; ++k)
                     {
-                        const double2 xv =
-                            __ldg(reinterpret_cast<const double2 *>(x + (col * 3 + j) * G + 2 * gq));
-#pragma unroll
-                        for (int i = 0; i < 3; ++i)
+                        if (k + SP_STAGES - 1 < maxlen)
+                            issue(k + SP_STAGES - 1);
+                        cp_async_commit();
+                        cp_async_wait<SP_STAGES - 1>();
+                        __syncwarp();
+                        if (k < len)
                         {
-                            acc[i][0] = fma(v[i * 3 + j], xv.x, acc[i][0]);
-                            acc[i][1] = fma(v[i * 3 + j], xv.y, acc[i][1]);
+                            const unsigned char *sp = wbase + (k % SP_STAGES) * SP_SB;
+                            const double *mv = reinterpret_cast<const double *>(sp + SP_XB + rs * 80);
+                            double v[9];
+#pragma unroll
+                            for (int q = 0; q < 4; ++q)
+                            {
+                                const double2 t = *reinterpret_cast<const double2 *>(mv + 2 * q);
+                                v[2 * q] = t.x;
+                                v[2 * q + 1] = t.y;
+                            }
+                            v[8] = mv[8];
+#pragma unroll
+                            for (int j = 0; j < 3; ++j)
+                            {
+                                const double2 xv = *reinterpret_cast<const double2 *>(sp + (lane * 3 + j) * 16);
+#pragma unroll
+                                for (int i = 0; i < 3; ++i)
+                                {
+                                    acc[i][0] = fma(v[i * 3 + j], xv.x, acc[i][0]);
+                                    acc[i][1] = fma(v[i * 3 + j], xv.y, acc[i][1]);
+                                }
+                            }
                         }
+                        __syncwarp();
                     }
+                    cp_async_wait<0>();
                 }
+                else
+                    for (int k = 0; k < maxlen; ++k)
+                    {
+                        double v[9];
+                        long long col = u;
+                        if (k < len)
+                        {
+                            const long long slot = s0 + k;
+                            col = ld_stream_s32(A.cols + slot * 32 + rb, pol);
+                            const double *blk = A.vals + slot * 32 * 9;
+#pragma unroll
+                            for (int q = 0; q < 4; ++q)
+                            {
+                                const double2 t = ld_stream_f64x2(blk + q * 64 + rb * 2, pol);
+                                v[2 * q] = t.x;
+                                v[2 * q + 1] = t.y;
+                            }
+                            v[8] = ld_stream_f64(blk + 256 + rb, pol);
+                        }
+                        else
+                        {
+#pragma unroll
+                            for (int q = 0; q < 9; ++q)
+                                v[q] = 0.0;
+                        }
+#pragma unroll
+                        for (int j = 0; j < 3; ++j)
+                        {
+                            const double2 xv =
+                                __ldg(reinterpret_cast<const double2 *>(x + (col * 3 + j) * G + 2 * gq));
+#pragma unroll
+                            for (int i = 0; i < 3; ++i)
+                            {
+                                acc[i][0] = fma(v[i * 3 + j], xv.x, acc[i][0]);
+                                acc[i][1] = fma(v[i * 3 + j], xv.y, acc[i][1]);
+                            }
+                        }
+                    }
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
                 {
@@ -441,6 +546,10 @@ namespace pmas
 
     void prepare_kernels_w()
     {
+        cuda_check(cudaFuncSetAttribute(k_spmv_w<SPMV_PAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, SP_SMEM),
+                   "wide spmv smem attribute");
+        cuda_check(cudaFuncSetAttribute(k_spmv_w<SPMV_RESIDUAL>, cudaFuncAttributeMaxDynamicSharedMemorySize, SP_SMEM),
+                   "wide spmv smem attribute");
         cuda_check(cudaFuncSetAttribute(k_update_xr_w, cudaFuncAttributeMaxDynamicSharedMemorySize, XR_SMEM),
                    "wide update smem attribute");
         cuda_check(cudaFuncSetAttribute(k_restrict_w, cudaFuncAttributeMaxDynamicSharedMemorySize, XR_SMEM),
@@ -455,9 +564,9 @@ namespace pmas
         if (A.banks == 0)
             return;
         auto go = [&](auto kernel) {
-            int grid = resident_per_sm(kernel, 0) * device_sm_count();
+            int grid = resident_per_sm(kernel, SP_SMEM) * device_sm_count();
             grid = std::min({grid, A.banks, red.capacity});
-            kernel<<<grid, WT_, 0, s>>>(A, x, y, b, st, red, iter, period);
+            kernel<<<grid, WT_, SP_SMEM, s>>>(A, x, y, b, st, red, iter, period);
         };
         if (mode == SPMV_PAP)
             go(k_spmv_w<SPMV_PAP>);
