@@ -618,7 +618,6 @@ struct mas_solver
                 A.scatter.reset();
                 build_banked(A, n_, nnz_, d_outer.get(), d_inner.get(), d_vals.get(), bd_, V_, banks, d_padded.get(),
                              stream);
-                wu_valid = false;
             }
             cuda_check(cudaStreamSynchronize(stream), "matrix upload");
             phase("matrix_upload");
@@ -1238,25 +1237,6 @@ struct mas_solver
         return factorized && mas.storage == STORE_F16 && !p.polak_ribiere && !p.initial_guess_input;
     }
 
-    // The distinct columns of every bank for the sixteen-wide SpMV (built at its first use after a
-    // factorization that built the banked matrix).
-    DevBuf<int> wu_cols, wu_count;
-    DevBuf<uint16_t> wu_lidx;
-    bool wu_valid = false;
-    WideCols wide_cols()
-    {
-        if (!wu_valid)
-        {
-            const size_t entries = (size_t)std::max<long long>(A.slots, 1) * 32;
-            wu_cols.alloc(entries, "device_buffers bank columns");
-            wu_lidx.alloc(entries, "device_buffers bank columns");
-            wu_count.alloc(std::max(banks, 1), "device_buffers bank columns");
-            launch_bank_unique(A.view(), wu_cols.get(), wu_lidx.get(), wu_count.get(), stream);
-            wu_valid = true;
-        }
-        return WideCols{wu_cols.get(), wu_lidx.get(), wu_count.get()};
-    }
-
     // Group width w (RHS_GROUP or RHS_WIDE) of the several-right-hand-side buffers and kernels.
     int gwidth = RHS_GROUP;
     bool wide() const { return gwidth == RHS_WIDE; }
@@ -1298,13 +1278,13 @@ struct mas_solver
         if (wide())
         {
             run("spmv_pap", 1,
-                [&] { launch_spmv_w(SPMV_PAP, Av, wide_cols(), gp.get(), gAp.get(), nullptr, S, red_g(), 1, 0, stream); });
+                [&] { launch_spmv_w(SPMV_PAP, Av, gp.get(), gAp.get(), nullptr, S, red_g(), 1, 0, stream); });
             run("update_xr", 1,
                 [&] { launch_update_xr_w(mv, gx.get(), gr.get(), gp.get(), gAp.get(), S, red_g(), P, stream); });
             if (residual)
             {
                 run("spmv_residual", 1, [&] {
-                    launch_spmv_w(SPMV_RESIDUAL, Av, wide_cols(), gx.get(), gr.get(), gb.get(), S, red_g(), 1, P, stream);
+                    launch_spmv_w(SPMV_RESIDUAL, Av, gx.get(), gr.get(), gb.get(), S, red_g(), 1, P, stream);
                 });
                 run("restrict", 0, [&] { return launch_restrict_w(mv, gr.get(), grp, P, stream); });
             }
@@ -1370,8 +1350,7 @@ struct mas_solver
         for (const void *ptr : {(const void *)gx.get(), (const void *)gb.get(), (const void *)gr.get(),
                                 (const void *)gp.get(), (const void *)gz.get(), (const void *)gAp.get(),
                                 (const void *)gst.get(), (const void *)gpartials.get(), (const void *)grc.get(),
-                                (const void *)Av.vals, mv.inv, (const void *)stream, (const void *)wu_cols.get(),
-                                (const void *)wu_lidx.get()})
+                                (const void *)Av.vals, mv.inv, (const void *)stream})
             mix((uint64_t)(uintptr_t)ptr);
         mix((uint64_t)cfg.max_iter);
         mix((uint64_t)cfg.check_period);
@@ -1418,7 +1397,7 @@ struct mas_solver
         if (wide())
         {
             run("spmv_residual", 1,
-                [&] { launch_spmv_w(SPMV_RESIDUAL, Av, wide_cols(), gx.get(), gr.get(), gb.get(), S, red_g(), 0, 0, stream); });
+                [&] { launch_spmv_w(SPMV_RESIDUAL, Av, gx.get(), gr.get(), gb.get(), S, red_g(), 0, 0, stream); });
             run("restrict", 0, [&] { return launch_restrict_w(mv, gr.get(), S + W, 0, stream); });
             run("coarse_levels", 0, [&] { return launch_coarse_levels_w(mv, S + W, stream); });
             run("mas_apply", 1, [&] { launch_mas_apply_w(mv, gr.get(), gz.get(), S, red_g(), cfg, 1, stream); });

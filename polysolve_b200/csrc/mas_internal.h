@@ -393,18 +393,8 @@ namespace pmas
     // values per CTA of wide_reduce_ctas() CTAs at most.
     constexpr int RHS_WIDE = 16;
     int wide_reduce_ctas();
-    // The distinct columns of every bank (at ucols[slice[bank] * 32 ..], ucount[bank] of them, -1
-    // for banks wider than 64 slots) and, per stored block, its column's index among them (lidx, in
-    // the layout of cols). Built once per pattern for the sixteen-wide SpMV.
-    struct WideCols
-    {
-        const int *ucols;
-        const uint16_t *lidx;
-        const int *ucount;
-    };
-    void launch_bank_unique(const BankedView &A, int *ucols, uint16_t *lidx, int *ucount, cudaStream_t s);
-    void launch_spmv_w(int mode, const BankedView &A, const WideCols &wc, const double *x, double *y, const double *b,
-                       PcgState *st, ReduceBuf red, int iter, int period, cudaStream_t s);
+    void launch_spmv_w(int mode, const BankedView &A, const double *x, double *y, const double *b, PcgState *st,
+                       ReduceBuf red, int iter, int period, cudaStream_t s);
     void launch_update_xr_w(const MasView &mas, double *x, double *r, const double *p, const double *Ap,
                             PcgState *st, ReduceBuf red, int period, cudaStream_t s);
     void launch_update_p_w(const MasView &mas, double *p, const double *z0, PcgState *st, int first, cudaStream_t s);

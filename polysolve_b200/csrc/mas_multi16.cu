@@ -39,113 +39,29 @@ namespace pmas
         static_assert(G == 16, "the lane mappings below assume 16 right-hand sides");
 
         // ---- SpMV: y = A x (PAP: p.Ap, alpha) or y = b - A x (RESIDUAL: r.r, b.b) ------------
-        // Sixteen right-hand sides make the x gathers the bulk of the traffic (384 B per stored block
-        // against 72 B of block values). A bank's 32 rows reference far fewer distinct columns than
-        // they store blocks (Morton subdomains: neighbours are shared), so the CTA first copies the
-        // x rows of the bank's distinct columns into shared memory (cp.async, 16 B per thread and
-        // copy), then every block multiplies from there. The distinct columns of each bank and each
-        // stored block's index into them are built once per pattern (k_bank_unique). Banks with more
-        // than SP_UMAX distinct columns gather directly.
-        constexpr int SP_UMAX = 176;
-        constexpr int SP_SMEM = SP_UMAX * VN * 8; // 67.6 KB: three CTAs per SM
-
-        // One warp per bank: the bank's stored columns sorted (bitonic, in shared memory), the
-        // distinct ones written to ucols[slice * 32 ..], their count to ucount (-1: wider than 64
-        // slots), and the index of every stored block's column among them to lidx.
-        constexpr int UQ_WARPS = 2, UQ_CAP = 64 * 32;
-        __global__ void __launch_bounds__(UQ_WARPS * 32) k_bank_unique(BankedView A, int *__restrict__ ucols,
-                                                                       uint16_t *__restrict__ lidx,
-                                                                       int *__restrict__ ucount)
-        {
-            __shared__ int E[UQ_WARPS][UQ_CAP];
-            __shared__ int U[UQ_WARPS][UQ_CAP];
-            const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-            const int bank = blockIdx.x * UQ_WARPS + w;
-            if (bank >= A.banks)
-                return;
-            const long long s0 = A.slice[bank];
-            const int width = (int)(A.slice[bank + 1] - s0);
-            if (width > UQ_CAP / 32)
-            {
-                if (lane == 0)
-                    ucount[bank] = -1;
-                return;
-            }
-            int *e = E[w], *uq = U[w];
-            const int n = width * 32;
-            int npow = 32;
-            while (npow < n)
-                npow <<= 1;
-            constexpr int NONE = 0x7FFFFFFF;
-            for (int i = lane; i < npow; i += 32)
-            {
-                int v = NONE;
-                if (i < n && (i >> 5) < A.rowlen[(long long)bank * 32 + (i & 31)])
-                    v = A.cols[(s0 + (i >> 5)) * 32 + (i & 31)];
-                e[i] = v;
-            }
-            __syncwarp();
-            for (int size = 2; size <= npow; size <<= 1)
-                for (int stride = size >> 1; stride > 0; stride >>= 1)
-                {
-                    for (int i = lane; i < npow; i += 32)
-                    {
-                        const int j = i ^ stride;
-                        if (j > i)
-                        {
-                            const bool asc = (i & size) == 0;
-                            const int a = e[i], b = e[j];
-                            if ((a > b) == asc)
-                            {
-                                e[i] = b;
-                                e[j] = a;
-                            }
-                        }
-                    }
-                    __syncwarp();
-                }
-            int nu = 0;
-            for (int c0 = 0; c0 < npow; c0 += 32)
-            {
-                const int i = c0 + lane;
-                const bool f = e[i] != NONE && (i == 0 || e[i] != e[i - 1]);
-                const unsigned bal = __ballot_sync(FULL, f);
-                if (f)
-                {
-                    const int pos = nu + __popc(bal & ((1u << lane) - 1u));
-                    uq[pos] = e[i];
-                    ucols[s0 * 32 + pos] = e[i];
-                }
-                nu += __popc(bal);
-            }
-            __syncwarp();
-            if (lane == 0)
-                ucount[bank] = nu;
-            for (int i = lane; i < n; i += 32)
-            {
-                const int k = i >> 5, r = i & 31;
-                if (k >= A.rowlen[(long long)bank * 32 + r])
-                    continue;
-                const int col = A.cols[(s0 + k) * 32 + r];
-                int lo = 0, hi = nu - 1;
-                while (lo < hi)
-                {
-                    const int mid = (lo + hi) >> 1;
-                    if (uq[mid] < col)
-                        lo = mid + 1;
-                    else
-                        hi = mid;
-                }
-                lidx[(s0 + k) * 32 + r] = (uint16_t)lo;
-            }
-        }
+        // Slots (stored blocks) of the warp's four rows go through a ring of SP_STAGES shared-memory
+        // stages filled by cp.async SP_STAGES - 1 slots ahead: each lane copies the three 16-byte x
+        // pieces it multiplies (x[col][j][2 gq .. 2 gq + 1]) and lanes 0-4 of each row the block's
+        // values (four 16-byte pairs, one 8-byte value). The copies need no registers, so a warp keeps
+        // five slots of gathers in flight; the columns come from registers loaded at the bank's start
+        // (slots gq + 8 i of the row in lane gq's register i, up to SP_MAXLEN slots; longer rows take
+        // the plain loop).
+        constexpr int SP_STAGES = 6;
+        constexpr int SP_XB = 32 * 3 * 16;       // x pieces of the 32 lanes
+        constexpr int SP_MB = 4 * 5 * 16;        // block values of the four rows
+        constexpr int SP_SB = SP_XB + SP_MB;     // one stage
+        constexpr int SP_WARP = SP_STAGES * SP_SB;
+        constexpr int SP_SMEM = WW * SP_WARP;
+        constexpr int SP_REGS = 8;
+        constexpr int SP_MAXLEN = 8 * SP_REGS;
+        static_assert(SP_SB % 16 == 0, "16-byte aligned stages");
 
         template <int MODE>
-        __global__ void __launch_bounds__(WT_) k_spmv_w(BankedView A, WideCols wc, const double *__restrict__ x,
+        __global__ void __launch_bounds__(WT_) k_spmv_w(BankedView A, const double *__restrict__ x,
                                                         double *__restrict__ y, const double *__restrict__ b,
                                                         PcgState *st, ReduceBuf red, int iter, int period)
         {
-            extern __shared__ __align__(16) double sp_x[];
+            extern __shared__ __align__(16) unsigned char sp_smem[];
             PcgState *grp = st + G;
             if (grp->done)
                 return;
@@ -155,6 +71,8 @@ namespace pmas
             const int rs = lane >> 3, gq = lane & 7; // row of the warp's four, pair of right-hand sides
             const int rb = w * 4 + rs;               // row within the bank
             const uint64_t pol = l2_evict_first_policy();
+            unsigned char *wbase = sp_smem + (size_t)w * SP_WARP;
+            const long long nodes = (long long)A.banks * 32;
             double part[2] = {0.0, 0.0}, bb[2] = {0.0, 0.0};
             for (int bank = blockIdx.x; bank < A.banks; bank += gridDim.x)
             {
@@ -167,49 +85,89 @@ namespace pmas
 #pragma unroll
                 for (int i = 0; i < 3; ++i)
                     acc[i][0] = acc[i][1] = 0.0;
-                const int nu = wc.ucount[bank]; // CTA-uniform
-                if (nu >= 0 && nu <= SP_UMAX)
+                if (maxlen <= SP_MAXLEN)
                 {
-                    // The bank's distinct x rows (384 B each) into shared memory.
-                    const int *uc = wc.ucols + s0 * 32;
-                    for (int c = threadIdx.x; c < nu * 24; c += WT_)
+                    int colr[SP_REGS];
+#pragma unroll
+                    for (int i = 0; i < SP_REGS; ++i)
                     {
-                        const int q = c / 24, piece = c - q * 24;
-                        cp_async16_ca(sp_x + (size_t)c * 2, x + (long long)uc[q] * VN + piece * 2);
+                        const int sl = gq + 8 * i;
+                        colr[i] = sl < len ? ld_stream_s32(A.cols + (s0 + sl) * 32 + rb, pol) : (int)u;
                     }
-                    cp_async_commit();
-                    cp_async_wait<0>();
-                    __syncthreads();
-                    for (int k = 0; k < maxlen; ++k)
-                    {
-                        if (k >= len)
-                            continue;
-                        const long long slot = s0 + k;
-                        const int li = wc.lidx[slot * 32 + rb];
-                        const double *blk = A.vals + slot * 32 * 9;
-                        double v[9];
+                    // Copies of slot sl (warp-uniform) into its stage.
+                    auto issue = [&](int sl) {
+                        int reg = colr[0];
 #pragma unroll
-                        for (int q = 0; q < 4; ++q)
+                        for (int i = 1; i < SP_REGS; ++i)
+                            if ((sl >> 3) == i)
+                                reg = colr[i];
+                        const long long col = __shfl_sync(FULL, reg, (lane & ~7) | (sl & 7));
+                        if (sl < len)
                         {
-                            const double2 t = ld_stream_f64x2(blk + q * 64 + rb * 2, pol);
-                            v[2 * q] = t.x;
-                            v[2 * q + 1] = t.y;
-                        }
-                        v[8] = ld_stream_f64(blk + 256 + rb, pol);
-                        const double *xr = sp_x + li * VN + 2 * gq;
-#pragma unroll
-                        for (int j = 0; j < 3; ++j)
-                        {
-                            const double2 xv = *reinterpret_cast<const double2 *>(xr + j * G);
-#pragma unroll
-                            for (int i = 0; i < 3; ++i)
+                            unsigned char *sp = wbase + (sl % SP_STAGES) * SP_SB;
+                            const double *blk = A.vals + (s0 + sl) * 32 * 9;
+                            const double *xs = x + (col * 3) * G + 2 * gq;
+                            // Self-check of every copy's source (column range, 16-byte alignment):
+                            // a bad one is recorded in the group's error word and skipped.
+                            const bool bad = col < 0 || col >= nodes ||
+                                             ((reinterpret_cast<uintptr_t>(xs) | reinterpret_cast<uintptr_t>(blk) |
+                                               reinterpret_cast<uintptr_t>(sp)) & 15) != 0;
+                            if (bad)
+                                atomicExch(&grp->error, ERR_CUDA);
+                            else
                             {
-                                acc[i][0] = fma(v[i * 3 + j], xv.x, acc[i][0]);
-                                acc[i][1] = fma(v[i * 3 + j], xv.y, acc[i][1]);
+#pragma unroll
+                                for (int j = 0; j < 3; ++j)
+                                    cp_async16_ca(sp + (lane * 3 + j) * 16, xs + j * G);
+                                if (gq < 4)
+                                    cp_async16_cg(sp + SP_XB + (rs * 5 + gq) * 16, blk + gq * 64 + rb * 2);
+                                else if (gq == 4)
+                                    cp_async8_ca(sp + SP_XB + (rs * 5 + 4) * 16, blk + 256 + rb);
                             }
                         }
+                    };
+#pragma unroll
+                    for (int d = 0; d < SP_STAGES - 1; ++d)
+                    {
+                        if (d < maxlen)
+                            issue(d);
+                        cp_async_commit();
                     }
-                    __syncthreads(); // the next bank's rows overwrite sp_x
+                    for (int k = 0; k < maxlen; ++k)
+                    {
+                        if (k + SP_STAGES - 1 < maxlen)
+                            issue(k + SP_STAGES - 1);
+                        cp_async_commit();
+                        cp_async_wait<SP_STAGES - 1>();
+                        __syncwarp();
+                        if (k < len)
+                        {
+                            const unsigned char *sp = wbase + (k % SP_STAGES) * SP_SB;
+                            const double *mv = reinterpret_cast<const double *>(sp + SP_XB + rs * 80);
+                            double v[9];
+#pragma unroll
+                            for (int q = 0; q < 4; ++q)
+                            {
+                                const double2 t = *reinterpret_cast<const double2 *>(mv + 2 * q);
+                                v[2 * q] = t.x;
+                                v[2 * q + 1] = t.y;
+                            }
+                            v[8] = mv[8];
+#pragma unroll
+                            for (int j = 0; j < 3; ++j)
+                            {
+                                const double2 xv = *reinterpret_cast<const double2 *>(sp + (lane * 3 + j) * 16);
+#pragma unroll
+                                for (int i = 0; i < 3; ++i)
+                                {
+                                    acc[i][0] = fma(v[i * 3 + j], xv.x, acc[i][0]);
+                                    acc[i][1] = fma(v[i * 3 + j], xv.y, acc[i][1]);
+                                }
+                            }
+                        }
+                        __syncwarp();
+                    }
+                    cp_async_wait<0>();
                 }
                 else
                     for (int k = 0; k < maxlen; ++k)
@@ -598,16 +556,8 @@ namespace pmas
                    "wide restrict smem attribute");
     }
 
-    void launch_bank_unique(const BankedView &A, int *ucols, uint16_t *lidx, int *ucount, cudaStream_t s)
-    {
-        if (A.banks == 0)
-            return;
-        k_bank_unique<<<(A.banks + UQ_WARPS - 1) / UQ_WARPS, UQ_WARPS * 32, 0, s>>>(A, ucols, lidx, ucount);
-        cuda_check(cudaGetLastError(), "bank columns launch");
-    }
-
-    void launch_spmv_w(int mode, const BankedView &A, const WideCols &wc, const double *x, double *y, const double *b,
-                       PcgState *st, ReduceBuf red, int iter, int period, cudaStream_t s)
+    void launch_spmv_w(int mode, const BankedView &A, const double *x, double *y, const double *b, PcgState *st,
+                       ReduceBuf red, int iter, int period, cudaStream_t s)
     {
         if (A.bd != 3)
             throw Error(ERR_INVALID, "[MAS] sixteen right-hand sides need block_dim 3");
@@ -616,7 +566,7 @@ namespace pmas
         auto go = [&](auto kernel) {
             int grid = resident_per_sm(kernel, SP_SMEM) * device_sm_count();
             grid = std::min({grid, A.banks, red.capacity});
-            kernel<<<grid, WT_, SP_SMEM, s>>>(A, wc, x, y, b, st, red, iter, period);
+            kernel<<<grid, WT_, SP_SMEM, s>>>(A, x, y, b, st, red, iter, period);
         };
         if (mode == SPMV_PAP)
             go(k_spmv_w<SPMV_PAP>);
