@@ -46,7 +46,7 @@ namespace pmas
         // five slots of gathers in flight; the columns come from registers loaded at the bank's start
         // (slots gq + 8 i of the row in lane gq's register i, up to SP_MAXLEN slots; longer rows take
         // the plain loop).
-        constexpr int SP_STAGES = 6;
+        constexpr int SP_STAGES = 4;
         constexpr int SP_XB = 32 * 3 * 16;       // x pieces of the 32 lanes
         constexpr int SP_MB = 4 * 5 * 16;        // block values of the four rows
         constexpr int SP_SB = SP_XB + SP_MB;     // one stage
@@ -55,6 +55,47 @@ namespace pmas
         constexpr int SP_REGS = 8;
         constexpr int SP_MAXLEN = 8 * SP_REGS;
         static_assert(SP_SB % 16 == 0, "16-byte aligned stages");
+
+        // The copies of slot sl (warp-uniform; every lane calls) of the lane's row into its stage: the
+        // column from register sl / 8 of lane (row base) + sl % 8, selected without indexing (the
+        // registers stay registers), then the lane's three x pieces and, in lanes 0-4 of the row,
+        // the block values. Sources are checked (column range, 16-byte alignment): a bad one is
+        // recorded in the group's error word and skipped.
+        struct ColRegs
+        {
+            int c0, c1, c2, c3, c4, c5, c6, c7;
+        };
+
+        __device__ __forceinline__ void sp_issue(unsigned char *wbase, ColRegs colr, int sl, int len,
+                                                 long long u, long long nodes, int lane, int rs, int gq, int rb,
+                                                 const double *x, const double *vals, long long s0, PcgState *grp)
+        {
+            const int r8 = sl >> 3;
+            const int reg = r8 < 4 ? (r8 < 2 ? (r8 == 0 ? colr.c0 : colr.c1) : (r8 == 2 ? colr.c2 : colr.c3))
+                                   : (r8 < 6 ? (r8 == 4 ? colr.c4 : colr.c5) : (r8 == 6 ? colr.c6 : colr.c7));
+            const long long col = __shfl_sync(FULL, reg, (lane & ~7) | (sl & 7));
+            if (sl >= len)
+                return;
+            unsigned char *sp = wbase + (sl % SP_STAGES) * SP_SB;
+            const double *blk = vals + (s0 + sl) * 32 * 9;
+            const double *xs = x + (col * 3) * G + 2 * gq;
+            const bool bad = col < 0 || col >= nodes ||
+                             ((reinterpret_cast<uintptr_t>(xs) | reinterpret_cast<uintptr_t>(blk) |
+                               reinterpret_cast<uintptr_t>(sp)) &
+                              15) != 0;
+            if (bad)
+            {
+                atomicExch(&grp->error, ERR_CUDA);
+                return;
+            }
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+                cp_async16_ca(sp + (lane * 3 + j) * 16, xs + j * G);
+            if (gq < 4)
+                cp_async16_cg(sp + SP_XB + (rs * 5 + gq) * 16, blk + gq * 64 + rb * 2);
+            else if (gq == 4)
+                cp_async8_ca(sp + SP_XB + (rs * 5 + 4) * 16, blk + 256 + rb);
+        }
 
         template <int MODE>
         __global__ void __launch_bounds__(WT_) k_spmv_w(BankedView A, const double *__restrict__ x,
@@ -87,56 +128,24 @@ namespace pmas
                     acc[i][0] = acc[i][1] = 0.0;
                 if (maxlen <= SP_MAXLEN)
                 {
-                    int colr[SP_REGS];
-#pragma unroll
-                    for (int i = 0; i < SP_REGS; ++i)
-                    {
+                    // Columns of slots gq + 8 i of the lane's row (i < 8).
+                    auto colat = [&](int i) -> int {
                         const int sl = gq + 8 * i;
-                        colr[i] = sl < len ? ld_stream_s32(A.cols + (s0 + sl) * 32 + rb, pol) : (int)u;
-                    }
-                    // Copies of slot sl (warp-uniform) into its stage.
-                    auto issue = [&](int sl) {
-                        int reg = colr[0];
-#pragma unroll
-                        for (int i = 1; i < SP_REGS; ++i)
-                            if ((sl >> 3) == i)
-                                reg = colr[i];
-                        const long long col = __shfl_sync(FULL, reg, (lane & ~7) | (sl & 7));
-                        if (sl < len)
-                        {
-                            unsigned char *sp = wbase + (sl % SP_STAGES) * SP_SB;
-                            const double *blk = A.vals + (s0 + sl) * 32 * 9;
-                            const double *xs = x + (col * 3) * G + 2 * gq;
-                            // Self-check of every copy's source (column range, 16-byte alignment):
-                            // a bad one is recorded in the group's error word and skipped.
-                            const bool bad = col < 0 || col >= nodes ||
-                                             ((reinterpret_cast<uintptr_t>(xs) | reinterpret_cast<uintptr_t>(blk) |
-                                               reinterpret_cast<uintptr_t>(sp)) & 15) != 0;
-                            if (bad)
-                                atomicExch(&grp->error, ERR_CUDA);
-                            else
-                            {
-#pragma unroll
-                                for (int j = 0; j < 3; ++j)
-                                    cp_async16_ca(sp + (lane * 3 + j) * 16, xs + j * G);
-                                if (gq < 4)
-                                    cp_async16_cg(sp + SP_XB + (rs * 5 + gq) * 16, blk + gq * 64 + rb * 2);
-                                else if (gq == 4)
-                                    cp_async8_ca(sp + SP_XB + (rs * 5 + 4) * 16, blk + 256 + rb);
-                            }
-                        }
+                        return sl < len ? ld_stream_s32(A.cols + (s0 + sl) * 32 + rb, pol) : (int)u;
                     };
+                    const ColRegs colr{colat(0), colat(1), colat(2), colat(3), colat(4), colat(5), colat(6), colat(7)};
 #pragma unroll
                     for (int d = 0; d < SP_STAGES - 1; ++d)
                     {
                         if (d < maxlen)
-                            issue(d);
+                            sp_issue(wbase, colr, d, len, u, nodes, lane, rs, gq, rb, x, A.vals, s0, grp);
                         cp_async_commit();
                     }
                     for (int k = 0; k < maxlen; ++k)
                     {
                         if (k + SP_STAGES - 1 < maxlen)
-                            issue(k + SP_STAGES - 1);
+                            sp_issue(wbase, colr, k + SP_STAGES - 1, len, u, nodes, lane, rs, gq, rb, x, A.vals, s0,
+                                     grp);
                         cp_async_commit();
                         cp_async_wait<SP_STAGES - 1>();
                         __syncwarp();
