@@ -509,6 +509,49 @@ struct mas_solver
         }
     }
 
+    // Device -> host copy into pageable memory, the reverse of upload_pageable: 16 MB chunks DMA'd
+    // into the pinned double buffer while host threads copy the previous chunk out.
+    void download_pageable(void *dst, const void *src, size_t bytes)
+    {
+        if (bytes < 2 * STAGE_BYTES)
+        {
+            cuda_check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream), "download");
+            cuda_check(cudaStreamSynchronize(stream), "download");
+            return;
+        }
+        if (!h_stage)
+        {
+            cuda_check(cudaMallocHost(&h_stage, 2 * STAGE_BYTES), "pinned staging");
+            for (cudaEvent_t &e : stage_ev)
+                cuda_check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+        }
+        const int threads = std::max(1, std::min(8, omp_get_max_threads()));
+        const size_t chunks = (bytes + STAGE_BYTES - 1) / STAGE_BYTES;
+        auto start = [&](size_t i) {
+            const size_t off = i * STAGE_BYTES, len = std::min(STAGE_BYTES, bytes - off);
+            cuda_check(cudaMemcpyAsync(h_stage + (i & 1) * STAGE_BYTES, static_cast<const char *>(src) + off, len,
+                                       cudaMemcpyDeviceToHost, stream),
+                       "download");
+            cuda_check(cudaEventRecord(stage_ev[i & 1], stream), "event");
+        };
+        start(0);
+        for (size_t i = 0; i < chunks; ++i)
+        {
+            if (i + 1 < chunks)
+                start(i + 1); // stream order: chunk i + 1 goes into the other buffer
+            cuda_check(cudaEventSynchronize(stage_ev[i & 1]), "staging");
+            const size_t off = i * STAGE_BYTES, len = std::min(STAGE_BYTES, bytes - off);
+            const char *buf = h_stage + (i & 1) * STAGE_BYTES;
+            char *to = static_cast<char *>(dst) + off;
+#pragma omp parallel for num_threads(threads) schedule(static)
+            for (int t = 0; t < threads; ++t)
+            {
+                const size_t a = len * t / threads, z = len * (t + 1) / threads;
+                std::memcpy(to + a, buf + a, z - a);
+            }
+        }
+    }
+
     // MASSolverImpl::factorize (MASSolver.cu:292-374).
     void factorize(int n_, const int *outer, const int *inner, const double *vals, long long nnz_)
     {
@@ -1506,9 +1549,7 @@ struct mas_solver
         for (int c0 = 0; c0 < nrhs; c0 += W)
         {
             const int cols = std::min(W, nrhs - c0);
-            cuda_check(cudaMemcpyAsync(gio.get(), hB + (size_t)c0 * n, sizeof(double) * (size_t)n * cols,
-                                       cudaMemcpyHostToDevice, stream),
-                       "upload B");
+            upload_pageable(gio.get(), hB + (size_t)c0 * n, sizeof(double) * (size_t)n * cols);
             run("permute_in", 2, [&] {
                 if (wide())
                     launch_permute_in_w(n, V, cols, d_padded.get(), gio.get(), gb.get(), glen, stream);
@@ -1523,10 +1564,7 @@ struct mas_solver
                 else
                     launch_permute_out_g(n, bd, cols, d_padded.get(), gx.get(), gio.get(), stream);
             });
-            cuda_check(cudaMemcpyAsync(hX + (size_t)c0 * n, gio.get(), sizeof(double) * (size_t)n * cols,
-                                       cudaMemcpyDeviceToHost, stream),
-                       "download X");
-            cuda_check(cudaStreamSynchronize(stream), "solve multi");
+            download_pageable(hX + (size_t)c0 * n, gio.get(), sizeof(double) * (size_t)n * cols);
             collect_profile();
         }
         solve_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
