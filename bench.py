@@ -675,6 +675,9 @@ def sequence_modes(N: int, S: int, seed: int, mode_filter: str = "all") -> tuple
 
     def step(run, A, b, timed):
         sv, ws = run["solver"], run["ws"]
+        # Every mode factorizes its own freshly written copy of the step's arrays, so no mode
+        # reads host arrays that another mode's factorize has just brought into the caches.
+        A = A.copy()
         t0 = time.perf_counter()
         sv.factorize(A)
         x0 = ws.guess(A.shape[0])

@@ -70,7 +70,10 @@ void mas_destroy(mas_solver *h);
  * time; 1, every time, as the reference), profile_kernels (bool: CUDA-event time per kernel kind,
  * reported by get_info), device_wait_limit (int >= 0: iterations of each bounded device-side wait
  * before the solve stops with MAS_ERR_TIMEOUT; default 1048576, 0 makes every wait give up at
- * once, which tests the timeout path). */
+ * once, which tests the timeout path), rhs_group (0 | 4 | 16: right-hand sides per group of
+ * mas_solve_multi; 0 picks 16 for more than four with block_dim 3, else 4), chained_launch (bool,
+ * default true: the single-right-hand-side PCG kernels use programmatic dependent launch, each
+ * becoming resident while its predecessor drains; results are the same either way). */
 int mas_set_parameters(mas_solver *h, const char *params_json);
 
 /* MASSolver::get_info (MASSolver.cu:214-219): writes a JSON object with solver_iter,

@@ -314,8 +314,6 @@ namespace pmas
             using Real = typename L::Real;
             constexpr int N = L::N, S = L::S, WARPS = L::WARPS;
             constexpr int THREADS = WARPS * 32;
-            if (MODE != 0 && st->done)
-                return;
             extern __shared__ __align__(128) unsigned char smem[];
             const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
             unsigned char *base = smem + (size_t)w * L::WARP_BYTES;
@@ -356,6 +354,16 @@ namespace pmas
             }
             // Copies issued and not yet consumed, per stage (drained if a wait gives up).
             bool pending[2] = {gw < items, gw + total_warps < items};
+            // The first two inverses are on their way (no kernel of a solve writes them); now wait
+            // for the predecessor (launched chained in a PCG iteration).
+            pdl_wait();
+            if (MODE != 0 && st->done)
+            {
+                if (lane == 0)
+                    mbar_drain(bar, pending, {0u, 0u});
+                __syncwarp();
+                return;
+            }
             double part[APPLY_PARTS];
 #pragma unroll
             for (int i = 0; i < APPLY_PARTS; ++i)
@@ -499,6 +507,7 @@ namespace pmas
                     mbar_drain(bar, pending, {phase0, phase1});
                 __syncwarp();
             }
+            pdl_release(); // this warp's items are done: the successor may start launching
             if (MODE == 0)
                 return;
             double tot[APPLY_PARTS];
@@ -990,6 +999,7 @@ namespace pmas
         template <int BD>
         __global__ void __launch_bounds__(LEVEL_THREADS) k_coarse_levels(MasView mas, const PcgState *st)
         {
+            pdl_wait();
             if (st && st->done)
                 return;
             constexpr int W = LEVEL_THREADS / 32;
@@ -1171,6 +1181,7 @@ namespace pmas
                                                           const int *__restrict__ cco0_base, double *rc,
                                                           const PcgState *st, int period)
         {
+            pdl_wait();
             if (st && st->done)
                 return;
             if (st && period > 0 && (st->iter + 1) % period != 0)
@@ -1246,8 +1257,10 @@ namespace pmas
                 grid = 1;
             if (MODE != 0 && grid > red.capacity)
                 throw Error(ERR_INVALID, "[MAS] reduction scratch too small");
-            k_mas_apply<BD, Store, MODE><<<grid, L::WARPS * 32, smem, s>>>(mas, r, z, st, red, cfg);
-            cuda_check(cudaGetLastError(), "apply launch");
+            // Chained in the PCG loop only: the kernel reads inverses before pdl_wait(), and a plain
+            // apply may follow the kernels that write them.
+            launch_chained(MODE != 0 && chained_launch(), k_mas_apply<BD, Store, MODE>, grid, L::WARPS * 32, smem, s,
+                           mas, r, z, st, red, cfg);
         }
 
         template <int BD, class Store>
@@ -1314,10 +1327,9 @@ namespace pmas
         if (mas.first_iso_bank <= 0 || mas.level_num <= 0)
             return 0;
         dispatch_bd(mas.bd, [&]<int BD>() {
-            k_restrict<BD><<<(mas.first_iso_bank + 7) / 8, 256, 0, s>>>(mas.first_iso_bank, r, mas.lcco0,
-                                                                       mas.cco0_base, mas.rc, st, period);
+            launch_chained(chained_launch(), k_restrict<BD>, (mas.first_iso_bank + 7) / 8, 256, 0, s,
+                           mas.first_iso_bank, r, mas.lcco0, mas.cco0_base, mas.rc, st, period);
         });
-        cuda_check(cudaGetLastError(), "restrict launch");
         return 1;
     }
 
@@ -1329,8 +1341,8 @@ namespace pmas
                                             : mas.real_count[2];
         if (grid <= 0)
             return 0;
-        dispatch_bd(mas.bd, [&]<int BD>() { k_coarse_levels<BD><<<grid, LEVEL_THREADS, 0, s>>>(mas, st); });
-        cuda_check(cudaGetLastError(), "coarse levels launch");
+        dispatch_bd(mas.bd,
+                    [&]<int BD>() { launch_chained(chained_launch(), k_coarse_levels<BD>, grid, LEVEL_THREADS, 0, s, mas, st); });
         return 1;
     }
 

@@ -70,12 +70,6 @@ namespace pmas
 
     namespace
     {
-        // Upper-triangle element lists of the 32-, 64- and 96-row subdomain matrices, packed
-        // (row << 8 | col) in row-major order: the sweep visits exactly the kept elements without
-        // index arithmetic. Filled once per device (ensure_tri_table).
-        constexpr int TRI_1 = 32 * 33 / 2, TRI_2 = 64 * 65 / 2, TRI_3 = 96 * 97 / 2;
-        __device__ uint16_t g_tri[TRI_1 + TRI_2 + TRI_3];
-        __host__ __device__ constexpr int tri_offset(int bd) { return bd == 1 ? 0 : (bd == 2 ? TRI_1 : TRI_1 + TRI_2); }
         __device__ __forceinline__ int ctz32(unsigned x) { return __ffs(x) - 1; }
 
         // Bitmask closure inside a warp; masks in shared memory (32 per warp). Returns the local
@@ -207,82 +201,194 @@ namespace pmas
             *o = __float2half_rn((float)(v * sc));
         }
 
-        // Inverts the symmetric N x N matrix A (shared memory, upper triangle used) and stores the
-        // inverse in `out` (tile-packed; binary16: mma16); *scale_out receives the factor that turns
-        // stored values back into matrix values (1 unless binary16); *ident_out (if given) 1 when
-        // the inverse is exactly the identity.
+        // Work matrix in shared memory: N x N FP64 with a row stride of N + 2 doubles, so eight
+        // consecutive rows at one column fall in eight different 16-byte bank groups (the tiled
+        // update below reads and writes 4-row x 4-column tiles and their transposes), followed
+        // by the pivot records of one block of INV_KB pivots.
+        constexpr int INV_KB = 8;
+        constexpr int INV_NCOEF = INV_KB * (2 * INV_KB + 1);
+        __host__ __device__ constexpr int inv_ld(int n) { return n + 2; }
+        __host__ __device__ constexpr size_t inv_smem_bytes(int n)
+        {
+            return ((size_t)n * inv_ld(n) + INV_NCOEF) * sizeof(double);
+        }
+
+        // Inverts the symmetric N x N matrix A (shared memory, stride inv_ld(N), both triangles
+        // kept) and stores the inverse in `out` (tile-packed; binary16: mma16); *scale_out
+        // receives the factor that turns stored values back into matrix values (1 unless
+        // binary16); *ident_out (if given) 1 when the inverse is exactly the identity.
         template <int BD, class Out>
-        __device__ void invert_and_store(double *A, double *col, Out *out, double *scale_out, int *ident_out,
+        __device__ void invert_and_store(double *A, double *coef, Out *out, double *scale_out, int *ident_out,
                                          int *flag)
         {
             constexpr int N = 32 * BD;
+            constexpr int LD = inv_ld(N);
             const int tid = threadIdx.x, nt = blockDim.x;
             __shared__ int bad;
             if (tid == 0)
                 bad = 0;
             for (int i = tid; i < N; i += nt)
-                if (A[i * N + i] == 0.0)
-                    A[i * N + i] = 1.0;
+                if (A[i * LD + i] == 0.0)
+                    A[i * LD + i] = 1.0;
             __syncthreads();
             // Blocked sweep (KB pivots per block; both triangles kept exactly symmetric):
             //  1. warp 0 sweeps the KB x KB pivot block pivot by pivot and records, per pivot q, its
             //     value d_q, pivot-row entries r_t = A[q][t] and scaled entries s_t = r_t / d_q;
             //  2. every column c outside the block replays those pivots on its KB panel entries
             //     (one thread per column, registers) with the single-pivot rule;
-            //  3. every thread applies the block's rank-KB update A[t][c] -= sum_q A[t][q] W[q][c]
-            //     to the upper triangle outside the block (A[t][q]: the block's columns, untouched
-            //     so far; W: the swept panel) and mirrors it; 4. the panel is mirrored into the
-            //     block's columns. The same operator as N single pivots (upper-triangle products
-            //     for both triangles), with N / KB rounds of block-wide barriers instead of N.
-            constexpr int KB = 8;
-            constexpr int NCOEF = KB * (2 * KB + 1);
-            static_assert(N % KB == 0, "pivot blocks");
-            // The pivot records live in col (2 N doubles) when it is large enough.
-            __shared__ double coef_extra[2 * N >= NCOEF ? 1 : NCOEF];
-            double *coef = 2 * N >= NCOEF ? col : coef_extra;
+            //  3. the block's rank-KB update A[t][c] -= sum_q A[t][q] W[q][c] of the upper triangle
+            //     outside the block (A[t][q]: the block's columns, untouched so far; W: the swept
+            //     panel), in 4 x 4 register tiles, one tile per thread, each mirrored;
+            //  4. the panel is mirrored into the block's columns. The same operator as N single
+            //     pivots (upper-triangle products for both triangles, each element's KB products
+            //     subtracted in pivot order), with N / KB rounds of block-wide barriers.
+            // Look-ahead: during step 3 warp 0 updates the next block's own tiles first and then
+            // runs step 1 for it, while the other warps update the remaining tiles; step 1 and
+            // step 3 touch disjoint elements (and the pivot records are free once step 2 is done).
+            constexpr int KB = INV_KB;
+            static_assert(N % KB == 0 && KB % 4 == 0, "pivot blocks of whole tiles");
             const int lane = tid & 31, warp = tid >> 5;
-            const uint16_t *tri = g_tri + tri_offset(BD);
             double *cd = coef;                // [KB] pivots
             double *cr = coef + KB;           // [KB][KB] pivot-row entries (0 at the pivot)
             double *cs = coef + KB + KB * KB; // [KB][KB] scaled entries
-            for (int b0 = 0; b0 < N; b0 += KB)
-            {
-                if (warp == 0)
+            constexpr int TR = N / 4;               // tile rows
+            constexpr int TK = TR - KB / 4;         // tile rows outside a pivot block
+            constexpr int TILES = TK * (TK + 1) / 2; // upper-triangle tiles outside it
+
+            // Step 1 for the block at bs (warp 0, all lanes).
+            auto sweep_block = [&](int bs) {
+                for (int qq = 0; qq < KB; ++qq)
                 {
-                    for (int qq = 0; qq < KB; ++qq)
+                    const int q = bs + qq;
+                    const double d = A[q * LD + q];
+                    if (lane == 0 && (!isfinite(d) || d == 0.0))
+                        bad = 1;
+                    if (lane < KB)
                     {
-                        const int q = b0 + qq;
-                        const double d = A[q * N + q];
-                        if (lane == 0 && (!isfinite(d) || d == 0.0))
+                        const double rq = (lane == qq) ? 0.0 : A[q * LD + bs + lane];
+                        cr[qq * KB + lane] = rq;
+                        cs[qq * KB + lane] = rq / d; // the row scale, one division per row
+                    }
+                    if (lane == 0)
+                        cd[qq] = d;
+                    __syncwarp();
+                    for (int e = lane; e < KB * KB; e += 32)
+                    {
+                        const int ti = e / KB, ci = e % KB;
+                        double u;
+                        if (ti == qq)
+                            u = (ci == qq) ? -1.0 / d : cs[qq * KB + ci];
+                        else if (ci == qq)
+                            u = cs[qq * KB + ti];
+                        else
+                            u = A[(bs + ti) * LD + bs + ci] -
+                                (ti <= ci ? cs[qq * KB + ti] * cr[qq * KB + ci] : cs[qq * KB + ci] * cr[qq * KB + ti]);
+                        if (!isfinite(u))
                             bad = 1;
-                        if (lane < KB)
-                        {
-                            const double rq = (lane == qq) ? 0.0 : A[q * N + b0 + lane];
-                            cr[qq * KB + lane] = rq;
-                            cs[qq * KB + lane] = rq / d; // the row scale, one division per row
-                        }
-                        if (lane == 0)
-                            cd[qq] = d;
-                        __syncwarp();
-                        for (int e = lane; e < KB * KB; e += 32)
-                        {
-                            const int ti = e / KB, ci = e % KB;
-                            double u;
-                            if (ti == qq)
-                                u = (ci == qq) ? -1.0 / d : cs[qq * KB + ci];
-                            else if (ci == qq)
-                                u = cs[qq * KB + ti];
-                            else
-                                u = A[(b0 + ti) * N + b0 + ci] -
-                                    (ti <= ci ? cs[qq * KB + ti] * cr[qq * KB + ci] : cs[qq * KB + ci] * cr[qq * KB + ti]);
-                            if (!isfinite(u))
-                                bad = 1;
-                            A[(b0 + ti) * N + b0 + ci] = u;
-                        }
-                        __syncwarp();
+                        A[(bs + ti) * LD + bs + ci] = u;
+                    }
+                    __syncwarp();
+                }
+            };
+
+            // Step 3 for tile (i, j), i <= j, of the TK x TK grid of tiles outside the block at b0
+            // (tile rows at or after the block's skip its KB / 4 tile rows). Threads with
+            // consecutive tile columns J of one tile row share a warp quarter, and the row stride
+            // is 49 16-byte units (1 mod 8): a thread reads and writes the two halves of a 4-wide
+            // row segment in the order set by bit 2 of J, and stores the transposed tile's rows in
+            // an order rotated by J, so the 16-byte accesses of a quarter warp fall in different
+            // bank groups.
+            auto update_tile = [&](int b0, int i, int j) {
+                const int pb = b0 / 4;
+                const int I = i < pb ? i : i + KB / 4;
+                const int J = j < pb ? j : j + KB / 4;
+                const int t0 = 4 * I, c0 = 4 * J;
+                const int h0 = (J >> 2) & 1; // half of a row segment accessed first
+                auto load_seg = [&](int row, double (&v)[4]) {
+                    const double2 f = *reinterpret_cast<const double2 *>(A + row * LD + c0 + 2 * h0);
+                    const double2 g = *reinterpret_cast<const double2 *>(A + row * LD + c0 + 2 - 2 * h0);
+                    v[0] = h0 ? g.x : f.x;
+                    v[1] = h0 ? g.y : f.y;
+                    v[2] = h0 ? f.x : g.x;
+                    v[3] = h0 ? f.y : g.y;
+                };
+                double u[4][4];
+#pragma unroll
+                for (int r = 0; r < 4; ++r)
+                    load_seg(t0 + r, u[r]);
+#pragma unroll
+                for (int q2 = 0; q2 < KB; q2 += 2)
+                {
+                    double pc[4][2], wr[2][4];
+#pragma unroll
+                    for (int r = 0; r < 4; ++r)
+                    {
+                        const double2 pv = *reinterpret_cast<const double2 *>(A + (t0 + r) * LD + b0 + q2);
+                        pc[r][0] = pv.x;
+                        pc[r][1] = pv.y;
+                    }
+#pragma unroll
+                    for (int h = 0; h < 2; ++h)
+                        load_seg(b0 + q2 + h, wr[h]);
+#pragma unroll
+                    for (int h = 0; h < 2; ++h)
+#pragma unroll
+                        for (int r = 0; r < 4; ++r)
+#pragma unroll
+                            for (int c = 0; c < 4; ++c)
+                                u[r][c] -= pc[r][h] * wr[h][c];
+                }
+                int badt = 0;
+#pragma unroll
+                for (int r = 0; r < 4; ++r)
+#pragma unroll
+                    for (int c = 0; c < 4; ++c)
+                        if (t0 != c0 || r <= c)
+                            badt |= !isfinite(u[r][c]);
+                if (badt)
+                    bad = 1;
+                if (t0 != c0)
+                {
+#pragma unroll
+                    for (int r = 0; r < 4; ++r)
+                    {
+                        double2 *row = reinterpret_cast<double2 *>(A + (t0 + r) * LD + c0);
+                        row[h0] = h0 ? make_double2(u[r][2], u[r][3]) : make_double2(u[r][0], u[r][1]);
+                        row[1 - h0] = h0 ? make_double2(u[r][0], u[r][1]) : make_double2(u[r][2], u[r][3]);
+                    }
+#pragma unroll
+                    for (int c = 0; c < 4; ++c)
+                    {
+                        const int cc = (c + J) & 3; // rotated transposed-row order
+                        double col[4];
+#pragma unroll
+                        for (int r = 0; r < 4; ++r)
+                            col[r] = cc == 0 ? u[r][0] : (cc == 1 ? u[r][1] : (cc == 2 ? u[r][2] : u[r][3]));
+                        *reinterpret_cast<double2 *>(A + (c0 + cc) * LD + t0) = make_double2(col[0], col[1]);
+                        *reinterpret_cast<double2 *>(A + (c0 + cc) * LD + t0 + 2) = make_double2(col[2], col[3]);
                     }
                 }
-                __syncthreads();
+                else
+                {
+                    // Diagonal tile: its upper triangle, mirrored (the lower products are not used,
+                    // as in the single-pivot sweep).
+#pragma unroll
+                    for (int r = 0; r < 4; ++r)
+#pragma unroll
+                        for (int c = r; c < 4; ++c)
+                        {
+                            A[(t0 + r) * LD + t0 + c] = u[r][c];
+                            A[(t0 + c) * LD + t0 + r] = u[r][c];
+                        }
+                }
+            };
+
+            if (warp == 0)
+                sweep_block(0);
+            __syncthreads();
+            for (int b0 = 0; b0 < N; b0 += KB)
+            {
+                // Step 2 with the records of block b0 (written by its step 1).
                 for (int c = tid; c < N; c += nt)
                 {
                     if ((unsigned)(c - b0) < (unsigned)KB)
@@ -290,7 +396,7 @@ namespace pmas
                     double v[KB];
 #pragma unroll
                     for (int i = 0; i < KB; ++i)
-                        v[i] = A[(b0 + i) * N + c];
+                        v[i] = A[(b0 + i) * LD + c];
                     int badc = 0;
 #pragma unroll
                     for (int qq = 0; qq < KB; ++qq)
@@ -312,33 +418,51 @@ namespace pmas
                     for (int i = 0; i < KB; ++i)
                     {
                         badc |= !isfinite(v[i]);
-                        A[(b0 + i) * N + c] = v[i];
+                        A[(b0 + i) * LD + c] = v[i];
                     }
                     if (badc)
                         bad = 1;
                 }
                 __syncthreads();
-                for (int k = tid; k < N * (N + 1) / 2; k += nt)
+                const int pb = b0 / 4;
+                const bool ahead = b0 + KB < N;
+                if (ahead && warp == 0)
                 {
-                    const unsigned tc = __ldg(tri + k);
-                    const int t = (int)(tc >> 8), c = (int)(tc & 255u);
-                    if ((unsigned)(t - b0) < (unsigned)KB || (unsigned)(c - b0) < (unsigned)KB)
-                        continue;
-                    double u = A[t * N + c];
-#pragma unroll
-                    for (int qq = 0; qq < KB; ++qq)
-                        u -= A[t * N + b0 + qq] * A[(b0 + qq) * N + c];
-                    if (!isfinite(u))
-                        bad = 1;
-                    A[t * N + c] = u;
-                    A[c * N + t] = u;
+                    // The next block's tiles (compressed (pb, pb), (pb, pb + 1), (pb + 1, pb + 1)),
+                    // then its step 1.
+                    if (lane < 3)
+                        update_tile(b0, pb + (lane == 2 ? 1 : 0), pb + (lane >= 1 ? 1 : 0));
+                    __syncwarp();
+                    sweep_block(b0 + KB);
+                }
+                else
+                {
+                    const int first = ahead ? 32 : 0;
+                    for (int k = tid - first; k < TILES; k += nt - first)
+                    {
+                        int i = 0, rem = k;
+                        while (rem >= TK - i)
+                        {
+                            rem -= TK - i;
+                            ++i;
+                        }
+                        const int j = i + rem;
+                        if (ahead && (unsigned)(i - pb) < 2u && j <= pb + 1)
+                            continue; // the next block's own tiles: warp 0
+                        update_tile(b0, i, j);
+                    }
                 }
                 __syncthreads();
-                for (int e = tid; e < KB * N; e += nt)
+                // The panel into the block's columns: one row t per thread, its KB entries written
+                // as contiguous pairs (consecutive rows: different bank groups).
+                for (int t = tid; t < N; t += nt)
                 {
-                    const int q = b0 + e / N, t = e % N;
-                    if ((unsigned)(t - b0) >= (unsigned)KB)
-                        A[t * N + q] = A[q * N + t];
+                    if ((unsigned)(t - b0) < (unsigned)KB)
+                        continue;
+#pragma unroll
+                    for (int q2 = 0; q2 < KB; q2 += 2)
+                        *reinterpret_cast<double2 *>(A + t * LD + b0 + q2) =
+                            make_double2(A[(b0 + q2) * LD + t], A[(b0 + q2 + 1) * LD + t]);
                 }
                 __syncthreads();
             }
@@ -358,7 +482,7 @@ namespace pmas
                     if (t > c)
                         continue;
                     // Non-negative doubles order like their bit patterns.
-                    const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(A[e]));
+                    const unsigned long long b = (unsigned long long)__double_as_longlong(fabs(A[t * LD + c]));
                     m = b > m ? b : m;
                 }
                 atomicMax(&amax_bits, m);
@@ -378,7 +502,7 @@ namespace pmas
                 for (int e = tid; e < N * N; e += nt)
                 {
                     const int t = e / N, c = e - t * N;
-                    if (t <= c && -A[e] != (t == c ? 1.0 : 0.0))
+                    if (t <= c && -A[t * LD + c] != (t == c ? 1.0 : 0.0))
                         is_id = 0;
                 }
                 __syncthreads();
@@ -393,7 +517,7 @@ namespace pmas
                 {
                     int row, cl;
                     mma16_rowcol(BD, idx, row, cl);
-                    const double v = -A[row * N + cl];
+                    const double v = -A[row * LD + cl];
                     if (!isfinite(v))
                         bad = 1;
                     store_value(out + idx, v, sc);
@@ -433,7 +557,7 @@ namespace pmas
                     row = 32 * J + (e - j * (j + 1) / 2);
                     cl = 32 * J + j;
                 }
-                const double v = -A[row * N + cl];
+                const double v = -A[row * LD + cl];
                 if (!isfinite(v))
                     bad = 1;
                 store_value(out + idx, v, sc);
@@ -443,18 +567,19 @@ namespace pmas
                 atomicExch(flag, ERR_INVERSE);
         }
 
+        // Three CTAs per SM (shared memory: 76 KB each at block_dim 3; registers capped to fit).
         template <int BD, class Out>
-        __global__ void __launch_bounds__(256) k_assemble_invert_lv0(BankedView A, const int *__restrict__ node_real,
-                                                                     Out *out, double *scale, int *flag)
+        __global__ void __launch_bounds__(256, 3) k_assemble_invert_lv0(BankedView A, const int *__restrict__ node_real,
+                                                                        Out *out, double *scale, int *flag)
         {
-            constexpr int N = 32 * BD;
+            constexpr int N = 32 * BD, LD = inv_ld(N);
             constexpr int S = StoreTraits<Out>::SCALED ? (2 * BD) * (2 * BD - 1) / 2 * 256 + 2 * BD * 192
                                                        : N * (N + 1) / 2;
             extern __shared__ __align__(16) double dsm[];
             double *M = dsm;
-            double *col = dsm + N * N;
+            double *coef = dsm + N * LD;
             const int bank = blockIdx.x;
-            for (int i = threadIdx.x; i < N * N; i += blockDim.x)
+            for (int i = threadIdx.x; i < N * LD; i += blockDim.x)
                 M[i] = 0.0;
             __syncthreads();
             // 8 threads per node, each walking a subset of the node's slots.
@@ -482,33 +607,33 @@ namespace pmas
                                 continue;
                             const double v = A.vals[banked_value_index(slot, lane, bi * BD + bj, BD)];
                             const int row = lane * BD + bi, cl = lw * BD + bj;
-                            M[row * N + cl] = v;
-                            M[cl * N + row] = v;
+                            M[row * LD + cl] = v;
+                            M[cl * LD + row] = v;
                         }
                 }
             }
             __syncthreads();
-            invert_and_store<BD, Out>(M, col, out + (size_t)bank * S, scale + bank, nullptr, flag);
+            invert_and_store<BD, Out>(M, coef, out + (size_t)bank * S, scale + bank, nullptr, flag);
         }
 
         template <int BD, class Out>
-        __global__ void __launch_bounds__(256) k_invert_coarse(const double *__restrict__ staging, Out *out,
-                                                               double *scale, int *identity, int *flag)
+        __global__ void __launch_bounds__(256, 3) k_invert_coarse(const double *__restrict__ staging, Out *out,
+                                                                  double *scale, int *identity, int *flag)
         {
-            constexpr int N = 32 * BD;
+            constexpr int N = 32 * BD, LD = inv_ld(N);
             constexpr int S = StoreTraits<Out>::SCALED ? (2 * BD) * (2 * BD - 1) / 2 * 256 + 2 * BD * 192
                                                        : N * (N + 1) / 2;
             extern __shared__ __align__(16) double dsm[];
             double *M = dsm;
-            double *col = dsm + N * N;
+            double *coef = dsm + N * LD;
             const double *src = staging + (size_t)blockIdx.x * N * N;
             for (int e = threadIdx.x; e < N * N; e += blockDim.x)
             {
                 const int r = e / N, c = e - r * N;
-                M[e] = (r <= c) ? src[r * N + c] : src[c * N + r];
+                M[r * LD + c] = (r <= c) ? src[r * N + c] : src[c * N + r];
             }
             __syncthreads();
-            invert_and_store<BD, Out>(M, col, out + (size_t)blockIdx.x * S, scale + blockIdx.x, identity + blockIdx.x,
+            invert_and_store<BD, Out>(M, coef, out + (size_t)blockIdx.x * S, scale + blockIdx.x, identity + blockIdx.x,
                                       flag);
         }
 
@@ -818,7 +943,7 @@ namespace pmas
         {
             double *scale = M.inv_scale.get();
             constexpr int N = 32 * BD;
-            const size_t smem = (size_t)(N * N + 2 * N) * sizeof(double);
+            const size_t smem = inv_smem_bytes(N);
             cuda_check(cudaFuncSetAttribute(k_assemble_invert_lv0<BD, Out>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             (int)smem),
                        "assemble smem attribute");
@@ -920,35 +1045,11 @@ namespace pmas
 
     namespace
     {
-        // The element lists, once per device (module data is per device).
-        void ensure_tri_table(cudaStream_t s)
-        {
-            static std::mutex mu;
-            static std::vector<int> done;
-            int dev = 0;
-            cuda_check(cudaGetDevice(&dev), "get device");
-            std::lock_guard<std::mutex> lock(mu);
-            if ((int)done.size() > dev && done[dev])
-                return;
-            std::vector<uint16_t> h;
-            h.reserve(TRI_1 + TRI_2 + TRI_3);
-            for (int n : {32, 64, 96})
-                for (int t = 0; t < n; ++t)
-                    for (int c = t; c < n; ++c)
-                        h.push_back((uint16_t)((t << 8) | c));
-            cuda_check(cudaMemcpyToSymbolAsync(g_tri, h.data(), h.size() * sizeof(uint16_t), 0, cudaMemcpyHostToDevice, s),
-                       "element lists");
-            cuda_check(cudaStreamSynchronize(s), "element lists");
-            if ((int)done.size() <= dev)
-                done.resize(dev + 1, 0);
-            done[dev] = 1;
-        }
     } // namespace
 
     void build_mas(MasDevice &M, const BankedMatrix &A, const int *d_node_real, int storage, int first_iso_bank,
                    cudaStream_t s)
     {
-        ensure_tri_table(s);
         const int bd = A.bd, banks = A.banks, nodes = A.nodes;
         M.bd = bd;
         M.banks = banks;

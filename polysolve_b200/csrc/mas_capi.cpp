@@ -60,6 +60,9 @@ namespace
         int preconditioner_refresh = 1;
         bool profile = false; // time every kernel launch with CUDA events
         bool graphs = true;   // replay chunks of iterations as a CUDA graph
+        // Launch the PCG iteration kernels with programmatic dependent launch (each may become
+        // resident while its predecessor drains); false: plain stream order.
+        bool chained = true;
         // Iterations of each bounded device-side wait before the solve stops with MAS_ERR_TIMEOUT
         // (0: every wait gives up at once -- the test of the timeout path).
         long long wait_limit = MBAR_SPIN_LIMIT_DEFAULT;
@@ -114,7 +117,7 @@ namespace
                                 "lazy_partitioning", "use_preconditioned_residual_norm", "precision",
                                 "true_residual_period", "check_period", "initial_guess", "beta", "ordering",
                                 "poll_period", "profile_kernels", "cuda_graphs", "preconditioner_refresh",
-                                "device_wait_limit", "rhs_group"};
+                                "device_wait_limit", "rhs_group", "chained_launch"};
 
     // MASSolverImpl::set_parameters (MASSolver.cu:198-212) plus the extension keys.
     void apply_mas_params(Params &p, const Json &m, bool strict)
@@ -192,6 +195,8 @@ namespace
             q.profile = get_bool(*v, "profile_kernels");
         if (auto *v = m.find("cuda_graphs"))
             q.graphs = get_bool(*v, "cuda_graphs");
+        if (auto *v = m.find("chained_launch"))
+            q.chained = get_bool(*v, "chained_launch");
         if (auto *v = m.find("poll_period"))
         {
             q.poll_period = get_int(*v, "poll_period");
@@ -577,7 +582,11 @@ struct mas_solver
         // below need them there.
         uint64_t h = 0;
         bool pattern_ok = false;
-        std::thread hasher([&] { h = pattern_hash(n_, outer, inner, nnz_, &pattern_ok); });
+        // Host threads split between the two (measured on a 16-core host: 8 + 8 beats sharing all
+        // cores between both, which oversubscribes them).
+        const int upload_threads = std::max(1, std::min(8, omp_get_max_threads()));
+        const int hash_threads = std::max(1, omp_get_max_threads() - upload_threads);
+        std::thread hasher([&] { h = pattern_hash(n_, outer, inner, nnz_, &pattern_ok, hash_threads); });
         try
         {
             refresh_vals.alloc(nnz_ > 0 ? nnz_ : 1, "MAS permuted_bsr input_csc");
@@ -844,6 +853,7 @@ struct mas_solver
         mix((uint64_t)cfg.use_prec_norm);
         mix((uint64_t)cfg.polak_ribiere);
         mix((uint64_t)cfg.wait_limit);
+        mix((uint64_t)chained_launch());
         uint64_t bits;
         std::memcpy(&bits, &cfg.rel_tol, 8);
         mix(bits);
@@ -878,6 +888,7 @@ struct mas_solver
             for (auto &ks : kstats)
                 ks.second = KStat{};
         keep_stats = false;
+        set_chained_launch(p.chained);
         launch_pcg_init_state(S, stream);
         // r = b - A x, rr0, the level-0 restriction of r, then z = M^-1 r
         run("spmv_residual", 1, [&] { launch_spmv(SPMV_RESIDUAL, Av, x.get(), r.get(), b.get(), S, red(), 0, 0, stream); });

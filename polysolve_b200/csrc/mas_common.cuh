@@ -11,6 +11,37 @@ namespace pmas
 {
     constexpr unsigned FULL = 0xFFFFFFFFu;
 
+    // ---------------------------------------------------------------------------------------
+    // Programmatic dependent launch. The PCG iteration kernels are launched with programmatic
+    // stream serialization (launch_chained): such a kernel may become resident while its
+    // predecessor in the stream drains, so it calls pdl_wait() before it reads or writes anything
+    // that the predecessor (or any earlier kernel) touches. pdl_wait() returns once the
+    // predecessor grid has completed and its writes are visible, and at once for a kernel
+    // launched without the attribute. pdl_release() lets the successor start launching once every
+    // CTA of this grid has called it or exited; it does not make any write visible early.
+    // ---------------------------------------------------------------------------------------
+    __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+    __device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+    // Launch `kernel` in stream order; with chained = true it may overlap the predecessor's tail
+    // (the kernel must start with pdl_wait()). Works under stream capture (programmatic edges).
+    template <class... P, class... A>
+    void launch_chained(bool chained, void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                        A &&...args)
+    {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = grid;
+        cfg.blockDim = block;
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = s;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        attr[0].val.programmaticStreamSerializationAllowed = chained ? 1 : 0;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cuda_check(cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...), "kernel launch");
+    }
+
     // Inverse storage types: the arithmetic type of each and loads of one / four consecutive
     // stored values converted to it. Binary16 values are read as IEEE bits (the buffers are
     // uint16_t on the host) and multiplied in FP32.

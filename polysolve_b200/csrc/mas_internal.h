@@ -328,6 +328,12 @@ namespace pmas
                       cudaStream_t s);
     void rescatter_values(BankedMatrix &M, long long nnz, const double *d_vals, cudaStream_t s);
 
+    // Programmatic dependent launch of the single-right-hand-side PCG kernels (SpMV, update_xr,
+    // restrict, coarse levels, MAS apply, update_p): each may become resident while its
+    // predecessor drains. On by default; per calling thread (mas_pcg.cu).
+    void set_chained_launch(bool on);
+    bool chained_launch();
+
     // mas_spmv.cu
     enum SpmvMode : int
     {

@@ -270,40 +270,61 @@ namespace pmas
         return padded;
     }
 
-    uint64_t pattern_hash(int n, const int *outer, const int *inner, long long nnz, bool *valid)
+    uint64_t pattern_hash(int n, const int *outer, const int *inner, long long nnz, bool *valid, int threads)
     {
-        const int chunks = 256;
-        std::vector<uint64_t> part(chunks, 0);
+        // FNV-1a over 32-bit words, split into chunks (threads) and, inside a chunk, into eight
+        // interleaved lanes (independent multiply chains: the loop runs at memory speed instead of
+        // the multiplier's latency). Column pointers are hashed and checked in the same chunks.
+        constexpr uint64_t OFFSET = 1469598103934665603ull, PRIME = 1099511628211ull;
+        constexpr int chunks = 256, LANES = 8;
+        std::vector<uint64_t> part(chunks, 0), opart(chunks, 0);
         std::vector<uint8_t> bad(chunks, 0);
-#pragma omp parallel for schedule(static)
+        if (threads <= 0)
+            threads = omp_get_max_threads();
+#pragma omp parallel for schedule(static) num_threads(threads)
         for (int c = 0; c < chunks; ++c)
         {
             const long long lo = nnz * c / chunks, hi = nnz * (c + 1) / chunks;
-            uint64_t h = 1469598103934665603ull ^ (uint64_t)c;
+            uint64_t h[LANES];
+            for (int l = 0; l < LANES; ++l)
+                h[l] = OFFSET ^ (uint64_t)(c * LANES + l);
             uint32_t out_of_range = 0; // negative rows wrap to large unsigned values
-            for (long long k = lo; k < hi; ++k)
+            long long k = lo;
+            for (; k + LANES <= hi; k += LANES)
+                for (int l = 0; l < LANES; ++l)
+                {
+                    const uint32_t i = (uint32_t)inner[k + l];
+                    out_of_range |= (uint32_t)(i >= (uint32_t)n);
+                    h[l] = (h[l] ^ (uint64_t)i) * PRIME;
+                }
+            for (; k < hi; ++k)
             {
                 const uint32_t i = (uint32_t)inner[k];
                 out_of_range |= (uint32_t)(i >= (uint32_t)n);
-                h ^= (uint64_t)i;
-                h *= 1099511628211ull;
+                h[0] = (h[0] ^ (uint64_t)i) * PRIME;
             }
-            part[c] = h;
-            bad[c] = (uint8_t)out_of_range;
+            uint64_t g = OFFSET;
+            for (int l = 0; l < LANES; ++l)
+                g = (g ^ h[l]) * PRIME;
+            part[c] = g;
+            // Column pointers j in [olo, ohi): hashed, and non-decreasing.
+            const long long olo = (long long)(n + 1) * c / chunks, ohi = (long long)(n + 1) * (c + 1) / chunks;
+            uint64_t ho = OFFSET ^ (uint64_t)c;
+            bool decreasing = false;
+            for (long long j = olo; j < ohi; ++j)
+            {
+                ho = (ho ^ (uint64_t)(uint32_t)outer[j]) * PRIME;
+                decreasing |= (j > 0 && outer[j] < outer[j - 1]);
+            }
+            opart[c] = ho;
+            bad[c] = (uint8_t)(out_of_range | (decreasing ? 1u : 0u));
         }
-        uint64_t h = 1469598103934665603ull ^ (uint64_t)n ^ ((uint64_t)nnz << 20);
+        uint64_t h = OFFSET ^ (uint64_t)n ^ ((uint64_t)nnz << 20);
         bool ok = outer[0] == 0 && (long long)outer[n] == nnz;
-        for (int j = 0; j <= n; ++j)
-        {
-            h ^= (uint64_t)(uint32_t)outer[j];
-            h *= 1099511628211ull;
-            if (j > 0 && outer[j] < outer[j - 1])
-                ok = false;
-        }
         for (int c = 0; c < chunks; ++c)
         {
-            h ^= part[c];
-            h *= 1099511628211ull;
+            h = (h ^ opart[c]) * PRIME;
+            h = (h ^ part[c]) * PRIME;
             ok = ok && !bad[c];
         }
         if (valid)

@@ -30,5 +30,7 @@ namespace pmas
     // 64-bit FNV-1a style hash of a CSC pattern (n, outer, inner), OpenMP-parallel. The same pass
     // checks the pattern: *valid (if given) is false unless outer runs from 0 to nnz without
     // decreasing and every row index lies in [0, n). Row order inside a column is free.
-    uint64_t pattern_hash(int n, const int *outer, const int *inner, long long nnz, bool *valid = nullptr);
+    // threads: OpenMP threads of the pass (0: all).
+    uint64_t pattern_hash(int n, const int *outer, const int *inner, long long nnz, bool *valid = nullptr,
+                          int threads = 0);
 } // namespace pmas

@@ -68,6 +68,10 @@ namespace pmas
             cudaFree(p);
     }
 
+    static thread_local bool t_chained_launch = true;
+    void set_chained_launch(bool on) { t_chained_launch = on; }
+    bool chained_launch() { return t_chained_launch; }
+
     namespace
     {
         constexpr int UPD_THREADS = 256;
@@ -82,6 +86,7 @@ namespace pmas
                                                                    const double *__restrict__ Ap, PcgState *st,
                                                                    ReduceBuf red, int period)
         {
+            pdl_wait();
             if (st->done)
                 return;
             const double alpha = st->alpha;
@@ -122,6 +127,7 @@ namespace pmas
                 if (restrict_r && bank < mas.first_iso_bank)
                     bank_restrict<BD>(rv, bank, mas.lcco0, mas.cco0_base, mas.rc);
             }
+            pdl_release();
             if (due)
                 return;
             double v1[1] = {part}, tot[1];
@@ -135,6 +141,7 @@ namespace pmas
                                                                   const double *__restrict__ z0, const PcgState *st,
                                                                   int first)
         {
+            pdl_wait();
             if (st->done)
                 return;
             const double beta = first ? 0.0 : st->beta;
@@ -283,7 +290,7 @@ namespace pmas
                 grid = 1;
             if (grid > red.capacity)
                 throw Error(ERR_INVALID, "[MAS] reduction scratch too small");
-            kernel<<<grid, UPD_THREADS, 0, s>>>(mas, x, r, p, Ap, st, red, period);
+            launch_chained(chained_launch(), kernel, grid, UPD_THREADS, 0, s, mas, x, r, p, Ap, st, red, period);
         };
         if (mas.bd == 1)
             go(k_update_xr<1>);
@@ -299,7 +306,7 @@ namespace pmas
         auto go = [&](auto kernel) {
             const int grid = bank_grid_all(mas.banks);
             if (grid > 0)
-                kernel<<<grid, UPD_THREADS, 0, s>>>(mas, p, z0, st, first);
+                launch_chained(chained_launch(), kernel, grid, UPD_THREADS, 0, s, mas, p, z0, st, first);
         };
         if (mas.bd == 1)
             go(k_update_p<1>);

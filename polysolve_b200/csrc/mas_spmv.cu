@@ -32,6 +32,7 @@ namespace pmas
         {
             constexpr int BS = BD * BD;
             constexpr int PAIRS = BS / 2;
+            pdl_wait();
             if (MODE != SPMV_PLAIN && st->done)
                 return;
             // In-loop true residual: only every `period`-th iteration (iteration = st->iter + 1).
@@ -108,6 +109,7 @@ namespace pmas
                     }
                 }
             }
+            pdl_release(); // the successor may start launching; the reduction below is the tail
             if (MODE == SPMV_PLAIN)
                 return;
             if (MODE == SPMV_RESIDUAL && period > 0)
@@ -146,16 +148,18 @@ namespace pmas
                 return;
             if (mode != SPMV_PLAIN && grid > red.capacity)
                 throw Error(ERR_INVALID, "[MAS] reduction scratch too small");
+            const bool ch = chained_launch();
             switch (mode)
             {
             case SPMV_PLAIN:
                 k_spmv<BD, SPMV_PLAIN><<<grid, SPMV_THREADS, 0, s>>>(A, x, y, b, st, red, iter, period);
                 break;
             case SPMV_PAP:
-                k_spmv<BD, SPMV_PAP><<<grid, SPMV_THREADS, 0, s>>>(A, x, y, b, st, red, iter, period);
+                launch_chained(ch, k_spmv<BD, SPMV_PAP>, grid, SPMV_THREADS, 0, s, A, x, y, b, st, red, iter, period);
                 break;
             default:
-                k_spmv<BD, SPMV_RESIDUAL><<<grid, SPMV_THREADS, 0, s>>>(A, x, y, b, st, red, iter, period);
+                launch_chained(ch, k_spmv<BD, SPMV_RESIDUAL>, grid, SPMV_THREADS, 0, s, A, x, y, b, st, red, iter,
+                               period);
                 break;
             }
             cuda_check(cudaGetLastError(), "spmv launch");

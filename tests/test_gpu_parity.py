@@ -416,6 +416,28 @@ def test_graph_replay_bit_identical_to_host_loop():
     assert out[0][1]["solver_iter"] == out[1][1]["solver_iter"]
 
 
+@pytest.mark.parametrize("precision", ["fp64", "fp16"])
+def test_chained_launch_bit_identical(precision):
+    """Programmatic dependent launch of the iteration kernels (each resident while its predecessor
+    drains) gives exactly the plain stream-ordered results, replayed as graphs or host-launched,
+    with true-residual and convergence-test iterations among them."""
+    system = synthetic.elasticity(10, young_sigma=1.0, jitter=0.2, seed=15, contact_pairs=80)
+    b = synthetic.rhs(system.n, 15)
+    out = []
+    for chained in (True, False):
+        for graphs in (True, False):
+            s = make_solver(system, 3, {"precision": precision, "true_residual_period": 6, "check_period": 1,
+                                        "cuda_graphs": graphs, "poll_period": 4, "chained_launch": chained})
+            x = np.zeros(system.n)
+            s.solve(b, x)
+            info = s.get_info()
+            assert info["solver_status"] == "Reach relative tolerance"
+            out.append((x, info["solver_iter"]))
+    for x, it in out[1:]:
+        np.testing.assert_array_equal(x, out[0][0])
+        assert it == out[0][1]
+
+
 @pytest.mark.parametrize("ordering", ["morton", "natural"])
 def test_isolated_rows_with_general_blocks(ordering):
     """Isolated block rows (no off-diagonal block) with non-identity SPD diagonal blocks. With a
