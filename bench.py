@@ -80,6 +80,8 @@ def parse_args():
                     help="grid80: the headline 1.6 M DOF solve; batch64: 64 independent uneven systems; "
                          "contact16: the 80^3 mesh with 20,000 contact pairs and 16 right-hand sides; "
                          "sequence60: a 60^3 sequence (new values each step) with warm starts")
+    ap.add_argument("--wide-apply", default="mma_sync", choices=["mma_sync", "tcgen05"],
+                    help="contact16: tensor-core path of the sixteen-wide MAS apply")
     ap.add_argument("--precision", default=CHOSEN["precision"], choices=["fp16", "fp32", "fp64"],
                     help="storage of the MAS inverses in the chosen configuration")
     return ap.parse_args()
@@ -553,7 +555,7 @@ def run_contact16(args) -> None:
     R = 16
     B = np.stack([synthetic.rhs(n, seed=args.seed * 100 + c) for c in range(R)])
     sv = Solver.create("MAS", "")
-    sv.set_parameters({"MAS": dict(CHOSEN, precision="fp16")})
+    sv.set_parameters({"MAS": dict(CHOSEN, precision="fp16", wide_apply=args.wide_apply)})
     sv.set_positions(system.positions)
     sv.analyze_pattern(A, n)
     sv.factorize(A)
@@ -583,6 +585,23 @@ def run_contact16(args) -> None:
     sv.solve_multi(B)
     g4_ms = (time.perf_counter() - t0) * 1000.0
     sv.set_parameters({"MAS": {"rhs_group": 0}})
+    # The group of sixteen with the other tensor-core path of the apply, and the apply's time per
+    # launch for both (CUDA events in a profiled solve).
+    other = "tcgen05" if args.wide_apply == "mma_sync" else "mma_sync"
+    sv.set_parameters({"MAS": {"wide_apply": other}})
+    sv.solve_multi(B)
+    t0 = time.perf_counter()
+    Xo = sv.solve_multi(B)
+    other_ms = (time.perf_counter() - t0) * 1000.0
+    other_worst = max(float(np.linalg.norm(A @ Xo[c] - B[c]) / np.linalg.norm(B[c])) for c in range(R))
+    apply_us = {}
+    for variant in ("mma_sync", "tcgen05"):
+        sv.set_parameters({"MAS": {"wide_apply": variant, "profile_kernels": True}})
+        sv.solve_multi(B)
+        pinf = sv.get_info()
+        km, kl = pinf.get("kernel_ms", {}), pinf.get("kernel_launches", {})
+        apply_us[variant] = round(1000.0 * km.get("mas_apply", 0.0) / max(1, kl.get("mas_apply", 1)), 2)
+    sv.set_parameters({"MAS": {"wide_apply": args.wide_apply, "profile_kernels": False}})
     # FP64 reference solutions (CHOLMOD is unavailable on this box): plain FP64 MAS-PCG to a
     # relative residual of 1e-11 (FP64 PCG stalls near 3e-12 here) for every right-hand side; the
     # worst relative solution error.
@@ -613,6 +632,9 @@ def run_contact16(args) -> None:
         "fp64_reference": "plain FP64 MAS-PCG to relative residual 1e-11 per right-hand side "
                           "(CHOLMOD unavailable on this box)",
         "groups_of_4_ms": round(g4_ms, 3),
+        "wide_apply": args.wide_apply,
+        "other_wide_apply": {"variant": other, "ms": round(other_ms, 3), "worst_relative_residual": other_worst},
+        "apply_us_per_launch": apply_us,
         "one_by_one_ms": round(float(t[1].item()), 3),
         "speedup_vs_one_by_one": round(float(t[1].item()) / float(t[0].item()), 3),
         "e2e": {"value": round(value, 3), "unit": "ms/16 RHS", "h2d_bytes_per_step": int(8 * n * R),

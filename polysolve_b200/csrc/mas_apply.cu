@@ -968,6 +968,318 @@ namespace pmas
             }
         }
 
+        // ---- Sixteen right-hand sides on the fifth-generation tensor cores (tcgen05) ------------
+        // Inverse storage "tc" (built from the mma16 storage, the same binary16 values): the full
+        // 96 x 96 matrix in 16 x 16 tiles, tile (i, s) (rows 16 i .., columns 16 s ..) at byte
+        // s * TC_SLAB_G + i * 512, each tile the four 8 x 8 core matrices [rows 0-7 | cols 0-7],
+        // [rows 0-7 | cols 8-15], [rows 8-15 | cols 0-7], [rows 8-15 | cols 8-15] of 16-byte rows:
+        // the canonical no-swizzle K-major operand layout with 128 bytes between the two K halves of
+        // a core pair and 256 bytes between 8-row groups. Column slab s is the A operand of one K = 16
+        // step; in shared memory the slabs are TC_SLAB_S apart with rows 96-127 zero (M = 128).
+        // The B operand is the item's 16 right-hand sides split into binary16 hi and lo parts
+        // (N = 32: columns g and 16 + g), D = A B^T accumulates in FP32 in tensor memory.
+        constexpr int TC_N = 96, TC_G = RHS_WIDE, TC_THREADS = 128;
+        constexpr int TC_SLAB_G = 6 * 512;          // bytes of a column slab in global memory
+        constexpr int TC_SLAB_S = 8 * 512;          // in shared memory (M = 128 rows)
+        constexpr int TC_MAT_BYTES = 6 * TC_SLAB_G; // 18432 bytes per matrix
+
+        __host__ __device__ constexpr int tc_offset(int row, int col)
+        {
+            return (col >> 4) * TC_SLAB_G + (row >> 4) * 512 + ((row >> 3) & 1) * 256 + ((col >> 3) & 1) * 128 +
+                   (row & 7) * 16 + (col & 7) * 2;
+        }
+
+        // B operand element (n, k): K steps 1 KB apart, 8-column groups 256 bytes apart.
+        __device__ __forceinline__ int tc_b_offset(int n, int k)
+        {
+            return (k >> 4) * 1024 + (n >> 3) * 256 + ((k >> 3) & 1) * 128 + (n & 7) * 16 + (k & 7) * 2;
+        }
+
+        struct TcLayout
+        {
+            static constexpr int A_BYTES = 6 * TC_SLAB_S;     // one stage of A
+            static constexpr int X_BYTES = TC_N * TC_G * 8;   // one stage of the FP64 input block
+            static constexpr int B_BYTES = 6 * 1024;
+            static constexpr int OFF_X = 2 * A_BYTES;
+            static constexpr int OFF_B = OFF_X + 2 * X_BYTES;
+            static constexpr int OFF_AMAX = OFF_B + B_BYTES;  // [8][16] doubles
+            static constexpr int OFF_XSC = OFF_AMAX + 8 * TC_G * 8;
+            static constexpr int OFF_WSUM = OFF_XSC + TC_G * 8; // [4 warps][3][16] doubles
+            static constexpr int OFF_BAR = OFF_WSUM + 4 * 3 * TC_G * 8;
+            static constexpr int BYTES = OFF_BAR + 64;
+            static_assert(OFF_X % 1024 == 0 && OFF_B % 128 == 0 && OFF_BAR % 16 == 0, "alignment");
+        };
+
+        // mma16 -> tc storage, one CTA per matrix.
+        __global__ void __launch_bounds__(256) k_inv_to_tc(const __half *__restrict__ inv, __half *__restrict__ out)
+        {
+            constexpr int S16 = 6 * 5 / 2 * 256 + 6 * 192;
+            const __half *src = inv + (size_t)blockIdx.x * S16;
+            unsigned char *dst = reinterpret_cast<unsigned char *>(out) + (size_t)blockIdx.x * TC_MAT_BYTES;
+            for (int e = threadIdx.x; e < TC_N * TC_N; e += blockDim.x)
+            {
+                const int row = e / TC_N, col = e - row * TC_N;
+                *reinterpret_cast<__half *>(dst + tc_offset(row, col)) = src[mma16_index(3, row, col)];
+            }
+        }
+
+        // The sixteen-right-hand-side MAS apply on tcgen05 (same work items, scales, outputs, dots
+        // and PCG steps as k_mas_apply_w). One CTA of four warps per item at a time, items strided
+        // over the grid; per item the inverse (six slab copies) and the 96 x 16 FP64 input block
+        // arrive by bulk copies on one mbarrier, two items ahead. The four warps split the input into
+        // binary16 hi / lo (per-column power-of-two scale), thread 0 issues six MMAs and commits them
+        // to an mbarrier, and warps 0-2 read rows 0-95 of the accumulator (tcgen05.ld), combine hi +
+        // lo, scale to FP64, store z and add the dots. Every wait is bounded (MAS_ERR_TIMEOUT).
+        template <int MODE>
+        __global__ void __launch_bounds__(TC_THREADS) k_mas_apply_tc(MasView mas, const __half *__restrict__ inv_tc,
+                                                                     const double *__restrict__ r,
+                                                                     double *__restrict__ z0, PcgState *st,
+                                                                     ReduceBuf red, PcgConfig cfg)
+        {
+            using L = TcLayout;
+            constexpr int N = TC_N, G = TC_G;
+            PcgState *grp = st + G;
+            if (grp->done)
+                return;
+            extern __shared__ __align__(1024) unsigned char smem[];
+            const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+            unsigned char *sA = smem, *sX = smem + L::OFF_X, *sB = smem + L::OFF_B;
+            double *amax_s = reinterpret_cast<double *>(smem + L::OFF_AMAX);
+            double *xsc_s = reinterpret_cast<double *>(smem + L::OFF_XSC);
+            double *wsum = reinterpret_cast<double *>(smem + L::OFF_WSUM);
+            uint64_t *tma_bar = reinterpret_cast<uint64_t *>(smem + L::OFF_BAR); // [2]
+            uint64_t *mma_bar = tma_bar + 2;
+            uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(tma_bar + 3);
+            const int banks = mas.banks, items = banks + mas.n_coarse_active;
+            auto mat_of = [&](int m) { return m < banks ? m : banks + mas.coarse_active[m - banks]; };
+            auto in_of = [&](int m) -> const double * {
+                return m < banks ? r + (size_t)m * N * G : mas.rc + (size_t)(mat_of(m) - banks) * N * G;
+            };
+            const uint64_t pol = l2_evict_first_policy();
+            if (tid == 0)
+            {
+                mbar_init(&tma_bar[0], 1);
+                mbar_init(&tma_bar[1], 1);
+                mbar_init(mma_bar, 1);
+                fence_mbar_init();
+            }
+            if (w == 0)
+                tmem_alloc(tmem_slot, 32);
+            // Rows 96-127 of every slab of both A stages: zero (the bulk copies fill rows 0-95).
+            for (int i = tid; i < 2 * 6 * 64; i += TC_THREADS)
+            {
+                const int stg = i / 384, rem = i - stg * 384, slab = rem >> 6, q = rem & 63;
+                reinterpret_cast<uint4 *>(sA + stg * L::A_BYTES + slab * TC_SLAB_S + 6 * 512)[q] = make_uint4(0, 0, 0, 0);
+            }
+            for (int i = tid; i < 4 * 3 * G; i += TC_THREADS)
+                wsum[i] = 0.0;
+            fence_proxy_async_smem();
+            tc_fence_before_sync();
+            __syncthreads();
+            tc_fence_after_sync();
+            const uint32_t taddr = *tmem_slot;
+            const int m0 = blockIdx.x, stride = gridDim.x;
+            // Thread 0: the inverse and the input block of item m into stage stg.
+            auto issue = [&](int m, int stg) {
+                const unsigned char *src = reinterpret_cast<const unsigned char *>(inv_tc) + (size_t)mat_of(m) * TC_MAT_BYTES;
+                mbar_arrive_expect_tx(&tma_bar[stg], TC_MAT_BYTES + L::X_BYTES);
+#pragma unroll 1
+                for (int s = 0; s < 6; ++s)
+                    bulk_copy_g2s_hint(sA + stg * L::A_BYTES + s * TC_SLAB_S, src + s * TC_SLAB_G, TC_SLAB_G,
+                                       &tma_bar[stg], pol);
+                bulk_copy_g2s(sX + stg * L::X_BYTES, in_of(m), L::X_BYTES, &tma_bar[stg]);
+            };
+            bool pending[2] = {m0 < items, m0 + stride < items};
+            if (tid == 0)
+            {
+                if (pending[0])
+                    issue(m0, 0);
+                if (pending[1])
+                    issue(m0 + stride, 1);
+            }
+            uint32_t tphase[2] = {0u, 0u}, mphase = 0u;
+            bool mma_pending = false, ok = true;
+            const uint32_t idesc = tc_idesc_f16_f32(128, 32);
+            double dsum[G];
+#pragma unroll
+            for (int gg = 0; gg < G; ++gg)
+                dsum[gg] = 0.0;
+            int cat = 0; // dots of coupled banks, isolated banks, coarse matrices
+            // This warp's running dots into its slots of category c (each category once per CTA:
+            // items increase, and the categories with them).
+            auto flush = [&](int c) {
+#pragma unroll
+                for (int gg = 0; gg < G; ++gg)
+                {
+                    const double v = warp_sum(dsum[gg]);
+                    if (lane == 0)
+                        wsum[(w * 3 + c) * G + gg] = v;
+                    dsum[gg] = 0.0;
+                }
+            };
+            const int g = tid & (G - 1), rg = tid >> 4; // input split: column g, rows 12 rg .. 12 rg + 11
+            int k = 0;
+            for (int m = m0; m < items; m += stride, ++k)
+            {
+                const int stg = k & 1;
+                const bool wok = mbar_wait_bounded(&tma_bar[stg], tphase[stg], &grp->error, cfg.wait_limit);
+                if (!__syncthreads_and(wok))
+                {
+                    ok = false;
+                    break;
+                }
+                pending[stg] = false;
+                tphase[stg] ^= 1u;
+                const bool coarse = m >= banks;
+                const int mat = mat_of(m);
+                const int mcat = coarse ? 2 : (m >= mas.first_iso_bank ? 1 : 0);
+                if (mcat != cat)
+                {
+                    flush(cat);
+                    cat = mcat;
+                }
+                const double *x = reinterpret_cast<const double *>(sX + stg * L::X_BYTES);
+                const bool ident = coarse && mas.identity[mat - banks];
+                double xv[12], am = 0.0;
+#pragma unroll
+                for (int i = 0; i < 12; ++i)
+                {
+                    xv[i] = x[(rg * 12 + i) * G + g];
+                    am = fmax(am, fabs(xv[i]));
+                }
+                amax_s[rg * G + g] = am;
+                __syncthreads();
+                double amx = 0.0;
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    amx = fmax(amx, amax_s[q * G + g]);
+                const double xscale = (amx > 0.0 && isfinite(amx)) ? ldexp(1.0, 14 - ilogb(amx)) : 1.0;
+                if (rg == 0)
+                    xsc_s[g] = mas.inv_scale[mat] / xscale; // column g's factor back to matrix values
+                if (!ident)
+                {
+                    // Row pairs (kk, kk + 1) are adjacent in the operand layout: one 32-bit store
+                    // per pair and part.
+#pragma unroll
+                    for (int i = 0; i < 12; i += 2)
+                    {
+                        const int kk = rg * 12 + i;
+                        const float v0 = (float)(xv[i] * xscale), v1 = (float)(xv[i + 1] * xscale);
+                        const __half h0 = __float2half_rn(v0), h1 = __float2half_rn(v1);
+                        *reinterpret_cast<__half2 *>(sB + tc_b_offset(g, kk)) = __halves2half2(h0, h1);
+                        *reinterpret_cast<__half2 *>(sB + tc_b_offset(G + g, kk)) =
+                            __halves2half2(__float2half_rn(v0 - __half2float(h0)), __float2half_rn(v1 - __half2float(h1)));
+                    }
+                    fence_proxy_async_smem();
+                }
+                tc_fence_before_sync();
+                __syncthreads();
+                if (!ident)
+                {
+                    if (tid == 0)
+                    {
+                        tc_fence_after_sync();
+                        const unsigned char *a = sA + stg * L::A_BYTES;
+#pragma unroll
+                        for (int s = 0; s < 6; ++s)
+                            tc_mma_f16(taddr, tc_smem_desc(a + s * TC_SLAB_S, 128, 256), tc_smem_desc(sB + s * 1024, 128, 256),
+                                       idesc, s > 0);
+                        tc_commit(mma_bar);
+                    }
+                    mma_pending = true;
+                    const bool mok = mbar_wait_bounded(mma_bar, mphase, &grp->error, cfg.wait_limit);
+                    if (!__syncthreads_and(mok))
+                    {
+                        ok = false;
+                        break;
+                    }
+                    mma_pending = false;
+                    mphase ^= 1u;
+                    tc_fence_after_sync();
+                }
+                if (w < 3)
+                {
+                    const int row = 32 * w + lane;
+                    double *out = (coarse ? mas.zc + (size_t)(mat - banks) * N * G : z0 + (size_t)m * N * G) + (size_t)row * G;
+                    const double *xr = x + row * G;
+                    float hi[16], lo[16];
+                    if (!ident)
+                    {
+                        const uint32_t ta = taddr + ((uint32_t)(32 * w) << 16);
+                        tc_ld16(ta, hi);
+                        tc_ld16(ta + 16, lo);
+                        tc_wait_ld();
+                    }
+#pragma unroll
+                    for (int gg = 0; gg < G; gg += 2)
+                    {
+                        double zv[2];
+#pragma unroll
+                        for (int h = 0; h < 2; ++h)
+                        {
+                            const double xin = xr[gg + h];
+                            zv[h] = ident ? xin : (double)(hi[gg + h] + lo[gg + h]) * xsc_s[gg + h];
+                            dsum[gg + h] = fma(zv[h], xin, dsum[gg + h]);
+                        }
+                        *reinterpret_cast<double2 *>(out + gg) = make_double2(zv[0], zv[1]);
+                    }
+                }
+                tc_fence_before_sync();
+                __syncthreads(); // accumulator read, the stage's A and X free
+                const int mn = m + 2 * stride;
+                pending[stg] = mn < items;
+                if (tid == 0 && mn < items)
+                    issue(mn, stg);
+            }
+            if (!ok && tid == 0)
+            {
+                // Leave nothing in flight: the MMAs and the bulk copies (bounded, default limit).
+                if (mma_pending)
+                    for (long long i = 0; i < MBAR_SPIN_LIMIT; ++i)
+                        if (mbar_try_wait(mma_bar, mphase))
+                            break;
+                mbar_drain(tma_bar, pending, {tphase[0], tphase[1]});
+            }
+            flush(cat);
+            tc_fence_before_sync();
+            __syncthreads();
+            if (w == 0)
+            {
+                tc_fence_after_sync();
+                tmem_dealloc(taddr, 32);
+            }
+            // CTA sums (warps in order) into the first warp's slots, then the grid sum.
+            double *cta = amax_s; // free now: 3 G doubles
+            if (tid < 3 * G)
+            {
+                double s = 0.0;
+                for (int ww = 0; ww < 4; ++ww)
+                    s += wsum[ww * 3 * G + tid];
+                cta[tid] = s;
+            }
+            __shared__ double totals[3 * G];
+            if (grid_reduce_cta<3 * G, TC_THREADS>(cta, red.rz_parts, &grp->counter[4], totals) && tid == 0)
+            {
+                const double Lc = (double)cfg.level_num;
+                int all_done = 1;
+                for (int gg = 0; gg < G; ++gg)
+                {
+                    PcgState *sg = st + gg;
+                    if (!sg->done)
+                    {
+                        sg->rz_coarse = totals[2 * G + gg] + Lc * totals[G + gg];
+                        pcg_finalize(sg, cfg, MODE, totals[gg] + totals[G + gg] + sg->rz_coarse, 0.0);
+                        if (sg->error)
+                            grp->error = sg->error;
+                    }
+                    all_done &= sg->done ? 1 : 0;
+                }
+                grp->iter = MODE == 1 ? 0 : grp->iter + 1;
+                if (all_done || grp->error)
+                    grp->done = 1;
+            }
+        }
+
         // Coarse levels above the first from its components rc (level 0 of the coarse vector).
         // Each real node of level l sums its (at most 32) children of level l - 1 in a warp
         // (lane = child, in increasing order; deterministic). With three or more levels one CTA
@@ -1363,6 +1675,12 @@ namespace pmas
                        "wide apply smem attribute");
             cuda_check(cudaFuncSetAttribute(k_mas_apply_w<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
                        "wide apply smem attribute");
+            cuda_check(cudaFuncSetAttribute(k_mas_apply_tc<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            TcLayout::BYTES),
+                       "tcgen05 apply smem attribute");
+            cuda_check(cudaFuncSetAttribute(k_mas_apply_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            TcLayout::BYTES),
+                       "tcgen05 apply smem attribute");
         }
     }
 
@@ -1434,6 +1752,37 @@ namespace pmas
         else
             k_mas_apply_w<2><<<grid, L::WARPS * 32, smem, s>>>(mas, r, z, st, red, cfg);
         cuda_check(cudaGetLastError(), "wide apply launch");
+    }
+
+    size_t tc_storage_bytes(const MasView &mas) { return (size_t)(mas.banks + mas.total_coarse) * TC_MAT_BYTES; }
+
+    void launch_inv_to_tc(const MasView &mas, void *out, cudaStream_t s)
+    {
+        if (mas.bd != 3 || mas.storage != STORE_F16)
+            throw Error(ERR_INVALID, "[MAS] the tcgen05 apply needs block_dim 3 and fp16 inverses");
+        const int mats = mas.banks + mas.total_coarse;
+        if (mats > 0)
+            k_inv_to_tc<<<mats, 256, 0, s>>>(static_cast<const __half *>(mas.inv), static_cast<__half *>(out));
+        cuda_check(cudaGetLastError(), "tc storage launch");
+    }
+
+    void launch_mas_apply_tc(const MasView &mas, const void *inv_tc_v, const double *r, double *z, PcgState *st,
+                             ReduceBuf red, PcgConfig cfg, int mode, cudaStream_t s)
+    {
+        const __half *inv_tc = static_cast<const __half *>(inv_tc_v);
+        if (mas.bd != 3 || mas.storage != STORE_F16 || !inv_tc)
+            throw Error(ERR_INVALID, "[MAS] the tcgen05 apply needs block_dim 3, fp16 inverses and the tc storage");
+        const int items = mas.banks + mas.n_coarse_active;
+        int grid = 2 * device_sm_count(); // two CTAs per SM (81 KB of shared memory each)
+        grid = grid > items ? items : grid;
+        grid = grid > red.capacity ? red.capacity : grid;
+        grid = grid < 1 ? 1 : grid;
+        const size_t smem = TcLayout::BYTES;
+        if (mode == 1)
+            k_mas_apply_tc<1><<<grid, TC_THREADS, smem, s>>>(mas, inv_tc, r, z, st, red, cfg);
+        else
+            k_mas_apply_tc<2><<<grid, TC_THREADS, smem, s>>>(mas, inv_tc, r, z, st, red, cfg);
+        cuda_check(cudaGetLastError(), "tcgen05 apply launch");
     }
 
     void launch_mas_apply(const MasView &mas, const double *r, double *z, PcgState *st, ReduceBuf red, PcgConfig cfg,

@@ -69,6 +69,10 @@ namespace
         // Right-hand sides per group of several-right-hand-side solves: 0 = 16 for more than four
         // right-hand sides with block_dim 3, else 4; or 4 / 16 explicitly.
         int rhs_group = 0;
+        // Sixteen-right-hand-side MAS apply: warp tensor cores (mma.sync, binary16 upper-triangle
+        // storage) or the fifth-generation tensor cores (tcgen05.mma into tensor memory, from a full
+        // binary16 copy of the inverses built on first use after each factorization).
+        bool wide_tc = false;
     };
 
     const char *status_string(int s)
@@ -117,7 +121,7 @@ namespace
                                 "lazy_partitioning", "use_preconditioned_residual_norm", "precision",
                                 "true_residual_period", "check_period", "initial_guess", "beta", "ordering",
                                 "poll_period", "profile_kernels", "cuda_graphs", "preconditioner_refresh",
-                                "device_wait_limit", "rhs_group", "chained_launch"};
+                                "device_wait_limit", "rhs_group", "chained_launch", "wide_apply"};
 
     // MASSolverImpl::set_parameters (MASSolver.cu:198-212) plus the extension keys.
     void apply_mas_params(Params &p, const Json &m, bool strict)
@@ -197,6 +201,13 @@ namespace
             q.graphs = get_bool(*v, "cuda_graphs");
         if (auto *v = m.find("chained_launch"))
             q.chained = get_bool(*v, "chained_launch");
+        if (auto *v = m.find("wide_apply"))
+        {
+            const std::string w = get_str(*v, "wide_apply");
+            if (w != "mma_sync" && w != "tcgen05")
+                throw Error(ERR_INVALID, "[MAS] wide_apply must be \"mma_sync\" or \"tcgen05\"");
+            q.wide_tc = (w == "tcgen05");
+        }
         if (auto *v = m.find("poll_period"))
         {
             q.poll_period = get_int(*v, "poll_period");
@@ -564,6 +575,7 @@ struct mas_solver
         auto tp = t0;
         factorize_phases.clear();
         ws_graph_valid = false; // the neighbour weights follow the values
+        inv_tc_valid = false;   // so does the tcgen05 copy of the inverses
         auto phase = [&](const char *name) {
             const auto now = std::chrono::steady_clock::now();
             factorize_phases.emplace_back(name, std::chrono::duration<double, std::milli>(now - tp).count());
@@ -1294,6 +1306,26 @@ struct mas_solver
     // Group width w (RHS_GROUP or RHS_WIDE) of the several-right-hand-side buffers and kernels.
     int gwidth = RHS_GROUP;
     bool wide() const { return gwidth == RHS_WIDE; }
+    // The tcgen05 apply's copy of the inverses (valid until the next factorization).
+    DevBuf<unsigned char> inv_tc;
+    bool inv_tc_valid = false;
+
+    void ensure_tc_storage(const MasView &mv)
+    {
+        if (inv_tc_valid)
+            return;
+        inv_tc.alloc(tc_storage_bytes(mv), "MAS tc inverse storage");
+        launch_inv_to_tc(mv, inv_tc.get(), stream);
+        inv_tc_valid = true;
+    }
+
+    void launch_wide_apply(const MasView &mv, const PcgConfig &cfg, int mode)
+    {
+        if (p.wide_tc)
+            launch_mas_apply_tc(mv, inv_tc.get(), gr.get(), gz.get(), gst.get(), red_g(), cfg, mode, stream);
+        else
+            launch_mas_apply_w(mv, gr.get(), gz.get(), gst.get(), red_g(), cfg, mode, stream);
+    }
     int red_capacity_g() const { return wide() ? wide_reduce_ctas() : red_capacity; }
 
     void alloc_multi(int width = RHS_GROUP)
@@ -1343,7 +1375,7 @@ struct mas_solver
                 run("restrict", 0, [&] { return launch_restrict_w(mv, gr.get(), grp, P, stream); });
             }
             run("coarse_levels", 0, [&] { return launch_coarse_levels_w(mv, grp, stream); });
-            run("mas_apply", 1, [&] { launch_mas_apply_w(mv, gr.get(), gz.get(), S, red_g(), cfg, 2, stream); });
+            run("mas_apply", 1, [&] { launch_wide_apply(mv, cfg, 2); });
             run("update_p", 1, [&] { launch_update_p_w(mv, gp.get(), gz.get(), S, 0, stream); });
             return;
         }
@@ -1411,6 +1443,8 @@ struct mas_solver
         mix((uint64_t)cfg.use_prec_norm);
         mix((uint64_t)cfg.wait_limit);
         mix((uint64_t)gwidth);
+        mix((uint64_t)p.wide_tc);
+        mix((uint64_t)(uintptr_t)inv_tc.get());
         uint64_t bits;
         std::memcpy(&bits, &cfg.rel_tol, 8);
         mix(bits);
@@ -1448,13 +1482,15 @@ struct mas_solver
             hinit[g].done = 1;
         cuda_check(cudaMemcpyAsync(S, hinit.data(), sizeof(PcgState) * (W + 1), cudaMemcpyHostToDevice, stream),
                    "state");
+        if (wide() && p.wide_tc)
+            ensure_tc_storage(mv);
         if (wide())
         {
             run("spmv_residual", 1,
                 [&] { launch_spmv_w(SPMV_RESIDUAL, Av, gx.get(), gr.get(), gb.get(), S, red_g(), 0, 0, stream); });
             run("restrict", 0, [&] { return launch_restrict_w(mv, gr.get(), S + W, 0, stream); });
             run("coarse_levels", 0, [&] { return launch_coarse_levels_w(mv, S + W, stream); });
-            run("mas_apply", 1, [&] { launch_mas_apply_w(mv, gr.get(), gz.get(), S, red_g(), cfg, 1, stream); });
+            run("mas_apply", 1, [&] { launch_wide_apply(mv, cfg, 1); });
             run("update_p", 1, [&] { launch_update_p_w(mv, gp.get(), gz.get(), S, 1, stream); });
         }
         else

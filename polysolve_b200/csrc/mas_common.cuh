@@ -341,6 +341,107 @@ namespace pmas
                      : "memory");
     }
 
+    // Arm a barrier for `bytes` of transactions (one arrival), then issue copies completing on it.
+    __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes)
+    {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                     : "memory");
+    }
+
+    // Global -> shared bulk copy completing on `bar` (armed separately); 16-byte aligned, multiple of 16.
+    __device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+    {
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                         smem_addr(dst)),
+                     "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                     : "memory");
+    }
+
+    __device__ __forceinline__ void bulk_copy_g2s_hint(void *dst, const void *src, uint32_t bytes, uint64_t *bar,
+                                                       uint64_t policy)
+    {
+        asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], "
+                     "%2, [%3], %4;" ::"r"(smem_addr(dst)),
+                     "l"(src), "r"(bytes), "r"(smem_addr(bar)), "l"(policy)
+                     : "memory");
+    }
+
+    // ---------------------------------------------------------------------------------------
+    // Fifth-generation tensor cores (tcgen05): tensor-memory allocation, MMA with both operands in
+    // shared memory, completion through an mbarrier, and loads of the accumulator.
+    // ---------------------------------------------------------------------------------------
+    // Allocate `cols` (power of two >= 32) tensor-memory columns; warp-wide. The address lands in
+    // *slot (shared memory).
+    __device__ __forceinline__ void tmem_alloc(uint32_t *slot, uint32_t cols)
+    {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(slot)),
+                     "r"(cols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+
+    __device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t cols)
+    {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(cols) : "memory");
+    }
+
+    __device__ __forceinline__ void tc_fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+    __device__ __forceinline__ void tc_fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+    // Shared-memory matrix descriptor, no swizzle: core matrices of 8 rows x 16 bytes (rows 16 bytes
+    // apart); lbo = bytes between the two 8-element halves of a 16-element K step, sbo = bytes
+    // between consecutive 8-row groups along M (or N). Version field 1 (bit 46).
+    __device__ __forceinline__ uint64_t tc_smem_desc(const void *p, uint32_t lbo, uint32_t sbo)
+    {
+        const uint32_t a = smem_addr(p);
+        return (uint64_t)((a >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+               ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+    }
+
+    // Instruction descriptor of kind::f16: binary16 A and B (both K-major), FP32 accumulator, M x N.
+    __host__ __device__ constexpr uint32_t tc_idesc_f16_f32(int m, int n)
+    {
+        return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+    }
+
+    // D (tensor memory) = A B^T (+ D when accumulate); issued by one thread.
+    __device__ __forceinline__ void tc_mma_f16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                               bool accumulate)
+    {
+        const uint32_t acc = accumulate ? 1u : 0u, zero = 0u;
+        asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n" ::"r"(d_tmem),
+                     "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc), "r"(zero)
+                     : "memory");
+    }
+
+    // Arrive on `bar` once every MMA issued so far by this thread has completed.
+    __device__ __forceinline__ void tc_commit(uint64_t *bar)
+    {
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         smem_addr(bar))
+                     : "memory");
+    }
+
+    // 16 consecutive FP32 columns of this thread's tensor-memory lane (warp w reads lanes
+    // 32 (w % 4) ..); completes at tc_wait_ld().
+    __device__ __forceinline__ void tc_ld16(uint32_t taddr, float (&v)[16])
+    {
+        uint32_t r[16];
+        asm volatile("tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+                     "%12, %13, %14, %15}, [%16];"
+                     : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                       "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                       "=r"(r[14]), "=r"(r[15])
+                     : "r"(taddr)
+                     : "memory");
+#pragma unroll
+        for (int i = 0; i < 16; ++i)
+            v[i] = __uint_as_float(r[i]);
+    }
+
+    __device__ __forceinline__ void tc_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
     __device__ __forceinline__ double2 ld_stream_f64x2(const double *p, uint64_t pol)
     {
         double2 v;

@@ -408,6 +408,13 @@ namespace pmas
     int launch_coarse_levels_w(const MasView &mas, const PcgState *grp, cudaStream_t s);
     void launch_mas_apply_w(const MasView &mas, const double *r, double *z0, PcgState *st, ReduceBuf red,
                             PcgConfig cfg, int mode, cudaStream_t s);
+    // The same on the fifth-generation tensor cores (tcgen05.mma, accumulator in tensor memory) from
+    // the "tc" storage of the inverses (full binary16 matrices in the canonical operand layout),
+    // built from the mma16 storage by launch_inv_to_tc into tc_storage_bytes(mas) bytes.
+    size_t tc_storage_bytes(const MasView &mas);
+    void launch_inv_to_tc(const MasView &mas, void *out, cudaStream_t s);
+    void launch_mas_apply_tc(const MasView &mas, const void *inv_tc, const double *r, double *z, PcgState *st,
+                             ReduceBuf red, PcgConfig cfg, int mode, cudaStream_t s);
     void launch_permute_in_w(int n, int V, int cols, const int *padded_of_block, const double *B, double *dst,
                              size_t dst_len, cudaStream_t s);
     void launch_permute_out_w(int n, int cols, const int *padded_of_block, const double *src, double *X,

@@ -106,11 +106,12 @@ def test_device_wait_timeout_is_reported_and_handle_recovers(precision, graphs):
     np.testing.assert_array_equal(x, x_ref)
 
 
-@pytest.mark.parametrize("group", [4, 16])
-def test_device_wait_timeout_several_right_hand_sides(group):
+@pytest.mark.parametrize("group,wide_apply", [(4, "mma_sync"), (16, "mma_sync"), (16, "tcgen05")])
+def test_device_wait_timeout_several_right_hand_sides(group, wide_apply):
     system = synthetic.elasticity(8, young_sigma=1.0, jitter=0.2, seed=52)
     B = synthetic.rhs(system.n, seed=52, count=4)
-    params = {"precision": "fp16", "check_period": 1, "true_residual_period": 50, "rhs_group": group}
+    params = {"precision": "fp16", "check_period": 1, "true_residual_period": 50, "rhs_group": group,
+              "wide_apply": wide_apply}
     s = _solver(system, params)
     s.factorize(system.scipy())
     X_ref = s.solve_multi(B)

@@ -112,6 +112,37 @@ def test_wide_and_narrow_groups_agree(contact_system):
         assert abs(i4[c] - i16[c]) <= 2
 
 
+@pytest.mark.parametrize("nrhs", [1, 6, 16])
+def test_tcgen05_wide_apply_matches_mma_sync(contact_system, nrhs):
+    """The sixteen-wide apply on the fifth-generation tensor cores (full binary16 inverses in the
+    tcgen05 operand layout, FP32 accumulation in tensor memory) is the same algorithm as the
+    mma.sync one: every column meets the tolerance, within 1e-6 of it, iteration counts within two;
+    repeated solves (graph replay) and solves after a refactorization give the same bits."""
+    system = contact_system
+    A = system.scipy()
+    B = np.stack([synthetic.rhs(system.n, seed=200 + c) for c in range(nrhs)])
+    sm = _solver(system, dict(CHOSEN, rhs_group=16))
+    st = _solver(system, dict(CHOSEN, rhs_group=16, wide_apply="tcgen05"))
+    Xm, Xt = sm.solve_multi(B), st.solve_multi(B)
+    im, it = sm.get_info()["rhs_iterations"], st.get_info()["rhs_iterations"]
+    assert all(v == "Reach relative tolerance" for v in st.get_info()["rhs_status"])
+    for c in range(nrhs):
+        assert np.linalg.norm(A @ Xt[c] - B[c]) <= 5e-8 * np.linalg.norm(B[c])
+        assert np.linalg.norm(Xt[c] - Xm[c]) <= 1e-6 * np.linalg.norm(Xm[c])
+        assert abs(im[c] - it[c]) <= 2
+    np.testing.assert_array_equal(st.solve_multi(B), Xt)
+    st.factorize(A)
+    np.testing.assert_array_equal(st.solve_multi(B), Xt)
+
+
+def test_wide_apply_is_validated():
+    from polysolve_b200 import MasError
+
+    s = Solver.create("MAS", "")
+    with pytest.raises(MasError):
+        s.set_parameters({"MAS": {"wide_apply": "wgmma"}})
+
+
 def test_rhs_group_is_validated():
     from polysolve_b200 import MasError
 
