@@ -1773,7 +1773,7 @@ namespace pmas
         if (mas.bd != 3 || mas.storage != STORE_F16 || !inv_tc)
             throw Error(ERR_INVALID, "[MAS] the tcgen05 apply needs block_dim 3, fp16 inverses and the tc storage");
         const int items = mas.banks + mas.n_coarse_active;
-        int grid = 2 * device_sm_count(); // two CTAs per SM (81 KB of shared memory each)
+        int grid = 2 * device_sm_count(); // two CTAs per SM (83 KB of shared memory each)
         grid = grid > items ? items : grid;
         grid = grid > red.capacity ? red.capacity : grid;
         grid = grid < 1 ? 1 : grid;
