@@ -514,7 +514,7 @@ def run_batch(args) -> None:
         "e2e": {"value": round(float(te[0].item()), 3), "unit": "ms/batch",
                 "h2d_bytes_per_step": int(8 * sum(ns)), "d2h_bytes_per_step": int(8 * sum(ns))},
         "gpu_launches": int(gpu_launches), "clocks": clk,
-        "autotune": {"poll_period": tuned["poll_period"], "threads": threads,
+        "autotune": {"poll_period": tuned["poll_period"], "spmv_unroll": tuned.get("spmv_unroll"), "threads": threads,
                      "tables": tuned.get("tables", {})},
     }
     if rank == 0:

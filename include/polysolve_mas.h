@@ -73,7 +73,10 @@ void mas_destroy(mas_solver *h);
  * once, which tests the timeout path), rhs_group (0 | 4 | 16: right-hand sides per group of
  * mas_solve_multi; 0 picks 16 for more than four with block_dim 3, else 4), chained_launch (bool,
  * default true: the single-right-hand-side PCG kernels use programmatic dependent launch, each
- * becoming resident while its predecessor drains; results are the same either way). */
+ * becoming resident while its predecessor drains; results are the same either way), spmv_unroll (1 |
+ * 2 | 4, default 2: block slots per loop trip of the SpMV, a launch shape the autotuner picks; the
+ * same bits either way), wide_apply ("mma_sync" | "tcgen05": tensor-core path of the sixteen-wide
+ * apply of mas_solve_multi). */
 int mas_set_parameters(mas_solver *h, const char *params_json);
 
 /* MASSolver::get_info (MASSolver.cu:214-219): writes a JSON object with solver_iter,

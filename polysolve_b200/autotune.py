@@ -1,9 +1,12 @@
 """Autotuner for the solver's launch-shape parameters, measured on the caller's own systems.
 
 The kernels' tile shapes are fixed by the data layout (a subdomain is a bank of 32 block rows, one
-warp; a subdomain matrix is 32 x block_dim rows), so what is tuned are the runtime choices that
-depend on the system sizes and the GPU:
+warp; a subdomain matrix is 32 x block_dim rows), so what is tuned are the launch shapes and
+runtime choices that depend on the system sizes and the GPU:
 
+* ``spmv_unroll`` - slots of the block SpMV per loop trip (1, 2 or 4; three compiled variants):
+  more slots keep more loads in flight per warp but cost registers (56, 80, 128) and so CTAs per
+  SM; small systems with few banks and large ones need different points.
 * ``poll_period`` - PCG iterations per replayed CUDA graph (and per host poll of the convergence
   flag): short graphs stop sooner after convergence, long ones cost fewer launches and polls.
   Small systems are launch-bound and prefer long graphs; large ones barely care.
@@ -52,18 +55,29 @@ def signature(ns) -> str:
     return "n=" + ",".join(str(n) for n in sorted(ns))
 
 
-def tune_poll_period(solvers, run, candidates=(5, 10, 20, 40), repeats: int = 3) -> dict:
-    """Sets ``poll_period`` on every solver to each candidate, times ``run()`` (which solves with
-    them), keeps the fastest and returns ``{"best": value, "ms": {candidate: median ms}}``."""
+def tune_param(solvers, run, key: str, candidates, repeats: int = 3) -> dict:
+    """Sets the integer parameter ``key`` on every solver to each candidate, times ``run()`` (which
+    solves with them), keeps the fastest and returns ``{"best": value, "ms": {candidate: median
+    ms}}`` with the best value left set."""
     table = {}
     for c in candidates:
         for s in solvers:
-            s.set_parameters({"MAS": {"poll_period": int(c)}})
+            s.set_parameters({"MAS": {key: int(c)}})
         table[int(c)] = _median_ms(run, repeats)
     best = min(table, key=table.get)
     for s in solvers:
-        s.set_parameters({"MAS": {"poll_period": best}})
+        s.set_parameters({"MAS": {key: best}})
     return {"best": best, "ms": table}
+
+
+def tune_poll_period(solvers, run, candidates=(5, 10, 20, 40), repeats: int = 3) -> dict:
+    """``tune_param`` for ``poll_period`` (iterations per replayed CUDA graph)."""
+    return tune_param(solvers, run, "poll_period", candidates, repeats)
+
+
+def tune_spmv_unroll(solvers, run, candidates=(1, 2, 4), repeats: int = 3) -> dict:
+    """``tune_param`` for ``spmv_unroll`` (slots of the block SpMV per loop trip)."""
+    return tune_param(solvers, run, "spmv_unroll", candidates, repeats)
 
 
 def tune_batch_threads(run_with_threads, candidates=(4, 8, 16, 32, 64), repeats: int = 3) -> dict:
@@ -74,11 +88,12 @@ def tune_batch_threads(run_with_threads, candidates=(4, 8, 16, 32, 64), repeats:
 
 
 def tune_batch(solvers, b_ptrs, x_ptrs, ns, *, cache_path: str | None = None, repeats: int = 3,
-               poll_candidates=(5, 10, 20, 40), thread_candidates=(4, 8, 16, 32, 64)) -> dict:
-    """Tunes ``poll_period`` (all solvers) and the host thread count of ``solve_batch_device`` for
-    these systems; returns ``{"poll_period": p, "threads": t, "tables": {...}, "cached": bool}``
-    and leaves ``poll_period`` set on the solvers. With ``cache_path`` a previous result for the
-    same sizes is reused."""
+               poll_candidates=(5, 10, 20, 40), unroll_candidates=(1, 2, 4),
+               thread_candidates=(4, 8, 16, 32, 64)) -> dict:
+    """Tunes ``poll_period`` and ``spmv_unroll`` (all solvers) and the host thread count of
+    ``solve_batch_device`` for these systems, one after another; returns ``{"poll_period": p,
+    "spmv_unroll": u, "threads": t, "tables": {...}, "cached": bool}`` and leaves both parameters
+    set on the solvers. With ``cache_path`` a previous result for the same sizes is reused."""
     from .solver import solve_batch_device
 
     key = signature(ns)
@@ -86,18 +101,20 @@ def tune_batch(solvers, b_ptrs, x_ptrs, ns, *, cache_path: str | None = None, re
     if key in cache:
         res = dict(cache[key], cached=True)
         for s in solvers:
-            s.set_parameters({"MAS": {"poll_period": int(res["poll_period"])}})
+            s.set_parameters({"MAS": {"poll_period": int(res["poll_period"]),
+                                      "spmv_unroll": int(res.get("spmv_unroll", 2))}})
         return res
     threads0 = min(32, max(1, len(solvers)))
-    poll = tune_poll_period(solvers, lambda: solve_batch_device(solvers, b_ptrs, x_ptrs, ns, threads=threads0),
-                            poll_candidates, repeats)
+    run0 = lambda: solve_batch_device(solvers, b_ptrs, x_ptrs, ns, threads=threads0)  # noqa: E731
+    poll = tune_poll_period(solvers, run0, poll_candidates, repeats)
+    unroll = tune_spmv_unroll(solvers, run0, unroll_candidates, repeats)
     thr = tune_batch_threads(lambda t: solve_batch_device(solvers, b_ptrs, x_ptrs, ns, threads=t),
                              [t for t in thread_candidates if t <= max(1, len(solvers))] or [1], repeats)
-    res = {"poll_period": poll["best"], "threads": thr["best"],
-           "tables": {"poll_period_ms": poll["ms"], "threads_ms": thr["ms"]}}
+    res = {"poll_period": poll["best"], "spmv_unroll": unroll["best"], "threads": thr["best"],
+           "tables": {"poll_period_ms": poll["ms"], "spmv_unroll_ms": unroll["ms"], "threads_ms": thr["ms"]}}
     cache[key] = res
     _store_cache(cache_path, cache)
     return dict(res, cached=False)
 
 
-__all__ = ["tune_poll_period", "tune_batch_threads", "tune_batch", "signature"]
+__all__ = ["tune_param", "tune_poll_period", "tune_spmv_unroll", "tune_batch_threads", "tune_batch", "signature"]

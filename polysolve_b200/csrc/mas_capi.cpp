@@ -73,6 +73,8 @@ namespace
         // storage) or the fifth-generation tensor cores (tcgen05.mma into tensor memory, from a full
         // binary16 copy of the inverses built on first use after each factorization).
         bool wide_tc = false;
+        // Slots per loop trip of the SpMV (1, 2, 4): a launch-shape choice for the autotuner.
+        int spmv_unroll = 2;
     };
 
     const char *status_string(int s)
@@ -121,7 +123,7 @@ namespace
                                 "lazy_partitioning", "use_preconditioned_residual_norm", "precision",
                                 "true_residual_period", "check_period", "initial_guess", "beta", "ordering",
                                 "poll_period", "profile_kernels", "cuda_graphs", "preconditioner_refresh",
-                                "device_wait_limit", "rhs_group", "chained_launch", "wide_apply"};
+                                "device_wait_limit", "rhs_group", "chained_launch", "wide_apply", "spmv_unroll"};
 
     // MASSolverImpl::set_parameters (MASSolver.cu:198-212) plus the extension keys.
     void apply_mas_params(Params &p, const Json &m, bool strict)
@@ -201,6 +203,12 @@ namespace
             q.graphs = get_bool(*v, "cuda_graphs");
         if (auto *v = m.find("chained_launch"))
             q.chained = get_bool(*v, "chained_launch");
+        if (auto *v = m.find("spmv_unroll"))
+        {
+            q.spmv_unroll = get_int(*v, "spmv_unroll");
+            if (q.spmv_unroll != 1 && q.spmv_unroll != 2 && q.spmv_unroll != 4)
+                throw Error(ERR_INVALID, "[MAS] spmv_unroll must be 1, 2 or 4");
+        }
         if (auto *v = m.find("wide_apply"))
         {
             const std::string w = get_str(*v, "wide_apply");
@@ -866,6 +874,7 @@ struct mas_solver
         mix((uint64_t)cfg.polak_ribiere);
         mix((uint64_t)cfg.wait_limit);
         mix((uint64_t)chained_launch());
+        mix((uint64_t)spmv_unroll());
         uint64_t bits;
         std::memcpy(&bits, &cfg.rel_tol, 8);
         mix(bits);
@@ -901,6 +910,7 @@ struct mas_solver
                 ks.second = KStat{};
         keep_stats = false;
         set_chained_launch(p.chained);
+        set_spmv_unroll(p.spmv_unroll);
         launch_pcg_init_state(S, stream);
         // r = b - A x, rr0, the level-0 restriction of r, then z = M^-1 r
         run("spmv_residual", 1, [&] { launch_spmv(SPMV_RESIDUAL, Av, x.get(), r.get(), b.get(), S, red(), 0, 0, stream); });

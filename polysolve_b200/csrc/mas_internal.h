@@ -333,6 +333,9 @@ namespace pmas
     // predecessor drains. On by default; per calling thread (mas_pcg.cu).
     void set_chained_launch(bool on);
     bool chained_launch();
+    // Slots per loop trip of the single-right-hand-side SpMV (1, 2 or 4); per calling thread.
+    void set_spmv_unroll(int u);
+    int spmv_unroll();
 
     // mas_spmv.cu
     enum SpmvMode : int

@@ -71,6 +71,9 @@ namespace pmas
     static thread_local bool t_chained_launch = true;
     void set_chained_launch(bool on) { t_chained_launch = on; }
     bool chained_launch() { return t_chained_launch; }
+    static thread_local int t_spmv_unroll = 2;
+    void set_spmv_unroll(int u) { t_spmv_unroll = u; }
+    int spmv_unroll() { return t_spmv_unroll; }
 
     namespace
     {

@@ -19,13 +19,12 @@ namespace pmas
     {
         constexpr int SPMV_THREADS = 256;
         constexpr int BANKS_PER_CTA = SPMV_THREADS / 32;
-        // Slots unrolled per loop trip (loads of both in flight; measured best of 1, 2, 4).
-        constexpr int SPMV_UNROLL = 2;
 
-        // Minimum one CTA per SM: the compiler then keeps both unrolled slots' loads in flight
-        // (80 registers, 3 CTAs per SM), measured faster than the occupancy-first 44-register
-        // build at 1.6 M DOF.
-        template <int BD, int MODE>
+        // UNROLL slots per loop trip, their loads in flight together (the spmv_unroll parameter:
+        // 1, 2 or 4; 2 measured best at 1.6 M DOF). Minimum one CTA per SM: the compiler then keeps
+        // the unrolled slots' loads in flight (80 registers at 2, 3 CTAs per SM), measured faster
+        // than the occupancy-first 44-register build at 1.6 M DOF.
+        template <int BD, int MODE, int UNROLL = 2>
         __global__ void __launch_bounds__(SPMV_THREADS, 1) k_spmv(BankedView A, const double *__restrict__ x,
                                                                double *__restrict__ y, const double *__restrict__ b,
                                                                PcgState *st, ReduceBuf red, int iter, int period)
@@ -55,7 +54,7 @@ namespace pmas
                 // The matrix streams through L2 with evict-first priority (x, the gathered vector,
                 // and the other PCG vectors stay resident); two slots' loads in flight per lane.
                 const uint64_t pol = l2_evict_first_policy();
-#pragma unroll SPMV_UNROLL
+#pragma unroll UNROLL
                 for (int k = 0; k < len; ++k)
                 {
                     const int col = ld_stream_s32(cp + (long long)k * 32, pol);
@@ -149,19 +148,29 @@ namespace pmas
             if (mode != SPMV_PLAIN && grid > red.capacity)
                 throw Error(ERR_INVALID, "[MAS] reduction scratch too small");
             const bool ch = chained_launch();
-            switch (mode)
-            {
-            case SPMV_PLAIN:
-                k_spmv<BD, SPMV_PLAIN><<<grid, SPMV_THREADS, 0, s>>>(A, x, y, b, st, red, iter, period);
-                break;
-            case SPMV_PAP:
-                launch_chained(ch, k_spmv<BD, SPMV_PAP>, grid, SPMV_THREADS, 0, s, A, x, y, b, st, red, iter, period);
-                break;
-            default:
-                launch_chained(ch, k_spmv<BD, SPMV_RESIDUAL>, grid, SPMV_THREADS, 0, s, A, x, y, b, st, red, iter,
-                               period);
-                break;
-            }
+            auto go = [&]<int U>() {
+                switch (mode)
+                {
+                case SPMV_PLAIN:
+                    k_spmv<BD, SPMV_PLAIN, U><<<grid, SPMV_THREADS, 0, s>>>(A, x, y, b, st, red, iter, period);
+                    break;
+                case SPMV_PAP:
+                    launch_chained(ch, k_spmv<BD, SPMV_PAP, U>, grid, SPMV_THREADS, 0, s, A, x, y, b, st, red, iter,
+                                   period);
+                    break;
+                default:
+                    launch_chained(ch, k_spmv<BD, SPMV_RESIDUAL, U>, grid, SPMV_THREADS, 0, s, A, x, y, b, st, red,
+                                   iter, period);
+                    break;
+                }
+            };
+            const int u = spmv_unroll();
+            if (u == 1)
+                go.template operator()<1>();
+            else if (u == 4)
+                go.template operator()<4>();
+            else
+                go.template operator()<2>();
             cuda_check(cudaGetLastError(), "spmv launch");
         }
         struct VecPtrs

@@ -37,3 +37,26 @@ def test_cache_round_trip(tmp_path):
     autotune._store_cache(str(path), cache)
     assert autotune._load_cache(str(path)) == cache
     assert autotune.signature([10, 30]) == autotune.signature([30, 10])
+
+
+def test_spmv_unroll_picks_the_fastest_and_leaves_it_set():
+    solvers = [FakeSolver(), FakeSolver()]
+    cost = {1: 0.02, 2: 0.012, 4: 0.004}
+
+    def run():
+        time.sleep(cost[solvers[0].params["spmv_unroll"]])
+
+    res = autotune.tune_spmv_unroll(solvers, run, repeats=2)
+    assert res["best"] == 4 and set(res["ms"]) == {1, 2, 4}
+    assert all(s.params["spmv_unroll"] == 4 for s in solvers)
+
+
+def test_cached_result_sets_both_parameters(tmp_path, monkeypatch):
+    path = tmp_path / "tune.json"
+    ns = [100, 200]
+    autotune._store_cache(str(path), {autotune.signature(ns): {"poll_period": 40, "spmv_unroll": 1, "threads": 8,
+                                                                "tables": {}}})
+    solvers = [FakeSolver(), FakeSolver()]
+    res = autotune.tune_batch(solvers, [0, 0], [0, 0], ns, cache_path=str(path))
+    assert res["cached"] and res["threads"] == 8
+    assert all(s.params == {"poll_period": 40, "spmv_unroll": 1} for s in solvers)

@@ -438,6 +438,25 @@ def test_chained_launch_bit_identical(precision):
         assert it == out[0][1]
 
 
+def test_spmv_unroll_variants_bit_identical():
+    """The SpMV's slots per loop trip (1, 2, 4: compiled variants the autotuner chooses between)
+    only change how many loads are in flight; every row still sums its slots in order."""
+    system = synthetic.elasticity(10, young_sigma=1.0, jitter=0.2, seed=16, contact_pairs=60)
+    b = synthetic.rhs(system.n, 16)
+    out = []
+    for u in (1, 2, 4):
+        s = make_solver(system, 3, {"precision": "fp16", "true_residual_period": 5, "check_period": 1,
+                                    "spmv_unroll": u})
+        x = np.zeros(system.n)
+        s.solve(b, x)
+        out.append((x, s.get_info()["solver_iter"]))
+    for x, it in out[1:]:
+        np.testing.assert_array_equal(x, out[0][0])
+        assert it == out[0][1]
+    with pytest.raises(MasError):
+        Solver.create("MAS", "").set_parameters({"MAS": {"spmv_unroll": 3}})
+
+
 @pytest.mark.parametrize("ordering", ["morton", "natural"])
 def test_isolated_rows_with_general_blocks(ordering):
     """Isolated block rows (no off-diagonal block) with non-identity SPD diagonal blocks. With a
