@@ -594,13 +594,15 @@ def run_contact16(args) -> None:
     Xo = sv.solve_multi(B)
     other_ms = (time.perf_counter() - t0) * 1000.0
     other_worst = max(float(np.linalg.norm(A @ Xo[c] - B[c]) / np.linalg.norm(B[c])) for c in range(R))
-    apply_us = {}
+    apply_us, kernel_us = {}, {}
     for variant in ("mma_sync", "tcgen05"):
         sv.set_parameters({"MAS": {"wide_apply": variant, "profile_kernels": True}})
         sv.solve_multi(B)
         pinf = sv.get_info()
         km, kl = pinf.get("kernel_ms", {}), pinf.get("kernel_launches", {})
         apply_us[variant] = round(1000.0 * km.get("mas_apply", 0.0) / max(1, kl.get("mas_apply", 1)), 2)
+        if variant == args.wide_apply:
+            kernel_us = {k: round(1000.0 * km[k] / max(1, kl.get(k, 1)), 2) for k in km if kl.get(k)}
     sv.set_parameters({"MAS": {"wide_apply": args.wide_apply, "profile_kernels": False}})
     # FP64 reference solutions (CHOLMOD is unavailable on this box): plain FP64 MAS-PCG to a
     # relative residual of 1e-11 (FP64 PCG stalls near 3e-12 here) for every right-hand side; the
@@ -635,6 +637,7 @@ def run_contact16(args) -> None:
         "wide_apply": args.wide_apply,
         "other_wide_apply": {"variant": other, "ms": round(other_ms, 3), "worst_relative_residual": other_worst},
         "apply_us_per_launch": apply_us,
+        "kernel_us_per_launch": kernel_us,
         "one_by_one_ms": round(float(t[1].item()), 3),
         "speedup_vs_one_by_one": round(float(t[1].item()) / float(t[0].item()), 3),
         "e2e": {"value": round(value, 3), "unit": "ms/16 RHS", "h2d_bytes_per_step": int(8 * n * R),
