@@ -807,7 +807,7 @@ struct mas_solver
             run("restrict", 0, [&] { return launch_restrict(mv, r.get(), S, P, stream); });
         }
         apply_levels(mv, cfg, 2);
-        run("update_p", 1, [&] { launch_update_p(mv, pv.get(), z.get(), S, 0, stream); });
+        run("update_p", 1, [&] { launch_update_p(mv, x.get(), pv.get(), z.get(), S, 0, stream); });
     }
 
     void drop_graph()
@@ -916,7 +916,7 @@ struct mas_solver
         run("spmv_residual", 1, [&] { launch_spmv(SPMV_RESIDUAL, Av, x.get(), r.get(), b.get(), S, red(), 0, 0, stream); });
         run("restrict", 0, [&] { return launch_restrict(mv, r.get(), S, 0, stream); });
         apply_levels(mv, cfg, 1);
-        run("update_p", 1, [&] { launch_update_p(mv, pv.get(), z.get(), S, 1, stream); });
+        run("update_p", 1, [&] { launch_update_p(mv, x.get(), pv.get(), z.get(), S, 1, stream); });
         cuda_check(cudaMemcpyAsync(&h_st[0], S, sizeof(PcgState), cudaMemcpyDeviceToHost, stream), "state");
         cuda_check(cudaStreamSynchronize(stream), "pcg init");
         rz0 = h_st[0].rz0;
@@ -1386,7 +1386,7 @@ struct mas_solver
             }
             run("coarse_levels", 0, [&] { return launch_coarse_levels_w(mv, grp, stream); });
             run("mas_apply", 1, [&] { launch_wide_apply(mv, cfg, 2); });
-            run("update_p", 1, [&] { launch_update_p_w(mv, gp.get(), gz.get(), S, 0, stream); });
+            run("update_p", 1, [&] { launch_update_p_w(mv, gx.get(), gp.get(), gz.get(), S, 0, stream); });
             return;
         }
         run("spmv_pap", 1, [&] { launch_spmv_g(SPMV_PAP, Av, gp.get(), gAp.get(), nullptr, S, red_g(), 1, 0, stream); });
@@ -1400,7 +1400,7 @@ struct mas_solver
         }
         run("coarse_levels", 0, [&] { return launch_coarse_levels_g(mv, stream); });
         run("mas_apply", 1, [&] { launch_mas_apply_g(mv, gr.get(), gz.get(), S, red_g(), cfg, 2, stream); });
-        run("update_p", 1, [&] { launch_update_p_g(mv, gp.get(), gz.get(), S, 0, stream); });
+        run("update_p", 1, [&] { launch_update_p_g(mv, gx.get(), gp.get(), gz.get(), S, 0, stream); });
     }
 
     void capture_g(int slot, const BankedView &Av, const MasView &mv, const PcgConfig &cfg, int P, int chunk,
@@ -1501,7 +1501,7 @@ struct mas_solver
             run("restrict", 0, [&] { return launch_restrict_w(mv, gr.get(), S + W, 0, stream); });
             run("coarse_levels", 0, [&] { return launch_coarse_levels_w(mv, S + W, stream); });
             run("mas_apply", 1, [&] { launch_wide_apply(mv, cfg, 1); });
-            run("update_p", 1, [&] { launch_update_p_w(mv, gp.get(), gz.get(), S, 1, stream); });
+            run("update_p", 1, [&] { launch_update_p_w(mv, gx.get(), gp.get(), gz.get(), S, 1, stream); });
         }
         else
         {
@@ -1510,7 +1510,7 @@ struct mas_solver
             run("restrict", 0, [&] { return launch_restrict_g(mv, gr.get(), S + W, 0, stream); });
             run("coarse_levels", 0, [&] { return launch_coarse_levels_g(mv, stream); });
             run("mas_apply", 1, [&] { launch_mas_apply_g(mv, gr.get(), gz.get(), S, red_g(), cfg, 1, stream); });
-            run("update_p", 1, [&] { launch_update_p_g(mv, gp.get(), gz.get(), S, 1, stream); });
+            run("update_p", 1, [&] { launch_update_p_g(mv, gx.get(), gp.get(), gz.get(), S, 1, stream); });
         }
         cuda_check(cudaMemcpyAsync(hs.data(), S, sizeof(PcgState) * (W + 1), cudaMemcpyDeviceToHost, stream), "state");
         cuda_check(cudaStreamSynchronize(stream), "pcg init");
@@ -2320,7 +2320,7 @@ extern "C" int mas_debug_apply_multi(mas_solver *h, const double *rin, double *z
         launch_restrict_g(mv, h->gr.get(), h->gst.get() + RHS_GROUP, 0, h->stream);
         launch_coarse_levels_g(mv, h->stream);
         launch_mas_apply_g(mv, h->gr.get(), h->gz.get(), h->gst.get(), h->red_g(), h->config(), 1, h->stream);
-        launch_update_p_g(mv, h->gp.get(), h->gz.get(), h->gst.get(), 1, h->stream);
+        launch_update_p_g(mv, h->gx.get(), h->gp.get(), h->gz.get(), h->gst.get(), 1, h->stream);
         cuda_check(cudaMemcpyAsync(zout, h->gp.get(), sizeof(double) * len, cudaMemcpyDeviceToHost, h->stream), "z");
         cuda_check(cudaStreamSynchronize(h->stream), "apply");
     });

@@ -269,6 +269,11 @@ namespace pmas
         int done;      // 1: converged / stopped; kernels return immediately
         int status;    // MAS_STATUS_*
         int error;     // device-detected error code (ERR_NONFINITE, ERR_TIMEOUT)
+        // x += alpha p runs in update_p (which reads p anyway) except on true-residual iterations:
+        // update_xr records the iteration it left the update for (x_defer; -1: none), update_p does
+        // it when x_defer is the finished iteration and x_applied is not, and the next SpMV p.Ap
+        // records x_applied = x_defer, so a replayed chunk after the stop never adds it twice.
+        int x_defer, x_applied;
         // Arrival tickets of the grid reductions: [0] SpMV p.Ap / initial residual, [1] update_xr,
         // [2] in-loop true residual, [4] MAS apply. The last CTA resets its ticket to zero.
         unsigned int counter[8];
@@ -356,8 +361,10 @@ namespace pmas
     // r -= alpha Ap, rr = r . r and the level-0 restriction of r into rc.
     void launch_update_xr(const MasView &mas, double *x, double *r, const double *p, const double *Ap, PcgState *st,
                           ReduceBuf red, int period, cudaStream_t s);
-    // p = z0 + prolongation(zc) + beta p (z0: level-0 part of z = M^-1 r)
-    void launch_update_p(const MasView &mas, double *p, const double *z0, PcgState *st, int first, cudaStream_t s);
+    // x += alpha p (deferred from update_xr, see PcgState::x_defer); p = z0 + prolongation(zc) + beta p
+    // (z0: level-0 part of z = M^-1 r)
+    void launch_update_p(const MasView &mas, double *x, double *p, const double *z0, PcgState *st, int first,
+                         cudaStream_t s);
     void launch_permute_in(int n, int bd, int V, const int *padded_of_block, const double *src, double *dst,
                            size_t dst_len, cudaStream_t s);
     void launch_permute_out(int n, int bd, int V, const int *padded_of_block, const double *src, double *dst,
@@ -385,7 +392,8 @@ namespace pmas
                        ReduceBuf red, int iter, int period, cudaStream_t s);
     void launch_update_xr_g(const MasView &mas, double *x, double *r, const double *p, const double *Ap,
                             PcgState *st, ReduceBuf red, int period, cudaStream_t s);
-    void launch_update_p_g(const MasView &mas, double *p, const double *z0, PcgState *st, int first, cudaStream_t s);
+    void launch_update_p_g(const MasView &mas, double *x, double *p, const double *z0, PcgState *st, int first,
+                           cudaStream_t s);
     int launch_restrict_g(const MasView &mas, const double *r, const PcgState *grp, int period, cudaStream_t s);
     int launch_coarse_levels_g(const MasView &mas, cudaStream_t s);
     void launch_mas_apply_g(const MasView &mas, const double *r, double *z0, PcgState *st, ReduceBuf red,
@@ -406,7 +414,8 @@ namespace pmas
                        ReduceBuf red, int iter, int period, cudaStream_t s);
     void launch_update_xr_w(const MasView &mas, double *x, double *r, const double *p, const double *Ap,
                             PcgState *st, ReduceBuf red, int period, cudaStream_t s);
-    void launch_update_p_w(const MasView &mas, double *p, const double *z0, PcgState *st, int first, cudaStream_t s);
+    void launch_update_p_w(const MasView &mas, double *x, double *p, const double *z0, PcgState *st, int first,
+                           cudaStream_t s);
     int launch_restrict_w(const MasView &mas, const double *r, const PcgState *grp, int period, cudaStream_t s);
     int launch_coarse_levels_w(const MasView &mas, const PcgState *grp, cudaStream_t s);
     void launch_mas_apply_w(const MasView &mas, const double *r, double *z0, PcgState *st, ReduceBuf red,

@@ -30,6 +30,9 @@ namespace pmas
             constexpr int BS = BD * BD;
             constexpr int PAIRS = BS / 2;
             PcgState *grp = st + G;
+            // The previous iteration's update_p has run: its deferred x update is applied.
+            if (MODE == SPMV_PAP && blockIdx.x == 0 && threadIdx.x == 0)
+                grp->x_applied = grp->x_defer;
             if (grp->done)
                 return;
             if (MODE == SPMV_RESIDUAL && period > 0 && (grp->iter + 1) % period != 0)
@@ -167,6 +170,8 @@ namespace pmas
             for (int g = 0; g < G; ++g)
                 alpha[g] = st[g].alpha;
             const bool due = period > 0 && (grp->iter + 1) % period == 0;
+            if (blockIdx.x == 0 && threadIdx.x == 0)
+                grp->x_defer = due ? -1 : grp->iter + 1; // x += alpha p otherwise runs in update_p
             const int lane = threadIdx.x & 31;
             const int total_warps = gridDim.x * (MT / 32);
             const bool restrict_r = !due && mas.level_num > 0;
@@ -181,11 +186,13 @@ namespace pmas
 #pragma unroll
                 for (int t = 0; t < BDG; ++t)
                 {
-                    xv[t] = x[b0 + t * 32];
-                    pv[t] = p[b0 + t * 32];
-                    av[t] = 0.0;
-                    rv[t] = 0.0;
-                    if (!due)
+                    xv[t] = pv[t] = av[t] = rv[t] = 0.0;
+                    if (due)
+                    {
+                        xv[t] = x[b0 + t * 32];
+                        pv[t] = p[b0 + t * 32];
+                    }
+                    else
                     {
                         av[t] = Ap[b0 + t * 32];
                         rv[t] = r[b0 + t * 32];
@@ -196,7 +203,8 @@ namespace pmas
                 {
                     const int g = (t * 32 + lane) % G; // G divides 32: g = lane % G
                     const double a = alpha[g];
-                    x[b0 + t * 32] = fma(a, pv[t], xv[t]);
+                    if (due)
+                        x[b0 + t * 32] = fma(a, pv[t], xv[t]);
                     if (!due)
                     {
                         rv[t] = fma(-a, av[t], rv[t]);
@@ -220,22 +228,27 @@ namespace pmas
                         st[g].rr = tot[g];
         }
 
+        // x_g += alpha_g p_g when update_xr left it (PcgState::x_defer);
         // p_g = z0_g + prolongation(zc_g) + beta_g p_g (first: p = z).
         template <int BD>
-        __global__ void __launch_bounds__(MT) k_update_p_g(MasView mas, double *__restrict__ p,
+        __global__ void __launch_bounds__(MT) k_update_p_g(MasView mas, double *__restrict__ x, double *__restrict__ p,
                                                           const double *__restrict__ z0, const PcgState *st,
                                                           int first)
         {
             constexpr int BDG = BD * G;
-            if (st[G].done)
+            const PcgState *grp = st + G;
+            const int it = grp->iter;
+            const bool xdo = !first && grp->x_defer == it && grp->x_applied != it;
+            if (grp->done && !xdo)
                 return;
-            double beta[G];
+            double beta[G], alpha[G];
             bool skip[G];
 #pragma unroll
             for (int g = 0; g < G; ++g)
             {
                 beta[g] = first ? 0.0 : st[g].beta;
-                skip[g] = st[g].done != 0;
+                alpha[g] = st[g].alpha;
+                skip[g] = st[g].done != 0 || grp->done != 0;
             }
             const int lane = threadIdx.x & 31;
             const double *__restrict__ zc = mas.zc;
@@ -245,7 +258,7 @@ namespace pmas
                 return;
             const long long b0 = (long long)bank * 32 * BDG;
             const bool iso = bank >= mas.first_iso_bank;
-            double zv[BDG], pold[BDG];
+            double zv[BDG], pold[BDG], xv[BDG];
             int4 cs[BDG];
 #pragma unroll
             for (int t = 0; t < BDG; ++t)
@@ -253,8 +266,21 @@ namespace pmas
                 const int e = t * 32 + lane; // node-local value: node * BDG + component * G + g
                 zv[t] = z0[b0 + e];
                 pold[t] = first ? 0.0 : p[b0 + e];
+                xv[t] = xdo ? x[b0 + e] : 0.0;
                 cs[t] = iso ? make_int4(-1, -1, -1, -1) : mas.cslot[(long long)bank * 32 + e / BDG];
             }
+            if (xdo)
+#pragma unroll
+                for (int t = 0; t < BDG; ++t)
+                {
+                    const int g = (t * 32 + lane) % G;
+                    double a = 0.0;
+#pragma unroll
+                    for (int h = 0; h < G; ++h)
+                        if (h == g)
+                            a = alpha[h];
+                    x[b0 + t * 32 + lane] = fma(a, pold[t], xv[t]);
+                }
 #pragma unroll
             for (int t = 0; t < BDG; ++t)
             {
@@ -391,12 +417,13 @@ namespace pmas
         cuda_check(cudaGetLastError(), "multi update_xr launch");
     }
 
-    void launch_update_p_g(const MasView &mas, double *p, const double *z0, PcgState *st, int first, cudaStream_t s)
+    void launch_update_p_g(const MasView &mas, double *x, double *p, const double *z0, PcgState *st, int first,
+                           cudaStream_t s)
     {
         const int grid = (mas.banks + MT / 32 - 1) / (MT / 32);
         if (grid == 0)
             return;
-        by_bd(mas.bd, [&]<int BD>() { k_update_p_g<BD><<<grid, MT, 0, s>>>(mas, p, z0, st, first); });
+        by_bd(mas.bd, [&]<int BD>() { k_update_p_g<BD><<<grid, MT, 0, s>>>(mas, x, p, z0, st, first); });
         cuda_check(cudaGetLastError(), "multi update_p launch");
     }
 

@@ -11,11 +11,12 @@
 //                  8 lanes read the same address) and the x gathers read 16 contiguous doubles per
 //                  column and component. Per-right-hand-side p.Ap / r.r (and b.b) by a deterministic
 //                  grid sum; alpha of every right-hand side in the last CTA.
-//   k_update_xr_w  x += alpha_g p ; r -= alpha_g Ap ; r.r per g ; the level-0 restriction of r,
+//   k_update_xr_w  r -= alpha_g Ap ; r.r per g ; the level-0 restriction of r (x += alpha_g p only on
+//                  true-residual iterations; otherwise in k_update_p_w, see PcgState::x_defer),
 //                  summed per bank component in shared memory in node order (48 values per node and
 //                  component: 3 components x 16 right-hand sides; within a step of 32 values no two
 //                  lanes touch the same sum).
-//   k_update_p_w   p_g = z0_g + prolongation(zc_g) + beta_g p_g.
+//   k_update_p_w   x_g += alpha_g p_g (deferred) ; p_g = z0_g + prolongation(zc_g) + beta_g p_g.
 //   k_restrict_w   the restriction alone (initial residual, true-residual iterations).
 //
 // One matrix pass serves all sixteen right-hand sides; the MAS apply of the group (every inverse
@@ -104,6 +105,9 @@ namespace pmas
         {
             extern __shared__ __align__(16) unsigned char sp_smem[];
             PcgState *grp = st + G;
+            // The previous iteration's update_p has run: its deferred x update is applied.
+            if (MODE == SPMV_PAP && blockIdx.x == 0 && threadIdx.x == 0)
+                grp->x_applied = grp->x_defer;
             if (grp->done)
                 return;
             if (MODE == SPMV_RESIDUAL && period > 0 && (grp->iter + 1) % period != 0)
@@ -346,6 +350,8 @@ namespace pmas
             const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
             const double a = st[lane & (G - 1)].alpha;
             const bool due = period > 0 && (grp->iter + 1) % period == 0;
+            if (blockIdx.x == 0 && threadIdx.x == 0)
+                grp->x_defer = due ? -1 : grp->iter + 1;
             const bool restrict_r = !due && mas.level_num > 0;
             double *acc = xr_acc + (size_t)w * 32 * VN;
             double part = 0.0;
@@ -363,8 +369,8 @@ namespace pmas
                     for (int j = 0; j < 4; ++j)
                     {
                         const long long e = b0 + (t0 + j) * 32 + lane;
-                        xv[j] = x[e];
-                        pv[j] = p[e];
+                        xv[j] = due ? x[e] : 0.0;
+                        pv[j] = due ? p[e] : 0.0;
                         av[j] = due ? 0.0 : Ap[e];
                         rv[j] = due ? 0.0 : r[e];
                     }
@@ -372,7 +378,8 @@ namespace pmas
                     for (int j = 0; j < 4; ++j)
                     {
                         const int el = (t0 + j) * 32 + lane;
-                        x[b0 + el] = fma(a, pv[j], xv[j]);
+                        if (due)
+                            x[b0 + el] = fma(a, pv[j], xv[j]);
                         if (!due)
                         {
                             rv[j] = fma(-a, av[j], rv[j]);
@@ -436,11 +443,15 @@ namespace pmas
         }
 
         // p_g = z0_g + sum_l zc_g[cslot_l(node)] + beta_g p_g (first: p = z); a warp per bank.
-        __global__ void __launch_bounds__(WT_) k_update_p_w(MasView mas, double *__restrict__ p,
+        __global__ void __launch_bounds__(WT_) k_update_p_w(MasView mas, double *__restrict__ x,
+                                                            double *__restrict__ p,
                                                             const double *__restrict__ z0, const PcgState *st,
                                                             int first)
         {
-            if (st[G].done)
+            const PcgState *grp = st + G;
+            const int it = grp->iter;
+            const bool xdo = !first && grp->x_defer == it && grp->x_applied != it;
+            if (grp->done && !xdo)
                 return;
             const int lane = threadIdx.x & 31;
             const int bank = blockIdx.x * WW + (threadIdx.x >> 5);
@@ -448,14 +459,15 @@ namespace pmas
                 return;
             const int g = lane & (G - 1);
             const double beta = first ? 0.0 : st[g].beta;
-            const bool skip = st[g].done != 0;
+            const double a = st[g].alpha;
+            const bool skip = st[g].done != 0 || grp->done != 0;
             const double *__restrict__ zc = mas.zc;
             const double iso_scale = 1.0 + mas.level_num;
             const bool iso = bank >= mas.first_iso_bank;
             const long long b0 = (long long)bank * 32 * VN;
             for (int t0 = 0; t0 < VN; t0 += 4)
             {
-                double zv[4], po[4];
+                double zv[4], po[4], xv[4];
                 int4 cs[4];
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
@@ -463,8 +475,13 @@ namespace pmas
                     const int el = (t0 + j) * 32 + lane;
                     zv[j] = z0[b0 + el];
                     po[j] = first ? 0.0 : p[b0 + el];
+                    xv[j] = xdo ? x[b0 + el] : 0.0;
                     cs[j] = iso ? make_int4(-1, -1, -1, -1) : mas.cslot[(long long)bank * 32 + el / VN];
                 }
+                if (xdo)
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                        x[b0 + (t0 + j) * 32 + lane] = fma(a, po[j], xv[j]);
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
                 {
@@ -594,11 +611,12 @@ namespace pmas
         cuda_check(cudaGetLastError(), "wide update_xr launch");
     }
 
-    void launch_update_p_w(const MasView &mas, double *p, const double *z0, PcgState *st, int first, cudaStream_t s)
+    void launch_update_p_w(const MasView &mas, double *x, double *p, const double *z0, PcgState *st, int first,
+                           cudaStream_t s)
     {
         const int grid = (mas.banks + WW - 1) / WW;
         if (grid > 0)
-            k_update_p_w<<<grid, WT_, 0, s>>>(mas, p, z0, st, first);
+            k_update_p_w<<<grid, WT_, 0, s>>>(mas, x, p, z0, st, first);
         cuda_check(cudaGetLastError(), "wide update_p launch");
     }
 

@@ -2,10 +2,11 @@
 //
 // The reference runs each vector step as its own launch (axpby / inner_product / scalar_division,
 // MASSolver.cu:46-81, InnerProduct.cu:16-45) with a memset and an FP64 atomicAdd per dot. Here:
-//   update_xr: x += alpha p ; r -= alpha Ap ; rr = r . r ; level-0 restriction of r  (one pass;
-//              on true-residual iterations only x, then r = b - A x follows in the SpMV)
-//   update_p:  p = z0 + P zc + beta p             (the MAS prolongation fused in; beta from the
-//                                                  device state, set by the MAS apply)
+//   update_xr: r -= alpha Ap ; rr = r . r ; level-0 restriction of r  (one pass; on true-residual
+//              iterations only x += alpha p, then r = b - A x follows in the SpMV)
+//   update_p:  x += alpha p (the iteration's x update, moved here: this pass reads p anyway);
+//              p = z0 + P zc + beta p    (the MAS prolongation fused in; beta from the device
+//                                         state, set by the MAS apply)
 // alpha / beta are read from the device-resident PcgState, and every dot is a deterministic
 // two-stage reduction, so no host round trip is needed inside the iteration.
 
@@ -79,10 +80,11 @@ namespace pmas
     {
         constexpr int UPD_THREADS = 256;
 
-        // x += alpha p ; r -= alpha Ap ; rr = r . r (ticket: the last CTA sums the partials) ; and
-        // the level-0 restriction of the new r (per-bank component sums, the MAS apply's first
-        // step). One warp per bank, its 32 * BD values read coalesced (value t * 32 + lane). On a
-        // true-residual iteration only x is updated: r, rr and the restriction follow the SpMV.
+        // r -= alpha Ap ; rr = r . r (ticket: the last CTA sums the partials) ; and the level-0
+        // restriction of the new r (per-bank component sums, the MAS apply's first step); x +=
+        // alpha p is left to update_p (st->x_defer). One warp per bank, its 32 * BD values read
+        // coalesced (value t * 32 + lane). On a true-residual iteration only x is updated here:
+        // r, rr and the restriction follow the SpMV.
         template <int BD>
         __global__ void __launch_bounds__(UPD_THREADS) k_update_xr(MasView mas, double *__restrict__ x,
                                                                    double *__restrict__ r, const double *__restrict__ p,
@@ -94,6 +96,8 @@ namespace pmas
                 return;
             const double alpha = st->alpha;
             const bool due = period > 0 && (st->iter + 1) % period == 0;
+            if (blockIdx.x == 0 && threadIdx.x == 0)
+                st->x_defer = due ? -1 : st->iter + 1;
             const int lane = threadIdx.x & 31;
             const int total_warps = gridDim.x * (UPD_THREADS / 32);
             const bool restrict_r = !due && mas.level_num > 0;
@@ -106,11 +110,13 @@ namespace pmas
 #pragma unroll
                 for (int t = 0; t < BD; ++t)
                 {
-                    xv[t] = x[b0 + t * 32];
-                    pv[t] = p[b0 + t * 32];
-                    av[t] = 0.0;
-                    rv[t] = 0.0;
-                    if (!due)
+                    xv[t] = pv[t] = av[t] = rv[t] = 0.0;
+                    if (due)
+                    {
+                        xv[t] = x[b0 + t * 32];
+                        pv[t] = p[b0 + t * 32];
+                    }
+                    else
                     {
                         av[t] = Ap[b0 + t * 32];
                         rv[t] = r[b0 + t * 32];
@@ -119,8 +125,9 @@ namespace pmas
 #pragma unroll
                 for (int t = 0; t < BD; ++t)
                 {
-                    x[b0 + t * 32] = fma(alpha, pv[t], xv[t]);
-                    if (!due)
+                    if (due)
+                        x[b0 + t * 32] = fma(alpha, pv[t], xv[t]);
+                    else
                     {
                         rv[t] = fma(-alpha, av[t], rv[t]);
                         r[b0 + t * 32] = rv[t];
@@ -138,15 +145,22 @@ namespace pmas
                 st->rr = tot[0];
         }
 
-        // p = z0 + sum_l zc[cslot_l(node)] + beta p; warps stride over banks, coalesced.
+        // x += alpha p when update_xr left it (see PcgState::x_defer), also on the iteration that
+        // stops the solve; p = z0 + sum_l zc[cslot_l(node)] + beta p; warps stride over banks,
+        // coalesced.
         template <int BD>
-        __global__ void __launch_bounds__(UPD_THREADS) k_update_p(MasView mas, double *__restrict__ p,
+        __global__ void __launch_bounds__(UPD_THREADS) k_update_p(MasView mas, double *__restrict__ x,
+                                                                  double *__restrict__ p,
                                                                   const double *__restrict__ z0, const PcgState *st,
                                                                   int first)
         {
             pdl_wait();
-            if (st->done)
+            const int it = st->iter;
+            const bool xdo = !first && st->x_defer == it && st->x_applied != it;
+            const bool pdo = !st->done;
+            if (!xdo && !pdo)
                 return;
+            const double alpha = st->alpha;
             const double beta = first ? 0.0 : st->beta;
             const int lane = threadIdx.x & 31;
             const int total_warps = gridDim.x * (UPD_THREADS / 32);
@@ -162,23 +176,36 @@ namespace pmas
                     for (int t = 0; t < BD; ++t)
                     {
                         const long long idx = b0 + t * 32 + lane;
-                        const double v = iso_scale * z0[idx];
-                        p[idx] = first ? v : fma(beta, p[idx], v);
+                        const double po = first ? 0.0 : p[idx];
+                        if (xdo)
+                            x[idx] = fma(alpha, po, x[idx]);
+                        if (pdo)
+                        {
+                            const double v = iso_scale * z0[idx];
+                            p[idx] = first ? v : fma(beta, po, v);
+                        }
                     }
                     continue;
                 }
-                // Loads first (z0, p and the coarse slots), then the coarse-value gathers.
-                double zv[BD], pold[BD];
+                // Loads first (z0, p, x and the coarse slots), then the coarse-value gathers.
+                double zv[BD], pold[BD], xv[BD];
                 int4 cs[BD];
 #pragma unroll
                 for (int t = 0; t < BD; ++t)
                 {
                     const int e = t * 32 + lane;
                     const int node = e / BD;
-                    zv[t] = z0[b0 + e];
+                    zv[t] = pdo ? z0[b0 + e] : 0.0;
                     pold[t] = first ? 0.0 : p[b0 + e];
-                    cs[t] = mas.cslot[(long long)bank * 32 + node];
+                    xv[t] = xdo ? x[b0 + e] : 0.0;
+                    cs[t] = pdo ? mas.cslot[(long long)bank * 32 + node] : make_int4(-1, -1, -1, -1);
                 }
+                if (xdo)
+#pragma unroll
+                    for (int t = 0; t < BD; ++t)
+                        x[b0 + t * 32 + lane] = fma(alpha, pold[t], xv[t]);
+                if (!pdo)
+                    continue;
 #pragma unroll
                 for (int t = 0; t < BD; ++t)
                 {
@@ -304,12 +331,13 @@ namespace pmas
         cuda_check(cudaGetLastError(), "update_xr launch");
     }
 
-    void launch_update_p(const MasView &mas, double *p, const double *z0, PcgState *st, int first, cudaStream_t s)
+    void launch_update_p(const MasView &mas, double *x, double *p, const double *z0, PcgState *st, int first,
+                         cudaStream_t s)
     {
         auto go = [&](auto kernel) {
             const int grid = bank_grid_all(mas.banks);
             if (grid > 0)
-                launch_chained(chained_launch(), kernel, grid, UPD_THREADS, 0, s, mas, p, z0, st, first);
+                launch_chained(chained_launch(), kernel, grid, UPD_THREADS, 0, s, mas, x, p, z0, st, first);
         };
         if (mas.bd == 1)
             go(k_update_p<1>);

@@ -32,6 +32,9 @@ namespace pmas
             constexpr int BS = BD * BD;
             constexpr int PAIRS = BS / 2;
             pdl_wait();
+            // The previous iteration's update_p has run: its deferred x update is applied.
+            if (MODE == SPMV_PAP && blockIdx.x == 0 && threadIdx.x == 0)
+                st->x_applied = st->x_defer;
             if (MODE != SPMV_PLAIN && st->done)
                 return;
             // In-loop true residual: only every `period`-th iteration (iteration = st->iter + 1).
