@@ -106,6 +106,13 @@ int mas_set_positions(mas_solver *h, const double *xyz, int nverts);
  * is used (checked in the same host pass that hashes the pattern). */
 int mas_factorize_csc(mas_solver *h, int n, const int *outer, const int *inner, const double *vals, int nnz);
 
+/* New, no reference counterpart: a values-only refactorization the caller declares. vals are the
+ * new values in the CSC order of the last factorized matrix (same pattern, nnz of them); the row
+ * indices are neither passed nor read, so the pattern check (a hash of 4 bytes per entry) is
+ * skipped. Requires an earlier factorization with unchanged positions, ordering, block_dim and
+ * precision (otherwise MAS_ERR_INVALID; MAS_ERR_NOT_FACTORIZED before any factorization). */
+int mas_factorize_values(mas_solver *h, const double *vals, int nnz);
+
 /* MASSolver::solve(b, x) (MASSolver.cu:376-409): host vectors of length n. With initial_guess
  * "zero" (the reference's behaviour, MASSolver.cu:395-398) x is output only; with "input" x is
  * also the starting guess. Synchronous. Non-convergence is not an error: see get_info. */

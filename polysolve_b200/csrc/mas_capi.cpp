@@ -577,7 +577,10 @@ struct mas_solver
     }
 
     // MASSolverImpl::factorize (MASSolver.cu:292-374).
-    void factorize(int n_, const int *outer, const int *inner, const double *vals, long long nnz_)
+    // declared: a values-only refactorization the caller declares (mas_factorize_values): the
+    // pattern is the last factorization's, so the row indices are neither read nor hashed.
+    void factorize(int n_, const int *outer, const int *inner, const double *vals, long long nnz_,
+                   bool declared = false)
     {
         auto t0 = std::chrono::steady_clock::now();
         auto tp = t0;
@@ -590,9 +593,16 @@ struct mas_solver
             tp = now;
         };
         cuda_check(cudaSetDevice(device), "set device");
-        if (n_ <= 0 || !outer || !inner || !vals)
+        if (declared)
+        {
+            if (!factorized)
+                throw Error(ERR_NOT_FACTORIZED, "[MAS] factorize_values: no earlier factorization to reuse.");
+            if (!vals || n_ != n || nnz_ != nnz)
+                throw Error(ERR_INVALID, "[MAS] factorize_values: the values do not match the factorized pattern.");
+        }
+        else if (n_ <= 0 || !outer || !inner || !vals)
             throw Error(ERR_INVALID, "[MAS] factorize: invalid matrix arguments.");
-        if (outer[0] != 0 || (long long)outer[n_] != nnz_ || nnz_ < 0)
+        if (!declared && (outer[0] != 0 || (long long)outer[n_] != nnz_ || nnz_ < 0))
             throw Error(ERR_INVALID, "[MAS] factorize: outer index array is inconsistent with nnz.");
         if (nnz_ > 2147483647LL)
             throw Error(ERR_INVALID, "[MAS] A is too large. Non-zero number exceeding int32 max.");
@@ -606,18 +616,28 @@ struct mas_solver
         // cores between both, which oversubscribes them).
         const int upload_threads = std::max(1, std::min(8, omp_get_max_threads()));
         const int hash_threads = std::max(1, omp_get_max_threads() - upload_threads);
-        std::thread hasher([&] { h = pattern_hash(n_, outer, inner, nnz_, &pattern_ok, hash_threads); });
-        try
+        if (declared)
         {
+            h = pattern;
+            pattern_ok = true;
             refresh_vals.alloc(nnz_ > 0 ? nnz_ : 1, "MAS permuted_bsr input_csc");
             upload_pageable(refresh_vals.get(), vals, sizeof(double) * (size_t)nnz_);
         }
-        catch (...)
+        else
         {
+            std::thread hasher([&] { h = pattern_hash(n_, outer, inner, nnz_, &pattern_ok, hash_threads); });
+            try
+            {
+                refresh_vals.alloc(nnz_ > 0 ? nnz_ : 1, "MAS permuted_bsr input_csc");
+                upload_pageable(refresh_vals.get(), vals, sizeof(double) * (size_t)nnz_);
+            }
+            catch (...)
+            {
+                hasher.join();
+                throw;
+            }
             hasher.join();
-            throw;
         }
-        hasher.join();
         if (!pattern_ok)
             throw Error(ERR_INVALID, "[MAS] Invalid CSC: row index out of range or decreasing column pointers.");
         // The ordering is a pure function of the pattern, the positions and the ordering
@@ -629,7 +649,10 @@ struct mas_solver
         const bool rebuild_order = !(shape_same && (p.lazy || inputs_same));
         const bool same_pattern = factorized && !rebuild_order && h == pattern && nnz_ == nnz && bd_ == A.bd &&
                                   mas.storage == p.storage;
-        phase("pattern_check_and_upload");
+        if (declared && !same_pattern)
+            throw Error(ERR_INVALID, "[MAS] factorize_values: positions, ordering, block_dim or precision changed "
+                                     "since the last factorization; call factorize.");
+        phase(declared ? "upload" : "pattern_check_and_upload");
 
         if (rebuild_order)
         {
@@ -1992,6 +2015,13 @@ extern "C" int mas_factorize_csc(mas_solver *h, int n, const int *outer, const i
     if (!h)
         return MAS_ERR_INVALID;
     return guarded(h, [&] { h->factorize(n, outer, inner, vals, nnz); });
+}
+
+extern "C" int mas_factorize_values(mas_solver *h, const double *vals, int nnz)
+{
+    if (!h)
+        return MAS_ERR_INVALID;
+    return guarded(h, [&] { h->factorize(h->n, nullptr, nullptr, vals, nnz, true); });
 }
 
 extern "C" int mas_solve(mas_solver *h, const double *b, double *x, int n)

@@ -38,7 +38,7 @@ MAS_ERR_NO_DEVICE = 8
 
 EXPORTED_SYMBOLS = [
     "mas_create", "mas_create_json", "mas_destroy", "mas_set_parameters", "mas_get_info", "mas_name",
-    "mas_analyze_pattern", "mas_set_positions", "mas_factorize_csc", "mas_solve", "mas_solve_multi",
+    "mas_analyze_pattern", "mas_set_positions", "mas_factorize_csc", "mas_factorize_values", "mas_solve", "mas_solve_multi",
     "mas_solve_device", "mas_solve_batch", "mas_set_stream", "mas_spmv_dot_noalloc", "mas_last_error", "mas_get_sizes", "mas_get_ordering", "mas_order_blocks",
     "mas_get_coarse_map", "mas_get_inverses", "mas_debug_spmv", "mas_debug_apply", "mas_debug_apply_multi",
     "mas_debug_spmv_multi", "mas_set_warm_start_model", "mas_reset_warm_start", "mas_debug_warm_start",
@@ -85,6 +85,7 @@ def library() -> ctypes.CDLL:
         L.mas_analyze_pattern.argtypes = [vp, i, vp, vp, i, i]
         L.mas_set_positions.argtypes = [vp, vp, i]
         L.mas_factorize_csc.argtypes = [vp, i, vp, vp, vp, i]
+        L.mas_factorize_values.argtypes = [vp, vp, i]
         L.mas_solve.argtypes = [vp, vp, vp, i]
         L.mas_solve_multi.argtypes = [vp, vp, vp, i, i]
         L.mas_solve_device.argtypes = [vp, ctypes.c_void_p, ctypes.c_void_p, i]
@@ -294,6 +295,19 @@ class Solver:
         _check(library().mas_factorize_csc(self._h, n, outer.ctypes.data, inner.ctypes.data, vals.ctypes.data,
                                            int(inner.size)), self._h)
         self._n = n
+
+    def factorize_values(self, A) -> None:
+        """New: values-only refactorization declared by the caller. A is a matrix with the pattern
+        of the last factorized one (only its values are used) or the values array itself, in that
+        matrix's CSC order; the pattern check is skipped."""
+        if hasattr(A, "tocsc"):
+            vals = A.tocsc().data
+        elif hasattr(A, "vals"):
+            vals = A.vals
+        else:
+            vals = A
+        vals = np.ascontiguousarray(vals, dtype=np.float64)
+        _check(library().mas_factorize_values(self._h, vals.ctypes.data, int(vals.size)), self._h)
 
     def solve(self, b: np.ndarray, x: np.ndarray) -> None:
         """Solve A x = b; x (float64, contiguous) is written in place."""

@@ -113,3 +113,40 @@ def test_pipelined_value_upload_on_a_large_system():
         s.solve(bk, x)
         assert np.linalg.norm(A @ x - bk) <= 2e-8 * np.linalg.norm(bk)
     assert "mas_inverses" in s.get_info({})["factorize_phases_ms"]  # the second one was values-only
+
+
+def test_declared_values_only_refactorization():
+    """mas_factorize_values (values in the last matrix's CSC order, no row indices, no pattern
+    check) gives exactly the solve of factorize on the same matrix; it is refused before any
+    factorization, with a different nnz, and after the positions changed."""
+    from polysolve_b200 import MasError
+
+    s0, b0 = synthetic.workload_sequence60(0, seed=4, N=9)
+    s1, b1 = synthetic.workload_sequence60(1, seed=4, N=9)
+    A0, A1 = s0.scipy().tocsc(), s1.scipy().tocsc()
+    params = {"block_dim": 3, "relative_tolerance": 1e-8, "absolute_tolerance": 0.0, "precision": "fp16",
+              "true_residual_period": 50, "check_period": 1}
+
+    def solver():
+        s = Solver.create("MAS", "")
+        s.set_parameters({"MAS": params})
+        s.set_positions(s0.positions)
+        return s
+
+    ref, dec = solver(), solver()
+    with pytest.raises(MasError):
+        dec.factorize_values(A1)
+    ref.factorize(A0)
+    ref.factorize(A1)
+    dec.factorize(A0)
+    dec.factorize_values(A1)
+    assert "upload" in dec.get_info({})["factorize_phases_ms"]
+    x_ref, x = np.zeros(A1.shape[0]), np.zeros(A1.shape[0])
+    ref.solve(b1, x_ref)
+    dec.solve(b1, x)
+    np.testing.assert_array_equal(x, x_ref)
+    with pytest.raises(MasError):
+        dec.factorize_values(A1.data[:-1])
+    dec.set_positions(s0.positions + 1e-3)
+    with pytest.raises(MasError):
+        dec.factorize_values(A1)
