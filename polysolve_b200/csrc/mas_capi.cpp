@@ -922,7 +922,6 @@ struct mas_solver
         const MasView mv = mas.view();
         const PcgConfig cfg = config();
         PcgState *S = st.get();
-        const int nodes = banks * 32;
         cudaEvent_t e0, e1;
         cuda_check(cudaEventCreate(&e0), "event");
         cuda_check(cudaEventCreate(&e1), "event");

@@ -124,7 +124,7 @@ namespace pmas
     __host__ __device__ inline int tile_packed_size(int bd) { return 32 * bd * (32 * bd + 1) / 2; }
 
     // Position of element (row, col) of the symmetric matrix in tile-packed storage.
-    __host__ __device__ inline int tile_packed_index(int bd, int row, int col)
+    __host__ __device__ inline int tile_packed_index(int /*bd*/, int row, int col)
     {
         if (row > col)
         {
