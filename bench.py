@@ -80,6 +80,9 @@ def parse_args():
                     help="grid80: the headline 1.6 M DOF solve; batch64: 64 independent uneven systems; "
                          "contact16: the 80^3 mesh with 20,000 contact pairs and 16 right-hand sides; "
                          "sequence60: a 60^3 sequence (new values each step) with warm starts")
+    ap.add_argument("--batch-launch", default="auto", choices=["auto", "fused", "streams"],
+                    help="batch64: one launch per PCG phase for the batch, one stream per system, or the "
+                         "autotuner's pick")
     ap.add_argument("--wide-apply", default="mma_sync", choices=["mma_sync", "tcgen05"],
                     help="contact16: tensor-core path of the sixteen-wide MAS apply")
     ap.add_argument("--precision", default=CHOSEN["precision"], choices=["fp16", "fp32", "fp64"],
@@ -453,8 +456,10 @@ def run_batch(args) -> None:
             dist.barrier()
 
     # graph length and host threads for these systems (untimed)
-    tuned = autotune.tune_batch(solvers, bptr, xptr, ns, repeats=2)
+    modes = ("fused", "streams") if args.batch_launch == "auto" else (args.batch_launch,)
+    tuned = autotune.tune_batch(solvers, bptr, xptr, ns, repeats=2, launch_candidates=modes)
     threads = int(tuned["threads"])
+    launch_mode = tuned.get("batch_launch", "fused")
     for _ in range(max(args.warmup, 3)):
         solve_batch_device(solvers, bptr, xptr, ns, threads=threads)
     torch.cuda.synchronize()
@@ -506,7 +511,10 @@ def run_batch(args) -> None:
         "config": {"workload": f"64 systems, edges {min(edges)}..{max(edges)}, "
                                f"{sum(3 * (e + 1) ** 3 for e in edges)} DOF in total",
                    "parallelism": f"systems sharded over {world} GPU(s) by cost (LPT, imbalance "
-                                  f"{batch.imbalance(costs, plan):.3f}); per GPU one CUDA stream per system",
+                                  f"{batch.imbalance(costs, plan):.3f}); per GPU "
+                                  + ("one launch per PCG phase for each of "
+                                     f"{tuned.get('batch_groups') or 1} size group(s) of its systems"
+                                     if launch_mode == "fused" else "one CUDA stream per system"),
                    "chosen": f"{args.precision} MAS, true residual every 50, convergence test every iteration"},
         "sequential_ms": round(float(te[1].item()), 3),
         "speedup_vs_sequential": round(float(te[1].item()) / value, 3) if value > 0 else None,
@@ -514,8 +522,9 @@ def run_batch(args) -> None:
         "e2e": {"value": round(float(te[0].item()), 3), "unit": "ms/batch",
                 "h2d_bytes_per_step": int(8 * sum(ns)), "d2h_bytes_per_step": int(8 * sum(ns))},
         "gpu_launches": int(gpu_launches), "clocks": clk,
-        "autotune": {"poll_period": tuned["poll_period"], "spmv_unroll": tuned.get("spmv_unroll"), "threads": threads,
-                     "tables": tuned.get("tables", {})},
+        "autotune": {"batch_launch": launch_mode, "batch_groups": tuned.get("batch_groups"),
+                     "poll_period": tuned["poll_period"],
+                     "spmv_unroll": tuned.get("spmv_unroll"), "threads": threads, "tables": tuned.get("tables", {})},
     }
     if rank == 0:
         print(json.dumps(out), flush=True)

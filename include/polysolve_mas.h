@@ -76,7 +76,9 @@ void mas_destroy(mas_solver *h);
  * becoming resident while its predecessor drains; results are the same either way), spmv_unroll (1 |
  * 2 | 4, default 2: block slots per loop trip of the SpMV, a launch shape the autotuner picks; the
  * same bits either way), wide_apply ("mma_sync" | "tcgen05": tensor-core path of the sixteen-wide
- * apply of mas_solve_multi). */
+ * apply of mas_solve_multi), batch_launch ("fused" | "streams", default streams: how
+ * mas_solve_batch runs the handle, see there), batch_groups (0..64, default 0 = 1: fused groups of
+ * a batch). */
 int mas_set_parameters(mas_solver *h, const char *params_json);
 
 /* MASSolver::get_info (MASSolver.cu:214-219): writes a JSON object with solver_iter,
@@ -166,10 +168,15 @@ int mas_solve_multi(mas_solver *h, const double *B, double *X, int n, int nrhs);
 
 /* Batched solves of independent systems (the 64-system workload; no reference counterpart in
  * MASSolver, which solves one system per call): every handle must be factorized and distinct;
- * b[i], x[i] have length n[i] (host arrays, or device arrays when device_pointers != 0). Each
- * handle runs on its own CUDA stream from a pool of `threads` host threads (<= 0: one per
- * hardware thread, at most 64), so small systems overlap on the GPU. statuses (optional, count
- * entries) receives each handle's status; the return value is the first non-zero status. */
+ * b[i], x[i] have length n[i] (host arrays, or device arrays when device_pointers != 0).
+ * Fused (every handle with batch_launch "fused", graphs on, no profiling, no learned warm start,
+ * the same device, block_dim, precision, true_residual_period, poll_period, spmv_unroll and
+ * batch_groups): the systems are cut by size into batch_groups groups, and each PCG phase is one
+ * launch for all unfinished systems of a group, on the group's own stream; each system's results
+ * are bit-identical to mas_solve's. Otherwise each handle runs on its own CUDA stream. In both
+ * forms a pool of `threads` host threads (<= 0: one per hardware thread, at most 64) runs the
+ * per-handle steps. statuses (optional, count entries) receives each handle's status; the return
+ * value is the first non-zero status. */
 int mas_solve_batch(mas_solver *const *handles, int count, const double *const *b, double *const *x,
                     const int *n, int device_pointers, int threads, int *statuses);
 

@@ -10,9 +10,13 @@ runtime choices that depend on the system sizes and the GPU:
 * ``poll_period`` - PCG iterations per replayed CUDA graph (and per host poll of the convergence
   flag): short graphs stop sooner after convergence, long ones cost fewer launches and polls.
   Small systems are launch-bound and prefer long graphs; large ones barely care.
-* ``threads`` of ``solve_batch`` / ``solve_batch_device`` - host threads (one CUDA stream each)
-  driving a batch of independent systems: too few leave the GPU idle between small solves, too
-  many contend on the host.
+* ``batch_launch`` of ``solve_batch`` / ``solve_batch_device`` - one launch per PCG phase for each
+  group of systems ("fused") or one CUDA stream per system ("streams"); with "fused",
+  ``batch_groups`` - how many such groups (each on its own stream) the batch is cut into by size.
+* ``threads`` of ``solve_batch`` / ``solve_batch_device`` - host threads driving a batch of
+  independent systems (with "streams" one CUDA stream each: too few leave the GPU idle between
+  small solves, too many contend on the host; with "fused" they run the per-system input and
+  result steps).
 
 Each candidate is timed with the real call (synchronous, host clock) after one untimed call, the
 median of ``repeats`` runs is kept, and the fastest candidate wins. Results can be cached in a JSON
@@ -87,13 +91,28 @@ def tune_batch_threads(run_with_threads, candidates=(4, 8, 16, 32, 64), repeats:
     return {"best": best, "ms": table}
 
 
+def tune_batch_launch(solvers, run, candidates=("fused", "streams"), repeats: int = 3) -> dict:
+    """Times ``run()`` with each ``batch_launch`` mode set on every solver; keeps the fastest."""
+    table = {}
+    for c in candidates:
+        for s in solvers:
+            s.set_parameters({"MAS": {"batch_launch": c}})
+        table[c] = _median_ms(run, repeats)
+    best = min(table, key=table.get)
+    for s in solvers:
+        s.set_parameters({"MAS": {"batch_launch": best}})
+    return {"best": best, "ms": table}
+
+
 def tune_batch(solvers, b_ptrs, x_ptrs, ns, *, cache_path: str | None = None, repeats: int = 3,
                poll_candidates=(5, 10, 20, 40), unroll_candidates=(1, 2, 4),
-               thread_candidates=(4, 8, 16, 32, 64)) -> dict:
-    """Tunes ``poll_period`` and ``spmv_unroll`` (all solvers) and the host thread count of
-    ``solve_batch_device`` for these systems, one after another; returns ``{"poll_period": p,
-    "spmv_unroll": u, "threads": t, "tables": {...}, "cached": bool}`` and leaves both parameters
-    set on the solvers. With ``cache_path`` a previous result for the same sizes is reused."""
+               thread_candidates=(4, 8, 16, 32, 64), launch_candidates=("fused", "streams"),
+               group_candidates=(1, 2, 4, 8)) -> dict:
+    """Tunes ``batch_launch`` (with ``batch_groups`` when fused), ``poll_period`` and
+    ``spmv_unroll`` (all solvers) and the host thread count of ``solve_batch_device`` for these
+    systems, one after another; returns ``{"batch_launch": m, "batch_groups": g, "poll_period": p,
+    "spmv_unroll": u, "threads": t, "tables": {...}, "cached": bool}`` and leaves the parameters set
+    on the solvers. With ``cache_path`` a previous result for the same sizes is reused."""
     from .solver import solve_batch_device
 
     key = signature(ns)
@@ -102,19 +121,31 @@ def tune_batch(solvers, b_ptrs, x_ptrs, ns, *, cache_path: str | None = None, re
         res = dict(cache[key], cached=True)
         for s in solvers:
             s.set_parameters({"MAS": {"poll_period": int(res["poll_period"]),
-                                      "spmv_unroll": int(res.get("spmv_unroll", 2))}})
+                                      "spmv_unroll": int(res.get("spmv_unroll", 2)),
+                                      "batch_launch": str(res.get("batch_launch", "streams")),
+                                      "batch_groups": int(res.get("batch_groups", 0))}})
         return res
     threads0 = min(32, max(1, len(solvers)))
     run0 = lambda: solve_batch_device(solvers, b_ptrs, x_ptrs, ns, threads=threads0)  # noqa: E731
+    groups = {"best": 0, "ms": {}}
+    if "fused" in launch_candidates:
+        for s in solvers:
+            s.set_parameters({"MAS": {"batch_launch": "fused"}})
+        cands = [g for g in group_candidates if g <= max(1, len(solvers))] or [1]
+        groups = tune_param(solvers, run0, "batch_groups", cands, repeats)
+    launch = tune_batch_launch(solvers, run0, launch_candidates, repeats)
     poll = tune_poll_period(solvers, run0, poll_candidates, repeats)
     unroll = tune_spmv_unroll(solvers, run0, unroll_candidates, repeats)
     thr = tune_batch_threads(lambda t: solve_batch_device(solvers, b_ptrs, x_ptrs, ns, threads=t),
                              [t for t in thread_candidates if t <= max(1, len(solvers))] or [1], repeats)
-    res = {"poll_period": poll["best"], "spmv_unroll": unroll["best"], "threads": thr["best"],
-           "tables": {"poll_period_ms": poll["ms"], "spmv_unroll_ms": unroll["ms"], "threads_ms": thr["ms"]}}
+    res = {"batch_launch": launch["best"], "batch_groups": groups["best"], "poll_period": poll["best"],
+           "spmv_unroll": unroll["best"], "threads": thr["best"],
+           "tables": {"batch_groups_ms": groups["ms"], "batch_launch_ms": launch["ms"], "poll_period_ms": poll["ms"],
+                      "spmv_unroll_ms": unroll["ms"], "threads_ms": thr["ms"]}}
     cache[key] = res
     _store_cache(cache_path, cache)
     return dict(res, cached=False)
 
 
-__all__ = ["tune_param", "tune_poll_period", "tune_spmv_unroll", "tune_batch_threads", "tune_batch", "signature"]
+__all__ = ["tune_param", "tune_poll_period", "tune_spmv_unroll", "tune_batch_launch", "tune_batch_threads", "tune_batch",
+           "signature"]

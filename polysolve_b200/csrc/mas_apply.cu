@@ -305,11 +305,16 @@ namespace pmas
         // Work item m: m < banks -> level-0 matrix m (input r, output z0); otherwise coarse matrix
         // g = coarse_active[m - banks] (matrix banks + g, input rc, output zc, 32 coarse nodes
         // from g * 32). mode 0: plain apply; 1: initial PCG apply (rz0); 2: PCG iteration.
+        // prefetch_first: issue the first two inverse copies before waiting for the predecessor
+        // (a chained launch of one system); otherwise a finished solve returns before any copy
+        // (the batched launch, where most CTAs may belong to finished systems).
         template <int BD, class Store, int MODE>
-        __global__ void __launch_bounds__(ApplyLayout<BD, Store>::WARPS * 32)
-            k_mas_apply(MasView mas, const double *__restrict__ r, double *__restrict__ z0, PcgState *st,
-                        ReduceBuf red, PcgConfig cfg)
+        __device__ __forceinline__ void mas_apply_body(const MasView &mas, const double *__restrict__ r,
+                                                       double *__restrict__ z0, PcgState *st, const ReduceBuf &red,
+                                                       const PcgConfig &cfg, Cta cta, bool prefetch_first)
         {
+            if (!prefetch_first && MODE != 0 && st->done)
+                return;
             using L = ApplyLayout<BD, Store>;
             using Real = typename L::Real;
             constexpr int N = L::N, S = L::S, WARPS = L::WARPS;
@@ -327,8 +332,8 @@ namespace pmas
             const Store *__restrict__ inv = static_cast<const Store *>(mas.inv);
             const int banks = mas.banks;
             const int items = banks + mas.n_coarse_active;
-            const int total_warps = gridDim.x * WARPS;
-            const int gw = blockIdx.x * WARPS + w;
+            const int total_warps = cta.n * WARPS;
+            const int gw = cta.x * WARPS + w;
             int *errp = st ? &st->error : nullptr;
             const bool pr = (MODE == 2) && cfg.polak_ribiere;
             // Matrix index and input vector of an item (coarse vectors: g * N).
@@ -511,7 +516,7 @@ namespace pmas
             if (MODE == 0)
                 return;
             double tot[APPLY_PARTS];
-            if (grid_reduce<APPLY_PARTS, THREADS>(part, red.rz_parts, &st->counter[4], tot) && threadIdx.x == 0)
+            if (grid_reduce<APPLY_PARTS, THREADS>(part, red.rz_parts, &st->counter[4], tot, cta) && threadIdx.x == 0)
             {
                 // Isolated rows: z = (1 + L) z0, so their r.z is (1 + L) r.z0 -- r.z0 is in the
                 // level-0 sums, the coarse levels add L r.z0.
@@ -520,6 +525,28 @@ namespace pmas
                 st->rzx_coarse = tot[5] + Lc * tot[3];
                 pcg_finalize(st, cfg, MODE, tot[0] + tot[2] + st->rz_coarse, tot[1] + tot[3] + st->rzx_coarse);
             }
+        }
+
+        template <int BD, class Store, int MODE>
+        __global__ void __launch_bounds__(ApplyLayout<BD, Store>::WARPS * 32)
+            k_mas_apply(MasView mas, const double *__restrict__ r, double *__restrict__ z0, PcgState *st,
+                        ReduceBuf red, PcgConfig cfg)
+        {
+            mas_apply_body<BD, Store, MODE>(mas, r, z0, st, red, cfg, native_cta(), true);
+        }
+
+        // The apply of every system of a batch (MODE 1: initial, 2: iteration) in one launch.
+        template <int BD, class Store, int MODE>
+        __global__ void __launch_bounds__(ApplyLayout<BD, Store>::WARPS * 32) k_mas_apply_batch(BatchView v)
+        {
+            const int4 e = batch_entry(v, BPH_APPLY);
+            const BatchSystem &sy = v.sys[e.x];
+            const Cta cta{e.y, e.z};
+            const MasView mas = sy.mas;
+            const ReduceBuf red = sy.red;
+            const PcgConfig cfg = sy.cfg;
+            mas_apply_body<BD, Store, MODE>(mas, sy.r, sy.z, sy.st, red, cfg, cta,
+                                            false);
         }
 
         // ---- G right-hand sides at once (binary16 inverses only): the B operand's eight columns
@@ -1309,7 +1336,7 @@ namespace pmas
         }
 
         template <int BD>
-        __global__ void __launch_bounds__(LEVEL_THREADS) k_coarse_levels(MasView mas, const PcgState *st)
+        __device__ __forceinline__ void coarse_levels_body(const MasView &mas, const PcgState *st, Cta cta)
         {
             pdl_wait();
             if (st && st->done)
@@ -1320,7 +1347,7 @@ namespace pmas
             __shared__ int is_last;
             if (mas.level_num == 2)
             {
-                const int i = blockIdx.x * W + w;
+                const int i = cta.x * W + w;
                 if (i >= mas.real_count[1])
                     return;
                 double v[BD];
@@ -1331,8 +1358,8 @@ namespace pmas
                         mas.rc[((size_t)mas.coff[1] + i) * BD + c] = v[c];
                 return;
             }
-            // Level-2 node j = blockIdx.x; warp w: its w-th level-1 child.
-            const int j = blockIdx.x;
+            // Level-2 node j = cta.x; warp w: its w-th level-1 child.
+            const int j = cta.x;
             const int kb = mas.kid_ptr[2][j], ke = mas.kid_ptr[2][j + 1];
             if (kb + w < ke)
             {
@@ -1364,7 +1391,7 @@ namespace pmas
             if (threadIdx.x == 0)
             {
                 __threadfence(); // cumulative: orders this CTA's stores (seen at the barrier) first
-                is_last = atomicAdd(mas.ticket, 1u) == gridDim.x - 1;
+                is_last = atomicAdd(mas.ticket, 1u) == (unsigned)cta.n - 1;
             }
             __syncthreads();
             if (!is_last)
@@ -1381,6 +1408,22 @@ namespace pmas
             }
             if (threadIdx.x == 0)
                 *mas.ticket = 0u;
+        }
+
+        template <int BD>
+        __global__ void __launch_bounds__(LEVEL_THREADS) k_coarse_levels(MasView mas, const PcgState *st)
+        {
+            coarse_levels_body<BD>(mas, st, native_cta());
+        }
+
+        template <int BD>
+        __global__ void __launch_bounds__(LEVEL_THREADS) k_coarse_levels_batch(BatchView v)
+        {
+            const int4 e = batch_entry(v, BPH_COARSE);
+            const BatchSystem &sy = v.sys[e.x];
+            const Cta cta{e.y, e.z};
+            const MasView mas = sy.mas;
+            coarse_levels_body<BD>(mas, sy.st, cta);
         }
 
         // The coarse levels for nodes of NC components (the wide groups: 3 components x 16 right-hand
@@ -1488,10 +1531,9 @@ namespace pmas
         // Level-0 restriction of r (initial residual, true-residual iterations, plain applies).
         // With period > 0 it runs only on iterations st->iter + 1 that are multiples of period.
         template <int BD>
-        __global__ void __launch_bounds__(256) k_restrict(int banks, const double *__restrict__ r,
-                                                          const int *__restrict__ lcco0,
-                                                          const int *__restrict__ cco0_base, double *rc,
-                                                          const PcgState *st, int period)
+        __device__ __forceinline__ void restrict_body(int banks, const double *__restrict__ r,
+                                                      const int *__restrict__ lcco0, const int *__restrict__ cco0_base,
+                                                      double *rc, const PcgState *st, int period, Cta cta)
         {
             pdl_wait();
             if (st && st->done)
@@ -1499,7 +1541,7 @@ namespace pmas
             if (st && period > 0 && (st->iter + 1) % period != 0)
                 return;
             const int lane = threadIdx.x & 31;
-            const int bank = blockIdx.x * 8 + (threadIdx.x >> 5);
+            const int bank = cta.x * 8 + (threadIdx.x >> 5);
             if (bank >= banks)
                 return;
             const long long b0 = (long long)bank * 32 * BD;
@@ -1508,6 +1550,25 @@ namespace pmas
             for (int t = 0; t < BD; ++t)
                 reg[t] = r[b0 + t * 32 + lane];
             bank_restrict<BD>(reg, bank, lcco0, cco0_base, rc);
+        }
+
+        template <int BD>
+        __global__ void __launch_bounds__(256) k_restrict(int banks, const double *__restrict__ r,
+                                                          const int *__restrict__ lcco0,
+                                                          const int *__restrict__ cco0_base, double *rc,
+                                                          const PcgState *st, int period)
+        {
+            restrict_body<BD>(banks, r, lcco0, cco0_base, rc, st, period, native_cta());
+        }
+
+        template <int BD>
+        __global__ void __launch_bounds__(256) k_restrict_batch(BatchView v, int period)
+        {
+            const int4 e = batch_entry(v, BPH_RESTRICT);
+            const BatchSystem &sy = v.sys[e.x];
+            const Cta cta{e.y, e.z};
+            restrict_body<BD>(sy.mas.first_iso_bank, sy.r, sy.mas.lcco0, sy.mas.cco0_base, sy.mas.rc, sy.st, period,
+                              cta);
         }
 
         template <int BD>
@@ -1552,6 +1613,12 @@ namespace pmas
             cuda_check(cudaFuncSetAttribute(k_mas_apply<BD, Store, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                             smem),
                        "apply smem attribute");
+            cuda_check(cudaFuncSetAttribute(k_mas_apply_batch<BD, Store, 1>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                       "apply smem attribute");
+            cuda_check(cudaFuncSetAttribute(k_mas_apply_batch<BD, Store, 2>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, smem),
+                       "apply smem attribute");
         }
 
         template <int BD, class Store, int MODE>
@@ -1559,14 +1626,8 @@ namespace pmas
                                PcgConfig cfg, cudaStream_t s)
         {
             using L = ApplyLayout<BD, Store>;
-            const int sms = device_sm_count();
             const size_t smem = (size_t)L::WARPS * L::WARP_BYTES;
-            const int items = mas.banks + mas.n_coarse_active;
-            int grid = (items + L::WARPS - 1) / L::WARPS;
-            if (grid > sms)
-                grid = sms;
-            if (grid < 1)
-                grid = 1;
+            const int grid = mas_apply_grid(mas);
             if (MODE != 0 && grid > red.capacity)
                 throw Error(ERR_INVALID, "[MAS] reduction scratch too small");
             // Chained in the PCG loop only: the kernel reads inverses before pdl_wait(), and a plain
@@ -1634,23 +1695,93 @@ namespace pmas
         dispatch(bd, storage, [&]<int BD, class Store>() { prepare_variant<BD, Store>(); });
     }
 
-    int launch_restrict(const MasView &mas, const double *r, const PcgState *st, int period, cudaStream_t s)
+    int restrict_grid(const MasView &mas)
     {
         if (mas.first_iso_bank <= 0 || mas.level_num <= 0)
             return 0;
+        return (mas.first_iso_bank + 7) / 8;
+    }
+
+    int coarse_levels_grid(const MasView &mas)
+    {
+        if (mas.level_num <= 1 || mas.real_count[1] <= 0)
+            return 0;
+        const int grid = mas.level_num == 2 ? (mas.real_count[1] + LEVEL_THREADS / 32 - 1) / (LEVEL_THREADS / 32)
+                                            : mas.real_count[2];
+        return grid > 0 ? grid : 0;
+    }
+
+    // At least APPLY_ITEMS_PER_WARP items per warp: a warp's two-stage copy pipeline then runs a
+    // few items past its start-up latency (small systems, and the batched launch where the
+    // CTAs of many small systems share the SMs one after another).
+    constexpr int APPLY_ITEMS_PER_WARP = 4;
+
+    int mas_apply_grid(const MasView &mas)
+    {
+        return dispatch(mas.bd, mas.storage, [&]<int BD, class Store>() {
+            using L = ApplyLayout<BD, Store>;
+            const int sms = device_sm_count();
+            const int items = mas.banks + mas.n_coarse_active;
+            constexpr int PER_CTA = L::WARPS * APPLY_ITEMS_PER_WARP;
+            int grid = (items + PER_CTA - 1) / PER_CTA;
+            if (grid > sms)
+                grid = sms;
+            return grid < 1 ? 1 : grid;
+        });
+    }
+
+    void launch_restrict_batch(const BatchView &v, int bd, int total, int period, cudaStream_t s)
+    {
+        if (total <= 0)
+            return;
+        dispatch_bd(bd, [&]<int BD>() {
+            launch_chained(chained_launch(), k_restrict_batch<BD>, total, 256, 0, s, v, period);
+        });
+        cuda_check(cudaGetLastError(), "batched restrict launch");
+    }
+
+    void launch_coarse_levels_batch(const BatchView &v, int bd, int total, cudaStream_t s)
+    {
+        if (total <= 0)
+            return;
+        dispatch_bd(bd, [&]<int BD>() {
+            launch_chained(chained_launch(), k_coarse_levels_batch<BD>, total, LEVEL_THREADS, 0, s, v);
+        });
+        cuda_check(cudaGetLastError(), "batched coarse levels launch");
+    }
+
+    void launch_mas_apply_batch(const BatchView &v, int bd, int storage, int total, int mode, cudaStream_t s)
+    {
+        if (mode != 1 && mode != 2)
+            throw Error(ERR_INVALID, "[MAS] internal: batched applies are the initial and the iteration apply");
+        if (total <= 0)
+            return;
+        dispatch(bd, storage, [&]<int BD, class Store>() {
+            using L = ApplyLayout<BD, Store>;
+            const size_t smem = (size_t)L::WARPS * L::WARP_BYTES;
+            if (mode == 1)
+                launch_chained(chained_launch(), k_mas_apply_batch<BD, Store, 1>, total, L::WARPS * 32, smem, s, v);
+            else
+                launch_chained(chained_launch(), k_mas_apply_batch<BD, Store, 2>, total, L::WARPS * 32, smem, s, v);
+        });
+        cuda_check(cudaGetLastError(), "batched apply launch");
+    }
+
+    int launch_restrict(const MasView &mas, const double *r, const PcgState *st, int period, cudaStream_t s)
+    {
+        const int grid = restrict_grid(mas);
+        if (grid <= 0)
+            return 0;
         dispatch_bd(mas.bd, [&]<int BD>() {
-            launch_chained(chained_launch(), k_restrict<BD>, (mas.first_iso_bank + 7) / 8, 256, 0, s,
-                           mas.first_iso_bank, r, mas.lcco0, mas.cco0_base, mas.rc, st, period);
+            launch_chained(chained_launch(), k_restrict<BD>, grid, 256, 0, s, mas.first_iso_bank, r, mas.lcco0,
+                           mas.cco0_base, mas.rc, st, period);
         });
         return 1;
     }
 
     int launch_coarse_levels(const MasView &mas, const PcgState *st, cudaStream_t s)
     {
-        if (mas.level_num <= 1 || mas.real_count[1] <= 0)
-            return 0;
-        const int grid = mas.level_num == 2 ? (mas.real_count[1] + LEVEL_THREADS / 32 - 1) / (LEVEL_THREADS / 32)
-                                            : mas.real_count[2];
+        const int grid = coarse_levels_grid(mas);
         if (grid <= 0)
             return 0;
         dispatch_bd(mas.bd,

@@ -19,6 +19,8 @@
 #include <cstring>
 #include <atomic>
 #include <limits>
+#include <memory>
+#include <mutex>
 #include <thread>
 #include <string>
 #include <type_traits>
@@ -75,6 +77,13 @@ namespace
         bool wide_tc = false;
         // Slots per loop trip of the SpMV (1, 2, 4): a launch-shape choice for the autotuner.
         int spmv_unroll = 2;
+        // mas_solve_batch: one launch per PCG phase for each group of systems (fused), or one
+        // CUDA stream per system driven by host threads (streams, measured faster on the
+        // 64-system workload: 37.7-37.9 against 38.2-38.4 ms per batch).
+        bool batch_fused = false;
+        // Fused groups of a batch, each on its own stream (systems split by size into groups of
+        // about equal work); 0 = automatic (1, measured best).
+        int batch_groups = 0;
     };
 
     const char *status_string(int s)
@@ -123,7 +132,8 @@ namespace
                                 "lazy_partitioning", "use_preconditioned_residual_norm", "precision",
                                 "true_residual_period", "check_period", "initial_guess", "beta", "ordering",
                                 "poll_period", "profile_kernels", "cuda_graphs", "preconditioner_refresh",
-                                "device_wait_limit", "rhs_group", "chained_launch", "wide_apply", "spmv_unroll"};
+                                "device_wait_limit", "rhs_group", "chained_launch", "wide_apply", "spmv_unroll",
+                                "batch_launch", "batch_groups"};
 
     // MASSolverImpl::set_parameters (MASSolver.cu:198-212) plus the extension keys.
     void apply_mas_params(Params &p, const Json &m, bool strict)
@@ -215,6 +225,19 @@ namespace
             if (w != "mma_sync" && w != "tcgen05")
                 throw Error(ERR_INVALID, "[MAS] wide_apply must be \"mma_sync\" or \"tcgen05\"");
             q.wide_tc = (w == "tcgen05");
+        }
+        if (auto *v = m.find("batch_launch"))
+        {
+            const std::string w = get_str(*v, "batch_launch");
+            if (w != "fused" && w != "streams")
+                throw Error(ERR_INVALID, "[MAS] batch_launch must be \"fused\" or \"streams\"");
+            q.batch_fused = (w == "fused");
+        }
+        if (auto *v = m.find("batch_groups"))
+        {
+            q.batch_groups = get_int(*v, "batch_groups");
+            if (q.batch_groups < 0 || q.batch_groups > 64)
+                throw Error(ERR_INVALID, "[MAS] batch_groups must be 0 (automatic) to 64");
         }
         if (auto *v = m.find("poll_period"))
         {
@@ -1690,6 +1713,99 @@ struct mas_solver
         cuda_check(cudaStreamSynchronize(stream), "solve");
     }
 
+    // ---- Fused batch (mas_solve_batch): this handle's share --------------------------------
+    // Solves that can join a fused batch: graphs on, no per-launch profiling, no learned warm
+    // start (its prediction pipeline is per handle), at least one iteration.
+    bool batch_fusable() const
+    {
+        return factorized && p.batch_fused && p.graphs && !p.profile && !learned_active() && p.max_iter >= 1;
+    }
+
+    BatchSystem batch_system()
+    {
+        BatchSystem s;
+        std::memset(&s, 0, sizeof(s));
+        s.A = A.view();
+        s.mas = mas.view();
+        s.cfg = config();
+        s.red = red();
+        s.st = st.get();
+        s.x = x.get();
+        s.r = r.get();
+        s.p = pv.get();
+        s.z = z.get();
+        s.Ap = Ap.get();
+        s.b = b.get();
+        return s;
+    }
+
+    // Input step of a fused batch solve on this handle's stream: b (and x0) into the padded
+    // vectors, as solve / solve_device do.
+    void batch_load(const double *src_b, const double *src_x, bool device_pointers, int len)
+    {
+        cuda_check(cudaSetDevice(device), "set device");
+        require_factorized(len);
+        if (!src_b || !src_x)
+            throw Error(ERR_INVALID, "[MAS] solve: null vector.");
+        last_multi = false;
+        for (auto &ks : kstats) // per-solve kernel statistics
+            ks.second = KStat{};
+        keep_stats = false;
+        if (device_pointers)
+            load_rhs_device(src_b, src_x);
+        else
+        {
+            cuda_check(cudaMemcpyAsync(io.get(), src_b, sizeof(double) * n, cudaMemcpyHostToDevice, stream),
+                       "upload b");
+            const size_t blen = (size_t)banks * 32 * bd;
+            run("permute_in", 2,
+                [&] { launch_permute_in(n, bd, V, d_padded.get(), io.get(), b.get(), blen, stream); });
+            if (p.initial_guess_input)
+            {
+                cuda_check(cudaMemcpyAsync(io.get(), src_x, sizeof(double) * n, cudaMemcpyHostToDevice, stream),
+                           "upload x");
+                run("permute_in", 2,
+                    [&] { launch_permute_in(n, bd, V, d_padded.get(), io.get(), x.get(), blen, stream); });
+            }
+            else
+                cuda_check(cudaMemsetAsync(x.get(), 0, x.bytes(), stream), "memset");
+        }
+        x0_source = p.initial_guess_input ? "input" : "zero";
+    }
+
+    // Result step: the final state (as pcg() reads it), then x back to the caller.
+    void batch_finish(const PcgState &f, int launched, double ms, double *dst_x, bool device_pointers)
+    {
+        cuda_check(cudaSetDevice(device), "set device");
+        rz0 = f.rz0;
+        rr0 = f.rr0;
+        solve_ms = ms;
+        launched_iterations = launched;
+        if (f.error == ERR_TIMEOUT)
+            throw Error(ERR_TIMEOUT, "[MAS] a device-side wait timed out.");
+        if ((f.error == ERR_NONFINITE && f.iter == 0) || std::isnan(f.rz0) || !std::isfinite(f.rz0))
+            throw Error(ERR_NONFINITE, "[MAS] Invalid initial residual.");
+        iterations = f.iter;
+        residual_norm = f.res_norm;
+        status = f.status;
+        if (device_pointers)
+            run("permute_out", 1, [&] { launch_permute_out(n, bd, V, d_padded.get(), x.get(), dst_x, stream); });
+        else
+        {
+            run("permute_out", 1, [&] { launch_permute_out(n, bd, V, d_padded.get(), x.get(), io.get(), stream); });
+            cuda_check(cudaMemcpyAsync(dst_x, io.get(), sizeof(double) * n, cudaMemcpyDeviceToHost, stream),
+                       "download x");
+        }
+        cuda_check(cudaStreamSynchronize(stream), "solve");
+    }
+
+    // Launches of a fused batch, counted on one handle of the batch (kernel_launches_total).
+    void add_launches(const char *kind, long long k)
+    {
+        kstats[stat_index(kind)].second.launches += k;
+        total_launches += k;
+    }
+
     void solve_device(const double *d_b, double *d_x, int len)
     {
         cuda_check(cudaSetDevice(device), "set device");
@@ -1870,6 +1986,416 @@ namespace
         }
         *out = h;
         return MAS_OK;
+    }
+
+    // Runs fn(i) for i in [0, count) on up to `workers` host threads.
+    template <class F>
+    void parallel_for(int count, int workers, F &&fn)
+    {
+        workers = std::max(1, std::min(workers, count));
+        std::atomic<int> next{0};
+        auto work = [&] {
+            for (int i = next.fetch_add(1); i < count; i = next.fetch_add(1))
+                fn(i);
+        };
+        if (workers <= 1)
+        {
+            work();
+            return;
+        }
+        std::vector<std::thread> pool;
+        pool.reserve((size_t)workers);
+        for (int w = 0; w < workers; ++w)
+            pool.emplace_back(work);
+        for (auto &t : pool)
+            t.join();
+    }
+
+    // A fused batch: the device copy of the batch's systems, the CTA tables of its unfinished
+    // systems, and the stream its launches run on. Kept for reuse while the systems (every
+    // pointer, size and PCG setting) stay the same.
+    struct FusedBatch
+    {
+        int device = -1;
+        cudaStream_t stream = nullptr;
+        std::vector<BatchSystem> host_sys;
+        int bd = 0, storage = 0;
+        std::vector<int> grids;         // BPH_COUNT CTAs per system (its own launches' grids)
+        DevBuf<BatchSystem> sys;
+        DevBuf<int4> table;              // the CTA entries of every phase (BatchView::map)
+        int4 *h_table = nullptr;         // pinned, 2 slots of the same size
+        DevBuf<PcgState> states;         // 2 slots of count gathered states
+        PcgState *h_states = nullptr;    // pinned, 2 slots
+        cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr}; // start, end, two chunk slots
+
+        int count() const { return (int)host_sys.size(); }
+        size_t table_len() const
+        {
+            size_t t = 0;
+            for (int g : grids)
+                t += (size_t)g;
+            return t > 0 ? t : 1;
+        }
+
+        ~FusedBatch()
+        {
+            if (device >= 0)
+                cudaSetDevice(device);
+            if (stream)
+                cudaStreamSynchronize(stream);
+            for (auto &e : ev)
+                if (e)
+                    cudaEventDestroy(e);
+            if (h_states)
+                cudaFreeHost(h_states);
+            if (h_table)
+                cudaFreeHost(h_table);
+            sys.reset();
+            table.reset();
+            states.reset();
+            if (stream)
+                cudaStreamDestroy(stream);
+        }
+
+        bool same(int dev, const std::vector<BatchSystem> &s, const std::vector<int> &g) const
+        {
+            return dev == device && s.size() == host_sys.size() && g == grids &&
+                   std::memcmp(s.data(), host_sys.data(), s.size() * sizeof(BatchSystem)) == 0;
+        }
+
+        void build(int dev, std::vector<BatchSystem> s, std::vector<int> g, int bd_, int storage_)
+        {
+            device = dev;
+            host_sys = std::move(s);
+            grids = std::move(g);
+            bd = bd_;
+            storage = storage_;
+            const int c = count();
+            cuda_check(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking), "batch stream");
+            for (auto &e : ev)
+                cuda_check(cudaEventCreate(&e), "event");
+            cuda_check(cudaMallocHost(&h_states, sizeof(PcgState) * 2 * (size_t)c), "pinned states");
+            cuda_check(cudaMallocHost(&h_table, sizeof(int4) * 2 * table_len()), "pinned tables");
+            sys.alloc((size_t)c, "batch systems");
+            table.alloc(table_len(), "batch tables");
+            states.alloc((size_t)2 * c, "batch states");
+            cuda_check(cudaMemcpyAsync(sys.get(), host_sys.data(), sizeof(BatchSystem) * (size_t)c,
+                                       cudaMemcpyHostToDevice, stream),
+                       "upload batch");
+            cuda_check(cudaStreamSynchronize(stream), "upload batch");
+        }
+
+        // Launch entries of the systems with active[k] set (each system's CTAs in order, the
+        // systems in batch order), written into pinned slot `slot` and copied (in stream order,
+        // after every earlier launch) to the device table; returns the view and the CTA totals
+        // per phase.
+        BatchView upload_active(const std::vector<char> &active, int slot, int (&totals)[BPH_COUNT])
+        {
+            const int c = count();
+            int4 *h = h_table + (size_t)slot * table_len();
+            BatchView v{sys.get(), table.get(), {}, c};
+            size_t e = 0;
+            for (int ph = 0; ph < BPH_COUNT; ++ph)
+            {
+                v.off[ph] = (int)e;
+                for (int k = 0; k < c; ++k)
+                {
+                    if (!active[(size_t)k])
+                        continue;
+                    const int g = grids[(size_t)k * BPH_COUNT + ph];
+                    for (int b = 0; b < g; ++b)
+                        h[e++] = make_int4(k, b, g, 0);
+                }
+                totals[ph] = (int)e - v.off[ph];
+            }
+            if (e > 0)
+                cuda_check(cudaMemcpyAsync(table.get(), h, sizeof(int4) * e, cudaMemcpyHostToDevice, stream),
+                           "upload tables");
+            return v;
+        }
+
+        // Every system (state reset and gather launches).
+        BatchView all() const { return BatchView{sys.get(), nullptr, {}, count()}; }
+
+        // One batched PCG iteration (the launch order of mas_solver::launch_iteration); returns
+        // the kernels launched.
+        long long iteration(const BatchView &v, const int (&totals)[BPH_COUNT], int P, bool residual)
+        {
+            long long k = 0;
+            auto counted = [&k](int total) { k += total > 0 ? 1 : 0; };
+            launch_spmv_batch(SPMV_PAP, v, bd, totals[BPH_SPMV], 1, 0, stream);
+            counted(totals[BPH_SPMV]);
+            launch_update_xr_batch(v, bd, totals[BPH_UPDATE_XR], P, stream);
+            counted(totals[BPH_UPDATE_XR]);
+            if (residual)
+            {
+                launch_spmv_batch(SPMV_RESIDUAL, v, bd, totals[BPH_SPMV], 1, P, stream);
+                counted(totals[BPH_SPMV]);
+                launch_restrict_batch(v, bd, totals[BPH_RESTRICT], P, stream);
+                counted(totals[BPH_RESTRICT]);
+            }
+            launch_coarse_levels_batch(v, bd, totals[BPH_COARSE], stream);
+            counted(totals[BPH_COARSE]);
+            launch_mas_apply_batch(v, bd, storage, totals[BPH_APPLY], 2, stream);
+            counted(totals[BPH_APPLY]);
+            launch_update_p_batch(v, bd, totals[BPH_UPDATE_P], 0, stream);
+            counted(totals[BPH_UPDATE_P]);
+            return k;
+        }
+    };
+
+    std::mutex g_fused_mu;
+    std::vector<std::unique_ptr<FusedBatch>> g_fused; // most recently used last
+    constexpr size_t FUSED_CACHE = 16;
+
+    // One fused group on its own stream: systems sys[k] (handles hs[k]), their ready events;
+    // writes each system's final state into out[k], the group's elapsed ms and launched
+    // iterations. The loop is pcg()'s: initial residual and apply, then chunks of poll_period
+    // iterations with the host reading all states one chunk behind and dropping finished
+    // systems from the next chunk's launch tables.
+    void run_fused_group(int dev, const std::vector<mas_solver *> &hs, std::vector<BatchSystem> sys,
+                         std::vector<int> grids, const std::vector<cudaEvent_t> &ready, std::vector<PcgState> &out,
+                         double &ms_out, int &launched_out)
+    {
+        cuda_check(cudaSetDevice(dev), "set device");
+        const Params &p0 = hs[0]->p;
+        const int P = p0.true_residual_period, chunk = p0.poll_period;
+        const int c = (int)hs.size();
+        int max_iter = 1;
+        for (const mas_solver *h : hs)
+            max_iter = std::max(max_iter, h->p.max_iter);
+        set_spmv_unroll(p0.spmv_unroll);
+        set_chained_launch(p0.chained);
+        std::unique_ptr<FusedBatch> fb;
+        {
+            std::lock_guard<std::mutex> lock(g_fused_mu);
+            for (size_t i = 0; i < g_fused.size(); ++i)
+                if (g_fused[i]->same(dev, sys, grids))
+                {
+                    fb = std::move(g_fused[i]);
+                    g_fused.erase(g_fused.begin() + (long)i);
+                    break;
+                }
+        }
+        if (!fb)
+        {
+            fb = std::make_unique<FusedBatch>();
+            fb->build(dev, std::move(sys), std::move(grids), hs[0]->bd, hs[0]->mas.storage);
+        }
+        FusedBatch &F = *fb;
+        cudaStream_t s = F.stream;
+        for (cudaEvent_t e : ready)
+            cuda_check(cudaStreamWaitEvent(s, e, 0), "batch wait");
+        cuda_check(cudaEventRecord(F.ev[0], s), "event");
+        long long launches = 0;
+        // pcg(): r = b - A x, rr0, the level-0 restriction, z = M^-1 r (rz0), p = z.
+        std::vector<char> active((size_t)c, 1);
+        int totals[BPH_COUNT];
+        int tslot = 0;
+        BatchView v = F.upload_active(active, tslot, totals);
+        launch_init_states_batch(F.all(), s);
+        launch_spmv_batch(SPMV_RESIDUAL, v, F.bd, totals[BPH_SPMV], 0, 0, s);
+        launch_restrict_batch(v, F.bd, totals[BPH_RESTRICT], 0, s);
+        launch_coarse_levels_batch(v, F.bd, totals[BPH_COARSE], s);
+        launch_mas_apply_batch(v, F.bd, F.storage, totals[BPH_APPLY], 1, s);
+        launch_update_p_batch(v, F.bd, totals[BPH_UPDATE_P], 1, s);
+        launches += 1;
+        for (int ph : {BPH_SPMV, BPH_RESTRICT, BPH_COARSE, BPH_APPLY, BPH_UPDATE_P})
+            launches += totals[ph] > 0 ? 1 : 0;
+        int launched = 0, pending = -1, flip = 0;
+        bool stop = false;
+        for (int k0 = 1; k0 <= max_iter && !stop; k0 += chunk)
+        {
+            for (int k = k0; k < k0 + chunk; ++k)
+                launches += F.iteration(v, totals, P, k % P == 0);
+            launched = std::min(max_iter, k0 + chunk - 1);
+            const int slot = (flip++) & 1;
+            launch_gather_states_batch(F.all(), F.states.get() + (size_t)slot * c, s);
+            launches += 1;
+            cuda_check(cudaMemcpyAsync(F.h_states + (size_t)slot * c, F.states.get() + (size_t)slot * c,
+                                       sizeof(PcgState) * (size_t)c, cudaMemcpyDeviceToHost, s),
+                       "states");
+            cuda_check(cudaEventRecord(F.ev[2 + slot], s), "event");
+            // The previous chunk's states (read while this chunk runs): stop when every system
+            // is done, else drop the finished ones from the next chunk's tables.
+            if (pending >= 0)
+            {
+                cuda_check(cudaEventSynchronize(F.ev[2 + pending]), "chunk");
+                bool changed = false, any = false;
+                for (int k = 0; k < c; ++k)
+                {
+                    const bool on = F.h_states[(size_t)pending * c + k].done == 0;
+                    changed = changed || (on != (active[(size_t)k] != 0));
+                    active[(size_t)k] = on ? 1 : 0;
+                    any = any || on;
+                }
+                stop = !any;
+                if (changed && !stop)
+                {
+                    // The pinned slot written two updates ago was copied before launches whose
+                    // chunk event has been waited on since.
+                    tslot ^= 1;
+                    v = F.upload_active(active, tslot, totals);
+                }
+            }
+            pending = slot;
+        }
+        cuda_check(cudaEventRecord(F.ev[1], s), "event");
+        launch_gather_states_batch(F.all(), F.states.get(), s);
+        launches += 1;
+        cuda_check(cudaMemcpyAsync(F.h_states, F.states.get(), sizeof(PcgState) * (size_t)c, cudaMemcpyDeviceToHost, s),
+                   "states");
+        cuda_check(cudaStreamSynchronize(s), "batch");
+        hs[0]->add_launches("batch", launches);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, F.ev[0], F.ev[1]);
+        out.assign(F.h_states, F.h_states + c);
+        ms_out = ms;
+        launched_out = launched;
+        std::lock_guard<std::mutex> lock(g_fused_mu);
+        g_fused.push_back(std::move(fb));
+        if (g_fused.size() > FUSED_CACHE)
+            g_fused.erase(g_fused.begin());
+    }
+
+    // mas_solve_batch with one launch per PCG phase for each group of unfinished systems:
+    // per-handle input steps on the handles' own streams (host threads), the groups' batched PCG
+    // on their own streams (one host thread each), then the per-handle result steps. The systems
+    // are sorted by size and cut into batch_groups runs of about equal work (dof^(4/3) each), so
+    // a group's systems finish after similar iteration counts and the groups' phase boundaries
+    // overlap on the GPU. Each system's kernels run the same bodies over the same CTA
+    // coordinates as in its own solve, so its iterates, iteration count and status are those of
+    // mas_solve bit for bit. Returns false (nothing done) when the handles cannot be fused.
+    bool solve_fused(mas_solver *const *handles, int count, const double *const *b, double *const *x, const int *n,
+                     bool device_pointers, int workers, std::vector<int> &rc)
+    {
+        const Params &p0 = handles[0]->p;
+        for (int i = 0; i < count; ++i)
+        {
+            const mas_solver *h = handles[i];
+            if (!h->batch_fusable() || h->device != handles[0]->device || h->bd != handles[0]->bd ||
+                h->mas.storage != handles[0]->mas.storage || h->p.true_residual_period != p0.true_residual_period ||
+                h->p.poll_period != p0.poll_period || h->p.spmv_unroll != p0.spmv_unroll ||
+                h->p.batch_groups != p0.batch_groups || h->p.chained != p0.chained)
+                return false;
+        }
+        const int dev = handles[0]->device;
+        cuda_check(cudaSetDevice(dev), "set device");
+        // Input steps; systems whose input is rejected keep their error and leave the batch.
+        std::vector<cudaEvent_t> ready((size_t)count, nullptr);
+        parallel_for(count, workers, [&](int i) {
+            mas_solver *h = handles[i];
+            rc[(size_t)i] = guarded(h, [&] {
+                h->batch_load(b[i], x[i], device_pointers, n[i]);
+                ready[(size_t)i] = h->pool_event();
+                cuda_check(cudaEventRecord(ready[(size_t)i], h->stream), "event");
+            });
+        });
+        std::vector<int> live;
+        for (int i = 0; i < count; ++i)
+            if (rc[(size_t)i] == MAS_OK)
+                live.push_back(i);
+        // The ready events are pool events: free them once the groups have waited on them.
+        struct FreeEvents
+        {
+            mas_solver *const *h;
+            int count;
+            ~FreeEvents()
+            {
+                for (int i = 0; i < count; ++i)
+                    h[i]->ev_used = 0;
+            }
+        } free_events{handles, count};
+        if (live.empty())
+            return true;
+        // Groups: live systems by size, cut into runs of about equal work.
+        std::sort(live.begin(), live.end(), [&](int a, int c2) {
+            return handles[a]->n != handles[c2]->n ? handles[a]->n > handles[c2]->n : a < c2;
+        });
+        const int G = std::max(1, std::min((int)live.size(), p0.batch_groups > 0 ? p0.batch_groups : 1));
+        std::vector<double> cost(live.size());
+        double total = 0.0;
+        for (size_t k = 0; k < live.size(); ++k)
+            total += (cost[k] = std::pow((double)handles[live[k]]->n, 4.0 / 3.0));
+        std::vector<std::vector<int>> groups;
+        double acc = 0.0;
+        for (size_t k = 0; k < live.size(); ++k)
+        {
+            const int g = std::min(G - 1, (int)(acc / total * G));
+            while ((int)groups.size() <= g)
+                groups.emplace_back();
+            groups[(size_t)g].push_back(live[k]);
+            acc += cost[k];
+        }
+        groups.erase(std::remove_if(groups.begin(), groups.end(), [](const std::vector<int> &g) { return g.empty(); }),
+                     groups.end());
+        struct GroupRun
+        {
+            std::vector<mas_solver *> hs;
+            std::vector<BatchSystem> sys;
+            std::vector<int> grids;
+            std::vector<cudaEvent_t> ready;
+            std::vector<PcgState> out;
+            double ms = 0.0;
+            int launched = 0;
+            int rc = MAS_OK;
+            std::string err;
+        };
+        std::vector<GroupRun> runs(groups.size());
+        for (size_t gi = 0; gi < groups.size(); ++gi)
+        {
+            GroupRun &R = runs[gi];
+            for (int i : groups[gi])
+            {
+                mas_solver *h = handles[i];
+                R.hs.push_back(h);
+                R.ready.push_back(ready[(size_t)i]);
+                R.sys.push_back(h->batch_system());
+                const BatchSystem &s = R.sys.back();
+                const int g[BPH_COUNT] = {spmv_grid(s.A),         update_xr_grid(s.mas), restrict_grid(s.mas),
+                                          coarse_levels_grid(s.mas), mas_apply_grid(s.mas), update_p_grid(s.mas)};
+                if (g[BPH_SPMV] > s.red.capacity || g[BPH_UPDATE_XR] > s.red.capacity ||
+                    g[BPH_APPLY] > s.red.capacity)
+                    throw Error(ERR_INVALID, "[MAS] reduction scratch too small");
+                R.grids.insert(R.grids.end(), g, g + BPH_COUNT);
+            }
+        }
+        parallel_for((int)runs.size(), (int)runs.size(), [&](int gi) {
+            GroupRun &R = runs[(size_t)gi];
+            try
+            {
+                run_fused_group(dev, R.hs, R.sys, R.grids, R.ready, R.out, R.ms, R.launched);
+            }
+            catch (const Error &e)
+            {
+                R.rc = e.code;
+                R.err = e.what();
+            }
+            catch (const std::exception &e)
+            {
+                R.rc = ERR_INVALID;
+                R.err = std::string("[MAS] ") + e.what();
+            }
+        });
+        // Result steps.
+        std::vector<std::pair<int, int>> work; // (group, position)
+        for (size_t gi = 0; gi < runs.size(); ++gi)
+            for (size_t k = 0; k < runs[gi].hs.size(); ++k)
+                work.push_back({(int)gi, (int)k});
+        parallel_for((int)work.size(), workers, [&](int w) {
+            const GroupRun &R = runs[(size_t)work[(size_t)w].first];
+            const int k = work[(size_t)w].second;
+            const int i = groups[(size_t)work[(size_t)w].first][(size_t)k];
+            mas_solver *h = handles[i];
+            if (R.rc != MAS_OK)
+            {
+                h->last_error = R.err;
+                rc[(size_t)i] = R.rc;
+                return;
+            }
+            rc[(size_t)i] = guarded(h, [&] { h->batch_finish(R.out[(size_t)k], R.launched, R.ms, x[i], device_pointers); });
+        });
+        return true;
     }
 } // namespace
 
@@ -2059,11 +2585,35 @@ extern "C" int mas_solve_batch(mas_solver *const *handles, int count, const doub
             }
     int workers = threads > 0 ? threads : (int)std::thread::hardware_concurrency();
     workers = std::max(1, std::min({workers, count, 64}));
-    std::atomic<int> next{0};
     std::vector<int> rc((size_t)count, MAS_OK);
-    auto work = [&] {
-        for (int i = next.fetch_add(1); i < count; i = next.fetch_add(1))
+    bool fused = false;
+    if (count > 0)
+    {
+        auto fail_all = [&](int code, const std::string &msg) {
+            fused = true;
+            for (int i = 0; i < count; ++i)
+                if (rc[(size_t)i] == MAS_OK)
+                {
+                    rc[(size_t)i] = code;
+                    handles[i]->last_error = msg;
+                }
+        };
+        try
         {
+            fused = solve_fused(handles, count, b, x, n, device_pointers != 0, workers, rc);
+        }
+        catch (const Error &e)
+        {
+            fail_all(e.code, e.what());
+        }
+        catch (const std::exception &e)
+        {
+            fail_all(ERR_INVALID, std::string("[MAS] ") + e.what());
+        }
+    }
+    // Otherwise one CUDA stream per system, driven by a pool of host threads.
+    if (!fused)
+        parallel_for(count, workers, [&](int i) {
             mas_solver *h = handles[i];
             rc[(size_t)i] = guarded(h, [&] {
                 if (device_pointers)
@@ -2071,19 +2621,7 @@ extern "C" int mas_solve_batch(mas_solver *const *handles, int count, const doub
                 else
                     h->solve(b[i], x[i], n[i]);
             });
-        }
-    };
-    if (workers <= 1)
-        work();
-    else
-    {
-        std::vector<std::thread> pool;
-        pool.reserve((size_t)workers);
-        for (int w = 0; w < workers; ++w)
-            pool.emplace_back(work);
-        for (auto &t : pool)
-            t.join();
-    }
+        });
     int first = MAS_OK;
     for (int i = 0; i < count; ++i)
     {

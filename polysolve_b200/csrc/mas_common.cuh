@@ -113,12 +113,31 @@ namespace pmas
         return t;
     }
 
+    // A CTA's place in the grid that serves one system: the hardware grid of a launch for one
+    // system, or the range of a batched launch's grid that serves one system of the batch. The
+    // kernel bodies index work and reduction partials by it, so both launches give the same bits.
+    struct Cta
+    {
+        int x; // index within the system's grid
+        int n; // CTAs serving the system
+    };
+
+    __device__ __forceinline__ Cta native_cta() { return Cta{(int)blockIdx.x, (int)gridDim.x}; }
+
+    // The system (x) and CTA coordinates (y of z) that this CTA of a batched launch serves in
+    // phase ph.
+    __device__ __forceinline__ int4 batch_entry(const BatchView &v, int ph)
+    {
+        return __ldg(v.map + v.off[ph] + blockIdx.x);
+    }
+
     // Deterministic grid-wide sum of NV values per CTA: every CTA writes its block sum to
-    // partials[blockIdx.x * NV + i]; the last CTA to arrive (atomic ticket) adds the partials in
-    // a fixed order. Returns true in the last CTA, with tot[] the totals (valid in all its
+    // partials[cta.x * NV + i]; the last CTA to arrive (atomic ticket) adds the partials in a
+    // fixed order. Returns true in the last CTA, with tot[] the totals (valid in all its
     // threads). Every thread of every CTA must call it.
     template <int NV, int THREADS>
-    __device__ __forceinline__ bool grid_reduce(double (&v)[NV], double *partials, unsigned *counter, double (&tot)[NV])
+    __device__ __forceinline__ bool grid_reduce(double (&v)[NV], double *partials, unsigned *counter, double (&tot)[NV],
+                                                Cta cta)
     {
         constexpr int W = THREADS / 32;
         __shared__ double sh[W][NV];
@@ -140,11 +159,11 @@ namespace pmas
                 double s = 0.0;
                 for (int ww = 0; ww < W; ++ww)
                     s += sh[ww][i];
-                partials[(size_t)blockIdx.x * NV + i] = s;
+                partials[(size_t)cta.x * NV + i] = s;
             }
             __threadfence();
             unsigned t = atomicAdd(counter, 1u);
-            is_last = (t == gridDim.x - 1);
+            is_last = (t == (unsigned)cta.n - 1);
         }
         __syncthreads();
         if (!is_last)
@@ -155,7 +174,7 @@ namespace pmas
         for (int i = 0; i < NV; ++i)
         {
             s[i] = 0.0;
-            for (int b = threadIdx.x; b < (int)gridDim.x; b += THREADS)
+            for (int b = threadIdx.x; b < cta.n; b += THREADS)
                 s[i] += __ldcg(partials + (size_t)b * NV + i);
             s[i] = warp_sum(s[i]);
         }
@@ -176,6 +195,12 @@ namespace pmas
         if (threadIdx.x == 0)
             *counter = 0u;
         return true;
+    }
+
+    template <int NV, int THREADS>
+    __device__ __forceinline__ bool grid_reduce(double (&v)[NV], double *partials, unsigned *counter, double (&tot)[NV])
+    {
+        return grid_reduce<NV, THREADS>(v, partials, counter, tot, native_cta());
     }
 
     // Deterministic grid-wide sum of NV values per CTA already summed into shared memory (vals, NV

@@ -305,6 +305,46 @@ namespace pmas
     };
 
     // ---------------------------------------------------------------------------------------
+    // Fused batch (mas_solve_batch): one launch per PCG phase serves every system of a batch.
+    // System s owns the CTAs [start[s], start[s + 1]) of a phase's launch and runs them as CTAs
+    // 0 .. start[s + 1] - start[s] - 1 of the launch it would get alone, through the same kernel
+    // body, so each system's iterates are those of its own solve bit for bit.
+    // ---------------------------------------------------------------------------------------
+    struct BatchSystem
+    {
+        BankedView A;
+        MasView mas;
+        PcgConfig cfg;
+        ReduceBuf red;
+        PcgState *st;
+        double *x, *r, *p, *z, *Ap;
+        const double *b;
+    };
+
+    enum BatchPhase : int
+    {
+        BPH_SPMV = 0,
+        BPH_UPDATE_XR,
+        BPH_RESTRICT,
+        BPH_COARSE,
+        BPH_APPLY,
+        BPH_UPDATE_P,
+        BPH_COUNT
+    };
+
+    // The systems of a batched launch: CTA b of phase ph serves system e.x of sys as CTA e.y of
+    // the e.z CTAs of that system's own launch, e = map[off[ph] + b] (one load per CTA). Only
+    // unfinished systems get entries; the state reset and gather launches take every system
+    // (map unused, count = all).
+    struct BatchView
+    {
+        const BatchSystem *sys; // every system of the batch (device memory)
+        const int4 *map;        // the phases' CTA entries (device memory)
+        int off[BPH_COUNT];     // first entry of each phase
+        int count;              // systems (state reset and gather)
+    };
+
+    // ---------------------------------------------------------------------------------------
     // Launchers (defined in the .cu files). All take the solver's stream.
     // ---------------------------------------------------------------------------------------
 
@@ -352,6 +392,10 @@ namespace pmas
     // period > 0 (SPMV_RESIDUAL in the PCG loop): runs only when (st->iter + 1) % period == 0.
     void launch_spmv(int mode, const BankedView &A, const double *x, double *y, const double *b, PcgState *st,
                      ReduceBuf red, int iter, int period, cudaStream_t s);
+    // CTAs of one system's SpMV launch; the batched SpMV (mode SPMV_PAP or SPMV_RESIDUAL) over
+    // `total` CTAs with the spmv_unroll variant of the calling thread.
+    int spmv_grid(const BankedView &A);
+    void launch_spmv_batch(int mode, const BatchView &v, int bd, int total, int iter, int period, cudaStream_t s);
     // y_v = A x_v for count (1..4) separate vectors in one pass over A.
     constexpr int SPMV_MAX_VECTORS = 4;
     void launch_spmv_vectors(const BankedView &A, const double *const *x, double *const *y, int count, cudaStream_t s);
@@ -370,6 +414,14 @@ namespace pmas
     void launch_permute_out(int n, int bd, int V, const int *padded_of_block, const double *src, double *dst,
                             cudaStream_t s);
     void launch_pcg_init_state(PcgState *st, cudaStream_t s);
+    // Grids of one system's update launches, and the batched launches (every system's state
+    // reset to zero by launch_init_states_batch, one CTA per system).
+    int update_xr_grid(const MasView &mas);
+    int update_p_grid(const MasView &mas);
+    void launch_update_xr_batch(const BatchView &v, int bd, int total, int period, cudaStream_t s);
+    void launch_update_p_batch(const BatchView &v, int bd, int total, int first, cudaStream_t s);
+    void launch_init_states_batch(const BatchView &v, cudaStream_t s);
+    void launch_gather_states_batch(const BatchView &v, PcgState *out, cudaStream_t s);
 
     // mas_apply.cu: the MAS apply. The coarse residual rc is built by the level-0 restriction
     // (fused into update_xr, or launch_restrict) and launch_coarse_levels; launch_mas_apply then
@@ -384,6 +436,14 @@ namespace pmas
     void launch_mas_apply(const MasView &mas, const double *r, double *z0, PcgState *st, ReduceBuf red,
                           PcgConfig cfg, int mode, cudaStream_t s);
     void launch_prolong(const MasView &mas, const double *z0, double *z, cudaStream_t s);
+    // Grids of one system's restrict, coarse-level and apply launches (0: none), and the
+    // batched launches (mode 1 / 2 applies only).
+    int restrict_grid(const MasView &mas);
+    int coarse_levels_grid(const MasView &mas);
+    int mas_apply_grid(const MasView &mas);
+    void launch_restrict_batch(const BatchView &v, int bd, int total, int period, cudaStream_t s);
+    void launch_coarse_levels_batch(const BatchView &v, int bd, int total, cudaStream_t s);
+    void launch_mas_apply_batch(const BatchView &v, int bd, int storage, int total, int mode, cudaStream_t s);
 
     // Several right-hand sides (groups of RHS_GROUP, interleaved vectors, state array of
     // RHS_GROUP + 1 entries: one per right-hand side, then the group record). mas_multi.cu and

@@ -86,23 +86,23 @@ namespace pmas
         // coalesced (value t * 32 + lane). On a true-residual iteration only x is updated here:
         // r, rr and the restriction follow the SpMV.
         template <int BD>
-        __global__ void __launch_bounds__(UPD_THREADS) k_update_xr(MasView mas, double *__restrict__ x,
-                                                                   double *__restrict__ r, const double *__restrict__ p,
-                                                                   const double *__restrict__ Ap, PcgState *st,
-                                                                   ReduceBuf red, int period)
+        __device__ __forceinline__ void update_xr_body(const MasView &mas, double *__restrict__ x,
+                                                       double *__restrict__ r, const double *__restrict__ p,
+                                                       const double *__restrict__ Ap, PcgState *st,
+                                                       const ReduceBuf &red, int period, Cta cta)
         {
             pdl_wait();
             if (st->done)
                 return;
             const double alpha = st->alpha;
             const bool due = period > 0 && (st->iter + 1) % period == 0;
-            if (blockIdx.x == 0 && threadIdx.x == 0)
+            if (cta.x == 0 && threadIdx.x == 0)
                 st->x_defer = due ? -1 : st->iter + 1;
             const int lane = threadIdx.x & 31;
-            const int total_warps = gridDim.x * (UPD_THREADS / 32);
+            const int total_warps = cta.n * (UPD_THREADS / 32);
             const bool restrict_r = !due && mas.level_num > 0;
             double part = 0.0;
-            for (int bank = blockIdx.x * (UPD_THREADS / 32) + (threadIdx.x >> 5); bank < mas.banks; bank += total_warps)
+            for (int bank = cta.x * (UPD_THREADS / 32) + (threadIdx.x >> 5); bank < mas.banks; bank += total_warps)
             {
                 const long long b0 = (long long)bank * 32 * BD + lane;
                 // All loads of the bank first (one memory round trip), then the updates.
@@ -141,18 +141,38 @@ namespace pmas
             if (due)
                 return;
             double v1[1] = {part}, tot[1];
-            if (grid_reduce<1, UPD_THREADS>(v1, red.rr_parts, &st->counter[1], tot) && threadIdx.x == 0)
+            if (grid_reduce<1, UPD_THREADS>(v1, red.rr_parts, &st->counter[1], tot, cta) && threadIdx.x == 0)
                 st->rr = tot[0];
+        }
+
+        template <int BD>
+        __global__ void __launch_bounds__(UPD_THREADS) k_update_xr(MasView mas, double *__restrict__ x,
+                                                                   double *__restrict__ r, const double *__restrict__ p,
+                                                                   const double *__restrict__ Ap, PcgState *st,
+                                                                   ReduceBuf red, int period)
+        {
+            update_xr_body<BD>(mas, x, r, p, Ap, st, red, period, native_cta());
+        }
+
+        template <int BD>
+        __global__ void __launch_bounds__(UPD_THREADS) k_update_xr_batch(BatchView v, int period)
+        {
+            const int4 e = batch_entry(v, BPH_UPDATE_XR);
+            const BatchSystem &sy = v.sys[e.x];
+            const Cta cta{e.y, e.z};
+            const MasView mas = sy.mas;
+            const ReduceBuf red = sy.red;
+            update_xr_body<BD>(mas, sy.x, sy.r, sy.p, sy.Ap, sy.st, red, period,
+                               cta);
         }
 
         // x += alpha p when update_xr left it (see PcgState::x_defer), also on the iteration that
         // stops the solve; p = z0 + sum_l zc[cslot_l(node)] + beta p; warps stride over banks,
         // coalesced.
         template <int BD>
-        __global__ void __launch_bounds__(UPD_THREADS) k_update_p(MasView mas, double *__restrict__ x,
-                                                                  double *__restrict__ p,
-                                                                  const double *__restrict__ z0, const PcgState *st,
-                                                                  int first)
+        __device__ __forceinline__ void update_p_body(const MasView &mas, double *__restrict__ x,
+                                                      double *__restrict__ p, const double *__restrict__ z0,
+                                                      const PcgState *st, int first, Cta cta)
         {
             pdl_wait();
             const int it = st->iter;
@@ -163,10 +183,10 @@ namespace pmas
             const double alpha = st->alpha;
             const double beta = first ? 0.0 : st->beta;
             const int lane = threadIdx.x & 31;
-            const int total_warps = gridDim.x * (UPD_THREADS / 32);
+            const int total_warps = cta.n * (UPD_THREADS / 32);
             const double *__restrict__ zc = mas.zc;
             const double iso_scale = 1.0 + mas.level_num;
-            for (int bank = blockIdx.x * (UPD_THREADS / 32) + (threadIdx.x >> 5); bank < mas.banks; bank += total_warps)
+            for (int bank = cta.x * (UPD_THREADS / 32) + (threadIdx.x >> 5); bank < mas.banks; bank += total_warps)
             {
                 const long long b0 = (long long)bank * 32 * BD;
                 if (bank >= mas.first_iso_bank)
@@ -224,6 +244,42 @@ namespace pmas
                     p[b0 + e] = first ? v : fma(beta, pold[t], v);
                 }
             }
+        }
+
+        template <int BD>
+        __global__ void __launch_bounds__(UPD_THREADS) k_update_p(MasView mas, double *__restrict__ x,
+                                                                  double *__restrict__ p,
+                                                                  const double *__restrict__ z0, const PcgState *st,
+                                                                  int first)
+        {
+            update_p_body<BD>(mas, x, p, z0, st, first, native_cta());
+        }
+
+        template <int BD>
+        __global__ void __launch_bounds__(UPD_THREADS) k_update_p_batch(BatchView v, int first)
+        {
+            const int4 e = batch_entry(v, BPH_UPDATE_P);
+            const BatchSystem &sy = v.sys[e.x];
+            const Cta cta{e.y, e.z};
+            const MasView mas = sy.mas;
+            update_p_body<BD>(mas, sy.x, sy.p, sy.z, sy.st, first, cta);
+        }
+
+        // Every system's PcgState copied into out[s] (one host read of the whole batch's states).
+        __global__ void k_gather_states_batch(BatchView v, PcgState *out)
+        {
+            const unsigned *src = reinterpret_cast<const unsigned *>(v.sys[blockIdx.x].st);
+            unsigned *dst = reinterpret_cast<unsigned *>(out + blockIdx.x);
+            for (int i = threadIdx.x; i < (int)(sizeof(PcgState) / sizeof(unsigned)); i += blockDim.x)
+                dst[i] = __ldcg(src + i);
+        }
+
+        // Every system's PcgState set to zero (the batched form of launch_pcg_init_state).
+        __global__ void k_init_states_batch(BatchView v)
+        {
+            unsigned *w = reinterpret_cast<unsigned *>(v.sys[blockIdx.x].st);
+            for (int i = threadIdx.x; i < (int)(sizeof(PcgState) / sizeof(unsigned)); i += blockDim.x)
+                w[i] = 0u;
         }
 
         // dst (padded, node-major, zero elsewhere) <- src (caller's order, length n)
@@ -310,14 +366,63 @@ namespace pmas
         int bank_grid_all(int banks) { return (banks + UPD_THREADS / 32 - 1) / (UPD_THREADS / 32); }
     } // namespace
 
+    int update_xr_grid(const MasView &mas)
+    {
+        // One resident wave: as many CTAs as fit on the device at once.
+        int grid = mas.bd == 1 ? bank_grid(mas.banks, k_update_xr<1>)
+                               : (mas.bd == 2 ? bank_grid(mas.banks, k_update_xr<2>) : bank_grid(mas.banks, k_update_xr<3>));
+        return grid < 1 ? 1 : grid;
+    }
+
+    int update_p_grid(const MasView &mas) { return bank_grid_all(mas.banks); }
+
+    void launch_update_xr_batch(const BatchView &v, int bd, int total, int period, cudaStream_t s)
+    {
+        if (total <= 0)
+            return;
+        if (bd == 1)
+            launch_chained(chained_launch(), k_update_xr_batch<1>, total, UPD_THREADS, 0, s, v, period);
+        else if (bd == 2)
+            launch_chained(chained_launch(), k_update_xr_batch<2>, total, UPD_THREADS, 0, s, v, period);
+        else
+            launch_chained(chained_launch(), k_update_xr_batch<3>, total, UPD_THREADS, 0, s, v, period);
+        cuda_check(cudaGetLastError(), "batched update_xr launch");
+    }
+
+    void launch_update_p_batch(const BatchView &v, int bd, int total, int first, cudaStream_t s)
+    {
+        if (total <= 0)
+            return;
+        if (bd == 1)
+            launch_chained(chained_launch(), k_update_p_batch<1>, total, UPD_THREADS, 0, s, v, first);
+        else if (bd == 2)
+            launch_chained(chained_launch(), k_update_p_batch<2>, total, UPD_THREADS, 0, s, v, first);
+        else
+            launch_chained(chained_launch(), k_update_p_batch<3>, total, UPD_THREADS, 0, s, v, first);
+        cuda_check(cudaGetLastError(), "batched update_p launch");
+    }
+
+    void launch_gather_states_batch(const BatchView &v, PcgState *out, cudaStream_t s)
+    {
+        if (v.count <= 0)
+            return;
+        k_gather_states_batch<<<v.count, 64, 0, s>>>(v, out);
+        cuda_check(cudaGetLastError(), "batched state gather launch");
+    }
+
+    void launch_init_states_batch(const BatchView &v, cudaStream_t s)
+    {
+        if (v.count <= 0)
+            return;
+        k_init_states_batch<<<v.count, 64, 0, s>>>(v);
+        cuda_check(cudaGetLastError(), "batched state reset launch");
+    }
+
     void launch_update_xr(const MasView &mas, double *x, double *r, const double *p, const double *Ap, PcgState *st,
                           ReduceBuf red, int period, cudaStream_t s)
     {
         auto go = [&](auto kernel) {
-            // One resident wave: as many CTAs as fit on the device at once.
-            int grid = bank_grid(mas.banks, kernel);
-            if (grid < 1)
-                grid = 1;
+            const int grid = update_xr_grid(mas);
             if (grid > red.capacity)
                 throw Error(ERR_INVALID, "[MAS] reduction scratch too small");
             launch_chained(chained_launch(), kernel, grid, UPD_THREADS, 0, s, mas, x, r, p, Ap, st, red, period);
@@ -335,7 +440,7 @@ namespace pmas
                          cudaStream_t s)
     {
         auto go = [&](auto kernel) {
-            const int grid = bank_grid_all(mas.banks);
+            const int grid = update_p_grid(mas);
             if (grid > 0)
                 launch_chained(chained_launch(), kernel, grid, UPD_THREADS, 0, s, mas, x, p, z0, st, first);
         };

@@ -24,16 +24,16 @@ namespace pmas
         // 1, 2 or 4; 2 measured best at 1.6 M DOF). Minimum one CTA per SM: the compiler then keeps
         // the unrolled slots' loads in flight (80 registers at 2, 3 CTAs per SM), measured faster
         // than the occupancy-first 44-register build at 1.6 M DOF.
-        template <int BD, int MODE, int UNROLL = 2>
-        __global__ void __launch_bounds__(SPMV_THREADS, 1) k_spmv(BankedView A, const double *__restrict__ x,
-                                                               double *__restrict__ y, const double *__restrict__ b,
-                                                               PcgState *st, ReduceBuf red, int iter, int period)
+        template <int BD, int MODE, int UNROLL>
+        __device__ __forceinline__ void spmv_body(const BankedView &A, const double *__restrict__ x,
+                                                  double *__restrict__ y, const double *__restrict__ b, PcgState *st,
+                                                  const ReduceBuf &red, int iter, int period, Cta cta)
         {
             constexpr int BS = BD * BD;
             constexpr int PAIRS = BS / 2;
             pdl_wait();
             // The previous iteration's update_p has run: its deferred x update is applied.
-            if (MODE == SPMV_PAP && blockIdx.x == 0 && threadIdx.x == 0)
+            if (MODE == SPMV_PAP && cta.x == 0 && threadIdx.x == 0)
                 st->x_applied = st->x_defer;
             if (MODE != SPMV_PLAIN && st->done)
                 return;
@@ -41,7 +41,7 @@ namespace pmas
             if (MODE == SPMV_RESIDUAL && period > 0 && (st->iter + 1) % period != 0)
                 return;
             const int lane = threadIdx.x & 31;
-            const int bank = blockIdx.x * BANKS_PER_CTA + (threadIdx.x >> 5);
+            const int bank = cta.x * BANKS_PER_CTA + (threadIdx.x >> 5);
             double part = 0.0, bb = 0.0;
             if (bank < A.banks)
             {
@@ -118,14 +118,14 @@ namespace pmas
             {
                 // In-loop true residual: rr = r . r (ticket on its own counter).
                 double v1[1] = {part}, t1[1];
-                if (grid_reduce<1, SPMV_THREADS>(v1, red.rr_parts, &st->counter[2], t1) && threadIdx.x == 0)
+                if (grid_reduce<1, SPMV_THREADS>(v1, red.rr_parts, &st->counter[2], t1, cta) && threadIdx.x == 0)
                     st->rr = t1[0];
                 return;
             }
             // rr0 = ||b||^2: equal to the reference's r.r at x = 0 (MASSolver.cu:488-494), and keeps
             // "relative" relative to ||b|| when an initial guess is used.
             double v2[2] = {part, bb}, tot[2];
-            if (grid_reduce<2, SPMV_THREADS>(v2, red.partials, &st->counter[0], tot) && threadIdx.x == 0)
+            if (grid_reduce<2, SPMV_THREADS>(v2, red.partials, &st->counter[0], tot, cta) && threadIdx.x == 0)
             {
                 if (MODE == SPMV_PAP)
                 {
@@ -141,11 +141,35 @@ namespace pmas
             }
         }
 
+        template <int BD, int MODE, int UNROLL = 2>
+        __global__ void __launch_bounds__(SPMV_THREADS, 1) k_spmv(BankedView A, const double *__restrict__ x,
+                                                               double *__restrict__ y, const double *__restrict__ b,
+                                                               PcgState *st, ReduceBuf red, int iter, int period)
+        {
+            spmv_body<BD, MODE, UNROLL>(A, x, y, b, st, red, iter, period, native_cta());
+        }
+
+        // The same SpMV for every system of a batch in one launch: p.Ap (MODE SPMV_PAP: x = p,
+        // y = Ap) or the true residual (x, y = r, b).
+        template <int BD, int MODE, int UNROLL = 2>
+        __global__ void __launch_bounds__(SPMV_THREADS, 1) k_spmv_batch(BatchView v, int iter, int period)
+        {
+            const int4 e = batch_entry(v, BPH_SPMV);
+            const BatchSystem &sy = v.sys[e.x];
+            const Cta cta{e.y, e.z};
+            const BankedView A = sy.A;
+            const ReduceBuf red = sy.red;
+            if (MODE == SPMV_PAP)
+                spmv_body<BD, MODE, UNROLL>(A, sy.p, sy.Ap, nullptr, sy.st, red, iter, period, cta);
+            else
+                spmv_body<BD, MODE, UNROLL>(A, sy.x, sy.r, sy.b, sy.st, red, iter, period, cta);
+        }
+
         template <int BD>
         void launch_bd(int mode, const BankedView &A, const double *x, double *y, const double *b, PcgState *st,
                        ReduceBuf red, int iter, int period, cudaStream_t s)
         {
-            const int grid = (A.banks + BANKS_PER_CTA - 1) / BANKS_PER_CTA;
+            const int grid = spmv_grid(A);
             if (grid == 0)
                 return;
             if (mode != SPMV_PLAIN && grid > red.capacity)
@@ -176,6 +200,26 @@ namespace pmas
                 go.template operator()<2>();
             cuda_check(cudaGetLastError(), "spmv launch");
         }
+        template <int BD>
+        void launch_batch_bd(int mode, const BatchView &v, int total, int iter, int period, cudaStream_t s)
+        {
+            auto go = [&]<int U>() {
+                if (mode == SPMV_PAP)
+                    launch_chained(chained_launch(), k_spmv_batch<BD, SPMV_PAP, U>, total, SPMV_THREADS, 0, s, v, iter, period);
+                else
+                    launch_chained(chained_launch(), k_spmv_batch<BD, SPMV_RESIDUAL, U>, total, SPMV_THREADS, 0, s, v, iter,
+                                   period);
+            };
+            const int u = spmv_unroll();
+            if (u == 1)
+                go.template operator()<1>();
+            else if (u == 4)
+                go.template operator()<4>();
+            else
+                go.template operator()<2>();
+            cuda_check(cudaGetLastError(), "batched spmv launch");
+        }
+
         struct VecPtrs
         {
             const double *x[SPMV_MAX_VECTORS];
@@ -264,6 +308,22 @@ namespace pmas
             cuda_check(cudaGetLastError(), "spmv vectors launch");
         }
     } // namespace
+
+    int spmv_grid(const BankedView &A) { return (A.banks + BANKS_PER_CTA - 1) / BANKS_PER_CTA; }
+
+    void launch_spmv_batch(int mode, const BatchView &v, int bd, int total, int iter, int period, cudaStream_t s)
+    {
+        if (mode != SPMV_PAP && mode != SPMV_RESIDUAL)
+            throw Error(ERR_INVALID, "[MAS] internal: batched SpMV modes are p.Ap and the true residual");
+        if (total <= 0)
+            return;
+        if (bd == 1)
+            launch_batch_bd<1>(mode, v, total, iter, period, s);
+        else if (bd == 2)
+            launch_batch_bd<2>(mode, v, total, iter, period, s);
+        else
+            launch_batch_bd<3>(mode, v, total, iter, period, s);
+    }
 
     void launch_spmv_vectors(const BankedView &A, const double *const *x, double *const *y, int count, cudaStream_t s)
     {

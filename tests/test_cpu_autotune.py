@@ -59,4 +59,18 @@ def test_cached_result_sets_both_parameters(tmp_path, monkeypatch):
     solvers = [FakeSolver(), FakeSolver()]
     res = autotune.tune_batch(solvers, [0, 0], [0, 0], ns, cache_path=str(path))
     assert res["cached"] and res["threads"] == 8
-    assert all(s.params == {"poll_period": 40, "spmv_unroll": 1} for s in solvers)
+    # an entry without batch_launch (older cache) restores the defaults
+    assert all(s.params == {"poll_period": 40, "spmv_unroll": 1, "batch_launch": "streams", "batch_groups": 0}
+               for s in solvers)
+
+
+def test_batch_launch_picks_the_fastest_and_leaves_it_set():
+    solvers = [FakeSolver(), FakeSolver()]
+    cost = {"fused": 0.004, "streams": 0.02}
+
+    def run():
+        time.sleep(cost[solvers[0].params["batch_launch"]])
+
+    res = autotune.tune_batch_launch(solvers, run, repeats=2)
+    assert res["best"] == "fused" and set(res["ms"]) == {"fused", "streams"}
+    assert all(s.params["batch_launch"] == "fused" for s in solvers)
