@@ -485,13 +485,22 @@ def run_batch(args) -> None:
     for (s, A, b), dx in zip(systems, dxs):
         x = dx.cpu().numpy()
         worst = max(worst, float(np.linalg.norm(A @ x - b) / np.linalg.norm(b)))
-    # the same share one system after another (single host thread, one solve per call)
+    # the same share one system after another (single host thread, one solve per call), with the
+    # lone-solve launch shapes (the defaults), not the batch's tuned ones
+    lone = {"apply_items_per_warp": 1, "spmv_unroll": 2, "poll_period": 10}
+    for sv in solvers:
+        sv.set_parameters({"MAS": lone})
+    for sv, bp, xp, n_ in zip(solvers, bptr, xptr, ns):
+        sv.solve_device(bp, xp, n_)  # untimed: graph capture with these shapes
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for sv, bp, xp, n_ in zip(solvers, bptr, xptr, ns):
         sv.solve_device(bp, xp, n_)
     torch.cuda.synchronize()
     seq_ms = (time.perf_counter() - t0) * 1000.0
+    for sv in solvers:
+        sv.set_parameters({"MAS": {k: int(tuned.get(k, v)) for k, v in lone.items()}})
+    solve_batch(solvers, [b for _, _, b in systems], threads=threads)  # untimed: back to the batch shapes
     # end to end from host arrays
     hbs = [b for _, _, b in systems]
     t0 = time.perf_counter()
@@ -522,7 +531,8 @@ def run_batch(args) -> None:
         "e2e": {"value": round(float(te[0].item()), 3), "unit": "ms/batch",
                 "h2d_bytes_per_step": int(8 * sum(ns)), "d2h_bytes_per_step": int(8 * sum(ns))},
         "gpu_launches": int(gpu_launches), "clocks": clk,
-        "autotune": {"batch_launch": launch_mode, "batch_groups": tuned.get("batch_groups"),
+        "autotune": {"apply_items_per_warp": tuned.get("apply_items_per_warp"), "batch_launch": launch_mode,
+                     "batch_groups": tuned.get("batch_groups"),
                      "poll_period": tuned["poll_period"],
                      "spmv_unroll": tuned.get("spmv_unroll"), "threads": threads, "tables": tuned.get("tables", {})},
     }

@@ -78,7 +78,9 @@ void mas_destroy(mas_solver *h);
  * same bits either way), wide_apply ("mma_sync" | "tcgen05": tensor-core path of the sixteen-wide
  * apply of mas_solve_multi), batch_launch ("fused" | "streams", default streams: how
  * mas_solve_batch runs the handle, see there), batch_groups (0..64, default 0 = 1: fused groups of
- * a batch). */
+ * a batch), apply_items_per_warp (1..64, default 1: the fewest inverses per warp of the MAS apply,
+ * which sets its grid; more suit batches of small systems, and the dot products' summation
+ * grouping follows the grid, so results can differ in the last bits between settings). */
 int mas_set_parameters(mas_solver *h, const char *params_json);
 
 /* MASSolver::get_info (MASSolver.cu:214-219): writes a JSON object with solver_iter,

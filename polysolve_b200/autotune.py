@@ -10,6 +10,9 @@ runtime choices that depend on the system sizes and the GPU:
 * ``poll_period`` - PCG iterations per replayed CUDA graph (and per host poll of the convergence
   flag): short graphs stop sooner after convergence, long ones cost fewer launches and polls.
   Small systems are launch-bound and prefer long graphs; large ones barely care.
+* ``apply_items_per_warp`` - the fewest inverses each warp of the MAS apply multiplies (1, 2, 4,
+  8): 1 gives a lone solve the most CTAs; in a batch of small systems more items per warp let the
+  apply's copy pipeline run past its start-up latency and leave SMs to the other systems.
 * ``batch_launch`` of ``solve_batch`` / ``solve_batch_device`` - one launch per PCG phase for each
   group of systems ("fused") or one CUDA stream per system ("streams"); with "fused",
   ``batch_groups`` - how many such groups (each on its own stream) the batch is cut into by size.
@@ -107,12 +110,13 @@ def tune_batch_launch(solvers, run, candidates=("fused", "streams"), repeats: in
 def tune_batch(solvers, b_ptrs, x_ptrs, ns, *, cache_path: str | None = None, repeats: int = 3,
                poll_candidates=(5, 10, 20, 40), unroll_candidates=(1, 2, 4),
                thread_candidates=(4, 8, 16, 32, 64), launch_candidates=("fused", "streams"),
-               group_candidates=(1, 2, 4, 8)) -> dict:
-    """Tunes ``batch_launch`` (with ``batch_groups`` when fused), ``poll_period`` and
-    ``spmv_unroll`` (all solvers) and the host thread count of ``solve_batch_device`` for these
-    systems, one after another; returns ``{"batch_launch": m, "batch_groups": g, "poll_period": p,
-    "spmv_unroll": u, "threads": t, "tables": {...}, "cached": bool}`` and leaves the parameters set
-    on the solvers. With ``cache_path`` a previous result for the same sizes is reused."""
+               group_candidates=(1, 2, 4, 8), ipw_candidates=(1, 2, 4, 8)) -> dict:
+    """Tunes ``apply_items_per_warp``, ``batch_launch`` (with ``batch_groups`` when fused),
+    ``poll_period`` and ``spmv_unroll`` (all solvers) and the host thread count of
+    ``solve_batch_device`` for these systems, one after another; returns ``{"apply_items_per_warp":
+    k, "batch_launch": m, "batch_groups": g, "poll_period": p, "spmv_unroll": u, "threads": t,
+    "tables": {...}, "cached": bool}`` and leaves the parameters set on the solvers. With
+    ``cache_path`` a previous result for the same sizes is reused."""
     from .solver import solve_batch_device
 
     key = signature(ns)
@@ -123,10 +127,12 @@ def tune_batch(solvers, b_ptrs, x_ptrs, ns, *, cache_path: str | None = None, re
             s.set_parameters({"MAS": {"poll_period": int(res["poll_period"]),
                                       "spmv_unroll": int(res.get("spmv_unroll", 2)),
                                       "batch_launch": str(res.get("batch_launch", "streams")),
-                                      "batch_groups": int(res.get("batch_groups", 0))}})
+                                      "batch_groups": int(res.get("batch_groups", 0)),
+                                      "apply_items_per_warp": int(res.get("apply_items_per_warp", 1))}})
         return res
     threads0 = min(32, max(1, len(solvers)))
     run0 = lambda: solve_batch_device(solvers, b_ptrs, x_ptrs, ns, threads=threads0)  # noqa: E731
+    ipw = tune_param(solvers, run0, "apply_items_per_warp", ipw_candidates, repeats)
     groups = {"best": 0, "ms": {}}
     if "fused" in launch_candidates:
         for s in solvers:
@@ -138,10 +144,11 @@ def tune_batch(solvers, b_ptrs, x_ptrs, ns, *, cache_path: str | None = None, re
     unroll = tune_spmv_unroll(solvers, run0, unroll_candidates, repeats)
     thr = tune_batch_threads(lambda t: solve_batch_device(solvers, b_ptrs, x_ptrs, ns, threads=t),
                              [t for t in thread_candidates if t <= max(1, len(solvers))] or [1], repeats)
-    res = {"batch_launch": launch["best"], "batch_groups": groups["best"], "poll_period": poll["best"],
-           "spmv_unroll": unroll["best"], "threads": thr["best"],
-           "tables": {"batch_groups_ms": groups["ms"], "batch_launch_ms": launch["ms"], "poll_period_ms": poll["ms"],
-                      "spmv_unroll_ms": unroll["ms"], "threads_ms": thr["ms"]}}
+    res = {"apply_items_per_warp": ipw["best"], "batch_launch": launch["best"], "batch_groups": groups["best"],
+           "poll_period": poll["best"], "spmv_unroll": unroll["best"], "threads": thr["best"],
+           "tables": {"apply_items_per_warp_ms": ipw["ms"], "batch_groups_ms": groups["ms"],
+                      "batch_launch_ms": launch["ms"], "poll_period_ms": poll["ms"], "spmv_unroll_ms": unroll["ms"],
+                      "threads_ms": thr["ms"]}}
     cache[key] = res
     _store_cache(cache_path, cache)
     return dict(res, cached=False)

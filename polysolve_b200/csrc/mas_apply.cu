@@ -1711,19 +1711,18 @@ namespace pmas
         return grid > 0 ? grid : 0;
     }
 
-    // At least APPLY_ITEMS_PER_WARP items per warp: a warp's two-stage copy pipeline then runs a
-    // few items past its start-up latency (small systems, and the batched launch where the
-    // CTAs of many small systems share the SMs one after another).
-    constexpr int APPLY_ITEMS_PER_WARP = 4;
-
+    // At least apply_items_per_warp() items per warp (1 by default: the most CTAs, the lowest
+    // latency for a lone solve). In batches of small systems more items per warp measured
+    // faster: a warp's two-stage copy pipeline runs past its start-up latency, and fewer SMs are
+    // held by one system's apply while other systems' kernels run.
     int mas_apply_grid(const MasView &mas)
     {
         return dispatch(mas.bd, mas.storage, [&]<int BD, class Store>() {
             using L = ApplyLayout<BD, Store>;
             const int sms = device_sm_count();
             const int items = mas.banks + mas.n_coarse_active;
-            constexpr int PER_CTA = L::WARPS * APPLY_ITEMS_PER_WARP;
-            int grid = (items + PER_CTA - 1) / PER_CTA;
+            const int per_cta = L::WARPS * apply_items_per_warp();
+            int grid = (items + per_cta - 1) / per_cta;
             if (grid > sms)
                 grid = sms;
             return grid < 1 ? 1 : grid;

@@ -81,6 +81,9 @@ namespace
         // CUDA stream per system driven by host threads (streams, measured faster on the
         // 64-system workload: 37.7-37.9 against 38.2-38.4 ms per batch).
         bool batch_fused = false;
+        // Minimum items per warp of the MAS apply (a launch shape for the autotuner: 1 suits a
+        // lone solve, more suits batches of small systems).
+        int apply_ipw = 1;
         // Fused groups of a batch, each on its own stream (systems split by size into groups of
         // about equal work); 0 = automatic (1, measured best).
         int batch_groups = 0;
@@ -133,7 +136,7 @@ namespace
                                 "true_residual_period", "check_period", "initial_guess", "beta", "ordering",
                                 "poll_period", "profile_kernels", "cuda_graphs", "preconditioner_refresh",
                                 "device_wait_limit", "rhs_group", "chained_launch", "wide_apply", "spmv_unroll",
-                                "batch_launch", "batch_groups"};
+                                "batch_launch", "batch_groups", "apply_items_per_warp"};
 
     // MASSolverImpl::set_parameters (MASSolver.cu:198-212) plus the extension keys.
     void apply_mas_params(Params &p, const Json &m, bool strict)
@@ -232,6 +235,12 @@ namespace
             if (w != "fused" && w != "streams")
                 throw Error(ERR_INVALID, "[MAS] batch_launch must be \"fused\" or \"streams\"");
             q.batch_fused = (w == "fused");
+        }
+        if (auto *v = m.find("apply_items_per_warp"))
+        {
+            q.apply_ipw = get_int(*v, "apply_items_per_warp");
+            if (q.apply_ipw < 1 || q.apply_ipw > 64)
+                throw Error(ERR_INVALID, "[MAS] apply_items_per_warp must be 1 to 64");
         }
         if (auto *v = m.find("batch_groups"))
         {
@@ -921,6 +930,7 @@ struct mas_solver
         mix((uint64_t)cfg.wait_limit);
         mix((uint64_t)chained_launch());
         mix((uint64_t)spmv_unroll());
+        mix((uint64_t)apply_items_per_warp());
         uint64_t bits;
         std::memcpy(&bits, &cfg.rel_tol, 8);
         mix(bits);
@@ -956,6 +966,7 @@ struct mas_solver
         keep_stats = false;
         set_chained_launch(p.chained);
         set_spmv_unroll(p.spmv_unroll);
+        set_apply_items_per_warp(p.apply_ipw);
         launch_pcg_init_state(S, stream);
         // r = b - A x, rr0, the level-0 restriction of r, then z = M^-1 r
         run("spmv_residual", 1, [&] { launch_spmv(SPMV_RESIDUAL, Av, x.get(), r.get(), b.get(), S, red(), 0, 0, stream); });
@@ -2166,6 +2177,7 @@ namespace
             max_iter = std::max(max_iter, h->p.max_iter);
         set_spmv_unroll(p0.spmv_unroll);
         set_chained_launch(p0.chained);
+        set_apply_items_per_warp(p0.apply_ipw);
         std::unique_ptr<FusedBatch> fb;
         {
             std::lock_guard<std::mutex> lock(g_fused_mu);
@@ -2276,11 +2288,13 @@ namespace
             if (!h->batch_fusable() || h->device != handles[0]->device || h->bd != handles[0]->bd ||
                 h->mas.storage != handles[0]->mas.storage || h->p.true_residual_period != p0.true_residual_period ||
                 h->p.poll_period != p0.poll_period || h->p.spmv_unroll != p0.spmv_unroll ||
-                h->p.batch_groups != p0.batch_groups || h->p.chained != p0.chained)
+                h->p.batch_groups != p0.batch_groups || h->p.chained != p0.chained ||
+                h->p.apply_ipw != p0.apply_ipw)
                 return false;
         }
         const int dev = handles[0]->device;
         cuda_check(cudaSetDevice(dev), "set device");
+        set_apply_items_per_warp(p0.apply_ipw); // the apply grids below are the handles' own
         // Input steps; systems whose input is rejected keep their error and leave the batch.
         std::vector<cudaEvent_t> ready((size_t)count, nullptr);
         parallel_for(count, workers, [&](int i) {

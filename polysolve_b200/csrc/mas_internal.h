@@ -381,6 +381,10 @@ namespace pmas
     // Slots per loop trip of the single-right-hand-side SpMV (1, 2 or 4); per calling thread.
     void set_spmv_unroll(int u);
     int spmv_unroll();
+    // Minimum items per warp of the single-right-hand-side MAS apply of the calling thread (its
+    // grid: min(SMs, items / (warps per CTA * this))); the apply_items_per_warp parameter.
+    void set_apply_items_per_warp(int k);
+    int apply_items_per_warp();
 
     // mas_spmv.cu
     enum SpmvMode : int

@@ -75,6 +75,9 @@ namespace pmas
     static thread_local int t_spmv_unroll = 2;
     void set_spmv_unroll(int u) { t_spmv_unroll = u; }
     int spmv_unroll() { return t_spmv_unroll; }
+    static thread_local int t_apply_ipw = 1;
+    void set_apply_items_per_warp(int k) { t_apply_ipw = k < 1 ? 1 : k; }
+    int apply_items_per_warp() { return t_apply_ipw; }
 
     namespace
     {

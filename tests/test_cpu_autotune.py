@@ -60,8 +60,8 @@ def test_cached_result_sets_both_parameters(tmp_path, monkeypatch):
     res = autotune.tune_batch(solvers, [0, 0], [0, 0], ns, cache_path=str(path))
     assert res["cached"] and res["threads"] == 8
     # an entry without batch_launch (older cache) restores the defaults
-    assert all(s.params == {"poll_period": 40, "spmv_unroll": 1, "batch_launch": "streams", "batch_groups": 0}
-               for s in solvers)
+    assert all(s.params == {"poll_period": 40, "spmv_unroll": 1, "batch_launch": "streams", "batch_groups": 0,
+                            "apply_items_per_warp": 1} for s in solvers)
 
 
 def test_batch_launch_picks_the_fastest_and_leaves_it_set():

@@ -195,3 +195,26 @@ def test_fused_batch_device_pointers_match_host_arrays(systems):
     torch.cuda.synchronize()
     for a, t in zip(host, dx):
         np.testing.assert_array_equal(a, t.cpu().numpy())
+
+
+def test_apply_items_per_warp_batches_match_single_solves(systems):
+    """apply_items_per_warp (a launch shape: fewer, longer-lived apply CTAs) changes the apply's
+    grid and so the grouping of its dot products; single solves, fused and stream batches with the
+    same setting agree bit for bit, and every setting meets the tolerance."""
+    bs = [synthetic.rhs(s.n, seed=110 + k) for k, s in enumerate(systems)]
+    base = [_single(_solver(s), b)[0] for s, b in zip(systems, bs)]
+    for ipw in (2, 4, 8):
+        solvers = [_solver(s, dict(FUSED, apply_items_per_warp=ipw)) for s in systems]
+        ref = [_single(s, b) for s, b in zip(solvers, bs)]
+        fused = [x.copy() for x in solve_batch(solvers, bs)]
+        for s in solvers:
+            s.set_parameters({"MAS": {"batch_launch": "streams"}})
+        streams = solve_batch(solvers, bs)
+        for (xr, it, _, _), xf, xs, x1, sysm, b in zip(ref, fused, streams, base, systems, bs):
+            np.testing.assert_array_equal(xf, xr)
+            np.testing.assert_array_equal(xs, xr)
+            A = sysm.scipy()
+            assert np.linalg.norm(A @ xr - b) <= 5e-8 * np.linalg.norm(b)
+            assert np.linalg.norm(xr - x1) <= 1e-6 * np.linalg.norm(x1)
+    with pytest.raises(MasError):
+        solvers[0].set_parameters({"MAS": {"apply_items_per_warp": 0}})
