@@ -1732,14 +1732,60 @@ struct mas_solver
         return factorized && p.batch_fused && p.graphs && !p.profile && !learned_active() && p.max_iter >= 1;
     }
 
+    // Byte-comparable (a fused batch's kept tables are matched by memcmp): every padding byte zero.
     BatchSystem batch_system()
     {
         BatchSystem s;
         std::memset(&s, 0, sizeof(s));
-        s.A = A.view();
-        s.mas = mas.view();
-        s.cfg = config();
-        s.red = red();
+        const BankedView av = A.view();
+        s.A.bd = av.bd;
+        s.A.banks = av.banks;
+        s.A.slice = av.slice;
+        s.A.rowlen = av.rowlen;
+        s.A.cols = av.cols;
+        s.A.vals = av.vals;
+        const MasView mv = mas.view();
+        static_assert(sizeof(MasView) == 248, "a MasView member was added: copy it below as well");
+        MasView &m = s.mas; // member by member into the zeroed record
+        m.bd = mv.bd;
+        m.banks = mv.banks;
+        m.level_num = mv.level_num;
+        m.total_coarse = mv.total_coarse;
+        std::copy(mv.coff, mv.coff + MAX_COARSE, m.coff);
+        std::copy(mv.mat_offsets, mv.mat_offsets + LEVELS, m.mat_offsets);
+        std::copy(mv.mat_counts, mv.mat_counts + LEVELS, m.mat_counts);
+        std::copy(mv.cco_nums, mv.cco_nums + MAX_COARSE, m.cco_nums);
+        m.storage = mv.storage;
+        m.first_iso_bank = mv.first_iso_bank;
+        std::copy(mv.real_count, mv.real_count + MAX_COARSE, m.real_count);
+        m.n_coarse_active = mv.n_coarse_active;
+        m.coarse_active = mv.coarse_active;
+        m.inv = mv.inv;
+        m.inv_scale = mv.inv_scale;
+        m.lcco0 = mv.lcco0;
+        m.cco0_base = mv.cco0_base;
+        m.cslot = mv.cslot;
+        m.parent = mv.parent;
+        m.ticket = mv.ticket;
+        std::copy(mv.kid_ptr, mv.kid_ptr + MAX_COARSE, m.kid_ptr);
+        m.kids = mv.kids;
+        m.identity = mv.identity;
+        m.rc = mv.rc;
+        m.zc = mv.zc;
+        const PcgConfig cf = config();
+        s.cfg.max_iter = cf.max_iter;
+        s.cfg.rel_tol = cf.rel_tol;
+        s.cfg.abs_tol = cf.abs_tol;
+        s.cfg.use_prec_norm = cf.use_prec_norm;
+        s.cfg.check_period = cf.check_period;
+        s.cfg.polak_ribiere = cf.polak_ribiere;
+        s.cfg.level_num = cf.level_num;
+        s.cfg.wait_limit = cf.wait_limit;
+        const ReduceBuf rb = red();
+        s.red.partials = rb.partials;
+        s.red.capacity = rb.capacity;
+        s.red.rr_parts = rb.rr_parts;
+        s.red.rz_parts = rb.rz_parts;
         s.st = st.get();
         s.x = x.get();
         s.r = r.get();
