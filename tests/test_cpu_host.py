@@ -63,6 +63,15 @@ def test_create_json_rejects_bad_params_before_device():
         Solver.create({"solver": "AMGCL"})
 
 
+@pytest.mark.parametrize("key,bad", [("batch_launch", "persistent"), ("batch_groups", -1), ("batch_groups", 65),
+                                     ("apply_items_per_warp", 0), ("apply_items_per_warp", 65),
+                                     ("spmv_unroll", 3)])
+def test_launch_shape_parameters_are_validated_before_device(key, bad):
+    with pytest.raises(MasError) as e:
+        Solver.create({"solver": "MAS", "MAS": {key: bad}})
+    assert key in str(e.value)
+
+
 @pytest.mark.parametrize("N,kw", [(5, {}), (12, dict(young_sigma=1.0, jitter=0.2)),
                                   (16, dict(jitter=0.2, contact_pairs=200))])
 def test_morton_ordering_matches_restatement(N, kw):
