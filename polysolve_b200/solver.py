@@ -124,9 +124,12 @@ def library() -> ctypes.CDLL:
 
 def solve_batch(solvers: list, bs: list, xs: list | None = None, *, threads: int = 0) -> list:
     """New: solve independent factorized systems concurrently (``mas_solve_batch``): solver i
-    solves A_i x_i = b_i on its own CUDA stream, from a pool of host threads. bs / xs hold float64
-    numpy arrays (written in place; allocated when xs is None). Returns xs. Raises the first
-    failing solver's error; every solver's status stays readable through its ``get_info``."""
+    solves A_i x_i = b_i, on its own CUDA stream (``"batch_launch": "streams"``, the default) or
+    in fused launches, one per PCG phase for all systems of a size group (``"fused"``, results
+    bit-identical to single solves), with a pool of host threads for the per-system steps.
+    bs / xs hold float64 numpy arrays (written in place; allocated when xs is None). Returns xs.
+    Raises the first failing solver's error; every solver's status stays readable through its
+    ``get_info``."""
     count = len(solvers)
     if len(bs) != count or (xs is not None and len(xs) != count):
         raise ValueError("solvers, bs and xs must have the same length")
