@@ -283,9 +283,9 @@ namespace pmas
     // Level-0 restriction of one bank: reg[t] holds the bank's values t * 32 + lane (coalesced
     // layout); the values are regrouped by node with shuffles and summed per connected component
     // of the bank into rc (first coarse level). Every lane of the warp must call it.
+    // key = lcco0[bank * 32 + lane], base = cco0_base[bank], loaded by the caller (ahead of time).
     template <int BD>
-    __device__ __forceinline__ void bank_restrict(const double (&reg)[BD], int bank, const int *__restrict__ lcco0,
-                                                  const int *__restrict__ cco0_base, double *rc)
+    __device__ __forceinline__ void bank_restrict_keyed(const double (&reg)[BD], int key, int base, double *rc)
     {
         const int lane = threadIdx.x & 31;
         double rv[BD];
@@ -304,7 +304,15 @@ namespace pmas
             }
             rv[i] = v;
         }
-        warp_segment_store<BD>(rv, lcco0[(long long)bank * 32 + lane], cco0_base[bank], rc);
+        warp_segment_store<BD>(rv, key, base, rc);
+    }
+
+    template <int BD>
+    __device__ __forceinline__ void bank_restrict(const double (&reg)[BD], int bank, const int *__restrict__ lcco0,
+                                                  const int *__restrict__ cco0_base, double *rc)
+    {
+        const int lane = threadIdx.x & 31;
+        bank_restrict_keyed<BD>(reg, lcco0[(long long)bank * 32 + lane], cco0_base[bank], rc);
     }
 
     // ---------------------------------------------------------------------------------------

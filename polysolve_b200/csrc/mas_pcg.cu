@@ -105,40 +105,65 @@ namespace pmas
             const int total_warps = cta.n * (UPD_THREADS / 32);
             const bool restrict_r = !due && mas.level_num > 0;
             double part = 0.0;
-            for (int bank = cta.x * (UPD_THREADS / 32) + (threadIdx.x >> 5); bank < mas.banks; bank += total_warps)
-            {
+            // Two-stage pipeline over the warp's banks (one or two in the resident grid): the next
+            // bank's loads (x and p, or Ap and r, and its restriction keys) are issued before this
+            // bank's update and restriction. Same arithmetic in the same order as one bank at a time.
+            double na[BD], nb[BD];
+            int nkey = -1, nbase = 0;
+            auto load = [&](int bank) {
                 const long long b0 = (long long)bank * 32 * BD + lane;
-                // All loads of the bank first (one memory round trip), then the updates.
-                double xv[BD], pv[BD], av[BD], rv[BD];
 #pragma unroll
                 for (int t = 0; t < BD; ++t)
                 {
-                    xv[t] = pv[t] = av[t] = rv[t] = 0.0;
                     if (due)
                     {
-                        xv[t] = x[b0 + t * 32];
-                        pv[t] = p[b0 + t * 32];
+                        na[t] = x[b0 + t * 32];
+                        nb[t] = p[b0 + t * 32];
                     }
                     else
                     {
-                        av[t] = Ap[b0 + t * 32];
-                        rv[t] = r[b0 + t * 32];
+                        na[t] = Ap[b0 + t * 32];
+                        nb[t] = r[b0 + t * 32];
                     }
                 }
+                if (restrict_r && bank < mas.first_iso_bank)
+                {
+                    nkey = mas.lcco0[(long long)bank * 32 + lane];
+                    nbase = mas.cco0_base[bank];
+                }
+            };
+            const int first = cta.x * (UPD_THREADS / 32) + (threadIdx.x >> 5);
+            if (first < mas.banks)
+                load(first);
+            for (int bank = first; bank < mas.banks; bank += total_warps)
+            {
+                double av[BD], bv[BD];
 #pragma unroll
                 for (int t = 0; t < BD; ++t)
                 {
+                    av[t] = na[t];
+                    bv[t] = nb[t];
+                }
+                const int key = nkey, base = nbase;
+                if (bank + total_warps < mas.banks)
+                    load(bank + total_warps);
+                const long long b0 = (long long)bank * 32 * BD + lane;
+                double rv[BD];
+#pragma unroll
+                for (int t = 0; t < BD; ++t)
+                {
+                    rv[t] = 0.0;
                     if (due)
-                        x[b0 + t * 32] = fma(alpha, pv[t], xv[t]);
+                        x[b0 + t * 32] = fma(alpha, bv[t], av[t]);
                     else
                     {
-                        rv[t] = fma(-alpha, av[t], rv[t]);
+                        rv[t] = fma(-alpha, av[t], bv[t]);
                         r[b0 + t * 32] = rv[t];
                         part = fma(rv[t], rv[t], part);
                     }
                 }
                 if (restrict_r && bank < mas.first_iso_bank)
-                    bank_restrict<BD>(rv, bank, mas.lcco0, mas.cco0_base, mas.rc);
+                    bank_restrict_keyed<BD>(rv, key, base, mas.rc);
             }
             pdl_release();
             if (due)
