@@ -74,3 +74,39 @@ def test_batch_launch_picks_the_fastest_and_leaves_it_set():
     res = autotune.tune_batch_launch(solvers, run, repeats=2)
     assert res["best"] == "fused" and set(res["ms"]) == {"fused", "streams"}
     assert all(s.params["batch_launch"] == "fused" for s in solvers)
+
+
+def test_tune_batch_searches_every_shape_and_caches(tmp_path, monkeypatch):
+    """The whole batch search with stand-in solvers: each parameter is searched with the earlier
+    choices in place, the fastest values are left set, and the result is cached by sizes."""
+    from polysolve_b200 import solver as solver_mod
+
+    solvers = [FakeSolver(), FakeSolver()]
+    best = {"apply_items_per_warp": 4, "batch_groups": 2, "batch_launch": "fused", "poll_period": 20,
+            "spmv_unroll": 1}
+    calls = []
+
+    def fake_batch(svs, bp, xp, ns, threads=0):
+        p = svs[0].params
+        calls.append(dict(p, threads=threads))
+        miss = sum(1 for k, v in best.items() if k in p and p[k] != v)
+        time.sleep(0.001 + 0.002 * miss + 0.001 * abs(threads - 8) / 8)
+
+    monkeypatch.setattr(solver_mod, "solve_batch_device", fake_batch)
+    path = tmp_path / "tune.json"
+    res = autotune.tune_batch(solvers, [0, 0], [0, 0], [10, 20], cache_path=str(path), repeats=2,
+                              thread_candidates=(1, 2, 8))
+    assert not res["cached"]
+    for k, v in best.items():
+        assert res[k] == v
+        assert all(s.params[k] == v for s in solvers)
+    # thread counts above the number of systems are not tried
+    assert res["threads"] == 2 and set(res["tables"]["threads_ms"]) == {1, 2}
+    assert set(res["tables"]) == {"apply_items_per_warp_ms", "batch_groups_ms", "batch_launch_ms", "poll_period_ms",
+                                  "spmv_unroll_ms", "threads_ms"}
+    # group counts above the number of systems are not tried, and they are timed in the fused form
+    assert set(res["tables"]["batch_groups_ms"]) == {1, 2}
+    assert any(c.get("batch_launch") == "fused" and c.get("batch_groups") == 2 for c in calls)
+    fresh = [FakeSolver(), FakeSolver()]
+    again = autotune.tune_batch(fresh, [0, 0], [0, 0], [20, 10], cache_path=str(path))
+    assert again["cached"] and all(s.params["batch_launch"] == "fused" and s.params["batch_groups"] == 2 for s in fresh)
